@@ -1,0 +1,360 @@
+"""Python host side of libbcgpu: exact betweenness centrality on one B200.
+
+Thin ctypes layer over the C ABI in include/bcgpu.h and include/bchost.h; all
+computation happens in libbcgpu.so (C++ host decomposition + sm_100a CUDA
+kernels). There is no CPU fallback: if the library or a CUDA device is missing,
+the calls raise.
+
+Mirrors the reference's interfaces (Goutam363/centrality-GPU):
+  * ``betc`` CLI                                -> lib/betc, ``betweenness``
+  * Graph(char*) edge-list input                -> ``Graph.load``
+  * begin_gpu free overload   (Codes/begin_gpupgm.cu:42-71)   -> ``begin_gpu_free``
+  * begin_gpu active overload (Codes/begin_gpupgm.cu:73-89)   -> ``begin_gpu_active``
+  * BiCC::to_eargraph loop    (Codes/to_eargraph_construct.cpp:54-200) -> ``Context.run``
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "lib" / "libbcgpu.so"
+BETC_PATH = _PKG / "lib" / "betc"
+
+OK, EINVAL, ECUDA, ENOMEM, ETIMEOUT, EIO, EOVERFLOW = range(7)
+MODE_PLAIN, MODE_BATCHED = 0, 1
+DELTA_FP64, DELTA_FP32C = 0, 1
+_ERRNAMES = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ETIMEOUT", 5: "EIO", 6: "EOVERFLOW"}
+
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
+
+
+class BcOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
+                ("stream", C.c_void_p), ("workspace_limit", C.c_int64)]
+
+
+class BcBccs(C.Structure):
+    _fields_ = [("n_bcc", C.c_int32), ("n_orig", C.c_int32), ("n_packed", C.c_int64), ("n_arcs", C.c_int64),
+                ("n_chains", C.c_int64), ("vtx_off", _i64p), ("row", _i64p), ("col", _i32p), ("reach", _i32p),
+                ("orig", _i32p), ("n_plain", _i32p), ("chain_off", _i64p), ("chain_start", _i32p),
+                ("chain_len", _i32p), ("chain_l", _i32p), ("chain_r", _i32p), ("art", _f64p)]
+
+
+class BcStats(C.Structure):
+    _fields_ = [("sources", C.c_int64), ("bfs_sources", C.c_int64), ("aux_bfs", C.c_int64), ("teps_edges", C.c_int64),
+                ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_int32),
+                ("batch_width", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BcDecompInfo(C.Structure):
+    _fields_ = [("n_components", C.c_int32), ("n_bcc_all", C.c_int32), ("n_bcc_packed", C.c_int32),
+                ("n_articulation", C.c_int32), ("n_chain_vertices", C.c_int64), ("n_chains", C.c_int64),
+                ("n_cycle_bccs", C.c_int64), ("host_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every symbol the C headers declare, with its ctypes signature.
+_SIGS = {
+    "bc_default_opts": (None, [C.POINTER(BcOpts)]),
+    "bc_create": (C.c_int, [C.POINTER(BcOpts), C.POINTER(C.c_void_p)]),
+    "bc_destroy": (None, [C.c_void_p]),
+    "bc_last_error": (C.c_char_p, [C.c_void_p]),
+    "bc_run_bccs": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), _f64p, C.POINTER(BcStats)]),
+    "bc_begin_free": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, _i32p, _f32p,
+                                _f64p]),
+    "bc_begin_active": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, C.c_int32,
+                                  _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f64p]),
+    "bc_plan_create": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), C.POINTER(C.c_void_p)]),
+    "bc_plan_destroy": (None, [C.c_void_p]),
+    "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
+    "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p]),
+    "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "bc_plan_reset": (C.c_int, [C.c_void_p]),
+    "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
+    "bc_plan_read": (C.c_int, [C.c_void_p, _f64p]),
+    "bc_plan_source_rows": (C.c_int, [C.c_void_p, C.c_int64, _i32p, _f64p]),
+    "bc_graph_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "bc_graph_from_edges": (C.c_int, [C.c_int32, C.c_int64, _i32p, _i32p, C.POINTER(C.c_void_p)]),
+    "bc_graph_free": (None, [C.c_void_p]),
+    "bc_graph_csr": (C.c_int, [C.c_void_p, _i32p, _i64p, C.POINTER(_i64p), C.POINTER(_i32p)]),
+    "bc_decompose": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bc_decomp_free": (None, [C.c_void_p]),
+    "bc_decomp_view": (C.POINTER(BcBccs), [C.c_void_p]),
+    "bc_decomp_get_info": (None, [C.c_void_p, C.POINTER(BcDecompInfo)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libbcgpu.so (built in-tree by build.py). Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"libbcgpu.so not built ({LIB_PATH}); run centrality-gpu_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class BcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Graph:
+    """Simple undirected graph (loops dropped, duplicates merged) in CSR."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = lib().bc_graph_load(str(path).encode(), C.byref(h), err, 512)
+        if rc:
+            raise BcError(rc, err.value.decode())
+        return cls(h.value)
+
+    @classmethod
+    def from_edges(cls, n, u, v):
+        u, v = _i32(u), _i32(v)
+        h = C.c_void_p()
+        rc = lib().bc_graph_from_edges(int(n), len(u), _ptr(u, _i32p), _ptr(v, _i32p), C.byref(h))
+        if rc:
+            raise BcError(rc, "bc_graph_from_edges")
+        return cls(h.value)
+
+    def csr(self):
+        n = C.c_int32()
+        m = C.c_int64()
+        row = _i64p()
+        col = _i32p()
+        lib().bc_graph_csr(self._h, C.byref(n), C.byref(m), C.byref(row), C.byref(col))
+        r = np.ctypeslib.as_array(row, shape=(n.value + 1,)).copy()
+        c = np.ctypeslib.as_array(col, shape=(max(m.value, 1),))[: m.value].copy() if m.value else np.zeros(0, np.int32)
+        return n.value, r, c
+
+    def close(self):
+        if self._h:
+            lib().bc_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _arr(ptr, count, dtype):
+    if count == 0 or not ptr:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(count,)).copy()
+
+
+class Decomposition:
+    """BCC split + reach + articulation terms + degree-2 chains (bc_decompose)."""
+
+    def __init__(self, graph: Graph):
+        self._graph = graph
+        h = C.c_void_p()
+        rc = lib().bc_decompose(graph._h, C.byref(h))
+        if rc:
+            raise BcError(rc, "bc_decompose")
+        self._h = h
+        self.view = lib().bc_decomp_view(h)
+        info = BcDecompInfo()
+        lib().bc_decomp_get_info(h, C.byref(info))
+        self.info = info.as_dict()
+
+    def arrays(self):
+        """Copies of the packed arrays as numpy (for tests and tools)."""
+        V = self.view.contents
+        nb, npk, na, nc = V.n_bcc, V.n_packed, V.n_arcs, V.n_chains
+        return {
+            "n_bcc": nb, "n_orig": V.n_orig, "n_packed": npk, "n_arcs": na, "n_chains": nc,
+            "vtx_off": _arr(V.vtx_off, nb + 1, np.int64), "row": _arr(V.row, npk + 1, np.int64),
+            "col": _arr(V.col, na, np.int32), "reach": _arr(V.reach, npk, np.int32),
+            "orig": _arr(V.orig, npk, np.int32), "n_plain": _arr(V.n_plain, nb, np.int32),
+            "chain_off": _arr(V.chain_off, nb + 1, np.int64), "chain_start": _arr(V.chain_start, nc, np.int32),
+            "chain_len": _arr(V.chain_len, nc, np.int32), "chain_l": _arr(V.chain_l, nc, np.int32),
+            "chain_r": _arr(V.chain_r, nc, np.int32), "art": _arr(V.art, V.n_orig, np.float64),
+        }
+
+    def close(self):
+        if self._h:
+            lib().bc_decomp_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One CUDA device and stream (bc_create)."""
+
+    def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
+                 workspace_limit=0):
+        o = BcOpts()
+        lib().bc_default_opts(C.byref(o))
+        o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
+        o.stream = stream
+        o.workspace_limit = workspace_limit
+        h = C.c_void_p()
+        rc = lib().bc_create(C.byref(o), C.byref(h))
+        if rc:
+            raise BcError(rc, lib().bc_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc:
+            raise BcError(rc, lib().bc_last_error(self._h).decode())
+
+    def run(self, decomp: Decomposition):
+        """All sources of all BCCs, host buffers in and out. Returns (bc, stats)."""
+        out = np.zeros(decomp.view.contents.n_orig, dtype=np.float64)
+        st = BcStats()
+        self._check(lib().bc_run_bccs(self._h, decomp.view, _ptr(out, _f64p), C.byref(st)))
+        return out, st.as_dict()
+
+    def plan(self, decomp: Decomposition):
+        return Plan(self, decomp)
+
+    def close(self):
+        if self._h:
+            lib().bc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """Device-resident packed BCCs + BC accumulator (bc_plan_*)."""
+
+    def __init__(self, ctx: Context, decomp: Decomposition):
+        self.ctx = ctx
+        self.decomp = decomp
+        h = C.c_void_p()
+        ctx._check(lib().bc_plan_create(ctx._h, decomp.view, C.byref(h)))
+        self._h = h
+        self.n_units = lib().bc_plan_num_units(h)
+        self.device_bytes = lib().bc_plan_device_bytes(h)
+
+    def unit_work(self, begin=0, end=None):
+        end = self.n_units if end is None else end
+        s = C.c_int64()
+        t = C.c_int64()
+        self.ctx._check(lib().bc_plan_unit_work(self._h, begin, end, C.byref(s), C.byref(t)))
+        return s.value, t.value
+
+    def reset(self):
+        self.ctx._check(lib().bc_plan_reset(self._h))
+
+    def run(self, begin=0, end=None, stats=True):
+        end = self.n_units if end is None else end
+        st = BcStats() if stats else None
+        self.ctx._check(lib().bc_plan_run(self._h, begin, end, C.byref(st) if stats else None))
+        return st.as_dict() if stats else None
+
+    def read(self):
+        out = np.zeros(self.decomp.view.contents.n_orig, dtype=np.float64)
+        self.ctx._check(lib().bc_plan_read(self._h, _ptr(out, _f64p)))
+        return out
+
+    def source_rows(self, packed, nb):
+        d = np.zeros(nb, dtype=np.int32)
+        s = np.zeros(nb, dtype=np.float64)
+        self.ctx._check(lib().bc_plan_source_rows(self._h, int(packed), _ptr(d, _i32p), _ptr(s, _f64p)))
+        return d, s
+
+    def close(self):
+        if self._h:
+            lib().bc_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def betweenness(n, u, v, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1):
+    """Exact BC (ordered pairs, FP64) of the graph given by edges (u, v)."""
+    g = Graph.from_edges(n, u, v)
+    d = Decomposition(g)
+    ctx = Context(mode=mode, delta=delta, batch_width=batch_width, device=device)
+    bc, st = ctx.run(d)
+    ctx.close()
+    return bc, st, d.info
+
+
+def begin_gpu_free(ctx: Context, R, Cc, n, m, req_nodes, artnodes, bc, time_s=0.0):
+    """Mirror of the reference's free-source begin_gpu: bc (float32, length n)
+    is overwritten; returns the accumulated device seconds."""
+    R, Cc, req, reach = _i32(R), _i32(Cc), _i32(req_nodes), _i32(artnodes)
+    assert bc.dtype == np.float32 and bc.flags.c_contiguous
+    t = C.c_double(time_s)
+    ctx._check(lib().bc_begin_free(ctx._h, _ptr(R, _i32p), _ptr(Cc, _i32p), int(n), int(m), _ptr(req, _i32p), len(req),
+                                   _ptr(reach, _i32p), _ptr(bc, _f32p), C.byref(t)))
+    return t.value
+
+
+def begin_gpu_active(ctx: Context, R, Cc, n, m, active, ears, artnodes, bc, time_s=0.0):
+    """Mirror of the reference's active/chain begin_gpu. ``ears``: list of
+    (lnode, rnode, [(ld, node, rd), ...]). bc (float32) is added to."""
+    R, Cc, act, reach = _i32(R), _i32(Cc), _i32(active), _i32(artnodes)
+    ln = _i32([e[0] for e in ears])
+    rn = _i32([e[1] for e in ears])
+    cnt = _i32([len(e[2]) for e in ears])
+    off = _i32(np.concatenate(([0], np.cumsum(cnt)[:-1])) if len(ears) else [])
+    flat = [x for e in ears for x in e[2]]
+    ld = _i32([x[0] for x in flat])
+    nodes = _i32([x[1] for x in flat])
+    rd = _i32([x[2] for x in flat])
+    assert bc.dtype == np.float32 and bc.flags.c_contiguous
+    t = C.c_double(time_s)
+    ctx._check(lib().bc_begin_active(ctx._h, _ptr(R, _i32p), _ptr(Cc, _i32p), int(n), int(m), _ptr(act, _i32p),
+                                     len(act), len(ears), _ptr(ln, _i32p), _ptr(rn, _i32p), _ptr(cnt, _i32p),
+                                     _ptr(off, _i32p), _ptr(nodes, _i32p), _ptr(ld, _i32p), _ptr(rd, _i32p),
+                                     _ptr(reach, _i32p), _ptr(bc, _f32p), C.byref(t)))
+    return t.value
+
+
+def declared_symbols():
+    """Names of every function declared in include/*.h."""
+    return sorted(_SIGS)

@@ -1,0 +1,35 @@
+// Host-visible interface of the BATCHED schedule (kernels_batched.cu).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "bcgpu.h"
+
+namespace bcg {
+
+struct BatchedConfig {
+  int width = 0;            // sources per pass (multiple of 32); 0 = choose
+  bool delta_fp32c = true;  // FP32 two-sum compensated dependencies (else FP64)
+  int sms = 148;
+  int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
+};
+
+struct BatchedPlan;
+
+// Builds the passes (host scheduling) and allocates device workspace. The
+// device pointers are owned by the caller and must outlive the plan.
+int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row, const int32_t *col,
+                   const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
+                   const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
+                   BatchedPlan **out, std::string *msg);
+void batched_destroy(BatchedPlan *p);
+int64_t batched_device_bytes(const BatchedPlan *p);
+int batched_width(const BatchedPlan *p);
+// Prefix sums over passes of sources, TEPS arcs, BFS sources and aux BFS runs.
+void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std::vector<int64_t> &teps,
+                       std::vector<int64_t> &bfs, std::vector<int64_t> &aux);
+int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream, int *launches, std::string *msg);
+
+}  // namespace bcg

@@ -1,0 +1,659 @@
+// libbcgpu context, plans and the C ABI of include/bcgpu.h.
+//
+// A plan uploads the packed BCCs once (the reference copies CSR, reach and
+// per-source scratch to the device and frees it again inside every begin_gpu
+// call, Codes/kernels_free.cu:40-101, Codes/kernels_active.cu:67-211), keeps
+// the BC accumulator on the device in FP64 (the reference accumulates FP32,
+// Codes/kernels_free.cu:425) and splits the sources into work units that can
+// be run in any ranges.
+#include "bcgpu.h"
+#include "batched.h"
+#include "common.cuh"
+#include "plain.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+struct bc_ctx {
+  bc_opts opts{};
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct bc_plan {
+  bc_ctx *ctx = nullptr;
+  int mode = BCGPU_MODE_PLAIN;
+  // host copies needed to read results
+  int32_t n_orig = 0;
+  int64_t n_packed = 0;
+  std::vector<int32_t> orig;
+  std::vector<double> art;
+  std::vector<int64_t> h_vtx_off, h_chain_off;
+  std::vector<int32_t> h_n_plain, h_chain_start, h_chain_len;
+  // device graph
+  int64_t *row = nullptr, *vtx_off = nullptr;
+  int32_t *col = nullptr, *reach = nullptr, *chain_start = nullptr, *chain_len = nullptr, *chain_l = nullptr,
+          *chain_r = nullptr;
+  double *bc = nullptr;
+  int *err = nullptr;
+  unsigned long long *counter = nullptr;
+  // PLAIN
+  bcg::PlainItem *items = nullptr;
+  int64_t n_items = 0;
+  int32_t *ws_i = nullptr, *epochs = nullptr;
+  double *ws_f = nullptr;
+  int64_t ws_n = 0;
+  int grid = 0;
+  // BATCHED
+  bcg::BatchedPlan *bp = nullptr;
+  // per-unit work (prefix sums over units)
+  std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux;
+  int64_t device_bytes = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+thread_local std::string g_create_err;
+
+int fail(bc_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  else g_create_err = msg;
+  return code;
+}
+
+int cuda_fail(bc_ctx *ctx, cudaError_t e, const char *what) {
+  cudaGetLastError();  // clear a sticky launch error of the calling thread
+  return fail(ctx, e == cudaErrorMemoryAllocation ? BCGPU_ENOMEM : BCGPU_ECUDA,
+              std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define CK(ctx, call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+template <typename T>
+int dalloc(bc_plan *p, T **ptr, int64_t count) {
+  size_t bytes = sizeof(T) * (size_t)std::max<int64_t>(count, 1);
+  cudaError_t e = cudaMalloc((void **)ptr, bytes);
+  if (e != cudaSuccess) return cuda_fail(p->ctx, e, "cudaMalloc");
+  p->allocs.push_back(*ptr);
+  p->device_bytes += (int64_t)bytes;
+  return BCGPU_OK;
+}
+
+template <typename T>
+int upload(bc_plan *p, T **ptr, const T *src, int64_t count) {
+  int rc = dalloc(p, ptr, count);
+  if (rc) return rc;
+  if (count > 0) CK(p->ctx, cudaMemcpyAsync(*ptr, src, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, p->ctx->stream));
+  return BCGPU_OK;
+}
+
+const char *dev_err_text(int code) {
+  switch (code) {
+    case bcg::kDevDisconnected: return "a BCC is not connected (row did not reach every vertex)";
+    case bcg::kDevWorkspace: return "BCC larger than the kernel workspace";
+    case bcg::kDevTimeout: return "device-side wait exceeded its iteration limit";
+    case bcg::kDevBadItem: return "work item references data out of range";
+    default: return "unknown device error";
+  }
+}
+
+int check_dev_err(bc_plan *p) {
+  int h = 0;
+  CK(p->ctx, cudaMemcpyAsync(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream));
+  CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  if (h != bcg::kDevOk)
+    return fail(p->ctx, h == bcg::kDevTimeout ? BCGPU_ETIMEOUT : BCGPU_EINVAL, dev_err_text(h));
+  return BCGPU_OK;
+}
+
+// Structural checks of the packed input (the kernels trust these).
+int validate(bc_ctx *ctx, const bc_bccs *B) {
+  if (!B || B->n_bcc < 0 || B->n_orig < 0) return fail(ctx, BCGPU_EINVAL, "null or negative bccs");
+  if (B->n_bcc > 0 && (!B->vtx_off || !B->row || !B->col || !B->reach || !B->orig || !B->n_plain || !B->chain_off))
+    return fail(ctx, BCGPU_EINVAL, "missing bccs array");
+  if (B->n_bcc == 0) return BCGPU_OK;
+  if (B->vtx_off[0] != 0 || B->vtx_off[B->n_bcc] != B->n_packed || B->row[0] != 0 || B->row[B->n_packed] != B->n_arcs ||
+      B->chain_off[0] != 0 || B->chain_off[B->n_bcc] != B->n_chains)
+    return fail(ctx, BCGPU_EINVAL, "inconsistent bccs totals");
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+    if (nb < 3 || nb > INT32_MAX - 4) return fail(ctx, BCGPU_EINVAL, "BCC size out of range");
+    if (B->n_plain[b] < 1 || B->n_plain[b] > nb) return fail(ctx, BCGPU_EINVAL, "n_plain out of range");
+    int64_t ch = 0;
+    for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) {
+      if (B->chain_start[c] < B->n_plain[b] || B->chain_len[c] < 1 || B->chain_start[c] + B->chain_len[c] > nb ||
+          B->chain_l[c] < 0 || B->chain_l[c] >= B->n_plain[b] || B->chain_r[c] < 0 || B->chain_r[c] >= B->n_plain[b])
+        return fail(ctx, BCGPU_EINVAL, "chain out of range");
+      if (c > B->chain_off[b] && B->chain_l[c] < B->chain_l[c - 1])
+        return fail(ctx, BCGPU_EINVAL, "chains must be sorted by left endpoint");
+      ch += B->chain_len[c];
+    }
+    if (ch != nb - B->n_plain[b]) return fail(ctx, BCGPU_EINVAL, "chain vertices do not cover the non-plain ids");
+    for (int64_t k = B->vtx_off[b]; k < B->vtx_off[b + 1]; ++k) {
+      if (B->orig[k] < 0 || B->orig[k] >= B->n_orig || B->reach[k] < 0)
+        return fail(ctx, BCGPU_EINVAL, "orig/reach out of range");
+      if (B->row[k + 1] < B->row[k]) return fail(ctx, BCGPU_EINVAL, "row offsets decrease");
+    }
+  }
+  for (int64_t e = 0; e < B->n_arcs; ++e)
+    if (B->col[e] < 0) return fail(ctx, BCGPU_EINVAL, "negative column id");
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+    for (int64_t e = B->row[B->vtx_off[b]]; e < B->row[B->vtx_off[b + 1]]; ++e)
+      if (B->col[e] >= nb) return fail(ctx, BCGPU_EINVAL, "column id outside its BCC");
+  }
+  return BCGPU_OK;
+}
+
+void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items) {
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    int64_t c = B->chain_off[b];
+    const int64_t ce = B->chain_off[b + 1];
+    for (int32_t s = 0; s < B->n_plain[b]; ++s) {
+      int64_t c0 = c;
+      while (c < ce && B->chain_l[c] == s) ++c;
+      items.push_back({b, s, (int32_t)c0, (int32_t)c});
+    }
+  }
+}
+
+int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan **out) {
+  int rc = validate(ctx, B);
+  if (rc) return rc;
+  CK(ctx, cudaSetDevice(ctx->device));
+  bc_plan *p = new (std::nothrow) bc_plan;
+  if (!p) return fail(ctx, BCGPU_ENOMEM, "host allocation");
+  p->ctx = ctx;
+  p->mode = ctx->opts.mode;
+  auto bail = [&](int code) {
+    bc_plan_destroy(p);
+    return code;
+  };
+  p->n_orig = B->n_orig;
+  p->n_packed = B->n_packed;
+  p->orig.assign(B->orig, B->orig + B->n_packed);
+  if (B->art) p->art.assign(B->art, B->art + B->n_orig);
+  p->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
+  p->h_chain_off.assign(B->chain_off, B->chain_off + B->n_bcc + 1);
+  p->h_n_plain.assign(B->n_plain, B->n_plain + B->n_bcc);
+  p->h_chain_start.assign(B->chain_start, B->chain_start + B->n_chains);
+  p->h_chain_len.assign(B->chain_len, B->chain_len + B->n_chains);
+  if ((rc = upload(p, &p->row, B->row, B->n_packed + 1)) || (rc = upload(p, &p->vtx_off, B->vtx_off, B->n_bcc + 1)) ||
+      (rc = upload(p, &p->col, B->col, B->n_arcs)) || (rc = upload(p, &p->reach, B->reach, B->n_packed)) ||
+      (rc = upload(p, &p->chain_start, B->chain_start, B->n_chains)) ||
+      (rc = upload(p, &p->chain_len, B->chain_len, B->n_chains)) ||
+      (rc = upload(p, &p->chain_l, B->chain_l, B->n_chains)) || (rc = upload(p, &p->chain_r, B->chain_r, B->n_chains)) ||
+      (rc = dalloc(p, &p->bc, B->n_packed)) || (rc = dalloc(p, &p->err, 1)) || (rc = dalloc(p, &p->counter, 1)))
+    return bail(rc);
+  if (cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(B->n_packed, 1), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(p->err, 0, sizeof(int), ctx->stream) != cudaSuccess)
+    return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
+  int64_t nb_max = 0;
+  for (int32_t b = 0; b < B->n_bcc; ++b) nb_max = std::max(nb_max, B->vtx_off[b + 1] - B->vtx_off[b]);
+
+  size_t free_b = 0, total_b = 0;
+  CK(ctx, cudaMemGetInfo(&free_b, &total_b));
+  int64_t limit = ctx->opts.workspace_limit > 0 ? ctx->opts.workspace_limit : (int64_t)(0.8 * (double)free_b);
+
+  if (p->mode == BCGPU_MODE_PLAIN) {
+    std::vector<bcg::PlainItem> items;
+    if (override_items) items = *override_items;
+    else plain_items(B, items);
+    p->n_items = (int64_t)items.size();
+    p->unit_sources.assign(items.size() + 1, 0);
+    p->unit_teps.assign(items.size() + 1, 0);
+    p->unit_bfs.assign(items.size() + 1, 0);
+    p->unit_aux.assign(items.size() + 1, 0);
+    for (size_t i = 0; i < items.size(); ++i) {
+      const auto &it = items[i];
+      int64_t src = 1, aux = 0;
+      int32_t prev = -1;
+      for (int32_t c = it.c0; c < it.c1; ++c) {
+        src += B->chain_len[c];
+        if (B->chain_r[c] != prev) { ++aux; prev = B->chain_r[c]; }
+      }
+      const int64_t arcs = B->row[B->vtx_off[it.bcc + 1]] - B->row[B->vtx_off[it.bcc]];
+      p->unit_sources[i + 1] = p->unit_sources[i] + src;
+      p->unit_teps[i + 1] = p->unit_teps[i] + src * arcs;
+      p->unit_bfs[i + 1] = p->unit_bfs[i] + 1;
+      p->unit_aux[i + 1] = p->unit_aux[i] + aux;
+    }
+    if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
+    p->ws_n = nb_max + 2;
+    const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
+    int grid = ctx->sms;  // one 1024-thread CTA per SM
+    int64_t avail = limit - p->device_bytes - 2 * (int64_t)sizeof(int32_t) * (grid + 1);
+    if (avail < 2 * per_slot) return bail(fail(ctx, BCGPU_ENOMEM, "workspace for the largest BCC exceeds the limit"));
+    grid = (int)std::min<int64_t>(grid, avail / per_slot - 1);
+    p->grid = std::max(1, grid);
+    const int64_t slots = p->grid + 1;  // + the row-export slot
+    if ((rc = dalloc(p, &p->ws_i, slots * 7 * p->ws_n)) || (rc = dalloc(p, &p->ws_f, slots * 4 * p->ws_n)) ||
+        (rc = dalloc(p, &p->epochs, 2 * slots)))
+      return bail(rc);
+    if (cudaMemsetAsync(p->ws_i, 0, sizeof(int32_t) * (size_t)(slots * 7 * p->ws_n), ctx->stream) != cudaSuccess)
+      return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
+    std::vector<int32_t> ep((size_t)(2 * slots), 1);
+    CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    bcg::BatchedConfig cfg;
+    cfg.width = ctx->opts.batch_width;
+    cfg.delta_fp32c = ctx->opts.delta == BCGPU_DELTA_FP32C;
+    cfg.sms = ctx->sms;
+    cfg.limit_bytes = limit - p->device_bytes;
+    std::string msg;
+    rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
+                             p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
+    if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
+    p->device_bytes += bcg::batched_device_bytes(p->bp);
+    bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux);
+  }
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = p;
+  return BCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" void bc_default_opts(bc_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->device = -1;
+  o->mode = BCGPU_MODE_PLAIN;
+  o->delta = BCGPU_DELTA_FP32C;
+  o->batch_width = 0;
+}
+
+extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
+  if (!out) return fail(nullptr, BCGPU_EINVAL, "null out");
+  bc_opts o;
+  if (opts) o = *opts;
+  else bc_default_opts(&o);
+  if (o.mode != BCGPU_MODE_PLAIN && o.mode != BCGPU_MODE_BATCHED) return fail(nullptr, BCGPU_EINVAL, "bad mode");
+  if (o.delta != BCGPU_DELTA_FP64 && o.delta != BCGPU_DELTA_FP32C) return fail(nullptr, BCGPU_EINVAL, "bad delta");
+  if (o.batch_width < 0 || o.batch_width > 1024 || (o.batch_width % 32) != 0)
+    return fail(nullptr, BCGPU_EINVAL, "batch_width must be a multiple of 32 in [0, 1024]");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(nullptr, BCGPU_ECUDA, std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "none"));
+  int dev = o.device;
+  if (dev < 0) {  // highest compute capability, as the reference's choose_device (Codes/begin_gpupgm.cu:8-39)
+    int best = -1;
+    for (int i = 0; i < count; ++i) {
+      cudaDeviceProp pr;
+      if (cudaGetDeviceProperties(&pr, i) != cudaSuccess) continue;
+      int cc = pr.major * 10 + pr.minor;
+      if (cc > best) { best = cc; dev = i; }
+    }
+  }
+  if (dev < 0 || dev >= count) return fail(nullptr, BCGPU_EINVAL, "device ordinal out of range");
+  bc_ctx *ctx = new (std::nothrow) bc_ctx;
+  if (!ctx) return fail(nullptr, BCGPU_ENOMEM, "host allocation");
+  ctx->opts = o;
+  ctx->device = dev;
+  auto bad = [&](cudaError_t err, const char *what) {
+    cuda_fail(nullptr, err, what);
+    bc_destroy(ctx);
+    return BCGPU_ECUDA;
+  };
+  if ((e = cudaSetDevice(dev)) != cudaSuccess) return bad(e, "cudaSetDevice");
+  cudaDeviceProp pr;
+  if ((e = cudaGetDeviceProperties(&pr, dev)) != cudaSuccess) return bad(e, "cudaGetDeviceProperties");
+  if (pr.major < 10) {
+    g_create_err = std::string("device ") + pr.name + " is not sm_100 (kernels are built for sm_100a only)";
+    bc_destroy(ctx);
+    return BCGPU_ECUDA;
+  }
+  ctx->sms = pr.multiProcessorCount;
+  if (o.stream) ctx->stream = (cudaStream_t)o.stream;
+  else {
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return bad(e, "cudaStreamCreate");
+    ctx->own_stream = true;
+  }
+  if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess)
+    return bad(e, "cudaEventCreate");
+  *out = ctx;
+  return BCGPU_OK;
+}
+
+extern "C" void bc_destroy(bc_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" const char *bc_last_error(const bc_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
+
+extern "C" int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out) {
+  if (!ctx || !out) return fail(ctx, BCGPU_EINVAL, "null argument");
+  return create_plan(ctx, bccs, nullptr, out);
+}
+
+extern "C" void bc_plan_destroy(bc_plan *p) {
+  if (!p) return;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  if (p->bp) bcg::batched_destroy(p->bp);
+  for (void *a : p->allocs) cudaFree(a);
+  delete p;
+}
+
+extern "C" int64_t bc_plan_num_units(const bc_plan *p) {
+  return p ? (int64_t)p->unit_sources.size() - 1 : 0;
+}
+
+extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, int64_t *sources, int64_t *teps) {
+  if (!p) return BCGPU_EINVAL;
+  const int64_t n = bc_plan_num_units(p);
+  if (begin < 0 || end < begin || end > n) return fail(p->ctx, BCGPU_EINVAL, "unit range out of bounds");
+  if (sources) *sources = p->unit_sources[end] - p->unit_sources[begin];
+  if (teps) *teps = p->unit_teps[end] - p->unit_teps[begin];
+  return BCGPU_OK;
+}
+
+extern "C" int64_t bc_plan_device_bytes(const bc_plan *p) { return p ? p->device_bytes : 0; }
+
+extern "C" int bc_plan_reset(bc_plan *p) {
+  if (!p) return BCGPU_EINVAL;
+  CK(p->ctx, cudaSetDevice(p->ctx->device));
+  CK(p->ctx, cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(p->n_packed, 1), p->ctx->stream));
+  CK(p->ctx, cudaMemsetAsync(p->err, 0, sizeof(int), p->ctx->stream));
+  return BCGPU_OK;
+}
+
+extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *stats) {
+  if (!p) return BCGPU_EINVAL;
+  bc_ctx *ctx = p->ctx;
+  const int64_t n = bc_plan_num_units(p);
+  if (begin < 0 || end < begin || end > n) return fail(ctx, BCGPU_EINVAL, "unit range out of bounds");
+  CK(ctx, cudaSetDevice(ctx->device));
+  int launches = 0;
+  if (stats) CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  if (end > begin) {
+    if (p->mode == BCGPU_MODE_PLAIN) {
+      CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
+      bcg::PlainArgs a{};
+      a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
+      a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
+      a.items = p->items; a.item_begin = begin; a.item_end = end; a.next_item = p->counter; a.bc = p->bc;
+      a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
+      a.err = p->err;
+      const int grid = (int)std::min<int64_t>(p->grid, end - begin);
+      CK(ctx, bcg::launch_plain(a, grid, ctx->stream));
+      launches = 1;
+    } else {
+      std::string msg;
+      int rc = bcg::batched_run(p->bp, begin, end, ctx->stream, &launches, &msg);
+      if (rc) return fail(ctx, rc, "batched run: " + msg);
+    }
+  }
+  if (stats) {
+    CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    int rc = check_dev_err(p);
+    if (rc) return rc;
+    float ms = 0.f;
+    CK(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    std::memset(stats, 0, sizeof(*stats));
+    stats->sources = p->unit_sources[end] - p->unit_sources[begin];
+    stats->bfs_sources = p->unit_bfs[end] - p->unit_bfs[begin];
+    stats->aux_bfs = p->unit_aux[end] - p->unit_aux[begin];
+    stats->teps_edges = p->unit_teps[end] - p->unit_teps[begin];
+    stats->kernel_ms = ms;
+    stats->total_ms = ms;
+    stats->kernel_launches = launches;
+    stats->batch_width = p->bp ? bcg::batched_width(p->bp) : 0;
+  }
+  return BCGPU_OK;
+}
+
+extern "C" int bc_plan_read(bc_plan *p, double *bc_out) {
+  if (!p || !bc_out) return BCGPU_EINVAL;
+  CK(p->ctx, cudaSetDevice(p->ctx->device));
+  int rc = check_dev_err(p);
+  if (rc) return rc;
+  std::vector<double> packed((size_t)p->n_packed);
+  if (p->n_packed)
+    CK(p->ctx, cudaMemcpyAsync(packed.data(), p->bc, sizeof(double) * (size_t)p->n_packed, cudaMemcpyDeviceToHost,
+                               p->ctx->stream));
+  CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] = p->art.empty() ? 0.0 : p->art[v];
+  for (int64_t k = 0; k < p->n_packed; ++k) bc_out[p->orig[k]] += packed[k];  // fixed order: deterministic
+  return BCGPU_OK;
+}
+
+extern "C" int bc_plan_source_rows(bc_plan *p, int64_t packed, int32_t *d_out, double *sigma_out) {
+  if (!p || !d_out || !sigma_out) return BCGPU_EINVAL;
+  bc_ctx *ctx = p->ctx;
+  if (packed < 0 || packed >= p->n_packed) return fail(ctx, BCGPU_EINVAL, "packed id out of range");
+  if (p->mode != BCGPU_MODE_PLAIN) return fail(ctx, BCGPU_EINVAL, "row export needs a PLAIN plan");
+  CK(ctx, cudaSetDevice(ctx->device));
+  const auto &vo = p->h_vtx_off;
+  const int32_t b = (int32_t)(std::upper_bound(vo.begin(), vo.end(), packed) - vo.begin() - 1);
+  const int32_t local = (int32_t)(packed - vo[b]);
+  const int32_t nb = (int32_t)(vo[b + 1] - vo[b]);
+  int32_t chain = -1;
+  if (local >= p->h_n_plain[b]) {
+    for (int64_t c = p->h_chain_off[b]; c < p->h_chain_off[b + 1]; ++c)
+      if (local >= p->h_chain_start[c] && local < p->h_chain_start[c] + p->h_chain_len[c]) chain = (int32_t)c;
+    if (chain < 0) return fail(ctx, BCGPU_EINVAL, "chain vertex without a chain");
+  }
+  int32_t *dd = nullptr;
+  double *ds = nullptr;
+  CK(ctx, cudaMallocAsync((void **)&dd, sizeof(int32_t) * (size_t)nb, ctx->stream));
+  CK(ctx, cudaMallocAsync((void **)&ds, sizeof(double) * (size_t)nb, ctx->stream));
+  bcg::PlainArgs a{};
+  a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
+  a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
+  a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid; a.err = p->err;
+  cudaError_t e = bcg::launch_rows(a, b, local, chain, dd, ds, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, dd, sizeof(int32_t) * (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_out, ds, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(dd, ctx->stream);
+  cudaFreeAsync(ds, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "row export");
+  return check_dev_err(p);
+}
+
+extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats) {
+  if (!ctx || !bccs || !bc_out) return fail(ctx, BCGPU_EINVAL, "null argument");
+  CK(ctx, cudaSetDevice(ctx->device));
+  cudaEvent_t t0, t1;
+  CK(ctx, cudaEventCreate(&t0));
+  CK(ctx, cudaEventCreate(&t1));
+  CK(ctx, cudaEventRecord(t0, ctx->stream));
+  bc_plan *p = nullptr;
+  int rc = create_plan(ctx, bccs, nullptr, &p);
+  bc_stats st{};
+  if (!rc) rc = bc_plan_run(p, 0, bc_plan_num_units(p), &st);
+  if (!rc) rc = bc_plan_read(p, bc_out);
+  if (!rc) {
+    if (cudaEventRecord(t1, ctx->stream) == cudaSuccess && cudaEventSynchronize(t1) == cudaSuccess) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t0, t1);
+      st.total_ms = ms;
+    }
+    if (stats) *stats = st;
+  }
+  bc_plan_destroy(p);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  return rc;
+}
+
+namespace {
+
+// One-BCC packed input built from a reference-style CSR (int32 offsets).
+struct OneBcc {
+  std::vector<int64_t> vtx_off, row, chain_off;
+  std::vector<int32_t> col, reach, orig, n_plain, chain_start, chain_len, chain_l, chain_r;
+  bc_bccs view{};
+  void finish(int32_t n) {
+    view.n_bcc = 1;
+    view.n_orig = n;
+    view.n_packed = n;
+    view.n_arcs = row[n];
+    view.n_chains = (int64_t)chain_start.size();
+    view.vtx_off = vtx_off.data(); view.row = row.data(); view.col = col.data(); view.reach = reach.data();
+    view.orig = orig.data(); view.n_plain = n_plain.data(); view.chain_off = chain_off.data();
+    view.chain_start = chain_start.data(); view.chain_len = chain_len.data(); view.chain_l = chain_l.data();
+    view.chain_r = chain_r.data(); view.art = nullptr;
+  }
+};
+
+int check_csr(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m, const int32_t *reach) {
+  if (!R || !C || !reach || n < 3 || m < 0) return fail(ctx, BCGPU_EINVAL, "bad CSR arguments (a BCC has >= 3 vertices)");
+  if (R[0] != 0 || R[n] != m) return fail(ctx, BCGPU_EINVAL, "R[0] must be 0 and R[n] must equal m (arcs)");
+  for (int32_t v = 0; v < n; ++v)
+    if (R[v + 1] < R[v]) return fail(ctx, BCGPU_EINVAL, "R decreases");
+  for (int32_t e = 0; e < m; ++e)
+    if (C[e] < 0 || C[e] >= n) return fail(ctx, BCGPU_EINVAL, "C out of range");
+  return BCGPU_OK;
+}
+
+int run_one(bc_ctx *ctx, OneBcc &o, const std::vector<bcg::PlainItem> &items, std::vector<double> &packed_bc,
+            double *time_s) {
+  bc_plan *p = nullptr;
+  const int saved = ctx->opts.mode;
+  ctx->opts.mode = BCGPU_MODE_PLAIN;  // explicit source lists are run with the per-source schedule
+  int rc = create_plan(ctx, &o.view, &items, &p);
+  ctx->opts.mode = saved;
+  if (rc) return rc;
+  bc_stats st{};
+  rc = bc_plan_run(p, 0, bc_plan_num_units(p), &st);
+  if (!rc) {
+    packed_bc.assign((size_t)o.view.n_orig, 0.0);
+    rc = bc_plan_read(p, packed_bc.data());  // orig is the identity here
+  }
+  if (!rc && time_s) *time_s += st.kernel_ms * 1e-3;
+  bc_plan_destroy(p);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m,
+                             const int32_t *req_nodes, int32_t n_req, const int32_t *reach, float *bc, double *time_s) {
+  if (!ctx || !bc || (n_req > 0 && !req_nodes)) return fail(ctx, BCGPU_EINVAL, "null argument");
+  int rc = check_csr(ctx, R, C, n, m, reach);
+  if (rc) return rc;
+  OneBcc o;
+  o.vtx_off = {0, n};
+  o.row.assign(R, R + n + 1);
+  o.col.assign(C, C + m);
+  o.reach.assign(reach, reach + n);
+  o.orig.resize(n);
+  for (int32_t v = 0; v < n; ++v) o.orig[v] = v;
+  o.n_plain = {n};
+  o.chain_off = {0, 0};
+  o.finish(n);
+  std::vector<bcg::PlainItem> items;
+  for (int32_t i = 0; i < n_req; ++i) {
+    if (req_nodes[i] < 0 || req_nodes[i] >= n) return fail(ctx, BCGPU_EINVAL, "req_nodes out of range");
+    items.push_back({0, req_nodes[i], 0, 0});
+  }
+  std::vector<double> out;
+  rc = run_one(ctx, o, items, out, time_s);
+  if (rc) return rc;
+  for (int32_t v = 0; v < n; ++v) bc[v] = (float)out[v];  // overwritten, as the reference's free call
+  return BCGPU_OK;
+}
+
+extern "C" int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m,
+                               const int32_t *active, int32_t n_active, int32_t n_ears, const int32_t *lnode,
+                               const int32_t *rnode, const int32_t *cnt, const int32_t *off, const int32_t *nodes,
+                               const int32_t *ld, const int32_t *rd, const int32_t *reach, float *bc, double *time_s) {
+  if (!ctx || !bc || (n_active > 0 && !active) || (n_ears > 0 && (!lnode || !rnode || !cnt || !off || !nodes || !ld || !rd)))
+    return fail(ctx, BCGPU_EINVAL, "null argument");
+  int rc = check_csr(ctx, R, C, n, m, reach);
+  if (rc) return rc;
+  // New ids: every vertex not on an ear first (original order), then each ear's
+  // vertices from its left end (ld = 1, 2, ...) to its right end.
+  std::vector<int32_t> nid((size_t)n, -1), old;
+  std::vector<char> on_ear((size_t)n, 0), is_active((size_t)n, 0);
+  for (int32_t i = 0; i < n_active; ++i) {
+    if (active[i] < 0 || active[i] >= n) return fail(ctx, BCGPU_EINVAL, "active vertex out of range");
+    is_active[active[i]] = 1;
+  }
+  for (int32_t e = 0; e < n_ears; ++e)
+    for (int32_t j = 0; j < cnt[e]; ++j) {
+      int32_t z = nodes[off[e] + j];
+      if (z < 0 || z >= n || on_ear[z]) return fail(ctx, BCGPU_EINVAL, "ear vertex out of range or repeated");
+      on_ear[z] = 1;
+    }
+  for (int32_t v = 0; v < n; ++v)
+    if (!on_ear[v]) { nid[v] = (int32_t)old.size(); old.push_back(v); }
+  const int32_t nplain = (int32_t)old.size();
+  // ears sorted by the new id of their left end (chains are grouped by owner)
+  std::vector<int32_t> order((size_t)n_ears);
+  for (int32_t e = 0; e < n_ears; ++e) {
+    order[e] = e;
+    if (lnode[e] < 0 || lnode[e] >= n || rnode[e] < 0 || rnode[e] >= n || on_ear[lnode[e]] || on_ear[rnode[e]] ||
+        lnode[e] == rnode[e] || !is_active[lnode[e]] || cnt[e] < 1)
+      return fail(ctx, BCGPU_EINVAL, "ear endpoints must be distinct active vertices");
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t a, int32_t b) { return std::make_pair(nid[lnode[a]], nid[rnode[a]]) <
+                                                      std::make_pair(nid[lnode[b]], nid[rnode[b]]); });
+  OneBcc o;
+  for (int32_t e : order) {
+    std::vector<std::pair<int32_t, int32_t>> byld;
+    for (int32_t j = 0; j < cnt[e]; ++j) {
+      const int32_t k = off[e] + j;
+      if (ld[k] < 1 || ld[k] > cnt[e] || ld[k] + rd[k] != cnt[e] + 1)
+        return fail(ctx, BCGPU_EINVAL, "ear distances must be 1..cnt with ld + rd = cnt + 1 (unit weights)");
+      byld.push_back({ld[k], nodes[k]});
+    }
+    std::sort(byld.begin(), byld.end());
+    o.chain_start.push_back((int32_t)old.size());
+    o.chain_len.push_back(cnt[e]);
+    o.chain_l.push_back(nid[lnode[e]]);
+    o.chain_r.push_back(nid[rnode[e]]);
+    for (auto &pr : byld) { nid[pr.second] = (int32_t)old.size(); old.push_back(pr.second); }
+  }
+  if ((int32_t)old.size() != n) return fail(ctx, BCGPU_EINVAL, "relabelling failed");
+  o.vtx_off = {0, n};
+  o.row.assign((size_t)n + 1, 0);
+  for (int32_t k = 0; k < n; ++k) o.row[k + 1] = o.row[k] + (R[old[k] + 1] - R[old[k]]);
+  o.col.resize((size_t)m);
+  o.reach.resize((size_t)n);
+  o.orig.resize((size_t)n);
+  for (int32_t k = 0; k < n; ++k) {
+    int64_t w = o.row[k];
+    for (int32_t e = R[old[k]]; e < R[old[k] + 1]; ++e) o.col[w++] = nid[C[e]];
+    o.reach[k] = reach[old[k]];
+    o.orig[k] = k;  // results are mapped back below
+  }
+  o.n_plain = {nplain};
+  o.chain_off = {0, (int64_t)o.chain_start.size()};
+  o.finish(n);
+  std::vector<bcg::PlainItem> items;
+  size_t c = 0;
+  for (int32_t k = 0; k < nplain; ++k) {
+    size_t c0 = c;
+    while (c < o.chain_l.size() && o.chain_l[c] == k) ++c;
+    if (is_active[old[k]] || c > c0) items.push_back({0, k, (int32_t)c0, (int32_t)c});
+  }
+  std::vector<double> out;
+  rc = run_one(ctx, o, items, out, time_s);
+  if (rc) return rc;
+  for (int32_t k = 0; k < n; ++k) bc[old[k]] += (float)out[k];  // added, as the reference seeds from bc
+  return BCGPU_OK;
+}

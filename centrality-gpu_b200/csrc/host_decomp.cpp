@@ -1,0 +1,474 @@
+// Host side of libbcgpu: edge-list ingest and the decomposition that feeds the
+// GPU kernels (C ABI in include/bchost.h).
+//
+// What it replaces in the reference and how it differs:
+//  * Graph::Graph(char*) (Codes/graph.cpp:38-59) reads with fscanf and keeps
+//    duplicates; here the file is parsed from one buffer and the graph is made
+//    simple (loops dropped, duplicates merged), the assumption the reference's
+//    BFS states (Codes/kernels_free.cu:248).
+//  * BiCC::bicc_tarjan (Codes/bicc.cpp:81-161) recurses once per vertex and
+//    assumes the DFS root is vertex 0 (:13,:86-87); here one iterative
+//    Hopcroft-Tarjan pass with explicit stacks handles every component.
+//  * fillbccparent/reachfunction (Codes/modified_apsp.cpp:77-220) walk an
+//    explicit block-cut tree; here reach and the articulation cross terms come
+//    straight from DFS subtree sizes: for BCC b with head h (the DFS-closest
+//    vertex) and first child c, reach_b(h) = |comp| - 1 - size(c), and for any
+//    other member x, reach_b(x) = sum of size(y) over DFS children y of x with
+//    low(y) >= disc(x) (subtrees split off at x). The cross term of x is
+//    S^2 - sum(part^2) over the parts of comp - x (S = |comp| - 1), i.e. the
+//    ordered pairs that x separates (Codes/modified_apsp.cpp:209).
+//  * bcc_bfs/preSum (Codes/bcc_bfs.cpp:100-236, :247-1330) find ears through a
+//    BFS tree, LCAs and "master" edges; the chains they emit are exactly the
+//    maximal paths of vertices of degree 2 inside the BCC (a BCC that is one
+//    cycle emits none: all its vertices stay free). Here those paths are
+//    walked directly from their endpoints in O(n_b + m_b).
+#include "bchost.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+struct bc_graph {
+  int32_t n = 0;
+  std::vector<int64_t> row;
+  std::vector<int32_t> col;
+};
+
+struct bc_decomp {
+  bc_bccs view{};
+  bc_decomp_info info{};
+  std::vector<int64_t> vtx_off, row, chain_off;
+  std::vector<int32_t> col, reach, orig, n_plain, chain_start, chain_len, chain_l, chain_r;
+  std::vector<double> art;
+};
+
+namespace {
+
+void set_err(char *err, size_t errlen, const std::string &msg) {
+  if (err && errlen) {
+    std::snprintf(err, errlen, "%s", msg.c_str());
+  }
+}
+
+int build_csr(int32_t n, int64_t m, const int32_t *u, const int32_t *v, bc_graph *g) {
+  g->n = n;
+  std::vector<int64_t> deg((size_t)n + 1, 0);
+  for (int64_t e = 0; e < m; ++e) {
+    if (u[e] < 0 || u[e] >= n || v[e] < 0 || v[e] >= n) return BCGPU_EINVAL;
+    if (u[e] == v[e]) continue;
+    deg[u[e] + 1]++;
+    deg[v[e] + 1]++;
+  }
+  for (int32_t i = 0; i < n; ++i) deg[i + 1] += deg[i];
+  std::vector<int32_t> col((size_t)deg[n]);
+  std::vector<int64_t> fill(deg.begin(), deg.end() - 1);
+  for (int64_t e = 0; e < m; ++e) {
+    if (u[e] == v[e]) continue;
+    col[fill[u[e]]++] = v[e];
+    col[fill[v[e]]++] = u[e];
+  }
+  // sort + dedup every adjacency list, then compact
+  std::vector<int64_t> keep((size_t)n + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int32_t i = 0; i < n; ++i) {
+    int32_t *b = col.data() + deg[i], *e = col.data() + deg[i + 1];
+    std::sort(b, e);
+    keep[i + 1] = std::unique(b, e) - b;
+  }
+  for (int32_t i = 0; i < n; ++i) keep[i + 1] += keep[i];
+  g->row = keep;
+  g->col.resize((size_t)keep[n]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int32_t i = 0; i < n; ++i)
+    std::copy(col.data() + deg[i], col.data() + deg[i] + (keep[i + 1] - keep[i]), g->col.data() + keep[i]);
+  return BCGPU_OK;
+}
+
+// Minimal integer scanner over a memory buffer.
+struct Scanner {
+  const char *p, *end;
+  bool next(int64_t &x) {
+    while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
+    if (p >= end) return false;
+    bool neg = false;
+    if (*p == '-') { neg = true; ++p; }
+    if (p >= end || *p < '0' || *p > '9') return false;
+    int64_t v = 0;
+    while (p < end && *p >= '0' && *p <= '9') { v = v * 10 + (*p - '0'); ++p; }
+    x = neg ? -v : v;
+    return true;
+  }
+};
+
+}  // namespace
+
+extern "C" int bc_graph_from_edges(int32_t n, int64_t m, const int32_t *u, const int32_t *v, bc_graph **out) {
+  if (!out || n < 0 || m < 0 || (m > 0 && (!u || !v))) return BCGPU_EINVAL;
+  bc_graph *g = new (std::nothrow) bc_graph;
+  if (!g) return BCGPU_ENOMEM;
+  int rc;
+  try {
+    rc = build_csr(n, m, u, v, g);
+  } catch (const std::bad_alloc &) {
+    rc = BCGPU_ENOMEM;
+  }
+  if (rc != BCGPU_OK) { delete g; return rc; }
+  *out = g;
+  return BCGPU_OK;
+}
+
+extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t errlen) {
+  if (!path || !out) { set_err(err, errlen, "null argument"); return BCGPU_EINVAL; }
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) { set_err(err, errlen, std::string("input file cannot be opened: ") + path); return BCGPU_EIO; }
+  std::fseek(fp, 0, SEEK_END);
+  long size = std::ftell(fp);
+  std::fseek(fp, 0, SEEK_SET);
+  std::vector<char> buf(size > 0 ? (size_t)size : 1);
+  size_t got = size > 0 ? std::fread(buf.data(), 1, (size_t)size, fp) : 0;
+  std::fclose(fp);
+  if ((long)got != size) { set_err(err, errlen, "short read"); return BCGPU_EIO; }
+  Scanner sc{buf.data(), buf.data() + got};
+  int64_t n, m;
+  if (!sc.next(n) || !sc.next(m) || n < 0 || m < 0 || n > INT32_MAX) {
+    set_err(err, errlen, "bad header: expected 'n m'");
+    return BCGPU_EIO;
+  }
+  std::vector<int32_t> u((size_t)m), v((size_t)m);
+  for (int64_t e = 0; e < m; ++e) {
+    int64_t a, b, w;
+    if (!sc.next(a) || !sc.next(b) || !sc.next(w)) {
+      set_err(err, errlen, "truncated edge list at edge " + std::to_string(e) + " of " + std::to_string(m));
+      return BCGPU_EIO;
+    }
+    if (a < 0 || a >= n || b < 0 || b >= n) {
+      set_err(err, errlen, "vertex id out of range at edge " + std::to_string(e));
+      return BCGPU_EIO;
+    }
+    u[e] = (int32_t)a;
+    v[e] = (int32_t)b;
+  }
+  int rc = bc_graph_from_edges((int32_t)n, m, u.data(), v.data(), out);
+  if (rc != BCGPU_OK) set_err(err, errlen, "graph construction failed");
+  return rc;
+}
+
+extern "C" void bc_graph_free(bc_graph *g) { delete g; }
+
+extern "C" int bc_graph_csr(const bc_graph *g, int32_t *n, int64_t *n_arcs, const int64_t **row, const int32_t **col) {
+  if (!g) return BCGPU_EINVAL;
+  if (n) *n = g->n;
+  if (n_arcs) *n_arcs = g->row.empty() ? 0 : g->row[g->n];
+  if (row) *row = g->row.data();
+  if (col) *col = g->col.data();
+  return BCGPU_OK;
+}
+
+namespace {
+
+int decompose(const bc_graph *g, bc_decomp *D) {
+  auto t0 = std::chrono::steady_clock::now();
+  const int32_t n = g->n;
+  const int64_t *R = g->row.data();
+  const int32_t *C = g->col.data();
+
+  // ---- iterative Hopcroft-Tarjan: DFS tree, low links, subtree sizes, BCCs
+  std::vector<int32_t> disc((size_t)n, -1), low((size_t)n), parent((size_t)n, -1), tbcc((size_t)n, -1),
+      locid((size_t)n, -1), comp((size_t)n, -1);
+  std::vector<int64_t> it((size_t)n), sz((size_t)n, 0), hang((size_t)n, 0);
+  std::vector<double> sq((size_t)n, 0.0);
+  std::vector<int64_t> comp_size;
+  std::vector<int32_t> head, child;          // per BCC
+  std::vector<int64_t> mem_off{0};           // per BCC member range
+  std::vector<int32_t> members;              // head stored last
+  std::vector<int32_t> stack, vstack;
+  stack.reserve(1024);
+  vstack.reserve(1024);
+  int32_t timer = 0;
+  for (int32_t r = 0; r < n; ++r) {
+    if (disc[r] >= 0) continue;
+    int32_t cid = (int32_t)comp_size.size();
+    disc[r] = low[r] = timer++;
+    it[r] = R[r];
+    sz[r] = 1;
+    comp[r] = cid;
+    stack.push_back(r);
+    vstack.push_back(r);
+    while (!stack.empty()) {
+      int32_t u = stack.back();
+      if (it[u] < R[u + 1]) {
+        int32_t w = C[it[u]++];
+        if (disc[w] < 0) {
+          parent[w] = u;
+          disc[w] = low[w] = timer++;
+          it[w] = R[w];
+          sz[w] = 1;
+          comp[w] = cid;
+          stack.push_back(w);
+          vstack.push_back(w);
+        } else if (w != parent[u] && disc[w] < low[u]) {
+          low[u] = disc[w];
+        }
+        continue;
+      }
+      stack.pop_back();
+      int32_t p = parent[u];
+      if (p < 0) continue;
+      if (low[u] < low[p]) low[p] = low[u];
+      sz[p] += sz[u];
+      if (low[u] >= disc[p]) {  // tree edge (p,u) closes a BCC headed by p
+        int32_t b = (int32_t)head.size();
+        head.push_back(p);
+        child.push_back(u);
+        int32_t w;
+        do {
+          w = vstack.back();
+          vstack.pop_back();
+          tbcc[w] = b;
+          locid[w] = (int32_t)(members.size() - (size_t)mem_off[b]);
+          members.push_back(w);
+        } while (w != u);
+        members.push_back(p);
+        mem_off.push_back((int64_t)members.size());
+        hang[p] += sz[u];
+        sq[p] += (double)sz[u] * (double)sz[u];
+      }
+    }
+    vstack.clear();  // only the root remains
+    comp_size.push_back(sz[r]);
+  }
+  const int32_t nbcc = (int32_t)head.size();
+
+  // ---- articulation cross terms
+  D->art.assign((size_t)n, 0.0);
+  int32_t n_art = 0;
+  for (int32_t x = 0; x < n; ++x) {
+    double S = (double)(comp_size[comp[x]] - 1);
+    double up = S - (double)hang[x];
+    double a = S * S - sq[x] - up * up;
+    D->art[x] = a;
+    n_art += a > 0.0;
+  }
+
+  // ---- BCC of every arc: the BCC of the tree edge into its deeper end
+  std::vector<int64_t> slot_off(mem_off);  // member slot of (b, local) = mem_off[b] + local
+  const int64_t n_slots = mem_off.back();
+  auto local_of = [&](int32_t x, int32_t b) -> int32_t {
+    return x == head[b] ? (int32_t)(mem_off[b + 1] - mem_off[b] - 1) : locid[x];
+  };
+  std::vector<int64_t> sdeg((size_t)n_slots + 1, 0);
+  for (int32_t x = 0; x < n; ++x)
+    for (int64_t e = R[x]; e < R[x + 1]; ++e) {
+      int32_t y = C[e];
+      int32_t b = tbcc[disc[x] > disc[y] ? x : y];
+      sdeg[mem_off[b] + local_of(x, b) + 1]++;
+    }
+  for (int64_t s = 0; s < n_slots; ++s) sdeg[s + 1] += sdeg[s];
+  std::vector<int32_t> sadj((size_t)sdeg[n_slots]);
+  {
+    std::vector<int64_t> fill(sdeg.begin(), sdeg.end() - 1);
+    for (int32_t x = 0; x < n; ++x)
+      for (int64_t e = R[x]; e < R[x + 1]; ++e) {
+        int32_t y = C[e];
+        int32_t b = tbcc[disc[x] > disc[y] ? x : y];
+        sadj[fill[mem_off[b] + local_of(x, b)]++] = local_of(y, b);
+      }
+  }
+
+  // ---- pack BCCs with >= 3 vertices, largest first
+  std::vector<int32_t> order;
+  for (int32_t b = 0; b < nbcc; ++b)
+    if (mem_off[b + 1] - mem_off[b] >= 3) order.push_back(b);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    return (mem_off[a + 1] - mem_off[a]) > (mem_off[b + 1] - mem_off[b]);
+  });
+  const int32_t np_bcc = (int32_t)order.size();
+  D->vtx_off.assign((size_t)np_bcc + 1, 0);
+  D->chain_off.assign((size_t)np_bcc + 1, 0);
+  D->n_plain.assign((size_t)np_bcc, 0);
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    int32_t b = order[i];
+    D->vtx_off[i + 1] = D->vtx_off[i] + (mem_off[b + 1] - mem_off[b]);
+  }
+  const int64_t n_packed = D->vtx_off[np_bcc];
+  D->row.assign((size_t)n_packed + 1, 0);
+  D->reach.assign((size_t)n_packed, 0);
+  D->orig.assign((size_t)n_packed, 0);
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    int32_t b = order[i];
+    for (int64_t k = mem_off[b]; k < mem_off[b + 1]; ++k) (void)k;
+  }
+  // arc offsets need the final ids; compute per BCC, in parallel
+  std::vector<std::vector<int32_t>> perm((size_t)np_bcc);           // new local -> old local
+  std::vector<std::vector<int32_t>> ch_start((size_t)np_bcc), ch_len((size_t)np_bcc), ch_l((size_t)np_bcc),
+      ch_r((size_t)np_bcc);
+  std::vector<int64_t> n_cycle((size_t)np_bcc, 0);
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    const int32_t b = order[i];
+    const int32_t nb = (int32_t)(mem_off[b + 1] - mem_off[b]);
+    const int64_t *sd = sdeg.data() + mem_off[b];
+    auto deg = [&](int32_t k) { return (int32_t)(sd[k + 1] - sd[k]); };
+    auto adj = [&](int32_t k) { return sadj.data() + sd[k]; };
+    bool cycle = true;
+    int32_t root = 0;
+    for (int32_t k = 0; k < nb; ++k) {
+      if (deg(k) != 2) cycle = false;
+      if (deg(k) > deg(root)) root = k;
+    }
+    n_cycle[i] = cycle;
+    // plain (non-chain) vertices in BFS order from the max-degree vertex
+    std::vector<int32_t> nid((size_t)nb, -1), old;
+    old.reserve((size_t)nb);
+    {
+      std::vector<char> seen((size_t)nb, 0);
+      std::vector<int32_t> q;
+      q.reserve((size_t)nb);
+      q.push_back(root);
+      seen[root] = 1;
+      for (size_t h = 0; h < q.size(); ++h) {
+        int32_t x = q[h];
+        if (cycle || deg(x) != 2) { nid[x] = (int32_t)old.size(); old.push_back(x); }
+        const int32_t *a = adj(x);
+        for (int32_t j = 0; j < deg(x); ++j)
+          if (!seen[a[j]]) { seen[a[j]] = 1; q.push_back(a[j]); }
+      }
+      if ((int32_t)q.size() != nb) bad = 1;  // a BCC is connected
+    }
+    const int32_t nplain = (int32_t)old.size();
+    if (!cycle) {
+      for (int32_t f = 0; f < nplain; ++f) {
+        int32_t x = old[f];
+        const int32_t *a = adj(x);
+        for (int32_t j = 0; j < deg(x); ++j) {
+          int32_t cur = a[j], prev = x;
+          if (deg(cur) != 2 || nid[cur] >= 0) continue;
+          int32_t start = (int32_t)old.size();
+          while (deg(cur) == 2) {
+            nid[cur] = (int32_t)old.size();
+            old.push_back(cur);
+            const int32_t *c2 = adj(cur);
+            int32_t nx = c2[0] == prev ? c2[1] : c2[0];
+            prev = cur;
+            cur = nx;
+          }
+          if (cur == x) bad = 1;  // a chain cannot return to its start inside a BCC
+          ch_start[i].push_back(start);
+          ch_len[i].push_back((int32_t)old.size() - start);
+          ch_l[i].push_back(f);
+          ch_r[i].push_back(cur);  // old id; mapped below
+        }
+      }
+      for (auto &r : ch_r[i]) r = nid[r];
+    }
+    if ((int32_t)old.size() != nb) bad = 1;
+    perm[i] = std::move(old);
+    D->n_plain[i] = nplain;
+  }
+  if (bad) return BCGPU_EINVAL;
+
+  // ---- write packed arrays
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    const int32_t b = order[i];
+    const int64_t base = D->vtx_off[i];
+    for (size_t k = 0; k < perm[i].size(); ++k) {
+      int32_t o = perm[i][k];
+      D->row[base + (int64_t)k + 1] = sdeg[mem_off[b] + o + 1] - sdeg[mem_off[b] + o];
+    }
+  }
+  for (int64_t k = 0; k < n_packed; ++k) D->row[k + 1] += D->row[k];
+  if (D->row[n_packed] > (int64_t)INT32_MAX * 8) return BCGPU_EOVERFLOW;
+  D->col.assign((size_t)D->row[n_packed], 0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    const int32_t b = order[i];
+    const int32_t nb = (int32_t)perm[i].size();
+    std::vector<int32_t> inv((size_t)nb);
+    for (int32_t k = 0; k < nb; ++k) inv[perm[i][k]] = k;
+    const int64_t base = D->vtx_off[i];
+    for (int32_t k = 0; k < nb; ++k) {
+      int32_t o = perm[i][k];
+      int64_t s = mem_off[b] + o;
+      int32_t *dst = D->col.data() + D->row[base + k];
+      int64_t d = sdeg[s + 1] - sdeg[s];
+      for (int64_t j = 0; j < d; ++j) dst[j] = inv[sadj[sdeg[s] + j]];
+      std::sort(dst, dst + d);
+      int32_t x = members[s];
+      D->orig[base + k] = x;
+      D->reach[base + k] =
+          (x == head[b]) ? (int32_t)(comp_size[comp[x]] - 1 - sz[child[b]]) : (int32_t)hang[x];
+    }
+  }
+  for (int32_t i = 0; i < np_bcc; ++i) D->chain_off[i + 1] = D->chain_off[i] + (int64_t)ch_start[i].size();
+  for (int32_t i = 0; i < np_bcc; ++i) {
+    D->chain_start.insert(D->chain_start.end(), ch_start[i].begin(), ch_start[i].end());
+    D->chain_len.insert(D->chain_len.end(), ch_len[i].begin(), ch_len[i].end());
+    D->chain_l.insert(D->chain_l.end(), ch_l[i].begin(), ch_l[i].end());
+    D->chain_r.insert(D->chain_r.end(), ch_r[i].begin(), ch_r[i].end());
+  }
+
+  bc_bccs &V = D->view;
+  V.n_bcc = np_bcc;
+  V.n_orig = n;
+  V.n_packed = n_packed;
+  V.n_arcs = D->row[n_packed];
+  V.n_chains = D->chain_off[np_bcc];
+  V.vtx_off = D->vtx_off.data();
+  V.row = D->row.data();
+  V.col = D->col.data();
+  V.reach = D->reach.data();
+  V.orig = D->orig.data();
+  V.n_plain = D->n_plain.data();
+  V.chain_off = D->chain_off.data();
+  V.chain_start = D->chain_start.data();
+  V.chain_len = D->chain_len.data();
+  V.chain_l = D->chain_l.data();
+  V.chain_r = D->chain_r.data();
+  V.art = D->art.data();
+
+  bc_decomp_info &I = D->info;
+  I.n_components = (int32_t)comp_size.size();
+  I.n_bcc_all = nbcc;
+  I.n_bcc_packed = np_bcc;
+  I.n_articulation = n_art;
+  I.n_chains = V.n_chains;
+  I.n_chain_vertices = 0;
+  for (auto l : D->chain_len) I.n_chain_vertices += l;
+  I.n_cycle_bccs = 0;
+  for (auto c : n_cycle) I.n_cycle_bccs += c;
+  I.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return BCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int bc_decompose(const bc_graph *g, bc_decomp **out) {
+  if (!g || !out) return BCGPU_EINVAL;
+  bc_decomp *D = new (std::nothrow) bc_decomp;
+  if (!D) return BCGPU_ENOMEM;
+  int rc;
+  try {
+    rc = decompose(g, D);
+  } catch (const std::bad_alloc &) {
+    rc = BCGPU_ENOMEM;
+  }
+  if (rc != BCGPU_OK) { delete D; return rc; }
+  *out = D;
+  return BCGPU_OK;
+}
+
+extern "C" void bc_decomp_free(bc_decomp *d) { delete d; }
+
+extern "C" const bc_bccs *bc_decomp_view(const bc_decomp *d) { return d ? &d->view : nullptr; }
+
+extern "C" void bc_decomp_get_info(const bc_decomp *d, bc_decomp_info *info) {
+  if (d && info) *info = d->info;
+}

@@ -1,0 +1,442 @@
+// PLAIN schedule: one source per CTA at a time, FP64 path counts and
+// dependencies, FP64 atomics into the per-vertex BC accumulator.
+//
+// Follows the reference's per-source Brandes (bc_kgpu_free / bc_kgpu_active,
+// Codes/kernels_free.cu:154-473, Codes/kernels_active.cu:263-602) and its
+// chain postprocessing (Codes/postprocesses.cu:205-470), re-designed:
+//  * no O(n) row reset per source: levels are stamped with a per-row epoch
+//    (level + base; anything below base is unvisited), the reference clears
+//    d/sigma/delta for every source (Codes/kernels_free.cu:205-218);
+//  * each vertex's adjacency is read once in the forward phase: when a
+//    frontier vertex is expanded it pulls sigma from its predecessors (all one
+//    level up, already final) and discovers its successors in the same scan,
+//    so sigma needs no atomics and its sum order is fixed;
+//  * neighbour scans are switched by degree: a thread per vertex up to 8 arcs,
+//    a warp up to 2048, the whole CTA above (the reference gives each frontier
+//    vertex one thread, Codes/kernels_free.cu:316-335);
+//  * the dependency sweep stores q(w) = (reach(w)+1+delta(w)) / sigma(w) so a
+//    predecessor reads one value per successor: delta(v) = sigma(v) * sum q(w)
+//    (same quantity as Codes/kernels_free.cu:391,409);
+//  * a chain vertex's rows are the merge of its endpoints' rows
+//    (Codes/postprocesses.cu:329-351) and its dependency sweep walks the
+//    endpoints' level buckets directly instead of radix-sorting n distance
+//    keys per source (Codes/postprocesses.cu:143-155).
+// A work item is one free/endpoint source plus the chains whose left endpoint
+// it is, so the left endpoint's BFS serves all of them and only the right
+// endpoint's BFS is repeated (forward only) per distinct right endpoint.
+#include "common.cuh"
+#include "plain.h"
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+namespace bcg {
+
+namespace {
+
+constexpr int kBlock = 1024;
+constexpr int kWarps = kBlock / 32;
+constexpr int kSmallDeg = 8;
+constexpr int kWarpDeg = 2048;
+
+struct Shared {
+  int tail;          // next free slot of the visit order S
+  int nwq, ncq;      // warp-tier / CTA-tier queue lengths
+  int flag;
+  int imax;
+  int item;
+  int base_a, base_b;  // epochs of rows A and B
+  double red[kWarps];
+  int wq[kBlock];
+  int cq[kBlock];
+};
+
+// Per-CTA workspace rows (capacity ws_n each).
+struct Rows {
+  int32_t *dA, *SA, *lvA, *dB, *SB, *lvB, *dM;
+  double *sA, *sB, *sM, *q;
+};
+
+__device__ __forceinline__ Rows rows_of(const PlainArgs &a, int64_t slot) {
+  Rows r;
+  const int64_t n = a.ws_n;
+  int32_t *wi = a.ws_i + slot * 7 * n;
+  double *wf = a.ws_f + slot * 4 * n;
+  r.dA = wi; r.SA = wi + n; r.lvA = wi + 2 * n; r.dB = wi + 3 * n; r.SB = wi + 4 * n; r.lvB = wi + 5 * n;
+  r.dM = wi + 6 * n;
+  r.sA = wf; r.sB = wf + n; r.sM = wf + 2 * n; r.q = wf + 3 * n;
+  return r;
+}
+
+// Appends x to S (warp-aggregated atomic on the shared tail).
+__device__ __forceinline__ void append(Shared &sh, int32_t *S, int32_t x) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int pos = 0;
+  if (g.thread_rank() == 0) pos = atomicAdd(&sh.tail, (int)g.size());
+  pos = g.shfl(pos, 0) + (int)g.thread_rank();
+  S[pos] = x;
+}
+
+// Forward step for one arc (w -> x) at level lev: accumulate sigma from a
+// predecessor, or claim an unvisited vertex for level lev+1.
+__device__ __forceinline__ void fwd_arc(Shared &sh, int32_t *d, const double *sig, int32_t *S, int32_t x, int dprev,
+                                        int dnext, int base, double &acc) {
+  int dx = __ldcg(d + x);
+  if (dx == dprev) {
+    acc += sig[x];
+  } else if (dx < base) {
+    int old = atomicMax(d + x, dnext);
+    if (old < base) append(sh, S, x);
+  }
+}
+
+__device__ __forceinline__ double block_sum(Shared &sh, double v) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh.red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kWarps; ++i) t += sh.red[i];  // fixed order
+    sh.red[0] = t;
+  }
+  __syncthreads();
+  t = sh.red[0];
+  __syncthreads();
+  return t;
+}
+
+// CTA-wide BFS from s over one BCC: fills d (epoch base), sigma, the level
+// order S and level offsets lv[0..nlev]. Returns nlev (number of levels).
+__device__ int cta_bfs(Shared &sh, const int64_t *R, const int32_t *C, int32_t nb, int32_t s, int32_t *d, double *sig,
+                       int32_t *S, int32_t *lv, int base) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    d[s] = base;
+    S[0] = s;
+    lv[0] = 0;
+    lv[1] = 1;
+    sh.tail = 1;
+  }
+  __syncthreads();
+  int lev = 0;
+  while (true) {
+    const int f0 = lv[lev], f1 = lv[lev + 1];
+    // the source has no predecessors; stale stamps are < base so they never match base+lev-1
+    const int dprev = lev == 0 ? INT_MIN : base + lev - 1, dnext = base + lev + 1;
+    for (int c0 = f0; c0 < f1; c0 += kBlock) {
+      if (tid == 0) { sh.nwq = 0; sh.ncq = 0; }
+      __syncthreads();
+      const int i = c0 + tid;
+      if (i < f1) {
+        const int32_t w = S[i];
+        const int64_t e0 = R[w], e1 = R[w + 1];
+        const int64_t deg = e1 - e0;
+        if (deg <= kSmallDeg) {
+          double acc = 0.0;
+          for (int64_t e = e0; e < e1; ++e) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+          sig[w] = lev == 0 ? 1.0 : acc;
+        } else if (deg <= kWarpDeg) {
+          sh.wq[atomicAdd(&sh.nwq, 1)] = w;
+        } else {
+          sh.cq[atomicAdd(&sh.ncq, 1)] = w;
+        }
+      }
+      __syncthreads();
+      for (int k = warp; k < sh.nwq; k += kWarps) {
+        const int32_t w = sh.wq[k];
+        const int64_t e0 = R[w], e1 = R[w + 1];
+        double acc = 0.0;
+        for (int64_t e = e0 + lane; e < e1; e += 32) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+        acc = warp_sum(acc);
+        if (lane == 0) sig[w] = lev == 0 ? 1.0 : acc;
+      }
+      const int ncq = sh.ncq;
+      for (int k = 0; k < ncq; ++k) {
+        const int32_t w = sh.cq[k];
+        const int64_t e0 = R[w], e1 = R[w + 1];
+        double acc = 0.0;
+        for (int64_t e = e0 + tid; e < e1; e += kBlock) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+        acc = block_sum(sh, acc);
+        if (tid == 0) sig[w] = lev == 0 ? 1.0 : acc;
+      }
+      __syncthreads();
+    }
+    const int tail = sh.tail;
+    if (tail == f1) break;
+    if (tid == 0) lv[lev + 2] = tail;
+    ++lev;
+    __syncthreads();
+  }
+  (void)nb;
+  return lev + 1;
+}
+
+// Dependency of w at level lev of a row (d stamped as base + level):
+// delta(w) = sigma(w) * sum over successors x of q(x); then q(w) and BC.
+__device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_t *C, const int32_t *d, const double *q,
+                                                  int32_t w, int dsucc) {
+  double acc = 0.0;
+  for (int64_t e = R[w]; e < R[w + 1]; ++e) {
+    int32_t x = ldg(C + e);
+    if (d[x] == dsucc) acc += q[x];
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void finish_vertex(int32_t w, double acc, const int32_t *rch, const double *sig, double *q,
+                                              double *bcb, double wsrc) {
+  const double sw = sig[w];
+  const double delta = sw * acc;
+  q[w] = ((double)rch[w] + 1.0 + delta) / sw;
+  if (delta != 0.0) atomicAdd(bcb + w, delta * wsrc);
+}
+
+// Vertex list of one backward level: up to three index ranges with filters.
+struct LevelList {
+  const int32_t *S0; int a0, b0;  // primary list
+  const int32_t *S1; int a1, b1;  // secondary list (merged rows: right endpoint's bucket)
+  int ck0, ck1;                   // chain vertices at direct distance (merged rows; -1 = none)
+};
+
+// mode 0: BFS row, every listed vertex is at this level.
+// mode 1: merged row: keep w iff dM(w) == lev, with duplicates removed
+//         (tie vertices listed in both buckets are taken from the primary one).
+struct MergeFilter {
+  const int32_t *dA; int baseA; int ld;
+  const int32_t *dB; int baseB; int rd;
+};
+
+__device__ __forceinline__ bool keep_vertex(int mode, int list, int32_t w, int lev, const int32_t *dM,
+                                            const MergeFilter &mf) {
+  if (mode == 0) return true;
+  if (dM[w] != lev) return false;
+  if (list == 0) return true;
+  const bool inA = (mf.dA[w] - mf.baseA) + mf.ld == lev;
+  if (list == 1) return !inA;
+  const bool inB = (mf.dB[w] - mf.baseB) + mf.rd == lev;
+  return !inA && !inB;
+}
+
+__device__ void cta_bwd_level(Shared &sh, const int64_t *R, const int32_t *C, const int32_t *d, const double *sig,
+                              double *q, const int32_t *rch, double *bcb, double wsrc, int dsucc, int lev, int mode,
+                              const LevelList &L, const MergeFilter &mf) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int list = 0; list < 3; ++list) {
+    const int32_t *S = list == 0 ? L.S0 : list == 1 ? L.S1 : nullptr;
+    int a = list == 0 ? L.a0 : list == 1 ? L.a1 : 0;
+    int b = list == 0 ? L.b0 : list == 1 ? L.b1 : (L.ck0 >= 0) + (L.ck1 >= 0);
+    if (b <= a) continue;
+    for (int c0 = a; c0 < b; c0 += kBlock) {
+      if (tid == 0) { sh.nwq = 0; sh.ncq = 0; }
+      __syncthreads();
+      const int i = c0 + tid;
+      if (i < b) {
+        int32_t w = list < 2 ? S[i] : (i == 0 && L.ck0 >= 0 ? L.ck0 : L.ck1);
+        if (keep_vertex(mode, list, w, lev, d, mf)) {
+          const int64_t deg = R[w + 1] - R[w];
+          if (deg <= kSmallDeg) {
+            finish_vertex(w, bwd_arcs_thread(R, C, d, q, w, dsucc), rch, sig, q, bcb, wsrc);
+          } else if (deg <= kWarpDeg) {
+            sh.wq[atomicAdd(&sh.nwq, 1)] = w;
+          } else {
+            sh.cq[atomicAdd(&sh.ncq, 1)] = w;
+          }
+        }
+      }
+      __syncthreads();
+      for (int k = warp; k < sh.nwq; k += kWarps) {
+        const int32_t w = sh.wq[k];
+        double acc = 0.0;
+        for (int64_t e = R[w] + lane; e < R[w + 1]; e += 32) {
+          int32_t x = ldg(C + e);
+          if (d[x] == dsucc) acc += q[x];
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) finish_vertex(w, acc, rch, sig, q, bcb, wsrc);
+      }
+      const int ncq = sh.ncq;
+      for (int k = 0; k < ncq; ++k) {
+        const int32_t w = sh.cq[k];
+        double acc = 0.0;
+        for (int64_t e = R[w] + tid; e < R[w + 1]; e += kBlock) {
+          int32_t x = ldg(C + e);
+          if (d[x] == dsucc) acc += q[x];
+        }
+        acc = block_sum(sh, acc);
+        if (tid == 0) finish_vertex(w, acc, rch, sig, q, bcb, wsrc);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Keeps epochs below 2^30: wraps the whole row (every BCC this CTA may see)
+// back to all-unvisited when the next BFS could overflow.
+__device__ void ensure_epoch(int32_t *d, int64_t cap, int &base, int span) {
+  if (base + span + 2 < (1 << 30)) return;
+  for (int64_t k = threadIdx.x; k < cap; k += kBlock) d[k] = 0;
+  __syncthreads();
+  base = 1;
+}
+
+// Rows of chain vertex (start+pos) from the endpoint rows A (left) and B
+// (right): d = min(dA+ld, dB+rd), sigma from the strictly shorter side or the
+// sum on ties (Codes/postprocesses.cu:334-350); then the chain's own vertices
+// are fixed along the chain (Codes/postprocesses.cu:205-274). Returns max level.
+__device__ int merge_rows(Shared &sh, const Rows &r, int baseA, int baseB, int32_t nb, int32_t start, int32_t len,
+                          int32_t pos, int *err) {
+  const int ld = pos + 1, rd = len - pos;
+  int mx = 0;
+  bool bad = false;
+  for (int k = threadIdx.x; k < nb; k += kBlock) {
+    const int la = __ldcg(r.dA + k) - baseA, lb = __ldcg(r.dB + k) - baseB;
+    bad |= (la < 0) | (lb < 0);
+    const int a = la + ld, b = lb + rd;
+    int dm;
+    double sm;
+    if (a < b) { dm = a; sm = r.sA[k]; }
+    else if (a > b) { dm = b; sm = r.sB[k]; }
+    else { dm = b; sm = r.sA[k] + r.sB[k]; }
+    r.dM[k] = dm;
+    r.sM[k] = sm;
+    mx = max(mx, dm);
+  }
+  if (bad) set_err(err, kDevDisconnected);
+  mx = warp_max(mx);
+  if (threadIdx.x == 0) sh.imax = 0;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) atomicMax(&sh.imax, mx);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < len; ++j) {
+      const int k = start + j;
+      const int dist = j > pos ? j - pos : pos - j;
+      if (r.dM[k] > dist) { r.dM[k] = dist; r.sM[k] = 1.0; }
+      else if (r.dM[k] == dist) r.sM[k] += 1.0;
+    }
+  }
+  __syncthreads();
+  return sh.imax;
+}
+
+__device__ void process_item(Shared &sh, const PlainArgs &a, const Rows &r, const PlainItem &it) {
+  const int32_t b = it.bcc;
+  const int64_t vo = a.vtx_off[b];
+  const int32_t nb = (int32_t)(a.vtx_off[b + 1] - vo);
+  if ((int64_t)nb + 2 > a.ws_n) { set_err(a.err, kDevWorkspace); return; }
+  const int64_t *R = a.row + vo;
+  const int32_t *rch = a.reach + vo;
+  double *bcb = a.bc + vo;
+  const MergeFilter none{nullptr, 0, 0, nullptr, 0, 0};
+
+  // own source: BFS into row A, then its dependency sweep
+  int baseA = sh.base_a;
+  ensure_epoch(r.dA, a.ws_n, baseA, nb);
+  const int nlevA = cta_bfs(sh, R, a.col, nb, it.src, r.dA, r.sA, r.SA, r.lvA, baseA);
+  const double wsrc = (double)rch[it.src] + 1.0;
+  for (int lev = nlevA - 1; lev >= 1; --lev) {
+    LevelList L{r.SA, r.lvA[lev], r.lvA[lev + 1], nullptr, 0, 0, -1, -1};
+    cta_bwd_level(sh, R, a.col, r.dA, r.sA, r.q, rch, bcb, wsrc, baseA + lev + 1, lev, 0, L, none);
+  }
+
+  int baseB = sh.base_b, nlevB = 0, prevR = -1;
+  for (int32_t c = it.c0; c < it.c1; ++c) {
+    const int32_t start = a.chain_start[c], len = a.chain_len[c], cr = a.chain_r[c];
+    if (a.chain_l[c] != it.src || start < 0 || start + len > nb) { set_err(a.err, kDevBadItem); break; }
+    if (cr != prevR) {
+      if (prevR >= 0) baseB += nlevB + 1;
+      ensure_epoch(r.dB, a.ws_n, baseB, nb);
+      nlevB = cta_bfs(sh, R, a.col, nb, cr, r.dB, r.sB, r.SB, r.lvB, baseB);
+      prevR = cr;
+    }
+    for (int32_t pos = 0; pos < len; ++pos) {
+      const int32_t z = start + pos;
+      const int ld = pos + 1, rd = len - pos;
+      const int maxlev = merge_rows(sh, r, baseA, baseB, nb, start, len, pos, a.err);
+      const double wz = (double)rch[z] + 1.0;
+      const MergeFilter mf{r.dA, baseA, ld, r.dB, baseB, rd};
+      for (int lev = maxlev; lev >= 1; --lev) {
+        LevelList L{r.SA, 0, 0, r.SB, 0, 0, -1, -1};
+        const int la = lev - ld, lb = lev - rd;
+        if (la >= 0 && la < nlevA) { L.a0 = r.lvA[la]; L.b0 = r.lvA[la + 1]; }
+        if (lb >= 0 && lb < nlevB) { L.a1 = r.lvB[lb]; L.b1 = r.lvB[lb + 1]; }
+        if (pos - lev >= 0) L.ck0 = start + pos - lev;
+        if (pos + lev < len) L.ck1 = start + pos + lev;
+        cta_bwd_level(sh, R, a.col, r.dM, r.sM, r.q, rch, bcb, wz, lev + 1, lev, 1, L, mf);
+      }
+    }
+  }
+  if (prevR >= 0) baseB += nlevB + 1;
+  if (threadIdx.x == 0) {
+    sh.base_a = baseA + nlevA + 1;
+    sh.base_b = baseB;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlock, 1) plain_kernel(PlainArgs a) {
+  __shared__ Shared sh;
+  const Rows r = rows_of(a, blockIdx.x);
+  if (threadIdx.x == 0) {
+    sh.base_a = a.epochs[2 * blockIdx.x];
+    sh.base_b = a.epochs[2 * blockIdx.x + 1];
+  }
+  __syncthreads();
+  while (true) {
+    if (threadIdx.x == 0) {
+      // stop early (uniformly for the CTA) once any CTA has flagged an error
+      const int64_t k = (int64_t)atomicAdd(a.next_item, 1ull);
+      sh.item = (*(volatile int *)a.err != kDevOk || a.item_begin + k >= a.item_end) ? -1 : (int)k;
+    }
+    __syncthreads();
+    if (sh.item < 0) break;
+    const PlainItem it = a.items[a.item_begin + sh.item];
+    process_item(sh, a, r, it);
+  }
+  if (threadIdx.x == 0) {
+    a.epochs[2 * blockIdx.x] = sh.base_a;
+    a.epochs[2 * blockIdx.x + 1] = sh.base_b;
+  }
+}
+
+// Rows of one source for the parity tests (one CTA).
+__global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bcc, int32_t src, int32_t chain,
+                                                         int32_t *d_out, double *s_out) {
+  __shared__ Shared sh;
+  const Rows r = rows_of(a, a.rows_slot);  // a slot no plain_kernel CTA uses
+  const int64_t vo = a.vtx_off[bcc];
+  const int32_t nb = (int32_t)(a.vtx_off[bcc + 1] - vo);
+  if ((int64_t)nb + 2 > a.ws_n) { set_err(a.err, kDevWorkspace); return; }
+  const int64_t *R = a.row + vo;
+  for (int k = threadIdx.x; k < nb; k += kBlock) { r.dA[k] = 0; r.dB[k] = 0; }
+  __syncthreads();
+  if (chain < 0) {
+    cta_bfs(sh, R, a.col, nb, src, r.dA, r.sA, r.SA, r.lvA, 1);
+    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dA[k] - 1; s_out[k] = r.sA[k]; }
+  } else {
+    const int32_t start = a.chain_start[chain], len = a.chain_len[chain];
+    cta_bfs(sh, R, a.col, nb, a.chain_l[chain], r.dA, r.sA, r.SA, r.lvA, 1);
+    cta_bfs(sh, R, a.col, nb, a.chain_r[chain], r.dB, r.sB, r.SB, r.lvB, 1);
+    merge_rows(sh, r, 1, 1, nb, start, len, src - start, a.err);
+    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dM[k]; s_out[k] = r.sM[k]; }
+  }
+}
+
+}  // namespace
+
+int plain_block() { return kBlock; }
+
+cudaError_t launch_plain(const PlainArgs &a, int grid, cudaStream_t stream) {
+  plain_kernel<<<grid, kBlock, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const PlainArgs &a, int32_t bcc, int32_t src, int32_t chain, int32_t *d_out, double *s_out,
+                        cudaStream_t stream) {
+  rows_kernel<<<1, kBlock, 0, stream>>>(a, bcc, src, chain, d_out, s_out);
+  return cudaGetLastError();
+}
+
+}  // namespace bcg

@@ -1,0 +1,161 @@
+/*
+ * libbcgpu — exact betweenness centrality on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI: plain pointers and sizes, status codes, no C++ or torch types.
+ * Every entry point returns BCGPU_OK (0) or an error code; the text of the
+ * last error is available from bc_last_error(). Nothing here calls exit().
+ * There is no CPU fallback: without a usable CUDA device bc_create fails.
+ *
+ * Method (the reference's, Goutam363/centrality-GPU): the graph is split into
+ * biconnected components (BCCs); every BCC of >= 3 vertices runs exact Brandes
+ * from each of its vertices, weighting sources and targets by reach + 1 (the
+ * number of vertices hanging off that vertex outside the BCC, itself
+ * included); sources on degree-2 chains take the merged rows of the chain's
+ * endpoints instead of a BFS; articulation points add the pairs they separate.
+ * BC counts ordered pairs (both directions).
+ */
+#ifndef BCGPU_H
+#define BCGPU_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status ---- */
+enum {
+  BCGPU_OK = 0,
+  BCGPU_EINVAL = 1,   /* bad argument or malformed input */
+  BCGPU_ECUDA = 2,    /* CUDA runtime error (no device, launch failure, ...) */
+  BCGPU_ENOMEM = 3,   /* device or host allocation failed / over the workspace limit */
+  BCGPU_ETIMEOUT = 4, /* a device-side wait ran out of its iteration limit */
+  BCGPU_EIO = 5,      /* file could not be read or parsed */
+  BCGPU_EOVERFLOW = 6 /* a size exceeds what the kernels index (e.g. > 2^31-1 arcs per BCC) */
+};
+
+/* Computation schedule. PLAIN: one source per CTA at a time, FP64 path
+ * counts and dependencies, FP64 atomics into BC. BATCHED: many sources per
+ * pass as a bitmask multi-source BFS, FP64 path counts with per-level
+ * power-of-two scaling, deterministic FP64 per-block BC partials. */
+enum { BCGPU_MODE_PLAIN = 0, BCGPU_MODE_BATCHED = 1 };
+/* Dependency (delta) arithmetic for the BATCHED mode. */
+enum { BCGPU_DELTA_FP64 = 0, BCGPU_DELTA_FP32C = 1 /* FP32 with two-sum compensated accumulation */ };
+
+typedef struct bc_opts {
+  int32_t device;        /* CUDA device ordinal; -1 = highest compute capability (reference choose_device) */
+  int32_t mode;          /* BCGPU_MODE_* */
+  int32_t delta;         /* BCGPU_DELTA_* (BATCHED only) */
+  int32_t batch_width;   /* sources per batched pass: multiple of 32, <= 1024; 0 = autotune */
+  void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context */
+  int64_t workspace_limit; /* device bytes the context may hold; 0 = 80% of free memory */
+} bc_opts;
+
+typedef struct bc_ctx bc_ctx;
+
+/* Fills opts with defaults (device -1, BATCHED, FP32C, autotuned width). */
+void bc_default_opts(bc_opts *opts);
+int bc_create(const bc_opts *opts, bc_ctx **out);
+void bc_destroy(bc_ctx *ctx);
+/* Message of the last failing call on ctx (or of bc_create when ctx is NULL). */
+const char *bc_last_error(const bc_ctx *ctx);
+
+/* -------------------------------------------------- packed BCC input ---- */
+/* All BCCs with >= 3 vertices, each a contiguous range of "packed" vertex ids.
+ * Within BCC b (n_b = vtx_off[b+1]-vtx_off[b] vertices) local ids run 0..n_b-1;
+ * local ids < n_plain[b] are free vertices or chain endpoints, the rest are
+ * degree-2 chain vertices, each chain contiguous from its left endpoint to its
+ * right endpoint. Arc lists use LOCAL neighbour ids; row[] holds global arc
+ * offsets. */
+typedef struct bc_bccs {
+  int32_t n_bcc;          /* BCCs listed (>= 3 vertices each) */
+  int32_t n_orig;         /* vertices of the original graph: length of BC output */
+  int64_t n_packed;       /* total packed vertices = vtx_off[n_bcc] */
+  int64_t n_arcs;         /* total arcs = row[n_packed] */
+  int64_t n_chains;       /* total chains = chain_off[n_bcc] */
+  const int64_t *vtx_off; /* [n_bcc+1] */
+  const int64_t *row;     /* [n_packed+1] global arc offsets */
+  const int32_t *col;     /* [n_arcs] local neighbour ids */
+  const int32_t *reach;   /* [n_packed] vertices hanging off the vertex outside its BCC */
+  const int32_t *orig;    /* [n_packed] original vertex id */
+  const int32_t *n_plain; /* [n_bcc] */
+  const int64_t *chain_off;   /* [n_bcc+1] chain-table range of each BCC */
+  const int32_t *chain_start; /* [n_chains] local id of the chain's first vertex (next to chain_l) */
+  const int32_t *chain_len;   /* [n_chains] degree-2 vertices on the chain */
+  const int32_t *chain_l;     /* [n_chains] local id of the left endpoint */
+  const int32_t *chain_r;     /* [n_chains] local id of the right endpoint */
+  const double *art;      /* [n_orig] articulation cross terms added to BC; may be NULL */
+} bc_bccs;
+
+typedef struct bc_stats {
+  int64_t sources;        /* sources whose dependencies were accumulated */
+  int64_t bfs_sources;    /* of which ran a forward BFS (the others were merged from chain endpoints) */
+  int64_t aux_bfs;        /* extra forward-only BFS runs for chain endpoints */
+  int64_t teps_edges;     /* sum over sources of the arcs of the source's BCC (TEPS numerator) */
+  double kernel_ms;       /* device time of the BC kernels (CUDA events) */
+  double total_ms;        /* device time of the whole call incl. copies */
+  int32_t kernel_launches;/* kernels this library launched */
+  int32_t batch_width;    /* width used (BATCHED) */
+} bc_stats;
+
+/* Whole computation, host buffers in and out: uploads the packed BCCs, runs
+ * every source of every BCC, adds the articulation terms and writes the BC of
+ * every original vertex (FP64, ordered pairs) to bc_out[n_orig] (overwritten).
+ * Replaces the per-BCC pair of begin_gpu calls in the reference's
+ * BiCC::to_eargraph loop (Codes/to_eargraph_construct.cpp:54-200). */
+int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats);
+
+/* ---------------------------------------------- mirrors of begin_gpu ---- */
+/* One BCC, free sources. Mirrors begin_gpu(R,C,F,n,m,ear_info,self_ear,
+ * req_nodes,artnodes,bc,time) (reference Codes/ear_graph.h:45-46,
+ * Codes/begin_gpupgm.cu:42-71): R[n+1], C[m] with m = number of ARCS (the
+ * reference passes 2x edges); sources req_nodes[n_req]; reach = artnodes[n].
+ * bc[n] is OVERWRITTEN with this call's contributions (FP64 computed, rounded
+ * to float as the reference's buffer type); *time_s is INCREASED by the device
+ * seconds spent. The reference's row-of-arc array F is not needed. */
+int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m, const int32_t *req_nodes,
+                  int32_t n_req, const int32_t *reach, float *bc, double *time_s);
+
+/* One BCC, chain endpoints ("active" vertices) and their chains ("ears").
+ * Mirrors the second begin_gpu overload (reference Codes/ear_graph.h:48-49,
+ * Codes/begin_gpupgm.cu:73-89, Codes/kernels_active.cu:18-223 with
+ * postprocess Codes/postprocesses.cu:8-203). Ears are flattened: ear e runs
+ * from lnode[e] to rnode[e] through cnt[e] degree-2 vertices
+ * nodes[off[e] .. off[e]+cnt[e]) with path distances ld/rd to the two ends
+ * (ear_premble, Codes/ear_graph.h:3-32). Every active vertex and every ear
+ * vertex is a source. bc[n] is READ and the contributions ADDED (the
+ * reference seeds its device buffer from bc, Codes/kernels_active.cu:78);
+ * *time_s is increased. */
+int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m, const int32_t *active,
+                    int32_t n_active, int32_t n_ears, const int32_t *lnode, const int32_t *rnode, const int32_t *cnt,
+                    const int32_t *off, const int32_t *nodes, const int32_t *ld, const int32_t *rd,
+                    const int32_t *reach, float *bc, double *time_s);
+
+/* ------------------------------------ device-resident plans (benchmark) -- */
+/* A plan uploads the packed BCCs once and keeps the BC accumulator on the
+ * device. Work is split into units (PLAIN: one free/endpoint source plus the
+ * chains it owns; BATCHED: one multi-source pass); running a range of units
+ * accumulates their contributions. */
+typedef struct bc_plan bc_plan;
+int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out);
+void bc_plan_destroy(bc_plan *plan);
+int64_t bc_plan_num_units(const bc_plan *plan);
+/* Sources and TEPS arcs covered by units [begin, end). */
+int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *sources, int64_t *teps_edges);
+/* Device buffers the plan consumes (for roofline accounting). */
+int64_t bc_plan_device_bytes(const bc_plan *plan);
+int bc_plan_reset(bc_plan *plan);
+/* Enqueues units [begin, end) on the context's stream; asynchronous unless
+ * stats is non-NULL (then synchronises and fills it). */
+int bc_plan_run(bc_plan *plan, int64_t begin, int64_t end, bc_stats *stats);
+/* Synchronises, copies BC to the host and adds the articulation terms. */
+int bc_plan_read(bc_plan *plan, double *bc_out);
+/* Levels and path counts of one source (packed id) as the GPU computes them
+ * (BFS, or the chain merge for chain vertices); d_out/sigma_out have the
+ * source's BCC size. For parity tests. */
+int bc_plan_source_rows(bc_plan *plan, int64_t packed_source, int32_t *d_out, double *sigma_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BCGPU_H */

@@ -1,0 +1,55 @@
+/*
+ * libbcgpu host side — graph ingest and the decomposition that feeds the GPU.
+ * Same C ABI conventions as bcgpu.h (status codes, no exit()).
+ *
+ * Replaces the reference's host pipeline ahead of begin_gpu:
+ *   Graph::Graph(char*)                Codes/graph.cpp:38-59     -> bc_graph_load / bc_graph_from_edges
+ *   BiCC::run_bicc / bicc_tarjan       Codes/bicc.cpp:39,81-161  -> bc_decompose (iterative, no recursion)
+ *   per-BCC relabel                    Codes/modified_apsp.cpp:273-363
+ *   fillbccparent / reachfunction      Codes/modified_apsp.cpp:77-220 (reach, articulation terms)
+ *   bcc_bfs + preSum (ear chains)      Codes/bcc_bfs.cpp:247-1330, :100-236
+ *   parse_active_nodes / read_ear_info Codes/make_ear_graph.cpp:119-218, Codes/readeardata.cpp:117-192
+ */
+#ifndef BCHOST_H
+#define BCHOST_H
+#include "bcgpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Simple undirected graph in CSR (self loops dropped, duplicate edges merged). */
+typedef struct bc_graph bc_graph;
+
+/* Reads the reference's edge-list file: "n m" then m lines "u v w" (0-based,
+ * w ignored as in the reference's BFS). Writes a message to err on failure. */
+int bc_graph_load(const char *path, bc_graph **out, char *err, size_t errlen);
+int bc_graph_from_edges(int32_t n, int64_t m, const int32_t *u, const int32_t *v, bc_graph **out);
+void bc_graph_free(bc_graph *g);
+/* Borrowed views of the CSR: row[n+1] (int64), col[row[n]] (int32). */
+int bc_graph_csr(const bc_graph *g, int32_t *n, int64_t *n_arcs, const int64_t **row, const int32_t **col);
+
+typedef struct bc_decomp bc_decomp;
+typedef struct bc_decomp_info {
+  int32_t n_components;   /* connected components (isolated vertices included) */
+  int32_t n_bcc_all;      /* all BCCs incl. bridges */
+  int32_t n_bcc_packed;   /* BCCs of >= 3 vertices (those with BFS work) */
+  int32_t n_articulation;
+  int64_t n_chain_vertices;
+  int64_t n_chains;
+  int64_t n_cycle_bccs;   /* BCCs that are a single cycle: all their vertices are free sources */
+  double host_ms;         /* wall time of bc_decompose */
+} bc_decomp_info;
+
+/* Splits g into BCCs, computes reach and articulation terms, finds degree-2
+ * chains and packs every BCC of >= 3 vertices (largest first). */
+int bc_decompose(const bc_graph *g, bc_decomp **out);
+void bc_decomp_free(bc_decomp *d);
+/* Borrowed view, valid until bc_decomp_free. */
+const bc_bccs *bc_decomp_view(const bc_decomp *d);
+void bc_decomp_get_info(const bc_decomp *d, bc_decomp_info *info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BCHOST_H */

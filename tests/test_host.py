@@ -1,0 +1,148 @@
+"""Host side of the product (C++ in libbcgpu.so): edge-list ingest and the
+BCC / reach / chain decomposition, checked against the reference's own host
+pipeline (golden dumps) and the brute-force oracle. CPU only."""
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, GOLDEN_CASES, graphs, has_gpu, load_case, oracle, pkg, product_bccs, rel_err
+from test_oracle import _oracle_bccs, compare_to_reference
+
+
+def decompose(n, u, v):
+    P = pkg()
+    return P.Decomposition(P.Graph.from_edges(n, u, v))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_decomposition_matches_reference(name):
+    n, u, v, _, ref = load_case(name)
+    arrs = decompose(n, u, v).arrays()
+    compare_to_reference(product_bccs(arrs), arrs["art"], ref, u, v)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_packed_bccs_give_golden_bc(name):
+    """The product's packing, driven through the oracle's per-BCC kernel."""
+    n, u, v, bc, _ = load_case(name)
+    arrs = decompose(n, u, v).arrays()
+    assert rel_err(oracle().method_bc_from_decomp(arrs), bc) < 1e-12
+
+
+def random_graph(seed):
+    """Disconnected graphs, isolated vertices, pendant cycles, loops and duplicates."""
+    G = graphs()
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 70))
+    m = int(rng.integers(0, 2 * n + 1))
+    u = rng.integers(0, n, m)
+    v = rng.integers(0, n, m)
+    if seed % 3 == 0 and n > 3:  # a ring
+        u = np.concatenate([u, np.arange(n)])
+        v = np.concatenate([v, (np.arange(n) + 1) % n])
+    uu, vv = G.simple_edges(n, u, v)
+    if len(uu) and seed % 2:
+        n, uu, vv = G.subdivide(n, uu, vv, 0.4, 1, 3, rng)
+    # what the product is fed: the simple edges plus reversed duplicates and loops
+    k = len(uu) // 3
+    ru = np.concatenate([uu, vv[:k], np.arange(min(n, 3))])
+    rv = np.concatenate([vv, uu[:k], np.arange(min(n, 3))])
+    return n, ru, rv, uu, vv
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_decomposition_matches_oracle(seed):
+    n, u_raw, v_raw, u, v = random_graph(seed)
+    P = pkg()
+    arrs = P.Decomposition(P.Graph.from_edges(n, u_raw, v_raw)).arrays()  # raw: loops + duplicates
+    mine = {b["verts"]: b for b in product_bccs(arrs)}
+    theirs, art = _oracle_bccs(n, u, v)
+    assert set(mine) == {b["verts"] for b in theirs}
+    for b in theirs:
+        m = mine[b["verts"]]
+        assert m["reach"] == b["reach"]
+        assert m["chains"] == b["chains"]
+        assert m["free"] == b["free"]
+    assert np.array_equal(arrs["art"], art)
+    row, col = oracle().csr(n, u, v)
+    assert rel_err(oracle().method_bc_from_decomp(arrs), oracle().brandes(n, row, col)) < 1e-12
+
+
+def test_packing_invariants():
+    G = graphs()
+    n, u, v = G.gen_rmat(10, 8, chain_frac=0.2, seed=11)
+    arrs = decompose(n, u, v).arrays()
+    vo, row, col = arrs["vtx_off"], arrs["row"], arrs["col"]
+    sizes = np.diff(vo)
+    assert np.all(sizes >= 3) and np.all(np.diff(sizes) <= 0)  # largest first
+    for b in range(arrs["n_bcc"]):
+        nb = sizes[b]
+        seg = col[row[vo[b]]:row[vo[b + 1]]]
+        assert seg.min() >= 0 and seg.max() < nb
+        for k in range(vo[b], vo[b + 1]):
+            adj = col[row[k]:row[k + 1]]
+            assert np.all(np.diff(adj) > 0)  # sorted, no duplicates
+        c0, c1 = arrs["chain_off"][b], arrs["chain_off"][b + 1]
+        assert np.all(np.diff(arrs["chain_l"][c0:c1]) >= 0)  # grouped by owner
+        covered = arrs["chain_len"][c0:c1].sum()
+        assert covered == nb - arrs["n_plain"][b]
+        for c in range(c0, c1):
+            s, ln = arrs["chain_start"][c], arrs["chain_len"][c]
+            for i in range(ln):  # every chain vertex has degree 2 and sits between its neighbours
+                k = vo[b] + s + i
+                assert row[k + 1] - row[k] == 2
+                prev = arrs["chain_l"][c] if i == 0 else s + i - 1
+                nxt = arrs["chain_r"][c] if i == ln - 1 else s + i + 1
+                assert set(col[row[k]:row[k + 1]].tolist()) == {prev, nxt}
+
+
+def test_graph_load_and_errors(tmp_path):
+    P = pkg()
+    g = P.Graph.load(GOLDEN / "sample1.txt")
+    n, row, col = g.csr()
+    assert n == 9 and row[-1] == 24
+    dup = tmp_path / "dup.txt"
+    dup.write_text("4 6\n0 1 1\n1 0 1\n1 1 1\n1 2 1\n2 3 1\n3 2 1\n")
+    n, row, col = P.Graph.load(dup).csr()
+    assert row.tolist() == [0, 1, 3, 5, 6]  # loop dropped, duplicates merged
+    bad = tmp_path / "trunc.txt"
+    bad.write_text("5 4\n0 1 1\n1 2 1\n")
+    with pytest.raises(P.BcError) as e:
+        P.Graph.load(bad)
+    assert e.value.code == P.EIO and "truncated" in str(e.value)
+    oob = tmp_path / "oob.txt"
+    oob.write_text("3 1\n0 7 1\n")
+    with pytest.raises(P.BcError) as e:
+        P.Graph.load(oob)
+    assert e.value.code == P.EIO
+    with pytest.raises(P.BcError):
+        P.Graph.load(tmp_path / "missing.txt")
+    empty = tmp_path / "empty.txt"
+    empty.write_text("0 0\n")
+    d = P.Decomposition(P.Graph.load(empty))
+    assert d.arrays()["n_bcc"] == 0
+
+
+def test_generators_are_simple_and_seeded():
+    G = graphs()
+    for gen in (lambda: G.gen_small(1), lambda: G.gen_rmat(9, 8, seed=3), lambda: G.gen_grid(24, leaves=50),
+                lambda: G.pack_graphs(G.gen_ba_batch(5, 50, 200))[:3]):
+        n, u, v = gen()
+        assert np.all(u < v) and len(np.unique(u.astype(np.int64) * n + v)) == len(u)
+        n2, u2, v2 = gen()
+        assert n == n2 and np.array_equal(u, u2) and np.array_equal(v, v2)
+    n, u, v = G.gen_small(1)
+    assert n == 2000
+    deg = np.bincount(np.concatenate([u, v]), minlength=n)
+    assert np.all(deg[1500:] == 2) and np.all(deg[1000:1500] >= 1)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure path")
+def test_betc_fails_loudly_without_gpu():
+    P = pkg()
+    r = subprocess.run([str(P.BETC_PATH), str(GOLDEN / "sample1.txt")], capture_output=True, text=True)
+    assert r.returncode == 4 and "CUDA" in r.stderr
+    with pytest.raises(P.BcError) as e:
+        P.Context()
+    assert e.value.code == P.ECUDA
