@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark: exact-BC TEPS on one B200 (or N, one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode batched|plain] [--workload rmat20|rmat16|grid|ba|small]
+
+A step is one pass of the BC kernels over one batch of sources of the
+workload graph (inputs resident in HBM). TEPS = sum over processed sources of
+the arcs of the source's biconnected component / device time. Prints ONE
+JSON line on rank 0.
+
+--impl reference times the reference method's CPU restatement (the oracle's
+per-BCC kernel, C + OpenMP, all host cores) on bounded source samples of the
+same workload: the reference itself has no CPU BC path.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "centrality-gpu_b200"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_pkg():
+    name = "centrality_gpu_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, PKG_DIR / "__init__.py", submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+WORKLOADS = {
+    "rmat20": ("RMAT scale 20, edge factor 16 (a,b,c)=(0.57,0.19,0.19), symmetrised/deduplicated, "
+               "10% of edges subdivided into chains of 1-4", lambda G: G.gen_rmat(20, 16, 0.1, 1, 4, seed=5)),
+    "rmat16": ("RMAT scale 16, edge factor 16, 20% of edges subdivided into chains of 1-8",
+               lambda G: G.gen_rmat(16, 16, 0.2, 1, 8, seed=2)),
+    "grid": ("512x512 grid, 10% edges deleted, p=0.3 chains of 1-4, 15000 leaves", lambda G: G.gen_grid(seed=3)),
+    "ba": ("4096 Barabasi-Albert m=2 graphs, n log-uniform 50..5000, 10% chains of 1-3, n/10 leaves, packed",
+           lambda G: G.pack_graphs(G.gen_ba_batch(4096, seed=4))[:3]),
+    "small": ("2000 vertices: 1000-vertex 3-out core, 500 pendants, 100 chains of 5", lambda G: G.gen_small(1)),
+}
+
+
+def clocks_start():
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=f, stderr=subprocess.DEVNULL)
+    except OSError:
+        p = None
+    return p, f.name
+
+
+def clocks_stop(handle, gpu_index):
+    p, path = handle
+    if p is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    p.terminate()
+    p.wait()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in Path(path).read_text().splitlines():
+        t = [x.strip() for x in line.split(",")]
+        if len(t) < 9 or t[0] != str(gpu_index):
+            continue
+        try:
+            sm.append(float(t[1]))
+            mx.append(float(t[2]))
+        except ValueError:
+            continue
+        for nme, val in zip(names, t[5:9]):
+            if val.lower() == "active":
+                reasons.add(nme)
+    os.unlink(path)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peak_hbm():
+    try:
+        d = json.loads(PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def step_ranges(plan, target_sources):
+    """Contiguous unit ranges holding >= target_sources sources each."""
+    n = plan.n_units
+    total = plan.unit_work(0, n)[0]
+    bounds = [0]
+    k = 1
+    while bounds[-1] < n:
+        want = k * target_sources
+        if want >= total:
+            bounds.append(n)
+            break
+        lo, hi = bounds[-1] + 1, n
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if plan.unit_work(0, mid)[0] >= want:
+                hi = mid
+            else:
+                lo = mid + 1
+        bounds.append(lo)
+        k += 1
+    return list(zip(bounds[:-1], bounds[1:]))
+
+
+def cpu_sample(P, arrs, budget_s, threads):
+    """Times the oracle's per-BCC kernel (CPU restatement of the method) on an
+    evenly spaced sample of the largest BCC's sources, sized to ~budget_s."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O  # the checker: CPU-baseline leg only
+    nb = int(arrs["vtx_off"][1] - arrs["vtx_off"][0])
+    arcs = int(arrs["row"][arrs["vtx_off"][1]] - arrs["row"][arrs["vtx_off"][0]])
+    probe = np.linspace(0, nb - 1, num=max(threads, 1), dtype=np.int64).astype(np.int32)
+    t = time.perf_counter()
+    O.bcc_sources(arrs, 0, probe, threads)
+    dt = time.perf_counter() - t
+    count = int(min(nb, max(len(probe), len(probe) * budget_s / max(dt, 1e-3))))
+    sample = np.linspace(0, nb - 1, num=count, dtype=np.int64).astype(np.int32)
+    t = time.perf_counter()
+    O.bcc_sources(arrs, 0, sample, threads)
+    dt = time.perf_counter() - t
+    return {"sources": count, "arcs": arcs, "vertices": nb, "seconds": dt, "gteps": count * arcs / dt / 1e9}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    P = load_pkg()
+    from centrality_gpu_b200 import graphs as G
+    desc, gen = WORKLOADS[args.workload]
+    n, u, v = gen(G)
+    d = P.Decomposition(P.Graph.from_edges(n, u, v))
+    arrs = d.arrays()
+    threads = len(os.sched_getaffinity(0))
+    for _ in range(args.warmup):
+        cpu_sample(P, arrs, 0.5, threads)
+    res = [cpu_sample(P, arrs, args.ref_step_s, threads) for _ in range(args.steps)]
+    secs = sum(r["seconds"] for r in res)
+    value = sum(r["sources"] * r["arcs"] for r in res) / secs / 1e9
+    line = {
+        "impl": "reference", "metric": "exact-BC TEPS (CPU restatement of the reference method)", "value": value,
+        "unit": "GTEPS", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{args.workload}: {desc}", "sample": "evenly spaced sources of the largest BCC"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
+                         "sample": f"{res[0]['sources']} sources/step of the largest BCC "
+                                   f"({res[0]['vertices']} vertices, {res[0]['arcs']} arcs)"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["batched", "plain"], default="plain")
+    ap.add_argument("--delta", choices=["fp32c", "fp64"], default="fp32c")
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat20")
+    ap.add_argument("--step-sources", type=int, default=0, help="sources per step (0 = by workload and mode)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--ref-step-s", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workspace-gb", type=float, default=0.0,
+                    help="cap the device workspace (0 = library default); used to keep profiler captures small")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    P = load_pkg()
+    from centrality_gpu_b200 import graphs as G
+    desc, gen = WORKLOADS[args.workload]
+    t0 = time.perf_counter()
+    n, u, v = gen(G)
+    graph = P.Graph.from_edges(n, u, v)
+    d = P.Decomposition(graph)
+    host_s = time.perf_counter() - t0
+    arrs = d.arrays()
+    mode = P.MODE_BATCHED if args.mode == "batched" else P.MODE_PLAIN
+    delta = P.DELTA_FP32C if args.delta == "fp32c" else P.DELTA_FP64
+    stream = torch.cuda.current_stream()
+    ctx = P.Context(mode=mode, delta=delta, batch_width=args.batch, device=local, stream=stream.cuda_stream,
+                    workspace_limit=int(args.workspace_gb * 2**30))
+    plan = ctx.plan(d)
+    target = args.step_sources or (16384 if mode == P.MODE_BATCHED else 2048)
+    ranges = step_ranges(plan, target)
+    mine = ranges[rank::world]
+    need = args.warmup + args.steps
+    sel = [mine[i % len(mine)] for i in range(need)]
+
+    for r0, r1 in sel[:args.warmup]:
+        plan.run(r0, r1, stats=False)
+    torch.cuda.synchronize()
+    st = plan.run(*sel[0], stats=True)  # launches per step
+    launches_per_unit = st["kernel_launches"]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks_start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i, (r0, r1) in enumerate(sel[args.warmup:]):
+        evs[i][0].record(stream)
+        plan.run(r0, r1, stats=False)
+        evs[i][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clocks_stop(clk, local)
+    elapsed = t_start.elapsed_time(t_end)
+    per_step = [a.elapsed_time(b) for a, b in evs]
+    work = np.array([plan.unit_work(r0, r1) for r0, r1 in sel[args.warmup:]], dtype=np.float64)
+    sources, teps, visits = work.sum(axis=0)
+    tot = torch.tensor([teps, sources, visits], dtype=torch.float64, device="cuda")
+    mx = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(tot)
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    teps_all, sources_all, visits_all = tot.tolist()
+    elapsed_max = mx.item()
+    value = teps_all / (elapsed_max * 1e-3) / 1e9
+
+    # roofline: algorithmic bytes per source (16 B per arc + 48 B per vertex of its BCC)
+    peak, peak_kind = peak_hbm()
+    alg_bytes = 16.0 * teps + 48.0 * visits
+    avg_launch_ms = float(np.mean(per_step))
+    achieved = alg_bytes / args.steps / (avg_launch_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": None,
+                "alg_bytes_per_launch": alg_bytes / args.steps, "avg_launch_ms": avg_launch_ms}
+
+    # end to end through the public API with host buffers (uploads + download inside)
+    e2e = None
+    if args.e2e_steps > 0:
+        torch.cuda.synchronize()
+        e_sel = sel[args.warmup:args.warmup + args.e2e_steps]
+        out = np.zeros(n, dtype=np.float64)
+        te = time.perf_counter()
+        for r0, r1 in e_sel:
+            ctx.run_units(d, r0, r1, with_art=False, out=out)
+        te = time.perf_counter() - te
+        e_teps = sum(plan.unit_work(r0, r1)[1] for r0, r1 in e_sel)
+        h2d = sum(int(arrs[k].nbytes) for k in ("vtx_off", "row", "col", "reach", "chain_start", "chain_len",
+                                               "chain_l", "chain_r"))
+        e2e = {"value": e_teps / te / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(arrs["n_packed"]) * 8, "steps": len(e_sel)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        s = cpu_sample(P, arrs, args.cpu_budget_s, len(os.sched_getaffinity(0)))
+        cpu = {"value": s["gteps"], "unit": "GTEPS", "cores": len(os.sched_getaffinity(0)), "kind": "port",
+               "sample": f"{s['sources']} evenly spaced sources of the largest BCC ({s['vertices']} vertices, "
+                         f"{s['arcs']} arcs), oracle per-BCC kernel, {s['seconds']:.1f} s"}
+
+    if rank == 0:
+        info = d.info
+        line = {
+            "metric": "exact-BC TEPS on 1 B200", "value": value, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if (mode == P.MODE_PLAIN or delta == P.DELTA_FP64) else "f32c",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"{args.workload}: {desc}", "mode": args.mode,
+                       "delta": "fp64" if mode == P.MODE_PLAIN else args.delta, "vertices": int(n),
+                       "edges": int(len(u)), "largest_bcc": int(arrs["vtx_off"][1]) if arrs["n_bcc"] else 0,
+                       "chain_vertices": info["n_chain_vertices"], "sources_per_step": sources_all / args.steps / world,
+                       "units_per_step": float(np.mean([r1 - r0 for r0, r1 in sel])),
+                       "host_decomposition_s": round(host_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
+                       "parallelism": f"sources sharded over {world} GPU(s)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": int(launches_per_unit * args.steps),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -72,6 +72,8 @@ _SIGS = {
     "bc_destroy": (None, [C.c_void_p]),
     "bc_last_error": (C.c_char_p, [C.c_void_p]),
     "bc_run_bccs": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), _f64p, C.POINTER(BcStats)]),
+    "bc_run_bccs_units": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), C.c_int64, C.c_int64, C.c_int32, _f64p,
+                                    C.POINTER(BcStats)]),
     "bc_begin_free": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, _i32p, _f32p,
                                 _f64p]),
     "bc_begin_active": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, C.c_int32,
@@ -79,7 +81,7 @@ _SIGS = {
     "bc_plan_create": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), C.POINTER(C.c_void_p)]),
     "bc_plan_destroy": (None, [C.c_void_p]),
     "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
-    "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p]),
+    "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p, _i64p]),
     "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
     "bc_plan_reset": (C.c_int, [C.c_void_p]),
     "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
@@ -247,6 +249,15 @@ class Context:
         self._check(lib().bc_run_bccs(self._h, decomp.view, _ptr(out, _f64p), C.byref(st)))
         return out, st.as_dict()
 
+    def run_units(self, decomp: Decomposition, begin, end, with_art=False, out=None):
+        """Units [begin, end) only, host buffers in and out (uploads included)."""
+        if out is None:
+            out = np.zeros(decomp.view.contents.n_orig, dtype=np.float64)
+        st = BcStats()
+        self._check(lib().bc_run_bccs_units(self._h, decomp.view, int(begin), int(end), int(with_art),
+                                            _ptr(out, _f64p), C.byref(st)))
+        return out, st.as_dict()
+
     def plan(self, decomp: Decomposition):
         return Plan(self, decomp)
 
@@ -275,11 +286,13 @@ class Plan:
         self.device_bytes = lib().bc_plan_device_bytes(h)
 
     def unit_work(self, begin=0, end=None):
+        """(sources, TEPS arcs, vertex visits) of units [begin, end)."""
         end = self.n_units if end is None else end
         s = C.c_int64()
         t = C.c_int64()
-        self.ctx._check(lib().bc_plan_unit_work(self._h, begin, end, C.byref(s), C.byref(t)))
-        return s.value, t.value
+        w = C.c_int64()
+        self.ctx._check(lib().bc_plan_unit_work(self._h, begin, end, C.byref(s), C.byref(t), C.byref(w)))
+        return s.value, t.value, w.value
 
     def reset(self):
         self.ctx._check(lib().bc_plan_reset(self._h))

@@ -27,9 +27,10 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
 void batched_destroy(BatchedPlan *p);
 int64_t batched_device_bytes(const BatchedPlan *p);
 int batched_width(const BatchedPlan *p);
-// Prefix sums over passes of sources, TEPS arcs, BFS sources and aux BFS runs.
+// Prefix sums over passes of sources, TEPS arcs, BFS sources, aux BFS runs
+// and vertex visits.
 void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std::vector<int64_t> &teps,
-                       std::vector<int64_t> &bfs, std::vector<int64_t> &aux);
+                       std::vector<int64_t> &bfs, std::vector<int64_t> &aux, std::vector<int64_t> &visits);
 int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream, int *launches, std::string *msg);
 
 }  // namespace bcg

@@ -52,11 +52,11 @@ struct bc_plan {
   int32_t *ws_i = nullptr, *epochs = nullptr;
   double *ws_f = nullptr;
   int64_t ws_n = 0;
-  int grid = 0;
+  int grid = 0, block = 1024;
   // BATCHED
   bcg::BatchedPlan *bp = nullptr;
   // per-unit work (prefix sums over units)
-  std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux;
+  std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux, unit_visits;
   int64_t device_bytes = 0;
   std::vector<void *> allocs;
 };
@@ -159,14 +159,26 @@ int validate(bc_ctx *ctx, const bc_bccs *B) {
   return BCGPU_OK;
 }
 
+// Chain vertices per PLAIN work item: bounds the longest item so the dynamic
+// queue stays balanced when a hub owns thousands of chains.
+constexpr int64_t kItemChainVertices = 16;
+
 void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items) {
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     int64_t c = B->chain_off[b];
     const int64_t ce = B->chain_off[b + 1];
     for (int32_t s = 0; s < B->n_plain[b]; ++s) {
-      int64_t c0 = c;
-      while (c < ce && B->chain_l[c] == s) ++c;
-      items.push_back({b, s, (int32_t)c0, (int32_t)c});
+      int32_t own = 1;
+      do {
+        const int64_t c0 = c;
+        int64_t verts = 0;
+        while (c < ce && B->chain_l[c] == s && (verts == 0 || verts + B->chain_len[c] <= kItemChainVertices)) {
+          verts += B->chain_len[c];
+          ++c;
+        }
+        items.push_back({b, s, (int32_t)c0, (int32_t)c, own});
+        own = 0;
+      } while (c < ce && B->chain_l[c] == s);
     }
   }
 }
@@ -218,9 +230,10 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     p->unit_teps.assign(items.size() + 1, 0);
     p->unit_bfs.assign(items.size() + 1, 0);
     p->unit_aux.assign(items.size() + 1, 0);
+    p->unit_visits.assign(items.size() + 1, 0);
     for (size_t i = 0; i < items.size(); ++i) {
       const auto &it = items[i];
-      int64_t src = 1, aux = 0;
+      int64_t src = it.own ? 1 : 0, aux = it.own ? 0 : 1;
       int32_t prev = -1;
       for (int32_t c = it.c0; c < it.c1; ++c) {
         src += B->chain_len[c];
@@ -229,16 +242,24 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
       const int64_t arcs = B->row[B->vtx_off[it.bcc + 1]] - B->row[B->vtx_off[it.bcc]];
       p->unit_sources[i + 1] = p->unit_sources[i] + src;
       p->unit_teps[i + 1] = p->unit_teps[i] + src * arcs;
-      p->unit_bfs[i + 1] = p->unit_bfs[i] + 1;
+      p->unit_bfs[i + 1] = p->unit_bfs[i] + (it.own ? 1 : 0);
       p->unit_aux[i + 1] = p->unit_aux[i] + aux;
+      p->unit_visits[i + 1] = p->unit_visits[i] + src * (B->vtx_off[it.bcc + 1] - B->vtx_off[it.bcc]);
     }
     if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
     p->ws_n = nb_max + 2;
     const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
-    int grid = ctx->sms;  // one 1024-thread CTA per SM
-    int64_t avail = limit - p->device_bytes - 2 * (int64_t)sizeof(int32_t) * (grid + 1);
+    // Four 256-thread CTAs per SM (four sources in flight) when their rows
+    // fit the budget, else two of 512, else one of 1024 per SM.
+    int64_t avail = limit - p->device_bytes - 64 * (int64_t)ctx->sms;
     if (avail < 2 * per_slot) return bail(fail(ctx, BCGPU_ENOMEM, "workspace for the largest BCC exceeds the limit"));
-    grid = (int)std::min<int64_t>(grid, avail / per_slot - 1);
+    int grid = 0;
+    for (int block : {256, 512, 1024}) {
+      const int want = ctx->sms * (1024 / block);
+      grid = (int)std::min<int64_t>(want, avail / per_slot - 1);
+      p->block = block;
+      if (grid == want) break;
+    }
     p->grid = std::max(1, grid);
     const int64_t slots = p->grid + 1;  // + the row-export slot
     if ((rc = dalloc(p, &p->ws_i, slots * 7 * p->ws_n)) || (rc = dalloc(p, &p->ws_f, slots * 4 * p->ws_n)) ||
@@ -259,7 +280,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
     if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
     p->device_bytes += bcg::batched_device_bytes(p->bp);
-    bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux);
+    bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux, p->unit_visits);
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   *out = p;
@@ -360,12 +381,14 @@ extern "C" int64_t bc_plan_num_units(const bc_plan *p) {
   return p ? (int64_t)p->unit_sources.size() - 1 : 0;
 }
 
-extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, int64_t *sources, int64_t *teps) {
+extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, int64_t *sources, int64_t *teps,
+                                 int64_t *visits) {
   if (!p) return BCGPU_EINVAL;
   const int64_t n = bc_plan_num_units(p);
   if (begin < 0 || end < begin || end > n) return fail(p->ctx, BCGPU_EINVAL, "unit range out of bounds");
   if (sources) *sources = p->unit_sources[end] - p->unit_sources[begin];
   if (teps) *teps = p->unit_teps[end] - p->unit_teps[begin];
+  if (visits) *visits = p->unit_visits[end] - p->unit_visits[begin];
   return BCGPU_OK;
 }
 
@@ -397,7 +420,7 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
       a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
       a.err = p->err;
       const int grid = (int)std::min<int64_t>(p->grid, end - begin);
-      CK(ctx, bcg::launch_plain(a, grid, ctx->stream));
+      CK(ctx, bcg::launch_plain(a, p->block, grid, ctx->stream));
       launches = 1;
     } else {
       std::string msg;
@@ -472,7 +495,10 @@ extern "C" int bc_plan_source_rows(bc_plan *p, int64_t packed, int32_t *d_out, d
   return check_dev_err(p);
 }
 
-extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats) {
+namespace {
+
+int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool all, bool with_art, double *bc_out,
+              bc_stats *stats) {
   if (!ctx || !bccs || !bc_out) return fail(ctx, BCGPU_EINVAL, "null argument");
   CK(ctx, cudaSetDevice(ctx->device));
   cudaEvent_t t0, t1;
@@ -482,8 +508,11 @@ extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_
   bc_plan *p = nullptr;
   int rc = create_plan(ctx, bccs, nullptr, &p);
   bc_stats st{};
-  if (!rc) rc = bc_plan_run(p, 0, bc_plan_num_units(p), &st);
+  if (!rc && all) { begin = 0; end = bc_plan_num_units(p); }
+  if (!rc) rc = bc_plan_run(p, begin, end, &st);
   if (!rc) rc = bc_plan_read(p, bc_out);
+  if (!rc && !with_art && !p->art.empty())
+    for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] -= p->art[v];
   if (!rc) {
     if (cudaEventRecord(t1, ctx->stream) == cudaSuccess && cudaEventSynchronize(t1) == cudaSuccess) {
       float ms = 0.f;
@@ -496,6 +525,17 @@ extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   return rc;
+}
+
+}  // namespace
+
+extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats) {
+  return run_units(ctx, bccs, 0, 0, true, true, bc_out, stats);
+}
+
+extern "C" int bc_run_bccs_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t unit_begin, int64_t unit_end,
+                                 int32_t with_art, double *bc_out, bc_stats *stats) {
+  return run_units(ctx, bccs, unit_begin, unit_end, false, with_art != 0, bc_out, stats);
 }
 
 namespace {
@@ -567,7 +607,7 @@ extern "C" int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, in
   std::vector<bcg::PlainItem> items;
   for (int32_t i = 0; i < n_req; ++i) {
     if (req_nodes[i] < 0 || req_nodes[i] >= n) return fail(ctx, BCGPU_EINVAL, "req_nodes out of range");
-    items.push_back({0, req_nodes[i], 0, 0});
+    items.push_back({0, req_nodes[i], 0, 0, 1});
   }
   std::vector<double> out;
   rc = run_one(ctx, o, items, out, time_s);
@@ -649,7 +689,7 @@ extern "C" int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, 
   for (int32_t k = 0; k < nplain; ++k) {
     size_t c0 = c;
     while (c < o.chain_l.size() && o.chain_l[c] == k) ++c;
-    if (is_active[old[k]] || c > c0) items.push_back({0, k, (int32_t)c0, (int32_t)c});
+    if (is_active[old[k]] || c > c0) items.push_back({0, k, (int32_t)c0, (int32_t)c, is_active[old[k]] ? 1 : 0});
   }
   std::vector<double> out;
   rc = run_one(ctx, o, items, out, time_s);

@@ -17,7 +17,7 @@ void batched_destroy(BatchedPlan *p) { delete p; }
 int64_t batched_device_bytes(const BatchedPlan *) { return 0; }
 int batched_width(const BatchedPlan *) { return 0; }
 void batched_unit_work(const BatchedPlan *, std::vector<int64_t> &, std::vector<int64_t> &, std::vector<int64_t> &,
-                       std::vector<int64_t> &) {}
+                       std::vector<int64_t> &, std::vector<int64_t> &) {}
 int batched_run(BatchedPlan *, int64_t, int64_t, cudaStream_t, int *, std::string *msg) {
   if (msg) *msg = "the BATCHED schedule is not available in this build";
   return BCGPU_EINVAL;

@@ -21,9 +21,10 @@
 //    (Codes/postprocesses.cu:329-351) and its dependency sweep walks the
 //    endpoints' level buckets directly instead of radix-sorting n distance
 //    keys per source (Codes/postprocesses.cu:143-155).
-// A work item is one free/endpoint source plus the chains whose left endpoint
-// it is, so the left endpoint's BFS serves all of them and only the right
-// endpoint's BFS is repeated (forward only) per distinct right endpoint.
+// A work item is one free/endpoint source plus (a bounded share of) the
+// chains whose left endpoint it is, so the left endpoint's BFS serves all of
+// them and only the right endpoint's BFS is repeated (forward only) per
+// distinct right endpoint.
 #include "common.cuh"
 #include "plain.h"
 
@@ -35,19 +36,19 @@ namespace bcg {
 
 namespace {
 
-constexpr int kBlock = 1024;
-constexpr int kWarps = kBlock / 32;
 constexpr int kSmallDeg = 8;
 constexpr int kWarpDeg = 2048;
 
+template <int kBlock>
 struct Shared {
+  static constexpr int kWarps = kBlock / 32;
   int tail;          // next free slot of the visit order S
   int nwq, ncq;      // warp-tier / CTA-tier queue lengths
   int flag;
   int imax;
   int item;
   int base_a, base_b;  // epochs of rows A and B
-  double red[kWarps];
+  double red[kBlock / 32];
   int wq[kBlock];
   int cq[kBlock];
 };
@@ -70,7 +71,8 @@ __device__ __forceinline__ Rows rows_of(const PlainArgs &a, int64_t slot) {
 }
 
 // Appends x to S (warp-aggregated atomic on the shared tail).
-__device__ __forceinline__ void append(Shared &sh, int32_t *S, int32_t x) {
+template <class SH>
+__device__ __forceinline__ void append(SH &sh, int32_t *S, int32_t x) {
   cg::coalesced_group g = cg::coalesced_threads();
   int pos = 0;
   if (g.thread_rank() == 0) pos = atomicAdd(&sh.tail, (int)g.size());
@@ -80,7 +82,8 @@ __device__ __forceinline__ void append(Shared &sh, int32_t *S, int32_t x) {
 
 // Forward step for one arc (w -> x) at level lev: accumulate sigma from a
 // predecessor, or claim an unvisited vertex for level lev+1.
-__device__ __forceinline__ void fwd_arc(Shared &sh, int32_t *d, const double *sig, int32_t *S, int32_t x, int dprev,
+template <class SH>
+__device__ __forceinline__ void fwd_arc(SH &sh, int32_t *d, const double *sig, int32_t *S, int32_t x, int dprev,
                                         int dnext, int base, double &acc) {
   int dx = __ldcg(d + x);
   if (dx == dprev) {
@@ -91,7 +94,9 @@ __device__ __forceinline__ void fwd_arc(Shared &sh, int32_t *d, const double *si
   }
 }
 
-__device__ __forceinline__ double block_sum(Shared &sh, double v) {
+template <int kBlock>
+__device__ __forceinline__ double block_sum(Shared<kBlock> &sh, double v) {
+  constexpr int kWarps = kBlock / 32;
   v = warp_sum(v);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) sh.red[warp] = v;
@@ -109,8 +114,10 @@ __device__ __forceinline__ double block_sum(Shared &sh, double v) {
 
 // CTA-wide BFS from s over one BCC: fills d (epoch base), sigma, the level
 // order S and level offsets lv[0..nlev]. Returns nlev (number of levels).
-__device__ int cta_bfs(Shared &sh, const int64_t *R, const int32_t *C, int32_t nb, int32_t s, int32_t *d, double *sig,
+template <int kBlock>
+__device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, int32_t nb, int32_t s, int32_t *d, double *sig,
                        int32_t *S, int32_t *lv, int base) {
+  constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     d[s] = base;
@@ -219,9 +226,11 @@ __device__ __forceinline__ bool keep_vertex(int mode, int list, int32_t w, int l
   return !inA && !inB;
 }
 
-__device__ void cta_bwd_level(Shared &sh, const int64_t *R, const int32_t *C, const int32_t *d, const double *sig,
+template <int kBlock>
+__device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, const int32_t *d, const double *sig,
                               double *q, const int32_t *rch, double *bcb, double wsrc, int dsucc, int lev, int mode,
                               const LevelList &L, const MergeFilter &mf) {
+  constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int list = 0; list < 3; ++list) {
     const int32_t *S = list == 0 ? L.S0 : list == 1 ? L.S1 : nullptr;
@@ -276,7 +285,7 @@ __device__ void cta_bwd_level(Shared &sh, const int64_t *R, const int32_t *C, co
 // back to all-unvisited when the next BFS could overflow.
 __device__ void ensure_epoch(int32_t *d, int64_t cap, int &base, int span) {
   if (base + span + 2 < (1 << 30)) return;
-  for (int64_t k = threadIdx.x; k < cap; k += kBlock) d[k] = 0;
+  for (int64_t k = threadIdx.x; k < cap; k += blockDim.x) d[k] = 0;
   __syncthreads();
   base = 1;
 }
@@ -285,7 +294,8 @@ __device__ void ensure_epoch(int32_t *d, int64_t cap, int &base, int span) {
 // (right): d = min(dA+ld, dB+rd), sigma from the strictly shorter side or the
 // sum on ties (Codes/postprocesses.cu:334-350); then the chain's own vertices
 // are fixed along the chain (Codes/postprocesses.cu:205-274). Returns max level.
-__device__ int merge_rows(Shared &sh, const Rows &r, int baseA, int baseB, int32_t nb, int32_t start, int32_t len,
+template <int kBlock>
+__device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int baseB, int32_t nb, int32_t start, int32_t len,
                           int32_t pos, int *err) {
   const int ld = pos + 1, rd = len - pos;
   int mx = 0;
@@ -321,7 +331,8 @@ __device__ int merge_rows(Shared &sh, const Rows &r, int baseA, int baseB, int32
   return sh.imax;
 }
 
-__device__ void process_item(Shared &sh, const PlainArgs &a, const Rows &r, const PlainItem &it) {
+template <int kBlock>
+__device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows &r, const PlainItem &it) {
   const int32_t b = it.bcc;
   const int64_t vo = a.vtx_off[b];
   const int32_t nb = (int32_t)(a.vtx_off[b + 1] - vo);
@@ -336,7 +347,7 @@ __device__ void process_item(Shared &sh, const PlainArgs &a, const Rows &r, cons
   ensure_epoch(r.dA, a.ws_n, baseA, nb);
   const int nlevA = cta_bfs(sh, R, a.col, nb, it.src, r.dA, r.sA, r.SA, r.lvA, baseA);
   const double wsrc = (double)rch[it.src] + 1.0;
-  for (int lev = nlevA - 1; lev >= 1; --lev) {
+  for (int lev = it.own ? nlevA - 1 : 0; lev >= 1; --lev) {
     LevelList L{r.SA, r.lvA[lev], r.lvA[lev + 1], nullptr, 0, 0, -1, -1};
     cta_bwd_level(sh, R, a.col, r.dA, r.sA, r.q, rch, bcb, wsrc, baseA + lev + 1, lev, 0, L, none);
   }
@@ -376,8 +387,9 @@ __device__ void process_item(Shared &sh, const PlainArgs &a, const Rows &r, cons
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlock, 1) plain_kernel(PlainArgs a) {
-  __shared__ Shared sh;
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) plain_kernel(PlainArgs a) {
+  __shared__ Shared<kBlock> sh;
   const Rows r = rows_of(a, blockIdx.x);
   if (threadIdx.x == 0) {
     sh.base_a = a.epochs[2 * blockIdx.x];
@@ -402,9 +414,10 @@ __global__ void __launch_bounds__(kBlock, 1) plain_kernel(PlainArgs a) {
 }
 
 // Rows of one source for the parity tests (one CTA).
+template <int kBlock>
 __global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bcc, int32_t src, int32_t chain,
                                                          int32_t *d_out, double *s_out) {
-  __shared__ Shared sh;
+  __shared__ Shared<kBlock> sh;
   const Rows r = rows_of(a, a.rows_slot);  // a slot no plain_kernel CTA uses
   const int64_t vo = a.vtx_off[bcc];
   const int32_t nb = (int32_t)(a.vtx_off[bcc + 1] - vo);
@@ -426,16 +439,19 @@ __global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bc
 
 }  // namespace
 
-int plain_block() { return kBlock; }
-
-cudaError_t launch_plain(const PlainArgs &a, int grid, cudaStream_t stream) {
-  plain_kernel<<<grid, kBlock, 0, stream>>>(a);
+cudaError_t launch_plain(const PlainArgs &a, int block, int grid, cudaStream_t stream) {
+  switch (block) {
+    case 256: plain_kernel<256><<<grid, 256, 0, stream>>>(a); break;
+    case 512: plain_kernel<512><<<grid, 512, 0, stream>>>(a); break;
+    case 1024: plain_kernel<1024><<<grid, 1024, 0, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_rows(const PlainArgs &a, int32_t bcc, int32_t src, int32_t chain, int32_t *d_out, double *s_out,
                         cudaStream_t stream) {
-  rows_kernel<<<1, kBlock, 0, stream>>>(a, bcc, src, chain, d_out, s_out);
+  rows_kernel<1024><<<1, 1024, 0, stream>>>(a, bcc, src, chain, d_out, s_out);
   return cudaGetLastError();
 }
 

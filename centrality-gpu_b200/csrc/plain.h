@@ -5,10 +5,12 @@
 
 namespace bcg {
 
-// One free/endpoint source (BCC-local id) plus the chains [c0, c1) of the
-// global chain table whose left endpoint it is.
+// One free/endpoint source (BCC-local id) plus chains [c0, c1) of the global
+// chain table whose left endpoint it is. A source owning many chains is split
+// into several items; only the one with own != 0 accumulates the source's own
+// dependencies, the others run its BFS forward only.
 struct PlainItem {
-  int32_t bcc, src, c0, c1;
+  int32_t bcc, src, c0, c1, own;
 };
 
 struct PlainArgs {
@@ -29,8 +31,8 @@ struct PlainArgs {
   int *err;
 };
 
-int plain_block();
-cudaError_t launch_plain(const PlainArgs &a, int grid, cudaStream_t stream);
+// block: 256, 512 or 1024 threads (1024 / block CTAs fit an SM).
+cudaError_t launch_plain(const PlainArgs &a, int block, int grid, cudaStream_t stream);
 // Rows (levels, path counts) of one source of BCC `bcc`; chain >= 0 selects
 // the merged rows of chain vertex src on that chain.
 cudaError_t launch_rows(const PlainArgs &a, int32_t bcc, int32_t src, int32_t chain, int32_t *d_out, double *s_out,

@@ -105,6 +105,14 @@ typedef struct bc_stats {
  * BiCC::to_eargraph loop (Codes/to_eargraph_construct.cpp:54-200). */
 int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats);
 
+/* Same, for a subset of the work: units [unit_begin, unit_end) of the plan
+ * bc_plan_create would build with this context's options (see below), e.g. a
+ * sampled estimate or one shard of a multi-GPU run. bc_out gets the
+ * contributions of those units (plus the articulation terms when
+ * with_art != 0). Host buffers in and out, uploads included. */
+int bc_run_bccs_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t unit_begin, int64_t unit_end, int32_t with_art,
+                      double *bc_out, bc_stats *stats);
+
 /* ---------------------------------------------- mirrors of begin_gpu ---- */
 /* One BCC, free sources. Mirrors begin_gpu(R,C,F,n,m,ear_info,self_ear,
  * req_nodes,artnodes,bc,time) (reference Codes/ear_graph.h:45-46,
@@ -140,8 +148,11 @@ typedef struct bc_plan bc_plan;
 int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out);
 void bc_plan_destroy(bc_plan *plan);
 int64_t bc_plan_num_units(const bc_plan *plan);
-/* Sources and TEPS arcs covered by units [begin, end). */
-int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *sources, int64_t *teps_edges);
+/* Work covered by units [begin, end): sources, TEPS arcs (sum over sources of
+ * their BCC's arcs) and vertex visits (sum over sources of their BCC's
+ * vertices); any output may be NULL. */
+int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *sources, int64_t *teps_edges,
+                      int64_t *vertex_visits);
 /* Device buffers the plan consumes (for roofline accounting). */
 int64_t bc_plan_device_bytes(const bc_plan *plan);
 int bc_plan_reset(bc_plan *plan);
