@@ -219,7 +219,10 @@ def main():
     arrs = d.arrays()
     mode = P.MODE_BATCHED if args.mode == "batched" else P.MODE_PLAIN
     delta = P.DELTA_FP32C if args.delta == "fp32c" else P.DELTA_FP64
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: torch's legacy default stream has handle 0, which the
+    # library reads as "use your own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = P.Context(mode=mode, delta=delta, batch_width=args.batch, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30))
     plan = ctx.plan(d)

@@ -37,7 +37,8 @@ _f32p = C.POINTER(C.c_float)
 
 class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
-                ("stream", C.c_void_p), ("workspace_limit", C.c_int64)]
+                ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -83,6 +84,7 @@ _SIGS = {
     "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
     "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p, _i64p]),
     "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "bc_plan_unit_sources": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_int64]),
     "bc_plan_reset": (C.c_int, [C.c_void_p]),
     "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
     "bc_plan_read": (C.c_int, [C.c_void_p, _f64p]),
@@ -226,12 +228,13 @@ class Context:
     """One CUDA device and stream (bc_create)."""
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
-                 workspace_limit=0):
+                 workspace_limit=0, rescale_exp=0):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
         o.stream = stream
         o.workspace_limit = workspace_limit
+        o.rescale_exp = rescale_exp
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:
@@ -293,6 +296,16 @@ class Plan:
         w = C.c_int64()
         self.ctx._check(lib().bc_plan_unit_work(self._h, begin, end, C.byref(s), C.byref(t), C.byref(w)))
         return s.value, t.value, w.value
+
+    def unit_sources(self, begin=0, end=None):
+        """Packed ids of the sources units [begin, end) accumulate."""
+        end = self.n_units if end is None else end
+        cnt = lib().bc_plan_unit_sources(self._h, begin, end, None, 0)
+        if cnt < 0:
+            raise BcError(-cnt, "bc_plan_unit_sources")
+        out = np.zeros(max(cnt, 1), dtype=np.int64)
+        lib().bc_plan_unit_sources(self._h, begin, end, _ptr(out, _i64p), cnt)
+        return out[:cnt]
 
     def reset(self):
         self.ctx._check(lib().bc_plan_reset(self._h))

@@ -14,6 +14,7 @@ struct BatchedConfig {
   bool delta_fp32c = true;  // FP32 two-sum compensated dependencies (else FP64)
   int sms = 148;
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
+  int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
 };
 
 struct BatchedPlan;
@@ -27,10 +28,15 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
 void batched_destroy(BatchedPlan *p);
 int64_t batched_device_bytes(const BatchedPlan *p);
 int batched_width(const BatchedPlan *p);
+// Packed ids of the own sources (own BFS + chain slots) of batches [begin, end).
+void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std::vector<int64_t> &out);
 // Prefix sums over passes of sources, TEPS arcs, BFS sources, aux BFS runs
 // and vertex visits.
 void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std::vector<int64_t> &teps,
                        std::vector<int64_t> &bfs, std::vector<int64_t> &aux, std::vector<int64_t> &visits);
 int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream, int *launches, std::string *msg);
+// Batches whose FP32 dependency values left FP32's exponent range (their
+// contributions were withheld); synchronises the stream.
+int batched_failed_batches(BatchedPlan *p, cudaStream_t stream, int64_t *count);
 
 }  // namespace bcg

@@ -39,6 +39,7 @@ struct bc_plan {
   std::vector<double> art;
   std::vector<int64_t> h_vtx_off, h_chain_off;
   std::vector<int32_t> h_n_plain, h_chain_start, h_chain_len;
+  std::vector<bcg::PlainItem> h_items;
   // device graph
   int64_t *row = nullptr, *vtx_off = nullptr;
   int32_t *col = nullptr, *reach = nullptr, *chain_start = nullptr, *chain_len = nullptr, *chain_l = nullptr,
@@ -117,6 +118,15 @@ int check_dev_err(bc_plan *p) {
   CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
   if (h != bcg::kDevOk)
     return fail(p->ctx, h == bcg::kDevTimeout ? BCGPU_ETIMEOUT : BCGPU_EINVAL, dev_err_text(h));
+  if (p->bp) {
+    int64_t bad = 0;
+    if (bcg::batched_failed_batches(p->bp, p->ctx->stream, &bad) != BCGPU_OK)
+      return fail(p->ctx, BCGPU_ECUDA, "reading batch status");
+    if (bad)
+      return fail(p->ctx, BCGPU_EOVERFLOW,
+                  std::to_string(bad) + " batch(es) left FP32's exponent range in the compensated-FP32 mode; "
+                  "their contributions were withheld: run with BCGPU_DELTA_FP64");
+  }
   return BCGPU_OK;
 }
 
@@ -247,6 +257,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
       p->unit_visits[i + 1] = p->unit_visits[i] + src * (B->vtx_off[it.bcc + 1] - B->vtx_off[it.bcc]);
     }
     if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
+    p->h_items = items;
     p->ws_n = nb_max + 2;
     const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
     // Four 256-thread CTAs per SM (four sources in flight) when their rows
@@ -275,6 +286,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     cfg.delta_fp32c = ctx->opts.delta == BCGPU_DELTA_FP32C;
     cfg.sms = ctx->sms;
     cfg.limit_bytes = limit - p->device_bytes;
+    cfg.rescale_exp = ctx->opts.rescale_exp;
     std::string msg;
     rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
@@ -393,6 +405,26 @@ extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, i
 }
 
 extern "C" int64_t bc_plan_device_bytes(const bc_plan *p) { return p ? p->device_bytes : 0; }
+
+extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t end, int64_t *out, int64_t cap) {
+  if (!p) return -BCGPU_EINVAL;
+  const int64_t n = bc_plan_num_units(p);
+  if (begin < 0 || end < begin || end > n) return -BCGPU_EINVAL;
+  std::vector<int64_t> ids;
+  if (p->mode == BCGPU_MODE_PLAIN) {
+    for (int64_t i = begin; i < end; ++i) {
+      const auto &it = p->h_items[i];
+      const int64_t vo = p->h_vtx_off[it.bcc];
+      if (it.own) ids.push_back(vo + it.src);
+      for (int32_t c = it.c0; c < it.c1; ++c)
+        for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
+    }
+  } else {
+    bcg::batched_unit_sources(p->bp, begin, end, ids);
+  }
+  for (int64_t i = 0; i < (int64_t)ids.size() && i < cap; ++i) out[i] = ids[i];
+  return (int64_t)ids.size();
+}
 
 extern "C" int bc_plan_reset(bc_plan *p) {
   if (!p) return BCGPU_EINVAL;

@@ -49,6 +49,9 @@ typedef struct bc_opts {
   int32_t batch_width;   /* sources per batched pass: multiple of 32, <= 1024; 0 = autotune */
   void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context */
   int64_t workspace_limit; /* device bytes the context may hold; 0 = 80% of free memory */
+  int32_t rescale_exp;   /* BATCHED: rescale a level's path counts above 2^rescale_exp; 0 = 900.
+                            Lower values only exercise the scaling path (tests). */
+  int32_t pad_;
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;
@@ -153,6 +156,10 @@ int64_t bc_plan_num_units(const bc_plan *plan);
  * vertices); any output may be NULL. */
 int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *sources, int64_t *teps_edges,
                       int64_t *vertex_visits);
+/* Packed ids of the sources whose dependencies units [begin, end) accumulate
+ * (forward-only helper BFS runs excluded). Writes up to cap ids to out and
+ * returns the total count (negative error code on failure). */
+int64_t bc_plan_unit_sources(const bc_plan *plan, int64_t begin, int64_t end, int64_t *out, int64_t cap);
 /* Device buffers the plan consumes (for roofline accounting). */
 int64_t bc_plan_device_bytes(const bc_plan *plan);
 int bc_plan_reset(bc_plan *plan);
