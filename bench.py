@@ -182,7 +182,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["batched", "plain"], default="plain")
+    ap.add_argument("--mode", choices=["batched", "plain"], default="batched")
     ap.add_argument("--delta", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat20")
@@ -226,7 +226,7 @@ def main():
     ctx = P.Context(mode=mode, delta=delta, batch_width=args.batch, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30))
     plan = ctx.plan(d)
-    target = args.step_sources or (16384 if mode == P.MODE_BATCHED else 2048)
+    target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
     ranges = step_ranges(plan, target)
     mine = ranges[rank::world]
     need = args.warmup + args.steps

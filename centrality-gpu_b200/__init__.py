@@ -14,8 +14,10 @@ Mirrors the reference's interfaces (Goutam363/centrality-GPU):
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -227,6 +229,8 @@ class Decomposition:
 class Context:
     """One CUDA device and stream (bc_create)."""
 
+    _live = weakref.WeakSet()
+
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
                  workspace_limit=0, rescale_exp=0):
         o = BcOpts()
@@ -240,6 +244,8 @@ class Context:
         if rc:
             raise BcError(rc, lib().bc_last_error(None).decode())
         self._h = h
+        self._plans = weakref.WeakSet()
+        Context._live.add(self)
 
     def _check(self, rc):
         if rc:
@@ -265,13 +271,26 @@ class Context:
         return Plan(self, decomp)
 
     def close(self):
+        """Releases the context; its plans are released with it."""
         if self._h:
+            for p in list(self._plans):
+                p._h = C.c_void_p()  # freed by bc_destroy
             lib().bc_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+@atexit.register
+def _close_all():
+    # before the CUDA runtime unloads: contexts (and with them their plans)
+    for c in list(Context._live):
+        try:
+            c.close()
         except Exception:
             pass
 
@@ -285,6 +304,7 @@ class Plan:
         h = C.c_void_p()
         ctx._check(lib().bc_plan_create(ctx._h, decomp.view, C.byref(h)))
         self._h = h
+        ctx._plans.add(self)
         self.n_units = lib().bc_plan_num_units(h)
         self.device_bytes = lib().bc_plan_device_bytes(h)
 
@@ -328,9 +348,9 @@ class Plan:
         return d, s
 
     def close(self):
-        if self._h:
+        if self._h and self.ctx._h:
             lib().bc_plan_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:

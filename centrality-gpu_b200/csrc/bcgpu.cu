@@ -16,8 +16,11 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <set>
 #include <string>
 #include <vector>
+
+struct bc_plan;
 
 struct bc_ctx {
   bc_opts opts{};
@@ -27,6 +30,7 @@ struct bc_ctx {
   bool own_stream = false;
   std::string err;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::set<bc_plan *> plans;  // live plans: bc_destroy releases them first
 };
 
 struct bc_plan {
@@ -295,6 +299,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux, p->unit_visits);
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->plans.insert(p);
   *out = p;
   return BCGPU_OK;
 }
@@ -366,6 +371,7 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
 
 extern "C" void bc_destroy(bc_ctx *ctx) {
   if (!ctx) return;
+  while (!ctx->plans.empty()) bc_plan_destroy(*ctx->plans.begin());
   cudaSetDevice(ctx->device);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -382,6 +388,7 @@ extern "C" int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out) {
 
 extern "C" void bc_plan_destroy(bc_plan *p) {
   if (!p) return;
+  p->ctx->plans.erase(p);
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
   if (p->bp) bcg::batched_destroy(p->bp);

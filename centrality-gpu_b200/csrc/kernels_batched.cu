@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 namespace bcg {
@@ -43,8 +44,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarpsPerCta = kThreads / 32;
-constexpr int kHeavyDeg = 512;     // vertices above this degree are scanned in chunks by whole CTAs
-constexpr int kChunkArcs = 4096;   // arcs per heavy chunk
+constexpr int kHeavyDeg = 256;     // vertices above this degree are scanned in chunks by whole CTAs
+constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr long long kSpinLimit = 1ll << 28;  // ~1 min of polling before giving up
 
 enum SlotKind : int32_t { kOwn = 0, kAux = 1, kChain = 2, kUnused = 3 };
@@ -59,7 +60,7 @@ struct Slot {
 struct Batch {
   int32_t bcc, nslots, words, max_off;  // max_off: largest chain distance ld/rd in the batch
   int64_t slot_off;   // into the slot table
-  int64_t mask_off;   // 3*words masks: bfs, own, chain
+  int64_t mask_off;   // 3 mask rows (bfs, own, chain), each padded to whole 4-word groups
 };
 
 // Control block in global memory (one per plan).
@@ -99,6 +100,8 @@ struct Args {
   uint32_t *lm;     // [tcap+2][n][W]
   uint32_t *seen;   // [n][W]
   int32_t *lmin, *lmax;
+  int32_t *gdone;   // [n] groups of the vertex already seen by all their BFS slots
+  int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
   double *bcpart;   // [n][W]
   int32_t *X;       // [B][tcap+2]
   int32_t *rexp;    // [B] per-level max exponent (rescale)
@@ -150,11 +153,34 @@ __device__ void grid_sync(const Args &a) {
   __syncthreads();
 }
 
+// Phase timers for profiling builds only (-DBCGPU_PHASE_TIMERS): CTA 0's
+// thread 0 accumulates %globaltimer deltas between grid barriers.
+#ifdef BCGPU_PHASE_TIMERS
+__device__ unsigned long long g_phase_ns[32];
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+#define PHASE_INIT() unsigned long long ph_t = (blockIdx.x == 0 && threadIdx.x == 0) ? gtimer() : 0ull
+#define PHASE_MARK(id)                                             \
+  do {                                                             \
+    if (blockIdx.x == 0 && threadIdx.x == 0) {                     \
+      const unsigned long long ph_n = gtimer();                    \
+      g_phase_ns[id] += ph_n - ph_t;                               \
+      ph_t = ph_n;                                                 \
+    }                                                              \
+  } while (0)
+#define PHASE_COUNT(id) do { if (blockIdx.x == 0 && threadIdx.x == 0) g_phase_ns[id] += 1; } while (0)
+#else
+#define PHASE_INIT() do {} while (0)
+#define PHASE_MARK(id) do {} while (0)
+#define PHASE_COUNT(id) do {} while (0)
+#endif
+
 __device__ __forceinline__ int64_t gwarp() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int64_t nwarps() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
 
-template <typename QT>
-__device__ __forceinline__ QT *qptr(const Args &a) { return reinterpret_cast<QT *>(a.q); }
 
 // ---- compensated FP32 accumulation (Neumaier's two-sum variant)
 struct Comp32 {
@@ -168,34 +194,118 @@ struct Comp32 {
 };
 
 // ============================================================== forward ====
+// A task is one vertex's whole row: lane j loads neighbour j's mask words for
+// up to kHalf words at once (aligned 16-byte loads, all in flight), the
+// (word, neighbour) pairs that hit are listed in shared memory, and the
+// neighbours' path-count rows are gathered eight at a time (lane = slot,
+// coalesced) into per-(word, slot) accumulators in shared memory. Adds to an
+// accumulator follow neighbour order, so sums are deterministic.
 
-// Pull step for one (vertex, word): neighbours' level-t masks against the
-// slots that have not seen v. Returns the new mask (uniform across the warp)
-// and leaves this lane's path-count sum in acc.
-__device__ __forceinline__ uint32_t pull_word(const Args &a, const int64_t *R, const int32_t *C, int64_t vrow_base,
-                                              int64_t e0, int64_t e1, int w, int t, uint32_t unseen, int lane,
-                                              double &acc) {
-  const int W = a.W;
-  const uint32_t *lmt = a.lm + (int64_t)t * a.n_cap * W;
-  uint32_t newm = 0;
-  (void)R;
-  for (int64_t e = e0; e < e1; e += 32) {
-    const int64_t ee = e + lane;
-    const int32_t mine = ee < e1 ? ldg(C + ee) : 0;
-    const int cnt = (int)(e1 - e < 32 ? e1 - e : 32);
-    for (int j = 0; j < cnt; ++j) {
-      const int32_t u = __shfl_sync(0xffffffffu, mine, j);
-      const uint32_t f = __ldcg(lmt + (int64_t)u * W + w) & unseen;
-      if (f) {
-        newm |= f;
-        if ((f >> lane) & 1u) acc += __ldcg(a.sig + ((int64_t)u * W + w) * 32 + lane);
-      }
-    }
+constexpr int kHalf = 8;  // words per pass over a vertex row
+
+struct WarpScratch {
+  uint32_t f[32][kHalf + 1];  // neighbour masks of the current 32-arc chunk (padded against bank conflicts)
+  uint16_t pairs[32 * kHalf]; // (word << 5 | neighbour lane) of the hits
+  double acc[kHalf][32];      // per (word, slot) sums (FP64, or two FP32 halves in the compensated mode)
+};
+
+__device__ __forceinline__ uint4 and4(uint4 a, uint4 b) { return make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w); }
+__device__ __forceinline__ uint4 ld4(const uint32_t *p) { return __ldcg(reinterpret_cast<const uint4 *>(p)); }
+
+// Loads the kHalf-word mask row at p (first nw words, nw a multiple of 4).
+__device__ __forceinline__ void load_row(const uint32_t *p, int nw, uint32_t (&m)[kHalf]) {
+#pragma unroll
+  for (int g = 0; g < kHalf / 4; ++g) {
+    const uint4 x = 4 * g < nw ? ld4(p + 4 * g) : make_uint4(0, 0, 0, 0);
+    m[4 * g] = x.x; m[4 * g + 1] = x.y; m[4 * g + 2] = x.z; m[4 * g + 3] = x.w;
   }
-  (void)vrow_base;
-  return newm;
 }
 
+template <typename T>
+__device__ __forceinline__ T warp_or(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One pull / successor pass over arcs [e0, e1) for words [w0, w0+nw):
+//   filt[k]  the slots of word w0+k that are looked for (uniform)
+//   masks    level masks of the neighbours (level t for the forward, t+1 for the backward)
+//   vals     per-slot values gathered on a hit (sigma, or q)
+// Accumulates into S.acc (ACC::add) and ORs the hits into any[k] (per lane).
+template <typename T, bool kComp>
+__device__ __forceinline__ void row_pass(const Args &a, WarpScratch &S, const uint32_t *masks, const T *vals,
+                                         int64_t e0, int64_t e1, int w0, int nw, const uint32_t (&filt)[kHalf],
+                                         uint32_t (&any)[kHalf], int lane) {
+  const int W = a.W;
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    const bool valid = e < e1;
+    const int32_t u = valid ? ldg(a.col + e) : 0;
+    uint32_t f[kHalf];
+    load_row(masks + (int64_t)u * W + w0, valid ? nw : 0, f);
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kHalf; ++k) {
+      f[k] &= filt[k];
+      S.f[lane][k] = f[k];
+      any[k] |= f[k];
+      cnt += f[k] != 0u;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int pos = incl - cnt;
+#pragma unroll
+    for (int k = 0; k < kHalf; ++k)
+      if (f[k]) S.pairs[pos++] = (uint16_t)((k << 5) | lane);
+    __syncwarp();
+    for (int i = 0; i < total; i += 8) {
+      T x[8];
+      int kk[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        x[r] = (T)0;
+        kk[r] = -1;
+        if (i + r < total) {  // uniform
+          const int p = S.pairs[i + r];
+          const int k = p >> 5, j = p & 31;
+          const uint32_t fj = S.f[j][k];
+          const int32_t uj = __shfl_sync(0xffffffffu, u, j);
+          if ((fj >> lane) & 1u) x[r] = __ldcg(vals + ((int64_t)uj * W + w0 + k) * 32 + lane);
+          kk[r] = ((fj >> lane) & 1u) ? k : -1;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        if (kk[r] < 0) continue;
+        if (kComp) {
+          float2 *c = reinterpret_cast<float2 *>(&S.acc[kk[r]][lane]);
+          Comp32 cc;
+          cc.s = c->x;
+          cc.c = c->y;
+          cc.add((float)x[r]);
+          *c = make_float2(cc.s, cc.c);
+        } else {
+          S.acc[kk[r]][lane] += (double)x[r];
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ double acc_value(const WarpScratch &S, int k, int lane, bool comp) {
+  if (!comp) return S.acc[k][lane];
+  const float2 c = *reinterpret_cast<const float2 *>(&S.acc[k][lane]);
+  return (double)c.x + (double)c.y;
+}
+
+// Stores the result of one (vertex, word) of the forward step.
 __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, uint32_t own,
                                             int lane, double acc) {
   if (!newm) return;
@@ -211,6 +321,7 @@ __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int
   if (lane == 0) {
     a.lm[((int64_t)(t + 1) * a.n_cap + v) * a.W + w] = newm;
     a.seen[(int64_t)v * a.W + w] |= newm;
+    a.ctrl->more = 1;
     if (newm & own) {
       atomicMin(a.lmin + v, t + 1);
       atomicMax(a.lmax + v, t + 1);
@@ -220,48 +331,12 @@ __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int
 
 // ============================================================== backward ===
 
-template <typename QT>
-__device__ __forceinline__ void push_q(const Args &a, int64_t idx, double val) {
-  qptr<QT>(a)[idx] = (QT)val;
-}
-
-template <typename QT>
-__device__ __forceinline__ double load_q(const Args &a, int64_t idx) {
-  return (double)__ldcg(qptr<QT>(a) + idx);
-}
-
-// Successor sum over arcs [e0, e1) of one (vertex, word): q of the slots in
-// `act` that sit one level deeper at the neighbour. FP32 mode accumulates the
-// q values with compensated (two-sum) FP32 arithmetic.
-template <typename QT>
-__device__ __forceinline__ double succ_sum(const Args &a, const uint32_t *lm_next, int64_t e0, int64_t e1, int w,
-                                           uint32_t act, int lane) {
-  constexpr bool kF32 = sizeof(QT) == 4;
-  const int W = a.W;
-  double acc = 0.0;
-  Comp32 acc32;
-  for (int64_t e = e0; e < e1; e += 32) {
-    const int64_t ee = e + lane;
-    const int32_t mine = ee < e1 ? ldg(a.col + ee) : 0;
-    const int cnt = (int)(e1 - e < 32 ? e1 - e : 32);
-    for (int j = 0; j < cnt; ++j) {
-      const int32_t u = __shfl_sync(0xffffffffu, mine, j);
-      const uint32_t sm = __ldcg(lm_next + (int64_t)u * W + w) & act;
-      if ((sm >> lane) & 1u) {
-        const double qv = load_q<QT>(a, ((int64_t)u * W + w) * 32 + lane);
-        if (kF32) acc32.add((float)qv);
-        else acc += qv;
-      }
-    }
-  }
-  return kF32 ? acc32.value() : acc;
-}
-
 // delta, q and the BC partial of one (vertex, word) at level lev.
 template <typename QT>
 __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, const int32_t *rch, int32_t v, int w,
                                            int lev, uint32_t act, int lane, double sum) {
   constexpr bool kF32 = sizeof(QT) == 4;
+  if (!act) return;
   const int W = a.W;
   double contrib = 0.0;
   if ((act >> lane) & 1u) {
@@ -275,11 +350,18 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
       const double aq = fabs(qv);
       if (!(aq >= (double)FLT_MIN * 0x1p24 && aq <= (double)FLT_MAX * 0x1p-24)) atomicExch(&a.ctrl->range_err, 1);
     }
-    push_q<QT>(a, idx, qv);
+    reinterpret_cast<QT *>(a.q)[idx] = (QT)qv;
     contrib = delta * ((double)rch[slots[b].src] + 1.0);
   }
   contrib = warp_sum(contrib);  // fixed-order reduction of this word's slots
   if (lane == 0) a.bcpart[(int64_t)v * W + w] += contrib;
+}
+
+// Next block of 32 vertices for this warp from the phase's work counter.
+__device__ __forceinline__ int64_t next_block(int *counter, int lane) {
+  int b = 0;
+  if (lane == 0) b = atomicAdd(counter, 1);
+  return __shfl_sync(0xffffffffu, b, 0);
 }
 
 }  // namespace
@@ -287,19 +369,25 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
 // --------------------------------------------------------------- kernel ----
 
 template <typename QT>
-__global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
-  __shared__ double s_red[kWarpsPerCta][32];
-  __shared__ uint32_t s_mask[kWarpsPerCta];
+__global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  WarpScratch *scratch = reinterpret_cast<WarpScratch *>(s_raw);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  WarpScratch &S = scratch[wib];
   const int W = a.W;
+  constexpr bool kComp = sizeof(QT) == 4;
+  PHASE_INIT();
 
   for (int64_t bi = a.b0; bi < a.b1; ++bi) {
     if (cta_failed(a)) return;
     const Batch bt = a.batches[bi];
     const Slot *slots = a.slots + bt.slot_off;
     const uint32_t *bfs_mask = a.masks + bt.mask_off;
-    const uint32_t *own_mask = bfs_mask + bt.words;
-    const uint32_t *chain_mask = own_mask + bt.words;
+    const int words = bt.words;
+    const int groups = (words + 3) / 4;
+    const int wpad = groups * 4;                 // masks are padded to whole groups
+    const uint32_t *own_mask = bfs_mask + wpad;
+    const uint32_t *chain_mask = own_mask + wpad;
     const int64_t vo = a.vtx_off[bt.bcc];
     const int32_t n = (int32_t)(a.vtx_off[bt.bcc + 1] - vo);
     const int64_t *R = a.row + vo;
@@ -311,31 +399,33 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
     const int32_t *hcv = a.hchunk_v + hc0;
     const int64_t *hce0 = a.hchunk_e0 + hc0, *hce1 = a.hchunk_e1 + hc0;
     const int32_t *hfst = a.hfirst + a.heavy_off[bt.bcc] + bt.bcc;  // nheavy+1 entries per BCC
-    const int words = bt.words;
+    const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nblk = ((int64_t)n + 31) / 32;  // vertex blocks of 32 (lane l takes vertex blk + l*nblk)
+    const int halves = (wpad + kHalf - 1) / kHalf;
 
-    // ---- init: seen = non-BFS slots, spans, partials, level-0 masks, X, rexp
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)n * W;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    // ---- init: seen = non-BFS slots, spans, partials, level-0/1 masks, X, rexp, work counters
+    for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) {
       const int w = (int)(i % W);
-      a.seen[i] = w < words ? ~bfs_mask[w] : 0xffffffffu;
+      a.seen[i] = w < wpad ? ~bfs_mask[w] : 0xffffffffu;
       a.bcpart[i] = 0.0;
-      a.lm[i] = 0;                                        // level 0
-      a.lm[(int64_t)a.n_cap * W + i] = 0;                 // level 1
-      if (w == 0) { a.lmin[i / W] = INT_MAX; a.lmax[i / W] = -1; }
+      a.lm[i] = 0;                         // level 0
+      a.lm[(int64_t)a.n_cap * W + i] = 0;  // level 1
+      if (w == 0) { a.lmin[i / W] = INT_MAX; a.lmax[i / W] = -1; a.gdone[i / W] = 0; }
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W * 32; i += gridDim.x * blockDim.x) {
+    for (int64_t i = gtid; i < (int64_t)W * 32; i += gthreads) {
       a.rexp[i] = INT_MIN;
-      a.X[(int64_t)i * (a.tcap + 2)] = 0;
+      a.X[i * (a.tcap + 2)] = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int64_t i = gtid; i < 2 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
+    if (gtid == 0) {
       a.ctrl->more = 0;
       a.ctrl->rescale = 0;
       a.ctrl->tmax = 0;
       a.ctrl->range_err = 0;
     }
     grid_sync(a);
-    // sources at level 0
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bt.nslots; b += gridDim.x * blockDim.x) {
+    for (int64_t b = gtid; b < bt.nslots; b += gthreads) {  // sources at level 0
       const Slot s = slots[b];
       if (s.kind != kOwn && s.kind != kAux) continue;
       const int64_t idx = ((int64_t)s.src * W + (b >> 5)) * 32 + (b & 31);
@@ -346,56 +436,103 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
       if (s.kind == kOwn) { atomicMin(a.lmin + s.src, 0); atomicMax(a.lmax + s.src, 0); }
     }
     grid_sync(a);
+    PHASE_MARK(0);
 
     // ---- forward: levels t -> t+1
     int t = 0;
     while (true) {
       if (t + 1 > a.tcap) { set_err(a.err, kDevWorkspace); break; }
-      // heavy vertices: chunks of their arc lists, one CTA per (chunk, word);
-      // partials are combined in chunk order after the barrier
-      for (int64_t task = blockIdx.x; task < nchunks * words; task += gridDim.x) {
-        const int64_t c = task / words;
-        const int w = (int)(task % words);
+      const uint32_t *lmt = a.lm + (int64_t)t * a.n_cap * W;
+      // heavy vertices: chunks of their arcs, one CTA per (chunk, half); partials
+      // are combined across the CTA's warps, then across chunks after the barrier
+      for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
+        const int64_t c = task / halves;
+        const int w0 = (int)(task % halves) * kHalf;
+        const int nw = min(kHalf, wpad - w0);
         const int32_t v = hv[hcv[c]];
-        const uint32_t unseen = ~__ldcg(a.seen + (int64_t)v * W + w);
-        double acc = 0.0;
-        uint32_t m = 0;
-        if (unseen) {  // uniform over the CTA
+        uint32_t unseen[kHalf], any[kHalf];
+        load_row(a.seen + (int64_t)v * W + w0, nw, unseen);
+        uint32_t u_any = 0;
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) { unseen[k] = k < nw ? ~unseen[k] : 0u; any[k] = 0; u_any |= unseen[k]; }
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+        if (u_any) {  // uniform over the CTA
           const int64_t e0 = hce0[c], e1 = hce1[c];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < s1) m = pull_word(a, R, a.col, 0, s0, s1, w, t, unseen, lane, acc);
+          if (s0 < s1) row_pass<double, false>(a, S, lmt, a.sig, s0, s1, w0, nw, unseen, any, lane);
         }
-        s_red[wib][lane] = acc;
-        if (lane == 0) s_mask[wib] = m;
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) {
+          any[k] = warp_or(any[k]);
+          if (lane == 0) S.f[0][k] = any[k];  // this warp's hit masks, for the combine
+        }
         __syncthreads();
-        if (wib == 0) {
+        for (int k = wib; k < nw; k += kWarpsPerCta) {  // fixed warp order
           double tot = 0.0;
           uint32_t mm = 0;
-          for (int k = 0; k < kWarpsPerCta; ++k) { tot += s_red[k][lane]; mm |= s_mask[k]; }  // fixed order
-          a.hacc[((hc0 + c) * W + w) * 32 + lane] = tot;
-          if (lane == 0) a.hmask[(hc0 + c) * W + w] = mm;
+          for (int x = 0; x < kWarpsPerCta; ++x) { tot += scratch[x].acc[k][lane]; mm |= scratch[x].f[0][k]; }
+          a.hacc[((hc0 + c) * W + w0 + k) * 32 + lane] = tot;
+          if (lane == 0) a.hmask[(hc0 + c) * W + w0 + k] = mm;
         }
         __syncthreads();
       }
-      // light vertices: one warp per (vertex, word)
-      for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
-        const int32_t v = (int32_t)(task / words);
-        const int w = (int)(task % words);
-        const int64_t e0 = R[v], e1 = R[v + 1];
-        if (e1 - e0 > kHeavyDeg) continue;
-        const uint32_t unseen = ~__ldcg(a.seen + (int64_t)v * W + w);
-        if (!unseen) continue;
-        double acc = 0.0;
-        const uint32_t m = pull_word(a, R, a.col, 0, e0, e1, w, t, unseen, lane, acc);
-        finish_pull(a, v, w, t, m, own_mask[w], lane, acc);
-        if (m && lane == 0) a.ctrl->more = 1;
+      // light vertices: dynamic blocks of 32, lane-parallel activity check
+      for (int64_t vb = next_block(a.wq + t, lane); vb < nblk; vb = next_block(a.wq + t, lane)) {
+        const int64_t vl = vb + (int64_t)lane * nblk;
+        int64_t e0l = 0, e1l = 0;
+        bool on = false;
+        if (vl < n) {
+          e0l = R[vl];
+          e1l = R[vl + 1];
+          on = e1l - e0l <= kHeavyDeg && __ldcg(a.gdone + vl) < groups;
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, on);
+        while (todo) {
+          const int j = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
+          const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
+          for (int w0 = 0; w0 < wpad; w0 += kHalf) {
+            const int nw = min(kHalf, wpad - w0);
+            uint32_t seen[kHalf], unseen[kHalf], any[kHalf];
+            load_row(a.seen + (int64_t)v * W + w0, nw, seen);
+            uint32_t u_any = 0;
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k) { unseen[k] = k < nw ? ~seen[k] : 0u; any[k] = 0; u_any |= unseen[k]; }
+            if (!u_any) continue;
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+            row_pass<double, false>(a, S, lmt, a.sig, e0, e1, w0, nw, unseen, any, lane);
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k) {
+              if (k >= nw) continue;
+              const uint32_t m = warp_or(any[k]);
+              finish_pull(a, v, w0 + k, t, m, own_mask[w0 + k], lane, S.acc[k][lane]);
+              any[k] = m;
+            }
+#pragma unroll
+            for (int g = 0; g < kHalf / 4; ++g) {  // groups now seen by all their BFS slots
+              if (4 * g >= nw || lane != 0) continue;
+              bool was = true, now = true;
+#pragma unroll
+              for (int k = 4 * g; k < 4 * g + 4; ++k) {
+                was = was && unseen[k] == 0u;
+                now = now && (unseen[k] & ~any[k]) == 0u;
+              }
+              if (now && !was) atomicAdd(a.gdone + v, 1);
+            }
+          }
+        }
       }
       grid_sync(a);
+      PHASE_MARK(1);
+      PHASE_COUNT(16);
       if (nheavy) {
-        for (int64_t task = gwarp(); task < (int64_t)nheavy * words; task += nwarps()) {
-          const int32_t h = (int32_t)(task / words);
-          const int w = (int)(task % words);
+        for (int64_t task = gwarp(); task < (int64_t)nheavy * wpad; task += nwarps()) {
+          const int32_t h = (int32_t)(task / wpad);
+          const int w = (int)(task % wpad);
           const int32_t v = hv[h];
           if (!~__ldcg(a.seen + (int64_t)v * W + w)) continue;
           double acc = 0.0;
@@ -405,17 +542,16 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
             m |= __ldcg(a.hmask + (hc0 + c) * W + w);
           }
           finish_pull(a, v, w, t, m, own_mask[w], lane, acc);
-          if (m && lane == 0) a.ctrl->more = 1;
         }
         grid_sync(a);
+        PHASE_MARK(2);
       }
       const int more = *(volatile int *)&a.ctrl->more;
       const int resc = *(volatile int *)&a.ctrl->rescale;
-      // base exponent of level t+1; rescale it when some slot's counts passed 2^kRescaleExp
-      for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < W * 32; b += gridDim.x * blockDim.x) {
+      // base exponent of level t+1; rescale it when some slot's counts passed 2^rescale_exp
+      for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) {
         const int re = __ldcg(a.rexp + b);
-        a.X[(int64_t)b * (a.tcap + 2) + t + 1] =
-            a.X[(int64_t)b * (a.tcap + 2) + t] + (re > a.rescale_exp ? re : 0);
+        a.X[b * (a.tcap + 2) + t + 1] = a.X[b * (a.tcap + 2) + t] + (re > a.rescale_exp ? re : 0);
       }
       if (resc) {
         for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
@@ -431,19 +567,18 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
       }
       grid_sync(a);  // everyone has read more/rescale/rexp
       if (resc)
-        for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < W * 32; b += gridDim.x * blockDim.x) a.rexp[b] = INT_MIN;
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) a.rexp[b] = INT_MIN;
+      if (gtid == 0) {
         a.ctrl->more = 0;
         a.ctrl->rescale = 0;
       }
       if (!more || cta_failed(a)) break;
       ++t;
-      // clear the next level's masks
-      for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)n * W;
-           i += (int64_t)gridDim.x * blockDim.x)
-        a.lm[((int64_t)(t + 1) * a.n_cap) * W + i] = 0;
+      for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 1) * a.n_cap * W + i] = 0;
       grid_sync(a);
+      PHASE_MARK(3);
     }
+    PHASE_MARK(3);
     if (cta_failed(a)) return;
     const int tbfs = t;  // deepest level with BFS vertices
 
@@ -451,11 +586,8 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
     // per-level base exponents, then the merge
     const int top = min(a.tcap + 1, tbfs + bt.max_off + 1);
     for (int lv = tbfs + 2; lv <= top; ++lv)
-      for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)n * W;
-           i += (int64_t)gridDim.x * blockDim.x)
-        a.lm[(int64_t)lv * a.n_cap * W + i] = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)bt.nslots * (a.tcap + 1);
-         i += (int64_t)gridDim.x * blockDim.x) {
+      for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)lv * a.n_cap * W + i] = 0;
+    for (int64_t i = gtid; i < (int64_t)bt.nslots * (a.tcap + 1); i += gthreads) {
       const int b = (int)(i / (a.tcap + 1));
       const int lv = (int)(i % (a.tcap + 1));
       const Slot s = slots[b];
@@ -518,7 +650,7 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
     if (lane == 0) atomicMax(&a.ctrl->tmax, tmax_local);
     grid_sync(a);
     // same-chain vertices: the direct distance along the chain wins or ties
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bt.nslots; b += gridDim.x * blockDim.x) {
+    for (int64_t b = gtid; b < bt.nslots; b += gthreads) {
       const Slot s = slots[b];
       if (s.kind != kChain) continue;
       for (int j = 0; j < s.clen; ++j) {
@@ -526,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
         const int dist = j > s.cpos ? j - s.cpos : s.cpos - j;
         const int64_t iz = ((int64_t)k * W + (b >> 5)) * 32 + (b & 31);
         const int cur = a.d[iz];
-        const double one = ldexp(1.0, -a.X[(int64_t)b * (a.tcap + 2) + dist]);
+        const double one = ldexp(1.0, -a.X[b * (a.tcap + 2) + dist]);
         if (cur > dist) {
           atomicAnd(a.lm + ((int64_t)cur * a.n_cap + k) * W + (b >> 5), ~(1u << (b & 31)));
           atomicOr(a.lm + ((int64_t)dist * a.n_cap + k) * W + (b >> 5), 1u << (b & 31));
@@ -542,50 +674,88 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
     const int tmax = *(volatile int *)&a.ctrl->tmax;
     if (tmax + 1 > a.tcap) set_err(a.err, kDevWorkspace);
     if (cta_failed(a)) return;
+    PHASE_MARK(4);
 
     // ---- backward: t = tmax .. 1
     for (int lev = tmax; lev >= 1; --lev) {
       const uint32_t *lm_here = a.lm + (int64_t)lev * a.n_cap * W;
       const uint32_t *lm_next = a.lm + (int64_t)(lev + 1) * a.n_cap * W;
+      const QT *q = reinterpret_cast<const QT *>(a.q);
       // heavy vertices: chunked successor sums, combined below
-      for (int64_t task = blockIdx.x; task < nchunks * words; task += gridDim.x) {
-        const int64_t c = task / words;
-        const int w = (int)(task % words);
+      for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
+        const int64_t c = task / halves;
+        const int w0 = (int)(task % halves) * kHalf;
+        const int nw = min(kHalf, wpad - w0);
         const int32_t v = hv[hcv[c]];
-        const uint32_t act = (lev < __ldcg(a.lmin + v) || lev > __ldcg(a.lmax + v))
-                                 ? 0u : (__ldcg(lm_here + (int64_t)v * W + w) & own_mask[w]);
-        double acc = 0.0;
-        if (act) {  // uniform over the CTA
+        uint32_t act[kHalf], any[kHalf];
+        load_row(lm_here + (int64_t)v * W + w0, nw, act);
+        const bool in_span = lev >= __ldcg(a.lmin + v) && lev <= __ldcg(a.lmax + v);
+        uint32_t a_any = 0;
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) {
+          act[k] = (in_span && k < nw) ? act[k] & own_mask[w0 + k] : 0u;
+          any[k] = 0;
+          a_any |= act[k];
+        }
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+        if (a_any) {  // uniform over the CTA
           const int64_t e0 = hce0[c], e1 = hce1[c];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < s1) acc = succ_sum<QT>(a, lm_next, s0, s1, w, act, lane);
+          if (s0 < s1) row_pass<QT, kComp>(a, S, lm_next, q, s0, s1, w0, nw, act, any, lane);
         }
-        s_red[wib][lane] = acc;
         __syncthreads();
-        if (wib == 0) {
+        for (int k = wib; k < nw; k += kWarpsPerCta) {  // fixed warp order
           double tot = 0.0;
-          for (int k = 0; k < kWarpsPerCta; ++k) tot += s_red[k][lane];  // fixed order
-          a.hacc[((hc0 + c) * W + w) * 32 + lane] = tot;
+          for (int x = 0; x < kWarpsPerCta; ++x) tot += acc_value(scratch[x], k, lane, kComp);
+          a.hacc[((hc0 + c) * W + w0 + k) * 32 + lane] = tot;
         }
         __syncthreads();
       }
-      for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
-        const int32_t v = (int32_t)(task / words);
-        const int w = (int)(task % words);
-        if (lev < __ldcg(a.lmin + v) || lev > __ldcg(a.lmax + v)) continue;
-        const int64_t e0 = R[v], e1 = R[v + 1];
-        if (e1 - e0 > kHeavyDeg) continue;
-        const uint32_t act = __ldcg(lm_here + (int64_t)v * W + w) & own_mask[w];
-        if (!act) continue;
-        const double sum = succ_sum<QT>(a, lm_next, e0, e1, w, act, lane);
-        finish_dep<QT>(a, slots, rch, v, w, lev, act, lane, sum);
+      const int wqi = a.tcap + 3 + lev;
+      for (int64_t vb = next_block(a.wq + wqi, lane); vb < nblk; vb = next_block(a.wq + wqi, lane)) {
+        const int64_t vl = vb + (int64_t)lane * nblk;
+        int64_t e0l = 0, e1l = 0;
+        bool on = false;
+        if (vl < n && lev >= __ldcg(a.lmin + vl) && lev <= __ldcg(a.lmax + vl)) {
+          e0l = R[vl];
+          e1l = R[vl + 1];
+          on = e1l - e0l <= kHeavyDeg;
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, on);
+        while (todo) {
+          const int j = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
+          const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
+          for (int w0 = 0; w0 < wpad; w0 += kHalf) {
+            const int nw = min(kHalf, wpad - w0);
+            uint32_t act[kHalf], any[kHalf];
+            load_row(lm_here + (int64_t)v * W + w0, nw, act);
+            uint32_t a_any = 0;
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k) {
+              act[k] = k < nw ? act[k] & own_mask[w0 + k] : 0u;
+              any[k] = 0;
+              a_any |= act[k];
+            }
+            if (!a_any) continue;
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+            row_pass<QT, kComp>(a, S, lm_next, q, e0, e1, w0, nw, act, any, lane);
+#pragma unroll
+            for (int k = 0; k < kHalf; ++k)
+              if (k < nw) finish_dep<QT>(a, slots, rch, v, w0 + k, lev, act[k], lane, acc_value(S, k, lane, kComp));
+          }
+        }
       }
       if (nheavy) {
         grid_sync(a);
-        for (int64_t task = gwarp(); task < (int64_t)nheavy * words; task += nwarps()) {
-          const int32_t h = (int32_t)(task / words);
-          const int w = (int)(task % words);
+        PHASE_MARK(5);
+        for (int64_t task = gwarp(); task < (int64_t)nheavy * wpad; task += nwarps()) {
+          const int32_t h = (int32_t)(task / wpad);
+          const int w = (int)(task % wpad);
           const int32_t v = hv[h];
           if (lev < __ldcg(a.lmin + v) || lev > __ldcg(a.lmax + v)) continue;
           const uint32_t act = __ldcg(lm_here + (int64_t)v * W + w) & own_mask[w];
@@ -596,19 +766,22 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(Args a) {
         }
       }
       grid_sync(a);
+      PHASE_MARK(6);
+      PHASE_COUNT(17);
     }
     // ---- fold the batch into BC (fixed word order), unless FP32 range failed
     const int bad = *(volatile int *)&a.ctrl->range_err;
     if (bad) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) a.redo[bi] = 1;
+      if (gtid == 0) a.redo[bi] = 1;
     } else {
-      for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+      for (int64_t v = gtid; v < n; v += gthreads) {
         double s = 0.0;
         for (int w = 0; w < words; ++w) s += a.bcpart[v * W + w];
         a.bc[vo + v] += s;
       }
     }
     grid_sync(a);
+    PHASE_MARK(7);
   }
 }
 
@@ -621,6 +794,7 @@ struct BatchedPlan {
   int64_t n_cap = 0;
   bool f32 = true;
   int grid = 0;
+  size_t smem = 0;
   int64_t bytes = 0;
   std::vector<void *> allocs;
   Args args{};
@@ -671,7 +845,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   int width = cfg.width > 0 ? cfg.width : 512;
   width = std::max(32, std::min(1024, (width + 31) / 32 * 32));
   P->width = width;
-  P->W = width / 32;
+  P->W = (width / 32 + 3) / 4 * 4;  // row stride: whole 4-word groups (16-byte mask loads)
   const int W = P->W;
 
   // ---- host scheduling: batches of slots per BCC
@@ -726,7 +900,8 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
       bt.words = (bt.nslots + 31) / 32;
       bt.slot_off = (int64_t)slots.size();
       bt.mask_off = (int64_t)masks.size();
-      std::vector<uint32_t> mb((size_t)bt.words, 0), mo((size_t)bt.words, 0), mc((size_t)bt.words, 0);
+      const int wpad = (bt.words + 3) / 4 * 4;  // masks padded to whole groups, 16-byte aligned
+      std::vector<uint32_t> mb((size_t)wpad, 0), mo((size_t)wpad, 0), mc((size_t)wpad, 0);
       for (int32_t i = 0; i < bt.nslots; ++i) {
         const uint32_t bit = 1u << (i & 31);
         if (cur[i].kind == kOwn || cur[i].kind == kAux) mb[i >> 5] |= bit;
@@ -768,22 +943,81 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
       else ++aux_cnt;
       return slot_of[x];
     };
-    for (int32_t s = 0; s < npl; ++s) {
+    // Source order: bounded BFS balls of nearby plain vertices, so a pass's
+    // sources see every vertex within a narrow band of levels (few active
+    // levels per vertex, dense 32-slot hits) and the right endpoints of the
+    // chains they own are mostly own slots of the same pass.
+    // Each chain is owned (scheduled with) its lower-degree endpoint: a pass
+    // then holds many small owners whose chains lead to the same few hubs,
+    // which appear once each as helper BFS slots.
+    auto degb = [&](int32_t x) { return B->row[vo + x + 1] - B->row[vo + x]; };
+    std::vector<int64_t> own_off((size_t)npl + 1, 0);
+    std::vector<int64_t> owned((size_t)(ce - B->chain_off[b]));
+    auto owner = [&](int64_t cc) {
+      const int32_t l = B->chain_l[cc], r = B->chain_r[cc];
+      return degb(l) <= degb(r) ? l : r;
+    };
+    for (int64_t cc = B->chain_off[b]; cc < ce; ++cc) own_off[owner(cc) + 1]++;
+    for (int32_t x = 0; x < npl; ++x) own_off[x + 1] += own_off[x];
+    {
+      std::vector<int64_t> fill(own_off.begin(), own_off.end() - 1);
+      for (int64_t cc = B->chain_off[b]; cc < ce; ++cc) owned[fill[owner(cc)]++] = cc;
+    }
+    auto slots_of = [&](int32_t s) {
+      int64_t k = 1;
+      for (int64_t i = own_off[s]; i < own_off[s + 1]; ++i) k += B->chain_len[owned[i]];
+      return k;
+    };
+    std::vector<int32_t> order;
+    order.reserve((size_t)npl);
+    {
+      std::vector<char> done((size_t)npl, 0);
+      std::vector<int32_t> stamp((size_t)nb, -1), q;
+      int32_t ball = 0;
+      const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
+      for (int32_t seed = 0; seed < npl; ++seed) {
+        if (done[seed]) continue;
+        q.clear();
+        q.push_back(seed);
+        stamp[seed] = ball;
+        int64_t got = 0, scanned = 0;
+        for (size_t h = 0; h < q.size() && got < width; ++h) {
+          const int32_t x = q[h];
+          if (x < npl && !done[x]) {
+            done[x] = 1;
+            order.push_back(x);
+            got += slots_of(x);
+          }
+          if (scanned >= arc_budget) continue;  // keep draining the queue, stop growing it
+          const int64_t e0 = B->row[vo + x], e1 = std::min(B->row[vo + x + 1], e0 + arc_budget - scanned);
+          scanned += e1 - e0;
+          for (int64_t e = e0; e < e1; ++e) {
+            const int32_t y = B->col[e];
+            if (stamp[y] != ball) { stamp[y] = ball; q.push_back(y); }
+          }
+        }
+        ++ball;
+      }
+    }
+    for (int32_t s : order) {
       if ((int)cur.size() + 1 > width) flush();
       bfs_slot(s, kOwn);
-      while (c < ce && B->chain_l[c] == s) {
-        const int32_t len = B->chain_len[c], r = B->chain_r[c];
-        const int need = len + (slot_of[r] >= 0 ? 0 : 1);
+      for (int64_t oi = own_off[s]; oi < own_off[s + 1]; ++oi) {
+        c = owned[oi];
+        const int32_t len = B->chain_len[c];
+        const int32_t other = B->chain_l[c] == s ? B->chain_r[c] : B->chain_l[c];
+        const int need = len + (slot_of[other] >= 0 ? 0 : 1);
         if ((int)cur.size() + need > width) {
           flush();
           bfs_slot(s, kAux);  // the owner returns as a forward-only slot
         }
-        if ((int)cur.size() + len + (slot_of[r] >= 0 ? 0 : 1) > width) {
+        if ((int)cur.size() + len + (slot_of[other] >= 0 ? 0 : 1) > width) {
           if (msg) *msg = "chain longer than the batch width";
           delete P;
           return BCGPU_EINVAL;
         }
-        const int32_t sl = slot_of[s], sr = bfs_slot(r, kAux);
+        bfs_slot(other, kAux);
+        const int32_t sl = slot_of[B->chain_l[c]], sr = slot_of[B->chain_r[c]];
         for (int32_t pos = 0; pos < len; ++pos) {
           Slot z{};
           z.kind = kChain;
@@ -794,7 +1028,6 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
           cur.push_back(z);
           ++src_cnt;
         }
-        ++c;
       }
     }
     flush();
@@ -813,7 +1046,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   // ---- device workspace
   const int64_t n = P->n_cap;
   const int64_t qb = P->f32 ? 4 : 8;
-  const int64_t need = n * W * 32 * (4 + 8 + qb) + (int64_t)(tcap + 2) * n * W * 4 + n * W * (4 + 8) + n * 8 +
+  const int64_t need = n * W * 32 * (4 + 8 + qb) + (int64_t)(tcap + 2) * n * W * 4 + n * W * (4 + 8) + n * 12 +
                        (int64_t)W * 32 * (tcap + 2) * 4;
   if (need > cfg.limit_bytes)
     return bail(BCGPU_ENOMEM, "batched workspace " + std::to_string(need >> 20) + " MiB exceeds the limit " +
@@ -834,6 +1067,8 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok &= ok && alloc(&p, n * W * 4); a.seen = (uint32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.lmin = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
+  ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
+  ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * (tcap + 2) * 4); a.X = (int32_t *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 4); a.rexp = (int32_t *)p;
@@ -883,8 +1118,13 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (!coop) return bail(BCGPU_ECUDA, "device lacks cooperative launch");
-  if (P->f32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_kernel<float>, kThreads, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_kernel<double>, kThreads, 0);
+  const size_t smem = sizeof(WarpScratch) * kWarpsPerCta;
+  if (cudaFuncSetAttribute(batched_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(batched_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return bail(BCGPU_ECUDA, "cannot reserve shared memory for the batched kernel");
+  if (P->f32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_kernel<float>, kThreads, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_kernel<double>, kThreads, smem);
+  P->smem = smem;
   if (per_sm < 1) return bail(BCGPU_ECUDA, "batched kernel does not fit an SM");
   P->grid = sms * per_sm;
   *out = P;
@@ -916,6 +1156,19 @@ void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std:
   sources = p->u_src; teps = p->u_teps; bfs = p->u_bfs; aux = p->u_aux; visits = p->u_visits;
 }
 
+#ifdef BCGPU_PHASE_TIMERS
+}  // namespace bcg
+extern "C" int bc_debug_phase_times(unsigned long long *out, int reset) {
+  if (cudaMemcpyFromSymbol(out, bcg::g_phase_ns, sizeof(unsigned long long) * 32) != cudaSuccess) return 2;
+  if (reset) {
+    unsigned long long z[32] = {0};
+    cudaMemcpyToSymbol(bcg::g_phase_ns, z, sizeof(z));
+  }
+  return 0;
+}
+namespace bcg {
+#endif
+
 int batched_failed_batches(BatchedPlan *p, cudaStream_t stream, int64_t *count) {
   std::vector<int> h((size_t)std::max<int64_t>(p->n_batches, 1), 0);
   cudaError_t e = cudaMemcpyAsync(h.data(), p->args.redo, h.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -935,8 +1188,8 @@ int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream,
   void *params[] = {&a};
   cudaError_t e = cudaMemsetAsync(&p->args.ctrl->bar_count, 0, 2 * sizeof(unsigned int), stream);
   if (e == cudaSuccess) {
-    if (p->f32) e = cudaLaunchCooperativeKernel((void *)batched_kernel<float>, p->grid, kThreads, params, 0, stream);
-    else e = cudaLaunchCooperativeKernel((void *)batched_kernel<double>, p->grid, kThreads, params, 0, stream);
+    if (p->f32) e = cudaLaunchCooperativeKernel((void *)batched_kernel<float>, p->grid, kThreads, params, p->smem, stream);
+    else e = cudaLaunchCooperativeKernel((void *)batched_kernel<double>, p->grid, kThreads, params, p->smem, stream);
   }
   if (e != cudaSuccess) {
     if (msg) *msg = std::string("cooperative launch: ") + cudaGetErrorString(e);

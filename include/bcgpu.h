@@ -59,6 +59,7 @@ typedef struct bc_ctx bc_ctx;
 /* Fills opts with defaults (device -1, BATCHED, FP32C, autotuned width). */
 void bc_default_opts(bc_opts *opts);
 int bc_create(const bc_opts *opts, bc_ctx **out);
+/* Releases the context and every plan still alive on it. */
 void bc_destroy(bc_ctx *ctx);
 /* Message of the last failing call on ctx (or of bc_create when ctx is NULL). */
 const char *bc_last_error(const bc_ctx *ctx);
@@ -149,6 +150,8 @@ int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, 
  * accumulates their contributions. */
 typedef struct bc_plan bc_plan;
 int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out);
+/* Must not be called after bc_destroy of the plan's context (which already
+ * released it). */
 void bc_plan_destroy(bc_plan *plan);
 int64_t bc_plan_num_units(const bc_plan *plan);
 /* Work covered by units [begin, end): sources, TEPS arcs (sum over sources of
