@@ -79,6 +79,8 @@ _SIGS = {
                                     C.POINTER(BcStats)]),
     "bc_begin_free": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, _i32p, _f32p,
                                 _f64p]),
+    "bc_begin_free_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                        C.c_int32, C.c_void_p, C.c_void_p, _f64p]),
     "bc_begin_active": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, C.c_int32,
                                   _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f64p]),
     "bc_plan_create": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), C.POINTER(C.c_void_p)]),
@@ -377,6 +379,17 @@ def begin_gpu_free(ctx: Context, R, Cc, n, m, req_nodes, artnodes, bc, time_s=0.
     t = C.c_double(time_s)
     ctx._check(lib().bc_begin_free(ctx._h, _ptr(R, _i32p), _ptr(Cc, _i32p), int(n), int(m), _ptr(req, _i32p), len(req),
                                    _ptr(reach, _i32p), _ptr(bc, _f32p), C.byref(t)))
+    return t.value
+
+
+def begin_gpu_free_noalloc(ctx: Context, R_dev, C_dev, n, m, req_dev, n_req, reach_dev, bc_dev, time_s=0.0):
+    """bc_begin_free_noalloc: device pointers (ints) in and out, no allocation
+    inside the call; bc_dev (FP64, n entries) is overwritten. Returns the
+    accumulated device seconds."""
+    t = C.c_double(time_s)
+    ctx._check(lib().bc_begin_free_noalloc(ctx._h, C.c_void_p(R_dev), C.c_void_p(C_dev), int(n), int(m),
+                                           C.c_void_p(req_dev), int(n_req), C.c_void_p(reach_dev),
+                                           C.c_void_p(bc_dev), C.byref(t)))
     return t.value
 
 

@@ -9,6 +9,7 @@
 #include "bcgpu.h"
 #include "batched.h"
 #include "common.cuh"
+#include "internal.h"
 #include "plain.h"
 
 #include <algorithm>
@@ -305,6 +306,16 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
 }
 
 }  // namespace
+
+namespace bcg {
+void ctx_device_stream(const bc_ctx *ctx, int *device, cudaStream_t *stream, cudaEvent_t *ev0, cudaEvent_t *ev1) {
+  *device = ctx->device;
+  *stream = ctx->stream;
+  *ev0 = ctx->ev0;
+  *ev1 = ctx->ev1;
+}
+void ctx_set_error(bc_ctx *ctx, const char *msg) { ctx->err = msg; }
+}  // namespace bcg
 
 extern "C" void bc_default_opts(bc_opts *o) {
   if (!o) return;

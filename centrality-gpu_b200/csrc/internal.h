@@ -1,0 +1,14 @@
+// Library-internal helpers shared between translation units (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "bcgpu.h"
+
+namespace bcg {
+
+// Device, stream and the two timing events a context owns.
+void ctx_device_stream(const bc_ctx *ctx, int *device, cudaStream_t *stream, cudaEvent_t *ev0, cudaEvent_t *ev1);
+// Records msg as the context's last error (read back by bc_last_error).
+void ctx_set_error(bc_ctx *ctx, const char *msg);
+
+}  // namespace bcg

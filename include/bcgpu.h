@@ -128,6 +128,25 @@ int bc_run_bccs_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t unit_begin, int6
 int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m, const int32_t *req_nodes,
                   int32_t n_req, const int32_t *reach, float *bc, double *time_s);
 
+/* Variant of bc_begin_free that allocates nothing (no reference counterpart).
+ * For callers that cannot create device allocations of their own -- their
+ * device memory belongs to another allocator (a framework's caching pool, an
+ * arena budgeted up front), so a cudaMalloc/cudaFree here would break that
+ * accounting or stall the device. Inputs and the output are the CALLER's
+ * DEVICE buffers: R[n+1], C[m] (m = arcs), req_nodes[n_req], reach[n], and
+ * bc[n] (FP64, overwritten). All other working memory is one file-scope
+ * __device__ array of about 16 MiB that every GPU loading this library holds
+ * until the process exits. Limits: n <= 16384 and n_req <= 16384
+ * (BCGPU_EOVERFLOW beyond, with the reason in bc_last_error).
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call reuses the same array and clears what it needs at start; calls
+ * that overlap on the GPU (several threads or streams at once) race on it,
+ * so serialise them. Runs on the context's stream and returns when done;
+ * *time_s (may be NULL) is increased by the device seconds spent. */
+int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m,
+                          const int32_t *req_nodes, int32_t n_req, const int32_t *reach, double *bc, double *time_s);
+
 /* One BCC, chain endpoints ("active" vertices) and their chains ("ears").
  * Mirrors the second begin_gpu overload (reference Codes/ear_graph.h:48-49,
  * Codes/begin_gpupgm.cu:73-89, Codes/kernels_active.cu:18-223 with
