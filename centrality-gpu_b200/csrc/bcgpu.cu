@@ -321,7 +321,7 @@ extern "C" void bc_default_opts(bc_opts *o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
   o->device = -1;
-  o->mode = BCGPU_MODE_PLAIN;
+  o->mode = BCGPU_MODE_BATCHED;
   o->delta = BCGPU_DELTA_FP32C;
   o->batch_width = 0;
 }
