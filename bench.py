@@ -145,6 +145,48 @@ def cpu_sample(P, arrs, budget_s, threads):
     return {"sources": count, "arcs": arcs, "vertices": nb, "seconds": dt, "gteps": count * arcs / dt / 1e9}
 
 
+def cpu_unit_check(P, plan, arrs, threads):
+    """CPU-baseline leg: times the oracle's per-BCC kernel (the method's CPU
+    restatement) on exactly the sources of one GPU work unit of the largest
+    BCC, on all host threads, and reports the max relative BC error of that
+    unit's GPU result against it."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O  # the checker: CPU-baseline leg only
+    v0, v1 = int(arrs["vtx_off"][0]), int(arrs["vtx_off"][1])
+    k0 = plan.n_units // 2
+    while k0 > 0:
+        ids = plan.unit_sources(k0, k0 + 1)
+        if len(ids) and ids.min() >= v0 and ids.max() < v1:
+            break
+        k0 -= 1
+    ids = plan.unit_sources(k0, k0 + 1)
+    plan.reset()
+    plan.run(k0, k0 + 1, stats=False)
+    got = plan.read()
+    local = (ids - v0).astype(np.int32)
+    t = time.perf_counter()
+    contrib = O.bcc_sources(arrs, 0, local, threads)
+    dt = time.perf_counter() - t
+    want = np.array(arrs["art"], dtype=np.float64)
+    np.add.at(want, arrs["orig"][v0:v1], contrib)
+    err = float(np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))))
+    arcs = int(arrs["row"][v1] - arrs["row"][v0])
+    return {"unit": k0, "sources": len(ids), "arcs": arcs, "vertices": v1 - v0, "seconds": dt,
+            "gteps": len(ids) * arcs / dt / 1e9, "max_rel_err": err}
+
+
+def traffic_per_source(mode, workload):
+    """DRAM bytes per source of the dominant kernel from the committed ncu
+    summary (profiles/<kernel>_<workload>.md, line 'traffic_bytes_per_source: X')."""
+    import re
+    name = ("batched_kernel" if mode == "batched" else "plain_kernel") + f"_{workload}.md"
+    f = ROOT / "profiles" / name
+    if not f.exists():
+        return None, None
+    m = re.search(r"traffic_bytes_per_source:\s*([0-9.eE+]+)", f.read_text())
+    return (float(m.group(1)), f"profiles/{name}") if m else (None, None)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -228,7 +270,8 @@ def main():
     plan = ctx.plan(d)
     target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
     ranges = step_ranges(plan, target)
-    mine = ranges[rank::world]
+    from centrality_gpu_b200 import multigpu
+    mine = multigpu.shard(ranges, rank, world)
     need = args.warmup + args.steps
     sel = [mine[i % len(mine)] for i in range(need)]
 
@@ -272,8 +315,12 @@ def main():
     alg_bytes = 16.0 * teps + 48.0 * visits
     avg_launch_ms = float(np.mean(per_step))
     achieved = alg_bytes / args.steps / (avg_launch_ms * 1e-3) / 1e9
+    tps, tsrc = traffic_per_source(args.mode, args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": None,
+                "peak_source": peak_kind,
+                "traffic": tps * sources / args.steps if tps else None,
+                "traffic_source": f"ncu dram__bytes_read.sum+dram__bytes_write.sum per source ({tsrc}) x sources "
+                                  f"per launch" if tps else None,
                 "alg_bytes_per_launch": alg_bytes / args.steps, "avg_launch_ms": avg_launch_ms}
 
     # end to end through the public API with host buffers (uploads + download inside)
@@ -292,12 +339,26 @@ def main():
         e2e = {"value": e_teps / te / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": int(arrs["n_packed"]) * 8, "steps": len(e_sel)}
 
+    # combine the ranks' BC (one FP64 all-reduce, outside the timed region)
+    if world > 1:
+        from centrality_gpu_b200 import multigpu
+        plan.reset()
+        for r0, r1 in sel[args.warmup:]:
+            plan.run(r0, r1, stats=False)
+        total = multigpu.combine_bc(plan.read() - arrs["art"], arrs["art"], dist, device="cuda")
+        if rank == 0:
+            print(f"combined BC over {world} ranks: sum {float(total.sum()):.6e}", file=sys.stderr)
+
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        s = cpu_sample(P, arrs, args.cpu_budget_s, len(os.sched_getaffinity(0)))
-        cpu = {"value": s["gteps"], "unit": "GTEPS", "cores": len(os.sched_getaffinity(0)), "kind": "port",
-               "sample": f"{s['sources']} evenly spaced sources of the largest BCC ({s['vertices']} vertices, "
+        threads = len(os.sched_getaffinity(0))
+        s = cpu_unit_check(P, plan, arrs, threads)
+        cpu = {"value": s["gteps"], "unit": "GTEPS", "cores": threads, "kind": "port",
+               "sample": f"the {s['sources']} sources of GPU unit {s['unit']} (largest BCC: {s['vertices']} vertices, "
                          f"{s['arcs']} arcs), oracle per-BCC kernel, {s['seconds']:.1f} s"}
+        accuracy = {"max_rel_err": s["max_rel_err"], "vs": "FP64 CPU oracle on the same sources",
+                    "sources": s["sources"], "bar": 1e-6}
 
     if rank == 0:
         info = d.info
@@ -314,7 +375,7 @@ def main():
                        "units_per_step": float(np.mean([r1 - r0 for r0, r1 in sel])),
                        "host_decomposition_s": round(host_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
                        "parallelism": f"sources sharded over {world} GPU(s)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "gpu_launches": int(launches_per_unit * args.steps),
         }
         print(json.dumps(line), flush=True)

@@ -167,3 +167,23 @@ def test_bad_input_is_rejected(ctx):
         P.begin_gpu_free(ctx, [0, 1, 2], [1, 0], 2, 2, [0], [0, 0], np.zeros(2, np.float32))  # BCC < 3 vertices
     with pytest.raises(P.BcError):
         P.begin_gpu_free(ctx, [0, 2, 4, 6], [1, 2, 0, 2, 0, 9], 3, 6, [0], [0, 0, 0], np.zeros(3, np.float32))
+
+
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+def test_betc_cli_matches_golden(tmp_path, mode):
+    """The drop-in command: same edge-list input, `v bc` per vertex out."""
+    import json
+    import subprocess
+
+    from helpers import GOLDEN
+    P = pkg()
+    for name in ("sample4", "rand4", "small2000"):
+        out = tmp_path / f"{name}.{mode}.out"
+        r = subprocess.run([str(P.BETC_PATH), str(GOLDEN / f"{name}.txt"), "--out", str(out), "--mode", mode],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        assert "GPU total time is" in r.stderr
+        vals = np.loadtxt(out, ndmin=2)
+        bc = np.array(json.loads((GOLDEN / f"{name}.bc.json").read_text())["bc"])
+        assert np.array_equal(vals[:, 0], np.arange(len(bc)))
+        assert rel_err(vals[:, 1], bc) < (TOL_PLAIN if mode == "plain" else 1e-6)
