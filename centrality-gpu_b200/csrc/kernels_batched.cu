@@ -884,7 +884,9 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
 
     // greedy packing: each plain source with the chains it owns
     std::vector<Slot> cur;
-    std::vector<int32_t> slot_of((size_t)npl, -1);
+    std::vector<int32_t> slot_of((size_t)nb, -1);
+    const bool merge = cfg.chain_merge;
+    const int32_t nsrc_bfs = merge ? npl : nb;  // vertices that become BFS slots
     std::vector<int32_t> touched;
     int64_t c = B->chain_off[b];
     const int64_t ce = B->chain_off[b + 1];
@@ -965,17 +967,21 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     }
     auto slots_of = [&](int32_t s) {
       int64_t k = 1;
-      for (int64_t i = own_off[s]; i < own_off[s + 1]; ++i) k += B->chain_len[owned[i]];
+      if (merge && s < npl)
+        for (int64_t i = own_off[s]; i < own_off[s + 1]; ++i) k += B->chain_len[owned[i]];
       return k;
     };
     std::vector<int32_t> order;
-    order.reserve((size_t)npl);
+    order.reserve((size_t)nsrc_bfs);
     {
-      std::vector<char> done((size_t)npl, 0);
+      std::vector<char> done((size_t)nsrc_bfs, 0);
       std::vector<int32_t> stamp((size_t)nb, -1), q;
       int32_t ball = 0;
       const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
-      for (int32_t seed = 0; seed < npl; ++seed) {
+      // A ball grows only through vertices it can still take (and, in the
+      // merge form, through chain vertices): each source's arcs are scanned
+      // once, so late balls cost no rescans of finished regions.
+      for (int32_t seed = 0; seed < nsrc_bfs; ++seed) {
         if (done[seed]) continue;
         q.clear();
         q.push_back(seed);
@@ -983,7 +989,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         int64_t got = 0, scanned = 0;
         for (size_t h = 0; h < q.size() && got < width; ++h) {
           const int32_t x = q[h];
-          if (x < npl && !done[x]) {
+          if (x < nsrc_bfs) {
             done[x] = 1;
             order.push_back(x);
             got += slots_of(x);
@@ -993,7 +999,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
           scanned += e1 - e0;
           for (int64_t e = e0; e < e1; ++e) {
             const int32_t y = B->col[e];
-            if (stamp[y] != ball) { stamp[y] = ball; q.push_back(y); }
+            if (stamp[y] != ball && (y >= nsrc_bfs || !done[y])) { stamp[y] = ball; q.push_back(y); }
           }
         }
         ++ball;
@@ -1002,6 +1008,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     for (int32_t s : order) {
       if ((int)cur.size() + 1 > width) flush();
       bfs_slot(s, kOwn);
+      if (!merge) continue;
       for (int64_t oi = own_off[s]; oi < own_off[s + 1]; ++oi) {
         c = owned[oi];
         const int32_t len = B->chain_len[c];
