@@ -28,7 +28,6 @@ BETC_PATH = _PKG / "lib" / "betc"
 
 OK, EINVAL, ECUDA, ENOMEM, ETIMEOUT, EIO, EOVERFLOW = range(7)
 MODE_PLAIN, MODE_BATCHED = 0, 1
-CHAINS_AUTO, CHAINS_MERGE, CHAINS_BFS = 0, 1, 2
 DELTA_FP64, DELTA_FP32C = 0, 1
 _ERRNAMES = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ETIMEOUT", 5: "EIO", 6: "EOVERFLOW"}
 
@@ -41,7 +40,7 @@ _f32p = C.POINTER(C.c_float)
 class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
                 ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
-                ("chain_sources", C.c_int32)]
+                ("pad_", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -235,14 +234,13 @@ class Context:
     _live = weakref.WeakSet()
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
-                 workspace_limit=0, rescale_exp=0, chain_sources=CHAINS_AUTO):
+                 workspace_limit=0, rescale_exp=0):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
         o.stream = stream
         o.workspace_limit = workspace_limit
         o.rescale_exp = rescale_exp
-        o.chain_sources = chain_sources
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:

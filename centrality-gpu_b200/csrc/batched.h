@@ -15,7 +15,6 @@ struct BatchedConfig {
   int sms = 148;
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
-  bool chain_merge = false;  // chain-vertex sources merged from endpoint columns (else BFS slots)
 };
 
 struct BatchedPlan;

@@ -292,7 +292,6 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     cfg.sms = ctx->sms;
     cfg.limit_bytes = limit - p->device_bytes;
     cfg.rescale_exp = ctx->opts.rescale_exp;
-    cfg.chain_merge = ctx->opts.chain_sources == BCGPU_CHAINS_MERGE;
     std::string msg;
     rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
@@ -334,8 +333,6 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
   else bc_default_opts(&o);
   if (o.mode != BCGPU_MODE_PLAIN && o.mode != BCGPU_MODE_BATCHED) return fail(nullptr, BCGPU_EINVAL, "bad mode");
   if (o.delta != BCGPU_DELTA_FP64 && o.delta != BCGPU_DELTA_FP32C) return fail(nullptr, BCGPU_EINVAL, "bad delta");
-  if (o.chain_sources < BCGPU_CHAINS_AUTO || o.chain_sources > BCGPU_CHAINS_BFS)
-    return fail(nullptr, BCGPU_EINVAL, "bad chain_sources");
   if (o.batch_width < 0 || o.batch_width > 1024 || (o.batch_width % 32) != 0)
     return fail(nullptr, BCGPU_EINVAL, "batch_width must be a multiple of 32 in [0, 1024]");
   int count = 0;

@@ -1,30 +1,45 @@
-// BATCHED schedule: many sources per pass as a bitmask multi-source BFS.
+// BATCHED schedule: many sources per pass as a bitmask multi-source BFS over
+// each BCC with its degree-2 chains contracted.
 //
-// One pass ("batch") covers up to B = 32*W sources ("slots") of one BCC:
-//   own BFS slots   free vertices / chain endpoints whose dependencies count,
-//   aux BFS slots   chain endpoints BFS'd only so their chains can merge,
-//   chain slots     degree-2 chain vertices: rows merged from the two endpoint
-//                   columns, d = min(dL+ld, dR+rd) (reference
-//                   Codes/postprocesses.cu:329-351, chain walk :205-274).
-// State is vertex-major, slot-minor ([v][B]) so a warp reads the 32 slots of
-// a word as one coalesced row segment, and every neighbour's row serves all
-// slots at once:
+// Contracted graph. Within a BCC the core vertices (local ids < n_plain) keep
+// their arcs to each other ("unit arcs"); a chain c of k degree-2 vertices
+// between the core endpoints L and R becomes one arc L-R of length k+1 in
+// both endpoint rows ("chain arcs", listed after the unit arcs of a row).
+// Chain vertices never enter the level-synchronous phases: their levels, path
+// counts and dependencies follow in closed form from the two endpoint columns
+// (the reference's ear postprocessing, Codes/postprocesses.cu:205-351, done
+// here for every source of the pass at once).
+//
+// Slots. One pass ("batch") covers up to B = 32*W sources of one BCC:
+//   core source     level 0 at the vertex;
+//   chain source    the vertex at position p (0-based from L) of a chain of
+//                   k vertices: seeded at L on level p+1 and at R on level
+//                   k-p, one path each (its two directions along the chain).
+// State of the core vertices, vertex-major and slot-minor ([v][B]) so a warp
+// reads the 32 slots of a word as one coalesced row segment:
 //   d[v][b]     level (int32)            sigma[v][b] path count (FP64, scaled)
 //   q[v][b]     (reach(v)+1+delta)/sigma (FP64, or FP32 in the compensated mode)
 //   lm[t][v][w] bitmask of the slots that reach v at level t: the frontier of
 //               the forward phase and the successor test of the backward phase
-// Forward: level-synchronous pull. For every vertex still unseen by some BFS
-// slot, the warp scans its neighbours once per 32-slot word, ORs their level-t
-// masks and sums the path counts of the slots that hit (the reference's
-// per-source atomicCAS/atomicAdd BFS, Codes/kernels_free.cu:286-362).
-// Backward: successor form (Codes/kernels_free.cu:377-421) with the level
-// masks as successor test: delta(v) = sigma(v) * sum over successors of q.
+// Forward: level-synchronous pull. A core vertex still unseen by some slot
+// scans its row once per 32-slot word: a unit arc to u hits the slots in
+// lm[t][u], a chain arc of length k+1 hits those in lm[t-k][u]; the hits'
+// path counts are summed (the reference's per-source atomicCAS/atomicAdd BFS,
+// Codes/kernels_free.cu:286-362).
+// Backward: successor form (Codes/kernels_free.cu:377-421), delta(v) =
+// sigma(v) * sum of q over successors, where a chain arc of length k+1 is a
+// successor arc when the chain carries the far end's shortest paths (the far
+// end sits on level lev+k+1), plus what v receives from the chain vertices
+// themselves: a closed form in prefix sums of reach+1 along the chain and the
+// two ends' path counts, evaluated for every (vertex, slot) in one parallel
+// phase between the forward and the backward sweeps.
+// Chain vertices: one warp per (chain, 32-slot word) evaluates every chain
+// vertex's dependency for the 32 slots from the endpoint columns.
 // Path counts carry a per-(slot, level) power-of-two base X so deep graphs do
 // not overflow FP64: a level is rescaled when its largest count passes
 // 2^rescale_exp (900 by default).
-// BC: per (vertex, word) FP64 partials summed over levels in fixed order, then
-// over words in fixed order -> deterministic (the reference uses FP32
-// atomics, Codes/kernels_free.cu:423-426).
+// BC: per (vertex, word) FP64 partials, summed over words in fixed order ->
+// deterministic (the reference uses FP32 atomics, Codes/kernels_free.cu:423-426).
 // The whole GPU works on one batch at a time: a cooperative persistent kernel
 // with a grid barrier whose waits are bounded (error flag, no hang).
 #include "batched.h"
@@ -32,6 +47,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -44,71 +60,88 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarpsPerCta = kThreads / 32;
-constexpr int kHeavyDeg = 256;     // vertices above this degree are scanned in chunks by whole CTAs
+constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs
 constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr long long kSpinLimit = 1ll << 28;  // ~1 min of polling before giving up
+constexpr int kHalf = 8;           // words per pass over a vertex row
 
-enum SlotKind : int32_t { kOwn = 0, kAux = 1, kChain = 2, kUnused = 3 };
-
+// One source of a pass. chain < 0: the core vertex src (level 0). Otherwise
+// src is the chain vertex at position pos of chain `chain` (global index).
 struct Slot {
-  int32_t kind, src;        // src: BFS source (local id) or the chain vertex itself
-  int32_t sl, sr, ld, rd;   // chain slots: endpoint slots and distances
-  int32_t cstart, clen, cpos;
-  int32_t pad;
+  int32_t src, chain, pos, pad;
+};
+
+// Where a chain source enters the core: slot reaches core vertex v on `level`
+// with one path along its chain.
+struct Seed {
+  int32_t v, level, slot, pad;
 };
 
 struct Batch {
-  int32_t bcc, nslots, words, max_off;  // max_off: largest chain distance ld/rd in the batch
-  int64_t slot_off;   // into the slot table
-  int64_t mask_off;   // 3 mask rows (bfs, own, chain), each padded to whole 4-word groups
+  int32_t bcc, nslots, words, nseeds;
+  int32_t max_seed;  // deepest seed level (0: none)
+  int32_t kmax;      // longest chain of the BCC: the longest arc is kmax+1
+  int64_t slot_off, seed_off;
 };
 
 // Control block in global memory (one per plan).
 struct Ctrl {
   unsigned int bar_count;
   unsigned int bar_gen;
-  int more;          // forward: some slot found a new vertex this level
-  int rescale;       // forward: some slot needs a rescale at this level
-  int tmax;          // deepest level of the batch (all slots)
-  int tbfs;          // deepest BFS level
-  int range_err;     // FP32 q left FP32's exponent range in this batch
+  int more;       // forward: some slot found a new vertex this level
+  int rescale;    // forward: some slot needs a rescale at this level
+  int range_err;  // FP32 q left FP32's exponent range in this batch
   int pad;
 };
 
 struct Args {
-  const int64_t *row;
-  const int32_t *col;
+  // contracted rows of the core vertices; BCC b's rows start at hvo[b]
+  const int64_t *hvo;
+  const int64_t *hrow;    // [n_core_rows + n_bcc] global arc offsets
+  const int64_t *hsplit;  // first chain arc of each row
+  const int32_t *hcol;    // neighbour (local core id)
+  const int32_t *hk;      // chain arcs: vertices on the chain (the arc is one longer)
+  const int32_t *hcid;    // chain arcs: chain index * 2 + (the row's vertex is the chain's right end)
   const int32_t *reach;
   const int64_t *vtx_off;
-  const int64_t *heavy_off;  // per BCC range in heavy[] (heavy vertices: degree > kHeavyDeg)
+  const int32_t *n_plain;
+  // chains (global index)
+  const int64_t *chain_off;
+  const int32_t *chain_start, *chain_len, *chain_l, *chain_r;
+  const int64_t *cpre_off;  // chain -> its k+1 prefix sums of reach+1 (from the left end) in cpre
+  const double *cpre;
+  // heavy rows (contracted degree > kHeavyDeg), chunked
+  const int64_t *heavy_off;  // per BCC range in heavy[]
   const int32_t *heavy;      // local ids
   const int64_t *hchunk_off; // per BCC range in the chunk table
   const int32_t *hchunk_v;   // chunk -> heavy index (within its BCC's heavy list)
   const int64_t *hchunk_e0;  // chunk arc range [e0, e1) (global arc offsets)
   const int64_t *hchunk_e1;
   const int32_t *hfirst;     // heavy index -> first chunk (BCC-relative), hfirst[h+1] ends it
-  double *hacc;              // [chunks][W][32] partial sums
+  double *hacc;              // [chunks][W][32] partial successor / path-count sums
   uint32_t *hmask;           // [chunks][W] partial masks
   const Batch *batches;
   const Slot *slots;
-  const uint32_t *masks;
+  const Seed *seeds;
   int64_t b0, b1;
-  // workspace
+  // workspace (core rows)
   int32_t *d;
   double *sig;
   void *q;
-  uint32_t *lm;     // [tcap+2][n][W]
-  uint32_t *seen;   // [n][W]
+  uint32_t *lm;     // [tcap+2][n_cap][W]
+  uint32_t *seen;   // [n_cap][W]
   int32_t *lmin, *lmax;
-  int32_t *gdone;   // [n] groups of the vertex already seen by all their BFS slots
+  int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
   int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
-  double *bcpart;   // [n][W]
+  double *bcpart;   // [nb_cap][W] every vertex of the BCC (chain vertices included)
+  double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
   int32_t *X;       // [B][tcap+2]
   int32_t *rexp;    // [B] per-level max exponent (rescale)
-  int64_t n_cap;    // rows allocated (>= largest BCC)
+  int64_t n_cap;    // core rows allocated (>= largest core)
   int32_t W;        // words per row (row stride)
   int32_t tcap;     // levels allocated
-  int32_t rescale_exp;  // rescale a level's path counts above 2^rescale_exp
+  int32_t rescale_exp;
+  int32_t pad;
   double *bc;
   Ctrl *ctrl;
   int *err;
@@ -181,7 +214,6 @@ __device__ __forceinline__ unsigned long long gtimer() {
 __device__ __forceinline__ int64_t gwarp() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int64_t nwarps() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
 
-
 // ---- compensated FP32 accumulation (Neumaier's two-sum variant)
 struct Comp32 {
   float s = 0.f, c = 0.f;
@@ -193,15 +225,83 @@ struct Comp32 {
   __device__ __forceinline__ double value() const { return (double)s + (double)c; }
 };
 
+// ============================================================ chain math ===
+// A stretch of a chain between two ends A and B holding m chain vertices,
+// seen from A: its vertex i (0 <= i < m) lies i+1 arcs from A and m-i from B.
+// pre(x) is the sum of reach+1 over its first x vertices counted from A.
+struct Stretch {
+  const double *P;  // the chain's prefix sums from its left end (k+1 entries)
+  int lo, hi;       // chain positions [lo, hi) of the stretch
+  bool rev;         // A is the right-hand end (position hi)
+  __device__ __forceinline__ int m() const { return hi - lo; }
+  __device__ __forceinline__ double pre(int x) const { return rev ? P[hi] - P[hi - x] : P[lo + x] - P[lo]; }
+  __device__ __forceinline__ double wt(int i) const { return pre(i + 1) - pre(i); }
+  __device__ __forceinline__ Stretch flip() const { return Stretch{P, lo, hi, !rev}; }
+};
+
+// An end of a stretch for one slot: its level and where its path count and q
+// live; idx < 0 marks the slot's own source (level 0, one path).
+struct End {
+  int d;
+  int64_t idx;
+};
+
+__device__ __forceinline__ double sig_of(const Args &a, const End &e, int b) {
+  return e.idx < 0 ? 1.0 : ldexp(__ldcg(a.sig + e.idx), __ldcg(a.X + (int64_t)b * (a.tcap + 2) + e.d));
+}
+template <typename QT>
+__device__ __forceinline__ double q_of(const Args &a, const End &e, int b) {
+  return ldexp((double)__ldcg(reinterpret_cast<const QT *>(a.q) + e.idx), -__ldcg(a.X + (int64_t)b * (a.tcap + 2) + e.d));
+}
+
+// Dependency of stretch vertex i on the slot's source when i takes its
+// shortest paths from A (2i < D): the chain vertices beyond i on the A-fed
+// side each add reach+1; the last A-fed vertex either ties (shares its paths
+// with B: adds its reach+1 times sigma_A / (sigma_A + sigma_B)) or, when it is
+// the vertex next to B and B's shortest paths run through the stretch, passes
+// on sigma_A * q(B). i = -1 gives what A itself receives through the stretch.
+template <typename QT, bool kTail>
+__device__ __forceinline__ double fed_dep(const Args &a, const Stretch &s, int i, const End &A, const End &B, int b,
+                                          int D) {
+  const int m = s.m();
+  const int P = min(m - 1, D / 2);  // last vertex fed from A
+  if ((D & 1) == 0 && D / 2 <= m - 1) {
+    const double sa = sig_of(a, A, b), sb = sig_of(a, B, b);
+    return s.pre(P) - s.pre(i + 1) + sa / (sa + sb) * s.wt(P);
+  }
+  double v = s.pre(P + 1) - s.pre(i + 1);
+  if (kTail && P == m - 1 && B.d == A.d + m + 1) v += sig_of(a, A, b) * q_of<QT>(a, B, b);
+  return v;
+}
+
+// Dependency of stretch vertex i (0 <= i < m) on the slot's source.
+template <typename QT>
+__device__ __forceinline__ double stretch_dep(const Args &a, const Stretch &s, int i, const End &A, const End &B,
+                                              int b) {
+  const int m = s.m();
+  const int D = B.d + m - A.d - 1;  // vertex i is fed from A iff 2i <= D, from B iff 2i >= D
+  if (2 * i < D) return fed_dep<QT, true>(a, s, i, A, B, b, D);
+  if (2 * i > D) return fed_dep<QT, true>(a, s.flip(), m - 1 - i, B, A, b, A.d + m - B.d - 1);
+  return 0.0;  // fed from both ends: no successor on the chain
+}
+
+// What end A receives from the stretch's vertices (its neighbour on the
+// stretch is its successor iff that neighbour is fed from A: D >= 0), less
+// the term through B (sigma_A * q(B) when B's paths run through the
+// stretch), which the backward sweep adds as a successor arc.
+__device__ __forceinline__ double end_dep(const Args &a, const Stretch &s, const End &A, const End &B, int b) {
+  const int D = B.d + s.m() - A.d - 1;
+  if (s.m() == 0 || D < 0) return 0.0;
+  return fed_dep<double, false>(a, s, -1, A, B, b, D);
+}
+
 // ============================================================== forward ====
 // A task is one vertex's whole row: lane j loads neighbour j's mask words for
 // up to kHalf words at once (aligned 16-byte loads, all in flight), the
 // (word, neighbour) pairs that hit are listed in shared memory, and the
-// neighbours' path-count rows are gathered eight at a time (lane = slot,
+// neighbours' value rows are gathered eight at a time (lane = slot,
 // coalesced) into per-(word, slot) accumulators in shared memory. Adds to an
-// accumulator follow neighbour order, so sums are deterministic.
-
-constexpr int kHalf = 8;  // words per pass over a vertex row
+// accumulator follow arc order, so sums are deterministic.
 
 struct WarpScratch {
   uint32_t f[32][kHalf + 1];  // neighbour masks of the current 32-arc chunk (padded against bank conflicts)
@@ -209,7 +309,6 @@ struct WarpScratch {
   double acc[kHalf][32];      // per (word, slot) sums (FP64, or two FP32 halves in the compensated mode)
 };
 
-__device__ __forceinline__ uint4 and4(uint4 a, uint4 b) { return make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w); }
 __device__ __forceinline__ uint4 ld4(const uint32_t *p) { return __ldcg(reinterpret_cast<const uint4 *>(p)); }
 
 // Loads the kHalf-word mask row at p (first nw words, nw a multiple of 4).
@@ -230,20 +329,33 @@ __device__ __forceinline__ T warp_or(T v) {
 
 // One pull / successor pass over arcs [e0, e1) for words [w0, w0+nw):
 //   filt[k]  the slots of word w0+k that are looked for (uniform)
-//   masks    level masks of the neighbours (level t for the forward, t+1 for the backward)
+//   masks    level masks: of level t (unit arcs, kLev == 0), or the
+//            level-0 base of lm for chain arcs, whose arc e reads level
+//            t - hk[e] (kLev == 1, forward: sigma rebased from that level's
+//            X to level t's) or level t + hk[e] (kLev == 2, backward: q
+//            rebased to level t's X; levels above tend are empty)
 //   vals     per-slot values gathered on a hit (sigma, or q)
-// Accumulates into S.acc (ACC::add) and ORs the hits into any[k] (per lane).
-template <typename T, bool kComp>
+// Accumulates into S.acc and ORs the hits into any[k] (per lane).
+template <typename T, bool kComp, int kLev>
 __device__ __forceinline__ void row_pass(const Args &a, WarpScratch &S, const uint32_t *masks, const T *vals,
                                          int64_t e0, int64_t e1, int w0, int nw, const uint32_t (&filt)[kHalf],
-                                         uint32_t (&any)[kHalf], int lane) {
+                                         uint32_t (&any)[kHalf], int lane, int t, int tend = 0) {
   const int W = a.W;
   for (int64_t base = e0; base < e1; base += 32) {
     const int64_t e = base + lane;
-    const bool valid = e < e1;
-    const int32_t u = valid ? ldg(a.col + e) : 0;
+    bool valid = e < e1;
+    const int32_t u = valid ? ldg(a.hcol + e) : 0;
+    int lvl = t;
+    if (kLev == 1) {
+      lvl = valid ? t - ldg(a.hk + e) : -1;
+      valid = valid && lvl >= 0;
+    } else if (kLev == 2) {
+      lvl = valid ? t + ldg(a.hk + e) : INT_MAX;
+      valid = valid && lvl <= tend;
+    }
     uint32_t f[kHalf];
-    load_row(masks + (int64_t)u * W + w0, valid ? nw : 0, f);
+    const uint32_t *mrow = kLev ? masks + ((int64_t)(valid ? lvl : 0) * a.n_cap + u) * W + w0 : masks + (int64_t)u * W + w0;
+    load_row(mrow, valid ? nw : 0, f);
     int cnt = 0;
 #pragma unroll
     for (int k = 0; k < kHalf; ++k) {
@@ -276,7 +388,15 @@ __device__ __forceinline__ void row_pass(const Args &a, WarpScratch &S, const ui
           const int k = p >> 5, j = p & 31;
           const uint32_t fj = S.f[j][k];
           const int32_t uj = __shfl_sync(0xffffffffu, u, j);
-          if ((fj >> lane) & 1u) x[r] = __ldcg(vals + ((int64_t)uj * W + w0 + k) * 32 + lane);
+          const int lj = kLev ? __shfl_sync(0xffffffffu, lvl, j) : 0;
+          if ((fj >> lane) & 1u) {
+            x[r] = __ldcg(vals + ((int64_t)uj * W + w0 + k) * 32 + lane);
+            if (kLev) {
+              const int32_t *xb = a.X + (int64_t)((w0 + k) * 32 + lane) * (a.tcap + 2);
+              const int sh = kLev == 1 ? __ldcg(xb + lj) - __ldcg(xb + t) : __ldcg(xb + t) - __ldcg(xb + lj);
+              x[r] = (T)ldexp((double)x[r], sh);
+            }
+          }
           kk[r] = ((fj >> lane) & 1u) ? k : -1;
         }
       }
@@ -306,8 +426,8 @@ __device__ __forceinline__ double acc_value(const WarpScratch &S, int k, int lan
 }
 
 // Stores the result of one (vertex, word) of the forward step.
-__device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, uint32_t own,
-                                            int lane, double acc) {
+__device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, int lane,
+                                            double acc) {
   if (!newm) return;
   const int64_t idx = ((int64_t)v * a.W + w) * 32 + lane;
   if ((newm >> lane) & 1u) {
@@ -322,19 +442,70 @@ __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int
     a.lm[((int64_t)(t + 1) * a.n_cap + v) * a.W + w] = newm;
     a.seen[(int64_t)v * a.W + w] |= newm;
     a.ctrl->more = 1;
-    if (newm & own) {
-      atomicMin(a.lmin + v, t + 1);
-      atomicMax(a.lmax + v, t + 1);
-    }
+    atomicMin(a.lmin + v, t + 1);
+    atomicMax(a.lmax + v, t + 1);
   }
 }
 
 // ============================================================== backward ===
 
+// What core vertex v receives from the vertices of its chains, for the 32
+// slots of word w (the part that needs only forward results): cdep[v][w][.].
+// Chain-arc data are loaded lane-parallel, 32 arcs at a time; the far ends'
+// levels four arcs at a time.
+__device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int nslots, int32_t v, int w, int64_t c0,
+                                         int64_t c1, int lane) {
+  const int W = a.W;
+  const int b = w * 32 + lane;
+  const bool live = b < nslots;
+  const int64_t iv = ((int64_t)v * W + w) * 32 + lane;
+  const End A{live ? __ldcg(a.d + iv) : 0, iv};
+  Slot sl{0, -1, 0, 0};
+  if (live) sl = slots[b];
+  double sum = 0.0;
+  for (int64_t base = c0; base < c1; base += 32) {
+    const int64_t e = base + lane;
+    int32_t u = 0, cid = 0, k = 0;
+    int64_t poff = 0;
+    if (e < c1) {
+      u = ldg(a.hcol + e);
+      cid = ldg(a.hcid + e);
+      k = ldg(a.hk + e);
+      poff = ldg(a.cpre_off + (cid >> 1));
+    }
+    const int cnt = (int)min((int64_t)32, c1 - base);
+    for (int j0 = 0; j0 < cnt; j0 += 4) {
+      int32_t uj[4], cj[4], kj[4], dB[4];
+      int64_t pj[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        uj[r] = __shfl_sync(0xffffffffu, u, (j0 + r) & 31);
+        cj[r] = __shfl_sync(0xffffffffu, cid, (j0 + r) & 31);
+        kj[r] = __shfl_sync(0xffffffffu, k, (j0 + r) & 31);
+        pj[r] = __shfl_sync(0xffffffffu, poff, (j0 + r) & 31);
+        dB[r] = (live && j0 + r < cnt) ? __ldcg(a.d + ((int64_t)uj[r] * W + w) * 32 + lane) : 0;
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (!live || j0 + r >= cnt) continue;
+        const bool right = cj[r] & 1;
+        End B{dB[r], ((int64_t)uj[r] * W + w) * 32 + lane};
+        Stretch st{a.cpre + pj[r], 0, kj[r], right};
+        if (sl.chain == (cj[r] >> 1)) {  // the source sits on this chain: the stretch ends at it
+          B = End{0, -1};
+          st = right ? Stretch{a.cpre + pj[r], sl.pos + 1, kj[r], true} : Stretch{a.cpre + pj[r], 0, sl.pos, false};
+        }
+        sum += end_dep(a, st, A, B, b);
+      }
+    }
+  }
+  a.cdep[iv] = sum;
+}
+
 // delta, q and the BC partial of one (vertex, word) at level lev.
 template <typename QT>
 __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, const int32_t *rch, int32_t v, int w,
-                                           int lev, uint32_t act, int lane, double sum) {
+                                           int lev, uint32_t act, int lane, double sum, bool chains) {
   constexpr bool kF32 = sizeof(QT) == 4;
   if (!act) return;
   const int W = a.W;
@@ -344,7 +515,7 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
     const int64_t idx = ((int64_t)v * W + w) * 32 + lane;
     const double sv = a.sig[idx];
     const int xd = a.X[(int64_t)b * (a.tcap + 2) + lev] - a.X[(int64_t)b * (a.tcap + 2) + lev + 1];
-    const double delta = ldexp(sv * sum, xd);
+    const double delta = ldexp(sv * sum, xd) + (chains ? __ldcg(a.cdep + idx) : 0.0);
     const double qv = ((double)rch[v] + 1.0 + delta) / sv;
     if (kF32) {
       const double aq = fabs(qv);
@@ -382,15 +553,15 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     if (cta_failed(a)) return;
     const Batch bt = a.batches[bi];
     const Slot *slots = a.slots + bt.slot_off;
-    const uint32_t *bfs_mask = a.masks + bt.mask_off;
+    const Seed *seeds = a.seeds + bt.seed_off;
     const int words = bt.words;
     const int groups = (words + 3) / 4;
-    const int wpad = groups * 4;                 // masks are padded to whole groups
-    const uint32_t *own_mask = bfs_mask + wpad;
-    const uint32_t *chain_mask = own_mask + wpad;
+    const int wpad = groups * 4;  // rows are processed in whole 4-word groups
     const int64_t vo = a.vtx_off[bt.bcc];
-    const int32_t n = (int32_t)(a.vtx_off[bt.bcc + 1] - vo);
-    const int64_t *R = a.row + vo;
+    const int32_t nb = (int32_t)(a.vtx_off[bt.bcc + 1] - vo);
+    const int32_t n = a.n_plain[bt.bcc];  // core vertices
+    const int64_t *HR = a.hrow + a.hvo[bt.bcc];
+    const int64_t *HS = a.hsplit + a.hvo[bt.bcc];
     const int32_t *rch = a.reach + vo;
     const int32_t *hv = a.heavy + a.heavy_off[bt.bcc];
     const int32_t nheavy = (int32_t)(a.heavy_off[bt.bcc + 1] - a.heavy_off[bt.bcc]);
@@ -404,10 +575,11 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     const int64_t nblk = ((int64_t)n + 31) / 32;  // vertex blocks of 32 (lane l takes vertex blk + l*nblk)
     const int halves = (wpad + kHalf - 1) / kHalf;
 
-    // ---- init: seen = non-BFS slots, spans, partials, level-0/1 masks, X, rexp, work counters
+    // ---- init: seen = slots beyond the batch, partials, level-0/1 masks, X, rexp, work counters
     for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) {
       const int w = (int)(i % W);
-      a.seen[i] = w < wpad ? ~bfs_mask[w] : 0xffffffffu;
+      const int live = min(32, max(0, bt.nslots - 32 * w));
+      a.seen[i] = live == 32 ? 0u : ~((1u << live) - 1u);
       a.bcpart[i] = 0.0;
       a.lm[i] = 0;                         // level 0
       a.lm[(int64_t)a.n_cap * W + i] = 0;  // level 1
@@ -421,29 +593,29 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     if (gtid == 0) {
       a.ctrl->more = 0;
       a.ctrl->rescale = 0;
-      a.ctrl->tmax = 0;
       a.ctrl->range_err = 0;
     }
     grid_sync(a);
-    for (int64_t b = gtid; b < bt.nslots; b += gthreads) {  // sources at level 0
+    for (int64_t b = gtid; b < bt.nslots; b += gthreads) {  // core sources at level 0
       const Slot s = slots[b];
-      if (s.kind != kOwn && s.kind != kAux) continue;
+      if (s.chain >= 0) continue;
       const int64_t idx = ((int64_t)s.src * W + (b >> 5)) * 32 + (b & 31);
       a.d[idx] = 0;
       a.sig[idx] = 1.0;
       atomicOr(a.lm + (int64_t)s.src * W + (b >> 5), 1u << (b & 31));
       atomicOr(a.seen + (int64_t)s.src * W + (b >> 5), 1u << (b & 31));
-      if (s.kind == kOwn) { atomicMin(a.lmin + s.src, 0); atomicMax(a.lmax + s.src, 0); }
+      atomicMin(a.lmin + s.src, 0);
+      atomicMax(a.lmax + s.src, 0);
     }
     grid_sync(a);
     PHASE_MARK(0);
 
     // ---- forward: levels t -> t+1
-    int t = 0;
+    int t = 0, tlast = 0;
     while (true) {
       if (t + 1 > a.tcap) { set_err(a.err, kDevWorkspace); break; }
       const uint32_t *lmt = a.lm + (int64_t)t * a.n_cap * W;
-      // heavy vertices: chunks of their arcs, one CTA per (chunk, half); partials
+      // heavy rows: chunks of their arcs, one CTA per (chunk, half); partials
       // are combined across the CTA's warps, then across chunks after the barrier
       for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
         const int64_t c = task / halves;
@@ -458,10 +630,11 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
         if (u_any) {  // uniform over the CTA
-          const int64_t e0 = hce0[c], e1 = hce1[c];
+          const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < s1) row_pass<double, false>(a, S, lmt, a.sig, s0, s1, w0, nw, unseen, any, lane);
+          if (s0 < min(s1, sp)) row_pass<double, false, 0>(a, S, lmt, a.sig, s0, min(s1, sp), w0, nw, unseen, any, lane, t);
+          if (max(s0, sp) < s1) row_pass<double, false, 1>(a, S, a.lm, a.sig, max(s0, sp), s1, w0, nw, unseen, any, lane, t);
         }
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) {
@@ -478,14 +651,15 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         }
         __syncthreads();
       }
-      // light vertices: dynamic blocks of 32, lane-parallel activity check
+      // light rows: dynamic blocks of 32 vertices, lane-parallel activity check
       for (int64_t vb = next_block(a.wq + t, lane); vb < nblk; vb = next_block(a.wq + t, lane)) {
         const int64_t vl = vb + (int64_t)lane * nblk;
-        int64_t e0l = 0, e1l = 0;
+        int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
         if (vl < n) {
-          e0l = R[vl];
-          e1l = R[vl + 1];
+          e0l = HR[vl];
+          e1l = HR[vl + 1];
+          spl = HS[vl];
           on = e1l - e0l <= kHeavyDeg && __ldcg(a.gdone + vl) < groups;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, on);
@@ -494,6 +668,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           todo &= todo - 1;
           const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
           const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
+          const int64_t sp = __shfl_sync(0xffffffffu, spl, j);
           for (int w0 = 0; w0 < wpad; w0 += kHalf) {
             const int nw = min(kHalf, wpad - w0);
             uint32_t seen[kHalf], unseen[kHalf], any[kHalf];
@@ -504,16 +679,17 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             if (!u_any) continue;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-            row_pass<double, false>(a, S, lmt, a.sig, e0, e1, w0, nw, unseen, any, lane);
+            if (e0 < sp) row_pass<double, false, 0>(a, S, lmt, a.sig, e0, sp, w0, nw, unseen, any, lane, t);
+            if (sp < e1) row_pass<double, false, 1>(a, S, a.lm, a.sig, sp, e1, w0, nw, unseen, any, lane, t);
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) {
               if (k >= nw) continue;
               const uint32_t m = warp_or(any[k]);
-              finish_pull(a, v, w0 + k, t, m, own_mask[w0 + k], lane, S.acc[k][lane]);
+              finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
               any[k] = m;
             }
 #pragma unroll
-            for (int g = 0; g < kHalf / 4; ++g) {  // groups now seen by all their BFS slots
+            for (int g = 0; g < kHalf / 4; ++g) {  // groups now seen by all their slots
               if (4 * g >= nw || lane != 0) continue;
               bool was = true, now = true;
 #pragma unroll
@@ -541,10 +717,32 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             acc += __ldcg(a.hacc + ((hc0 + c) * W + w) * 32 + lane);
             m |= __ldcg(a.hmask + (hc0 + c) * W + w);
           }
-          finish_pull(a, v, w, t, m, own_mask[w], lane, acc);
+          finish_pull(a, v, w, t, m, lane, acc);
         }
         grid_sync(a);
         PHASE_MARK(2);
+      }
+      if (bt.nseeds) {  // chain sources entering the core at level t+1 (one path each)
+        for (int64_t i = gtid; i < bt.nseeds; i += gthreads) {
+          const Seed s = seeds[i];
+          if (s.level != t + 1) continue;
+          const int b = s.slot, w = b >> 5;
+          const uint32_t bit = 1u << (b & 31);
+          const int64_t idx = ((int64_t)s.v * W + w) * 32 + (b & 31);
+          const double one = ldexp(1.0, -a.X[(int64_t)b * (a.tcap + 2) + t]);
+          const uint32_t old = atomicOr(a.seen + (int64_t)s.v * W + w, bit);
+          if (!(old & bit)) {
+            a.d[idx] = t + 1;
+            a.sig[idx] = one;
+            atomicOr(a.lm + ((int64_t)(t + 1) * a.n_cap + s.v) * W + w, bit);
+            atomicMin(a.lmin + s.v, t + 1);
+            atomicMax(a.lmax + s.v, t + 1);
+            a.ctrl->more = 1;
+          } else if (a.d[idx] == t + 1) {
+            a.sig[idx] += one;  // reached on this level from the core as well
+          }
+        }
+        grid_sync(a);
       }
       const int more = *(volatile int *)&a.ctrl->more;
       const int resc = *(volatile int *)&a.ctrl->rescale;
@@ -572,7 +770,10 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         a.ctrl->more = 0;
         a.ctrl->rescale = 0;
       }
-      if (!more || cta_failed(a)) break;
+      if (more) tlast = t + 1;
+      if (cta_failed(a)) break;
+      // level t+2 needs a non-empty level within the longest arc, or a seed
+      if (t + 1 - tlast > bt.kmax && t + 2 > bt.max_seed) break;
       ++t;
       for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 1) * a.n_cap * W + i] = 0;
       grid_sync(a);
@@ -580,108 +781,30 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     }
     PHASE_MARK(3);
     if (cta_failed(a)) return;
-    const int tbfs = t;  // deepest level with BFS vertices
-
-    // ---- chain slots: clear the levels above the BFS depth they may use,
-    // per-level base exponents, then the merge
-    const int top = min(a.tcap + 1, tbfs + bt.max_off + 1);
-    for (int lv = tbfs + 2; lv <= top; ++lv)
-      for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)lv * a.n_cap * W + i] = 0;
-    for (int64_t i = gtid; i < (int64_t)bt.nslots * (a.tcap + 1); i += gthreads) {
-      const int b = (int)(i / (a.tcap + 1));
-      const int lv = (int)(i % (a.tcap + 1));
-      const Slot s = slots[b];
-      if (s.kind != kChain) continue;
-      int x = INT_MIN;
-      if (lv - s.ld >= 0 && lv - s.ld <= tbfs) x = max(x, a.X[(int64_t)s.sl * (a.tcap + 2) + lv - s.ld]);
-      if (lv - s.rd >= 0 && lv - s.rd <= tbfs) x = max(x, a.X[(int64_t)s.sr * (a.tcap + 2) + lv - s.rd]);
-      a.X[(int64_t)b * (a.tcap + 2) + lv] = x == INT_MIN ? 0 : x;
+    // every slot must have reached every core vertex of the BCC
+    for (int64_t i = gtid; i < (int64_t)n * words; i += gthreads) {
+      const int32_t v = (int32_t)(i / words);
+      const int w = (int)(i % words);
+      if (~__ldcg(a.seen + (int64_t)v * W + w) != 0u) set_err(a.err, kDevDisconnected);
     }
-    grid_sync(a);
-    int tmax_local = tbfs;
-    for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
-      const int32_t v = (int32_t)(task / words);
-      const int w = (int)(task % words);
-      // every BFS slot must have reached every vertex of the BCC
-      if (lane == 0 && ~__ldcg(a.seen + (int64_t)v * W + w) != 0u) set_err(a.err, kDevDisconnected);
-      const uint32_t cm = chain_mask[w];
-      if (!cm) continue;
-      const int b = w * 32 + lane;
-      int lvl = -1;
-      if ((cm >> lane) & 1u) {
-        const Slot s = slots[b];
-        const int64_t il = ((int64_t)v * W + (s.sl >> 5)) * 32 + (s.sl & 31);
-        const int64_t ir = ((int64_t)v * W + (s.sr >> 5)) * 32 + (s.sr & 31);
-        int dl = a.d[il], dr = a.d[ir];
-        if (dl < 0 || dl > tbfs || dr < 0 || dr > tbfs) {  // unreached (flagged above): keep indices in range
-          set_err(a.err, kDevDisconnected);
-          dl = dr = 0;
-        }
-        const int x1 = dl + s.ld, x2 = dr + s.rd;
-        lvl = min(x1, x2);
-        if (lvl > a.tcap) {  // cannot happen within the eccentricity bound; keep indices in range
-          set_err(a.err, kDevWorkspace);
-          lvl = a.tcap;
-        }
-        const int xz = a.X[(int64_t)b * (a.tcap + 2) + lvl];
-        double sg = 0.0;
-        if (x1 <= x2) sg += ldexp(a.sig[il], a.X[(int64_t)s.sl * (a.tcap + 2) + dl] - xz);
-        if (x2 <= x1) sg += ldexp(a.sig[ir], a.X[(int64_t)s.sr * (a.tcap + 2) + dr] - xz);
-        const int64_t iz = ((int64_t)v * W + w) * 32 + lane;
-        a.d[iz] = lvl;
-        a.sig[iz] = sg;
-        tmax_local = max(tmax_local, lvl);
+    // what the core vertices receive from their chains' vertices
+    if (bt.kmax) {
+      for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
+        const int32_t v = (int32_t)(task / words);
+        const int w = (int)(task % words);
+        const int64_t c0 = HS[v], c1 = HR[v + 1];
+        if (c0 < c1) chain_in(a, slots, bt.nslots, v, w, c0, c1, lane);
       }
-      // set level bits: one writer per (vertex, word) in this phase
-      uint32_t todo = __ballot_sync(0xffffffffu, lvl >= 0);
-      while (todo) {
-        const int leader = __ffs(todo) - 1;
-        const int L = __shfl_sync(0xffffffffu, lvl, leader);
-        const uint32_t grp = __ballot_sync(0xffffffffu, lvl == L);
-        if (lane == leader) {
-          a.lm[((int64_t)L * a.n_cap + v) * W + w] |= grp;
-          atomicMin(a.lmin + v, L);
-          atomicMax(a.lmax + v, L);
-        }
-        todo &= ~grp;
-      }
+      grid_sync(a);
     }
-    tmax_local = warp_max(tmax_local);
-    if (lane == 0) atomicMax(&a.ctrl->tmax, tmax_local);
-    grid_sync(a);
-    // same-chain vertices: the direct distance along the chain wins or ties
-    for (int64_t b = gtid; b < bt.nslots; b += gthreads) {
-      const Slot s = slots[b];
-      if (s.kind != kChain) continue;
-      for (int j = 0; j < s.clen; ++j) {
-        const int32_t k = s.cstart + j;
-        const int dist = j > s.cpos ? j - s.cpos : s.cpos - j;
-        const int64_t iz = ((int64_t)k * W + (b >> 5)) * 32 + (b & 31);
-        const int cur = a.d[iz];
-        const double one = ldexp(1.0, -a.X[b * (a.tcap + 2) + dist]);
-        if (cur > dist) {
-          atomicAnd(a.lm + ((int64_t)cur * a.n_cap + k) * W + (b >> 5), ~(1u << (b & 31)));
-          atomicOr(a.lm + ((int64_t)dist * a.n_cap + k) * W + (b >> 5), 1u << (b & 31));
-          atomicMin(a.lmin + k, dist);
-          a.d[iz] = dist;
-          a.sig[iz] = one;
-        } else if (cur == dist) {
-          a.sig[iz] += one;
-        }
-      }
-    }
-    grid_sync(a);
-    const int tmax = *(volatile int *)&a.ctrl->tmax;
-    if (tmax + 1 > a.tcap) set_err(a.err, kDevWorkspace);
-    if (cta_failed(a)) return;
     PHASE_MARK(4);
 
-    // ---- backward: t = tmax .. 1
-    for (int lev = tmax; lev >= 1; --lev) {
+    // ---- backward: lev = tlast .. 1
+    for (int lev = tlast; lev >= 1; --lev) {
       const uint32_t *lm_here = a.lm + (int64_t)lev * a.n_cap * W;
       const uint32_t *lm_next = a.lm + (int64_t)(lev + 1) * a.n_cap * W;
       const QT *q = reinterpret_cast<const QT *>(a.q);
-      // heavy vertices: chunked successor sums, combined below
+      // heavy rows: chunked successor sums, combined below
       for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
         const int64_t c = task / halves;
         const int w0 = (int)(task % halves) * kHalf;
@@ -693,17 +816,18 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         uint32_t a_any = 0;
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) {
-          act[k] = (in_span && k < nw) ? act[k] & own_mask[w0 + k] : 0u;
+          act[k] = (in_span && k < nw) ? act[k] : 0u;
           any[k] = 0;
           a_any |= act[k];
         }
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
         if (a_any) {  // uniform over the CTA
-          const int64_t e0 = hce0[c], e1 = hce1[c];
+          const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < s1) row_pass<QT, kComp>(a, S, lm_next, q, s0, s1, w0, nw, act, any, lane);
+          if (s0 < min(s1, sp)) row_pass<QT, kComp, 0>(a, S, lm_next, q, s0, min(s1, sp), w0, nw, act, any, lane, lev + 1);
+          if (max(s0, sp) < s1) row_pass<QT, kComp, 2>(a, S, a.lm, q, max(s0, sp), s1, w0, nw, act, any, lane, lev + 1, tlast);
         }
         __syncthreads();
         for (int k = wib; k < nw; k += kWarpsPerCta) {  // fixed warp order
@@ -716,11 +840,12 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       const int wqi = a.tcap + 3 + lev;
       for (int64_t vb = next_block(a.wq + wqi, lane); vb < nblk; vb = next_block(a.wq + wqi, lane)) {
         const int64_t vl = vb + (int64_t)lane * nblk;
-        int64_t e0l = 0, e1l = 0;
+        int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
         if (vl < n && lev >= __ldcg(a.lmin + vl) && lev <= __ldcg(a.lmax + vl)) {
-          e0l = R[vl];
-          e1l = R[vl + 1];
+          e0l = HR[vl];
+          e1l = HR[vl + 1];
+          spl = HS[vl];
           on = e1l - e0l <= kHeavyDeg;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, on);
@@ -729,6 +854,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           todo &= todo - 1;
           const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
           const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
+          const int64_t sp = __shfl_sync(0xffffffffu, spl, j);
           for (int w0 = 0; w0 < wpad; w0 += kHalf) {
             const int nw = min(kHalf, wpad - w0);
             uint32_t act[kHalf], any[kHalf];
@@ -736,17 +862,19 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             uint32_t a_any = 0;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) {
-              act[k] = k < nw ? act[k] & own_mask[w0 + k] : 0u;
+              act[k] = k < nw ? act[k] : 0u;
               any[k] = 0;
               a_any |= act[k];
             }
             if (!a_any) continue;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-            row_pass<QT, kComp>(a, S, lm_next, q, e0, e1, w0, nw, act, any, lane);
+            if (e0 < sp) row_pass<QT, kComp, 0>(a, S, lm_next, q, e0, sp, w0, nw, act, any, lane, lev + 1);
+            if (sp < e1) row_pass<QT, kComp, 2>(a, S, a.lm, q, sp, e1, w0, nw, act, any, lane, lev + 1, tlast);
 #pragma unroll
             for (int k = 0; k < kHalf; ++k)
-              if (k < nw) finish_dep<QT>(a, slots, rch, v, w0 + k, lev, act[k], lane, acc_value(S, k, lane, kComp));
+              if (k < nw)
+                finish_dep<QT>(a, slots, rch, v, w0 + k, lev, act[k], lane, acc_value(S, k, lane, kComp), sp < e1);
           }
         }
       }
@@ -758,23 +886,56 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int w = (int)(task % wpad);
           const int32_t v = hv[h];
           if (lev < __ldcg(a.lmin + v) || lev > __ldcg(a.lmax + v)) continue;
-          const uint32_t act = __ldcg(lm_here + (int64_t)v * W + w) & own_mask[w];
+          const uint32_t act = __ldcg(lm_here + (int64_t)v * W + w);
           if (!act) continue;
           double sum = 0.0;
           for (int32_t c = hfst[h]; c < hfst[h + 1]; ++c) sum += __ldcg(a.hacc + ((hc0 + c) * W + w) * 32 + lane);
-          finish_dep<QT>(a, slots, rch, v, w, lev, act, lane, sum);
+          finish_dep<QT>(a, slots, rch, v, w, lev, act, lane, sum, HS[v] < HR[v + 1]);
         }
       }
       grid_sync(a);
       PHASE_MARK(6);
       PHASE_COUNT(17);
     }
+
+    // ---- chain vertices: one warp per (chain, word), every vertex of the chain
+    {
+      const int64_t ch0 = a.chain_off[bt.bcc];
+      const int64_t nch = a.chain_off[bt.bcc + 1] - ch0;
+      for (int64_t task = gwarp(); task < nch * words; task += nwarps()) {
+        const int64_t c = ch0 + task / words;
+        const int w = (int)(task % words);
+        const int b = w * 32 + lane;
+        const bool live = b < bt.nslots;
+        const int32_t L = a.chain_l[c], R = a.chain_r[c], cs = a.chain_start[c], k = a.chain_len[c];
+        const double *P = a.cpre + a.cpre_off[c];
+        const int64_t iL = ((int64_t)L * W + w) * 32 + lane, iR = ((int64_t)R * W + w) * 32 + lane;
+        const End eL{live ? __ldcg(a.d + iL) : 0, iL}, eR{live ? __ldcg(a.d + iR) : 0, iR};
+        Slot sl{0, -1, 0, 0};
+        if (live) sl = slots[b];
+        const int on = sl.chain == c ? sl.pos : -1;
+        const double wsrc = live ? (double)rch[sl.src] + 1.0 : 0.0;
+        for (int j = 0; j < k; ++j) {
+          double dep = 0.0;
+          if (live) {
+            if (on < 0) dep = stretch_dep<QT>(a, Stretch{P, 0, k, false}, j, eL, eR, b);
+            else if (j < on) dep = stretch_dep<QT>(a, Stretch{P, 0, on, false}, j, eL, End{0, -1}, b);
+            else if (j > on) dep = stretch_dep<QT>(a, Stretch{P, on + 1, k, false}, j - on - 1, End{0, -1}, eR, b);
+          }
+          const double tot = warp_sum(dep * wsrc);
+          if (lane == 0) a.bcpart[(int64_t)(cs + j) * W + w] = tot;
+        }
+      }
+    }
+    grid_sync(a);
+    PHASE_MARK(8);
+
     // ---- fold the batch into BC (fixed word order), unless FP32 range failed
     const int bad = *(volatile int *)&a.ctrl->range_err;
     if (bad) {
       if (gtid == 0) a.redo[bi] = 1;
     } else {
-      for (int64_t v = gtid; v < n; v += gthreads) {
+      for (int64_t v = gtid; v < nb; v += gthreads) {
         double s = 0.0;
         for (int w = 0; w < words; ++w) s += a.bcpart[v * W + w];
         a.bc[vo + v] += s;
@@ -807,8 +968,8 @@ struct BatchedPlan {
 
 namespace {
 
-// Eccentricity bound of a BCC (BFS from local vertex 0): every level of every
-// source is < 2 * ecc + 1.
+// Eccentricity of local vertex 0 in the BCC: every level of every source is
+// at most 2 * ecc.
 int bcc_ecc(const int64_t *row, const int32_t *col, int64_t vo, int32_t nb, std::vector<int32_t> &dist,
             std::vector<int32_t> &queue) {
   dist.assign((size_t)nb, -1);
@@ -834,7 +995,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
                    const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
                    const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
                    BatchedPlan **out, std::string *msg) {
-  (void)chain_start; (void)chain_len; (void)chain_l; (void)chain_r;
+  (void)row; (void)col;
   auto *P = new BatchedPlan;
   auto bail = [&](int code, const std::string &m) {
     if (msg) *msg = m;
@@ -848,140 +1009,110 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   P->W = (width / 32 + 3) / 4 * 4;  // row stride: whole 4-word groups (16-byte mask loads)
   const int W = P->W;
 
-  // ---- host scheduling: batches of slots per BCC
+  // ---- contracted rows, chain prefix sums, heavy chunks, passes
+  std::vector<int64_t> hvo, hrow, hsplit, cpre_off;
+  std::vector<int32_t> hcol, hk, hcid;
+  std::vector<double> cpre;
   std::vector<Slot> slots;
-  std::vector<uint32_t> masks;
+  std::vector<Seed> seeds;
   std::vector<int64_t> heavy_off{0}, hchunk_off{0}, hchunk_e0, hchunk_e1;
   std::vector<int32_t> heavy, hchunk_v, hfirst;
   std::vector<int32_t> dist, queue;
-  int64_t nmax = 0;
+  std::vector<int32_t> cof, cpos;  // chain vertex -> chain (global), position
+  int64_t ncap = 1, nbcap = 1;
   int tcap = 2;
+  cpre_off.resize((size_t)B->n_chains);
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     const int64_t vo = B->vtx_off[b];
     const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
     const int32_t npl = B->n_plain[b];
-    nmax = std::max<int64_t>(nmax, nb);
+    const int64_t ce0 = B->chain_off[b], ce1 = B->chain_off[b + 1];
+    ncap = std::max<int64_t>(ncap, npl);
+    nbcap = std::max<int64_t>(nbcap, nb);
     const int64_t arcs = B->row[vo + nb] - B->row[vo];
+    // chain membership, and the shape the closed forms rely on: each chain
+    // vertex has exactly its two chain neighbours, the ends are distinct core vertices
+    cof.assign((size_t)nb, -1);
+    cpos.assign((size_t)nb, -1);
+    int kmax = 0;
+    for (int64_t c = ce0; c < ce1; ++c) {
+      const int32_t s = B->chain_start[c], k = B->chain_len[c], L = B->chain_l[c], R = B->chain_r[c];
+      if (L == R) return bail(BCGPU_EINVAL, "a chain whose two ends are the same vertex");
+      kmax = std::max(kmax, k);
+      for (int32_t j = 0; j < k; ++j) {
+        if (cof[s + j] >= 0) return bail(BCGPU_EINVAL, "chains overlap");
+        cof[s + j] = (int32_t)c;
+        cpos[s + j] = j;
+      }
+      for (int32_t j = 0; j < k; ++j) {
+        const int32_t x = s + j, prev = j == 0 ? L : x - 1, next = j == k - 1 ? R : x + 1;
+        const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
+        if (e1 - e0 != 2 || !((B->col[e0] == prev && B->col[e0 + 1] == next) || (B->col[e0] == next && B->col[e0 + 1] == prev)))
+          return bail(BCGPU_EINVAL, "a chain vertex whose neighbours are not its chain neighbours");
+      }
+      cpre_off[c] = (int64_t)cpre.size();
+      double acc = 0.0;
+      cpre.push_back(0.0);
+      for (int32_t j = 0; j < k; ++j) {
+        acc += (double)B->reach[vo + s + j] + 1.0;
+        cpre.push_back(acc);
+      }
+    }
+    // contracted rows: unit arcs first, then chain arcs
+    hvo.push_back((int64_t)hrow.size());
     int32_t hidx = 0;
-    for (int32_t k = 0; k < nb; ++k) {
-      const int64_t e0 = B->row[vo + k], e1 = B->row[vo + k + 1];
-      if (e1 - e0 <= kHeavyDeg) continue;
-      heavy.push_back(k);
+    for (int32_t x = 0; x < npl; ++x) {
+      const int64_t r0 = (int64_t)hcol.size();
+      hrow.push_back(r0);
+      const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
+      for (int64_t e = e0; e < e1; ++e)
+        if (B->col[e] < npl) { hcol.push_back(B->col[e]); hk.push_back(0); hcid.push_back(-1); }
+      hsplit.push_back((int64_t)hcol.size());
+      for (int64_t e = e0; e < e1; ++e) {
+        const int32_t y = B->col[e];
+        if (y < npl) continue;
+        const int64_t c = cof[y];
+        if (c < 0) return bail(BCGPU_EINVAL, "a non-core vertex outside every chain");
+        const int32_t k = B->chain_len[c];
+        int right;
+        if (x == B->chain_l[c] && cpos[y] == 0) right = 0;
+        else if (x == B->chain_r[c] && cpos[y] == k - 1) right = 1;
+        else return bail(BCGPU_EINVAL, "a core vertex adjacent to the inside of a chain");
+        hcol.push_back(right ? B->chain_l[c] : B->chain_r[c]);
+        hk.push_back(k);
+        hcid.push_back((int32_t)(c * 2 + right));
+      }
+      const int64_t r1 = (int64_t)hcol.size();
+      if (r1 - r0 <= kHeavyDeg) continue;
+      heavy.push_back(x);
       hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
-      for (int64_t e = e0; e < e1; e += kChunkArcs) {
+      for (int64_t e = r0; e < r1; e += kChunkArcs) {
         hchunk_v.push_back(hidx);
         hchunk_e0.push_back(e);
-        hchunk_e1.push_back(std::min<int64_t>(e1, e + kChunkArcs));
+        hchunk_e1.push_back(std::min<int64_t>(r1, e + kChunkArcs));
       }
       ++hidx;
     }
+    hrow.push_back((int64_t)hcol.size());
+    hsplit.push_back((int64_t)hcol.size());
     hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
     heavy_off.push_back((int64_t)heavy.size());
     hchunk_off.push_back((int64_t)hchunk_v.size());
-    int maxchain = 0;
-    for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) maxchain = std::max(maxchain, B->chain_len[c]);
-    tcap = std::max(tcap, 2 * bcc_ecc(B->row, B->col, vo, nb, dist, queue) + maxchain + 3);
+    tcap = std::max(tcap, 2 * bcc_ecc(B->row, B->col, vo, nb, dist, queue) + kmax + 3);
 
-    // greedy packing: each plain source with the chains it owns
-    std::vector<Slot> cur;
-    std::vector<int32_t> slot_of((size_t)nb, -1);
-    const bool merge = cfg.chain_merge;
-    const int32_t nsrc_bfs = merge ? npl : nb;  // vertices that become BFS slots
-    std::vector<int32_t> touched;
-    int64_t c = B->chain_off[b];
-    const int64_t ce = B->chain_off[b + 1];
-    int64_t src_cnt = 0, bfs_cnt = 0, aux_cnt = 0;
-    auto flush = [&]() {
-      if (cur.empty()) return;
-      Batch bt{};
-      bt.bcc = b;
-      bt.nslots = (int32_t)cur.size();
-      bt.max_off = 0;
-      for (const Slot &z : cur)
-        if (z.kind == kChain) bt.max_off = std::max(bt.max_off, std::max(z.ld, z.rd));
-      bt.words = (bt.nslots + 31) / 32;
-      bt.slot_off = (int64_t)slots.size();
-      bt.mask_off = (int64_t)masks.size();
-      const int wpad = (bt.words + 3) / 4 * 4;  // masks padded to whole groups, 16-byte aligned
-      std::vector<uint32_t> mb((size_t)wpad, 0), mo((size_t)wpad, 0), mc((size_t)wpad, 0);
-      for (int32_t i = 0; i < bt.nslots; ++i) {
-        const uint32_t bit = 1u << (i & 31);
-        if (cur[i].kind == kOwn || cur[i].kind == kAux) mb[i >> 5] |= bit;
-        if (cur[i].kind == kOwn || cur[i].kind == kChain) mo[i >> 5] |= bit;
-        if (cur[i].kind == kChain) mc[i >> 5] |= bit;
-      }
-      masks.insert(masks.end(), mb.begin(), mb.end());
-      masks.insert(masks.end(), mo.begin(), mo.end());
-      masks.insert(masks.end(), mc.begin(), mc.end());
-      slots.insert(slots.end(), cur.begin(), cur.end());
-      P->h_batches.push_back(bt);
-      const int64_t prev = P->u_src.empty() ? 0 : P->u_src.back();
-      (void)prev;
-      P->u_src.push_back(src_cnt);
-      P->u_teps.push_back(src_cnt * arcs);
-      P->u_bfs.push_back(bfs_cnt);
-      P->u_aux.push_back(aux_cnt);
-      P->u_visits.push_back(src_cnt * nb);
-      for (int32_t x : touched) slot_of[x] = -1;
-      touched.clear();
-      cur.clear();
-      src_cnt = bfs_cnt = aux_cnt = 0;
-    };
-    auto bfs_slot = [&](int32_t x, int32_t kind) -> int32_t {
-      if (slot_of[x] >= 0) {
-        if (kind == kOwn && cur[slot_of[x]].kind == kAux) {
-          cur[slot_of[x]].kind = kOwn;
-          ++src_cnt; ++bfs_cnt; --aux_cnt;
-        }
-        return slot_of[x];
-      }
-      Slot s{};
-      s.kind = kind;
-      s.src = x;
-      slot_of[x] = (int32_t)cur.size();
-      touched.push_back(x);
-      cur.push_back(s);
-      if (kind == kOwn) { ++src_cnt; ++bfs_cnt; }
-      else ++aux_cnt;
-      return slot_of[x];
-    };
-    // Source order: bounded BFS balls of nearby plain vertices, so a pass's
-    // sources see every vertex within a narrow band of levels (few active
-    // levels per vertex, dense 32-slot hits) and the right endpoints of the
-    // chains they own are mostly own slots of the same pass.
-    // Each chain is owned (scheduled with) its lower-degree endpoint: a pass
-    // then holds many small owners whose chains lead to the same few hubs,
-    // which appear once each as helper BFS slots.
-    auto degb = [&](int32_t x) { return B->row[vo + x + 1] - B->row[vo + x]; };
-    std::vector<int64_t> own_off((size_t)npl + 1, 0);
-    std::vector<int64_t> owned((size_t)(ce - B->chain_off[b]));
-    auto owner = [&](int64_t cc) {
-      const int32_t l = B->chain_l[cc], r = B->chain_r[cc];
-      return degb(l) <= degb(r) ? l : r;
-    };
-    for (int64_t cc = B->chain_off[b]; cc < ce; ++cc) own_off[owner(cc) + 1]++;
-    for (int32_t x = 0; x < npl; ++x) own_off[x + 1] += own_off[x];
-    {
-      std::vector<int64_t> fill(own_off.begin(), own_off.end() - 1);
-      for (int64_t cc = B->chain_off[b]; cc < ce; ++cc) owned[fill[owner(cc)]++] = cc;
-    }
-    auto slots_of = [&](int32_t s) {
-      int64_t k = 1;
-      if (merge && s < npl)
-        for (int64_t i = own_off[s]; i < own_off[s + 1]; ++i) k += B->chain_len[owned[i]];
-      return k;
-    };
+    // Source order: bounded BFS balls of nearby vertices (chain vertices
+    // included), so a pass's sources see every vertex within a narrow band of
+    // levels: few active levels per vertex, dense 32-slot hits. A ball grows
+    // only through vertices not yet taken, so each vertex's arcs are scanned
+    // once and late balls cost no rescans of finished regions.
     std::vector<int32_t> order;
-    order.reserve((size_t)nsrc_bfs);
+    order.reserve((size_t)nb);
     {
-      std::vector<char> done((size_t)nsrc_bfs, 0);
+      std::vector<char> done((size_t)nb, 0);
       std::vector<int32_t> stamp((size_t)nb, -1), q;
       int32_t ball = 0;
       const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
-      // A ball grows only through vertices it can still take (and, in the
-      // merge form, through chain vertices): each source's arcs are scanned
-      // once, so late balls cost no rescans of finished regions.
-      for (int32_t seed = 0; seed < nsrc_bfs; ++seed) {
+      for (int32_t seed = 0; seed < nb; ++seed) {
         if (done[seed]) continue;
         q.clear();
         q.push_back(seed);
@@ -989,60 +1120,55 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         int64_t got = 0, scanned = 0;
         for (size_t h = 0; h < q.size() && got < width; ++h) {
           const int32_t x = q[h];
-          if (x < nsrc_bfs) {
-            done[x] = 1;
-            order.push_back(x);
-            got += slots_of(x);
-          }
+          done[x] = 1;
+          order.push_back(x);
+          ++got;
           if (scanned >= arc_budget) continue;  // keep draining the queue, stop growing it
           const int64_t e0 = B->row[vo + x], e1 = std::min(B->row[vo + x + 1], e0 + arc_budget - scanned);
           scanned += e1 - e0;
           for (int64_t e = e0; e < e1; ++e) {
             const int32_t y = B->col[e];
-            if (stamp[y] != ball && (y >= nsrc_bfs || !done[y])) { stamp[y] = ball; q.push_back(y); }
+            if (stamp[y] != ball && !done[y]) { stamp[y] = ball; q.push_back(y); }
           }
         }
         ++ball;
       }
     }
-    for (int32_t s : order) {
-      if ((int)cur.size() + 1 > width) flush();
-      bfs_slot(s, kOwn);
-      if (!merge) continue;
-      for (int64_t oi = own_off[s]; oi < own_off[s + 1]; ++oi) {
-        c = owned[oi];
-        const int32_t len = B->chain_len[c];
-        const int32_t other = B->chain_l[c] == s ? B->chain_r[c] : B->chain_l[c];
-        const int need = len + (slot_of[other] >= 0 ? 0 : 1);
-        if ((int)cur.size() + need > width) {
-          flush();
-          bfs_slot(s, kAux);  // the owner returns as a forward-only slot
+    for (size_t i0 = 0; i0 < order.size(); i0 += (size_t)width) {
+      const size_t i1 = std::min(order.size(), i0 + (size_t)width);
+      Batch bt{};
+      bt.bcc = b;
+      bt.nslots = (int32_t)(i1 - i0);
+      bt.words = (bt.nslots + 31) / 32;
+      bt.kmax = kmax;
+      bt.slot_off = (int64_t)slots.size();
+      bt.seed_off = (int64_t)seeds.size();
+      for (size_t i = i0; i < i1; ++i) {
+        const int32_t s = order[i];
+        const int32_t slot = (int32_t)(i - i0);
+        if (s < npl) {
+          slots.push_back(Slot{s, -1, 0, 0});
+          continue;
         }
-        if ((int)cur.size() + len + (slot_of[other] >= 0 ? 0 : 1) > width) {
-          if (msg) *msg = "chain longer than the batch width";
-          delete P;
-          return BCGPU_EINVAL;
-        }
-        bfs_slot(other, kAux);
-        const int32_t sl = slot_of[B->chain_l[c]], sr = slot_of[B->chain_r[c]];
-        for (int32_t pos = 0; pos < len; ++pos) {
-          Slot z{};
-          z.kind = kChain;
-          z.src = B->chain_start[c] + pos;
-          z.sl = sl; z.sr = sr;
-          z.ld = pos + 1; z.rd = len - pos;
-          z.cstart = B->chain_start[c]; z.clen = len; z.cpos = pos;
-          cur.push_back(z);
-          ++src_cnt;
-        }
+        const int64_t c = cof[s];
+        const int32_t p = cpos[s], k = B->chain_len[c];
+        slots.push_back(Slot{s, (int32_t)c, p, 0});
+        seeds.push_back(Seed{B->chain_l[c], p + 1, slot, 0});
+        seeds.push_back(Seed{B->chain_r[c], k - p, slot, 0});
+        bt.max_seed = std::max(bt.max_seed, std::max(p + 1, k - p));
       }
+      bt.nseeds = (int32_t)((int64_t)seeds.size() - bt.seed_off);
+      P->h_batches.push_back(bt);
+      P->u_src.push_back(bt.nslots);
+      P->u_teps.push_back((int64_t)bt.nslots * arcs);
+      P->u_bfs.push_back(bt.nslots);
+      P->u_aux.push_back(0);
+      P->u_visits.push_back((int64_t)bt.nslots * nb);
     }
-    flush();
   }
   P->tcap = tcap;
-  P->n_cap = std::max<int64_t>(nmax, 1);
+  P->n_cap = ncap;
   P->n_batches = (int64_t)P->h_batches.size();
-  // prefix sums over batches
   auto prefix = [](std::vector<int64_t> &v) {
     std::vector<int64_t> p(v.size() + 1, 0);
     for (size_t i = 0; i < v.size(); ++i) p[i + 1] = p[i] + v[i];
@@ -1053,8 +1179,9 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   // ---- device workspace
   const int64_t n = P->n_cap;
   const int64_t qb = P->f32 ? 4 : 8;
-  const int64_t need = n * W * 32 * (4 + 8 + qb) + (int64_t)(tcap + 2) * n * W * 4 + n * W * (4 + 8) + n * 12 +
-                       (int64_t)W * 32 * (tcap + 2) * 4;
+  const int64_t nch = (int64_t)hchunk_v.size();
+  const int64_t need = n * W * 32 * (4 + 8 + 8 + qb) + (int64_t)(tcap + 2) * n * W * 4 + n * W * 4 + n * 12 +
+                       nbcap * W * 8 + (int64_t)W * 32 * (tcap + 2) * 4 + nch * W * 32 * 8;
   if (need > cfg.limit_bytes)
     return bail(BCGPU_ENOMEM, "batched workspace " + std::to_string(need >> 20) + " MiB exceeds the limit " +
                                   std::to_string(cfg.limit_bytes >> 20) + " MiB (lower the batch width)");
@@ -1076,46 +1203,49 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
   ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
-  ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
+  ok &= ok && alloc(&p, nbcap * W * 8); a.bcpart = (double *)p;
+  ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * (tcap + 2) * 4); a.X = (int32_t *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 4); a.rexp = (int32_t *)p;
   ok &= ok && alloc(&p, sizeof(Ctrl)); a.ctrl = (Ctrl *)p;
   ok &= ok && alloc(&p, (int64_t)std::max<int64_t>(P->n_batches, 1) * 4); a.redo = (int *)p;
-  ok &= ok && alloc(&p, (int64_t)heavy_off.size() * 8); a.heavy_off = (int64_t *)p;
-  ok &= ok && alloc(&p, (int64_t)std::max<size_t>(heavy.size(), 1) * 4); a.heavy = (int32_t *)p;
-  const int64_t nch = (int64_t)hchunk_v.size();
-  ok &= ok && alloc(&p, (int64_t)hchunk_off.size() * 8); a.hchunk_off = (int64_t *)p;
-  ok &= ok && alloc(&p, std::max<int64_t>(nch, 1) * 4); a.hchunk_v = (int32_t *)p;
-  ok &= ok && alloc(&p, std::max<int64_t>(nch, 1) * 8); a.hchunk_e0 = (int64_t *)p;
-  ok &= ok && alloc(&p, std::max<int64_t>(nch, 1) * 8); a.hchunk_e1 = (int64_t *)p;
-  ok &= ok && alloc(&p, (int64_t)hfirst.size() * 4); a.hfirst = (int32_t *)p;
-  ok &= ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 32 * 8); a.hacc = (double *)p;
-  ok &= ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 4); a.hmask = (uint32_t *)p;
-  ok &= ok && alloc(&p, (int64_t)std::max<size_t>(P->h_batches.size(), 1) * sizeof(Batch)); a.batches = (Batch *)p;
-  ok &= ok && alloc(&p, (int64_t)std::max<size_t>(slots.size(), 1) * sizeof(Slot)); a.slots = (Slot *)p;
-  ok &= ok && alloc(&p, (int64_t)std::max<size_t>(masks.size(), 1) * 4); a.masks = (uint32_t *)p;
-  if (!ok) return bail(BCGPU_ENOMEM, "cudaMalloc of the batched workspace failed");
-  cudaError_t e = cudaSuccess;
-  e = cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), stream);
+  // tables
+  auto upload = [&](const void **dst, const void *src, int64_t bytes) -> bool {
+    if (!alloc(&p, bytes)) return false;
+    *dst = p;
+    return bytes == 0 || cudaMemcpyAsync(p, src, (size_t)bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess;
+  };
+  ok = ok && upload((const void **)&a.hvo, hvo.data(), (int64_t)hvo.size() * 8);
+  ok = ok && upload((const void **)&a.hrow, hrow.data(), (int64_t)hrow.size() * 8);
+  ok = ok && upload((const void **)&a.hsplit, hsplit.data(), (int64_t)hsplit.size() * 8);
+  ok = ok && upload((const void **)&a.hcol, hcol.data(), (int64_t)hcol.size() * 4);
+  ok = ok && upload((const void **)&a.hk, hk.data(), (int64_t)hk.size() * 4);
+  ok = ok && upload((const void **)&a.hcid, hcid.data(), (int64_t)hcid.size() * 4);
+  ok = ok && upload((const void **)&a.n_plain, B->n_plain, (int64_t)B->n_bcc * 4);
+  ok = ok && upload((const void **)&a.chain_off, B->chain_off, (int64_t)(B->n_bcc + 1) * 8);
+  ok = ok && upload((const void **)&a.cpre_off, cpre_off.data(), (int64_t)cpre_off.size() * 8);
+  ok = ok && upload((const void **)&a.cpre, cpre.data(), (int64_t)cpre.size() * 8);
+  ok = ok && upload((const void **)&a.heavy_off, heavy_off.data(), (int64_t)heavy_off.size() * 8);
+  ok = ok && upload((const void **)&a.heavy, heavy.data(), (int64_t)heavy.size() * 4);
+  ok = ok && upload((const void **)&a.hchunk_off, hchunk_off.data(), (int64_t)hchunk_off.size() * 8);
+  ok = ok && upload((const void **)&a.hchunk_v, hchunk_v.data(), nch * 4);
+  ok = ok && upload((const void **)&a.hchunk_e0, hchunk_e0.data(), nch * 8);
+  ok = ok && upload((const void **)&a.hchunk_e1, hchunk_e1.data(), nch * 8);
+  ok = ok && upload((const void **)&a.hfirst, hfirst.data(), (int64_t)hfirst.size() * 4);
+  ok = ok && upload((const void **)&a.batches, P->h_batches.data(), (int64_t)P->h_batches.size() * (int64_t)sizeof(Batch));
+  ok = ok && upload((const void **)&a.slots, slots.data(), (int64_t)slots.size() * (int64_t)sizeof(Slot));
+  ok = ok && upload((const void **)&a.seeds, seeds.data(), (int64_t)seeds.size() * (int64_t)sizeof(Seed));
+  ok = ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 32 * 8); a.hacc = (double *)p;
+  ok = ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 4); a.hmask = (uint32_t *)p;
+  if (!ok) return bail(BCGPU_ENOMEM, "cudaMalloc or upload of the batched workspace failed");
+  cudaError_t e = cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(a.redo, 0, (size_t)std::max<int64_t>(P->n_batches, 1) * 4, stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)a.heavy_off, heavy_off.data(), heavy_off.size() * 8, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && !heavy.empty()) e = cudaMemcpyAsync((void *)a.heavy, heavy.data(), heavy.size() * 4, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)a.hchunk_off, hchunk_off.data(), hchunk_off.size() * 8, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && nch) e = cudaMemcpyAsync((void *)a.hchunk_v, hchunk_v.data(), nch * 4, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && nch) e = cudaMemcpyAsync((void *)a.hchunk_e0, hchunk_e0.data(), nch * 8, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && nch) e = cudaMemcpyAsync((void *)a.hchunk_e1, hchunk_e1.data(), nch * 8, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)a.hfirst, hfirst.data(), hfirst.size() * 4, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && !P->h_batches.empty())
-    e = cudaMemcpyAsync((void *)a.batches, P->h_batches.data(), P->h_batches.size() * sizeof(Batch), cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && !slots.empty())
-    e = cudaMemcpyAsync((void *)a.slots, slots.data(), slots.size() * sizeof(Slot), cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess && !masks.empty())
-    e = cudaMemcpyAsync((void *)a.masks, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
   P->h_slots = slots;
   P->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
   if (e != cudaSuccess) return bail(BCGPU_ECUDA, std::string("batched upload: ") + cudaGetErrorString(e));
-  a.row = row; a.col = col; a.reach = reach; a.vtx_off = vtx_off;
+  a.reach = reach; a.vtx_off = vtx_off;
+  a.chain_start = chain_start; a.chain_len = chain_len; a.chain_l = chain_l; a.chain_r = chain_r;
   a.n_cap = P->n_cap; a.W = W; a.tcap = tcap; a.bc = bc; a.err = err;
   a.rescale_exp = cfg.rescale_exp > 0 ? cfg.rescale_exp : 900;
 
@@ -1151,10 +1281,7 @@ void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std:
   for (int64_t bi = begin; bi < end; ++bi) {
     const Batch &bt = p->h_batches[bi];
     const int64_t vo = p->h_vtx_off[bt.bcc];
-    for (int32_t i = 0; i < bt.nslots; ++i) {
-      const Slot &s = p->h_slots[bt.slot_off + i];
-      if (s.kind == kOwn || s.kind == kChain) out.push_back(vo + s.src);
-    }
+    for (int32_t i = 0; i < bt.nslots; ++i) out.push_back(vo + p->h_slots[bt.slot_off + i].src);
   }
 }
 

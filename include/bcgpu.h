@@ -51,16 +51,8 @@ typedef struct bc_opts {
   int64_t workspace_limit; /* device bytes the context may hold; 0 = 80% of free memory */
   int32_t rescale_exp;   /* BATCHED: rescale a level's path counts above 2^rescale_exp; 0 = 900.
                             Lower values only exercise the scaling path (tests). */
-  int32_t chain_sources; /* BATCHED: how degree-2 chain vertices act as sources: BCGPU_CHAINS_* */
+  int32_t pad_;
 } bc_opts;
-
-/* BATCHED treatment of chain-vertex sources. MERGE: their rows are merged
- * from the chain endpoints' columns (the reference's ear postprocessing,
- * Codes/begin_gpupgm.cu); BFS: they are ordinary bitmask-BFS slots;
- * AUTO: the library's choice, currently BFS (a pass's forward work is per
- * vertex row, not per slot, so the merge saves little BFS work while it adds
- * forward-only endpoint slots and a merge phase). */
-enum { BCGPU_CHAINS_AUTO = 0, BCGPU_CHAINS_MERGE = 1, BCGPU_CHAINS_BFS = 2 };
 
 typedef struct bc_ctx bc_ctx;
 

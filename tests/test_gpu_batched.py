@@ -11,18 +11,16 @@ pytestmark = pytest.mark.gpu
 TOL = {"fp64": 1e-12, "fp32c": 1e-6}
 
 
-def ctx_for(delta, width=0, rescale_exp=0, chains="auto"):
+def ctx_for(delta, width=0, rescale_exp=0):
     P = pkg()
-    cs = {"auto": P.CHAINS_AUTO, "merge": P.CHAINS_MERGE, "bfs": P.CHAINS_BFS}[chains]
     return P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C,
-                     batch_width=width, rescale_exp=rescale_exp, chain_sources=cs)
+                     batch_width=width, rescale_exp=rescale_exp)
 
 
-@pytest.fixture(scope="module", params=["fp64-merge", "fp32c-merge", "fp64-bfs", "fp32c-bfs"])
+@pytest.fixture(scope="module", params=["fp64", "fp32c"])
 def bctx(request):
-    delta, chains = request.param.split("-")
-    c = ctx_for(delta, chains=chains)
-    c.tol = TOL[delta]
+    c = ctx_for(request.param)
+    c.tol = TOL[request.param]
     yield c
     c.close()
 
@@ -64,8 +62,8 @@ def test_batched_widths(width):
     """Several passes per BCC (width << sources): owners return as helper BFS
     slots, chains split across passes."""
     n, u, v = graphs().gen_small(2)
-    for delta, chains in (("fp64", "merge"), ("fp32c", "merge"), ("fp32c", "bfs")):
-        c = ctx_for(delta, width, chains=chains)
+    for delta in ("fp64", "fp32c"):
+        c = ctx_for(delta, width)
         got, st = c.run(decomp(n, u, v))
         assert st["batch_width"] == width
         assert rel_err(got, oracle_bc(n, u, v)) < TOL[delta]
