@@ -187,6 +187,39 @@ def traffic_per_source(mode, workload):
     return (float(m.group(1)), f"profiles/{name}") if m else (None, None)
 
 
+def plain_sample(P, d, device, stream, waves, batched_gteps):
+    """Times the plain FP64 schedule (one source per CTA) on `waves` full
+    waves of its work items, taken from two places in the largest BCC's item
+    list, with CUDA events; returns its TEPS and the batched/plain ratio."""
+    import torch
+    pctx = P.Context(mode=P.MODE_PLAIN, device=device, stream=stream.cuda_stream)
+    pplan = pctx.plan(d)
+    slots = pplan.concurrency
+    per = max(1, waves * slots // 2)
+    n = pplan.n_units
+    picks = [(max(0, int(f * n) - per // 2), max(0, int(f * n) - per // 2) + per) for f in (0.25, 0.75)]
+    picks = [(a, min(n, b)) for a, b in picks]
+    pplan.run(picks[0][0], min(picks[0][1], picks[0][0] + slots), stats=False)  # warm-up wave
+    torch.cuda.synchronize()
+    ms = teps = src = 0.0
+    for a, b in picks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pplan.run(a, b, stats=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        w = pplan.unit_work(a, b)
+        src += w[0]
+        teps += w[1]
+    pplan.close()
+    pctx.close()
+    g = teps / (ms * 1e-3) / 1e9
+    return {"value": g, "unit": "GTEPS", "dtype": "f64", "items": sum(b - a for a, b in picks), "sources": int(src),
+            "ms": ms, "resident_ctas": slots, "batched_over_plain": batched_gteps / g,
+            "sample": f"{waves} full waves of plain work items ({slots} resident CTAs) at 25% and 75% of the item list"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -233,6 +266,9 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-waves", type=int, default=2,
+                    help="batched runs: also time the plain FP64 schedule on this many full waves of its work "
+                         "items (one item per resident CTA), the denominator of batched vs plain (0 = skip)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
     args = ap.parse_args()
@@ -349,6 +385,10 @@ def main():
         if rank == 0:
             print(f"combined BC over {world} ranks: sum {float(total.sum()):.6e}", file=sys.stderr)
 
+    plain = None
+    if rank == 0 and world == 1 and mode == P.MODE_BATCHED and args.plain_waves > 0:
+        plain = plain_sample(P, d, local, stream, args.plain_waves, value)
+
     cpu = None
     accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -376,6 +416,7 @@ def main():
                        "host_decomposition_s": round(host_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
+            "plain": plain,
             "gpu_launches": int(launches_per_unit * args.steps),
         }
         print(json.dumps(line), flush=True)

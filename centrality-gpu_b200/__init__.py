@@ -88,6 +88,7 @@ _SIGS = {
     "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
     "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p, _i64p]),
     "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "bc_plan_concurrency": (C.c_int, [C.c_void_p]),
     "bc_plan_unit_sources": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_int64]),
     "bc_plan_reset": (C.c_int, [C.c_void_p]),
     "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
@@ -309,6 +310,7 @@ class Plan:
         ctx._plans.add(self)
         self.n_units = lib().bc_plan_num_units(h)
         self.device_bytes = lib().bc_plan_device_bytes(h)
+        self.concurrency = lib().bc_plan_concurrency(h)
 
     def unit_work(self, begin=0, end=None):
         """(sources, TEPS arcs, vertex visits) of units [begin, end)."""

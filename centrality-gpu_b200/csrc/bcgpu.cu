@@ -423,6 +423,7 @@ extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, i
 }
 
 extern "C" int64_t bc_plan_device_bytes(const bc_plan *p) { return p ? p->device_bytes : 0; }
+extern "C" int bc_plan_concurrency(const bc_plan *p) { return !p ? 0 : p->bp ? 1 : p->grid; }
 
 extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t end, int64_t *out, int64_t cap) {
   if (!p) return -BCGPU_EINVAL;

@@ -92,6 +92,7 @@ struct Ctrl {
   int rescale;    // forward: some slot needs a rescale at this level
   int range_err;  // FP32 q left FP32's exponent range in this batch
   int pad;
+  unsigned long long found;  // forward: (core vertex, slot) pairs reached so far
 };
 
 struct Args {
@@ -239,60 +240,56 @@ struct Stretch {
   __device__ __forceinline__ Stretch flip() const { return Stretch{P, lo, hi, !rev}; }
 };
 
-// An end of a stretch for one slot: its level and where its path count and q
-// live; idx < 0 marks the slot's own source (level 0, one path).
+// An end of a stretch for one slot, as loaded: its level d, path count
+// sigma = s * 2^x and q = qs * 2^-x (qs only read when the stretch carries
+// the end's shortest paths). The slot's own source is {0, 0, 1, 0}.
 struct End {
-  int d;
-  int64_t idx;
+  int d, x;
+  double s, qs;
 };
-
-__device__ __forceinline__ double sig_of(const Args &a, const End &e, int b) {
-  return e.idx < 0 ? 1.0 : ldexp(__ldcg(a.sig + e.idx), __ldcg(a.X + (int64_t)b * (a.tcap + 2) + e.d));
-}
-template <typename QT>
-__device__ __forceinline__ double q_of(const Args &a, const End &e, int b) {
-  return ldexp((double)__ldcg(reinterpret_cast<const QT *>(a.q) + e.idx), -__ldcg(a.X + (int64_t)b * (a.tcap + 2) + e.d));
-}
+__device__ __forceinline__ End source_end() { return End{0, 0, 1.0, 0.0}; }
 
 // Dependency of stretch vertex i on the slot's source when i takes its
 // shortest paths from A (2i < D): the chain vertices beyond i on the A-fed
 // side each add reach+1; the last A-fed vertex either ties (shares its paths
 // with B: adds its reach+1 times sigma_A / (sigma_A + sigma_B)) or, when it is
 // the vertex next to B and B's shortest paths run through the stretch, passes
-// on sigma_A * q(B). i = -1 gives what A itself receives through the stretch.
-template <typename QT, bool kTail>
-__device__ __forceinline__ double fed_dep(const Args &a, const Stretch &s, int i, const End &A, const End &B, int b,
-                                          int D) {
+// on sigma_A * q(B) (kTail). i = -1 gives what A itself receives.
+template <bool kTail>
+__device__ __forceinline__ double fed_dep(const Stretch &s, int i, const End &A, const End &B, int D) {
   const int m = s.m();
   const int P = min(m - 1, D / 2);  // last vertex fed from A
-  if ((D & 1) == 0 && D / 2 <= m - 1) {
-    const double sa = sig_of(a, A, b), sb = sig_of(a, B, b);
-    return s.pre(P) - s.pre(i + 1) + sa / (sa + sb) * s.wt(P);
-  }
+  if ((D & 1) == 0 && D / 2 <= m - 1) return s.pre(P) - s.pre(i + 1) + s.wt(P) / (1.0 + ldexp(B.s / A.s, B.x - A.x));
   double v = s.pre(P + 1) - s.pre(i + 1);
-  if (kTail && P == m - 1 && B.d == A.d + m + 1) v += sig_of(a, A, b) * q_of<QT>(a, B, b);
+  if (kTail && P == m - 1 && B.d == A.d + m + 1) v += ldexp(A.s * B.qs, A.x - B.x);
   return v;
 }
 
-// Dependency of stretch vertex i (0 <= i < m) on the slot's source.
-template <typename QT>
-__device__ __forceinline__ double stretch_dep(const Args &a, const Stretch &s, int i, const End &A, const End &B,
-                                              int b) {
+// Dependency of stretch vertex i (0 <= i < m) on the slot's source (out of
+// line: only the rare slots whose source sits on the chain take this path).
+__device__ __noinline__ double stretch_dep(const Stretch &s, int i, const End &A, const End &B) {
   const int m = s.m();
   const int D = B.d + m - A.d - 1;  // vertex i is fed from A iff 2i <= D, from B iff 2i >= D
-  if (2 * i < D) return fed_dep<QT, true>(a, s, i, A, B, b, D);
-  if (2 * i > D) return fed_dep<QT, true>(a, s.flip(), m - 1 - i, B, A, b, A.d + m - B.d - 1);
+  if (2 * i < D) return fed_dep<true>(s, i, A, B, D);
+  if (2 * i > D) return fed_dep<true>(s.flip(), m - 1 - i, B, A, A.d + m - B.d - 1);
   return 0.0;  // fed from both ends: no successor on the chain
+}
+
+// Whether what A receives from the stretch needs B's path count (the vertex
+// where the two sides meet ties).
+__device__ __forceinline__ bool end_needs_sigma(int m, int dA, int dB) {
+  const int D = dB + m - dA - 1;
+  return m > 0 && D >= 0 && (D & 1) == 0 && D / 2 <= m - 1;
 }
 
 // What end A receives from the stretch's vertices (its neighbour on the
 // stretch is its successor iff that neighbour is fed from A: D >= 0), less
 // the term through B (sigma_A * q(B) when B's paths run through the
 // stretch), which the backward sweep adds as a successor arc.
-__device__ __forceinline__ double end_dep(const Args &a, const Stretch &s, const End &A, const End &B, int b) {
+__device__ __forceinline__ double end_dep(const Stretch &s, const End &A, const End &B) {
   const int D = B.d + s.m() - A.d - 1;
   if (s.m() == 0 || D < 0) return 0.0;
-  return fed_dep<double, false>(a, s, -1, A, B, b, D);
+  return fed_dep<false>(s, -1, A, B, D);
 }
 
 // ============================================================== forward ====
@@ -425,10 +422,11 @@ __device__ __forceinline__ double acc_value(const WarpScratch &S, int k, int lan
   return (double)c.x + (double)c.y;
 }
 
-// Stores the result of one (vertex, word) of the forward step.
-__device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, int lane,
-                                            double acc) {
-  if (!newm) return;
+// Stores the result of one (vertex, word) of the forward step; returns the
+// number of slots that reached the vertex (uniform over the warp).
+__device__ __forceinline__ int finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, int lane,
+                                           double acc) {
+  if (!newm) return 0;
   const int64_t idx = ((int64_t)v * a.W + w) * 32 + lane;
   if ((newm >> lane) & 1u) {
     a.d[idx] = t + 1;
@@ -445,6 +443,7 @@ __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int
     atomicMin(a.lmin + v, t + 1);
     atomicMax(a.lmax + v, t + 1);
   }
+  return __popc(newm);
 }
 
 // ============================================================== backward ===
@@ -452,16 +451,22 @@ __device__ __forceinline__ void finish_pull(const Args &a, int32_t v, int w, int
 // What core vertex v receives from the vertices of its chains, for the 32
 // slots of word w (the part that needs only forward results): cdep[v][w][.].
 // Chain-arc data are loaded lane-parallel, 32 arcs at a time; the far ends'
-// levels four arcs at a time.
+// levels four arcs at a time, then the path counts the ties need.
+constexpr int kArcGroup = 4;
 __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int nslots, int32_t v, int w, int64_t c0,
                                          int64_t c1, int lane) {
   const int W = a.W;
   const int b = w * 32 + lane;
   const bool live = b < nslots;
   const int64_t iv = ((int64_t)v * W + w) * 32 + lane;
-  const End A{live ? __ldcg(a.d + iv) : 0, iv};
+  const int32_t *xb = a.X + (int64_t)b * (a.tcap + 2);
+  End A{0, 0, 1.0, 0.0};
   Slot sl{0, -1, 0, 0};
-  if (live) sl = slots[b];
+  if (live) {
+    A.d = __ldcg(a.d + iv);
+    sl = slots[b];
+  }
+  bool have_a = false;  // A's path count, loaded on the first tie
   double sum = 0.0;
   for (int64_t base = c0; base < c1; base += 32) {
     const int64_t e = base + lane;
@@ -474,29 +479,44 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
       poff = ldg(a.cpre_off + (cid >> 1));
     }
     const int cnt = (int)min((int64_t)32, c1 - base);
-    for (int j0 = 0; j0 < cnt; j0 += 4) {
-      int32_t uj[4], cj[4], kj[4], dB[4];
-      int64_t pj[4];
+    for (int j0 = 0; j0 < cnt; j0 += kArcGroup) {
+      End B[kArcGroup];
+      Stretch st[kArcGroup];
+      int64_t ib[kArcGroup];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        uj[r] = __shfl_sync(0xffffffffu, u, (j0 + r) & 31);
-        cj[r] = __shfl_sync(0xffffffffu, cid, (j0 + r) & 31);
-        kj[r] = __shfl_sync(0xffffffffu, k, (j0 + r) & 31);
-        pj[r] = __shfl_sync(0xffffffffu, poff, (j0 + r) & 31);
-        dB[r] = (live && j0 + r < cnt) ? __ldcg(a.d + ((int64_t)uj[r] * W + w) * 32 + lane) : 0;
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (!live || j0 + r >= cnt) continue;
-        const bool right = cj[r] & 1;
-        End B{dB[r], ((int64_t)uj[r] * W + w) * 32 + lane};
-        Stretch st{a.cpre + pj[r], 0, kj[r], right};
-        if (sl.chain == (cj[r] >> 1)) {  // the source sits on this chain: the stretch ends at it
-          B = End{0, -1};
-          st = right ? Stretch{a.cpre + pj[r], sl.pos + 1, kj[r], true} : Stretch{a.cpre + pj[r], 0, sl.pos, false};
+      for (int r = 0; r < kArcGroup; ++r) {
+        const int j = (j0 + r) & 31;
+        const int32_t uj = __shfl_sync(0xffffffffu, u, j);
+        const int32_t cj = __shfl_sync(0xffffffffu, cid, j);
+        const int32_t kj = __shfl_sync(0xffffffffu, k, j);
+        const int64_t pj = __shfl_sync(0xffffffffu, poff, j);
+        ib[r] = ((int64_t)uj * W + w) * 32 + lane;
+        B[r] = End{(live && j0 + r < cnt) ? __ldcg(a.d + ib[r]) : 0, 0, 1.0, 0.0};
+        const bool right = cj & 1;
+        st[r] = Stretch{a.cpre + pj, 0, kj, right};
+        if (sl.chain == (cj >> 1)) {  // the source sits on this chain: the stretch ends at it
+          ib[r] = -1;
+          st[r] = right ? Stretch{a.cpre + pj, sl.pos + 1, kj, true} : Stretch{a.cpre + pj, 0, sl.pos, false};
         }
-        sum += end_dep(a, st, A, B, b);
       }
+#pragma unroll
+      for (int r = 0; r < kArcGroup; ++r) {  // path counts of the far ends where the middle vertex ties
+        if (ib[r] < 0) B[r] = source_end();
+        if (live && j0 + r < cnt && end_needs_sigma(st[r].m(), A.d, B[r].d)) {
+          if (ib[r] >= 0) {
+            B[r].s = __ldcg(a.sig + ib[r]);
+            B[r].x = __ldcg(xb + B[r].d);
+          }
+          if (!have_a) {
+            A.s = __ldcg(a.sig + iv);
+            A.x = __ldcg(xb + A.d);
+            have_a = true;
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kArcGroup; ++r)
+        if (live && j0 + r < cnt) sum += end_dep(st[r], A, B[r]);
     }
   }
   a.cdep[iv] = sum;
@@ -594,6 +614,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       a.ctrl->more = 0;
       a.ctrl->rescale = 0;
       a.ctrl->range_err = 0;
+      a.ctrl->found = 0;
     }
     grid_sync(a);
     for (int64_t b = gtid; b < bt.nslots; b += gthreads) {  // core sources at level 0
@@ -606,13 +627,16 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       atomicOr(a.seen + (int64_t)s.src * W + (b >> 5), 1u << (b & 31));
       atomicMin(a.lmin + s.src, 0);
       atomicMax(a.lmax + s.src, 0);
+      atomicAdd(&a.ctrl->found, 1ull);
     }
     grid_sync(a);
     PHASE_MARK(0);
 
     // ---- forward: levels t -> t+1
     int t = 0, tlast = 0;
+    const unsigned long long all_found = (unsigned long long)n * (unsigned long long)bt.nslots;
     while (true) {
+      unsigned long long nf = 0;  // pairs this warp found on this level
       if (t + 1 > a.tcap) { set_err(a.err, kDevWorkspace); break; }
       const uint32_t *lmt = a.lm + (int64_t)t * a.n_cap * W;
       // heavy rows: chunks of their arcs, one CTA per (chunk, half); partials
@@ -685,7 +709,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             for (int k = 0; k < kHalf; ++k) {
               if (k >= nw) continue;
               const uint32_t m = warp_or(any[k]);
-              finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
+              nf += finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
               any[k] = m;
             }
 #pragma unroll
@@ -702,6 +726,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           }
         }
       }
+      if (lane == 0 && nf) atomicAdd(&a.ctrl->found, nf);
+      nf = 0;
       grid_sync(a);
       PHASE_MARK(1);
       PHASE_COUNT(16);
@@ -717,8 +743,9 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             acc += __ldcg(a.hacc + ((hc0 + c) * W + w) * 32 + lane);
             m |= __ldcg(a.hmask + (hc0 + c) * W + w);
           }
-          finish_pull(a, v, w, t, m, lane, acc);
+          nf += finish_pull(a, v, w, t, m, lane, acc);
         }
+        if (lane == 0 && nf) atomicAdd(&a.ctrl->found, nf);
         grid_sync(a);
         PHASE_MARK(2);
       }
@@ -738,6 +765,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             atomicMin(a.lmin + s.v, t + 1);
             atomicMax(a.lmax + s.v, t + 1);
             a.ctrl->more = 1;
+            atomicAdd(&a.ctrl->found, 1ull);
           } else if (a.d[idx] == t + 1) {
             a.sig[idx] += one;  // reached on this level from the core as well
           }
@@ -746,6 +774,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       }
       const int more = *(volatile int *)&a.ctrl->more;
       const int resc = *(volatile int *)&a.ctrl->rescale;
+      const unsigned long long found = *(volatile unsigned long long *)&a.ctrl->found;
       // base exponent of level t+1; rescale it when some slot's counts passed 2^rescale_exp
       for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) {
         const int re = __ldcg(a.rexp + b);
@@ -772,7 +801,10 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       }
       if (more) tlast = t + 1;
       if (cta_failed(a)) break;
-      // level t+2 needs a non-empty level within the longest arc, or a seed
+      // done when every slot has reached every core vertex (later seeds then
+      // reach seen vertices only); else level t+2 needs a non-empty level
+      // within the longest arc, or a seed
+      if (found >= all_found) break;
       if (t + 1 - tlast > bt.kmax && t + 2 > bt.max_seed) break;
       ++t;
       for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 1) * a.n_cap * W + i] = 0;
@@ -799,7 +831,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     }
     PHASE_MARK(4);
 
-    // ---- backward: lev = tlast .. 1
+    // ---- backward: lev = tlast .. 1 (level tlast+1 is empty and not cleared:
+    // the deepest level has no unit-arc successors)
     for (int lev = tlast; lev >= 1; --lev) {
       const uint32_t *lm_here = a.lm + (int64_t)lev * a.n_cap * W;
       const uint32_t *lm_next = a.lm + (int64_t)(lev + 1) * a.n_cap * W;
@@ -826,7 +859,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < min(s1, sp)) row_pass<QT, kComp, 0>(a, S, lm_next, q, s0, min(s1, sp), w0, nw, act, any, lane, lev + 1);
+          if (lev < tlast && s0 < min(s1, sp))
+            row_pass<QT, kComp, 0>(a, S, lm_next, q, s0, min(s1, sp), w0, nw, act, any, lane, lev + 1);
           if (max(s0, sp) < s1) row_pass<QT, kComp, 2>(a, S, a.lm, q, max(s0, sp), s1, w0, nw, act, any, lane, lev + 1, tlast);
         }
         __syncthreads();
@@ -869,7 +903,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             if (!a_any) continue;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-            if (e0 < sp) row_pass<QT, kComp, 0>(a, S, lm_next, q, e0, sp, w0, nw, act, any, lane, lev + 1);
+            if (lev < tlast && e0 < sp) row_pass<QT, kComp, 0>(a, S, lm_next, q, e0, sp, w0, nw, act, any, lane, lev + 1);
             if (sp < e1) row_pass<QT, kComp, 2>(a, S, a.lm, q, sp, e1, w0, nw, act, any, lane, lev + 1, tlast);
 #pragma unroll
             for (int k = 0; k < kHalf; ++k)
@@ -910,17 +944,72 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         const int32_t L = a.chain_l[c], R = a.chain_r[c], cs = a.chain_start[c], k = a.chain_len[c];
         const double *P = a.cpre + a.cpre_off[c];
         const int64_t iL = ((int64_t)L * W + w) * 32 + lane, iR = ((int64_t)R * W + w) * 32 + lane;
-        const End eL{live ? __ldcg(a.d + iL) : 0, iL}, eR{live ? __ldcg(a.d + iR) : 0, iR};
+        End eL{0, 0, 1.0, 0.0}, eR{0, 0, 1.0, 0.0};
         Slot sl{0, -1, 0, 0};
-        if (live) sl = slots[b];
-        const int on = sl.chain == c ? sl.pos : -1;
+        int on = -1;
+        if (live) {  // the ends' levels, then only the path counts / q the closed forms use
+          eL.d = __ldcg(a.d + iL);
+          eR.d = __ldcg(a.d + iR);
+          sl = slots[b];
+          on = sl.chain == c ? sl.pos : -1;
+          // stretches: [L, R] or, with the source on the chain, [L, source] and [source, R]
+          const int mL = on < 0 ? k : on, dBL = on < 0 ? eR.d : 0;   // stretch seen from L
+          const int mR = on < 0 ? k : k - 1 - on, dBR = on < 0 ? eL.d : 0;  // stretch seen from R
+          const int DL = dBL + mL - eL.d - 1, DR = dBR + mR - eR.d - 1;
+          const bool tieL = mL > 0 && DL >= 0 && (DL & 1) == 0 && DL / 2 <= mL - 1;
+          const bool tieR = mR > 0 && DR >= 0 && (DR & 1) == 0 && DR / 2 <= mR - 1;
+          // B's paths through the stretch: R fed via the chain from L, or L from R
+          const bool viaL = on < 0 && eR.d == eL.d + k + 1, viaR = on < 0 && eL.d == eR.d + k + 1;
+          const bool srcL = on >= 0 && eL.d == on + 1, srcR = on >= 0 && eR.d == k - on;  // fed from the source
+          const int32_t *xb = a.X + (int64_t)b * (a.tcap + 2);
+          const QT *qq = reinterpret_cast<const QT *>(a.q);
+          if (tieL || tieR || viaL || viaR) {
+            eL.s = __ldcg(a.sig + iL);
+            eL.x = __ldcg(xb + eL.d);
+            eR.s = __ldcg(a.sig + iR);
+            eR.x = __ldcg(xb + eR.d);
+          }
+          if (viaR || srcL) {
+            eL.qs = (double)__ldcg(qq + iL);
+            if (!(tieL || tieR || viaL || viaR)) eL.x = __ldcg(xb + eL.d);
+          }
+          if (viaL || srcR) {
+            eR.qs = (double)__ldcg(qq + iR);
+            if (!(tieL || tieR || viaL || viaR)) eR.x = __ldcg(xb + eR.d);
+          }
+        }
         const double wsrc = live ? (double)rch[sl.src] + 1.0 : 0.0;
+        // Source off the chain (the common case), in prefix sums from L:
+        // vertex j is fed from L iff 2j <= D; a tie vertex t = D/2 shares its
+        // reach+1 between the sides in proportion to sigma_L, sigma_R; else
+        // the L-fed vertices end at pl, and the far end's q enters when the
+        // chain carries its shortest paths.
+        int D = 0, tv = -1, pl = -1;
+        double fL = 0.0, fR = 0.0;  // L-side and R-side constants
+        if (live && on < 0) {
+          D = eR.d + k - eL.d - 1;
+          if (D >= 0 && (D & 1) == 0 && D / 2 <= k - 1) {
+            tv = D / 2;
+            const double w = P[tv + 1] - P[tv];
+            fL = P[tv] + w / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
+            fR = -P[tv + 1] + w / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
+          } else {
+            pl = D >= 0 ? min(k - 1, D / 2) : -1;
+            fL = P[pl + 1] + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
+            fR = -P[pl + 1] + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
+          }
+        }
         for (int j = 0; j < k; ++j) {
           double dep = 0.0;
           if (live) {
-            if (on < 0) dep = stretch_dep<QT>(a, Stretch{P, 0, k, false}, j, eL, eR, b);
-            else if (j < on) dep = stretch_dep<QT>(a, Stretch{P, 0, on, false}, j, eL, End{0, -1}, b);
-            else if (j > on) dep = stretch_dep<QT>(a, Stretch{P, on + 1, k, false}, j - on - 1, End{0, -1}, eR, b);
+            if (on < 0) {
+              const bool from_l = tv >= 0 ? j < tv : j <= pl;
+              if (j != tv) dep = from_l ? fL - P[j + 1] : P[j] + fR;
+            } else if (j < on) {
+              dep = stretch_dep(Stretch{P, 0, on, false}, j, eL, source_end());
+            } else if (j > on) {
+              dep = stretch_dep(Stretch{P, on + 1, k, false}, j - on - 1, source_end(), eR);
+            }
           }
           const double tot = warp_sum(dep * wsrc);
           if (lane == 0) a.bcpart[(int64_t)(cs + j) * W + w] = tot;

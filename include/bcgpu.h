@@ -184,6 +184,10 @@ int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *
 int64_t bc_plan_unit_sources(const bc_plan *plan, int64_t begin, int64_t end, int64_t *out, int64_t cap);
 /* Device buffers the plan consumes (for roofline accounting). */
 int64_t bc_plan_device_bytes(const bc_plan *plan);
+/* Work units that run at once: PLAIN, the resident CTAs (one item each);
+ * BATCHED, 1 (one pass at a time over the whole GPU). No reference
+ * counterpart: the reference launches one source at a time. */
+int bc_plan_concurrency(const bc_plan *plan);
 int bc_plan_reset(bc_plan *plan);
 /* Enqueues units [begin, end) on the context's stream; asynchronous unless
  * stats is non-NULL (then synchronises and fills it). */
