@@ -63,7 +63,7 @@ constexpr int kWarpsPerCta = kThreads / 32;
 constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs
 constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr long long kSpinLimit = 1ll << 28;  // ~1 min of polling before giving up
-constexpr int kHalf = 8;           // words per pass over a vertex row
+constexpr int kHalf = 4;           // words per pass over a vertex row
 
 // One source of a pass. chain < 0: the core vertex src (level 0). Otherwise
 // src is the chain vertex at position pos of chain `chain` (global index).
@@ -88,8 +88,8 @@ struct Batch {
 struct Ctrl {
   unsigned int bar_count;
   unsigned int bar_gen;
-  int more;       // forward: some slot found a new vertex this level
-  int rescale;    // forward: some slot needs a rescale at this level
+  int more[2];    // forward, by level parity: some slot found a new vertex on the level
+  int rescale[2]; // forward, by level parity: some slot needs a rescale on the level
   int range_err;  // FP32 q left FP32's exponent range in this batch
   int pad;
   unsigned long long found;  // forward: (core vertex, slot) pairs reached so far
@@ -433,13 +433,13 @@ __device__ __forceinline__ int finish_pull(const Args &a, int32_t v, int w, int 
     a.sig[idx] = acc;
     if (acc > ldexp(1.0, a.rescale_exp)) {
       atomicMax(a.rexp + w * 32 + lane, ilogb(acc));
-      a.ctrl->rescale = 1;
+      a.ctrl->rescale[t & 1] = 1;
     }
   }
   if (lane == 0) {
     a.lm[((int64_t)(t + 1) * a.n_cap + v) * a.W + w] = newm;
     a.seen[(int64_t)v * a.W + w] |= newm;
-    a.ctrl->more = 1;
+    a.ctrl->more[t & 1] = 1;
     atomicMin(a.lmin + v, t + 1);
     atomicMax(a.lmax + v, t + 1);
   }
@@ -548,11 +548,13 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
   if (lane == 0) a.bcpart[(int64_t)v * W + w] += contrib;
 }
 
-// Next block of 32 vertices for this warp from the phase's work counter.
+// Vertex blocks of a phase: each warp's first block is its own index, later
+// ones come from the phase's work counter (no atomics at all when the level
+// has no more blocks than the grid has warps).
 __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
   int b = 0;
   if (lane == 0) b = atomicAdd(counter, 1);
-  return __shfl_sync(0xffffffffu, b, 0);
+  return nwarps() + __shfl_sync(0xffffffffu, b, 0);
 }
 
 }  // namespace
@@ -592,7 +594,12 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     const int32_t *hfst = a.hfirst + a.heavy_off[bt.bcc] + bt.bcc;  // nheavy+1 entries per BCC
     const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nblk = ((int64_t)n + 31) / 32;  // vertex blocks of 32 (lane l takes vertex blk + l*nblk)
+    // vertex blocks of bs <= 32 (lane l < bs takes vertex blk + l*nblk): whole
+    // 32-vertex blocks on large cores, smaller ones on small cores so that
+    // every warp of the grid gets work on a level
+    const int64_t bs_want = ((int64_t)n + nwarps() * 8 - 1) / (nwarps() * 8);
+    const int bs = bs_want >= 32 ? 32 : bs_want < 1 ? 1 : (int)bs_want;
+    const int64_t nblk = ((int64_t)n + bs - 1) / bs;
     const int halves = (wpad + kHalf - 1) / kHalf;
 
     // ---- init: seen = slots beyond the batch, partials, level-0/1 masks, X, rexp, work counters
@@ -611,8 +618,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     }
     for (int64_t i = gtid; i < 2 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
     if (gtid == 0) {
-      a.ctrl->more = 0;
-      a.ctrl->rescale = 0;
+      a.ctrl->more[0] = a.ctrl->more[1] = 0;
+      a.ctrl->rescale[0] = a.ctrl->rescale[1] = 0;
       a.ctrl->range_err = 0;
       a.ctrl->found = 0;
     }
@@ -639,6 +646,12 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       unsigned long long nf = 0;  // pairs this warp found on this level
       if (t + 1 > a.tcap) { set_err(a.err, kDevWorkspace); break; }
       const uint32_t *lmt = a.lm + (int64_t)t * a.n_cap * W;
+      // the next level's flags and masks start clear (nothing reads them on this level)
+      if (gtid == 0) {
+        a.ctrl->more[(t + 1) & 1] = 0;
+        a.ctrl->rescale[(t + 1) & 1] = 0;
+      }
+      for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 2) * a.n_cap * W + i] = 0;
       // heavy rows: chunks of their arcs, one CTA per (chunk, half); partials
       // are combined across the CTA's warps, then across chunks after the barrier
       for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
@@ -676,11 +689,11 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         __syncthreads();
       }
       // light rows: dynamic blocks of 32 vertices, lane-parallel activity check
-      for (int64_t vb = next_block(a.wq + t, lane); vb < nblk; vb = next_block(a.wq + t, lane)) {
+      for (int64_t vb = gwarp(); vb < nblk; vb = next_block(a.wq + t, lane)) {
         const int64_t vl = vb + (int64_t)lane * nblk;
         int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
-        if (vl < n) {
+        if (lane < bs && vl < n) {
           e0l = HR[vl];
           e1l = HR[vl + 1];
           spl = HS[vl];
@@ -764,7 +777,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             atomicOr(a.lm + ((int64_t)(t + 1) * a.n_cap + s.v) * W + w, bit);
             atomicMin(a.lmin + s.v, t + 1);
             atomicMax(a.lmax + s.v, t + 1);
-            a.ctrl->more = 1;
+            a.ctrl->more[t & 1] = 1;
             atomicAdd(&a.ctrl->found, 1ull);
           } else if (a.d[idx] == t + 1) {
             a.sig[idx] += one;  // reached on this level from the core as well
@@ -772,8 +785,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         }
         grid_sync(a);
       }
-      const int more = *(volatile int *)&a.ctrl->more;
-      const int resc = *(volatile int *)&a.ctrl->rescale;
+      const int more = *(volatile int *)&a.ctrl->more[t & 1];
+      const int resc = *(volatile int *)&a.ctrl->rescale[t & 1];
       const unsigned long long found = *(volatile unsigned long long *)&a.ctrl->found;
       // base exponent of level t+1; rescale it when some slot's counts passed 2^rescale_exp
       for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) {
@@ -792,12 +805,10 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           }
         }
       }
-      grid_sync(a);  // everyone has read more/rescale/rexp
-      if (resc)
+      grid_sync(a);  // level t+1's base and counts are final; everyone has read the flags
+      if (resc) {
         for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) a.rexp[b] = INT_MIN;
-      if (gtid == 0) {
-        a.ctrl->more = 0;
-        a.ctrl->rescale = 0;
+        grid_sync(a);
       }
       if (more) tlast = t + 1;
       if (cta_failed(a)) break;
@@ -807,8 +818,6 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       if (found >= all_found) break;
       if (t + 1 - tlast > bt.kmax && t + 2 > bt.max_seed) break;
       ++t;
-      for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 1) * a.n_cap * W + i] = 0;
-      grid_sync(a);
       PHASE_MARK(3);
     }
     PHASE_MARK(3);
@@ -872,11 +881,11 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         __syncthreads();
       }
       const int wqi = a.tcap + 3 + lev;
-      for (int64_t vb = next_block(a.wq + wqi, lane); vb < nblk; vb = next_block(a.wq + wqi, lane)) {
+      for (int64_t vb = gwarp(); vb < nblk; vb = next_block(a.wq + wqi, lane)) {
         const int64_t vl = vb + (int64_t)lane * nblk;
         int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
-        if (vl < n && lev >= __ldcg(a.lmin + vl) && lev <= __ldcg(a.lmax + vl)) {
+        if (lane < bs && vl < n && lev >= __ldcg(a.lmin + vl) && lev <= __ldcg(a.lmax + vl)) {
           e0l = HR[vl];
           e1l = HR[vl + 1];
           spl = HS[vl];
