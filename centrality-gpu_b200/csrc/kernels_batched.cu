@@ -594,13 +594,16 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     const int32_t *hfst = a.hfirst + a.heavy_off[bt.bcc] + bt.bcc;  // nheavy+1 entries per BCC
     const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // vertex blocks of bs <= 32 (lane l < bs takes vertex blk + l*nblk): whole
-    // 32-vertex blocks on large cores, smaller ones on small cores so that
-    // every warp of the grid gets work on a level
-    const int64_t bs_want = ((int64_t)n + nwarps() * 8 - 1) / (nwarps() * 8);
+    // Warp tasks of the light rows: (vertex block, kHalf-word quarter of the
+    // row), so a row's quarters run on different warps. Blocks hold bs <= 32
+    // vertices (lane l < bs takes vertex blk + l*nblk): whole 32-vertex blocks
+    // on large cores, smaller ones on small cores so that every warp of the
+    // grid gets work on a level.
+    const int halves = wpad / kHalf;
+    const int64_t bs_want = ((int64_t)n * halves + nwarps() * 8 - 1) / (nwarps() * 8);
     const int bs = bs_want >= 32 ? 32 : bs_want < 1 ? 1 : (int)bs_want;
     const int64_t nblk = ((int64_t)n + bs - 1) / bs;
-    const int halves = (wpad + kHalf - 1) / kHalf;
+    const int64_t ntask = nblk * halves;
 
     // ---- init: seen = slots beyond the batch, partials, level-0/1 masks, X, rexp, work counters
     for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) {
@@ -688,8 +691,11 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         }
         __syncthreads();
       }
-      // light rows: dynamic blocks of 32 vertices, lane-parallel activity check
-      for (int64_t vb = gwarp(); vb < nblk; vb = next_block(a.wq + t, lane)) {
+      // light rows: (vertex block, quarter) tasks, lane-parallel activity check
+      for (int64_t tk = gwarp(); tk < ntask; tk = next_block(a.wq + t, lane)) {
+        const int64_t vb = tk / halves;
+        const int w0 = (int)(tk % halves) * kHalf;
+        const int nw = kHalf;
         const int64_t vl = vb + (int64_t)lane * nblk;
         int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
@@ -706,8 +712,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
           const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
           const int64_t sp = __shfl_sync(0xffffffffu, spl, j);
-          for (int w0 = 0; w0 < wpad; w0 += kHalf) {
-            const int nw = min(kHalf, wpad - w0);
+          {
             uint32_t seen[kHalf], unseen[kHalf], any[kHalf];
             load_row(a.seen + (int64_t)v * W + w0, nw, seen);
             uint32_t u_any = 0;
@@ -881,7 +886,10 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         __syncthreads();
       }
       const int wqi = a.tcap + 3 + lev;
-      for (int64_t vb = gwarp(); vb < nblk; vb = next_block(a.wq + wqi, lane)) {
+      for (int64_t tk = gwarp(); tk < ntask; tk = next_block(a.wq + wqi, lane)) {
+        const int64_t vb = tk / halves;
+        const int w0 = (int)(tk % halves) * kHalf;
+        const int nw = kHalf;
         const int64_t vl = vb + (int64_t)lane * nblk;
         int64_t e0l = 0, e1l = 0, spl = 0;
         bool on = false;
@@ -898,8 +906,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int32_t v = (int32_t)(vb + (int64_t)j * nblk);
           const int64_t e0 = __shfl_sync(0xffffffffu, e0l, j), e1 = __shfl_sync(0xffffffffu, e1l, j);
           const int64_t sp = __shfl_sync(0xffffffffu, spl, j);
-          for (int w0 = 0; w0 < wpad; w0 += kHalf) {
-            const int nw = min(kHalf, wpad - w0);
+          {
             uint32_t act[kHalf], any[kHalf];
             load_row(lm_here + (int64_t)v * W + w0, nw, act);
             uint32_t a_any = 0;
