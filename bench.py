@@ -309,7 +309,9 @@ def main():
     from centrality_gpu_b200 import multigpu
     mine = multigpu.shard(ranges, rank, world)
     need = args.warmup + args.steps
-    sel = [mine[i % len(mine)] for i in range(need)]
+    # steps evenly spaced over the whole source order (passes differ by region)
+    pick = np.linspace(0, len(mine) - 1, num=need).round().astype(int) if len(mine) >= need else np.arange(need) % len(mine)
+    sel = [mine[i] for i in pick]
 
     for r0, r1 in sel[:args.warmup]:
         plan.run(r0, r1, stats=False)

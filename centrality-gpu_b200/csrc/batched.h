@@ -15,6 +15,7 @@ struct BatchedConfig {
   int sms = 148;
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
+  const std::vector<char> *bccs_on = nullptr;  // BCCs this plan schedules (null: all)
 };
 
 struct BatchedPlan;

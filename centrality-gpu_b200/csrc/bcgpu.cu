@@ -59,8 +59,10 @@ struct bc_plan {
   double *ws_f = nullptr;
   int64_t ws_n = 0;
   int grid = 0, block = 1024;
-  // BATCHED
+  // BATCHED: multi-source passes are units [0, n_bat); the BCCs routed to
+  // the per-source schedule follow as PLAIN items
   bcg::BatchedPlan *bp = nullptr;
+  int64_t n_bat = 0;
   // per-unit work (prefix sums over units)
   std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux, unit_visits;
   int64_t device_bytes = 0;
@@ -178,8 +180,36 @@ int validate(bc_ctx *ctx, const bc_bccs *B) {
 // queue stays balanced when a hub owns thousands of chains.
 constexpr int64_t kItemChainVertices = 16;
 
-void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items) {
+// BATCHED routing: multi-source passes pay off on large, shallow cores; a
+// BCC with a core under kBatchedMinCore vertices, or with levels deeper than
+// kBatchedMaxLevels (2 x eccentricity of its first vertex + longest chain),
+// runs on the per-source schedule, whose rows stay in L2 and whose levels
+// need no grid-wide barrier.
+constexpr int32_t kBatchedMinCore = 8192;
+constexpr int kBatchedMaxLevels = 96;
+
+int bcc_ecc0(const bc_bccs *B, int32_t b, std::vector<int32_t> &dist, std::vector<int32_t> &queue) {
+  const int64_t vo = B->vtx_off[b];
+  const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
+  dist.assign((size_t)nb, -1);
+  queue.resize((size_t)nb);
+  int head = 0, tail = 0, ecc = 0;
+  queue[tail++] = 0;
+  dist[0] = 0;
+  while (head < tail) {
+    const int32_t x = queue[head++];
+    ecc = std::max(ecc, dist[x]);
+    for (int64_t e = B->row[vo + x]; e < B->row[vo + x + 1]; ++e) {
+      const int32_t y = B->col[e];
+      if (dist[y] < 0) { dist[y] = dist[x] + 1; queue[tail++] = y; }
+    }
+  }
+  return ecc;
+}
+
+void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items, const std::vector<char> *skip = nullptr) {
   for (int32_t b = 0; b < B->n_bcc; ++b) {
+    if (skip && (*skip)[b]) continue;
     int64_t c = B->chain_off[b];
     const int64_t ce = B->chain_off[b + 1];
     for (int32_t s = 0; s < B->n_plain[b]; ++s) {
@@ -236,16 +266,54 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
   CK(ctx, cudaMemGetInfo(&free_b, &total_b));
   int64_t limit = ctx->opts.workspace_limit > 0 ? ctx->opts.workspace_limit : (int64_t)(0.8 * (double)free_b);
 
+  // BATCHED: which BCCs take multi-source passes (the others: per-source items)
+  std::vector<char> on;
+  int64_t n_on = 0;
+  if (p->mode == BCGPU_MODE_BATCHED) {
+    on.assign((size_t)B->n_bcc, 1);
+    if (ctx->opts.plain_core >= 0) {
+      const int32_t min_core = ctx->opts.plain_core > 0 ? ctx->opts.plain_core : kBatchedMinCore;
+      std::vector<int32_t> dist, queue;
+      for (int32_t b = 0; b < B->n_bcc; ++b) {
+        int kmax = 0;
+        for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) kmax = std::max(kmax, B->chain_len[c]);
+        on[b] = B->n_plain[b] >= min_core && 2 * bcc_ecc0(B, b, dist, queue) + kmax <= kBatchedMaxLevels;
+      }
+    }
+    for (char x : on) n_on += x;
+  }
+  std::vector<bcg::PlainItem> items;
   if (p->mode == BCGPU_MODE_PLAIN) {
-    std::vector<bcg::PlainItem> items;
     if (override_items) items = *override_items;
     else plain_items(B, items);
+  } else if (n_on < B->n_bcc) {
+    plain_items(B, items, &on);
+  }
+  if (p->mode == BCGPU_MODE_BATCHED && n_on > 0) {
+    bcg::BatchedConfig cfg;
+    cfg.width = ctx->opts.batch_width;
+    cfg.delta_fp32c = ctx->opts.delta == BCGPU_DELTA_FP32C;
+    cfg.sms = ctx->sms;
+    cfg.limit_bytes = limit - p->device_bytes;
+    cfg.rescale_exp = ctx->opts.rescale_exp;
+    cfg.bccs_on = &on;
+    std::string msg;
+    rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
+                             p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
+    if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
+    p->device_bytes += bcg::batched_device_bytes(p->bp);
+    bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux, p->unit_visits);
+    p->n_bat = (int64_t)p->unit_sources.size() - 1;
+  } else {
+    p->unit_sources.assign(1, 0);
+    p->unit_teps.assign(1, 0);
+    p->unit_bfs.assign(1, 0);
+    p->unit_aux.assign(1, 0);
+    p->unit_visits.assign(1, 0);
+  }
+  if (!items.empty() || p->mode == BCGPU_MODE_PLAIN) {
     p->n_items = (int64_t)items.size();
-    p->unit_sources.assign(items.size() + 1, 0);
-    p->unit_teps.assign(items.size() + 1, 0);
-    p->unit_bfs.assign(items.size() + 1, 0);
-    p->unit_aux.assign(items.size() + 1, 0);
-    p->unit_visits.assign(items.size() + 1, 0);
+    int64_t nb_plain = 0;
     for (size_t i = 0; i < items.size(); ++i) {
       const auto &it = items[i];
       int64_t src = it.own ? 1 : 0, aux = it.own ? 0 : 1;
@@ -254,16 +322,18 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
         src += B->chain_len[c];
         if (B->chain_r[c] != prev) { ++aux; prev = B->chain_r[c]; }
       }
+      const int64_t nb = B->vtx_off[it.bcc + 1] - B->vtx_off[it.bcc];
+      nb_plain = std::max(nb_plain, nb);
       const int64_t arcs = B->row[B->vtx_off[it.bcc + 1]] - B->row[B->vtx_off[it.bcc]];
-      p->unit_sources[i + 1] = p->unit_sources[i] + src;
-      p->unit_teps[i + 1] = p->unit_teps[i] + src * arcs;
-      p->unit_bfs[i + 1] = p->unit_bfs[i] + (it.own ? 1 : 0);
-      p->unit_aux[i + 1] = p->unit_aux[i] + aux;
-      p->unit_visits[i + 1] = p->unit_visits[i] + src * (B->vtx_off[it.bcc + 1] - B->vtx_off[it.bcc]);
+      p->unit_sources.push_back(p->unit_sources.back() + src);
+      p->unit_teps.push_back(p->unit_teps.back() + src * arcs);
+      p->unit_bfs.push_back(p->unit_bfs.back() + (it.own ? 1 : 0));
+      p->unit_aux.push_back(p->unit_aux.back() + aux);
+      p->unit_visits.push_back(p->unit_visits.back() + src * nb);
     }
     if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
     p->h_items = items;
-    p->ws_n = nb_max + 2;
+    p->ws_n = (p->mode == BCGPU_MODE_PLAIN ? nb_max : nb_plain) + 2;
     const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
     // Four 256-thread CTAs per SM (four sources in flight) when their rows
     // fit the budget, else two of 512, else one of 1024 per SM.
@@ -285,19 +355,6 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
       return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
     std::vector<int32_t> ep((size_t)(2 * slots), 1);
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
-  } else {
-    bcg::BatchedConfig cfg;
-    cfg.width = ctx->opts.batch_width;
-    cfg.delta_fp32c = ctx->opts.delta == BCGPU_DELTA_FP32C;
-    cfg.sms = ctx->sms;
-    cfg.limit_bytes = limit - p->device_bytes;
-    cfg.rescale_exp = ctx->opts.rescale_exp;
-    std::string msg;
-    rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
-                             p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
-    if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
-    p->device_bytes += bcg::batched_device_bytes(p->bp);
-    bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux, p->unit_visits);
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->plans.insert(p);
@@ -423,23 +480,20 @@ extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, i
 }
 
 extern "C" int64_t bc_plan_device_bytes(const bc_plan *p) { return p ? p->device_bytes : 0; }
-extern "C" int bc_plan_concurrency(const bc_plan *p) { return !p ? 0 : p->bp ? 1 : p->grid; }
+extern "C" int bc_plan_concurrency(const bc_plan *p) { return !p ? 0 : p->mode == BCGPU_MODE_BATCHED ? 1 : p->grid; }
 
 extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t end, int64_t *out, int64_t cap) {
   if (!p) return -BCGPU_EINVAL;
   const int64_t n = bc_plan_num_units(p);
   if (begin < 0 || end < begin || end > n) return -BCGPU_EINVAL;
   std::vector<int64_t> ids;
-  if (p->mode == BCGPU_MODE_PLAIN) {
-    for (int64_t i = begin; i < end; ++i) {
-      const auto &it = p->h_items[i];
-      const int64_t vo = p->h_vtx_off[it.bcc];
-      if (it.own) ids.push_back(vo + it.src);
-      for (int32_t c = it.c0; c < it.c1; ++c)
-        for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
-    }
-  } else {
-    bcg::batched_unit_sources(p->bp, begin, end, ids);
+  if (p->bp && begin < p->n_bat) bcg::batched_unit_sources(p->bp, begin, std::min(end, p->n_bat), ids);
+  for (int64_t i = std::max(begin, p->n_bat) - p->n_bat; i < end - p->n_bat; ++i) {  // per-source items
+    const auto &it = p->h_items[i];
+    const int64_t vo = p->h_vtx_off[it.bcc];
+    if (it.own) ids.push_back(vo + it.src);
+    for (int32_t c = it.c0; c < it.c1; ++c)
+      for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
   }
   for (int64_t i = 0; i < (int64_t)ids.size() && i < cap; ++i) out[i] = ids[i];
   return (int64_t)ids.size();
@@ -461,23 +515,23 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
   CK(ctx, cudaSetDevice(ctx->device));
   int launches = 0;
   if (stats) CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-  if (end > begin) {
-    if (p->mode == BCGPU_MODE_PLAIN) {
-      CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
-      bcg::PlainArgs a{};
-      a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
-      a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
-      a.items = p->items; a.item_begin = begin; a.item_end = end; a.next_item = p->counter; a.bc = p->bc;
-      a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
-      a.err = p->err;
-      const int grid = (int)std::min<int64_t>(p->grid, end - begin);
-      CK(ctx, bcg::launch_plain(a, p->block, grid, ctx->stream));
-      launches = 1;
-    } else {
-      std::string msg;
-      int rc = bcg::batched_run(p->bp, begin, end, ctx->stream, &launches, &msg);
-      if (rc) return fail(ctx, rc, "batched run: " + msg);
-    }
+  if (p->bp && begin < p->n_bat) {  // multi-source passes
+    std::string msg;
+    int rc = bcg::batched_run(p->bp, begin, std::min(end, p->n_bat), ctx->stream, &launches, &msg);
+    if (rc) return fail(ctx, rc, "batched run: " + msg);
+  }
+  const int64_t i0 = std::max(begin, p->n_bat) - p->n_bat, i1 = end - p->n_bat;
+  if (i1 > i0) {  // per-source items
+    CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
+    bcg::PlainArgs a{};
+    a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
+    a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
+    a.items = p->items; a.item_begin = i0; a.item_end = i1; a.next_item = p->counter; a.bc = p->bc;
+    a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
+    a.err = p->err;
+    const int grid = (int)std::min<int64_t>(p->grid, i1 - i0);
+    CK(ctx, bcg::launch_plain(a, p->block, grid, ctx->stream));
+    ++launches;
   }
   if (stats) {
     CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));

@@ -60,7 +60,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarpsPerCta = kThreads / 32;
-constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs
+constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs ...
+constexpr int kHeavyDegSmall = 32; // ... or than this, on cores small enough that one row is a level's critical path
+constexpr int kSmallCore = 16384;  // cores below this many vertices use kHeavyDegSmall
 constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr long long kSpinLimit = 1ll << 28;  // ~1 min of polling before giving up
 constexpr int kHalf = 4;           // words per pass over a vertex row
@@ -81,6 +83,8 @@ struct Batch {
   int32_t bcc, nslots, words, nseeds;
   int32_t max_seed;  // deepest seed level (0: none)
   int32_t kmax;      // longest chain of the BCC: the longest arc is kmax+1
+  int32_t heavy_deg; // rows longer than this are chunked over whole CTAs
+  int32_t pad;
   int64_t slot_off, seed_off;
 };
 
@@ -703,7 +707,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           e0l = HR[vl];
           e1l = HR[vl + 1];
           spl = HS[vl];
-          on = e1l - e0l <= kHeavyDeg && __ldcg(a.gdone + vl) < groups;
+          on = e1l - e0l <= bt.heavy_deg && __ldcg(a.gdone + vl) < groups;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, on);
         while (todo) {
@@ -897,7 +901,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           e0l = HR[vl];
           e1l = HR[vl + 1];
           spl = HS[vl];
-          on = e1l - e0l <= kHeavyDeg;
+          on = e1l - e0l <= bt.heavy_deg;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, on);
         while (todo) {
@@ -1132,6 +1136,13 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
     const int32_t npl = B->n_plain[b];
     const int64_t ce0 = B->chain_off[b], ce1 = B->chain_off[b + 1];
+    if (cfg.bccs_on && !(*cfg.bccs_on)[b]) {  // scheduled elsewhere: empty per-BCC table entries
+      hvo.push_back((int64_t)hrow.size());
+      hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
+      heavy_off.push_back((int64_t)heavy.size());
+      hchunk_off.push_back((int64_t)hchunk_v.size());
+      continue;
+    }
     ncap = std::max<int64_t>(ncap, npl);
     nbcap = std::max<int64_t>(nbcap, nb);
     const int64_t arcs = B->row[vo + nb] - B->row[vo];
@@ -1165,6 +1176,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     }
     // contracted rows: unit arcs first, then chain arcs
     hvo.push_back((int64_t)hrow.size());
+    const int heavy_deg = npl < kSmallCore ? kHeavyDegSmall : kHeavyDeg;
     int32_t hidx = 0;
     for (int32_t x = 0; x < npl; ++x) {
       const int64_t r0 = (int64_t)hcol.size();
@@ -1188,7 +1200,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         hcid.push_back((int32_t)(c * 2 + right));
       }
       const int64_t r1 = (int64_t)hcol.size();
-      if (r1 - r0 <= kHeavyDeg) continue;
+      if (r1 - r0 <= heavy_deg) continue;
       heavy.push_back(x);
       hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
       for (int64_t e = r0; e < r1; e += kChunkArcs) {
@@ -1246,6 +1258,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
       bt.nslots = (int32_t)(i1 - i0);
       bt.words = (bt.nslots + 31) / 32;
       bt.kmax = kmax;
+      bt.heavy_deg = heavy_deg;
       bt.slot_off = (int64_t)slots.size();
       bt.seed_off = (int64_t)seeds.size();
       for (size_t i = i0; i < i1; ++i) {

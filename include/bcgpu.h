@@ -51,7 +51,11 @@ typedef struct bc_opts {
   int64_t workspace_limit; /* device bytes the context may hold; 0 = 80% of free memory */
   int32_t rescale_exp;   /* BATCHED: rescale a level's path counts above 2^rescale_exp; 0 = 900.
                             Lower values only exercise the scaling path (tests). */
-  int32_t pad_;
+  int32_t plain_core;    /* BATCHED: BCCs whose core (the vertices off degree-2 chains) has fewer
+                            vertices than this, or whose levels run deeper than 96, use the
+                            per-source schedule inside the same plan (small or deep BCCs
+                            gain nothing from multi-source passes); 0 = 8192, negative =
+                            every BCC in multi-source passes */
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;

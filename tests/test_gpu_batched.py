@@ -1,6 +1,9 @@
-"""GPU parity of the BATCHED schedule (bitmask multi-source BFS) against the
-oracle: FP64 dependencies within 1e-12 relative, compensated FP32
-dependencies within 1e-6 relative (the metric's accuracy bar)."""
+"""GPU parity of the BATCHED schedule (bitmask multi-source BFS over the
+chain-contracted graph) against the oracle: FP64 dependencies within 1e-12
+relative, compensated FP32 dependencies within 1e-6 relative (the metric's
+accuracy bar). "multi" forces every BCC into multi-source passes (the kernel
+under test on small graphs); "auto" is the default routing, where small or
+deep BCCs take the per-source schedule inside the same plan."""
 import numpy as np
 import pytest
 
@@ -11,16 +14,17 @@ pytestmark = pytest.mark.gpu
 TOL = {"fp64": 1e-12, "fp32c": 1e-6}
 
 
-def ctx_for(delta, width=0, rescale_exp=0):
+def ctx_for(delta, width=0, rescale_exp=0, route="multi"):
     P = pkg()
     return P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C,
-                     batch_width=width, rescale_exp=rescale_exp)
+                     batch_width=width, rescale_exp=rescale_exp, plain_core=-1 if route == "multi" else 0)
 
 
-@pytest.fixture(scope="module", params=["fp64", "fp32c"])
+@pytest.fixture(scope="module", params=["fp64-multi", "fp32c-multi", "fp32c-auto"])
 def bctx(request):
-    c = ctx_for(request.param)
-    c.tol = TOL[request.param]
+    delta, route = request.param.split("-")
+    c = ctx_for(delta, route=route)
+    c.tol = TOL[delta]
     yield c
     c.close()
 
@@ -168,3 +172,25 @@ def test_batched_vs_plain_same_numbers():
     assert rel_err(b, a) < 1e-12
     p.close()
     b_ctx.close()
+
+
+def test_routing_mixes_both_schedules():
+    """Twelve BA graphs of mixed sizes: with the core threshold at 500, the
+    five BCCs whose cores reach it take multi-source passes and the seven
+    smaller ones per-source items, in one plan (two launches)."""
+    G = graphs()
+    n, u, v, _ = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))
+    d = decomp(n, u, v)
+    arrs = d.arrays()
+    cores = [int(x) for x in arrs["n_plain"]]
+    assert sum(c >= 500 for c in cores) == 5 and sum(c < 500 for c in cores) == 7
+    P = pkg()
+    for delta in ("fp64", "fp32c"):
+        c = P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C, plain_core=500)
+        plan = c.plan(d)
+        st = plan.run(0, plan.n_units)
+        assert st["kernel_launches"] == 2
+        assert st["sources"] == int(arrs["n_packed"])
+        assert rel_err(plan.read(), oracle_bc(n, u, v)) < TOL[delta]
+        plan.close()
+        c.close()
