@@ -113,7 +113,7 @@ struct Args {
   // chains (global index)
   const int64_t *chain_off;
   const int32_t *chain_start, *chain_len, *chain_l, *chain_r;
-  const int64_t *cpre_off;  // chain -> its k+1 prefix sums of reach+1 (from the left end) in cpre
+  const int64_t *cpre_off;  // chain -> its k+1 prefix sums of reach+1 (from the left end) in cpre; -1: all reach 0
   const double *cpre;
   // heavy rows (contracted degree > kHeavyDeg), chunked
   const int64_t *heavy_off;  // per BCC range in heavy[]
@@ -140,6 +140,7 @@ struct Args {
   int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
   double *bcpart;   // [nb_cap][W] every vertex of the BCC (chain vertices included)
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
+  double *wsrc;     // [B] reach(source)+1 of each slot of the pass
   int32_t *X;       // [B][tcap+2]
   int32_t *rexp;    // [B] per-level max exponent (rescale)
   int64_t n_cap;    // core rows allocated (>= largest core)
@@ -234,12 +235,18 @@ struct Comp32 {
 // A stretch of a chain between two ends A and B holding m chain vertices,
 // seen from A: its vertex i (0 <= i < m) lies i+1 arcs from A and m-i from B.
 // pre(x) is the sum of reach+1 over its first x vertices counted from A.
+// Prefix sum x of a chain: P[x], or x itself on a chain whose vertices have
+// nothing hanging off them (P null: no table, no load).
+__device__ __forceinline__ double chain_pre(const double *P, int x) { return P ? __ldg(P + x) : (double)x; }
+
 struct Stretch {
-  const double *P;  // the chain's prefix sums from its left end (k+1 entries)
+  const double *P;  // the chain's prefix sums from its left end (k+1 entries), or null (all reach 0)
   int lo, hi;       // chain positions [lo, hi) of the stretch
   bool rev;         // A is the right-hand end (position hi)
   __device__ __forceinline__ int m() const { return hi - lo; }
-  __device__ __forceinline__ double pre(int x) const { return rev ? P[hi] - P[hi - x] : P[lo + x] - P[lo]; }
+  __device__ __forceinline__ double pre(int x) const {
+    return rev ? chain_pre(P, hi) - chain_pre(P, hi - x) : chain_pre(P, lo + x) - chain_pre(P, lo);
+  }
   __device__ __forceinline__ double wt(int i) const { return pre(i + 1) - pre(i); }
   __device__ __forceinline__ Stretch flip() const { return Stretch{P, lo, hi, !rev}; }
 };
@@ -497,10 +504,11 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
         ib[r] = ((int64_t)uj * W + w) * 32 + lane;
         B[r] = End{(live && j0 + r < cnt) ? __ldcg(a.d + ib[r]) : 0, 0, 1.0, 0.0};
         const bool right = cj & 1;
-        st[r] = Stretch{a.cpre + pj, 0, kj, right};
+        const double *Pj = pj < 0 ? nullptr : a.cpre + pj;
+        st[r] = Stretch{Pj, 0, kj, right};
         if (sl.chain == (cj >> 1)) {  // the source sits on this chain: the stretch ends at it
           ib[r] = -1;
-          st[r] = right ? Stretch{a.cpre + pj, sl.pos + 1, kj, true} : Stretch{a.cpre + pj, 0, sl.pos, false};
+          st[r] = right ? Stretch{Pj, sl.pos + 1, kj, true} : Stretch{Pj, 0, sl.pos, false};
         }
       }
 #pragma unroll
@@ -546,7 +554,7 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
       if (!(aq >= (double)FLT_MIN * 0x1p24 && aq <= (double)FLT_MAX * 0x1p-24)) atomicExch(&a.ctrl->range_err, 1);
     }
     reinterpret_cast<QT *>(a.q)[idx] = (QT)qv;
-    contrib = delta * ((double)rch[slots[b].src] + 1.0);
+    contrib = delta * a.wsrc[b];
   }
   contrib = warp_sum(contrib);  // fixed-order reduction of this word's slots
   if (lane == 0) a.bcpart[(int64_t)v * W + w] += contrib;
@@ -622,6 +630,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     for (int64_t i = gtid; i < (int64_t)W * 32; i += gthreads) {
       a.rexp[i] = INT_MIN;
       a.X[i * (a.tcap + 2)] = 0;
+      a.wsrc[i] = i < bt.nslots ? (double)rch[slots[i].src] + 1.0 : 0.0;
     }
     for (int64_t i = gtid; i < 2 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
     if (gtid == 0) {
@@ -962,7 +971,8 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         const int b = w * 32 + lane;
         const bool live = b < bt.nslots;
         const int32_t L = a.chain_l[c], R = a.chain_r[c], cs = a.chain_start[c], k = a.chain_len[c];
-        const double *P = a.cpre + a.cpre_off[c];
+        const int64_t poff = a.cpre_off[c];
+        const double *P = poff < 0 ? nullptr : a.cpre + poff;
         const int64_t iL = ((int64_t)L * W + w) * 32 + lane, iR = ((int64_t)R * W + w) * 32 + lane;
         End eL{0, 0, 1.0, 0.0}, eR{0, 0, 1.0, 0.0};
         Slot sl{0, -1, 0, 0};
@@ -998,7 +1008,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             if (!(tieL || tieR || viaL || viaR)) eR.x = __ldcg(xb + eR.d);
           }
         }
-        const double wsrc = live ? (double)rch[sl.src] + 1.0 : 0.0;
+        const double wsrc = live ? a.wsrc[b] : 0.0;
         // Source off the chain (the common case), in prefix sums from L:
         // vertex j is fed from L iff 2j <= D; a tie vertex t = D/2 shares its
         // reach+1 between the sides in proportion to sigma_L, sigma_R; else
@@ -1010,13 +1020,14 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           D = eR.d + k - eL.d - 1;
           if (D >= 0 && (D & 1) == 0 && D / 2 <= k - 1) {
             tv = D / 2;
-            const double w = P[tv + 1] - P[tv];
-            fL = P[tv] + w / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
-            fR = -P[tv + 1] + w / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
+            const double p0 = chain_pre(P, tv), p1 = chain_pre(P, tv + 1), w = p1 - p0;
+            fL = p0 + w / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
+            fR = -p1 + w / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
           } else {
             pl = D >= 0 ? min(k - 1, D / 2) : -1;
-            fL = P[pl + 1] + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
-            fR = -P[pl + 1] + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
+            const double p1 = chain_pre(P, pl + 1);
+            fL = p1 + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
+            fR = -p1 + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
           }
         }
         for (int j = 0; j < k; ++j) {
@@ -1024,7 +1035,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           if (live) {
             if (on < 0) {
               const bool from_l = tv >= 0 ? j < tv : j <= pl;
-              if (j != tv) dep = from_l ? fL - P[j + 1] : P[j] + fR;
+              if (j != tv) dep = from_l ? fL - chain_pre(P, j + 1) : chain_pre(P, j) + fR;
             } else if (j < on) {
               dep = stretch_dep(Stretch{P, 0, on, false}, j, eL, source_end());
             } else if (j > on) {
@@ -1166,12 +1177,16 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         if (e1 - e0 != 2 || !((B->col[e0] == prev && B->col[e0 + 1] == next) || (B->col[e0] == next && B->col[e0 + 1] == prev)))
           return bail(BCGPU_EINVAL, "a chain vertex whose neighbours are not its chain neighbours");
       }
-      cpre_off[c] = (int64_t)cpre.size();
-      double acc = 0.0;
-      cpre.push_back(0.0);
-      for (int32_t j = 0; j < k; ++j) {
-        acc += (double)B->reach[vo + s + j] + 1.0;
-        cpre.push_back(acc);
+      bool flat = true;
+      for (int32_t j = 0; j < k; ++j) flat = flat && B->reach[vo + s + j] == 0;
+      cpre_off[c] = flat ? -1 : (int64_t)cpre.size();
+      if (!flat) {
+        double acc = 0.0;
+        cpre.push_back(0.0);
+        for (int32_t j = 0; j < k; ++j) {
+          acc += (double)B->reach[vo + s + j] + 1.0;
+          cpre.push_back(acc);
+        }
       }
     }
     // contracted rows: unit arcs first, then chain arcs
@@ -1323,6 +1338,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, nbcap * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
+  ok &= ok && alloc(&p, (int64_t)W * 32 * 8); a.wsrc = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * (tcap + 2) * 4); a.X = (int32_t *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 4); a.rexp = (int32_t *)p;
   ok &= ok && alloc(&p, sizeof(Ctrl)); a.ctrl = (Ctrl *)p;
