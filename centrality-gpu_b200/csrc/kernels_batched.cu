@@ -84,8 +84,9 @@ struct Batch {
   int32_t max_seed;  // deepest seed level (0: none)
   int32_t kmax;      // longest chain of the BCC: the longest arc is kmax+1
   int32_t heavy_deg; // rows longer than this are chunked over whole CTAs
-  int32_t pad;
+  int32_t narm;      // entries of the pass's arming list
   int64_t slot_off, seed_off;
+  int64_t arm_off;   // arming list: (vertex, level) of the core sources and seeded vertices
 };
 
 // Control block in global memory (one per plan).
@@ -128,6 +129,7 @@ struct Args {
   const Batch *batches;
   const Slot *slots;
   const Seed *seeds;
+  const int2 *arms;
   int64_t b0, b1;
   // workspace (core rows)
   int32_t *d;
@@ -137,6 +139,7 @@ struct Args {
   uint32_t *seen;   // [n_cap][W]
   int32_t *lmin, *lmax;
   int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
+  int32_t *armed;   // [n_cap] first level on which some slot can reach the vertex (a neighbour was reached)
   int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
   double *bcpart;   // [nb_cap][W] every vertex of the BCC (chain vertices included)
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
@@ -434,10 +437,12 @@ __device__ __forceinline__ double acc_value(const WarpScratch &S, int k, int lan
 }
 
 // Stores the result of one (vertex, word) of the forward step; returns the
-// number of slots that reached the vertex (uniform over the warp).
+// number of slots that reached the vertex, plus 256 when this is the first
+// time any slot reached it (uniform over the warp).
 __device__ __forceinline__ int finish_pull(const Args &a, int32_t v, int w, int t, uint32_t newm, int lane,
                                            double acc) {
   if (!newm) return 0;
+  int first = 0;
   const int64_t idx = ((int64_t)v * a.W + w) * 32 + lane;
   if ((newm >> lane) & 1u) {
     a.d[idx] = t + 1;
@@ -451,10 +456,16 @@ __device__ __forceinline__ int finish_pull(const Args &a, int32_t v, int w, int 
     a.lm[((int64_t)(t + 1) * a.n_cap + v) * a.W + w] = newm;
     a.seen[(int64_t)v * a.W + w] |= newm;
     a.ctrl->more[t & 1] = 1;
-    atomicMin(a.lmin + v, t + 1);
+    first = atomicMin(a.lmin + v, t + 1) == INT_MAX;
     atomicMax(a.lmax + v, t + 1);
   }
-  return __popc(newm);
+  return __popc(newm) + (__shfl_sync(0xffffffffu, first, 0) << 8);
+}
+
+// Arms the neighbours of a vertex first reached on level lvl: a neighbour
+// across an arc of length k+1 can be reached from it on level lvl+k+1.
+__device__ __forceinline__ void arm_arcs(const Args &a, int64_t e0, int64_t e1, int lvl, int64_t tid, int64_t nthr) {
+  for (int64_t e = e0 + tid; e < e1; e += nthr) atomicMin(a.armed + ldg(a.hcol + e), lvl + 1 + ldg(a.hk + e));
 }
 
 // ============================================================== backward ===
@@ -625,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       a.bcpart[i] = 0.0;
       a.lm[i] = 0;                         // level 0
       a.lm[(int64_t)a.n_cap * W + i] = 0;  // level 1
-      if (w == 0) { a.lmin[i / W] = INT_MAX; a.lmax[i / W] = -1; a.gdone[i / W] = 0; }
+      if (w == 0) { a.lmin[i / W] = INT_MAX; a.lmax[i / W] = -1; a.gdone[i / W] = 0; a.armed[i / W] = INT_MAX; }
     }
     for (int64_t i = gtid; i < (int64_t)W * 32; i += gthreads) {
       a.rexp[i] = INT_MIN;
@@ -651,6 +662,10 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       atomicMin(a.lmin + s.src, 0);
       atomicMax(a.lmax + s.src, 0);
       atomicAdd(&a.ctrl->found, 1ull);
+    }
+    for (int64_t i = gwarp(); i < bt.narm; i += nwarps()) {  // neighbours of sources and seeded vertices
+      const int2 m = a.arms[bt.arm_off + i];
+      arm_arcs(a, HR[m.x], HR[m.x + 1], m.y, lane, 32);
     }
     grid_sync(a);
     PHASE_MARK(0);
@@ -682,7 +697,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         for (int k = 0; k < kHalf; ++k) { unseen[k] = k < nw ? ~unseen[k] : 0u; any[k] = 0; u_any |= unseen[k]; }
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-        if (u_any) {  // uniform over the CTA
+        if (u_any && __ldcg(a.armed + v) <= t + 1) {  // uniform over the CTA
           const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
@@ -716,7 +731,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           e0l = HR[vl];
           e1l = HR[vl + 1];
           spl = HS[vl];
-          on = e1l - e0l <= bt.heavy_deg && __ldcg(a.gdone + vl) < groups;
+          on = e1l - e0l <= bt.heavy_deg && __ldcg(a.gdone + vl) < groups && __ldcg(a.armed + vl) <= t + 1;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, on);
         while (todo) {
@@ -736,13 +751,17 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
             if (e0 < sp) row_pass<double, false, 0>(a, S, lmt, a.sig, e0, sp, w0, nw, unseen, any, lane, t);
             if (sp < e1) row_pass<double, false, 1>(a, S, a.lm, a.sig, sp, e1, w0, nw, unseen, any, lane, t);
+            int first = 0;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) {
               if (k >= nw) continue;
               const uint32_t m = warp_or(any[k]);
-              nf += finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
+              const int r = finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
+              nf += r & 255;
+              first |= r >> 8;
               any[k] = m;
             }
+            if (first) arm_arcs(a, e0, e1, t + 1, lane, 32);
 #pragma unroll
             for (int g = 0; g < kHalf / 4; ++g) {  // groups now seen by all their slots
               if (4 * g >= nw || lane != 0) continue;
@@ -774,7 +793,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             acc += __ldcg(a.hacc + ((hc0 + c) * W + w) * 32 + lane);
             m |= __ldcg(a.hmask + (hc0 + c) * W + w);
           }
-          nf += finish_pull(a, v, w, t, m, lane, acc);
+          nf += finish_pull(a, v, w, t, m, lane, acc) & 255;  // heavy rows arm in the next phase
         }
         if (lane == 0 && nf) atomicAdd(&a.ctrl->found, nf);
         grid_sync(a);
@@ -806,6 +825,9 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       const int more = *(volatile int *)&a.ctrl->more[t & 1];
       const int resc = *(volatile int *)&a.ctrl->rescale[t & 1];
       const unsigned long long found = *(volatile unsigned long long *)&a.ctrl->found;
+      // heavy rows first reached on level t+1 arm their neighbours, one CTA per chunk
+      for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x)
+        if (__ldcg(a.lmin + hv[hcv[c]]) == t + 1) arm_arcs(a, hce0[c], hce1[c], t + 1, threadIdx.x, blockDim.x);
       // base exponent of level t+1; rescale it when some slot's counts passed 2^rescale_exp
       for (int64_t b = gtid; b < (int64_t)W * 32; b += gthreads) {
         const int re = __ldcg(a.rexp + b);
@@ -1135,6 +1157,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   std::vector<double> cpre;
   std::vector<Slot> slots;
   std::vector<Seed> seeds;
+  std::vector<int2> arms, arm_tmp;
   std::vector<int64_t> heavy_off{0}, hchunk_off{0}, hchunk_e0, hchunk_e1;
   std::vector<int32_t> heavy, hchunk_v, hfirst;
   std::vector<int32_t> dist, queue;
@@ -1291,6 +1314,16 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         bt.max_seed = std::max(bt.max_seed, std::max(p + 1, k - p));
       }
       bt.nseeds = (int32_t)((int64_t)seeds.size() - bt.seed_off);
+      // arming list: each core source (level 0) and seeded vertex (its lowest seed level), once
+      arm_tmp.clear();
+      for (int64_t i = bt.slot_off; i < bt.slot_off + bt.nslots; ++i)
+        if (slots[i].chain < 0) arm_tmp.push_back(make_int2(slots[i].src, 0));
+      for (int64_t i = bt.seed_off; i < bt.seed_off + bt.nseeds; ++i) arm_tmp.push_back(make_int2(seeds[i].v, seeds[i].level));
+      std::sort(arm_tmp.begin(), arm_tmp.end(), [](const int2 &x, const int2 &y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
+      bt.arm_off = (int64_t)arms.size();
+      for (size_t i = 0; i < arm_tmp.size(); ++i)
+        if (i == 0 || arm_tmp[i].x != arm_tmp[i - 1].x) arms.push_back(arm_tmp[i]);
+      bt.narm = (int32_t)((int64_t)arms.size() - bt.arm_off);
       P->h_batches.push_back(bt);
       P->u_src.push_back(bt.nslots);
       P->u_teps.push_back((int64_t)bt.nslots * arcs);
@@ -1335,6 +1368,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok &= ok && alloc(&p, n * 4); a.lmin = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
+  ok &= ok && alloc(&p, n * 4); a.armed = (int32_t *)p;
   ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, nbcap * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
@@ -1369,6 +1403,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok = ok && upload((const void **)&a.batches, P->h_batches.data(), (int64_t)P->h_batches.size() * (int64_t)sizeof(Batch));
   ok = ok && upload((const void **)&a.slots, slots.data(), (int64_t)slots.size() * (int64_t)sizeof(Slot));
   ok = ok && upload((const void **)&a.seeds, seeds.data(), (int64_t)seeds.size() * (int64_t)sizeof(Seed));
+  ok = ok && upload((const void **)&a.arms, arms.data(), (int64_t)arms.size() * (int64_t)sizeof(int2));
   ok = ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 32 * 8); a.hacc = (double *)p;
   ok = ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 4); a.hmask = (uint32_t *)p;
   if (!ok) return bail(BCGPU_ENOMEM, "cudaMalloc or upload of the batched workspace failed");
