@@ -259,7 +259,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["batched", "plain"], default="batched")
     ap.add_argument("--delta", choices=["fp32c", "fp64"], default="fp32c")
-    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=0, help="sources per multi-source pass (0 = autotune)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat20")
     ap.add_argument("--step-sources", type=int, default=0, help="sources per step (0 = by workload and mode)")
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -301,7 +301,14 @@ def main():
     # library reads as "use your own stream"
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    ctx = P.Context(mode=mode, delta=delta, batch_width=args.batch, device=local, stream=stream.cuda_stream,
+    width, tuned = args.batch, None
+    if mode == P.MODE_BATCHED and args.batch == 0:  # the library's autotuner, outside the timed region
+        tctx = P.Context(mode=mode, delta=delta, device=local, stream=stream.cuda_stream,
+                         workspace_limit=int(args.workspace_gb * 2**30))
+        width, per = tctx.autotune_width(d, passes=4)
+        tctx.close()
+        tuned = {str(k): round(v, 2) for k, v in per.items()}
+    ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30))
     plan = ctx.plan(d)
     target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
@@ -416,6 +423,7 @@ def main():
                        "chain_vertices": info["n_chain_vertices"], "sources_per_step": sources_all / args.steps / world,
                        "units_per_step": float(np.mean([r1 - r0 for r0, r1 in sel])),
                        "host_decomposition_s": round(host_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
+                       "batch_width": st.get("batch_width"), "autotune_gteps": tuned,
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "plain": plain,

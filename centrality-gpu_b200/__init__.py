@@ -89,6 +89,7 @@ _SIGS = {
     "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p, _i64p]),
     "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
     "bc_plan_concurrency": (C.c_int, [C.c_void_p]),
+    "bc_autotune_width": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "bc_plan_unit_sources": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_int64]),
     "bc_plan_reset": (C.c_int, [C.c_void_p]),
     "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
@@ -273,6 +274,14 @@ class Context:
 
     def plan(self, decomp: Decomposition):
         return Plan(self, decomp)
+
+    def autotune_width(self, decomp: Decomposition, passes: int = 4):
+        """Times up to `passes` multi-source passes at widths 128/256/512/1024
+        (bc_autotune_width); returns (best width or 0, {width: GTEPS})."""
+        w = C.c_int32(0)
+        g = (C.c_double * 4)()
+        self._check(lib().bc_autotune_width(self._h, decomp.view, passes, C.byref(w), g))
+        return w.value, {c: g[i] for i, c in enumerate((128, 256, 512, 1024))}
 
     def close(self):
         """Releases the context; its plans are released with it."""

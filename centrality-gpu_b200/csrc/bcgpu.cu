@@ -454,6 +454,36 @@ extern "C" int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out) {
   return create_plan(ctx, bccs, nullptr, out);
 }
 
+extern "C" int bc_autotune_width(bc_ctx *ctx, const bc_bccs *bccs, int32_t passes, int32_t *width, double *gteps_out) {
+  if (!ctx || !bccs || !width) return fail(ctx, BCGPU_EINVAL, "null argument");
+  if (ctx->opts.mode != BCGPU_MODE_BATCHED) return fail(ctx, BCGPU_EINVAL, "autotuning needs a BATCHED context");
+  const int cand[4] = {128, 256, 512, 1024};
+  const int32_t saved = ctx->opts.batch_width;
+  double best = -1.0;
+  *width = 0;
+  for (int i = 0; i < 4; ++i) {
+    if (gteps_out) gteps_out[i] = 0.0;
+    ctx->opts.batch_width = cand[i];
+    bc_plan *p = nullptr;
+    int rc = create_plan(ctx, bccs, nullptr, &p);
+    if (rc == BCGPU_ENOMEM) continue;  // this width does not fit
+    if (rc) { ctx->opts.batch_width = saved; return rc; }
+    if (p->n_bat == 0) { bc_plan_destroy(p); break; }
+    const int64_t k = std::max<int64_t>(1, std::min<int64_t>(std::max(passes, 1), p->n_bat));
+    const int64_t b0 = std::max<int64_t>(0, p->n_bat / 2 - k / 2), b1 = std::min(p->n_bat, b0 + k);
+    bc_stats st;
+    rc = bc_plan_run(p, b0, std::min(b1, b0 + 1), nullptr);  // warm-up
+    if (!rc) rc = bc_plan_run(p, b0, b1, &st);
+    bc_plan_destroy(p);
+    if (rc) { ctx->opts.batch_width = saved; return rc; }
+    const double g = st.kernel_ms > 0 ? (double)st.teps_edges / (st.kernel_ms * 1e6) : 0.0;
+    if (gteps_out) gteps_out[i] = g;
+    if (g > best) { best = g; *width = cand[i]; }
+  }
+  ctx->opts.batch_width = saved;
+  return BCGPU_OK;
+}
+
 extern "C" void bc_plan_destroy(bc_plan *p) {
   if (!p) return;
   p->ctx->plans.erase(p);

@@ -192,6 +192,16 @@ int64_t bc_plan_device_bytes(const bc_plan *plan);
  * BATCHED, 1 (one pass at a time over the whole GPU). No reference
  * counterpart: the reference launches one source at a time. */
 int bc_plan_concurrency(const bc_plan *plan);
+
+/* Batch-width autotuner (no reference counterpart: the reference has one
+ * source per launch). For each candidate width 128, 256, 512, 1024 it builds a
+ * BATCHED plan of these BCCs with ctx's other options, times up to
+ * `passes` multi-source passes from the middle of the source order (after one
+ * warm-up pass) and writes the fastest width to *width; gteps_out (4 entries,
+ * may be NULL) receives each candidate's TEPS / 1e9 (0 if it did not fit). A
+ * plan without multi-source passes (every BCC routed per-source) leaves
+ * *width = 0. Pass the width back as bc_opts.batch_width. */
+int bc_autotune_width(bc_ctx *ctx, const bc_bccs *bccs, int32_t passes, int32_t *width, double *gteps_out);
 int bc_plan_reset(bc_plan *plan);
 /* Enqueues units [begin, end) on the context's stream; asynchronous unless
  * stats is non-NULL (then synchronises and fills it). */

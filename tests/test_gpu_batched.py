@@ -194,3 +194,19 @@ def test_routing_mixes_both_schedules():
         assert rel_err(plan.read(), oracle_bc(n, u, v)) < TOL[delta]
         plan.close()
         c.close()
+
+
+def test_autotune_width():
+    """The width autotuner times each candidate on this graph's passes and
+    returns one of them; a plan at that width gives the oracle's BC."""
+    n, u, v = graphs().gen_rmat(11, 16, chain_frac=0.2, chain_hi=8, seed=2)
+    d = decomp(n, u, v)
+    c = ctx_for("fp32c")
+    w, per = c.autotune_width(d, passes=2)
+    assert w in (128, 256, 512, 1024) and per[w] == max(per.values()) > 0
+    c.close()
+    c = ctx_for("fp32c", w)
+    got, st = c.run(d)
+    assert st["batch_width"] == w
+    assert rel_err(got, oracle_bc(n, u, v)) < TOL["fp32c"]
+    c.close()
