@@ -307,17 +307,32 @@ __device__ __forceinline__ double end_dep(const Stretch &s, const End &A, const 
 }
 
 // ============================================================== forward ====
-// A task is one vertex's whole row: lane j loads neighbour j's mask words for
-// up to kHalf words at once (aligned 16-byte loads, all in flight), the
-// (word, neighbour) pairs that hit are listed in shared memory, and the
-// neighbours' value rows are gathered eight at a time (lane = slot,
-// coalesced) into per-(word, slot) accumulators in shared memory. Adds to an
-// accumulator follow arc order, so sums are deterministic.
+// A task is one vertex row for kHalf 32-slot words: lane j loads arc j's
+// neighbour and its mask words (one aligned 16-byte load), then, word by
+// word, the arcs that hit (a ballot) are walked in arc order and their value
+// rows gathered eight at a time (lane = slot, coalesced) into per-(word,
+// slot) accumulators held in registers. Adds follow arc order, so sums are
+// deterministic.
 
+// Per-(word, slot) accumulator of a row pass: FP64, or compensated FP32.
+template <bool kComp>
+struct Acc {
+  double s = 0.0;
+  __device__ __forceinline__ void add(double x) { s += x; }
+  __device__ __forceinline__ double value() const { return s; }
+};
+template <>
+struct Acc<true> {
+  Comp32 c;
+  __device__ __forceinline__ void add(double x) { c.add((float)x); }
+  __device__ __forceinline__ double value() const { return c.value(); }
+};
+
+// Per-warp shared memory: partial sums and hit masks of the heavy-row chunks,
+// combined across the CTA's warps in fixed order.
 struct WarpScratch {
-  uint32_t f[32][kHalf + 1];  // neighbour masks of the current 32-arc chunk (padded against bank conflicts)
-  uint16_t pairs[32 * kHalf]; // (word << 5 | neighbour lane) of the hits
-  double acc[kHalf][32];      // per (word, slot) sums (FP64, or two FP32 halves in the compensated mode)
+  double acc[kHalf][32];
+  uint32_t any[kHalf];
 };
 
 __device__ __forceinline__ uint4 ld4(const uint32_t *p) { return __ldcg(reinterpret_cast<const uint4 *>(p)); }
@@ -346,11 +361,11 @@ __device__ __forceinline__ T warp_or(T v) {
 //            X to level t's) or level t + hk[e] (kLev == 2, backward: q
 //            rebased to level t's X; levels above tend are empty)
 //   vals     per-slot values gathered on a hit (sigma, or q)
-// Accumulates into S.acc and ORs the hits into any[k] (per lane).
+// Adds into acc[k] and ORs the hits into any[k] (per lane).
 template <typename T, bool kComp, int kLev>
-__device__ __forceinline__ void row_pass(const Args &a, WarpScratch &S, const uint32_t *masks, const T *vals,
-                                         int64_t e0, int64_t e1, int w0, int nw, const uint32_t (&filt)[kHalf],
-                                         uint32_t (&any)[kHalf], int lane, int t, int tend = 0) {
+__device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, const T *vals, int64_t e0, int64_t e1,
+                                         int w0, int nw, const uint32_t (&filt)[kHalf], uint32_t (&any)[kHalf],
+                                         Acc<kComp> (&acc)[kHalf], int lane, int t, int tend = 0) {
   const int W = a.W;
   for (int64_t base = e0; base < e1; base += 32) {
     const int64_t e = base + lane;
@@ -367,73 +382,39 @@ __device__ __forceinline__ void row_pass(const Args &a, WarpScratch &S, const ui
     uint32_t f[kHalf];
     const uint32_t *mrow = kLev ? masks + ((int64_t)(valid ? lvl : 0) * a.n_cap + u) * W + w0 : masks + (int64_t)u * W + w0;
     load_row(mrow, valid ? nw : 0, f);
-    int cnt = 0;
 #pragma unroll
     for (int k = 0; k < kHalf; ++k) {
       f[k] &= filt[k];
-      S.f[lane][k] = f[k];
       any[k] |= f[k];
-      cnt += f[k] != 0u;
     }
-    int incl = cnt;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    int pos = incl - cnt;
+    for (int k = 0; k < kHalf; ++k) {
+      uint32_t hits = __ballot_sync(0xffffffffu, f[k] != 0u);
+      const T *vk = vals + (int64_t)(w0 + k) * 32 + lane;
+      const int32_t *xb = kLev ? a.X + (int64_t)((w0 + k) * 32 + lane) * (a.tcap + 2) : nullptr;
+      const int xt = kLev ? __ldcg(xb + t) : 0;
+      while (hits) {  // uniform
+        T x[8];
 #pragma unroll
-    for (int k = 0; k < kHalf; ++k)
-      if (f[k]) S.pairs[pos++] = (uint16_t)((k << 5) | lane);
-    __syncwarp();
-    for (int i = 0; i < total; i += 8) {
-      T x[8];
-      int kk[8];
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        x[r] = (T)0;
-        kk[r] = -1;
-        if (i + r < total) {  // uniform
-          const int p = S.pairs[i + r];
-          const int k = p >> 5, j = p & 31;
-          const uint32_t fj = S.f[j][k];
-          const int32_t uj = __shfl_sync(0xffffffffu, u, j);
-          const int lj = kLev ? __shfl_sync(0xffffffffu, lvl, j) : 0;
-          if ((fj >> lane) & 1u) {
-            x[r] = __ldcg(vals + ((int64_t)uj * W + w0 + k) * 32 + lane);
-            if (kLev) {
-              const int32_t *xb = a.X + (int64_t)((w0 + k) * 32 + lane) * (a.tcap + 2);
-              const int sh = kLev == 1 ? __ldcg(xb + lj) - __ldcg(xb + t) : __ldcg(xb + t) - __ldcg(xb + lj);
-              x[r] = (T)ldexp((double)x[r], sh);
+        for (int r = 0; r < 8; ++r) {
+          x[r] = (T)0;
+          if (hits) {  // uniform
+            const int j = __ffs(hits) - 1;
+            hits &= hits - 1;
+            const uint32_t fj = __shfl_sync(0xffffffffu, f[k], j);
+            const int32_t uj = __shfl_sync(0xffffffffu, u, j);
+            const int lj = kLev ? __shfl_sync(0xffffffffu, lvl, j) : 0;
+            if ((fj >> lane) & 1u) {
+              x[r] = __ldcg(vk + (int64_t)uj * W * 32);
+              if (kLev) x[r] = (T)ldexp((double)x[r], kLev == 1 ? __ldcg(xb + lj) - xt : xt - __ldcg(xb + lj));
             }
           }
-          kk[r] = ((fj >> lane) & 1u) ? k : -1;
         }
-      }
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        if (kk[r] < 0) continue;
-        if (kComp) {
-          float2 *c = reinterpret_cast<float2 *>(&S.acc[kk[r]][lane]);
-          Comp32 cc;
-          cc.s = c->x;
-          cc.c = c->y;
-          cc.add((float)x[r]);
-          *c = make_float2(cc.s, cc.c);
-        } else {
-          S.acc[kk[r]][lane] += (double)x[r];
-        }
+        for (int r = 0; r < 8; ++r) acc[k].add((double)x[r]);
       }
     }
-    __syncwarp();
   }
-}
-
-__device__ __forceinline__ double acc_value(const WarpScratch &S, int k, int lane, bool comp) {
-  if (!comp) return S.acc[k][lane];
-  const float2 c = *reinterpret_cast<const float2 *>(&S.acc[k][lane]);
-  return (double)c.x + (double)c.y;
 }
 
 // Stores the result of one (vertex, word) of the forward step; returns the
@@ -695,25 +676,25 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
         uint32_t u_any = 0;
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) { unseen[k] = k < nw ? ~unseen[k] : 0u; any[k] = 0; u_any |= unseen[k]; }
-#pragma unroll
-        for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+        Acc<false> acc[kHalf];
         if (u_any && __ldcg(a.armed + v) <= t + 1) {  // uniform over the CTA
           const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
-          if (s0 < min(s1, sp)) row_pass<double, false, 0>(a, S, lmt, a.sig, s0, min(s1, sp), w0, nw, unseen, any, lane, t);
-          if (max(s0, sp) < s1) row_pass<double, false, 1>(a, S, a.lm, a.sig, max(s0, sp), s1, w0, nw, unseen, any, lane, t);
+          if (s0 < min(s1, sp)) row_pass<double, false, 0>(a, lmt, a.sig, s0, min(s1, sp), w0, nw, unseen, any, acc, lane, t);
+          if (max(s0, sp) < s1) row_pass<double, false, 1>(a, a.lm, a.sig, max(s0, sp), s1, w0, nw, unseen, any, acc, lane, t);
         }
 #pragma unroll
         for (int k = 0; k < kHalf; ++k) {
           any[k] = warp_or(any[k]);
-          if (lane == 0) S.f[0][k] = any[k];  // this warp's hit masks, for the combine
+          S.acc[k][lane] = acc[k].value();
+          if (lane == 0) S.any[k] = any[k];  // this warp's hit masks, for the combine
         }
         __syncthreads();
         for (int k = wib; k < nw; k += kWarpsPerCta) {  // fixed warp order
           double tot = 0.0;
           uint32_t mm = 0;
-          for (int x = 0; x < kWarpsPerCta; ++x) { tot += scratch[x].acc[k][lane]; mm |= scratch[x].f[0][k]; }
+          for (int x = 0; x < kWarpsPerCta; ++x) { tot += scratch[x].acc[k][lane]; mm |= scratch[x].any[k]; }
           a.hacc[((hc0 + c) * W + w0 + k) * 32 + lane] = tot;
           if (lane == 0) a.hmask[(hc0 + c) * W + w0 + k] = mm;
         }
@@ -747,16 +728,15 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) { unseen[k] = k < nw ? ~seen[k] : 0u; any[k] = 0; u_any |= unseen[k]; }
             if (!u_any) continue;
-#pragma unroll
-            for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-            if (e0 < sp) row_pass<double, false, 0>(a, S, lmt, a.sig, e0, sp, w0, nw, unseen, any, lane, t);
-            if (sp < e1) row_pass<double, false, 1>(a, S, a.lm, a.sig, sp, e1, w0, nw, unseen, any, lane, t);
+            Acc<false> acc[kHalf];
+            if (e0 < sp) row_pass<double, false, 0>(a, lmt, a.sig, e0, sp, w0, nw, unseen, any, acc, lane, t);
+            if (sp < e1) row_pass<double, false, 1>(a, a.lm, a.sig, sp, e1, w0, nw, unseen, any, acc, lane, t);
             int first = 0;
 #pragma unroll
             for (int k = 0; k < kHalf; ++k) {
               if (k >= nw) continue;
               const uint32_t m = warp_or(any[k]);
-              const int r = finish_pull(a, v, w0 + k, t, m, lane, S.acc[k][lane]);
+              const int r = finish_pull(a, v, w0 + k, t, m, lane, acc[k].value());
               nf += r & 255;
               first |= r >> 8;
               any[k] = m;
@@ -902,20 +882,21 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           any[k] = 0;
           a_any |= act[k];
         }
-#pragma unroll
-        for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
+        Acc<kComp> acc[kHalf];
         if (a_any) {  // uniform over the CTA
           const int64_t e0 = hce0[c], e1 = hce1[c], sp = HS[v];
           const int64_t per = (e1 - e0 + kWarpsPerCta - 1) / kWarpsPerCta;
           const int64_t s0 = e0 + wib * per, s1 = min(e1, s0 + per);
           if (lev < tlast && s0 < min(s1, sp))
-            row_pass<QT, kComp, 0>(a, S, lm_next, q, s0, min(s1, sp), w0, nw, act, any, lane, lev + 1);
-          if (max(s0, sp) < s1) row_pass<QT, kComp, 2>(a, S, a.lm, q, max(s0, sp), s1, w0, nw, act, any, lane, lev + 1, tlast);
+            row_pass<QT, kComp, 0>(a, lm_next, q, s0, min(s1, sp), w0, nw, act, any, acc, lane, lev + 1);
+          if (max(s0, sp) < s1) row_pass<QT, kComp, 2>(a, a.lm, q, max(s0, sp), s1, w0, nw, act, any, acc, lane, lev + 1, tlast);
         }
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = acc[k].value();
         __syncthreads();
         for (int k = wib; k < nw; k += kWarpsPerCta) {  // fixed warp order
           double tot = 0.0;
-          for (int x = 0; x < kWarpsPerCta; ++x) tot += acc_value(scratch[x], k, lane, kComp);
+          for (int x = 0; x < kWarpsPerCta; ++x) tot += scratch[x].acc[k][lane];
           a.hacc[((hc0 + c) * W + w0 + k) * 32 + lane] = tot;
         }
         __syncthreads();
@@ -952,14 +933,12 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
               a_any |= act[k];
             }
             if (!a_any) continue;
-#pragma unroll
-            for (int k = 0; k < kHalf; ++k) S.acc[k][lane] = 0.0;
-            if (lev < tlast && e0 < sp) row_pass<QT, kComp, 0>(a, S, lm_next, q, e0, sp, w0, nw, act, any, lane, lev + 1);
-            if (sp < e1) row_pass<QT, kComp, 2>(a, S, a.lm, q, sp, e1, w0, nw, act, any, lane, lev + 1, tlast);
+            Acc<kComp> acc[kHalf];
+            if (lev < tlast && e0 < sp) row_pass<QT, kComp, 0>(a, lm_next, q, e0, sp, w0, nw, act, any, acc, lane, lev + 1);
+            if (sp < e1) row_pass<QT, kComp, 2>(a, a.lm, q, sp, e1, w0, nw, act, any, acc, lane, lev + 1, tlast);
 #pragma unroll
             for (int k = 0; k < kHalf; ++k)
-              if (k < nw)
-                finish_dep<QT>(a, slots, rch, v, w0 + k, lev, act[k], lane, acc_value(S, k, lane, kComp), sp < e1);
+              if (k < nw) finish_dep<QT>(a, slots, rch, v, w0 + k, lev, act[k], lane, acc[k].value(), sp < e1);
           }
         }
       }
