@@ -310,7 +310,7 @@ __device__ __forceinline__ double end_dep(const Stretch &s, const End &A, const 
 // A task is one vertex row for kHalf 32-slot words: lane j loads arc j's
 // neighbour and its mask words (one aligned 16-byte load), then, word by
 // word, the arcs that hit (a ballot) are walked in arc order and their value
-// rows gathered eight at a time (lane = slot, coalesced) into per-(word,
+// rows gathered four at a time (lane = slot, coalesced) into per-(word,
 // slot) accumulators held in registers. Adds follow arc order, so sums are
 // deterministic.
 
@@ -394,9 +394,9 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
       const int32_t *xb = kLev ? a.X + (int64_t)((w0 + k) * 32 + lane) * (a.tcap + 2) : nullptr;
       const int xt = kLev ? __ldcg(xb + t) : 0;
       while (hits) {  // uniform
-        T x[8];
+        T x[4];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
+        for (int r = 0; r < 4; ++r) {
           x[r] = (T)0;
           if (hits) {  // uniform
             const int j = __ffs(hits) - 1;
@@ -411,7 +411,7 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
           }
         }
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[k].add((double)x[r]);
+        for (int r = 0; r < 4; ++r) acc[k].add((double)x[r]);
       }
     }
   }
