@@ -483,33 +483,54 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
     }
     const int cnt = (int)min((int64_t)32, c1 - base);
     for (int j0 = 0; j0 < cnt; j0 += kArcGroup) {
-      End B[kArcGroup];
-      Stretch st[kArcGroup];
-      int64_t ib[kArcGroup];
+      int32_t uj[kArcGroup], cj[kArcGroup], kj[kArcGroup], dB[kArcGroup];
+      int64_t pj[kArcGroup];
 #pragma unroll
-      for (int r = 0; r < kArcGroup; ++r) {
+      for (int r = 0; r < kArcGroup; ++r) {  // the far ends' levels, all in flight
         const int j = (j0 + r) & 31;
-        const int32_t uj = __shfl_sync(0xffffffffu, u, j);
-        const int32_t cj = __shfl_sync(0xffffffffu, cid, j);
-        const int32_t kj = __shfl_sync(0xffffffffu, k, j);
-        const int64_t pj = __shfl_sync(0xffffffffu, poff, j);
-        ib[r] = ((int64_t)uj * W + w) * 32 + lane;
-        B[r] = End{(live && j0 + r < cnt) ? __ldcg(a.d + ib[r]) : 0, 0, 1.0, 0.0};
-        const bool right = cj & 1;
-        const double *Pj = pj < 0 ? nullptr : a.cpre + pj;
-        st[r] = Stretch{Pj, 0, kj, right};
-        if (sl.chain == (cj >> 1)) {  // the source sits on this chain: the stretch ends at it
-          ib[r] = -1;
-          st[r] = right ? Stretch{Pj, sl.pos + 1, kj, true} : Stretch{Pj, 0, sl.pos, false};
-        }
+        uj[r] = __shfl_sync(0xffffffffu, u, j);
+        cj[r] = __shfl_sync(0xffffffffu, cid, j);
+        kj[r] = __shfl_sync(0xffffffffu, k, j);
+        pj[r] = __shfl_sync(0xffffffffu, poff, j);
+        dB[r] = (live && j0 + r < cnt) ? __ldcg(a.d + ((int64_t)uj[r] * W + w) * 32 + lane) : 0;
       }
 #pragma unroll
-      for (int r = 0; r < kArcGroup; ++r) {  // path counts of the far ends where the middle vertex ties
-        if (ib[r] < 0) B[r] = source_end();
-        if (live && j0 + r < cnt && end_needs_sigma(st[r].m(), A.d, B[r].d)) {
-          if (ib[r] >= 0) {
-            B[r].s = __ldcg(a.sig + ib[r]);
-            B[r].x = __ldcg(xb + B[r].d);
+      for (int r = 0; r < kArcGroup; ++r) {
+        if (!live || j0 + r >= cnt) continue;
+        const bool same = sl.chain == (cj[r] >> 1);  // the source sits on this chain
+        const int64_t ib = ((int64_t)uj[r] * W + w) * 32 + lane;
+        if (pj[r] < 0 && !same) {
+          // nothing hangs off the chain: prefix sums are positions; the
+          // vertices up to P = D/2 are fed from A, the one at D/2 ties when D is even
+          const int D = dB[r] + kj[r] - A.d - 1;
+          if (D < 0) continue;
+          const int P = D >> 1;
+          if ((D & 1) == 0 && P <= kj[r] - 1) {
+            if (!have_a) {
+              A.s = __ldcg(a.sig + iv);
+              A.x = __ldcg(xb + A.d);
+              have_a = true;
+            }
+            const double sb = __ldcg(a.sig + ib);
+            const int xbb = __ldcg(xb + dB[r]);
+            sum += (double)P + 1.0 / (1.0 + ldexp(sb / A.s, xbb - A.x));
+          } else {
+            sum += (double)(min(kj[r] - 1, P) + 1);
+          }
+          continue;
+        }
+        const bool right = cj[r] & 1;
+        const double *Pj = pj[r] < 0 ? nullptr : a.cpre + pj[r];
+        Stretch st{Pj, 0, kj[r], right};
+        End B{dB[r], 0, 1.0, 0.0};
+        if (same) {  // the stretch ends at the source
+          B = source_end();
+          st = right ? Stretch{Pj, sl.pos + 1, kj[r], true} : Stretch{Pj, 0, sl.pos, false};
+        }
+        if (end_needs_sigma(st.m(), A.d, B.d)) {
+          if (!same) {
+            B.s = __ldcg(a.sig + ib);
+            B.x = __ldcg(xb + B.d);
           }
           if (!have_a) {
             A.s = __ldcg(a.sig + iv);
@@ -517,10 +538,8 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
             have_a = true;
           }
         }
+        sum += end_dep(st, A, B);
       }
-#pragma unroll
-      for (int r = 0; r < kArcGroup; ++r)
-        if (live && j0 + r < cnt) sum += end_dep(st[r], A, B[r]);
     }
   }
   a.cdep[iv] = sum;
