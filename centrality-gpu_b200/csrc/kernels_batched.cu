@@ -141,7 +141,7 @@ struct Args {
   int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
   int32_t *armed;   // [n_cap] first level on which some slot can reach the vertex (a neighbour was reached)
   int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
-  double *bcpart;   // [nb_cap][W] every vertex of the BCC (chain vertices included)
+  double *bcpart;   // [n_cap][W] BC partials of the core vertices
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
   double *wsrc;     // [B] reach(source)+1 of each slot of the pass
   int32_t *X;       // [B][tcap+2]
@@ -981,89 +981,112 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
       PHASE_COUNT(17);
     }
 
-    // ---- chain vertices: one warp per (chain, word), every vertex of the chain
+    // ---- chain vertices: one warp per chain, every word; each lane sums its
+    // slots' contributions over the words (registers for chains of up to
+    // kRegVerts vertices), then one warp reduction per chain vertex goes
+    // straight into BC (one writer per vertex: fixed order)
     {
+      constexpr int kRegVerts = 8;
+      const int bad = *(volatile int *)&a.ctrl->range_err;
       const int64_t ch0 = a.chain_off[bt.bcc];
       const int64_t nch = a.chain_off[bt.bcc + 1] - ch0;
-      for (int64_t task = gwarp(); task < nch * words; task += nwarps()) {
-        const int64_t c = ch0 + task / words;
-        const int w = (int)(task % words);
-        const int b = w * 32 + lane;
-        const bool live = b < bt.nslots;
+      for (int64_t task = gwarp(); task < nch; task += nwarps()) {
+        const int64_t c = ch0 + task;
         const int32_t L = a.chain_l[c], R = a.chain_r[c], cs = a.chain_start[c], k = a.chain_len[c];
         const int64_t poff = a.cpre_off[c];
         const double *P = poff < 0 ? nullptr : a.cpre + poff;
-        const int64_t iL = ((int64_t)L * W + w) * 32 + lane, iR = ((int64_t)R * W + w) * 32 + lane;
-        End eL{0, 0, 1.0, 0.0}, eR{0, 0, 1.0, 0.0};
-        Slot sl{0, -1, 0, 0};
-        int on = -1;
-        if (live) {  // the ends' levels, then only the path counts / q the closed forms use
-          eL.d = __ldcg(a.d + iL);
-          eR.d = __ldcg(a.d + iR);
-          sl = slots[b];
-          on = sl.chain == c ? sl.pos : -1;
-          // stretches: [L, R] or, with the source on the chain, [L, source] and [source, R]
-          const int mL = on < 0 ? k : on, dBL = on < 0 ? eR.d : 0;   // stretch seen from L
-          const int mR = on < 0 ? k : k - 1 - on, dBR = on < 0 ? eL.d : 0;  // stretch seen from R
-          const int DL = dBL + mL - eL.d - 1, DR = dBR + mR - eR.d - 1;
-          const bool tieL = mL > 0 && DL >= 0 && (DL & 1) == 0 && DL / 2 <= mL - 1;
-          const bool tieR = mR > 0 && DR >= 0 && (DR & 1) == 0 && DR / 2 <= mR - 1;
-          // B's paths through the stretch: R fed via the chain from L, or L from R
-          const bool viaL = on < 0 && eR.d == eL.d + k + 1, viaR = on < 0 && eL.d == eR.d + k + 1;
-          const bool srcL = on >= 0 && eL.d == on + 1, srcR = on >= 0 && eR.d == k - on;  // fed from the source
-          const int32_t *xb = a.X + (int64_t)b * (a.tcap + 2);
-          const QT *qq = reinterpret_cast<const QT *>(a.q);
-          if (tieL || tieR || viaL || viaR) {
-            eL.s = __ldcg(a.sig + iL);
-            eL.x = __ldcg(xb + eL.d);
-            eR.s = __ldcg(a.sig + iR);
-            eR.x = __ldcg(xb + eR.d);
-          }
-          if (viaR || srcL) {
-            eL.qs = (double)__ldcg(qq + iL);
-            if (!(tieL || tieR || viaL || viaR)) eL.x = __ldcg(xb + eL.d);
-          }
-          if (viaL || srcR) {
-            eR.qs = (double)__ldcg(qq + iR);
-            if (!(tieL || tieR || viaL || viaR)) eR.x = __ldcg(xb + eR.d);
-          }
-        }
-        const double wsrc = live ? a.wsrc[b] : 0.0;
-        // Source off the chain (the common case), in prefix sums from L:
-        // vertex j is fed from L iff 2j <= D; a tie vertex t = D/2 shares its
-        // reach+1 between the sides in proportion to sigma_L, sigma_R; else
-        // the L-fed vertices end at pl, and the far end's q enters when the
-        // chain carries its shortest paths.
-        int D = 0, tv = -1, pl = -1;
-        double fL = 0.0, fR = 0.0;  // L-side and R-side constants
-        if (live && on < 0) {
-          D = eR.d + k - eL.d - 1;
-          if (D >= 0 && (D & 1) == 0 && D / 2 <= k - 1) {
-            tv = D / 2;
-            const double p0 = chain_pre(P, tv), p1 = chain_pre(P, tv + 1), w = p1 - p0;
-            fL = p0 + w / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
-            fR = -p1 + w / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
-          } else {
-            pl = D >= 0 ? min(k - 1, D / 2) : -1;
-            const double p1 = chain_pre(P, pl + 1);
-            fL = p1 + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
-            fR = -p1 + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
-          }
-        }
-        for (int j = 0; j < k; ++j) {
-          double dep = 0.0;
-          if (live) {
-            if (on < 0) {
-              const bool from_l = tv >= 0 ? j < tv : j <= pl;
-              if (j != tv) dep = from_l ? fL - chain_pre(P, j + 1) : chain_pre(P, j) + fR;
-            } else if (j < on) {
-              dep = stretch_dep(Stretch{P, 0, on, false}, j, eL, source_end());
-            } else if (j > on) {
-              dep = stretch_dep(Stretch{P, on + 1, k, false}, j - on - 1, source_end(), eR);
+        double part[kRegVerts];
+#pragma unroll
+        for (int j = 0; j < kRegVerts; ++j) part[j] = 0.0;
+        for (int w = 0; w < words; ++w) {
+          const int b = w * 32 + lane;
+          const bool live = b < bt.nslots;
+          const int64_t iL = ((int64_t)L * W + w) * 32 + lane, iR = ((int64_t)R * W + w) * 32 + lane;
+          End eL{0, 0, 1.0, 0.0}, eR{0, 0, 1.0, 0.0};
+          int on = -1;
+          if (live) {  // the ends' levels, then only the path counts / q the closed forms use
+            eL.d = __ldcg(a.d + iL);
+            eR.d = __ldcg(a.d + iR);
+            const Slot sl = slots[b];
+            on = sl.chain == c ? sl.pos : -1;
+            // stretches: [L, R] or, with the source on the chain, [L, source] and [source, R]
+            const int mL = on < 0 ? k : on, dBL = on < 0 ? eR.d : 0;           // seen from L
+            const int mR = on < 0 ? k : k - 1 - on, dBR = on < 0 ? eL.d : 0;  // seen from R
+            const int DL = dBL + mL - eL.d - 1, DR = dBR + mR - eR.d - 1;
+            const bool tieL = mL > 0 && DL >= 0 && (DL & 1) == 0 && DL / 2 <= mL - 1;
+            const bool tieR = mR > 0 && DR >= 0 && (DR & 1) == 0 && DR / 2 <= mR - 1;
+            // B's paths through the stretch: R fed via the chain from L, or L from R
+            const bool viaL = on < 0 && eR.d == eL.d + k + 1, viaR = on < 0 && eL.d == eR.d + k + 1;
+            const bool srcL = on >= 0 && eL.d == on + 1, srcR = on >= 0 && eR.d == k - on;  // fed from the source
+            const int32_t *xb = a.X + (int64_t)b * (a.tcap + 2);
+            const QT *qq = reinterpret_cast<const QT *>(a.q);
+            const bool sig = tieL || tieR || viaL || viaR;
+            if (sig) {
+              eL.s = __ldcg(a.sig + iL);
+              eL.x = __ldcg(xb + eL.d);
+              eR.s = __ldcg(a.sig + iR);
+              eR.x = __ldcg(xb + eR.d);
+            }
+            if (viaR || srcL) {
+              eL.qs = (double)__ldcg(qq + iL);
+              if (!sig) eL.x = __ldcg(xb + eL.d);
+            }
+            if (viaL || srcR) {
+              eR.qs = (double)__ldcg(qq + iR);
+              if (!sig) eR.x = __ldcg(xb + eR.d);
             }
           }
-          const double tot = warp_sum(dep * wsrc);
-          if (lane == 0) a.bcpart[(int64_t)(cs + j) * W + w] = tot;
+          const double wsrc = live ? a.wsrc[b] : 0.0;
+          // Source off the chain (the common case), in prefix sums from L:
+          // vertex j is fed from L iff 2j <= D; a tie vertex t = D/2 shares
+          // its reach+1 between the sides in proportion to sigma_L, sigma_R;
+          // else the L-fed vertices end at pl, and the far end's q enters
+          // when the chain carries its shortest paths.
+          int tv = -1, pl = -1;
+          double fL = 0.0, fR = 0.0;  // L-side and R-side constants
+          if (live && on < 0) {
+            const int D = eR.d + k - eL.d - 1;
+            if (D >= 0 && (D & 1) == 0 && D / 2 <= k - 1) {
+              tv = D / 2;
+              const double p0 = chain_pre(P, tv), p1 = chain_pre(P, tv + 1), wt = p1 - p0;
+              fL = p0 + wt / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
+              fR = -p1 + wt / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
+            } else {
+              pl = D >= 0 ? min(k - 1, D / 2) : -1;
+              const double p1 = chain_pre(P, pl + 1);
+              fL = p1 + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
+              fR = -p1 + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
+            }
+          }
+          auto dep_of = [&](int j) -> double {
+            if (!live) return 0.0;
+            if (on < 0) {
+              if (j == tv) return 0.0;
+              const bool from_l = tv >= 0 ? j < tv : j <= pl;
+              return (from_l ? fL - chain_pre(P, j + 1) : chain_pre(P, j) + fR) * wsrc;
+            }
+            if (j < on) return stretch_dep(Stretch{P, 0, on, false}, j, eL, source_end()) * wsrc;
+            if (j > on) return stretch_dep(Stretch{P, on + 1, k, false}, j - on - 1, source_end(), eR) * wsrc;
+            return 0.0;
+          };
+          if (k <= kRegVerts) {
+#pragma unroll
+            for (int j = 0; j < kRegVerts; ++j)
+              if (j < k) part[j] += dep_of(j);
+          } else {
+            for (int j = 0; j < k; ++j) {
+              const double tot = warp_sum(dep_of(j));
+              if (lane == 0 && !bad) a.bc[vo + cs + j] += tot;
+            }
+          }
+        }
+        if (k <= kRegVerts) {
+#pragma unroll
+          for (int j = 0; j < kRegVerts; ++j) {
+            if (j >= k) continue;
+            const double tot = warp_sum(part[j]);
+            if (lane == 0 && !bad) a.bc[vo + cs + j] += tot;
+          }
         }
       }
     }
@@ -1075,7 +1098,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     if (bad) {
       if (gtid == 0) a.redo[bi] = 1;
     } else {
-      for (int64_t v = gtid; v < nb; v += gthreads) {
+      for (int64_t v = gtid; v < n; v += gthreads) {  // core vertices (chain vertices were added above)
         double s = 0.0;
         for (int w = 0; w < words; ++w) s += a.bcpart[v * W + w];
         a.bc[vo + v] += s;
@@ -1160,7 +1183,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   std::vector<int32_t> heavy, hchunk_v, hfirst;
   std::vector<int32_t> dist, queue;
   std::vector<int32_t> cof, cpos;  // chain vertex -> chain (global), position
-  int64_t ncap = 1, nbcap = 1;
+  int64_t ncap = 1;
   int tcap = 2;
   cpre_off.resize((size_t)B->n_chains);
   for (int32_t b = 0; b < B->n_bcc; ++b) {
@@ -1176,7 +1199,6 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
       continue;
     }
     ncap = std::max<int64_t>(ncap, npl);
-    nbcap = std::max<int64_t>(nbcap, nb);
     const int64_t arcs = B->row[vo + nb] - B->row[vo];
     // chain membership, and the shape the closed forms rely on: each chain
     // vertex has exactly its two chain neighbours, the ends are distinct core vertices
@@ -1345,7 +1367,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   const int64_t qb = P->f32 ? 4 : 8;
   const int64_t nch = (int64_t)hchunk_v.size();
   const int64_t need = n * W * 32 * (4 + 8 + 8 + qb) + (int64_t)(tcap + 2) * n * W * 4 + n * W * 4 + n * 12 +
-                       nbcap * W * 8 + (int64_t)W * 32 * (tcap + 2) * 4 + nch * W * 32 * 8;
+                       n * W * 8 + (int64_t)W * 32 * (tcap + 2) * 4 + nch * W * 32 * 8;
   if (need > cfg.limit_bytes)
     return bail(BCGPU_ENOMEM, "batched workspace " + std::to_string(need >> 20) + " MiB exceeds the limit " +
                                   std::to_string(cfg.limit_bytes >> 20) + " MiB (lower the batch width)");
@@ -1368,7 +1390,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.armed = (int32_t *)p;
   ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
-  ok &= ok && alloc(&p, nbcap * W * 8); a.bcpart = (double *)p;
+  ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 8); a.wsrc = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * (tcap + 2) * 4); a.X = (int32_t *)p;
