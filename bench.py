@@ -269,6 +269,9 @@ def main():
     ap.add_argument("--plain-waves", type=int, default=2,
                     help="batched runs: also time the plain FP64 schedule on this many full waves of its work "
                          "items (one item per resident CTA), the denominator of batched vs plain (0 = skip)")
+    ap.add_argument("--graph", type=int, choices=[0, 1], default=1,
+                    help="1: every step is one launch of a CUDA graph of the step's device work, recorded "
+                         "(stream capture, nothing runs) before the warm-up; 0: the work is enqueued directly")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
     args = ap.parse_args()
@@ -309,7 +312,7 @@ def main():
         tctx.close()
         tuned = {str(k): round(v, 2) for k, v in per.items()}
     ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
-                    workspace_limit=int(args.workspace_gb * 2**30))
+                    workspace_limit=int(args.workspace_gb * 2**30), graph=bool(args.graph))
     plan = ctx.plan(d)
     target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
     ranges = step_ranges(plan, target)
@@ -319,6 +322,9 @@ def main():
     # steps evenly spaced over the whole source order (passes differ by region)
     pick = np.linspace(0, len(mine) - 1, num=need).round().astype(int) if len(mine) >= need else np.arange(need) % len(mine)
     sel = [mine[i] for i in pick]
+    if args.graph:  # record each step's graph up front (capture only: no device work runs)
+        for r0, r1 in dict.fromkeys(sel):
+            plan.record(r0, r1)
 
     for r0, r1 in sel[:args.warmup]:
         plan.run(r0, r1, stats=False)
@@ -424,6 +430,7 @@ def main():
                        "units_per_step": float(np.mean([r1 - r0 for r0, r1 in sel])),
                        "host_decomposition_s": round(host_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
                        "batch_width": st.get("batch_width"), "autotune_gteps": tuned,
+                       "cuda_graph": bool(args.graph),
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "plain": plain,

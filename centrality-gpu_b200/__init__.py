@@ -40,7 +40,7 @@ _f32p = C.POINTER(C.c_float)
 class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
                 ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
-                ("plain_core", C.c_int32)]
+                ("plain_core", C.c_int32), ("graph", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -93,6 +93,7 @@ _SIGS = {
     "bc_plan_unit_sources": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_int64]),
     "bc_plan_reset": (C.c_int, [C.c_void_p]),
     "bc_plan_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(BcStats)]),
+    "bc_plan_record": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
     "bc_plan_read": (C.c_int, [C.c_void_p, _f64p]),
     "bc_plan_source_rows": (C.c_int, [C.c_void_p, C.c_int64, _i32p, _f64p]),
     "bc_graph_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
@@ -236,7 +237,7 @@ class Context:
     _live = weakref.WeakSet()
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
-                 workspace_limit=0, rescale_exp=0, plain_core=0):
+                 workspace_limit=0, rescale_exp=0, plain_core=0, graph=False):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
@@ -244,6 +245,7 @@ class Context:
         o.workspace_limit = workspace_limit
         o.rescale_exp = rescale_exp
         o.plain_core = plain_core
+        o.graph = 1 if graph else 0
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:
@@ -349,6 +351,11 @@ class Plan:
         st = BcStats() if stats else None
         self.ctx._check(lib().bc_plan_run(self._h, begin, end, C.byref(st) if stats else None))
         return st.as_dict() if stats else None
+
+    def record(self, begin=0, end=None):
+        """Graph mode: records units [begin, end) into a CUDA graph without running it."""
+        end = self.n_units if end is None else end
+        self.ctx._check(lib().bc_plan_record(self._h, begin, end))
 
     def read(self):
         out = np.zeros(self.decomp.view.contents.n_orig, dtype=np.float64)

@@ -16,6 +16,7 @@ struct BatchedConfig {
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
   const std::vector<char> *bccs_on = nullptr;  // BCCs this plan schedules (null: all)
+  const std::vector<int32_t> *ecc0 = nullptr;  // per BCC: eccentricity of local vertex 0 if known (< 0: compute)
 };
 
 struct BatchedPlan;

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <set>
 #include <string>
@@ -67,6 +68,12 @@ struct bc_plan {
   std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux, unit_visits;
   int64_t device_bytes = 0;
   std::vector<void *> allocs;
+  // graph mode: instantiated graph and kernel-launch count per recorded unit range
+  struct Recorded {
+    cudaGraphExec_t exec;
+    int launches;
+  };
+  std::map<std::pair<int64_t, int64_t>, Recorded> graphs;
 };
 
 namespace {
@@ -146,32 +153,47 @@ int validate(bc_ctx *ctx, const bc_bccs *B) {
   if (B->vtx_off[0] != 0 || B->vtx_off[B->n_bcc] != B->n_packed || B->row[0] != 0 || B->row[B->n_packed] != B->n_arcs ||
       B->chain_off[0] != 0 || B->chain_off[B->n_bcc] != B->n_chains)
     return fail(ctx, BCGPU_EINVAL, "inconsistent bccs totals");
+  // per BCC: the first failing check in the order below (0 = none); the
+  // lowest failing BCC is reported, as a sequential scan would
+  static const char *const kWhat[] = {"", "BCC size out of range", "n_plain out of range", "chain out of range",
+                                      "chains must be sorted by left endpoint",
+                                      "chain vertices do not cover the non-plain ids", "orig/reach out of range",
+                                      "row offsets decrease", "negative column id", "column id outside its BCC"};
+  std::vector<int8_t> bad((size_t)B->n_bcc, 0);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
-    if (nb < 3 || nb > INT32_MAX - 4) return fail(ctx, BCGPU_EINVAL, "BCC size out of range");
-    if (B->n_plain[b] < 1 || B->n_plain[b] > nb) return fail(ctx, BCGPU_EINVAL, "n_plain out of range");
+    if (nb < 3 || nb > INT32_MAX - 4) { bad[b] = 1; continue; }
+    if (B->n_plain[b] < 1 || B->n_plain[b] > nb) { bad[b] = 2; continue; }
     int64_t ch = 0;
-    for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) {
+    for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1] && !bad[b]; ++c) {
       if (B->chain_start[c] < B->n_plain[b] || B->chain_len[c] < 1 || B->chain_start[c] + B->chain_len[c] > nb ||
           B->chain_l[c] < 0 || B->chain_l[c] >= B->n_plain[b] || B->chain_r[c] < 0 || B->chain_r[c] >= B->n_plain[b])
-        return fail(ctx, BCGPU_EINVAL, "chain out of range");
-      if (c > B->chain_off[b] && B->chain_l[c] < B->chain_l[c - 1])
-        return fail(ctx, BCGPU_EINVAL, "chains must be sorted by left endpoint");
+        bad[b] = 3;
+      else if (c > B->chain_off[b] && B->chain_l[c] < B->chain_l[c - 1])
+        bad[b] = 4;
       ch += B->chain_len[c];
     }
-    if (ch != nb - B->n_plain[b]) return fail(ctx, BCGPU_EINVAL, "chain vertices do not cover the non-plain ids");
+    if (bad[b]) continue;
+    if (ch != nb - B->n_plain[b]) { bad[b] = 5; continue; }
     for (int64_t k = B->vtx_off[b]; k < B->vtx_off[b + 1]; ++k) {
-      if (B->orig[k] < 0 || B->orig[k] >= B->n_orig || B->reach[k] < 0)
-        return fail(ctx, BCGPU_EINVAL, "orig/reach out of range");
-      if (B->row[k + 1] < B->row[k]) return fail(ctx, BCGPU_EINVAL, "row offsets decrease");
+      if (B->orig[k] < 0 || B->orig[k] >= B->n_orig || B->reach[k] < 0) { bad[b] = 6; break; }
+      if (B->row[k + 1] < B->row[k]) { bad[b] = 7; break; }
     }
   }
-  for (int64_t e = 0; e < B->n_arcs; ++e)
-    if (B->col[e] < 0) return fail(ctx, BCGPU_EINVAL, "negative column id");
+  for (int32_t b = 0; b < B->n_bcc; ++b)
+    if (bad[b]) return fail(ctx, BCGPU_EINVAL, kWhat[bad[b]]);
+  int neg = 0;
+#pragma omp parallel for schedule(static) reduction(| : neg)
+  for (int64_t e = 0; e < B->n_arcs; ++e) neg |= B->col[e] < 0;
+  if (neg) return fail(ctx, BCGPU_EINVAL, kWhat[8]);
+  int out = 0;
   for (int32_t b = 0; b < B->n_bcc; ++b) {
-    int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
-    for (int64_t e = B->row[B->vtx_off[b]]; e < B->row[B->vtx_off[b + 1]]; ++e)
-      if (B->col[e] >= nb) return fail(ctx, BCGPU_EINVAL, "column id outside its BCC");
+    const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+    const int64_t e0 = B->row[B->vtx_off[b]], e1 = B->row[B->vtx_off[b + 1]];
+#pragma omp parallel for schedule(static) reduction(| : out) if (e1 - e0 > (1 << 16))
+    for (int64_t e = e0; e < e1; ++e) out |= B->col[e] >= nb;
+    if (out) return fail(ctx, BCGPU_EINVAL, kWhat[9]);
   }
   return BCGPU_OK;
 }
@@ -268,16 +290,24 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
 
   // BATCHED: which BCCs take multi-source passes (the others: per-source items)
   std::vector<char> on;
+  std::vector<int32_t> ecc0;  // eccentricity of each BCC's local vertex 0 (the batched plan reuses it)
   int64_t n_on = 0;
   if (p->mode == BCGPU_MODE_BATCHED) {
     on.assign((size_t)B->n_bcc, 1);
+    ecc0.assign((size_t)B->n_bcc, -1);
     if (ctx->opts.plain_core >= 0) {
       const int32_t min_core = ctx->opts.plain_core > 0 ? ctx->opts.plain_core : kBatchedMinCore;
-      std::vector<int32_t> dist, queue;
-      for (int32_t b = 0; b < B->n_bcc; ++b) {
-        int kmax = 0;
-        for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) kmax = std::max(kmax, B->chain_len[c]);
-        on[b] = B->n_plain[b] >= min_core && 2 * bcc_ecc0(B, b, dist, queue) + kmax <= kBatchedMaxLevels;
+#pragma omp parallel
+      {
+        std::vector<int32_t> dist, queue;
+#pragma omp for schedule(dynamic, 1)
+        for (int32_t b = 0; b < B->n_bcc; ++b) {
+          if (B->n_plain[b] < min_core) { on[b] = 0; continue; }
+          int kmax = 0;
+          for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) kmax = std::max(kmax, B->chain_len[c]);
+          ecc0[b] = bcc_ecc0(B, b, dist, queue);
+          on[b] = 2 * ecc0[b] + kmax <= kBatchedMaxLevels;
+        }
       }
     }
     for (char x : on) n_on += x;
@@ -297,6 +327,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     cfg.limit_bytes = limit - p->device_bytes;
     cfg.rescale_exp = ctx->opts.rescale_exp;
     cfg.bccs_on = &on;
+    cfg.ecc0 = &ecc0;
     std::string msg;
     rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
@@ -489,6 +520,7 @@ extern "C" void bc_plan_destroy(bc_plan *p) {
   p->ctx->plans.erase(p);
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
+  for (auto &g : p->graphs) cudaGraphExecDestroy(g.second.exec);
   if (p->bp) bcg::batched_destroy(p->bp);
   for (void *a : p->allocs) cudaFree(a);
   delete p;
@@ -537,17 +569,15 @@ extern "C" int bc_plan_reset(bc_plan *p) {
   return BCGPU_OK;
 }
 
-extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *stats) {
-  if (!p) return BCGPU_EINVAL;
+namespace {
+
+// The device work of units [begin, end) (range already checked), enqueued on
+// the context's stream: the multi-source passes, then the per-source items.
+int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
   bc_ctx *ctx = p->ctx;
-  const int64_t n = bc_plan_num_units(p);
-  if (begin < 0 || end < begin || end > n) return fail(ctx, BCGPU_EINVAL, "unit range out of bounds");
-  CK(ctx, cudaSetDevice(ctx->device));
-  int launches = 0;
-  if (stats) CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   if (p->bp && begin < p->n_bat) {  // multi-source passes
     std::string msg;
-    int rc = bcg::batched_run(p->bp, begin, std::min(end, p->n_bat), ctx->stream, &launches, &msg);
+    int rc = bcg::batched_run(p->bp, begin, std::min(end, p->n_bat), ctx->stream, launches, &msg);
     if (rc) return fail(ctx, rc, "batched run: " + msg);
   }
   const int64_t i0 = std::max(begin, p->n_bat) - p->n_bat, i1 = end - p->n_bat;
@@ -561,7 +591,79 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
     a.err = p->err;
     const int grid = (int)std::min<int64_t>(p->grid, i1 - i0);
     CK(ctx, bcg::launch_plain(a, p->block, grid, ctx->stream));
-    ++launches;
+    ++*launches;
+  }
+  return BCGPU_OK;
+}
+
+// Captures enqueue_units of the range into a graph and instantiates it (the
+// capture records the work; nothing runs).
+int record_units(bc_plan *p, int64_t begin, int64_t end, bc_plan::Recorded *out) {
+  bc_ctx *ctx = p->ctx;
+  CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int launches = 0;
+  const int rc = enqueue_units(p, begin, end, &launches);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc ? rc : cuda_fail(ctx, e, "cudaStreamEndCapture");
+  }
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+  *out = bc_plan::Recorded{ex, launches};
+  return BCGPU_OK;
+}
+
+int check_range(bc_plan *p, int64_t begin, int64_t end) {
+  const int64_t n = bc_plan_num_units(p);
+  if (begin < 0 || end < begin || end > n) return fail(p->ctx, BCGPU_EINVAL, "unit range out of bounds");
+  return BCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int bc_plan_record(bc_plan *p, int64_t begin, int64_t end) {
+  if (!p) return BCGPU_EINVAL;
+  bc_ctx *ctx = p->ctx;
+  if (!ctx->opts.graph) return fail(ctx, BCGPU_EINVAL, "bc_plan_record needs a context with bc_opts.graph set");
+  int rc = check_range(p, begin, end);
+  if (rc) return rc;
+  CK(ctx, cudaSetDevice(ctx->device));
+  bc_plan::Recorded r{};
+  if ((rc = record_units(p, begin, end, &r))) return rc;
+  auto it = p->graphs.find({begin, end});
+  if (it != p->graphs.end()) {
+    CK(ctx, cudaStreamSynchronize(ctx->stream));  // the old graph may still be running
+    cudaGraphExecDestroy(it->second.exec);
+    it->second = r;
+  } else {
+    p->graphs.emplace(std::make_pair(begin, end), r);
+  }
+  return BCGPU_OK;
+}
+
+extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *stats) {
+  if (!p) return BCGPU_EINVAL;
+  bc_ctx *ctx = p->ctx;
+  int rc = check_range(p, begin, end);
+  if (rc) return rc;
+  CK(ctx, cudaSetDevice(ctx->device));
+  int launches = 0;
+  if (ctx->opts.graph) {
+    auto it = p->graphs.find({begin, end});
+    if (it == p->graphs.end()) {
+      if ((rc = bc_plan_record(p, begin, end))) return rc;
+      it = p->graphs.find({begin, end});
+    }
+    if (stats) CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+    launches = it->second.launches;
+  } else {
+    if (stats) CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((rc = enqueue_units(p, begin, end, &launches))) return rc;
   }
   if (stats) {
     CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));

@@ -1178,7 +1178,7 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   std::vector<double> cpre;
   std::vector<Slot> slots;
   std::vector<Seed> seeds;
-  std::vector<int2> arms, arm_tmp;
+  std::vector<int2> arms;
   std::vector<int64_t> heavy_off{0}, hchunk_off{0}, hchunk_e0, hchunk_e1;
   std::vector<int32_t> heavy, hchunk_v, hfirst;
   std::vector<int32_t> dist, queue;
@@ -1235,29 +1235,49 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     // contracted rows: unit arcs first, then chain arcs
     hvo.push_back((int64_t)hrow.size());
     const int heavy_deg = npl < kSmallCore ? kHeavyDegSmall : kHeavyDeg;
-    int32_t hidx = 0;
+    // Every arc of a core vertex becomes one contracted arc (a unit arc, or
+    // the chain arc of the chain vertex it leads to), so the contracted rows
+    // have the original degrees: offsets first, then the rows in parallel.
+    const size_t rb = hrow.size();
+    hrow.resize(rb + (size_t)npl + 1);
+    hsplit.resize(rb + (size_t)npl + 1);
+    hrow[rb] = (int64_t)hcol.size();
+    for (int32_t x = 0; x < npl; ++x) hrow[rb + x + 1] = hrow[rb + x] + (B->row[vo + x + 1] - B->row[vo + x]);
+    hsplit[rb + npl] = hrow[rb + npl];
+    hcol.resize((size_t)hrow[rb + npl]);
+    hk.resize(hcol.size());
+    hcid.resize(hcol.size());
+    int row_bad = 0;
+#pragma omp parallel for schedule(dynamic, 2048) reduction(| : row_bad)
     for (int32_t x = 0; x < npl; ++x) {
-      const int64_t r0 = (int64_t)hcol.size();
-      hrow.push_back(r0);
       const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
+      int64_t o = hrow[rb + x];
       for (int64_t e = e0; e < e1; ++e)
-        if (B->col[e] < npl) { hcol.push_back(B->col[e]); hk.push_back(0); hcid.push_back(-1); }
-      hsplit.push_back((int64_t)hcol.size());
+        if (B->col[e] < npl) { hcol[o] = B->col[e]; hk[o] = 0; hcid[o] = -1; ++o; }
+      hsplit[rb + x] = o;
       for (int64_t e = e0; e < e1; ++e) {
         const int32_t y = B->col[e];
         if (y < npl) continue;
         const int64_t c = cof[y];
-        if (c < 0) return bail(BCGPU_EINVAL, "a non-core vertex outside every chain");
+        if (c < 0) { row_bad |= 1; continue; }
         const int32_t k = B->chain_len[c];
         int right;
         if (x == B->chain_l[c] && cpos[y] == 0) right = 0;
         else if (x == B->chain_r[c] && cpos[y] == k - 1) right = 1;
-        else return bail(BCGPU_EINVAL, "a core vertex adjacent to the inside of a chain");
-        hcol.push_back(right ? B->chain_l[c] : B->chain_r[c]);
-        hk.push_back(k);
-        hcid.push_back((int32_t)(c * 2 + right));
+        else { row_bad |= 2; continue; }
+        hcol[o] = right ? B->chain_l[c] : B->chain_r[c];
+        hk[o] = k;
+        hcid[o] = (int32_t)(c * 2 + right);
+        ++o;
       }
-      const int64_t r1 = (int64_t)hcol.size();
+    }
+    if (row_bad & 1) return bail(BCGPU_EINVAL, "a non-core vertex outside every chain");
+    if (row_bad & 2) return bail(BCGPU_EINVAL, "a core vertex adjacent to the inside of a chain");
+    hrow.pop_back();  // the BCC's end offset is pushed below, after its heavy rows
+    hsplit.pop_back();
+    int32_t hidx = 0;
+    for (int32_t x = 0; x < npl; ++x) {
+      const int64_t r0 = hrow[rb + x], r1 = x + 1 < npl ? hrow[rb + x + 1] : (int64_t)hcol.size();
       if (r1 - r0 <= heavy_deg) continue;
       heavy.push_back(x);
       hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
@@ -1273,7 +1293,8 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
     hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
     heavy_off.push_back((int64_t)heavy.size());
     hchunk_off.push_back((int64_t)hchunk_v.size());
-    tcap = std::max(tcap, 2 * bcc_ecc(B->row, B->col, vo, nb, dist, queue) + kmax + 3);
+    const int32_t ecc = cfg.ecc0 && (*cfg.ecc0)[b] >= 0 ? (*cfg.ecc0)[b] : bcc_ecc(B->row, B->col, vo, nb, dist, queue);
+    tcap = std::max(tcap, 2 * ecc + kmax + 3);
 
     // Source order: bounded BFS balls of nearby vertices (chain vertices
     // included), so a pass's sources see every vertex within a narrow band of
@@ -1309,42 +1330,70 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
         ++ball;
       }
     }
-    for (size_t i0 = 0; i0 < order.size(); i0 += (size_t)width) {
-      const size_t i1 = std::min(order.size(), i0 + (size_t)width);
+    // Passes of `width` consecutive sources of the order. Slots and seeds are
+    // sized up front (a chain source has two seeds), then every pass fills
+    // its own ranges in parallel; the arming lists (variable length after
+    // deduplication) are built per pass and concatenated in pass order.
+    const int64_t nbat = ((int64_t)order.size() + width - 1) / width;
+    const size_t bat0 = P->h_batches.size(), slot0 = slots.size(), seed0 = seeds.size();
+    std::vector<int64_t> seed_at((size_t)nbat + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < nbat; ++j) {
+      const size_t i0 = (size_t)j * width, i1 = std::min(order.size(), i0 + (size_t)width);
+      int64_t cnt = 0;
+      for (size_t i = i0; i < i1; ++i) cnt += order[i] >= npl ? 2 : 0;
+      seed_at[j + 1] = cnt;
+    }
+    for (int64_t j = 0; j < nbat; ++j) seed_at[j + 1] += seed_at[j];
+    P->h_batches.resize(bat0 + (size_t)nbat);
+    slots.resize(slot0 + order.size());
+    seeds.resize(seed0 + (size_t)seed_at[nbat]);
+    std::vector<std::vector<int2>> arm_of((size_t)nbat);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nbat; ++j) {
+      const size_t i0 = (size_t)j * width, i1 = std::min(order.size(), i0 + (size_t)width);
       Batch bt{};
       bt.bcc = b;
       bt.nslots = (int32_t)(i1 - i0);
       bt.words = (bt.nslots + 31) / 32;
       bt.kmax = kmax;
       bt.heavy_deg = heavy_deg;
-      bt.slot_off = (int64_t)slots.size();
-      bt.seed_off = (int64_t)seeds.size();
+      bt.slot_off = (int64_t)(slot0 + i0);
+      bt.seed_off = (int64_t)seed0 + seed_at[j];
+      int64_t sd = bt.seed_off;
+      std::vector<int2> &arm = arm_of[j];
+      arm.reserve((size_t)bt.nslots * 2);
       for (size_t i = i0; i < i1; ++i) {
         const int32_t s = order[i];
         const int32_t slot = (int32_t)(i - i0);
         if (s < npl) {
-          slots.push_back(Slot{s, -1, 0, 0});
+          slots[slot0 + i] = Slot{s, -1, 0, 0};
+          arm.push_back(make_int2(s, 0));
           continue;
         }
         const int64_t c = cof[s];
         const int32_t p = cpos[s], k = B->chain_len[c];
-        slots.push_back(Slot{s, (int32_t)c, p, 0});
-        seeds.push_back(Seed{B->chain_l[c], p + 1, slot, 0});
-        seeds.push_back(Seed{B->chain_r[c], k - p, slot, 0});
+        slots[slot0 + i] = Slot{s, (int32_t)c, p, 0};
+        seeds[sd++] = Seed{B->chain_l[c], p + 1, slot, 0};
+        seeds[sd++] = Seed{B->chain_r[c], k - p, slot, 0};
         bt.max_seed = std::max(bt.max_seed, std::max(p + 1, k - p));
       }
-      bt.nseeds = (int32_t)((int64_t)seeds.size() - bt.seed_off);
+      bt.nseeds = (int32_t)(sd - bt.seed_off);
       // arming list: each core source (level 0) and seeded vertex (its lowest seed level), once
-      arm_tmp.clear();
-      for (int64_t i = bt.slot_off; i < bt.slot_off + bt.nslots; ++i)
-        if (slots[i].chain < 0) arm_tmp.push_back(make_int2(slots[i].src, 0));
-      for (int64_t i = bt.seed_off; i < bt.seed_off + bt.nseeds; ++i) arm_tmp.push_back(make_int2(seeds[i].v, seeds[i].level));
-      std::sort(arm_tmp.begin(), arm_tmp.end(), [](const int2 &x, const int2 &y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
+      for (int64_t i = bt.seed_off; i < sd; ++i) arm.push_back(make_int2(seeds[i].v, seeds[i].level));
+      std::sort(arm.begin(), arm.end(), [](const int2 &x, const int2 &y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
+      size_t u = 0;
+      for (size_t i = 0; i < arm.size(); ++i)
+        if (i == 0 || arm[i].x != arm[i - 1].x) arm[u++] = arm[i];
+      arm.resize(u);
+      bt.narm = (int32_t)u;
+      P->h_batches[bat0 + j] = bt;
+    }
+    for (int64_t j = 0; j < nbat; ++j) {
+      Batch &bt = P->h_batches[bat0 + j];
       bt.arm_off = (int64_t)arms.size();
-      for (size_t i = 0; i < arm_tmp.size(); ++i)
-        if (i == 0 || arm_tmp[i].x != arm_tmp[i - 1].x) arms.push_back(arm_tmp[i]);
-      bt.narm = (int32_t)((int64_t)arms.size() - bt.arm_off);
-      P->h_batches.push_back(bt);
+      arms.insert(arms.end(), arm_of[j].begin(), arm_of[j].end());
+      std::vector<int2>().swap(arm_of[j]);
       P->u_src.push_back(bt.nslots);
       P->u_teps.push_back((int64_t)bt.nslots * arcs);
       P->u_bfs.push_back(bt.nslots);
@@ -1510,9 +1559,24 @@ int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream,
   a.b1 = end;
   void *params[] = {&a};
   cudaError_t e = cudaMemsetAsync(&p->args.ctrl->bar_count, 0, 2 * sizeof(unsigned int), stream);
-  if (e == cudaSuccess) {
-    if (p->f32) e = cudaLaunchCooperativeKernel((void *)batched_kernel<float>, p->grid, kThreads, params, p->smem, stream);
-    else e = cudaLaunchCooperativeKernel((void *)batched_kernel<double>, p->grid, kThreads, params, p->smem, stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (e == cudaSuccess) e = cudaStreamIsCapturing(stream, &cap);
+  const void *fn = p->f32 ? (const void *)batched_kernel<float> : (const void *)batched_kernel<double>;
+  if (e == cudaSuccess && cap == cudaStreamCaptureStatusActive) {
+    // recorded into a CUDA graph: a kernel node carrying the cooperative attribute
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(p->grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = p->smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelExC(&cfg, fn, params);
+  } else if (e == cudaSuccess) {
+    e = cudaLaunchCooperativeKernel(fn, p->grid, kThreads, params, p->smem, stream);
   }
   if (e != cudaSuccess) {
     if (msg) *msg = std::string("cooperative launch: ") + cudaGetErrorString(e);

@@ -94,6 +94,40 @@ __device__ __forceinline__ void fwd_arc(SH &sh, int32_t *d, const double *sig, i
   }
 }
 
+// Forward scan of a low-degree vertex by one thread, kGather arcs at a time:
+// the neighbour ids, then their levels, then the predecessors' path counts
+// are each issued as independent loads (one memory round trip per group
+// instead of one per arc). Sums and claims follow arc order, so sigma is the
+// same value the arc-by-arc form computes.
+constexpr int kGather = 4;
+
+template <class SH>
+__device__ __forceinline__ double fwd_small(SH &sh, const int32_t *Ce, int deg, int32_t *d, const double *sig, int32_t *S,
+                                            int dprev, int dnext, int base) {
+  double acc = 0.0;
+  for (int g = 0; g < deg; g += kGather) {
+    int32_t x[kGather];
+    int dx[kGather];
+    double s[kGather];
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) x[j] = g + j < deg ? ldg(Ce + g + j) : -1;
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) dx[j] = x[j] >= 0 ? __ldcg(d + x[j]) : INT_MAX;  // INT_MAX: skipped
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) s[j] = dx[j] == dprev ? sig[x[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) {
+      if (dx[j] == dprev) {
+        acc += s[j];
+      } else if (dx[j] < base) {
+        const int old = atomicMax(d + x[j], dnext);
+        if (old < base) append(sh, S, x[j]);
+      }
+    }
+  }
+  return acc;
+}
+
 template <int kBlock>
 __device__ __forceinline__ double block_sum(Shared<kBlock> &sh, double v) {
   constexpr int kWarps = kBlock / 32;
@@ -141,8 +175,7 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         const int64_t e0 = R[w], e1 = R[w + 1];
         const int64_t deg = e1 - e0;
         if (deg <= kSmallDeg) {
-          double acc = 0.0;
-          for (int64_t e = e0; e < e1; ++e) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+          const double acc = fwd_small(sh, C + e0, (int)deg, d, sig, S, dprev, dnext, base);
           sig[w] = lev == 0 ? 1.0 : acc;
         } else if (deg <= kWarpDeg) {
           sh.wq[atomicAdd(&sh.nwq, 1)] = w;
@@ -182,12 +215,26 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
 
 // Dependency of w at level lev of a row (d stamped as base + level):
 // delta(w) = sigma(w) * sum over successors x of q(x); then q(w) and BC.
+// (one thread; ids, levels and successor values gathered kGather at a time,
+// summed in arc order as in fwd_small)
 __device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_t *C, const int32_t *d, const double *q,
                                                   int32_t w, int dsucc) {
   double acc = 0.0;
-  for (int64_t e = R[w]; e < R[w + 1]; ++e) {
-    int32_t x = ldg(C + e);
-    if (d[x] == dsucc) acc += q[x];
+  const int64_t e0 = R[w];
+  const int deg = (int)(R[w + 1] - e0);
+  for (int g = 0; g < deg; g += kGather) {
+    int32_t x[kGather];
+    bool hit[kGather];
+    double v[kGather];
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) x[j] = g + j < deg ? ldg(C + e0 + g + j) : -1;
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) hit[j] = x[j] >= 0 && d[x[j]] == dsucc;
+#pragma unroll
+    for (int j = 0; j < kGather; ++j) v[j] = hit[j] ? q[x[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < kGather; ++j)
+      if (hit[j]) acc += v[j];
   }
   return acc;
 }

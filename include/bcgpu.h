@@ -56,6 +56,11 @@ typedef struct bc_opts {
                             per-source schedule inside the same plan (small or deep BCCs
                             gain nothing from multi-source passes); 0 = 8192, negative =
                             every BCC in multi-source passes */
+  int32_t graph;         /* nonzero: bc_plan_run replays a CUDA graph of each unit range's device
+                            work (counter resets + the persistent kernels), recorded by stream
+                            capture on bc_plan_record or on the range's first run; 0 = enqueue
+                            the work directly on every run. The stream must be capturable
+                            (not the legacy NULL stream). */
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;
@@ -204,8 +209,16 @@ int bc_plan_concurrency(const bc_plan *plan);
 int bc_autotune_width(bc_ctx *ctx, const bc_bccs *bccs, int32_t passes, int32_t *width, double *gteps_out);
 int bc_plan_reset(bc_plan *plan);
 /* Enqueues units [begin, end) on the context's stream; asynchronous unless
- * stats is non-NULL (then synchronises and fills it). */
+ * stats is non-NULL (then synchronises and fills it). With bc_opts.graph set
+ * the work is one cudaGraphLaunch of the range's recorded graph. */
 int bc_plan_run(bc_plan *plan, int64_t begin, int64_t end, bc_stats *stats);
+/* Graph mode (bc_opts.graph != 0) only: records the device work of units
+ * [begin, end) into a CUDA graph by stream capture and instantiates it,
+ * WITHOUT running it, so that later bc_plan_run calls of that exact range are
+ * single graph launches (recording again replaces the graph). No reference
+ * counterpart: the reference launches kernels one source batch at a time
+ * from host loops (Codes/kernels_active.cu:98-180). */
+int bc_plan_record(bc_plan *plan, int64_t begin, int64_t end);
 /* Synchronises, copies BC to the host and adds the articulation terms. */
 int bc_plan_read(bc_plan *plan, double *bc_out);
 /* Levels and path counts of one source (packed id) as the GPU computes them
