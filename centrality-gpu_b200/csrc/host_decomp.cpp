@@ -263,7 +263,10 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   auto local_of = [&](int32_t x, int32_t b) -> int32_t {
     return x == head[b] ? (int32_t)(mem_off[b + 1] - mem_off[b] - 1) : locid[x];
   };
+  // A member slot (b, local id of x in b) only receives arcs of x itself, so
+  // both passes run in parallel over x with each slot filled in x's arc order.
   std::vector<int64_t> sdeg((size_t)n_slots + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
   for (int32_t x = 0; x < n; ++x)
     for (int64_t e = R[x]; e < R[x + 1]; ++e) {
       int32_t y = C[e];
@@ -274,6 +277,7 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   std::vector<int32_t> sadj((size_t)sdeg[n_slots]);
   {
     std::vector<int64_t> fill(sdeg.begin(), sdeg.end() - 1);
+#pragma omp parallel for schedule(dynamic, 4096)
     for (int32_t x = 0; x < n; ++x)
       for (int64_t e = R[x]; e < R[x + 1]; ++e) {
         int32_t y = C[e];
@@ -387,13 +391,16 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   for (int64_t k = 0; k < n_packed; ++k) D->row[k + 1] += D->row[k];
   if (D->row[n_packed] > (int64_t)INT32_MAX * 8) return BCGPU_EOVERFLOW;
   D->col.assign((size_t)D->row[n_packed], 0);
-#pragma omp parallel for schedule(dynamic, 1)
-  for (int32_t i = 0; i < np_bcc; ++i) {
+  // Each BCC writes its own packed range: large BCCs one at a time with their
+  // vertices in parallel, the others one BCC per thread.
+  constexpr int32_t kBigBcc = 1 << 16;
+  auto write_bcc = [&](int32_t i, bool inner_parallel) {
     const int32_t b = order[i];
     const int32_t nb = (int32_t)perm[i].size();
     std::vector<int32_t> inv((size_t)nb);
     for (int32_t k = 0; k < nb; ++k) inv[perm[i][k]] = k;
     const int64_t base = D->vtx_off[i];
+#pragma omp parallel for schedule(dynamic, 4096) if (inner_parallel)
     for (int32_t k = 0; k < nb; ++k) {
       int32_t o = perm[i][k];
       int64_t s = mem_off[b] + o;
@@ -406,7 +413,12 @@ int decompose(const bc_graph *g, bc_decomp *D) {
       D->reach[base + k] =
           (x == head[b]) ? (int32_t)(comp_size[comp[x]] - 1 - sz[child[b]]) : (int32_t)hang[x];
     }
-  }
+  };
+  for (int32_t i = 0; i < np_bcc; ++i)
+    if ((int32_t)perm[i].size() >= kBigBcc) write_bcc(i, true);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int32_t i = 0; i < np_bcc; ++i)
+    if ((int32_t)perm[i].size() < kBigBcc) write_bcc(i, false);
   for (int32_t i = 0; i < np_bcc; ++i) D->chain_off[i + 1] = D->chain_off[i] + (int64_t)ch_start[i].size();
   for (int32_t i = 0; i < np_bcc; ++i) {
     D->chain_start.insert(D->chain_start.end(), ch_start[i].begin(), ch_start[i].end());
