@@ -146,3 +146,37 @@ def test_betc_fails_loudly_without_gpu():
     with pytest.raises(P.BcError) as e:
         P.Context()
     assert e.value.code == P.ECUDA
+
+
+_HASH_SCRIPT = """
+import hashlib, sys
+sys.path.insert(0, {tests!r})
+from helpers import graphs, pkg
+P = pkg()
+n, u, v = graphs().gen_rmat(16, 16, 0.2, 1, 8, seed=2)
+arrs = P.Decomposition(P.Graph.from_edges(n, u, v)).arrays()
+h = hashlib.sha256()
+for k in sorted(arrs):
+    h.update(k.encode())
+    h.update(arrs[k].tobytes() if hasattr(arrs[k], "tobytes") else str(arrs[k]).encode())
+print(int(arrs["vtx_off"][1]), h.hexdigest())
+"""
+
+
+def test_decomposition_independent_of_thread_count():
+    """The decomposition's parallel passes (arc-to-BCC assignment, packed
+    writes; the RMAT-16 giant BCC takes the large-BCC path) give the same
+    arrays with 1 and 4 host threads."""
+    import os
+    import sys
+    from pathlib import Path
+
+    script = _HASH_SCRIPT.format(tests=str(Path(__file__).resolve().parent))
+    out = []
+    for threads in ("1", "4"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        r = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        out.append(r.stdout.split())
+    assert int(out[0][0]) >= 1 << 16  # the giant BCC is written with its vertices in parallel
+    assert out[0] == out[1]
