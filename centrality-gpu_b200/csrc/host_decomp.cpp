@@ -59,20 +59,41 @@ void set_err(char *err, size_t errlen, const std::string &msg) {
 
 int build_csr(int32_t n, int64_t m, const int32_t *u, const int32_t *v, bc_graph *g) {
   g->n = n;
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (int64_t e = 0; e < m; ++e) bad |= u[e] < 0 || u[e] >= n || v[e] < 0 || v[e] >= n;
+  if (bad) return BCGPU_EINVAL;
+  // Degrees and the scatter in parallel without atomics: thread t owns the
+  // vertices [lo_t, hi_t) and scans every edge, keeping the endpoints it
+  // owns, so each adjacency list is filled in edge order by one thread.
   std::vector<int64_t> deg((size_t)n + 1, 0);
-  for (int64_t e = 0; e < m; ++e) {
-    if (u[e] < 0 || u[e] >= n || v[e] < 0 || v[e] >= n) return BCGPU_EINVAL;
-    if (u[e] == v[e]) continue;
-    deg[u[e] + 1]++;
-    deg[v[e] + 1]++;
+  auto owned = [n](int32_t &lo, int32_t &hi) {
+    const int T = omp_get_num_threads(), t = omp_get_thread_num();
+    lo = (int32_t)((int64_t)n * t / T);
+    hi = (int32_t)((int64_t)n * (t + 1) / T);
+  };
+#pragma omp parallel
+  {
+    int32_t lo, hi;
+    owned(lo, hi);
+    for (int64_t e = 0; e < m; ++e) {
+      if (u[e] == v[e]) continue;
+      if (u[e] >= lo && u[e] < hi) deg[u[e] + 1]++;
+      if (v[e] >= lo && v[e] < hi) deg[v[e] + 1]++;
+    }
   }
   for (int32_t i = 0; i < n; ++i) deg[i + 1] += deg[i];
   std::vector<int32_t> col((size_t)deg[n]);
-  std::vector<int64_t> fill(deg.begin(), deg.end() - 1);
-  for (int64_t e = 0; e < m; ++e) {
-    if (u[e] == v[e]) continue;
-    col[fill[u[e]]++] = v[e];
-    col[fill[v[e]]++] = u[e];
+#pragma omp parallel
+  {
+    int32_t lo, hi;
+    owned(lo, hi);  // any split works: each vertex is filled by exactly one thread
+    std::vector<int64_t> fill(deg.begin() + lo, deg.begin() + hi);
+    for (int64_t e = 0; e < m; ++e) {
+      if (u[e] == v[e]) continue;
+      if (u[e] >= lo && u[e] < hi) col[fill[u[e] - lo]++] = v[e];
+      if (v[e] >= lo && v[e] < hi) col[fill[v[e] - lo]++] = u[e];
+    }
   }
   // sort + dedup every adjacency list, then compact
   std::vector<int64_t> keep((size_t)n + 1, 0);
@@ -141,19 +162,69 @@ extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t
     set_err(err, errlen, "bad header: expected 'n m'");
     return BCGPU_EIO;
   }
+  // The edge tokens are parsed in parallel: the rest of the buffer is cut
+  // into chunks at whitespace (a number never spans a cut), each chunk is
+  // scanned twice -- once to count the numbers before its first bad
+  // character, once to place number t (global order) as field t % 3 of
+  // edge t / 3. Errors are those of a sequential scan: the first edge that
+  // is incomplete ("truncated") or, before it, has an id out of range.
+  const char *p0 = sc.p, *pend = buf.data() + got;
+  const int nchunk = std::max(1, 4 * omp_get_max_threads());
+  std::vector<const char *> cut((size_t)nchunk + 1);
+  cut[0] = p0;
+  for (int k = 1; k < nchunk; ++k) {
+    const char *c = std::max(cut[k - 1], p0 + (pend - p0) * k / nchunk);
+    while (c < pend && !(*c == ' ' || *c == '\n' || *c == '\r' || *c == '\t')) ++c;
+    cut[k] = c;
+  }
+  cut[nchunk] = pend;
+  std::vector<int64_t> cnt((size_t)nchunk + 1, 0);
+  std::vector<char> broke((size_t)nchunk, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = 0; k < nchunk; ++k) {
+    Scanner s{cut[k], cut[k + 1]};
+    int64_t x, c = 0;
+    const char *last = s.p;  // where the failing call started
+    while (s.next(x)) {
+      ++c;
+      last = s.p;
+    }
+    while (last < s.end && (*last == ' ' || *last == '\n' || *last == '\r' || *last == '\t')) ++last;
+    cnt[k + 1] = c;
+    broke[k] = last < s.end;  // something other than whitespace followed: it starts no number
+  }
+  int64_t valid = 0;  // numbers before the first bad character
+  for (int k = 0; k < nchunk; ++k) {
+    valid += cnt[k + 1];
+    if (broke[k]) break;
+  }
+  for (int k = 0; k < nchunk; ++k) cnt[k + 1] += cnt[k];
+  const int64_t need = 3 * m, have = std::min(valid, need);
   std::vector<int32_t> u((size_t)m), v((size_t)m);
-  for (int64_t e = 0; e < m; ++e) {
-    int64_t a, b, w;
-    if (!sc.next(a) || !sc.next(b) || !sc.next(w)) {
-      set_err(err, errlen, "truncated edge list at edge " + std::to_string(e) + " of " + std::to_string(m));
-      return BCGPU_EIO;
+  int64_t first_oob = INT64_MAX;
+#pragma omp parallel for schedule(dynamic, 1) reduction(min : first_oob)
+  for (int k = 0; k < nchunk; ++k) {
+    Scanner s{cut[k], cut[k + 1]};
+    int64_t x;
+    for (int64_t t = cnt[k]; t < have && s.next(x); ++t) {
+      const int64_t e = t / 3;
+      const int f = (int)(t % 3);
+      if (f == 2) continue;  // the weight: read, not used (as the reference's BFS)
+      if (x < 0 || x >= n) {
+        first_oob = std::min(first_oob, e);
+        x = 0;
+      }
+      (f == 0 ? u : v)[(size_t)e] = (int32_t)x;
     }
-    if (a < 0 || a >= n || b < 0 || b >= n) {
-      set_err(err, errlen, "vertex id out of range at edge " + std::to_string(e));
-      return BCGPU_EIO;
-    }
-    u[e] = (int32_t)a;
-    v[e] = (int32_t)b;
+  }
+  const int64_t trunc_at = have < need ? have / 3 : INT64_MAX;
+  if (first_oob < trunc_at) {
+    set_err(err, errlen, "vertex id out of range at edge " + std::to_string(first_oob));
+    return BCGPU_EIO;
+  }
+  if (trunc_at != INT64_MAX) {
+    set_err(err, errlen, "truncated edge list at edge " + std::to_string(trunc_at) + " of " + std::to_string(m));
+    return BCGPU_EIO;
   }
   int rc = bc_graph_from_edges((int32_t)n, m, u.data(), v.data(), out);
   if (rc != BCGPU_OK) set_err(err, errlen, "graph construction failed");

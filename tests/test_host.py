@@ -180,3 +180,58 @@ def test_decomposition_independent_of_thread_count():
         out.append(r.stdout.split())
     assert int(out[0][0]) >= 1 << 16  # the giant BCC is written with its vertices in parallel
     assert out[0] == out[1]
+
+
+_LOAD_SCRIPT = """
+import sys
+sys.path.insert(0, {tests!r})
+from helpers import pkg
+P = pkg()
+for path in sys.argv[1:]:
+    try:
+        n, row, col = P.Graph.load(path).csr()
+        print("ok", n, row.tolist(), col.tolist())
+    except P.BcError as e:
+        print("err", e.code, str(e))
+"""
+
+
+def test_graph_load_token_rules_any_thread_count(tmp_path):
+    """The parallel parser reads numbers exactly as a sequential scan would
+    (whitespace of any kind between them, a leading minus sign, nothing
+    after the m-th edge looked at) and reports the first bad edge, with 1,
+    3 and 8 host threads (chunk cuts fall in different places)."""
+    import os
+    import sys
+    from pathlib import Path
+
+    cases = {
+        "one_line": "4 3 0 1 1 1 2 1 2 3 1",
+        "mixed_ws": "4 3\r\n0\t1 1\n\n1  2 1\r\n2 3 1",
+        "glued": "4 2\n0 1 1 2-3 1\n",            # '2-3' reads as 2 then -3: out of range at edge 1
+        "junk_after": "3 2\n0 1 1\n1 2 1\nthis is ignored",
+        "bad_token": "5 3\n0 1 1\n1 x 1\n2 3 1\n",   # edge 1 is incomplete
+        "oob_before_trunc": "5 3\n0 9 1\n1 2 1\n2 3",
+        "lone_minus": "5 2\n0 1 - 2 3 1\n",   # no digit after the sign: edge 0 is incomplete
+    }
+    paths = []
+    for name, text in cases.items():
+        f = tmp_path / f"{name}.txt"
+        f.write_text(text)
+        paths.append(str(f))
+    script = _LOAD_SCRIPT.format(tests=str(Path(__file__).resolve().parent))
+    runs = []
+    for threads in ("1", "3", "8"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        r = subprocess.run([sys.executable, "-c", script] + paths, env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        runs.append(r.stdout.splitlines())
+    assert runs[0] == runs[1] == runs[2]
+    got = dict(zip(cases, runs[0]))
+    path_graph = "ok 4 [0, 1, 3, 5, 6] [1, 0, 2, 1, 3, 2]"
+    assert got["one_line"] == path_graph and got["mixed_ws"] == path_graph
+    assert got["glued"].startswith("err 5") and "out of range at edge 1" in got["glued"]
+    assert got["junk_after"] == "ok 3 [0, 1, 3, 4] [1, 0, 2, 1]"
+    assert got["bad_token"].startswith("err 5") and "truncated edge list at edge 1 of 3" in got["bad_token"]
+    assert "out of range at edge 0" in got["oob_before_trunc"]
+    assert "truncated edge list at edge 0 of 2" in got["lone_minus"]  # the minus sign is edge 0's weight
