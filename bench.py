@@ -272,6 +272,10 @@ def main():
     ap.add_argument("--graph", type=int, choices=[0, 1], default=1,
                     help="1: every step is one launch of a CUDA graph of the step's device work, recorded "
                          "(stream capture, nothing runs) before the warm-up; 0: the work is enqueued directly")
+    ap.add_argument("--phase-times", action="store_true",
+                    help="print the multi-source kernel's per-phase times of the timed steps to stderr "
+                         "(needs an instrumented build: build.py --variant phase -DBCGPU_PHASE_TIMERS, "
+                         "BCGPU_LIB_DIR=centrality-gpu_b200/lib_phase)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
     args = ap.parse_args()
@@ -334,6 +338,8 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.phase_times:
+        P.phase_times(reset=True)
     clk = clocks_start()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
@@ -348,6 +354,8 @@ def main():
     if dist:
         dist.barrier()
     clocks = clocks_stop(clk, local)
+    if args.phase_times:
+        print(json.dumps({"phase_ms": P.phase_times(reset=True)}), file=sys.stderr, flush=True)
     elapsed = t_start.elapsed_time(t_end)
     per_step = [a.elapsed_time(b) for a, b in evs]
     work = np.array([plan.unit_work(r0, r1) for r0, r1 in sel[args.warmup:]], dtype=np.float64)

@@ -23,8 +23,11 @@ from pathlib import Path
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "lib" / "libbcgpu.so"
-BETC_PATH = _PKG / "lib" / "betc"
+# BCGPU_LIB_DIR selects another in-tree build (e.g. an instrumented variant from
+# build.py --variant); the default is lib/.
+_LIB_DIR = Path(os.environ["BCGPU_LIB_DIR"]) if os.environ.get("BCGPU_LIB_DIR") else _PKG / "lib"
+LIB_PATH = _LIB_DIR / "libbcgpu.so"
+BETC_PATH = _LIB_DIR / "betc"
 
 OK, EINVAL, ECUDA, ENOMEM, ETIMEOUT, EIO, EOVERFLOW = range(7)
 MODE_PLAIN, MODE_BATCHED = 0, 1
@@ -436,3 +439,26 @@ def begin_gpu_active(ctx: Context, R, Cc, n, m, active, ears, artnodes, bc, time
 def declared_symbols():
     """Names of every function declared in include/*.h."""
     return sorted(_SIGS)
+
+
+# Phases of the multi-source kernel as numbered by its PHASE_MARK points.
+PHASES = {0: "pass init", 1: "forward rows", 2: "forward heavy combine", 3: "forward level end",
+          4: "chain inflow", 5: "backward heavy chunks", 6: "backward rows", 8: "chain vertices", 7: "fold into BC"}
+
+
+def phase_times(reset=True):
+    """Instrumented builds only (build.py --variant NAME -DBCGPU_PHASE_TIMERS,
+    loaded with BCGPU_LIB_DIR): milliseconds CTA 0 spent in each phase of the
+    multi-source kernel since the last reset, plus the forward and backward
+    level counts; None with the default build."""
+    L = lib()
+    if not hasattr(L, "bc_debug_phase_times"):
+        return None
+    buf = (C.c_ulonglong * 32)()
+    L.bc_debug_phase_times.restype = C.c_int
+    if L.bc_debug_phase_times(buf, 1 if reset else 0) != 0:
+        return None
+    out = {name: buf[i] / 1e6 for i, name in PHASES.items()}
+    out["forward levels"] = int(buf[16])
+    out["backward levels"] = int(buf[17])
+    return out

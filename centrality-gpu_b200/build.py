@@ -1,6 +1,9 @@
 """Builds libbcgpu.so and the betc CLI in-tree (lib/), for sm_100a only.
 
     python centrality-gpu_b200/build.py          # or __graft_entry__.build()
+    python centrality-gpu_b200/build.py --variant phase -DBCGPU_PHASE_TIMERS
+        # an instrumented copy in lib_phase/ (objects in _build_phase/); load it
+        # with BCGPU_LIB_DIR=<package>/lib_phase. The default build is unaffected.
 """
 from __future__ import annotations
 
@@ -42,31 +45,34 @@ def _stale(target: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    OBJ.mkdir(exist_ok=True)
-    LIB.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, variant: str = "", defines=()) -> Path:
+    obj_dir = OBJ if not variant else PKG / f"_build_{variant}"
+    lib_dir = LIB if not variant else PKG / f"lib_{variant}"
+    obj_dir.mkdir(exist_ok=True)
+    lib_dir.mkdir(exist_ok=True)
+    extra = list(defines)
     headers = list(SRC.glob("*.h")) + list(SRC.glob("*.cuh")) + list(INC.glob("*.h"))
     jobs = []
     objs = []
     for s in CU_SOURCES:
-        o = OBJ / (s + ".o")
+        o = obj_dir / (s + ".o")
         objs.append(o)
         if force or _stale(o, [SRC / s] + headers):
-            jobs.append([NVCC] + CU_FLAGS + ["-c", str(SRC / s), "-o", str(o)])
+            jobs.append([NVCC] + CU_FLAGS + extra + ["-c", str(SRC / s), "-o", str(o)])
     for s in CXX_SOURCES:
-        o = OBJ / (s + ".o")
+        o = obj_dir / (s + ".o")
         objs.append(o)
         if force or _stale(o, [SRC / s] + headers):
-            jobs.append([HOSTCXX] + CXX_FLAGS + ["-c", str(SRC / s), "-o", str(o)])
+            jobs.append([HOSTCXX] + CXX_FLAGS + extra + ["-c", str(SRC / s), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         for out in ex.map(_run, jobs):
             if verbose and out.strip():
                 print(out)
-    lib = LIB / "libbcgpu.so"
+    lib = lib_dir / "libbcgpu.so"
     if force or _stale(lib, objs):
         _run([NVCC] + ARCH + ["-shared", "-ccbin", HOSTCXX, "-o", str(lib)] + [str(o) for o in objs] +
              ["-lgomp", "-Xlinker", "-soname=libbcgpu.so"])
-    betc = LIB / "betc"
+    betc = lib_dir / "betc"
     main = SRC / "betc_main.cpp"
     if force or _stale(betc, [main, lib] + headers):
         _run([HOSTCXX] + CXX_FLAGS + [str(main), "-o", str(betc), "-L" + str(LIB), "-lbcgpu",
@@ -75,5 +81,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force="-f" in sys.argv)
-    print("built", LIB / "libbcgpu.so", LIB / "betc")
+    argv = sys.argv[1:]
+    var = argv[argv.index("--variant") + 1] if "--variant" in argv else ""
+    lib_path = build(verbose="-v" in argv, force="-f" in argv, variant=var,
+                     defines=[a for a in argv if a.startswith("-D")])
+    print("built", lib_path, lib_path.parent / "betc")
