@@ -250,51 +250,63 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   const int64_t *R = g->row.data();
   const int32_t *C = g->col.data();
 
-  // ---- iterative Hopcroft-Tarjan: DFS tree, low links, subtree sizes, BCCs
-  std::vector<int32_t> disc((size_t)n, -1), low((size_t)n), parent((size_t)n, -1), tbcc((size_t)n, -1),
-      locid((size_t)n, -1), comp((size_t)n, -1);
-  std::vector<int64_t> it((size_t)n), sz((size_t)n, 0), hang((size_t)n, 0);
+  // ---- iterative Hopcroft-Tarjan: DFS tree, low links, subtree sizes, BCCs.
+  // The explicit stack holds one frame per open vertex (its arc cursor, low
+  // link and subtree size), so the scan of a vertex's arcs touches only its
+  // frame and the neighbours' discovery times.
+  std::vector<int32_t> disc((size_t)n, -1), tbcc((size_t)n, -1), locid((size_t)n, -1), comp((size_t)n, -1);
+  std::vector<int64_t> sz((size_t)n, 0), hang((size_t)n, 0);
   std::vector<double> sq((size_t)n, 0.0);
   std::vector<int64_t> comp_size;
   std::vector<int32_t> head, child;          // per BCC
   std::vector<int64_t> mem_off{0};           // per BCC member range
   std::vector<int32_t> members;              // head stored last
-  std::vector<int32_t> stack, vstack;
+  struct Frame {
+    int64_t e, e1;  // arc cursor and end
+    int64_t size;   // subtree size so far
+    int32_t u, parent, disc, low;
+  };
+  std::vector<Frame> stack;
+  std::vector<int32_t> vstack;
   stack.reserve(1024);
   vstack.reserve(1024);
   int32_t timer = 0;
   for (int32_t r = 0; r < n; ++r) {
     if (disc[r] >= 0) continue;
     int32_t cid = (int32_t)comp_size.size();
-    disc[r] = low[r] = timer++;
-    it[r] = R[r];
-    sz[r] = 1;
+    disc[r] = timer;
     comp[r] = cid;
-    stack.push_back(r);
+    stack.push_back(Frame{R[r], R[r + 1], 1, r, -1, timer, timer});
+    ++timer;
     vstack.push_back(r);
     while (!stack.empty()) {
-      int32_t u = stack.back();
-      if (it[u] < R[u + 1]) {
-        int32_t w = C[it[u]++];
-        if (disc[w] < 0) {
-          parent[w] = u;
-          disc[w] = low[w] = timer++;
-          it[w] = R[w];
-          sz[w] = 1;
-          comp[w] = cid;
-          stack.push_back(w);
-          vstack.push_back(w);
-        } else if (w != parent[u] && disc[w] < low[u]) {
-          low[u] = disc[w];
-        }
+      Frame &f = stack.back();
+      int32_t next = -1;
+      while (f.e < f.e1) {
+        const int32_t w = C[f.e++];
+        const int32_t dw = disc[w];
+        if (dw < 0) { next = w; break; }
+        if (w != f.parent && dw < f.low) f.low = dw;
+      }
+      if (next >= 0) {
+        const int32_t w = next, pu = f.u;  // f is not used past the push
+        disc[w] = timer;
+        comp[w] = cid;
+        stack.push_back(Frame{R[w], R[w + 1], 1, w, pu, timer, timer});
+        ++timer;
+        vstack.push_back(w);
         continue;
       }
+      const Frame done = stack.back();
       stack.pop_back();
-      int32_t p = parent[u];
-      if (p < 0) continue;
-      if (low[u] < low[p]) low[p] = low[u];
-      sz[p] += sz[u];
-      if (low[u] >= disc[p]) {  // tree edge (p,u) closes a BCC headed by p
+      const int32_t u = done.u;
+      sz[u] = done.size;
+      if (stack.empty()) continue;  // the root
+      Frame &pf = stack.back();
+      const int32_t p = pf.u;
+      if (done.low < pf.low) pf.low = done.low;
+      pf.size += done.size;
+      if (done.low >= pf.disc) {  // tree edge (p,u) closes a BCC headed by p
         int32_t b = (int32_t)head.size();
         head.push_back(p);
         child.push_back(u);
@@ -308,8 +320,8 @@ int decompose(const bc_graph *g, bc_decomp *D) {
         } while (w != u);
         members.push_back(p);
         mem_off.push_back((int64_t)members.size());
-        hang[p] += sz[u];
-        sq[p] += (double)sz[u] * (double)sz[u];
+        hang[p] += done.size;
+        sq[p] += (double)done.size * (double)done.size;
       }
     }
     vstack.clear();  // only the root remains
