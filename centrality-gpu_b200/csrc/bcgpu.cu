@@ -210,14 +210,44 @@ constexpr int64_t kItemChainVertices = 16;
 constexpr int32_t kBatchedMinCore = 8192;
 constexpr int kBatchedMaxLevels = 96;
 
-int bcc_ecc0(const bc_bccs *B, int32_t b, std::vector<int32_t> &dist, std::vector<int32_t> &queue) {
+// Eccentricity of a BCC's local vertex 0 (BFS levels). BCCs of at least
+// kParallelBfs vertices expand each level's frontier in parallel: a vertex
+// joins the next level once, by compare-and-swap on its level; the levels,
+// and so the eccentricity, are those of the sequential BFS.
+constexpr int32_t kParallelBfs = 1 << 16;
+
+int bcc_ecc0(const bc_bccs *B, int32_t b, std::vector<int32_t> &dist, std::vector<int32_t> &queue, bool parallel) {
   const int64_t vo = B->vtx_off[b];
   const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
   dist.assign((size_t)nb, -1);
+  dist[0] = 0;
+  if (parallel) {
+    std::vector<int32_t> frontier{0}, next;
+    int lev = 0;
+    while (true) {
+      next.clear();
+#pragma omp parallel
+      {
+        std::vector<int32_t> mine;
+#pragma omp for schedule(dynamic, 256) nowait
+        for (size_t i = 0; i < frontier.size(); ++i) {
+          const int32_t x = frontier[i];
+          for (int64_t e = B->row[vo + x]; e < B->row[vo + x + 1]; ++e) {
+            const int32_t y = B->col[e];
+            if (dist[y] < 0 && __sync_bool_compare_and_swap(&dist[y], -1, lev + 1)) mine.push_back(y);
+          }
+        }
+#pragma omp critical
+        next.insert(next.end(), mine.begin(), mine.end());
+      }
+      if (next.empty()) return lev;
+      frontier.swap(next);
+      ++lev;
+    }
+  }
   queue.resize((size_t)nb);
   int head = 0, tail = 0, ecc = 0;
   queue[tail++] = 0;
-  dist[0] = 0;
   while (head < tail) {
     const int32_t x = queue[head++];
     ecc = std::max(ecc, dist[x]);
@@ -297,17 +327,25 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     ecc0.assign((size_t)B->n_bcc, -1);
     if (ctx->opts.plain_core >= 0) {
       const int32_t min_core = ctx->opts.plain_core > 0 ? ctx->opts.plain_core : kBatchedMinCore;
+      auto route = [&](int32_t b, std::vector<int32_t> &dist, std::vector<int32_t> &queue, bool parallel) {
+        if (B->n_plain[b] < min_core) { on[b] = 0; return; }
+        int kmax = 0;
+        for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) kmax = std::max(kmax, B->chain_len[c]);
+        ecc0[b] = bcc_ecc0(B, b, dist, queue, parallel);
+        on[b] = 2 * ecc0[b] + kmax <= kBatchedMaxLevels;
+      };
+      auto big = [&](int32_t b) { return B->vtx_off[b + 1] - B->vtx_off[b] >= kParallelBfs; };
+      {
+        std::vector<int32_t> dist, queue;
+        for (int32_t b = 0; b < B->n_bcc; ++b)
+          if (big(b)) route(b, dist, queue, true);  // one BCC at a time, its levels in parallel
+      }
 #pragma omp parallel
       {
         std::vector<int32_t> dist, queue;
 #pragma omp for schedule(dynamic, 1)
-        for (int32_t b = 0; b < B->n_bcc; ++b) {
-          if (B->n_plain[b] < min_core) { on[b] = 0; continue; }
-          int kmax = 0;
-          for (int64_t c = B->chain_off[b]; c < B->chain_off[b + 1]; ++c) kmax = std::max(kmax, B->chain_len[c]);
-          ecc0[b] = bcc_ecc0(B, b, dist, queue);
-          on[b] = 2 * ecc0[b] + kmax <= kBatchedMaxLevels;
-        }
+        for (int32_t b = 0; b < B->n_bcc; ++b)
+          if (!big(b)) route(b, dist, queue, false);
       }
     }
     for (char x : on) n_on += x;
