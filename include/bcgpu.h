@@ -46,7 +46,8 @@ typedef struct bc_opts {
   int32_t device;        /* CUDA device ordinal; -1 = highest compute capability (reference choose_device) */
   int32_t mode;          /* BCGPU_MODE_* */
   int32_t delta;         /* BCGPU_DELTA_* (BATCHED only) */
-  int32_t batch_width;   /* sources per batched pass: multiple of 32, <= 1024; 0 = autotune */
+  int32_t batch_width;   /* sources per batched pass: multiple of 32, <= 1024; 0 = 512
+                            (bc_autotune_width measures the best width for a graph) */
   void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context */
   int64_t workspace_limit; /* device bytes the context may hold; 0 = 80% of free memory */
   int32_t rescale_exp;   /* BATCHED: rescale a level's path counts above 2^rescale_exp; 0 = 900.
@@ -65,7 +66,7 @@ typedef struct bc_opts {
 
 typedef struct bc_ctx bc_ctx;
 
-/* Fills opts with defaults (device -1, BATCHED, FP32C, autotuned width). */
+/* Fills opts with defaults (device -1, BATCHED, FP32C, width 0 = 512, graph off). */
 void bc_default_opts(bc_opts *opts);
 int bc_create(const bc_opts *opts, bc_ctx **out);
 /* Releases the context and every plan still alive on it. */
@@ -215,7 +216,8 @@ int bc_plan_run(bc_plan *plan, int64_t begin, int64_t end, bc_stats *stats);
 /* Graph mode (bc_opts.graph != 0) only: records the device work of units
  * [begin, end) into a CUDA graph by stream capture and instantiates it,
  * WITHOUT running it, so that later bc_plan_run calls of that exact range are
- * single graph launches (recording again replaces the graph). No reference
+ * single graph launches (recording again replaces the graph). Each recorded
+ * range keeps its instantiated graph until the plan is destroyed. No reference
  * counterpart: the reference launches kernels one source batch at a time
  * from host loops (Codes/kernels_active.cu:98-180). */
 int bc_plan_record(bc_plan *plan, int64_t begin, int64_t end);
