@@ -388,15 +388,24 @@ def main():
         torch.cuda.synchronize()
         e_sel = sel[args.warmup:args.warmup + args.e2e_steps]
         out = np.zeros(n, dtype=np.float64)
+        if dist:
+            dist.barrier()  # ranks start together; the job's time is the slowest rank's
         te = time.perf_counter()
         for r0, r1 in e_sel:
             ctx.run_units(d, r0, r1, with_art=False, out=out)
         te = time.perf_counter() - te
-        e_teps = sum(plan.unit_work(r0, r1)[1] for r0, r1 in e_sel)
+        e_teps = float(sum(plan.unit_work(r0, r1)[1] for r0, r1 in e_sel))
+        if dist:
+            t_sum = torch.tensor([e_teps], dtype=torch.float64, device="cuda")
+            t_max = torch.tensor([te], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t_sum)
+            dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+            e_teps, te = t_sum.item(), t_max.item()
         h2d = sum(int(arrs[k].nbytes) for k in ("vtx_off", "row", "col", "reach", "chain_start", "chain_len",
                                                "chain_l", "chain_r"))
-        e2e = {"value": e_teps / te / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(arrs["n_packed"]) * 8, "steps": len(e_sel)}
+        # every rank uploads the packed graph and reads back its BC each step
+        e2e = {"value": e_teps / te / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d * world,
+               "d2h_bytes_per_step": int(arrs["n_packed"]) * 8 * world, "steps": len(e_sel)}
 
     # combine the ranks' BC (one FP64 all-reduce, outside the timed region)
     if world > 1:
