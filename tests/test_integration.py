@@ -9,9 +9,10 @@ import re
 import subprocess
 from pathlib import Path
 
+import numpy as np
 import pytest
 
-from helpers import GOLDEN, GOLDEN_CASES, ROOT, canonical_chains, has_gpu, load_case, product_bccs
+from helpers import GOLDEN, GOLDEN_CASES, ROOT, canonical_chains, has_gpu, load_case, oracle, product_bccs
 from helpers import pkg as P
 
 BINDING = ROOT / "centrality-gpu_b200" / "reference_binding" / "begin_gpupgm_bcgpu.cpp"
@@ -70,3 +71,76 @@ def test_binding_hands_on_the_products_chains(tmp_path, name):
     for b in product_bccs(arrs):
         want.update(b["chains"])
     assert canonical_chains(got) == want
+
+
+REFBETC_CPU = ROOT / "oracle" / "_ref" / "refbetc_cpu"
+
+
+def _bc_lines(stdout, n):
+    """The per-vertex BC lines refbetc_main prints last (the reference prints progress before)."""
+    rows = [ln.split() for ln in stdout.splitlines()][-n:]
+    assert [int(r[0]) for r in rows] == list(range(n))
+    return np.array([float(r[1]) for r in rows])
+
+
+def reference_semantics_bc(n, u, v):
+    """What the reference's betc computes when its two begin_gpu calls return
+    exact contributions: per BCC of >= 3 vertices, the free call's buffer F
+    is added to the result, and -- when the BCC has ears -- the active call,
+    which starts from that same buffer, adds F + A again
+    (Codes/to_eargraph_construct.cpp:117,163-180); A = the chain endpoints'
+    and chain vertices' contributions. Plus the articulation terms. Built from
+    the product's decomposition and the oracle's per-BCC Brandes."""
+    arrs = P().Decomposition(P().Graph.from_edges(n, u, v)).arrays()
+    O = oracle()
+    out = np.array(arrs["art"], dtype=np.float64)
+    for b in range(arrs["n_bcc"]):
+        v0, v1 = int(arrs["vtx_off"][b]), int(arrs["vtx_off"][b + 1])
+        c0, c1 = int(arrs["chain_off"][b]), int(arrs["chain_off"][b + 1])
+        npl = int(arrs["n_plain"][b])
+        ends = set(arrs["chain_l"][c0:c1].tolist()) | set(arrs["chain_r"][c0:c1].tolist())
+        free = np.array([k for k in range(npl) if k not in ends], dtype=np.int32)
+        act = np.array(sorted(ends) + list(range(npl, v1 - v0)), dtype=np.int32)
+        F = O.bcc_sources(arrs, b, free) if len(free) else np.zeros(v1 - v0)
+        A = O.bcc_sources(arrs, b, act) if len(act) else np.zeros(v1 - v0)
+        part = F + ((F + A) if c1 > c0 else 0.0)
+        np.add.at(out, arrs["orig"][v0:v1], part)
+    return out
+
+
+@pytest.mark.skipif(not REFBETC_CPU.exists(), reason="reference sources absent: refbetc_cpu not built")
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_reference_betc_on_the_binding_gives_reference_semantics(tmp_path, name):
+    """The reference's own betc rebuilt on the binding (library calls computed
+    by the oracle on the CPU) prints the reference's semantics -- its free
+    contributions counted twice in BCCs with ears -- and, where a BCC has no
+    ears, the exact BC."""
+    n, u, v, golden, _ = load_case(name)
+    r = subprocess.run([str(REFBETC_CPU), str(GOLDEN / f"{name}.txt")], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = _bc_lines(r.stdout, n)
+    want = reference_semantics_bc(n, u, v)
+    assert np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))) < 1e-5  # the reference's float buffers
+    if P().Decomposition(P().Graph.from_edges(n, u, v)).arrays()["n_chains"] == 0:
+        assert np.max(np.abs(got - golden) / np.maximum(1.0, np.abs(golden))) < 1e-5
+
+
+@pytest.mark.skipif(not REFBETC_CPU.exists(), reason="reference sources absent: refbetc_cpu not built")
+def test_reference_betc_without_ears_gives_exact_bc(tmp_path):
+    """A wheel (hub 0, rim 1..5: no degree-2 vertex, so no ears) with a
+    pendant path 1-6-7: only free calls, so the reference's betc on the
+    binding prints the exact BC (articulation terms through reach)."""
+    edges = [(0, k) for k in range(1, 6)] + [(k, k % 5 + 1) for k in range(1, 6)] + [(1, 6), (6, 7)]
+    f = tmp_path / "wheel.txt"
+    f.write_text(f"8 {len(edges)}\n" + "".join(f"{a} {b} 1\n" for a, b in edges))
+    r = subprocess.run([str(REFBETC_CPU), str(f)], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = _bc_lines(r.stdout, 8)
+    O = oracle()
+    u = np.array([a for a, _ in edges], dtype=np.int32)
+    v = np.array([b for _, b in edges], dtype=np.int32)
+    row, col = O.csr(8, u, v)
+    want = O.brandes(8, row, col)
+    assert want[1] > 0 and want[0] > 0
+    assert np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))) < 1e-5
