@@ -145,8 +145,9 @@ extern "C" int bc_graph_from_edges(int32_t n, int64_t m, const int32_t *u, const
   return BCGPU_OK;
 }
 
-extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t errlen) {
-  if (!path || !out) { set_err(err, errlen, "null argument"); return BCGPU_EINVAL; }
+namespace {
+
+int graph_load(const char *path, bc_graph **out, char *err, size_t errlen) {
   FILE *fp = std::fopen(path, "rb");
   if (!fp) { set_err(err, errlen, std::string("input file cannot be opened: ") + path); return BCGPU_EIO; }
   std::fseek(fp, 0, SEEK_END);
@@ -199,8 +200,11 @@ extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t
     if (broke[k]) break;
   }
   for (int k = 0; k < nchunk; ++k) cnt[k + 1] += cnt[k];
-  const int64_t need = 3 * m, have = std::min(valid, need);
-  std::vector<int32_t> u((size_t)m), v((size_t)m);
+  const int64_t need = m > INT64_MAX / 3 ? INT64_MAX : 3 * m, have = std::min(valid, need);
+  // the edge arrays are sized from the header only once the file holds that
+  // many numbers (a header that overstates m is a truncated list, not an allocation)
+  const bool complete = have == need;
+  std::vector<int32_t> u(complete ? (size_t)m : 0), v(complete ? (size_t)m : 0);
   int64_t first_oob = INT64_MAX;
 #pragma omp parallel for schedule(dynamic, 1) reduction(min : first_oob)
   for (int k = 0; k < nchunk; ++k) {
@@ -214,7 +218,7 @@ extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t
         first_oob = std::min(first_oob, e);
         x = 0;
       }
-      (f == 0 ? u : v)[(size_t)e] = (int32_t)x;
+      if (complete) (f == 0 ? u : v)[(size_t)e] = (int32_t)x;
     }
   }
   const int64_t trunc_at = have < need ? have / 3 : INT64_MAX;
@@ -229,6 +233,18 @@ extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t
   int rc = bc_graph_from_edges((int32_t)n, m, u.data(), v.data(), out);
   if (rc != BCGPU_OK) set_err(err, errlen, "graph construction failed");
   return rc;
+}
+
+}  // namespace
+
+extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t errlen) {
+  if (!path || !out) { set_err(err, errlen, "null argument"); return BCGPU_EINVAL; }
+  try {
+    return graph_load(path, out, err, errlen);
+  } catch (const std::bad_alloc &) {
+    set_err(err, errlen, "out of host memory reading the edge list");
+    return BCGPU_ENOMEM;
+  }
 }
 
 extern "C" void bc_graph_free(bc_graph *g) { delete g; }

@@ -213,6 +213,7 @@ def test_graph_load_token_rules_any_thread_count(tmp_path):
         "bad_token": "5 3\n0 1 1\n1 x 1\n2 3 1\n",   # edge 1 is incomplete
         "oob_before_trunc": "5 3\n0 9 1\n1 2 1\n2 3",
         "lone_minus": "5 2\n0 1 - 2 3 1\n",   # no digit after the sign: edge 0 is incomplete
+        "huge_m": "5 99999999999\n0 1 1\n",     # a header overstating m: truncated, nothing sized from it
     }
     paths = []
     for name, text in cases.items():
@@ -235,3 +236,4 @@ def test_graph_load_token_rules_any_thread_count(tmp_path):
     assert got["bad_token"].startswith("err 5") and "truncated edge list at edge 1 of 3" in got["bad_token"]
     assert "out of range at edge 0" in got["oob_before_trunc"]
     assert "truncated edge list at edge 0 of 2" in got["lone_minus"]  # the minus sign is edge 0's weight
+    assert got["huge_m"].startswith("err 5") and "truncated edge list at edge 1 of 99999999999" in got["huge_m"]
