@@ -98,6 +98,17 @@ int cuda_fail(bc_ctx *ctx, cudaError_t e, const char *what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
+// Runs an entry point's body; a host allocation that throws becomes
+// BCGPU_ENOMEM, so no C++ exception leaves the C ABI.
+template <class F>
+int guard(bc_ctx *ctx, F &&body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc &) {
+    return fail(ctx, BCGPU_ENOMEM, "host allocation failed");
+  }
+}
+
 template <typename T>
 int dalloc(bc_plan *p, T **ptr, int64_t count) {
   size_t bytes = sizeof(T) * (size_t)std::max<int64_t>(count, 1);
@@ -280,18 +291,10 @@ void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items, const std
   }
 }
 
-int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan **out) {
-  int rc = validate(ctx, B);
-  if (rc) return rc;
-  CK(ctx, cudaSetDevice(ctx->device));
-  bc_plan *p = new (std::nothrow) bc_plan;
-  if (!p) return fail(ctx, BCGPU_ENOMEM, "host allocation");
-  p->ctx = ctx;
-  p->mode = ctx->opts.mode;
-  auto bail = [&](int code) {
-    bc_plan_destroy(p);
-    return code;
-  };
+// Fills plan p (allocated by create_plan, which releases it on any failure).
+int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan *p) {
+  int rc = BCGPU_OK;
+  auto bail = [](int code) { return code; };
   p->n_orig = B->n_orig;
   p->n_packed = B->n_packed;
   p->orig.assign(B->orig, B->orig + B->n_packed);
@@ -426,7 +429,33 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->plans.insert(p);
+  return BCGPU_OK;
+}
+
+// Validates the input and builds a plan; on any failure -- a status code, or
+// a host allocation that throws -- the partial plan and its device buffers are
+// released and no C++ exception leaves the library.
+int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan **out) {
+  bc_plan *p = nullptr;
+  int rc;
+  try {
+    rc = validate(ctx, B);
+    if (rc == BCGPU_OK) {
+      const cudaError_t e = cudaSetDevice(ctx->device);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+      p = new bc_plan;
+      p->ctx = ctx;
+      p->mode = ctx->opts.mode;
+      rc = build_plan(ctx, B, override_items, p);
+      if (rc == BCGPU_OK) ctx->plans.insert(p);
+    }
+  } catch (const std::bad_alloc &) {
+    rc = fail(ctx, BCGPU_ENOMEM, "host allocation failed while building the plan");
+  }
+  if (rc != BCGPU_OK) {
+    if (p) bc_plan_destroy(p);
+    return rc;
+  }
   *out = p;
   return BCGPU_OK;
 }
@@ -587,13 +616,17 @@ extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t
   const int64_t n = bc_plan_num_units(p);
   if (begin < 0 || end < begin || end > n) return -BCGPU_EINVAL;
   std::vector<int64_t> ids;
-  if (p->bp && begin < p->n_bat) bcg::batched_unit_sources(p->bp, begin, std::min(end, p->n_bat), ids);
-  for (int64_t i = std::max(begin, p->n_bat) - p->n_bat; i < end - p->n_bat; ++i) {  // per-source items
-    const auto &it = p->h_items[i];
-    const int64_t vo = p->h_vtx_off[it.bcc];
-    if (it.own) ids.push_back(vo + it.src);
-    for (int32_t c = it.c0; c < it.c1; ++c)
-      for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
+  try {
+    if (p->bp && begin < p->n_bat) bcg::batched_unit_sources(p->bp, begin, std::min(end, p->n_bat), ids);
+    for (int64_t i = std::max(begin, p->n_bat) - p->n_bat; i < end - p->n_bat; ++i) {  // per-source items
+      const auto &it = p->h_items[i];
+      const int64_t vo = p->h_vtx_off[it.bcc];
+      if (it.own) ids.push_back(vo + it.src);
+      for (int32_t c = it.c0; c < it.c1; ++c)
+        for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
+    }
+  } catch (const std::bad_alloc &) {
+    return -BCGPU_ENOMEM;
   }
   for (int64_t i = 0; i < (int64_t)ids.size() && i < cap; ++i) out[i] = ids[i];
   return (int64_t)ids.size();
@@ -723,18 +756,20 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
 }
 
 extern "C" int bc_plan_read(bc_plan *p, double *bc_out) {
-  if (!p || !bc_out) return BCGPU_EINVAL;
-  CK(p->ctx, cudaSetDevice(p->ctx->device));
-  int rc = check_dev_err(p);
-  if (rc) return rc;
-  std::vector<double> packed((size_t)p->n_packed);
-  if (p->n_packed)
-    CK(p->ctx, cudaMemcpyAsync(packed.data(), p->bc, sizeof(double) * (size_t)p->n_packed, cudaMemcpyDeviceToHost,
-                               p->ctx->stream));
-  CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
-  for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] = p->art.empty() ? 0.0 : p->art[v];
-  for (int64_t k = 0; k < p->n_packed; ++k) bc_out[p->orig[k]] += packed[k];  // fixed order: deterministic
-  return BCGPU_OK;
+  return guard(p ? p->ctx : nullptr, [&]() -> int {
+    if (!p || !bc_out) return BCGPU_EINVAL;
+    CK(p->ctx, cudaSetDevice(p->ctx->device));
+    int rc = check_dev_err(p);
+    if (rc) return rc;
+    std::vector<double> packed((size_t)p->n_packed);
+    if (p->n_packed)
+      CK(p->ctx, cudaMemcpyAsync(packed.data(), p->bc, sizeof(double) * (size_t)p->n_packed, cudaMemcpyDeviceToHost,
+                                 p->ctx->stream));
+    CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+    for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] = p->art.empty() ? 0.0 : p->art[v];
+    for (int64_t k = 0; k < p->n_packed; ++k) bc_out[p->orig[k]] += packed[k];  // fixed order: deterministic
+    return BCGPU_OK;
+  });
 }
 
 extern "C" int bc_plan_source_rows(bc_plan *p, int64_t packed, int32_t *d_out, double *sigma_out) {
@@ -805,12 +840,16 @@ int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool
 }  // namespace
 
 extern "C" int bc_run_bccs(bc_ctx *ctx, const bc_bccs *bccs, double *bc_out, bc_stats *stats) {
-  return run_units(ctx, bccs, 0, 0, true, true, bc_out, stats);
+  return guard(ctx, [&]() -> int {
+    return run_units(ctx, bccs, 0, 0, true, true, bc_out, stats);
+  });
 }
 
 extern "C" int bc_run_bccs_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t unit_begin, int64_t unit_end,
                                  int32_t with_art, double *bc_out, bc_stats *stats) {
-  return run_units(ctx, bccs, unit_begin, unit_end, false, with_art != 0, bc_out, stats);
+  return guard(ctx, [&]() -> int {
+    return run_units(ctx, bccs, unit_begin, unit_end, false, with_art != 0, bc_out, stats);
+  });
 }
 
 namespace {
@@ -866,109 +905,113 @@ int run_one(bc_ctx *ctx, OneBcc &o, const std::vector<bcg::PlainItem> &items, st
 
 extern "C" int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m,
                              const int32_t *req_nodes, int32_t n_req, const int32_t *reach, float *bc, double *time_s) {
-  if (!ctx || !bc || (n_req > 0 && !req_nodes)) return fail(ctx, BCGPU_EINVAL, "null argument");
-  int rc = check_csr(ctx, R, C, n, m, reach);
-  if (rc) return rc;
-  OneBcc o;
-  o.vtx_off = {0, n};
-  o.row.assign(R, R + n + 1);
-  o.col.assign(C, C + m);
-  o.reach.assign(reach, reach + n);
-  o.orig.resize(n);
-  for (int32_t v = 0; v < n; ++v) o.orig[v] = v;
-  o.n_plain = {n};
-  o.chain_off = {0, 0};
-  o.finish(n);
-  std::vector<bcg::PlainItem> items;
-  for (int32_t i = 0; i < n_req; ++i) {
-    if (req_nodes[i] < 0 || req_nodes[i] >= n) return fail(ctx, BCGPU_EINVAL, "req_nodes out of range");
-    items.push_back({0, req_nodes[i], 0, 0, 1});
-  }
-  std::vector<double> out;
-  rc = run_one(ctx, o, items, out, time_s);
-  if (rc) return rc;
-  for (int32_t v = 0; v < n; ++v) bc[v] = (float)out[v];  // overwritten, as the reference's free call
-  return BCGPU_OK;
+  return guard(ctx, [&]() -> int {
+    if (!ctx || !bc || (n_req > 0 && !req_nodes)) return fail(ctx, BCGPU_EINVAL, "null argument");
+    int rc = check_csr(ctx, R, C, n, m, reach);
+    if (rc) return rc;
+    OneBcc o;
+    o.vtx_off = {0, n};
+    o.row.assign(R, R + n + 1);
+    o.col.assign(C, C + m);
+    o.reach.assign(reach, reach + n);
+    o.orig.resize(n);
+    for (int32_t v = 0; v < n; ++v) o.orig[v] = v;
+    o.n_plain = {n};
+    o.chain_off = {0, 0};
+    o.finish(n);
+    std::vector<bcg::PlainItem> items;
+    for (int32_t i = 0; i < n_req; ++i) {
+      if (req_nodes[i] < 0 || req_nodes[i] >= n) return fail(ctx, BCGPU_EINVAL, "req_nodes out of range");
+      items.push_back({0, req_nodes[i], 0, 0, 1});
+    }
+    std::vector<double> out;
+    rc = run_one(ctx, o, items, out, time_s);
+    if (rc) return rc;
+    for (int32_t v = 0; v < n; ++v) bc[v] = (float)out[v];  // overwritten, as the reference's free call
+    return BCGPU_OK;
+  });
 }
 
 extern "C" int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, int32_t m,
                                const int32_t *active, int32_t n_active, int32_t n_ears, const int32_t *lnode,
                                const int32_t *rnode, const int32_t *cnt, const int32_t *off, const int32_t *nodes,
                                const int32_t *ld, const int32_t *rd, const int32_t *reach, float *bc, double *time_s) {
-  if (!ctx || !bc || (n_active > 0 && !active) || (n_ears > 0 && (!lnode || !rnode || !cnt || !off || !nodes || !ld || !rd)))
-    return fail(ctx, BCGPU_EINVAL, "null argument");
-  int rc = check_csr(ctx, R, C, n, m, reach);
-  if (rc) return rc;
-  // New ids: every vertex not on an ear first (original order), then each ear's
-  // vertices from its left end (ld = 1, 2, ...) to its right end.
-  std::vector<int32_t> nid((size_t)n, -1), old;
-  std::vector<char> on_ear((size_t)n, 0), is_active((size_t)n, 0);
-  for (int32_t i = 0; i < n_active; ++i) {
-    if (active[i] < 0 || active[i] >= n) return fail(ctx, BCGPU_EINVAL, "active vertex out of range");
-    is_active[active[i]] = 1;
-  }
-  for (int32_t e = 0; e < n_ears; ++e)
-    for (int32_t j = 0; j < cnt[e]; ++j) {
-      int32_t z = nodes[off[e] + j];
-      if (z < 0 || z >= n || on_ear[z]) return fail(ctx, BCGPU_EINVAL, "ear vertex out of range or repeated");
-      on_ear[z] = 1;
+  return guard(ctx, [&]() -> int {
+    if (!ctx || !bc || (n_active > 0 && !active) || (n_ears > 0 && (!lnode || !rnode || !cnt || !off || !nodes || !ld || !rd)))
+      return fail(ctx, BCGPU_EINVAL, "null argument");
+    int rc = check_csr(ctx, R, C, n, m, reach);
+    if (rc) return rc;
+    // New ids: every vertex not on an ear first (original order), then each ear's
+    // vertices from its left end (ld = 1, 2, ...) to its right end.
+    std::vector<int32_t> nid((size_t)n, -1), old;
+    std::vector<char> on_ear((size_t)n, 0), is_active((size_t)n, 0);
+    for (int32_t i = 0; i < n_active; ++i) {
+      if (active[i] < 0 || active[i] >= n) return fail(ctx, BCGPU_EINVAL, "active vertex out of range");
+      is_active[active[i]] = 1;
     }
-  for (int32_t v = 0; v < n; ++v)
-    if (!on_ear[v]) { nid[v] = (int32_t)old.size(); old.push_back(v); }
-  const int32_t nplain = (int32_t)old.size();
-  // ears sorted by the new id of their left end (chains are grouped by owner)
-  std::vector<int32_t> order((size_t)n_ears);
-  for (int32_t e = 0; e < n_ears; ++e) {
-    order[e] = e;
-    if (lnode[e] < 0 || lnode[e] >= n || rnode[e] < 0 || rnode[e] >= n || on_ear[lnode[e]] || on_ear[rnode[e]] ||
-        lnode[e] == rnode[e] || !is_active[lnode[e]] || cnt[e] < 1)
-      return fail(ctx, BCGPU_EINVAL, "ear endpoints must be distinct active vertices");
-  }
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int32_t a, int32_t b) { return std::make_pair(nid[lnode[a]], nid[rnode[a]]) <
-                                                      std::make_pair(nid[lnode[b]], nid[rnode[b]]); });
-  OneBcc o;
-  for (int32_t e : order) {
-    std::vector<std::pair<int32_t, int32_t>> byld;
-    for (int32_t j = 0; j < cnt[e]; ++j) {
-      const int32_t k = off[e] + j;
-      if (ld[k] < 1 || ld[k] > cnt[e] || ld[k] + rd[k] != cnt[e] + 1)
-        return fail(ctx, BCGPU_EINVAL, "ear distances must be 1..cnt with ld + rd = cnt + 1 (unit weights)");
-      byld.push_back({ld[k], nodes[k]});
+    for (int32_t e = 0; e < n_ears; ++e)
+      for (int32_t j = 0; j < cnt[e]; ++j) {
+        int32_t z = nodes[off[e] + j];
+        if (z < 0 || z >= n || on_ear[z]) return fail(ctx, BCGPU_EINVAL, "ear vertex out of range or repeated");
+        on_ear[z] = 1;
+      }
+    for (int32_t v = 0; v < n; ++v)
+      if (!on_ear[v]) { nid[v] = (int32_t)old.size(); old.push_back(v); }
+    const int32_t nplain = (int32_t)old.size();
+    // ears sorted by the new id of their left end (chains are grouped by owner)
+    std::vector<int32_t> order((size_t)n_ears);
+    for (int32_t e = 0; e < n_ears; ++e) {
+      order[e] = e;
+      if (lnode[e] < 0 || lnode[e] >= n || rnode[e] < 0 || rnode[e] >= n || on_ear[lnode[e]] || on_ear[rnode[e]] ||
+          lnode[e] == rnode[e] || !is_active[lnode[e]] || cnt[e] < 1)
+        return fail(ctx, BCGPU_EINVAL, "ear endpoints must be distinct active vertices");
     }
-    std::sort(byld.begin(), byld.end());
-    o.chain_start.push_back((int32_t)old.size());
-    o.chain_len.push_back(cnt[e]);
-    o.chain_l.push_back(nid[lnode[e]]);
-    o.chain_r.push_back(nid[rnode[e]]);
-    for (auto &pr : byld) { nid[pr.second] = (int32_t)old.size(); old.push_back(pr.second); }
-  }
-  if ((int32_t)old.size() != n) return fail(ctx, BCGPU_EINVAL, "relabelling failed");
-  o.vtx_off = {0, n};
-  o.row.assign((size_t)n + 1, 0);
-  for (int32_t k = 0; k < n; ++k) o.row[k + 1] = o.row[k] + (R[old[k] + 1] - R[old[k]]);
-  o.col.resize((size_t)m);
-  o.reach.resize((size_t)n);
-  o.orig.resize((size_t)n);
-  for (int32_t k = 0; k < n; ++k) {
-    int64_t w = o.row[k];
-    for (int32_t e = R[old[k]]; e < R[old[k] + 1]; ++e) o.col[w++] = nid[C[e]];
-    o.reach[k] = reach[old[k]];
-    o.orig[k] = k;  // results are mapped back below
-  }
-  o.n_plain = {nplain};
-  o.chain_off = {0, (int64_t)o.chain_start.size()};
-  o.finish(n);
-  std::vector<bcg::PlainItem> items;
-  size_t c = 0;
-  for (int32_t k = 0; k < nplain; ++k) {
-    size_t c0 = c;
-    while (c < o.chain_l.size() && o.chain_l[c] == k) ++c;
-    if (is_active[old[k]] || c > c0) items.push_back({0, k, (int32_t)c0, (int32_t)c, is_active[old[k]] ? 1 : 0});
-  }
-  std::vector<double> out;
-  rc = run_one(ctx, o, items, out, time_s);
-  if (rc) return rc;
-  for (int32_t k = 0; k < n; ++k) bc[old[k]] += (float)out[k];  // added, as the reference seeds from bc
-  return BCGPU_OK;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return std::make_pair(nid[lnode[a]], nid[rnode[a]]) <
+                                                        std::make_pair(nid[lnode[b]], nid[rnode[b]]); });
+    OneBcc o;
+    for (int32_t e : order) {
+      std::vector<std::pair<int32_t, int32_t>> byld;
+      for (int32_t j = 0; j < cnt[e]; ++j) {
+        const int32_t k = off[e] + j;
+        if (ld[k] < 1 || ld[k] > cnt[e] || ld[k] + rd[k] != cnt[e] + 1)
+          return fail(ctx, BCGPU_EINVAL, "ear distances must be 1..cnt with ld + rd = cnt + 1 (unit weights)");
+        byld.push_back({ld[k], nodes[k]});
+      }
+      std::sort(byld.begin(), byld.end());
+      o.chain_start.push_back((int32_t)old.size());
+      o.chain_len.push_back(cnt[e]);
+      o.chain_l.push_back(nid[lnode[e]]);
+      o.chain_r.push_back(nid[rnode[e]]);
+      for (auto &pr : byld) { nid[pr.second] = (int32_t)old.size(); old.push_back(pr.second); }
+    }
+    if ((int32_t)old.size() != n) return fail(ctx, BCGPU_EINVAL, "relabelling failed");
+    o.vtx_off = {0, n};
+    o.row.assign((size_t)n + 1, 0);
+    for (int32_t k = 0; k < n; ++k) o.row[k + 1] = o.row[k] + (R[old[k] + 1] - R[old[k]]);
+    o.col.resize((size_t)m);
+    o.reach.resize((size_t)n);
+    o.orig.resize((size_t)n);
+    for (int32_t k = 0; k < n; ++k) {
+      int64_t w = o.row[k];
+      for (int32_t e = R[old[k]]; e < R[old[k] + 1]; ++e) o.col[w++] = nid[C[e]];
+      o.reach[k] = reach[old[k]];
+      o.orig[k] = k;  // results are mapped back below
+    }
+    o.n_plain = {nplain};
+    o.chain_off = {0, (int64_t)o.chain_start.size()};
+    o.finish(n);
+    std::vector<bcg::PlainItem> items;
+    size_t c = 0;
+    for (int32_t k = 0; k < nplain; ++k) {
+      size_t c0 = c;
+      while (c < o.chain_l.size() && o.chain_l[c] == k) ++c;
+      if (is_active[old[k]] || c > c0) items.push_back({0, k, (int32_t)c0, (int32_t)c, is_active[old[k]] ? 1 : 0});
+    }
+    std::vector<double> out;
+    rc = run_one(ctx, o, items, out, time_s);
+    if (rc) return rc;
+    for (int32_t k = 0; k < n; ++k) bc[old[k]] += (float)out[k];  // added, as the reference seeds from bc
+    return BCGPU_OK;
+  });
 }

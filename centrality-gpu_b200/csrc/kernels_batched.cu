@@ -50,6 +50,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <numeric>
 #include <type_traits>
 #include <vector>
@@ -1154,15 +1155,14 @@ int bcc_ecc(const int64_t *row, const int32_t *col, int64_t vo, int32_t nb, std:
 
 }  // namespace
 
-int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row, const int32_t *col,
-                   const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
-                   const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
-                   BatchedPlan **out, std::string *msg) {
-  (void)row; (void)col;
-  auto *P = new BatchedPlan;
+namespace {
+
+// Fills P (allocated by batched_create, which releases it on any failure).
+int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *reach, const int64_t *vtx_off,
+                  const int32_t *chain_start, const int32_t *chain_len, const int32_t *chain_l, const int32_t *chain_r,
+                  double *bc, int *err, cudaStream_t stream, BatchedPlan *P, std::string *msg) {
   auto bail = [&](int code, const std::string &m) {
     if (msg) *msg = m;
-    batched_destroy(P);
     return code;
   };
   P->f32 = cfg.delta_fp32c;
@@ -1502,6 +1502,29 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
   P->smem = smem;
   if (per_sm < 1) return bail(BCGPU_ECUDA, "batched kernel does not fit an SM");
   P->grid = sms * per_sm;
+  return BCGPU_OK;
+}
+
+}  // namespace
+
+int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row, const int32_t *col,
+                   const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
+                   const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
+                   BatchedPlan **out, std::string *msg) {
+  (void)row; (void)col;
+  BatchedPlan *P = nullptr;
+  int rc;
+  try {  // a host allocation that throws releases the partial plan like any other failure
+    P = new BatchedPlan;
+    rc = batched_build(B, cfg, reach, vtx_off, chain_start, chain_len, chain_l, chain_r, bc, err, stream, P, msg);
+  } catch (const std::bad_alloc &) {
+    if (msg) *msg = "host allocation failed while building the passes";
+    rc = BCGPU_ENOMEM;
+  }
+  if (rc != BCGPU_OK) {
+    batched_destroy(P);
+    return rc;
+  }
   *out = P;
   return BCGPU_OK;
 }
