@@ -1,0 +1,269 @@
+"""libbcgpu's host logic on the CPU: the library's own objects (built by
+build.py) linked against a stand-in CUDA runtime (tests/stub_cudart/: device
+memory is host memory, kernels are counted but do not run). This reaches
+the code the rest of the CPU suite cannot -- plan construction, routing
+between the two schedules, the pass and work-item scheduling, the unit
+bookkeeping behind TEPS, CUDA-graph record/replay and the input checks of
+every entry point. BC values are not checked here (no kernel runs): the GPU
+tests pin them. Each check runs in a subprocess that loads the stub build
+through BCGPU_LIB_DIR, so this process keeps the real library."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from helpers import ROOT
+
+PKG = ROOT / "centrality-gpu_b200"
+STUB = ROOT / "tests" / "stub_cudart"
+BUILD = STUB / "_build"
+
+PRELUDE = """
+import json, sys
+import ctypes as C
+import numpy as np
+sys.path.insert(0, {tests!r})
+from helpers import GOLDEN_CASES, graphs, load_case, pkg
+P = pkg()
+L = P.lib()
+L.stub_cudart_launches.restype = C.c_longlong
+G = graphs()
+out = {{}}
+
+def decomp(n, u, v):
+    return P.Decomposition(P.Graph.from_edges(n, u, v))
+
+def raises(f):
+    try:
+        f()
+    except P.BcError as e:
+        return [int(e.code), str(e)]
+    return None
+"""
+
+
+@pytest.fixture(scope="module")
+def stub_dir():
+    objs = sorted((PKG / "_build").glob("*.o"))
+    if len(objs) < 5:
+        sys.path.insert(0, str(PKG))
+        import build as pkg_build  # centrality-gpu_b200/build.py
+        pkg_build.build()
+        objs = sorted((PKG / "_build").glob("*.o"))
+    BUILD.mkdir(exist_ok=True)
+    stub_o = BUILD / "stub_cudart.o"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-I/usr/local/cuda/include", "-c",
+                    str(STUB / "stub_cudart.cpp"), "-o", str(stub_o)], check=True)
+    subprocess.run(["g++", "-shared", "-o", str(BUILD / "libbcgpu.so")] + [str(o) for o in objs] +
+                   [str(stub_o), "-lgomp", "-Wl,--no-undefined"], check=True)
+    return BUILD
+
+
+def run_stub(stub_dir, code):
+    env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir))
+    script = PRELUDE.format(tests=str(ROOT / "tests")) + code + "\nprint(json.dumps(out))\n"
+    r = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_stub_library_is_loaded(stub_dir):
+    res = run_stub(stub_dir, "out['lib'] = str(P.LIB_PATH)\nout['stub'] = hasattr(L, 'stub_cudart_launches')")
+    assert res["lib"] == str(stub_dir / "libbcgpu.so") and res["stub"]
+
+
+def test_every_source_is_scheduled_exactly_once(stub_dir):
+    """In every schedule and batch width, the units of a plan hold every
+    vertex of every BCC exactly once as a source, and the work they report
+    (sources, TEPS arcs, vertex visits) adds up to the BCCs' own."""
+    res = run_stub(stub_dir, """
+graphs_ = [("small2000", G.gen_small(1)),
+           ("rmat11", G.gen_rmat(11, 16, chain_frac=0.2, chain_hi=8, seed=2)),
+           ("grid30", G.gen_grid(30, leaves=100, seed=3)),
+           ("ba12", G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3])]
+graphs_ += [(c, load_case(c)[:3]) for c in GOLDEN_CASES]
+modes = [dict(mode=P.MODE_PLAIN), dict(mode=P.MODE_BATCHED), dict(mode=P.MODE_BATCHED, plain_core=500),
+         dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=32),
+         dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=128),
+         dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=1024)]
+bad = []
+for name, (n, u, v) in graphs_:
+    d = decomp(n, u, v)
+    a = d.arrays()
+    nb = np.diff(a["vtx_off"])
+    arcs = a["row"][a["vtx_off"][1:]] - a["row"][a["vtx_off"][:-1]]
+    want = [int(a["n_packed"]), int((nb * arcs).sum()), int((nb * nb).sum())]
+    for opts in modes:
+        ctx = P.Context(**opts)
+        plan = ctx.plan(d)
+        ids = plan.unit_sources()
+        if sorted(ids.tolist()) != list(range(int(a["n_packed"]))):
+            bad.append([name, str(opts), "sources"])
+        if list(plan.unit_work()) != want:
+            bad.append([name, str(opts), "work", list(plan.unit_work()), want])
+        for k in range(0, plan.n_units, max(1, plan.n_units // 7)):
+            if len(plan.unit_sources(k, k + 1)) != plan.unit_work(k, k + 1)[0]:
+                bad.append([name, str(opts), "unit", k])
+        plan.close()
+        ctx.close()
+out["bad"] = bad
+""")
+    assert res["bad"] == []
+
+
+def test_routing_between_the_schedules(stub_dir):
+    """Twelve BA graphs with the core threshold at 500: the multi-source
+    passes come first and hold exactly the sources of the five BCCs whose
+    cores reach it; the per-source items hold the seven others; one run over
+    all units launches each schedule once. A deep BCC is routed
+    per-source by its depth alone (60x60 grid); forcing multi-source passes
+    overrides it."""
+    res = run_stub(stub_dir, """
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
+d = decomp(n, u, v)
+a = d.arrays()
+big = [b for b in range(a["n_bcc"]) if a["n_plain"][b] >= 500]
+owner = np.repeat(np.arange(a["n_bcc"]), np.diff(a["vtx_off"]))
+ctx = P.Context(mode=P.MODE_BATCHED, plain_core=500)
+plan = ctx.plan(d)
+kinds = [bool(np.isin(owner[plan.unit_sources(k, k + 1)], big).all()) for k in range(plan.n_units)]
+first_item = kinds.index(False)
+out["big"] = len(big)
+out["passes_first"] = all(kinds[:first_item]) and not any(kinds[first_item:])
+out["pass_sources"] = int(plan.unit_work(0, first_item)[0])
+out["big_vertices"] = int(sum(a["vtx_off"][b + 1] - a["vtx_off"][b] for b in big))
+l0 = L.stub_cudart_launches()
+st = plan.run()
+out["launches"] = [st["kernel_launches"], L.stub_cudart_launches() - l0]
+plan.close()
+ctx.close()
+g = decomp(*G.gen_grid(60, delete_frac=0.0, sub_p=0.0, leaves=0, seed=9))  # levels deeper than 96 from any vertex
+ga = g.arrays()
+units = {}
+for name, opts in (("plain", dict(mode=P.MODE_PLAIN)), ("auto", dict(mode=P.MODE_BATCHED, plain_core=100)),
+                   ("multi", dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=128))):
+    c = P.Context(**opts)
+    p = c.plan(g)
+    units[name] = p.n_units
+    p.close()
+    c.close()
+out["grid_core"] = int(ga["n_plain"][0])
+out["grid_units"] = units
+""")
+    assert res["big"] == 5 and res["passes_first"]
+    assert res["pass_sources"] == res["big_vertices"]
+    assert res["launches"] == [2, 2]
+    assert res["grid_core"] >= 100  # above the threshold given: only the depth routes it
+    assert res["grid_units"]["auto"] == res["grid_units"]["plain"]
+    assert res["grid_units"]["multi"] == -(-3600 // 128)
+
+
+def test_graph_mode_records_then_replays(stub_dir):
+    """Recording enqueues nothing; each replay of a recorded range launches
+    what the range holds; a range run without recording is recorded on its
+    first run; without graph mode, recording is refused."""
+    res = run_stub(stub_dir, """
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]  # both schedules at this threshold
+d = decomp(n, u, v)
+c = P.Context(mode=P.MODE_BATCHED, plain_core=500, graph=True)
+plan = c.plan(d)
+k = plan.n_units
+l0 = L.stub_cudart_launches()
+plan.record(0, k)
+out["after_record"] = L.stub_cudart_launches() - l0
+st1 = plan.run(0, k)
+l1 = L.stub_cudart_launches()
+st2 = plan.run(0, k)
+out["replays"] = [st1["kernel_launches"], st2["kernel_launches"], L.stub_cudart_launches() - l1]
+st3 = plan.run(1, k)  # not recorded before: recorded on this run
+out["fresh"] = st3["kernel_launches"]
+plan.close()
+c.close()
+c = P.Context(mode=P.MODE_PLAIN)
+plan = c.plan(d)
+out["refused"] = raises(lambda: plan.record(0, 1))
+plan.close()
+c.close()
+""")
+    assert res["after_record"] == 0
+    assert res["replays"] == [2, 2, 2]
+    assert res["fresh"] == 2
+    assert res["refused"] is not None and res["refused"][0] == 1
+
+
+def test_malformed_input_is_rejected(stub_dir):
+    """Every structural check of the packed input, and of the begin_gpu
+    mirrors, returns BCGPU_EINVAL (1) with its message; sizes beyond the
+    no-allocation variant's fixed scratch return BCGPU_EOVERFLOW (6); a
+    workspace limit below one BCC's rows returns BCGPU_ENOMEM (3)."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_small(1)
+d = decomp(n, u, v)
+a = d.arrays()
+ctx = P.Context(mode=P.MODE_PLAIN)
+
+class Packed:  # a bc_bccs over numpy copies that a case may corrupt
+    def __init__(self, **change):
+        self.arr = {k: np.array(x, copy=True) for k, x in a.items() if isinstance(x, np.ndarray)}
+        for k, x in change.items():
+            self.arr[k] = x(self.arr[k])
+        b = P.BcBccs()
+        b.n_bcc, b.n_orig, b.n_packed, b.n_arcs, b.n_chains = a["n_bcc"], a["n_orig"], a["n_packed"], a["n_arcs"], a["n_chains"]
+        for k, x in self.arr.items():
+            ptype = dict(b._fields_)[k]
+            setattr(b, k, x.ctypes.data_as(ptype))
+        self.view = C.pointer(b)
+
+def bump(i, val):
+    def f(x):
+        x[i] = val
+        return x
+    return f
+
+cases = {
+    "ok": Packed(),
+    "col": Packed(col=bump(5, 10 ** 6)),
+    "neg_col": Packed(col=bump(5, -1)),
+    "reach": Packed(reach=bump(3, -2)),
+    "orig": Packed(orig=bump(3, 10 ** 7)),
+    "n_plain": Packed(n_plain=bump(0, 0)),
+    "chain_len": Packed(chain_len=bump(0, 0)),
+    "row": Packed(row=bump(5, 0)),
+}
+res = {}
+for name, pk in cases.items():
+    res[name] = raises(lambda: ctx.run(pk))
+out["packed"] = res
+R = [0, 2, 4, 6]
+Cc = [1, 2, 0, 2, 0, 1]
+out["free_ok"] = raises(lambda: P.begin_gpu_free(ctx, R, Cc, 3, 6, [0, 1, 2], [0, 0, 0], np.zeros(3, np.float32)))
+out["free_small"] = raises(lambda: P.begin_gpu_free(ctx, [0, 1, 2], [1, 0], 2, 2, [0], [0, 0], np.zeros(2, np.float32)))
+out["free_col"] = raises(lambda: P.begin_gpu_free(ctx, [0, 2, 4, 6], [1, 2, 0, 2, 0, 9], 3, 6, [0], [0, 0, 0], np.zeros(3, np.float32)))
+out["free_src"] = raises(lambda: P.begin_gpu_free(ctx, R, Cc, 3, 6, [7], [0, 0, 0], np.zeros(3, np.float32)))
+# a 4-cycle 0-1-2-3 seen as ears (0, 2) through 1 and 3
+R4, C4 = [0, 2, 4, 6, 8], [1, 3, 0, 2, 1, 3, 0, 2]
+good = [(0, 2, [(1, 1, 1)]), (0, 2, [(1, 3, 1)])]
+out["active_ok"] = raises(lambda: P.begin_gpu_active(ctx, R4, C4, 4, 8, [0, 2], good, [0] * 4, np.zeros(4, np.float32)))
+out["active_dist"] = raises(lambda: P.begin_gpu_active(ctx, R4, C4, 4, 8, [0, 2], [(0, 2, [(2, 1, 2)])], [0] * 4,
+                                                      np.zeros(4, np.float32)))
+out["active_end"] = raises(lambda: P.begin_gpu_active(ctx, R4, C4, 4, 8, [2], good, [0] * 4, np.zeros(4, np.float32)))
+out["noalloc_big"] = raises(lambda: P.begin_gpu_free_noalloc(ctx, 16, 16, 20000, 4, 16, 1, 16, 16))
+ctx.close()
+small = P.Context(mode=P.MODE_PLAIN, workspace_limit=120 << 10)  # below two slots of rows
+out["limit"] = raises(lambda: small.run(d))
+small.close()
+""")
+    p = res["packed"]
+    assert p["ok"] is None
+    want = {"col": "column id outside its BCC", "neg_col": "negative column id", "reach": "orig/reach out of range",
+            "orig": "orig/reach out of range", "n_plain": "n_plain out of range", "chain_len": "chain out of range",
+            "row": "row offsets decrease"}
+    for name, msg in want.items():
+        assert p[name] is not None and p[name][0] == 1 and msg in p[name][1], (name, p[name])
+    assert res["free_ok"] is None and res["active_ok"] is None
+    for name in ("free_small", "free_col", "free_src", "active_dist", "active_end"):
+        assert res[name] is not None and res[name][0] == 1, (name, res[name])
+    assert res["noalloc_big"][0] == 6 and "16384" in res["noalloc_big"][1]
+    assert res["limit"][0] == 3 and "exceeds the limit" in res["limit"][1]
