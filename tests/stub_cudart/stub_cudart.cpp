@@ -24,6 +24,8 @@ namespace {
 // other objects' static initialisers, possibly before this file's globals exist.
 std::mutex g_mu;  // constant-initialised
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_live{0};        // device allocations not yet freed
+std::atomic<long long> g_fail_after{-1};  // allocations left before one fails (-1: none fails)
 std::map<const void *, size_t> &var_size() {  // registered __device__ variables: host shadow -> size
   static std::map<const void *, size_t> m;
   return m;
@@ -74,6 +76,9 @@ extern "C" {
 
 // ---- test hooks
 long long stub_cudart_launches() { return g_launches.load(); }
+long long stub_cudart_live_allocs() { return g_live.load(); }
+// The (n+1)-th device allocation from now on fails (n < 0: none fails).
+void stub_cudart_fail_malloc_after(long long n) { g_fail_after = n; }
 
 // ---- module registration (called by nvcc-generated static initialisers)
 void **__cudaRegisterFatBinary(void *) {
@@ -132,12 +137,24 @@ cudaError_t cudaMemGetInfo(size_t *free_b, size_t *total_b) {
 
 // ---- memory
 cudaError_t cudaMalloc(void **p, size_t bytes) {
+  *p = nullptr;
+  if (g_fail_after.load() == 0) {
+    g_fail_after = -1;
+    return cudaErrorMemoryAllocation;
+  }
+  if (g_fail_after.load() > 0) --g_fail_after;
   *p = std::malloc(bytes ? bytes : 1);
-  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+  if (!*p) return cudaErrorMemoryAllocation;
+  ++g_live;
+  return cudaSuccess;
 }
-cudaError_t cudaFree(void *p) { std::free(p); return cudaSuccess; }
+cudaError_t cudaFree(void *p) {
+  if (p) --g_live;
+  std::free(p);
+  return cudaSuccess;
+}
 cudaError_t cudaMallocAsync(void **p, size_t bytes, cudaStream_t) { return cudaMalloc(p, bytes); }
-cudaError_t cudaFreeAsync(void *p, cudaStream_t) { std::free(p); return cudaSuccess; }
+cudaError_t cudaFreeAsync(void *p, cudaStream_t) { return cudaFree(p); }
 cudaError_t cudaMemcpyAsync(void *dst, const void *src, size_t bytes, cudaMemcpyKind, cudaStream_t s) {
   return on_stream(s, [=] { std::memcpy(dst, src, bytes); });
 }

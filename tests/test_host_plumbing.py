@@ -267,3 +267,40 @@ small.close()
         assert res[name] is not None and res[name][0] == 1, (name, res[name])
     assert res["noalloc_big"][0] == 6 and "16384" in res["noalloc_big"][1]
     assert res["limit"][0] == 3 and "exceeds the limit" in res["limit"][1]
+
+
+def test_failed_plan_builds_release_everything(stub_dir):
+    """A device allocation failing at any point of a plan build (PLAIN, and
+    multi-source with per-source items) returns BCGPU_ENOMEM (3) and leaves
+    no device allocation behind; the context stays usable."""
+    res = run_stub(stub_dir, """
+L.stub_cudart_live_allocs.restype = C.c_longlong
+L.stub_cudart_fail_malloc_after.argtypes = [C.c_longlong]
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
+d = decomp(n, u, v)
+seen = {}
+leaks = []
+for name, opts in (("plain", dict(mode=P.MODE_PLAIN)), ("mixed", dict(mode=P.MODE_BATCHED, plain_core=500))):
+    ctx = P.Context(**opts)
+    base = L.stub_cudart_live_allocs()
+    codes = []
+    for k in range(80):
+        L.stub_cudart_fail_malloc_after(k)
+        r = raises(lambda: ctx.run(d))
+        codes.append(0 if r is None else r[0])
+        if L.stub_cudart_live_allocs() != base:
+            leaks.append([name, k, L.stub_cudart_live_allocs() - base])
+        if r is None:
+            break
+    L.stub_cudart_fail_malloc_after(-1)
+    ok = raises(lambda: ctx.run(d))
+    seen[name] = [codes, ok]
+    ctx.close()
+out["seen"] = seen
+out["leaks"] = leaks
+""")
+    assert res["leaks"] == []
+    for name, (codes, ok) in res["seen"].items():
+        assert codes[-1] == 0 and len(codes) > 10, name  # every allocation of the build was made to fail once
+        assert set(codes[:-1]) == {3}, (name, codes)
+        assert ok is None
