@@ -25,6 +25,7 @@ namespace {
 std::mutex g_mu;  // constant-initialised
 std::atomic<long long> g_launches{0};
 std::atomic<long long> g_live{0};        // device allocations not yet freed
+std::atomic<long long> g_mallocs{0};     // device allocation calls so far
 std::atomic<long long> g_fail_after{-1};  // allocations left before one fails (-1: none fails)
 std::map<const void *, size_t> &var_size() {  // registered __device__ variables: host shadow -> size
   static std::map<const void *, size_t> m;
@@ -77,6 +78,7 @@ extern "C" {
 // ---- test hooks
 long long stub_cudart_launches() { return g_launches.load(); }
 long long stub_cudart_live_allocs() { return g_live.load(); }
+long long stub_cudart_mallocs() { return g_mallocs.load(); }
 // The (n+1)-th device allocation from now on fails (n < 0: none fails).
 void stub_cudart_fail_malloc_after(long long n) { g_fail_after = n; }
 
@@ -137,6 +139,7 @@ cudaError_t cudaMemGetInfo(size_t *free_b, size_t *total_b) {
 
 // ---- memory
 cudaError_t cudaMalloc(void **p, size_t bytes) {
+  ++g_mallocs;
   *p = nullptr;
   if (g_fail_after.load() == 0) {
     g_fail_after = -1;

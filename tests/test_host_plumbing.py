@@ -304,3 +304,32 @@ out["leaks"] = leaks
         assert codes[-1] == 0 and len(codes) > 10, name  # every allocation of the build was made to fail once
         assert set(codes[:-1]) == {3}, (name, codes)
         assert ok is None
+
+
+def test_noalloc_entry_point_allocates_nothing(stub_dir):
+    """bc_begin_free_noalloc makes no device allocation on any call, the
+    first included (its scratch is the library's fixed __device__ array,
+    found with cudaGetSymbolAddress), and rejects sizes beyond it."""
+    res = run_stub(stub_dir, """
+L.stub_cudart_mallocs.restype = C.c_longlong
+n, u, v = G.gen_small(1)
+a = decomp(n, u, v).arrays()
+v0, v1 = int(a["vtx_off"][0]), int(a["vtx_off"][1])
+R = (a["row"][v0:v1 + 1] - a["row"][v0]).astype(np.int32)
+Cc = np.ascontiguousarray(a["col"][a["row"][v0]:a["row"][v1]], dtype=np.int32)
+reach = np.ascontiguousarray(a["reach"][v0:v1], dtype=np.int32)
+nb = v1 - v0
+src = np.arange(nb, dtype=np.int32)
+bc = np.zeros(nb, dtype=np.float64)
+ctx = P.Context(mode=P.MODE_PLAIN)
+m0 = L.stub_cudart_mallocs()
+for _ in range(3):  # device memory is host memory here: host arrays stand in for the caller's buffers
+    P.begin_gpu_free_noalloc(ctx, R.ctypes.data, Cc.ctypes.data, nb, len(Cc), src.ctypes.data, nb,
+                             reach.ctypes.data, bc.ctypes.data)
+out["mallocs"] = L.stub_cudart_mallocs() - m0
+out["too_big"] = raises(lambda: P.begin_gpu_free_noalloc(ctx, R.ctypes.data, Cc.ctypes.data, 16385, len(Cc),
+                                                         src.ctypes.data, 1, reach.ctypes.data, bc.ctypes.data))
+ctx.close()
+""")
+    assert res["mallocs"] == 0
+    assert res["too_big"][0] == 6
