@@ -370,3 +370,41 @@ def test_integration_python_example_runs(stub_dir, tmp_path):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.split() == ["4", "4"]
+
+
+def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
+    """The drop-in command's options, output format and exit codes, with the
+    in-tree betc loading the stand-in library (its RUNPATH yields to
+    LD_LIBRARY_PATH): `v bc` per vertex to --out, usage errors (1), unreadable
+    input (2), a rejected option value (4), an unwritable output (6)."""
+    from helpers import GOLDEN
+
+    betc = PKG / "lib" / "betc"
+    env = dict(os.environ, LD_LIBRARY_PATH=str(stub_dir))
+
+    def run(*args):
+        return subprocess.run([str(betc)] + [str(a) for a in args], env=env, capture_output=True, text=True,
+                              timeout=120, cwd=tmp_path)
+
+    g = GOLDEN / "sample4.txt"
+    n = int(g.read_text().split()[0])
+    out = tmp_path / "bc.txt"
+    for extra in ([], ["--mode", "plain"], ["--mode", "batched", "--delta", "fp64", "--batch", "64"]):
+        r = run(g, "--out", out, *extra)
+        assert r.returncode == 0, r.stderr
+        assert "GPU total time is" in r.stderr
+        rows = [ln.split() for ln in out.read_text().splitlines()]
+        assert [int(a) for a, _ in rows] == list(range(n))
+        [float(b) for _, b in rows]
+    r = run(g, "--quiet")
+    assert r.returncode == 0 and len(r.stdout.splitlines()) == n
+    assert run().returncode == 1
+    assert run(g, "--mode", "bogus").returncode == 1
+    assert run(g, "--delta").returncode == 1  # option without its value
+    assert run("-h").returncode == 0
+    r = run(tmp_path / "missing.txt")
+    assert r.returncode == 2 and "cannot be opened" in r.stderr
+    r = run(g, "--batch", "33")
+    assert r.returncode == 4 and "multiple of 32" in r.stderr
+    r = run(g, "--out", tmp_path / "no" / "such" / "dir.txt")
+    assert r.returncode == 6
