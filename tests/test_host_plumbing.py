@@ -46,12 +46,11 @@ def raises(f):
 
 @pytest.fixture(scope="module")
 def stub_dir():
-    objs = sorted((PKG / "_build").glob("*.o"))
-    if len(objs) < 5:
-        sys.path.insert(0, str(PKG))
-        import build as pkg_build  # centrality-gpu_b200/build.py
+    sys.path.insert(0, str(PKG))
+    import build as pkg_build  # centrality-gpu_b200/build.py: its source list names the library's objects
+    objs = [PKG / "_build" / (s + ".o") for s in pkg_build.CU_SOURCES + pkg_build.CXX_SOURCES]
+    if not all(o.exists() for o in objs):
         pkg_build.build()
-        objs = sorted((PKG / "_build").glob("*.o"))
     BUILD.mkdir(exist_ok=True)
     stub_o = BUILD / "stub_cudart.o"
     subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-I/usr/local/cuda/include", "-c",
