@@ -413,9 +413,11 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   std::vector<std::vector<int32_t>> ch_start((size_t)np_bcc), ch_len((size_t)np_bcc), ch_l((size_t)np_bcc),
       ch_r((size_t)np_bcc);
   std::vector<int64_t> n_cycle((size_t)np_bcc, 0);
-  int bad = 0;
-#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
-  for (int32_t i = 0; i < np_bcc; ++i) {
+  // Large BCCs are handled one at a time with their chain walks in parallel,
+  // the others one BCC per thread; the result is the same either way.
+  constexpr int32_t kBigBcc = 1 << 16;
+  auto order_bcc = [&](int32_t i, bool par) -> int {
+    int bad = 0;
     const int32_t b = order[i];
     const int32_t nb = (int32_t)(mem_off[b + 1] - mem_off[b]);
     const int64_t *sd = sdeg.data() + mem_off[b];
@@ -447,35 +449,89 @@ int decompose(const bc_graph *g, bc_decomp *D) {
       if ((int32_t)q.size() != nb) bad = 1;  // a BCC is connected
     }
     const int32_t nplain = (int32_t)old.size();
-    if (!cycle) {
+    if (!cycle && !bad) {
+      // Chains, in the order of a scan of the plain vertices (BFS order) and
+      // their arcs: a chain is numbered from whichever end comes first, its
+      // vertices from that end. Pass 1 finds, per plain vertex, the chains it
+      // owns (the far end comes later) and their lengths; prefix sums give
+      // every chain's and vertex's position; pass 2 writes them.
+      auto walk = [&](int32_t x, int32_t cur, int32_t *len) {  // far end of the chain leaving x through cur
+        int32_t prev = x, k = 0;
+        while (deg(cur) == 2 && k <= nb) {
+          const int32_t *c2 = adj(cur);
+          const int32_t nx = c2[0] == prev ? c2[1] : c2[0];
+          prev = cur;
+          cur = nx;
+          ++k;
+        }
+        *len = k;
+        return cur;
+      };
+      std::vector<int64_t> cnt((size_t)nplain + 1, 0), vcnt((size_t)nplain + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1024) if (par) reduction(| : bad)
       for (int32_t f = 0; f < nplain; ++f) {
-        int32_t x = old[f];
+        const int32_t x = old[f];
         const int32_t *a = adj(x);
         for (int32_t j = 0; j < deg(x); ++j) {
-          int32_t cur = a[j], prev = x;
-          if (deg(cur) != 2 || nid[cur] >= 0) continue;
-          int32_t start = (int32_t)old.size();
-          while (deg(cur) == 2) {
-            nid[cur] = (int32_t)old.size();
-            old.push_back(cur);
-            const int32_t *c2 = adj(cur);
-            int32_t nx = c2[0] == prev ? c2[1] : c2[0];
-            prev = cur;
-            cur = nx;
-          }
-          if (cur == x) bad = 1;  // a chain cannot return to its start inside a BCC
-          ch_start[i].push_back(start);
-          ch_len[i].push_back((int32_t)old.size() - start);
-          ch_l[i].push_back(f);
-          ch_r[i].push_back(cur);  // old id; mapped below
+          if (deg(a[j]) != 2) continue;
+          int32_t len;
+          const int32_t far = walk(x, a[j], &len);
+          if (len > nb || far == x) { bad = 1; continue; }  // no end, or a chain back to its start
+          if (nid[far] < f) continue;                       // numbered from its other end
+          cnt[f + 1] += 1;
+          vcnt[f + 1] += len;
         }
       }
-      for (auto &r : ch_r[i]) r = nid[r];
+      if (!bad) {
+        for (int32_t f = 0; f < nplain; ++f) {
+          cnt[f + 1] += cnt[f];
+          vcnt[f + 1] += vcnt[f];
+        }
+        old.resize((size_t)(nplain + vcnt[nplain]));
+        ch_start[i].resize((size_t)cnt[nplain]);
+        ch_len[i].resize((size_t)cnt[nplain]);
+        ch_l[i].resize((size_t)cnt[nplain]);
+        ch_r[i].resize((size_t)cnt[nplain]);
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
+        for (int32_t f = 0; f < nplain; ++f) {
+          const int32_t x = old[f];
+          const int32_t *a = adj(x);
+          int64_t c = cnt[f];
+          int32_t pos = (int32_t)(nplain + vcnt[f]);
+          for (int32_t j = 0; j < deg(x); ++j) {
+            if (deg(a[j]) != 2) continue;
+            int32_t len;
+            const int32_t far = walk(x, a[j], &len);
+            if (nid[far] < f) continue;
+            ch_start[i][c] = pos;
+            ch_len[i][c] = len;
+            ch_l[i][c] = f;
+            ch_r[i][c] = nid[far];
+            ++c;
+            int32_t cur = a[j], prev = x;
+            for (int32_t k = 0; k < len; ++k) {
+              nid[cur] = pos;
+              old[pos++] = cur;
+              const int32_t *c2 = adj(cur);
+              const int32_t nx = c2[0] == prev ? c2[1] : c2[0];
+              prev = cur;
+              cur = nx;
+            }
+          }
+        }
+      }
     }
     if ((int32_t)old.size() != nb) bad = 1;
     perm[i] = std::move(old);
     D->n_plain[i] = nplain;
-  }
+    return bad;
+  };
+  int bad = 0;
+  for (int32_t i = 0; i < np_bcc; ++i)
+    if (mem_off[order[i] + 1] - mem_off[order[i]] >= kBigBcc) bad |= order_bcc(i, true);
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+  for (int32_t i = 0; i < np_bcc; ++i)
+    if (mem_off[order[i] + 1] - mem_off[order[i]] < kBigBcc) bad |= order_bcc(i, false);
   if (bad) return BCGPU_EINVAL;
 
   // ---- write packed arrays
@@ -492,7 +548,6 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   D->col.assign((size_t)D->row[n_packed], 0);
   // Each BCC writes its own packed range: large BCCs one at a time with their
   // vertices in parallel, the others one BCC per thread.
-  constexpr int32_t kBigBcc = 1 << 16;
   auto write_bcc = [&](int32_t i, bool inner_parallel) {
     const int32_t b = order[i];
     const int32_t nb = (int32_t)perm[i].size();
