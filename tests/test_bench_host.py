@@ -44,3 +44,33 @@ def test_shards_partition_the_steps():
         got = [multigpu.shard(steps, r, world) for r in range(world)]
         assert sorted(x for g in got for x in g) == steps
         assert max(map(len, got)) - min(map(len, got)) <= 1
+
+
+def test_reference_arm_line(tmp_path):
+    """bench.py --impl reference (the reference method's CPU path on the host
+    cores) prints one JSON line with this engine's metric, unit and
+    direction, its cpu_baseline and a zero-copy e2e; under torchrun every rank
+    but 0 exits 0 without output."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    from helpers import ROOT
+
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", "small", "--steps", "2",
+           "--warmup", "1", "--ref-step-s", "0.2"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC
+    assert d["unit"] == "GTEPS" and d["higher_is_better"] is True and d["value"] > 0
+    assert d["steps"] == 2 and d["warmup"] == 1 and d["config"]["workload"].startswith("small")
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["kind"] == "port" and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=tmp_path,
+                       env=dict(os.environ, RANK="1", WORLD_SIZE="2"))
+    assert r.returncode == 0 and r.stdout.strip() == ""
