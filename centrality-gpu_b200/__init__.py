@@ -56,7 +56,7 @@ class BcBccs(C.Structure):
 class BcStats(C.Structure):
     _fields_ = [("sources", C.c_int64), ("bfs_sources", C.c_int64), ("aux_bfs", C.c_int64), ("teps_edges", C.c_int64),
                 ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_int32),
-                ("batch_width", C.c_int32)]
+                ("batch_width", C.c_int32), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -29,6 +29,9 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
                    BatchedPlan **out, std::string *msg);
 void batched_destroy(BatchedPlan *p);
 int64_t batched_device_bytes(const BatchedPlan *p);
+// Bytes batched_create copied host -> device; bytes batched_failed_batches reads back.
+int64_t batched_h2d_bytes(const BatchedPlan *p);
+int64_t batched_status_bytes(const BatchedPlan *p);
 int batched_width(const BatchedPlan *p);
 // Packed ids of the own sources (own BFS + chain slots) of batches [begin, end).
 void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std::vector<int64_t> &out);

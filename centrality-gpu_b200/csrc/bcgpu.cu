@@ -67,6 +67,7 @@ struct bc_plan {
   // per-unit work (prefix sums over units)
   std::vector<int64_t> unit_sources, unit_teps, unit_bfs, unit_aux, unit_visits;
   int64_t device_bytes = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;  // copied so far by this plan (batched tables counted in bp)
   std::vector<void *> allocs;
   // graph mode: instantiated graph and kernel-launch count per recorded unit range
   struct Recorded {
@@ -124,6 +125,7 @@ int upload(bc_plan *p, T **ptr, const T *src, int64_t count) {
   int rc = dalloc(p, ptr, count);
   if (rc) return rc;
   if (count > 0) CK(p->ctx, cudaMemcpyAsync(*ptr, src, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, p->ctx->stream));
+  p->h2d_bytes += (int64_t)sizeof(T) * count;
   return BCGPU_OK;
 }
 
@@ -141,12 +143,14 @@ int check_dev_err(bc_plan *p) {
   int h = 0;
   CK(p->ctx, cudaMemcpyAsync(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream));
   CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  p->d2h_bytes += (int64_t)sizeof(int);
   if (h != bcg::kDevOk)
     return fail(p->ctx, h == bcg::kDevTimeout ? BCGPU_ETIMEOUT : BCGPU_EINVAL, dev_err_text(h));
   if (p->bp) {
     int64_t bad = 0;
     if (bcg::batched_failed_batches(p->bp, p->ctx->stream, &bad) != BCGPU_OK)
       return fail(p->ctx, BCGPU_ECUDA, "reading batch status");
+    p->d2h_bytes += bcg::batched_status_bytes(p->bp);
     if (bad)
       return fail(p->ctx, BCGPU_EOVERFLOW,
                   std::to_string(bad) + " batch(es) left FP32's exponent range in the compensated-FP32 mode; "
@@ -427,6 +431,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
       return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
     std::vector<int32_t> ep((size_t)(2 * slots), 1);
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
+    p->h2d_bytes += (int64_t)(sizeof(int32_t) * ep.size());
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return BCGPU_OK;
@@ -738,6 +743,7 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
   }
   if (stats) {
     CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    const int64_t d2h0 = p->d2h_bytes;
     int rc = check_dev_err(p);
     if (rc) return rc;
     float ms = 0.f;
@@ -751,6 +757,7 @@ extern "C" int bc_plan_run(bc_plan *p, int64_t begin, int64_t end, bc_stats *sta
     stats->total_ms = ms;
     stats->kernel_launches = launches;
     stats->batch_width = p->bp ? bcg::batched_width(p->bp) : 0;
+    stats->d2h_bytes = p->d2h_bytes - d2h0;  // the status words read back (the run copies nothing in)
   }
   return BCGPU_OK;
 }
@@ -766,6 +773,7 @@ extern "C" int bc_plan_read(bc_plan *p, double *bc_out) {
       CK(p->ctx, cudaMemcpyAsync(packed.data(), p->bc, sizeof(double) * (size_t)p->n_packed, cudaMemcpyDeviceToHost,
                                  p->ctx->stream));
     CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+    p->d2h_bytes += (int64_t)sizeof(double) * p->n_packed;
     for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] = p->art.empty() ? 0.0 : p->art[v];
     for (int64_t k = 0; k < p->n_packed; ++k) bc_out[p->orig[k]] += packed[k];  // fixed order: deterministic
     return BCGPU_OK;
@@ -829,6 +837,9 @@ int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool
       cudaEventElapsedTime(&ms, t0, t1);
       st.total_ms = ms;
     }
+    // everything this call copied: the plan's uploads and every read-back
+    st.h2d_bytes = p->h2d_bytes + (p->bp ? bcg::batched_h2d_bytes(p->bp) : 0);
+    st.d2h_bytes = p->d2h_bytes;
     if (stats) *stats = st;
   }
   bc_plan_destroy(p);

@@ -1121,6 +1121,7 @@ struct BatchedPlan {
   int grid = 0;
   size_t smem = 0;
   int64_t bytes = 0;
+  int64_t h2d = 0;  // bytes uploaded by batched_create
   std::vector<void *> allocs;
   Args args{};
   std::vector<int64_t> u_src, u_teps, u_bfs, u_aux, u_visits;
@@ -1450,7 +1451,10 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   auto upload = [&](const void **dst, const void *src, int64_t bytes) -> bool {
     if (!alloc(&p, bytes)) return false;
     *dst = p;
-    return bytes == 0 || cudaMemcpyAsync(p, src, (size_t)bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess;
+    if (bytes == 0) return true;
+    if (cudaMemcpyAsync(p, src, (size_t)bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) return false;
+    P->h2d += bytes;
+    return true;
   };
   ok = ok && upload((const void **)&a.hvo, hvo.data(), (int64_t)hvo.size() * 8);
   ok = ok && upload((const void **)&a.hrow, hrow.data(), (int64_t)hrow.size() * 8);
@@ -1536,6 +1540,10 @@ void batched_destroy(BatchedPlan *p) {
 }
 
 int64_t batched_device_bytes(const BatchedPlan *p) { return p ? p->bytes : 0; }
+int64_t batched_h2d_bytes(const BatchedPlan *p) { return p ? p->h2d : 0; }
+int64_t batched_status_bytes(const BatchedPlan *p) {
+  return p ? (int64_t)sizeof(int) * std::max<int64_t>(p->n_batches, 1) : 0;
+}
 int batched_width(const BatchedPlan *p) { return p ? p->width : 0; }
 
 void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std::vector<int64_t> &out) {

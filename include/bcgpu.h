@@ -110,6 +110,8 @@ typedef struct bc_stats {
   double total_ms;        /* device time of the whole call incl. copies */
   int32_t kernel_launches;/* kernels this library launched */
   int32_t batch_width;    /* width used (BATCHED) */
+  int64_t h2d_bytes;      /* bytes the call copied host -> device (the packed BCCs and the tables built from them) */
+  int64_t d2h_bytes;      /* bytes the call copied device -> host (BC and status words) */
 } bc_stats;
 
 /* Whole computation, host buffers in and out: uploads the packed BCCs, runs

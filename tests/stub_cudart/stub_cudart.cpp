@@ -26,6 +26,7 @@ std::mutex g_mu;  // constant-initialised
 std::atomic<long long> g_launches{0};
 std::atomic<long long> g_live{0};        // device allocations not yet freed
 std::atomic<long long> g_mallocs{0};     // device allocation calls so far
+std::atomic<long long> g_h2d{0}, g_d2h{0};  // bytes copied host->device, device->host (when executed)
 std::atomic<long long> g_fail_after{-1};  // allocations left before one fails (-1: none fails)
 std::map<const void *, size_t> &var_size() {  // registered __device__ variables: host shadow -> size
   static std::map<const void *, size_t> m;
@@ -79,6 +80,8 @@ extern "C" {
 long long stub_cudart_launches() { return g_launches.load(); }
 long long stub_cudart_live_allocs() { return g_live.load(); }
 long long stub_cudart_mallocs() { return g_mallocs.load(); }
+long long stub_cudart_h2d() { return g_h2d.load(); }
+long long stub_cudart_d2h() { return g_d2h.load(); }
 // The (n+1)-th device allocation from now on fails (n < 0: none fails).
 void stub_cudart_fail_malloc_after(long long n) { g_fail_after = n; }
 
@@ -158,8 +161,12 @@ cudaError_t cudaFree(void *p) {
 }
 cudaError_t cudaMallocAsync(void **p, size_t bytes, cudaStream_t) { return cudaMalloc(p, bytes); }
 cudaError_t cudaFreeAsync(void *p, cudaStream_t) { return cudaFree(p); }
-cudaError_t cudaMemcpyAsync(void *dst, const void *src, size_t bytes, cudaMemcpyKind, cudaStream_t s) {
-  return on_stream(s, [=] { std::memcpy(dst, src, bytes); });
+cudaError_t cudaMemcpyAsync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  return on_stream(s, [=] {
+    std::memcpy(dst, src, bytes);
+    if (kind == cudaMemcpyHostToDevice) g_h2d += (long long)bytes;
+    if (kind == cudaMemcpyDeviceToHost) g_d2h += (long long)bytes;
+  });
 }
 cudaError_t cudaMemsetAsync(void *dst, int value, size_t bytes, cudaStream_t s) {
   return on_stream(s, [=] { std::memset(dst, value, bytes); });

@@ -407,3 +407,33 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     assert r.returncode == 4 and "multiple of 32" in r.stderr
     r = run(g, "--out", tmp_path / "no" / "such" / "dir.txt")
     assert r.returncode == 6
+
+
+def test_reported_copy_bytes_are_the_copies_made(stub_dir):
+    """bc_run_bccs_units reports in bc_stats exactly the bytes it copied each
+    way (counted by the stand-in runtime), in both schedules; the host->device
+    bytes include the tables the library builds, beyond the packed input."""
+    res = run_stub(stub_dir, """
+L.stub_cudart_h2d.restype = C.c_longlong
+L.stub_cudart_d2h.restype = C.c_longlong
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
+d = decomp(n, u, v)
+a = d.arrays()
+packed = sum(int(a[k].nbytes) for k in ("vtx_off", "row", "col", "reach", "chain_start", "chain_len", "chain_l",
+                                        "chain_r"))
+rows = []
+for opts in (dict(mode=P.MODE_PLAIN), dict(mode=P.MODE_BATCHED, plain_core=500),
+             dict(mode=P.MODE_BATCHED, plain_core=-1)):
+    ctx = P.Context(**opts)
+    h0, d0 = L.stub_cudart_h2d(), L.stub_cudart_d2h()
+    _, st = ctx.run_units(d, 0, 3)
+    rows.append([st["h2d_bytes"], L.stub_cudart_h2d() - h0, st["d2h_bytes"], L.stub_cudart_d2h() - d0])
+    ctx.close()
+out["rows"] = rows
+out["packed"] = packed
+out["n_packed"] = int(a["n_packed"])
+""")
+    for h2d, h2d_seen, d2h, d2h_seen in res["rows"]:
+        assert h2d == h2d_seen and d2h == d2h_seen
+        assert h2d >= res["packed"] and d2h >= 8 * res["n_packed"]
+    assert res["rows"][2][0] > res["rows"][0][0]  # the multi-source schedule also uploads its contracted rows
