@@ -237,3 +237,46 @@ def test_graph_load_token_rules_any_thread_count(tmp_path):
     assert "out of range at edge 0" in got["oob_before_trunc"]
     assert "truncated edge list at edge 0 of 2" in got["lone_minus"]  # the minus sign is edge 0's weight
     assert got["huge_m"].startswith("err 5") and "truncated edge list at edge 1 of 99999999999" in got["huge_m"]
+
+
+def larger_random_graph(seed):
+    """A few hundred vertices: a random core, parallel chains between some
+    pairs of its vertices, every edge subdivided with probability 0.3 into
+    chains of 1-6, pendant trees, and a second small component."""
+    G = graphs()
+    rng = np.random.default_rng(1000 + seed)
+    n = int(rng.integers(80, 250))
+    m = int(rng.integers(n, 3 * n))
+    u = rng.integers(0, n, m)
+    v = rng.integers(0, n, m)
+    a, b = rng.integers(0, n, 2)
+    u = np.concatenate([u, [a, a, a]])  # three parallel paths a-x-b after subdivision below
+    v = np.concatenate([v, [b, b, b]])
+    uu, vv = G.simple_edges(n, u, v)
+    n, uu, vv = G.subdivide(n, uu, vv, 0.3, 1, 6, rng)
+    for _ in range(3):  # parallel chains: new vertices x between a and b
+        uu = np.concatenate([uu, [a, n]]).astype(np.int32)
+        vv = np.concatenate([vv, [n, b]]).astype(np.int32)
+        n += 1
+    n, uu, vv = G.attach_leaves(n, uu, vv, int(rng.integers(5, 40)), n, rng)
+    k = n  # a separate 5-cycle with a chord
+    uu = np.concatenate([uu, [k, k + 1, k + 2, k + 3, k + 4, k]]).astype(np.int32)
+    vv = np.concatenate([vv, [k + 1, k + 2, k + 3, k + 4, k, k + 2]]).astype(np.int32)
+    n += 5
+    return (n,) + G.simple_edges(n, uu, vv)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_larger_decomposition_matches_oracle(seed):
+    n, u, v = larger_random_graph(seed)
+    P = pkg()
+    arrs = P.Decomposition(P.Graph.from_edges(n, u, v)).arrays()
+    mine = {b["verts"]: b for b in product_bccs(arrs)}
+    theirs, art = _oracle_bccs(n, u, v)
+    assert set(mine) == {b["verts"] for b in theirs}
+    for b in theirs:
+        m = mine[b["verts"]]
+        assert m["reach"] == b["reach"] and m["chains"] == b["chains"] and m["free"] == b["free"]
+    assert np.array_equal(arrs["art"], art)
+    row, col = oracle().csr(n, u, v)
+    assert rel_err(oracle().method_bc_from_decomp(arrs), oracle().brandes(n, row, col)) < 1e-12
