@@ -102,6 +102,7 @@ _SIGS = {
     "bc_graph_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "bc_graph_from_edges": (C.c_int, [C.c_int32, C.c_int64, _i32p, _i32p, C.POINTER(C.c_void_p)]),
     "bc_graph_free": (None, [C.c_void_p]),
+    "bc_graph_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_size_t]),
     "bc_graph_csr": (C.c_int, [C.c_void_p, _i32p, _i64p, C.POINTER(_i64p), C.POINTER(_i32p)]),
     "bc_decompose": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bc_decomp_free": (None, [C.c_void_p]),
@@ -164,6 +165,13 @@ class Graph:
         if rc:
             raise BcError(rc, "bc_graph_from_edges")
         return cls(h.value)
+
+    def save(self, path):
+        """Writes the CSR in the binary form Graph.load reads back (bc_graph_save)."""
+        err = C.create_string_buffer(512)
+        rc = lib().bc_graph_save(self._h, str(path).encode(), err, 512)
+        if rc:
+            raise BcError(rc, err.value.decode())
 
     def csr(self):
         n = C.c_int32()

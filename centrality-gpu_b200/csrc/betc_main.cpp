@@ -18,12 +18,13 @@
 static void usage() {
   std::fprintf(stderr,
                "usage: betc INPUT_FILE [--out FILE] [--mode plain|batched] [--delta fp64|fp32c]\n"
-               "            [--batch WIDTH] [--device ORDINAL] [--quiet]\n");
+               "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE]\n"
+               "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr\n");
 }
 
 int main(int argc, char **argv) {
   if (argc < 2) { usage(); return 1; }
-  const char *input = nullptr, *out_path = nullptr;
+  const char *input = nullptr, *out_path = nullptr, *save_path = nullptr;
   bc_opts opts;
   bc_default_opts(&opts);
   bool quiet = false;
@@ -47,6 +48,7 @@ int main(int argc, char **argv) {
     } else if (a == "--batch") opts.batch_width = std::atoi(next());
     else if (a == "--device") opts.device = std::atoi(next());
     else if (a == "--quiet") quiet = true;
+    else if (a == "--save-csr") save_path = next();
     else if (a == "-h" || a == "--help") { usage(); return 0; }
     else if (!input) input = argv[i];
     else { usage(); return 1; }
@@ -58,6 +60,11 @@ int main(int argc, char **argv) {
   bc_graph *g = nullptr;
   int rc = bc_graph_load(input, &g, err, sizeof(err));
   if (rc) { std::fprintf(stderr, "betc: %s\n", err); return 2; }
+  if (save_path && bc_graph_save(g, save_path, err, sizeof(err))) {
+    std::fprintf(stderr, "betc: %s\n", err);
+    bc_graph_free(g);
+    return 6;
+  }
   bc_decomp *d = nullptr;
   rc = bc_decompose(g, &d);
   if (rc) { std::fprintf(stderr, "betc: decomposition failed (code %d)\n", rc); bc_graph_free(g); return 3; }

@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -147,11 +148,82 @@ extern "C" int bc_graph_from_edges(int32_t n, int64_t m, const int32_t *u, const
 
 namespace {
 
+constexpr char kCsrMagic[8] = {'B', 'C', 'G', 'C', 'S', 'R', '1', '\0'};
+constexpr size_t kCsrHeader = 24;  // magic, int32 n, int32 0, int64 arcs
+
+// 64-bit mixing of an ordered vertex pair (splitmix64 finaliser).
+inline uint64_t pair_hash(int32_t x, int32_t y) {
+  uint64_t z = ((uint64_t)(uint32_t)x << 32 | (uint32_t)y) + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// The binary CSR of bc_graph_save, read straight into the graph and checked
+// to be what the text path builds: offsets from 0 to arcs, every list
+// strictly increasing (sorted, no duplicates), no loops, and every arc present
+// in both directions -- the sums of pair_hash over (x, y) and over (y, x)
+// agree exactly when the arc multiset is symmetric, barring a 2^-64 collision.
+int load_binary(FILE *fp, long size, bc_graph **out, char *err, size_t errlen) {
+  auto bad = [&](const char *why) {
+    set_err(err, errlen, std::string("binary CSR: ") + why);
+    return BCGPU_EIO;
+  };
+  char head[kCsrHeader];
+  if (size < (long)kCsrHeader || std::fread(head, 1, kCsrHeader, fp) != kCsrHeader) return bad("truncated header");
+  int32_t n, pad;
+  int64_t arcs;
+  std::memcpy(&n, head + 8, 4);
+  std::memcpy(&pad, head + 12, 4);
+  std::memcpy(&arcs, head + 16, 8);
+  if (n < 0 || pad != 0 || arcs < 0 || arcs > (int64_t)size / 4) return bad("bad header");
+  const uint64_t want = kCsrHeader + 8ull * ((uint64_t)n + 1) + 4ull * (uint64_t)arcs;
+  if (want != (uint64_t)size) return bad("file size does not match its header");
+  std::unique_ptr<bc_graph> g(new bc_graph);
+  g->n = n;
+  g->row.resize((size_t)n + 1);
+  g->col.resize((size_t)arcs);
+  if (std::fread(g->row.data(), 8, (size_t)n + 1, fp) != (size_t)n + 1 ||
+      (arcs && std::fread(g->col.data(), 4, (size_t)arcs, fp) != (size_t)arcs))
+    return bad("short read");
+  const int64_t *R = g->row.data();
+  const int32_t *C = g->col.data();
+  int fault = R[0] != 0 || R[n] != arcs;
+  uint64_t fwd = 0, rev = 0;
+  if (!fault) {
+#pragma omp parallel for schedule(dynamic, 4096) reduction(| : fault) reduction(+ : fwd, rev)
+    for (int32_t x = 0; x < n; ++x) {
+      if (R[x + 1] < R[x] || R[x + 1] > arcs) { fault |= 1; continue; }
+      for (int64_t e = R[x]; e < R[x + 1]; ++e) {
+        const int32_t y = C[e];
+        if (y < 0 || y >= n || y == x || (e > R[x] && C[e - 1] >= y)) { fault |= 2; break; }
+        fwd += pair_hash(x, y);
+        rev += pair_hash(y, x);
+      }
+    }
+  }
+  if (!fault && fwd != rev) fault = 4;
+  if (fault)
+    return bad(fault & 1 ? "row offsets out of order" : fault & 2 ? "a neighbour list that is not sorted, "
+               "repeats a vertex, holds a loop or an id out of range" : "an arc without its reverse");
+  *out = g.release();
+  return BCGPU_OK;
+}
+
 int graph_load(const char *path, bc_graph **out, char *err, size_t errlen) {
   FILE *fp = std::fopen(path, "rb");
   if (!fp) { set_err(err, errlen, std::string("input file cannot be opened: ") + path); return BCGPU_EIO; }
   std::fseek(fp, 0, SEEK_END);
   long size = std::ftell(fp);
+  std::fseek(fp, 0, SEEK_SET);
+  char magic[sizeof kCsrMagic];
+  if (size >= (long)sizeof kCsrMagic && std::fread(magic, 1, sizeof magic, fp) == sizeof magic &&
+      std::memcmp(magic, kCsrMagic, sizeof magic) == 0) {  // a CSR written by bc_graph_save
+    std::fseek(fp, 0, SEEK_SET);
+    const int rc = load_binary(fp, size, out, err, errlen);
+    std::fclose(fp);
+    return rc;
+  }
   std::fseek(fp, 0, SEEK_SET);
   std::vector<char> buf(size > 0 ? (size_t)size : 1);
   size_t got = size > 0 ? std::fread(buf.data(), 1, (size_t)size, fp) : 0;
@@ -248,6 +320,23 @@ extern "C" int bc_graph_load(const char *path, bc_graph **out, char *err, size_t
 }
 
 extern "C" void bc_graph_free(bc_graph *g) { delete g; }
+
+extern "C" int bc_graph_save(const bc_graph *g, const char *path, char *err, size_t errlen) {
+  if (!g || !path) { set_err(err, errlen, "null argument"); return BCGPU_EINVAL; }
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) { set_err(err, errlen, std::string("cannot write ") + path); return BCGPU_EIO; }
+  const int32_t n = g->n, pad = 0;
+  const int64_t arcs = g->row.empty() ? 0 : g->row[(size_t)n];
+  bool ok = std::fwrite(kCsrMagic, 1, sizeof kCsrMagic, fp) == sizeof kCsrMagic &&
+            std::fwrite(&n, 4, 1, fp) == 1 && std::fwrite(&pad, 4, 1, fp) == 1 && std::fwrite(&arcs, 8, 1, fp) == 1;
+  const int64_t zero = 0;
+  if (ok && g->row.empty()) ok = std::fwrite(&zero, 8, 1, fp) == 1;  // an empty graph: row = {0}
+  else if (ok) ok = std::fwrite(g->row.data(), 8, (size_t)n + 1, fp) == (size_t)n + 1;
+  if (ok && arcs) ok = std::fwrite(g->col.data(), 4, (size_t)arcs, fp) == (size_t)arcs;
+  ok = (std::fclose(fp) == 0) && ok;
+  if (!ok) { set_err(err, errlen, std::string("short write to ") + path); return BCGPU_EIO; }
+  return BCGPU_OK;
+}
 
 extern "C" int bc_graph_csr(const bc_graph *g, int32_t *n, int64_t *n_arcs, const int64_t **row, const int32_t **col) {
   if (!g) return BCGPU_EINVAL;

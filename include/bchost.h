@@ -22,8 +22,18 @@ extern "C" {
 typedef struct bc_graph bc_graph;
 
 /* Reads the reference's edge-list file: "n m" then m lines "u v w" (0-based,
- * w ignored as in the reference's BFS). Writes a message to err on failure. */
+ * w ignored as in the reference's BFS). Writes a message to err on failure.
+ * A file written by bc_graph_save (it starts with the bytes "BCGCSR1\0") is
+ * read as that CSR instead, with no parsing: it must describe a simple
+ * undirected graph (sorted adjacency, no loops or duplicates, every arc
+ * mirrored), else BCGPU_EIO with the reason. */
 int bc_graph_load(const char *path, bc_graph **out, char *err, size_t errlen);
+/* Writes g's CSR in the binary form bc_graph_load reads back: the 8 bytes
+ * "BCGCSR1\0", int32 n, int32 0, int64 arcs, int64 row[n+1], int32 col[arcs]
+ * (host byte order). A cache of a large edge list: reloading it skips the
+ * text parse, the deduplication and the sort. No reference counterpart (the
+ * reference re-reads the text file every run, Codes/graph.cpp:38-59). */
+int bc_graph_save(const bc_graph *g, const char *path, char *err, size_t errlen);
 int bc_graph_from_edges(int32_t n, int64_t m, const int32_t *u, const int32_t *v, bc_graph **out);
 void bc_graph_free(bc_graph *g);
 /* Borrowed views of the CSR: row[n+1] (int64), col[row[n]] (int32). */

@@ -280,3 +280,56 @@ def test_larger_decomposition_matches_oracle(seed):
     assert np.array_equal(arrs["art"], art)
     row, col = oracle().csr(n, u, v)
     assert rel_err(oracle().method_bc_from_decomp(arrs), oracle().brandes(n, row, col)) < 1e-12
+
+
+def test_binary_csr_round_trip(tmp_path):
+    """A graph saved with bc_graph_save loads back (detected by its magic
+    bytes, no text parsing) to the same CSR and the same decomposition."""
+    P = pkg()
+    G = graphs()
+    n, u, v = G.gen_rmat(12, 8, chain_frac=0.2, seed=4)
+    g = P.Graph.from_edges(n, u, v)
+    path = tmp_path / "g.csr"
+    g.save(path)
+    h = P.Graph.load(path)
+    n1, r1, c1 = g.csr()
+    n2, r2, c2 = h.csr()
+    assert n1 == n2 and np.array_equal(r1, r2) and np.array_equal(c1, c2)
+    a = P.Decomposition(g).arrays()
+    b = P.Decomposition(h).arrays()
+    assert all(np.array_equal(a[k], b[k]) for k in a)
+    empty = P.Graph.from_edges(3, np.zeros(0, np.int32), np.zeros(0, np.int32))
+    empty.save(tmp_path / "e.csr")
+    assert P.Graph.load(tmp_path / "e.csr").csr()[0] == 3
+
+
+def test_binary_csr_is_checked(tmp_path):
+    """A binary CSR that is not a simple undirected graph, or whose size does
+    not match its header, is rejected with the reason."""
+    import struct
+
+    P = pkg()
+
+    def write(n, row, col, pad=0, cut=0):
+        data = b"BCGCSR1\0" + struct.pack("<iiq", n, pad, len(col)) + struct.pack(f"<{len(row)}q", *row) + \
+            struct.pack(f"<{len(col)}i", *col)
+        f = tmp_path / "g.csr"
+        f.write_bytes(data[:len(data) - cut])
+        return f
+
+    def reason(*a, **k):
+        with pytest.raises(P.BcError) as e:
+            P.Graph.load(write(*a, **k))
+        assert e.value.code == P.EIO
+        return str(e.value)
+
+    tri = (3, [0, 2, 4, 6], [1, 2, 0, 2, 0, 1])
+    assert P.Graph.load(write(*tri)).csr()[0] == 3  # a triangle is fine
+    assert "size" in reason(*tri, cut=4)
+    assert "header" in reason(*tri, pad=1)
+    assert "order" in reason(3, [0, 2, 1, 6], [1, 2, 0, 2, 0, 1])
+    assert "not sorted" in reason(3, [0, 2, 4, 6], [2, 1, 0, 2, 0, 1])
+    assert "not sorted" in reason(3, [0, 2, 4, 6], [1, 1, 0, 2, 0, 1])  # repeated neighbour
+    assert "loop" in reason(2, [0, 1, 2], [0, 1])
+    assert "out of range" in reason(2, [0, 1, 2], [1, 7])
+    assert "reverse" in reason(3, [0, 1, 1, 1], [1])

@@ -437,3 +437,22 @@ out["n_packed"] = int(a["n_packed"])
         assert h2d == h2d_seen and d2h == d2h_seen
         assert h2d >= res["packed"] and d2h >= 8 * res["n_packed"]
     assert res["rows"][2][0] > res["rows"][0][0]  # the multi-source schedule also uploads its contracted rows
+
+
+def test_betc_reads_the_csr_it_saved(stub_dir, tmp_path):
+    """betc --save-csr writes the loaded graph as a binary CSR; betc given
+    that file prints what it printed for the edge list."""
+    from helpers import GOLDEN
+
+    betc = PKG / "lib" / "betc"
+    env = dict(os.environ, LD_LIBRARY_PATH=str(stub_dir))
+    csr = tmp_path / "g.csr"
+    a = subprocess.run([str(betc), str(GOLDEN / "small2000.txt"), "--save-csr", str(csr), "--quiet"], env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert a.returncode == 0, a.stderr
+    b = subprocess.run([str(betc), str(csr), "--quiet"], env=env, capture_output=True, text=True, timeout=120)
+    assert b.returncode == 0, b.stderr
+    assert a.stdout == b.stdout and len(a.stdout.splitlines()) == 2000
+    r = subprocess.run([str(betc), str(GOLDEN / "sample1.txt"), "--save-csr", str(tmp_path / "no" / "x.csr")], env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 6 and "cannot write" in r.stderr
