@@ -456,3 +456,61 @@ def test_betc_reads_the_csr_it_saved(stub_dir, tmp_path):
     r = subprocess.run([str(betc), str(GOLDEN / "sample1.txt"), "--save-csr", str(tmp_path / "no" / "x.csr")], env=env,
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 6 and "cannot write" in r.stderr
+
+
+def test_autotune_width_candidates(stub_dir):
+    """bc_autotune_width builds a plan per candidate width, times passes from
+    the middle of the source order, reports every candidate and returns one of
+    them; a candidate whose workspace does not fit the limit scores 0 and is
+    never chosen; a plan with no multi-source pass returns width 0."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_rmat(12, 16, chain_frac=0.2, chain_hi=8, seed=2)
+d = decomp(n, u, v)
+c = P.Context(mode=P.MODE_BATCHED, plain_core=-1)
+w, per = c.autotune_width(d, passes=2)
+out["free"] = [w, per]
+c.close()
+c = P.Context(mode=P.MODE_BATCHED, plain_core=-1, workspace_limit=12 << 20)
+w, per = c.autotune_width(d, passes=2)
+out["tight"] = [w, per]
+c.close()
+c = P.Context(mode=P.MODE_BATCHED)  # default routing: every BCC of this graph runs per source
+w, per = c.autotune_width(decomp(*G.gen_small(1)), passes=2)
+out["none"] = w
+c.close()
+c = P.Context(mode=P.MODE_PLAIN)
+out["plain"] = raises(lambda: c.autotune_width(d, passes=2))
+c.close()
+""")
+    w, per = res["free"]
+    assert w in (128, 256, 512, 1024) and sorted(per) == ["1024", "128", "256", "512"]
+    assert per[str(w)] == max(per.values()) > 0
+    w, per = res["tight"]
+    assert per["1024"] == 0 and w in (128, 256, 512) and per[str(w)] > 0
+    assert res["none"] == 0
+    assert res["plain"] is not None and res["plain"][0] == 1
+
+
+def test_source_rows_arguments(stub_dir):
+    """Row export (for the parity tests) is for PLAIN plans and packed ids in
+    range; anything else is BCGPU_EINVAL."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_small(1)
+d = decomp(n, u, v)
+a = d.arrays()
+nb = int(a["vtx_off"][1] - a["vtx_off"][0])
+c = P.Context(mode=P.MODE_PLAIN)
+plan = c.plan(d)
+out["ok"] = raises(lambda: plan.source_rows(0, nb))
+out["chain_vertex"] = raises(lambda: plan.source_rows(int(a["n_plain"][0]), nb))
+out["range"] = raises(lambda: plan.source_rows(int(a["n_packed"]), nb))
+plan.close()
+c.close()
+c = P.Context(mode=P.MODE_BATCHED, plain_core=-1)
+plan = c.plan(d)
+out["batched"] = raises(lambda: plan.source_rows(0, nb))
+plan.close()
+c.close()
+""")
+    assert res["ok"] is None and res["chain_vertex"] is None
+    assert res["range"][0] == 1 and res["batched"][0] == 1 and "PLAIN" in res["batched"][1]
