@@ -55,8 +55,10 @@ def stub_dir():
     stub_o = BUILD / "stub_cudart.o"
     subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-I/usr/local/cuda/include", "-c",
                     str(STUB / "stub_cudart.cpp"), "-o", str(stub_o)], check=True)
+    # -Bsymbolic: the library's calls bind to these stand-ins even when a real
+    # CUDA runtime is already loaded in the process (torch brings one)
     subprocess.run(["g++", "-shared", "-o", str(BUILD / "libbcgpu.so")] + [str(o) for o in objs] +
-                   [str(stub_o), "-lgomp", "-Wl,--no-undefined"], check=True)
+                   [str(stub_o), "-lgomp", "-Wl,--no-undefined", "-Wl,-Bsymbolic"], check=True)
     return BUILD
 
 
@@ -514,3 +516,34 @@ c.close()
 """)
     assert res["ok"] is None and res["chain_vertex"] is None
     assert res["range"][0] == 1 and res["batched"][0] == 1 and "PLAIN" in res["batched"][1]
+
+
+def test_bench_main_arm_line(stub_dir, tmp_path):
+    """bench.py's main arm runs end to end on the stand-in runtime (torch.cuda
+    stood in by tests/stub_cudart/torch_cuda_stub.py) and prints one JSON line
+    with every key of the contract; the numbers are meaningless here."""
+    code = ("import runpy, sys\n"
+            f"sys.path.insert(0, {str(STUB)!r})\n"
+            "import torch_cuda_stub\n"
+            "sys.argv = ['bench.py', '--workload', 'small', '--steps', '3', '--warmup', '3', '--plain-waves', '1',\n"
+            "            '--e2e-steps', '1', '--cpu-budget-s', '1']\n"
+            f"runpy.run_path({str(ROOT / 'bench.py')!r}, run_name='__main__')\n")
+    env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir))
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    import bench
+    assert d["metric"] == bench.METRIC and d["unit"] == "GTEPS" and d["higher_is_better"] is True
+    for k in ("value", "n_gpus", "steps", "warmup", "ms_per_step", "scaling", "vs_baseline", "dtype", "data", "config",
+              "roofline", "cpu_baseline", "e2e", "clocks", "gpu_launches", "plain", "accuracy"):
+        assert k in d, k
+    assert d["steps"] == 3 and d["warmup"] == 3 and d["n_gpus"] == 1 and d["gpu_launches"] >= 3
+    assert d["config"]["workload"].startswith("small") and d["config"]["cuda_graph"] is True
+    assert {"bound", "achieved", "peak", "unit", "frac", "traffic"} <= set(d["roofline"])
+    assert {"value", "unit", "cores", "kind", "sample"} <= set(d["cpu_baseline"])
+    e = d["e2e"]
+    assert e["unit"] == "GTEPS" and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] >= 8 * 1500
+    assert d["config"]["host_decomposition_s"] >= 0 and d["config"]["generator_s"] >= 0
