@@ -289,11 +289,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    # NCCL between the GPUs; BCGPU_DIST_BACKEND=gloo runs the ranks' reductions on
+    # host tensors instead (the CPU tests of this multi-rank path use it)
+    backend = os.environ.get("BCGPU_DIST_BACKEND", "nccl")
+    rdev = "cuda" if backend == "nccl" else "cpu"
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
 
     P = load_pkg()
     from centrality_gpu_b200 import graphs as G
@@ -314,16 +318,27 @@ def main():
     torch.cuda.set_stream(stream)
     width, tuned = args.batch, None
     if mode == P.MODE_BATCHED and args.batch == 0:  # the library's autotuner, outside the timed region
-        tctx = P.Context(mode=mode, delta=delta, device=local, stream=stream.cuda_stream,
-                         workspace_limit=int(args.workspace_gb * 2**30))
-        width, per = tctx.autotune_width(d, passes=4)
-        tctx.close()
-        tuned = {str(k): round(v, 2) for k, v in per.items()}
+        if rank == 0:  # every rank must build the same plan: rank 0 tunes, the others take its width
+            tctx = P.Context(mode=mode, delta=delta, device=local, stream=stream.cuda_stream,
+                             workspace_limit=int(args.workspace_gb * 2**30))
+            width, per = tctx.autotune_width(d, passes=4)
+            tctx.close()
+            tuned = {str(k): round(v, 2) for k, v in per.items()}
+        if dist:
+            wt = torch.tensor([width], dtype=torch.int64, device=rdev)
+            dist.broadcast(wt, src=0)
+            width = int(wt.item())
     ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30), graph=bool(args.graph))
     plan = ctx.plan(d)
+    # steps of this many sources, small enough that every rank gets at least one
+    total_sources = plan.unit_work(0, plan.n_units)[0]
     target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
+    target = max(1, min(target, total_sources // world))
     ranges = step_ranges(plan, target)
+    if len(ranges) < world:  # the same on every rank (same plan): all stop here, before any collective
+        print(f"bench: {len(ranges)} step(s) of work for {world} ranks: use a larger workload", file=sys.stderr)
+        return 1
     from centrality_gpu_b200 import multigpu
     mine = multigpu.shard(ranges, rank, world)
     need = args.warmup + args.steps
@@ -364,8 +379,8 @@ def main():
     per_step = [a.elapsed_time(b) for a, b in evs]
     work = np.array([plan.unit_work(r0, r1) for r0, r1 in sel[args.warmup:]], dtype=np.float64)
     sources, teps, visits = work.sum(axis=0)
-    tot = torch.tensor([teps, sources, visits], dtype=torch.float64, device="cuda")
-    mx = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([teps, sources, visits], dtype=torch.float64, device=rdev)
+    mx = torch.tensor([elapsed], dtype=torch.float64, device=rdev)
     if dist:
         dist.all_reduce(tot)
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
@@ -402,8 +417,8 @@ def main():
         te = time.perf_counter() - te
         e_teps = float(sum(plan.unit_work(r0, r1)[1] for r0, r1 in e_sel))
         if dist:
-            t_sum = torch.tensor([e_teps], dtype=torch.float64, device="cuda")
-            t_max = torch.tensor([te], dtype=torch.float64, device="cuda")
+            t_sum = torch.tensor([e_teps], dtype=torch.float64, device=rdev)
+            t_max = torch.tensor([te], dtype=torch.float64, device=rdev)
             dist.all_reduce(t_sum)
             dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
             e_teps, te = t_sum.item(), t_max.item()
@@ -420,7 +435,7 @@ def main():
         plan.reset()
         for r0, r1 in sel[args.warmup:]:
             plan.run(r0, r1, stats=False)
-        total = multigpu.combine_bc(plan.read() - arrs["art"], arrs["art"], dist, device="cuda")
+        total = multigpu.combine_bc(plan.read() - arrs["art"], arrs["art"], dist, device=rdev)
         if rank == 0:
             print(f"combined BC over {world} ranks: sum {float(total.sum()):.6e}", file=sys.stderr)
 

@@ -3,8 +3,9 @@
 // build.py) are linked against this file instead of cudart: "device" memory
 // is host memory, copies and memsets are memcpy/memset, kernel launches do
 // nothing but are counted, stream capture records the stream's copies and
-// memsets (and counts its launches) into a replayable list. One fake sm_100
-// device with 148 SMs. Nothing here computes BC: tests built on it check plan
+// memsets (and counts its launches) into a replayable list. Eight identical
+// fake sm_100 devices with 148 SMs (one per rank under torchrun); memory is
+// not per device. Nothing here computes BC: tests built on it check plan
 // construction, routing, unit bookkeeping, graph record/replay, argument
 // validation and error paths -- never numbers, which the GPU tests pin.
 #include <cuda_runtime_api.h>
@@ -109,11 +110,17 @@ cudaError_t __cudaPopCallConfiguration(dim3 *grid, dim3 *block, size_t *smem, vo
 }  // extern "C"
 
 // ---- device and errors
-cudaError_t cudaGetDeviceCount(int *count) { *count = 1; return cudaSuccess; }
-cudaError_t cudaSetDevice(int device) { return device == 0 ? cudaSuccess : cudaErrorInvalidDevice; }
-cudaError_t cudaGetDevice(int *device) { *device = 0; return cudaSuccess; }
+constexpr int kDevices = 8;
+thread_local int t_device = 0;
+cudaError_t cudaGetDeviceCount(int *count) { *count = kDevices; return cudaSuccess; }
+cudaError_t cudaSetDevice(int device) {
+  if (device < 0 || device >= kDevices) return cudaErrorInvalidDevice;
+  t_device = device;
+  return cudaSuccess;
+}
+cudaError_t cudaGetDevice(int *device) { *device = t_device; return cudaSuccess; }
 cudaError_t cudaGetDeviceProperties_v2(cudaDeviceProp *prop, int device) {
-  if (device != 0) return cudaErrorInvalidDevice;
+  if (device < 0 || device >= kDevices) return cudaErrorInvalidDevice;
   std::memset(prop, 0, sizeof(*prop));
   std::strcpy(prop->name, "stub sm_100 (no GPU)");
   prop->major = 10;

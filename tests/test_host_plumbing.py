@@ -522,15 +522,10 @@ def test_bench_main_arm_line(stub_dir, tmp_path):
     """bench.py's main arm runs end to end on the stand-in runtime (torch.cuda
     stood in by tests/stub_cudart/torch_cuda_stub.py) and prints one JSON line
     with every key of the contract; the numbers are meaningless here."""
-    code = ("import runpy, sys\n"
-            f"sys.path.insert(0, {str(STUB)!r})\n"
-            "import torch_cuda_stub\n"
-            "sys.argv = ['bench.py', '--workload', 'small', '--steps', '3', '--warmup', '3', '--plain-waves', '1',\n"
-            "            '--e2e-steps', '1', '--cpu-budget-s', '1']\n"
-            f"runpy.run_path({str(ROOT / 'bench.py')!r}, run_name='__main__')\n")
+    args = ["--workload", "small", "--steps", "3", "--warmup", "3", "--plain-waves", "1", "--e2e-steps", "1"]
     env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir))
-    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600,
-                       cwd=tmp_path)
+    r = subprocess.run([sys.executable, str(STUB / "bench_on_stub.py")] + args, env=env, capture_output=True,
+                       text=True, timeout=600, cwd=tmp_path)
     assert r.returncode == 0, r.stderr[-3000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
@@ -547,3 +542,27 @@ def test_bench_main_arm_line(stub_dir, tmp_path):
     e = d["e2e"]
     assert e["unit"] == "GTEPS" and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] >= 8 * 1500
     assert d["config"]["host_decomposition_s"] >= 0 and d["config"]["generator_s"] >= 0
+
+
+def test_bench_two_ranks_under_torchrun(stub_dir, tmp_path):
+    """bench.py's multi-rank path (one process per GPU under torchrun) on two
+    CPU ranks over gloo: every rank takes the same collective steps, rank 0
+    alone prints the line, which reports 2 GPUs and the whole job's work."""
+    import socket
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(STUB / "bench_on_stub.py"),
+           "--gpus", "2", "--workload", "small", "--steps", "3", "--warmup", "3", "--e2e-steps", "1"]
+    env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir), BCGPU_DIST_BACKEND="gloo", OMP_NUM_THREADS="2")
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["scaling"] == "weak" and d["steps"] == 3
+    assert d["cpu_baseline"] is None and d["plain"] is None  # single-GPU legs only
+    assert d["e2e"]["h2d_bytes_per_step"] > 0
+    assert "combined BC over 2 ranks" in r.stderr
