@@ -518,11 +518,13 @@ c.close()
     assert res["range"][0] == 1 and res["batched"][0] == 1 and "PLAIN" in res["batched"][1]
 
 
-def test_bench_main_arm_line(stub_dir, tmp_path):
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_bench_main_arm_line(stub_dir, tmp_path, mode):
     """bench.py's main arm runs end to end on the stand-in runtime (torch.cuda
     stood in by tests/stub_cudart/torch_cuda_stub.py) and prints one JSON line
     with every key of the contract; the numbers are meaningless here."""
-    args = ["--workload", "small", "--steps", "3", "--warmup", "3", "--plain-waves", "1", "--e2e-steps", "1"]
+    args = ["--workload", "small", "--steps", "3", "--warmup", "3", "--plain-waves", "1", "--e2e-steps", "1",
+            "--mode", mode]
     env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir))
     r = subprocess.run([sys.executable, str(STUB / "bench_on_stub.py")] + args, env=env, capture_output=True,
                        text=True, timeout=600, cwd=tmp_path)
@@ -542,6 +544,8 @@ def test_bench_main_arm_line(stub_dir, tmp_path):
     e = d["e2e"]
     assert e["unit"] == "GTEPS" and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] >= 8 * 1500
     assert d["config"]["host_decomposition_s"] >= 0 and d["config"]["generator_s"] >= 0
+    assert d["config"]["mode"] == mode and (d["plain"] is None) == (mode == "plain")
+    assert d["dtype"] == ("f64" if mode == "plain" else "f32c")
 
 
 def test_bench_two_ranks_under_torchrun(stub_dir, tmp_path):
