@@ -570,3 +570,26 @@ def test_bench_two_ranks_under_torchrun(stub_dir, tmp_path):
     assert d["cpu_baseline"] is None and d["plain"] is None  # single-GPU legs only
     assert d["e2e"]["h2d_bytes_per_step"] > 0
     assert "combined BC over 2 ranks" in r.stderr
+
+
+@pytest.mark.skipif(not (ROOT / "oracle" / "_ref" / "refbetc").exists(), reason="reference sources absent")
+def test_reference_betc_calls_are_accepted(stub_dir, tmp_path):
+    """The reference's own betc rebuilt on the binding (oracle/_ref/refbetc),
+    run on the library's host code (stand-in runtime: kernels do not run):
+    on every golden fixture the library accepts every begin_gpu call the
+    reference makes, and what is left in the result -- no kernel adds to it --
+    is the articulation terms of the reference's reach computation."""
+    from helpers import GOLDEN, GOLDEN_CASES, load_case
+    from helpers import pkg as real_pkg
+
+    env = dict(os.environ, LD_LIBRARY_PATH=str(stub_dir))
+    for name in GOLDEN_CASES:
+        n, u, v, _, _ = load_case(name)
+        r = subprocess.run([str(ROOT / "oracle" / "_ref" / "refbetc"), str(GOLDEN / f"{name}.txt")], env=env,
+                           cwd=tmp_path, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (name, r.stderr[-2000:])
+        rows = [ln.split() for ln in r.stdout.splitlines()][-n:]
+        got = [float(b) for _, b in rows]
+        art = real_pkg().Decomposition(real_pkg().Graph.from_edges(n, u, v)).arrays()["art"]
+        assert [int(a) for a, _ in rows] == list(range(n))
+        assert max(abs(g - a) / max(1.0, abs(a)) for g, a in zip(got, art)) < 1e-6, name
