@@ -255,18 +255,20 @@ def run_reference(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--gpus", type=int, default=1,
+                    help="GPUs of the run: one process per GPU under torchrun, which sets the ranks (WORLD_SIZE)")
+    ap.add_argument("--steps", type=int, default=5, help="timed steps (ranges of work units)")
+    ap.add_argument("--warmup", type=int, default=3, help="untimed steps before them")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["batched", "plain"], default="batched")
     ap.add_argument("--delta", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--batch", type=int, default=0, help="sources per multi-source pass (0 = autotune)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat20")
     ap.add_argument("--step-sources", type=int, default=0, help="sources per step (0 = by workload and mode)")
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
-    ap.add_argument("--ref-step-s", type=float, default=8.0)
+    ap.add_argument("--e2e-steps", type=int, default=2,
+                    help="steps timed end to end through bc_run_bccs_units with host buffers (0 = skip)")
+    ap.add_argument("--ref-step-s", type=float, default=8.0,
+                    help="--impl reference: seconds of CPU work per step (its sources are sized to it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-waves", type=int, default=2,
                     help="batched runs: also time the plain FP64 schedule on this many full waves of its work "
