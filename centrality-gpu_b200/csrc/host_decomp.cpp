@@ -7,14 +7,16 @@
 //    simple (loops dropped, duplicates merged), the assumption the reference's
 //    BFS states (Codes/kernels_free.cu:248).
 //  * BiCC::bicc_tarjan (Codes/bicc.cpp:81-161) recurses once per vertex and
-//    assumes the DFS root is vertex 0 (:13,:86-87); here one iterative
-//    Hopcroft-Tarjan pass with explicit stacks handles every component.
+//    assumes the DFS root is vertex 0 (:13,:86-87); here Tarjan and
+//    Vishkin's method over a BFS forest (split_bccs) finds the BCCs of every
+//    component in parallel loops, with no DFS.
 //  * fillbccparent/reachfunction (Codes/modified_apsp.cpp:77-220) walk an
 //    explicit block-cut tree; here reach and the articulation cross terms come
-//    straight from DFS subtree sizes: for BCC b with head h (the DFS-closest
-//    vertex) and first child c, reach_b(h) = |comp| - 1 - size(c), and for any
-//    other member x, reach_b(x) = sum of size(y) over DFS children y of x with
-//    low(y) >= disc(x) (subtrees split off at x). The cross term of x is
+//    straight from forest subtree sizes: for BCC b with head h (its vertex
+//    closest to the component's root) and below(b) the vertices under b's
+//    topmost tree edges, reach_b(h) = |comp| - 1 - below(b), and for any
+//    other member x, reach_b(x) = the sum of below over the BCCs that x heads
+//    (the subtrees split off at x). The cross term of x is
 //    S^2 - sum(part^2) over the parts of comp - x (S = |comp| - 1), i.e. the
 //    ordered pairs that x separates (Codes/modified_apsp.cpp:209).
 //  * bcc_bfs/preSum (Codes/bcc_bfs.cpp:100-236, :247-1330) find ears through a
@@ -349,103 +351,439 @@ extern "C" int bc_graph_csr(const bc_graph *g, int32_t *n, int64_t *n_arcs, cons
 
 namespace {
 
+// ---- data-parallel building blocks. Every loop below is a parallel loop
+// over vertices, frontier positions or BCCs whose body touches only its own
+// outputs, atomics (GCC builtins, relaxed: each loop ends at an OpenMP
+// barrier) or data that no iteration of the same loop writes.
+template <class T> inline T ald(const T *p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+template <class T> inline void ast(T *p, T v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
+template <class T> inline T aadd(T *p, T v) { return __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
+template <class T> inline bool acas(T *p, T expect, T v) {
+  return __atomic_compare_exchange_n(p, &expect, v, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED);
+}
+template <class T> inline void amin(T *p, T v) {
+  T c = ald(p);
+  while (v < c && !__atomic_compare_exchange_n(p, &c, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+  }
+}
+template <class T> inline void amax(T *p, T v) {
+  T c = ald(p);
+  while (v > c && !__atomic_compare_exchange_n(p, &c, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+  }
+}
+
+// Union-find whose set roots are the sets' smallest members: a link hangs the
+// larger root under the smaller one, so p[x] <= x at all times and concurrent
+// finds (with path halving) and links need nothing but compare-and-swap.
+int32_t uf_find(int32_t *p, int32_t x) {
+  for (;;) {
+    const int32_t y = ald(&p[x]);
+    if (y == x) return x;
+    const int32_t z = ald(&p[y]);
+    if (z != y) acas(&p[x], y, z);
+    x = z;
+  }
+}
+void uf_union(int32_t *p, int32_t a, int32_t b) {
+  for (;;) {
+    a = uf_find(p, a);
+    b = uf_find(p, b);
+    if (a == b) return;
+    if (a > b) std::swap(a, b);
+    if (acas(&p[b], b, a)) return;
+  }
+}
+
+constexpr int64_t kParFrontier = 2048;  // narrower BFS levels run on one thread
+
+// f(a, b) over chunks [a, b) of [k0, k1): in parallel when the range is
+// wide, else as one chunk on this thread (an OpenMP region costs
+// microseconds, and deep graphs have thousands of narrow levels).
+template <class F>
+void for_chunks(int64_t k0, int64_t k1, F &&f) {
+  constexpr int64_t kChunk = 1024;
+  if (k1 - k0 < kParFrontier) {
+    if (k1 > k0) f(k0, k1);
+    return;
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t c = k0; c < k1; c += kChunk) f(c, std::min(k1, c + kChunk));
+}
+
+// Level-synchronous BFS that lists the vertices in exactly the order of the
+// sequential queue BFS from the same sources: the sources in the given order,
+// then level by level the undiscovered neighbours of each frontier vertex in
+// adjacency order, frontier vertices in their own order. On a wide level a
+// vertex is claimed by the earliest frontier position adjacent to it (atomic
+// min), the claims are counted per position and a prefix sum places each
+// position's vertices; a narrow level is one pass of the sequential queue.
+// adj(x, &ptr) returns the degree of x and points ptr at its neighbours.
+// Returns the visit order (the vertices reached).
+template <class Adj>
+std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
+  std::vector<int32_t> order((size_t)nv), claim;
+  std::vector<char> seen((size_t)nv, 0);
+  std::vector<int64_t> cnt;
+  order[0] = src;
+  seen[src] = 1;
+  int64_t f0 = 0, f1 = 1;
+  while (f1 > f0) {
+    const int64_t fn = f1 - f0;
+    int64_t f2 = f1;
+    if (fn < kParFrontier) {
+      for (int64_t i = f0; i < f1; ++i) {
+        const int32_t *a;
+        const int32_t d = adj(order[i], &a);
+        for (int32_t j = 0; j < d; ++j)
+          if (!seen[a[j]]) {
+            seen[a[j]] = 1;
+            order[f2++] = a[j];
+          }
+      }
+    } else {
+      if (claim.empty()) claim.assign((size_t)nv, INT32_MAX);
+      int32_t *cl = claim.data();
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < fn; ++i) {
+        const int32_t *a;
+        const int32_t d = adj(order[f0 + i], &a);
+        for (int32_t j = 0; j < d; ++j)
+          if (!seen[a[j]]) amin(&cl[a[j]], (int32_t)i);
+      }
+      cnt.assign((size_t)fn + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < fn; ++i) {
+        const int32_t *a;
+        const int32_t d = adj(order[f0 + i], &a);
+        int64_t c = 0;
+        for (int32_t j = 0; j < d; ++j) c += !seen[a[j]] && ald(&cl[a[j]]) == (int32_t)i;
+        cnt[i + 1] = c;
+      }
+      for (int64_t i = 0; i < fn; ++i) cnt[i + 1] += cnt[i];
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < fn; ++i) {
+        const int32_t *a;
+        const int32_t d = adj(order[f0 + i], &a);
+        int64_t at = f1 + cnt[i];
+        for (int32_t j = 0; j < d; ++j)
+          if (!seen[a[j]] && ald(&cl[a[j]]) == (int32_t)i) order[at++] = a[j];
+      }
+      f2 = f1 + cnt[fn];
+#pragma omp parallel for schedule(static)
+      for (int64_t k = f1; k < f2; ++k) seen[order[k]] = 1;
+    }
+    f0 = f1;
+    f1 = f2;
+  }
+  order.resize((size_t)f1);
+  return order;
+}
+
+// A BFS forest of the CSR graph from the given roots, one level at a time:
+// a vertex's parent is whichever adjacent frontier vertex claims it first
+// (compare-and-swap), so the forest depends on thread timing -- the callers
+// only use properties every BFS forest has. par[x] = -1 for a root; level L
+// is order[lvl_off[L], lvl_off[L + 1]).
+void bfs_forest(int32_t n, const int64_t *R, const int32_t *C, const std::vector<int32_t> &roots,
+                std::vector<int32_t> &par, std::vector<int32_t> &order, std::vector<int64_t> &lvl_off) {
+  par.assign((size_t)n, -2);
+  order.resize((size_t)n);
+  for (size_t i = 0; i < roots.size(); ++i) {
+    order[i] = roots[i];
+    par[roots[i]] = -1;
+  }
+  lvl_off.assign({0, (int64_t)roots.size()});
+  const int nt = omp_get_max_threads();
+  std::vector<std::vector<int32_t>> buf((size_t)nt);
+  std::vector<int64_t> boff((size_t)nt + 1);
+  int32_t *P = par.data(), *O = order.data();
+  int64_t f0 = 0, f1 = (int64_t)roots.size();
+  while (f1 > f0) {
+    int64_t f2 = f1;
+    if (f1 - f0 < kParFrontier) {
+      for (int64_t i = f0; i < f1; ++i) {
+        const int32_t x = O[i];
+        for (int64_t e = R[x]; e < R[x + 1]; ++e)
+          if (P[C[e]] == -2) {
+            P[C[e]] = x;
+            O[f2++] = C[e];
+          }
+      }
+    } else {
+#pragma omp parallel
+      {
+        const int t = omp_get_thread_num();
+        std::vector<int32_t> &b = buf[t];
+        b.clear();
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = f0; i < f1; ++i) {
+          const int32_t x = O[i];
+          for (int64_t e = R[x]; e < R[x + 1]; ++e) {
+            const int32_t y = C[e];
+            if (ald(&P[y]) == -2 && acas(&P[y], -2, x)) b.push_back(y);
+          }
+        }
+#pragma omp single
+        {
+          boff[0] = f1;
+          for (int u = 0; u < nt; ++u) boff[u + 1] = boff[u] + (u < omp_get_num_threads() ? (int64_t)buf[u].size() : 0);
+        }
+        std::copy(b.begin(), b.end(), O + boff[t]);
+      }
+      f2 = boff[(size_t)nt];
+    }
+    f0 = f1;
+    f1 = f2;
+    lvl_off.push_back(f1);
+  }
+  lvl_off.pop_back();  // the last, empty level
+}
+
+// BCCs of a simple undirected graph by Tarjan and Vishkin's method over a
+// BFS spanning forest (any rooted spanning forest serves), every step a
+// parallel loop:
+//  1. components by union-find over the edges; each is rooted at its
+//     smallest vertex;
+//  2. one BFS from all roots at once gives the forest (parent, children);
+//  3. subtree sizes nd bottom-up, preorder numbers pre top-down, and
+//     low/high: the least/greatest pre over a subtree and the non-tree
+//     neighbours of its vertices, bottom-up;
+//  4. tree edges, named by their child vertex, are joined by union-find
+//     (roots again the smallest members) when
+//       - a non-tree edge joins two unrelated vertices v, w: tree edges of v
+//         and w, or
+//       - the subtree of w escapes the subtree of its parent v (low(w) <
+//         pre(v) or high(w) >= pre(v) + nd(v)) and v is not a root: tree
+//         edges of v and w;
+//     the sets are the BCCs; a non-tree edge belongs to the BCC of the tree
+//     edge into its endpoint with the larger pre.
+// A BCC is named by its smallest non-head member, the root of its set, and
+// BCCs are numbered in that order, so the result does not depend on the
+// forest or on thread timing. Its head is the parent of its topmost tree
+// edges; below(b), the vertices under those edges, gives reach and the
+// articulation terms: a member x other than the head reaches the subtrees of
+// its children in other BCCs (hang(x), the sum of below over the BCCs x
+// heads), the head reaches the rest of its component.
+// Replaces the DFS of Codes/bicc.cpp:81-161 and the block-cut tree walk of
+// Codes/modified_apsp.cpp:77-220.
+struct Split {
+  int32_t nbcc = 0;
+  std::vector<int32_t> comp, tbcc, pre, head, locid, members;
+  std::vector<int64_t> comp_size, below, hang, sq, mem_off;
+};
+
+void split_bccs(const bc_graph *g, Split &S) {
+  const int32_t n = g->n;
+  const int64_t *R = g->row.data();
+  const int32_t *C = g->col.data();
+
+  // 1. components
+  std::vector<int32_t> uf((size_t)n);
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) uf[x] = x;
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t x = 0; x < n; ++x)
+    for (int64_t e = R[x]; e < R[x + 1]; ++e)
+      if (C[e] < x) uf_union(uf.data(), x, C[e]);
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) uf[x] = uf_find(uf.data(), x);
+  std::vector<int32_t> roots;
+  S.comp.assign((size_t)n, -1);
+  for (int32_t x = 0; x < n; ++x)
+    if (uf[x] == x) {
+      S.comp[x] = (int32_t)roots.size();
+      roots.push_back(x);
+    }
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) S.comp[x] = S.comp[uf[x]];
+
+  // 2. BFS forest
+  std::vector<int32_t> parv, orderv;
+  std::vector<int64_t> lvl_off;
+  bfs_forest(n, R, C, roots, parv, orderv, lvl_off);
+  const int32_t *par = parv.data(), *order = orderv.data();
+  const int64_t nlev = (int64_t)lvl_off.size() - 1;
+
+  // 3. nd bottom-up, pre top-down (siblings in any order: each takes the
+  // next range of its parent's interval), low/high bottom-up. A level lists
+  // the children of one parent mostly in runs (a claiming thread appends
+  // them together), so each run updates its parent with one atomic.
+  auto runs = [&](int64_t a, int64_t b, auto &&g) {  // g(parent, run begin, run end)
+    for (int64_t k = a; k < b;) {
+      const int32_t p = par[order[k]];
+      int64_t j = k + 1;
+      while (j < b && par[order[j]] == p) ++j;
+      g(p, k, j);
+      k = j;
+    }
+  };
+  std::vector<int64_t> nd((size_t)n, 1), cur((size_t)n);
+  for (int64_t L = nlev - 1; L >= 1; --L)
+    for_chunks(lvl_off[L], lvl_off[L + 1], [&](int64_t a, int64_t b) {
+      runs(a, b, [&](int32_t p, int64_t k, int64_t j) {
+        int64_t s = 0;
+        for (int64_t t = k; t < j; ++t) s += nd[order[t]];
+        aadd(&nd[p], s);
+      });
+    });
+  S.pre.assign((size_t)n, 0);
+  S.comp_size.resize(roots.size());
+  int32_t *pre = S.pre.data();
+  {
+    int64_t q = 0;
+    for (size_t i = 0; i < roots.size(); ++i) {
+      pre[roots[i]] = (int32_t)q;
+      cur[roots[i]] = q + 1;
+      S.comp_size[i] = nd[roots[i]];
+      q += nd[roots[i]];
+    }
+  }
+  for (int64_t L = 1; L < nlev; ++L)
+    for_chunks(lvl_off[L], lvl_off[L + 1], [&](int64_t a, int64_t b) {
+      runs(a, b, [&](int32_t p, int64_t k, int64_t j) {
+        int64_t s = 0;
+        for (int64_t t = k; t < j; ++t) s += nd[order[t]];
+        int64_t q = aadd(&cur[p], s);
+        for (int64_t t = k; t < j; ++t) {
+          const int32_t x = order[t];
+          pre[x] = (int32_t)q;
+          cur[x] = q + 1;
+          q += nd[x];
+        }
+      });
+    });
+  std::vector<int32_t> lo((size_t)n), hi((size_t)n);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t x = 0; x < n; ++x) {
+    int32_t l = pre[x], h = pre[x];
+    for (int64_t e = R[x]; e < R[x + 1]; ++e)
+      if (C[e] != par[x]) {
+        l = std::min(l, pre[C[e]]);
+        h = std::max(h, pre[C[e]]);
+      }
+    lo[x] = l;
+    hi[x] = h;
+  }
+  for (int64_t L = nlev - 1; L >= 1; --L)
+    for_chunks(lvl_off[L], lvl_off[L + 1], [&](int64_t a, int64_t b) {
+      runs(a, b, [&](int32_t p, int64_t k, int64_t j) {
+        int32_t l = lo[order[k]], h = hi[order[k]];
+        for (int64_t t = k + 1; t < j; ++t) {
+          l = std::min(l, lo[order[t]]);
+          h = std::max(h, hi[order[t]]);
+        }
+        amin(&lo[p], l);
+        amax(&hi[p], h);
+      });
+    });
+
+  // 4. tree edges joined into BCCs
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) uf[x] = x;
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t w = 0; w < n; ++w) {
+    const int32_t v = par[w];
+    if (v >= 0 && par[v] >= 0 && (lo[w] < pre[v] || (int64_t)hi[w] >= (int64_t)pre[v] + nd[v]))
+      uf_union(uf.data(), v, w);
+    for (int64_t e = R[w]; e < R[w + 1]; ++e) {
+      const int32_t y = C[e];
+      if (y <= w || y == par[w] || w == par[y]) continue;
+      const int32_t a = pre[w] < pre[y] ? w : y, b = a == w ? y : w;
+      if ((int64_t)pre[b] >= (int64_t)pre[a] + nd[a]) uf_union(uf.data(), w, y);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) uf[x] = uf_find(uf.data(), x);
+
+  // BCC ids in the order of their names; head, below, hang, sq
+  S.tbcc.assign((size_t)n, -1);
+  int32_t nbcc = 0;
+  for (int32_t x = 0; x < n; ++x)
+    if (par[x] >= 0 && uf[x] == x) S.tbcc[x] = nbcc++;
+  S.nbcc = nbcc;
+  int32_t *tbcc = S.tbcc.data();
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x)
+    if (par[x] >= 0 && uf[x] != x) tbcc[x] = tbcc[uf[x]];  // uf[x] is a name, only read here
+  S.head.assign((size_t)nbcc, -1);
+  S.below.assign((size_t)nbcc, 0);
+  S.hang.assign((size_t)n, 0);
+  S.sq.assign((size_t)n, 0);
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x) {
+    const int32_t p = par[x];
+    if (p >= 0 && tbcc[p] != tbcc[x]) {  // a topmost tree edge of its BCC (a root's tbcc is -1)
+      ast(&S.head[tbcc[x]], p);
+      aadd(&S.below[tbcc[x]], nd[x]);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int32_t b = 0; b < nbcc; ++b) {
+    aadd(&S.hang[S.head[b]], S.below[b]);
+    aadd(&S.sq[S.head[b]], S.below[b] * S.below[b]);
+  }
+
+  // members: a BCC's non-head members are the child vertices of its tree
+  // edges; each chunk of vertices sorts its own by BCC and reserves one range
+  // per BCC it touches. Their order inside a BCC is immaterial: everything
+  // written out is keyed by vertex ids.
+  S.locid.assign((size_t)n, -1);
+  std::vector<int64_t> fill((size_t)nbcc, 0);
+  constexpr int32_t kChunk = 4096;
+#pragma omp parallel
+  {
+    std::vector<std::pair<int32_t, int32_t>> v;
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t c0 = 0; c0 < n; c0 += kChunk) {
+      v.clear();
+      for (int32_t x = (int32_t)c0; x < (int32_t)std::min<int64_t>(n, c0 + kChunk); ++x)
+        if (tbcc[x] >= 0) v.emplace_back(tbcc[x], x);
+      std::sort(v.begin(), v.end());
+      for (size_t i = 0; i < v.size();) {
+        size_t j = i;
+        while (j < v.size() && v[j].first == v[i].first) ++j;
+        int64_t base = aadd(&fill[v[i].first], (int64_t)(j - i));
+        for (size_t k = i; k < j; ++k) S.locid[v[k].second] = (int32_t)(base + (int64_t)(k - i));
+        i = j;
+      }
+    }
+  }
+  S.mem_off.assign((size_t)nbcc + 1, 0);
+  for (int32_t b = 0; b < nbcc; ++b) S.mem_off[b + 1] = S.mem_off[b] + fill[b] + 1;
+  S.members.assign((size_t)S.mem_off[nbcc], -1);
+#pragma omp parallel for schedule(static)
+  for (int32_t x = 0; x < n; ++x)
+    if (tbcc[x] >= 0) S.members[S.mem_off[tbcc[x]] + S.locid[x]] = x;
+#pragma omp parallel for schedule(static)
+  for (int32_t b = 0; b < nbcc; ++b) S.members[S.mem_off[b + 1] - 1] = S.head[b];
+}
+
 int decompose(const bc_graph *g, bc_decomp *D) {
   auto t0 = std::chrono::steady_clock::now();
   const int32_t n = g->n;
   const int64_t *R = g->row.data();
   const int32_t *C = g->col.data();
 
-  // ---- iterative Hopcroft-Tarjan: DFS tree, low links, subtree sizes, BCCs.
-  // The explicit stack holds one frame per open vertex (its arc cursor, low
-  // link and subtree size), so the scan of a vertex's arcs touches only its
-  // frame and the neighbours' discovery times.
-  std::vector<int32_t> disc((size_t)n, -1), tbcc((size_t)n, -1), locid((size_t)n, -1), comp((size_t)n, -1);
-  std::vector<int64_t> sz((size_t)n, 0), hang((size_t)n, 0);
-  std::vector<double> sq((size_t)n, 0.0);
-  std::vector<int64_t> comp_size;
-  std::vector<int32_t> head, child;          // per BCC
-  std::vector<int64_t> mem_off{0};           // per BCC member range
-  std::vector<int32_t> members;              // head stored last
-  struct Frame {
-    int64_t e, e1;  // arc cursor and end
-    int64_t size;   // subtree size so far
-    int32_t u, parent, disc, low;
-  };
-  std::vector<Frame> stack;
-  std::vector<int32_t> vstack;
-  stack.reserve(1024);
-  vstack.reserve(1024);
-  int32_t timer = 0;
-  for (int32_t r = 0; r < n; ++r) {
-    if (disc[r] >= 0) continue;
-    int32_t cid = (int32_t)comp_size.size();
-    disc[r] = timer;
-    comp[r] = cid;
-    stack.push_back(Frame{R[r], R[r + 1], 1, r, -1, timer, timer});
-    ++timer;
-    vstack.push_back(r);
-    while (!stack.empty()) {
-      Frame &f = stack.back();
-      int32_t next = -1;
-      while (f.e < f.e1) {
-        const int32_t w = C[f.e++];
-        const int32_t dw = disc[w];
-        if (dw < 0) { next = w; break; }
-        if (w != f.parent && dw < f.low) f.low = dw;
-      }
-      if (next >= 0) {
-        const int32_t w = next, pu = f.u;  // f is not used past the push
-        disc[w] = timer;
-        comp[w] = cid;
-        stack.push_back(Frame{R[w], R[w + 1], 1, w, pu, timer, timer});
-        ++timer;
-        vstack.push_back(w);
-        continue;
-      }
-      const Frame done = stack.back();
-      stack.pop_back();
-      const int32_t u = done.u;
-      sz[u] = done.size;
-      if (stack.empty()) continue;  // the root
-      Frame &pf = stack.back();
-      const int32_t p = pf.u;
-      if (done.low < pf.low) pf.low = done.low;
-      pf.size += done.size;
-      if (done.low >= pf.disc) {  // tree edge (p,u) closes a BCC headed by p
-        int32_t b = (int32_t)head.size();
-        head.push_back(p);
-        child.push_back(u);
-        int32_t w;
-        do {
-          w = vstack.back();
-          vstack.pop_back();
-          tbcc[w] = b;
-          locid[w] = (int32_t)(members.size() - (size_t)mem_off[b]);
-          members.push_back(w);
-        } while (w != u);
-        members.push_back(p);
-        mem_off.push_back((int64_t)members.size());
-        hang[p] += done.size;
-        sq[p] += (double)done.size * (double)done.size;
-      }
-    }
-    vstack.clear();  // only the root remains
-    comp_size.push_back(sz[r]);
-  }
-  const int32_t nbcc = (int32_t)head.size();
+  Split SP;
+  split_bccs(g, SP);
+  const int32_t nbcc = SP.nbcc;
+  const std::vector<int32_t> &comp = SP.comp, &tbcc = SP.tbcc, &pre = SP.pre, &head = SP.head,
+                             &locid = SP.locid, &members = SP.members;
+  const std::vector<int64_t> &comp_size = SP.comp_size, &below = SP.below, &hang = SP.hang, &sq = SP.sq,
+                             &mem_off = SP.mem_off;
 
-  // ---- articulation cross terms
+  // ---- articulation cross terms: S^2 - sum of squared parts of comp - x
   D->art.assign((size_t)n, 0.0);
   int32_t n_art = 0;
+#pragma omp parallel for schedule(static) reduction(+ : n_art)
   for (int32_t x = 0; x < n; ++x) {
-    double S = (double)(comp_size[comp[x]] - 1);
-    double up = S - (double)hang[x];
-    double a = S * S - sq[x] - up * up;
-    D->art[x] = a;
-    n_art += a > 0.0;
+    const int64_t S = comp_size[comp[x]] - 1, up = S - hang[x];
+    const int64_t a = S * S - sq[x] - up * up;
+    D->art[x] = (double)a;
+    n_art += a > 0;
   }
 
-  // ---- BCC of every arc: the BCC of the tree edge into its deeper end
+  // ---- BCC of every arc: the BCC of the tree edge into its endpoint with the larger pre
   std::vector<int64_t> slot_off(mem_off);  // member slot of (b, local) = mem_off[b] + local
   const int64_t n_slots = mem_off.back();
   auto local_of = [&](int32_t x, int32_t b) -> int32_t {
@@ -458,7 +796,7 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   for (int32_t x = 0; x < n; ++x)
     for (int64_t e = R[x]; e < R[x + 1]; ++e) {
       int32_t y = C[e];
-      int32_t b = tbcc[disc[x] > disc[y] ? x : y];
+      int32_t b = tbcc[pre[x] > pre[y] ? x : y];
       sdeg[mem_off[b] + local_of(x, b) + 1]++;
     }
   for (int64_t s = 0; s < n_slots; ++s) sdeg[s + 1] += sdeg[s];
@@ -469,7 +807,7 @@ int decompose(const bc_graph *g, bc_decomp *D) {
     for (int32_t x = 0; x < n; ++x)
       for (int64_t e = R[x]; e < R[x + 1]; ++e) {
         int32_t y = C[e];
-        int32_t b = tbcc[disc[x] > disc[y] ? x : y];
+        int32_t b = tbcc[pre[x] > pre[y] ? x : y];
         sadj[fill[mem_off[b] + local_of(x, b)]++] = local_of(y, b);
       }
   }
@@ -512,29 +850,37 @@ int decompose(const bc_graph *g, bc_decomp *D) {
     const int64_t *sd = sdeg.data() + mem_off[b];
     auto deg = [&](int32_t k) { return (int32_t)(sd[k + 1] - sd[k]); };
     auto adj = [&](int32_t k) { return sadj.data() + sd[k]; };
+    const int32_t *vid = members.data() + mem_off[b];  // local id -> vertex id
     bool cycle = true;
     int32_t root = 0;
     for (int32_t k = 0; k < nb; ++k) {
       if (deg(k) != 2) cycle = false;
-      if (deg(k) > deg(root)) root = k;
+      if (deg(k) > deg(root) || (deg(k) == deg(root) && vid[k] < vid[root])) root = k;
     }
     n_cycle[i] = cycle;
-    // plain (non-chain) vertices in BFS order from the max-degree vertex
+    // plain (non-chain) vertices in BFS order from the max-degree vertex (the
+    // smallest vertex id among equals); large BCCs level-synchronously, in
+    // the same order
     std::vector<int32_t> nid((size_t)nb, -1), old;
     old.reserve((size_t)nb);
     {
-      std::vector<char> seen((size_t)nb, 0);
       std::vector<int32_t> q;
-      q.reserve((size_t)nb);
-      q.push_back(root);
-      seen[root] = 1;
-      for (size_t h = 0; h < q.size(); ++h) {
-        int32_t x = q[h];
-        if (cycle || deg(x) != 2) { nid[x] = (int32_t)old.size(); old.push_back(x); }
-        const int32_t *a = adj(x);
-        for (int32_t j = 0; j < deg(x); ++j)
-          if (!seen[a[j]]) { seen[a[j]] = 1; q.push_back(a[j]); }
+      if (par) {
+        q = bfs_exact_order(nb, root, [&](int32_t x, const int32_t **a) { *a = adj(x); return deg(x); });
+      } else {
+        std::vector<char> seen((size_t)nb, 0);
+        q.reserve((size_t)nb);
+        q.push_back(root);
+        seen[root] = 1;
+        for (size_t h = 0; h < q.size(); ++h) {
+          const int32_t x = q[h];
+          const int32_t *a = adj(x);
+          for (int32_t j = 0; j < deg(x); ++j)
+            if (!seen[a[j]]) { seen[a[j]] = 1; q.push_back(a[j]); }
+        }
       }
+      for (const int32_t x : q)
+        if (cycle || deg(x) != 2) { nid[x] = (int32_t)old.size(); old.push_back(x); }
       if ((int32_t)q.size() != nb) bad = 1;  // a BCC is connected
     }
     const int32_t nplain = (int32_t)old.size();
@@ -654,7 +1000,7 @@ int decompose(const bc_graph *g, bc_decomp *D) {
       int32_t x = members[s];
       D->orig[base + k] = x;
       D->reach[base + k] =
-          (x == head[b]) ? (int32_t)(comp_size[comp[x]] - 1 - sz[child[b]]) : (int32_t)hang[x];
+          (x == head[b]) ? (int32_t)(comp_size[comp[x]] - 1 - below[b]) : (int32_t)hang[x];
     }
   };
   for (int32_t i = 0; i < np_bcc; ++i)

@@ -4,7 +4,7 @@
  *
  * Replaces the reference's host pipeline ahead of begin_gpu:
  *   Graph::Graph(char*)                Codes/graph.cpp:38-59     -> bc_graph_load / bc_graph_from_edges
- *   BiCC::run_bicc / bicc_tarjan       Codes/bicc.cpp:39,81-161  -> bc_decompose (iterative, no recursion)
+ *   BiCC::run_bicc / bicc_tarjan       Codes/bicc.cpp:39,81-161  -> bc_decompose (parallel, no recursion)
  *   per-BCC relabel                    Codes/modified_apsp.cpp:273-363
  *   fillbccparent / reachfunction      Codes/modified_apsp.cpp:77-220 (reach, articulation terms)
  *   bcc_bfs + preSum (ear chains)      Codes/bcc_bfs.cpp:247-1330, :100-236
@@ -52,7 +52,10 @@ typedef struct bc_decomp_info {
 } bc_decomp_info;
 
 /* Splits g into BCCs, computes reach and articulation terms, finds degree-2
- * chains and packs every BCC of >= 3 vertices (largest first). */
+ * chains and packs every BCC of >= 3 vertices (largest first; equal sizes in
+ * the order of their smallest vertex other than the head, the member closest
+ * to the smallest vertex of the component). The result depends only on g,
+ * not on the host thread count. */
 int bc_decompose(const bc_graph *g, bc_decomp **out);
 void bc_decomp_free(bc_decomp *d);
 /* Borrowed view, valid until bc_decomp_free. */

@@ -164,7 +164,8 @@ print(int(arrs["vtx_off"][1]), h.hexdigest())
 
 
 def test_decomposition_independent_of_thread_count():
-    """The decomposition's parallel passes (arc-to-BCC assignment, packed
+    """The decomposition's parallel passes (the BCC split, whose BFS forest
+    and union-finds depend on thread timing; arc-to-BCC assignment, packed
     writes; the RMAT-16 giant BCC takes the large-BCC path) give the same
     arrays with 1 and 4 host threads."""
     import os
@@ -274,6 +275,42 @@ def test_larger_decomposition_matches_oracle(seed):
     mine = {b["verts"]: b for b in product_bccs(arrs)}
     theirs, art = _oracle_bccs(n, u, v)
     assert set(mine) == {b["verts"] for b in theirs}
+    for b in theirs:
+        m = mine[b["verts"]]
+        assert m["reach"] == b["reach"] and m["chains"] == b["chains"] and m["free"] == b["free"]
+    assert np.array_equal(arrs["art"], art)
+    row, col = oracle().csr(n, u, v)
+    assert rel_err(oracle().method_bc_from_decomp(arrs), oracle().brandes(n, row, col)) < 1e-12
+
+
+def wide_level_graph(seed):
+    """A component whose BFS forest has a level of more than 2048 vertices
+    (vertex 0, the root, adjacent to 2600 others), so the BCC split takes its
+    parallel BFS and sweep paths: random edges among the hub's neighbours,
+    edges subdivided into chains, pendant trees, and a second, deep component
+    (a long cycle with chords)."""
+    G = graphs()
+    rng = np.random.default_rng(2000 + seed)
+    n = 3200
+    u = np.concatenate([np.zeros(2600, np.int64), rng.integers(1, n, 1400)])
+    v = np.concatenate([np.arange(1, 2601), rng.integers(1, n, 1400)])
+    uu, vv = G.simple_edges(n, u, v)
+    n, uu, vv = G.subdivide(n, uu, vv, 0.3, 1, 3, rng)
+    n, uu, vv = G.attach_leaves(n, uu, vv, 300, n, rng)
+    k = n  # a 600-cycle with 40 chords
+    cu = np.concatenate([k + np.arange(600), k + rng.integers(0, 600, 40)])
+    cv = np.concatenate([k + (np.arange(600) + 1) % 600, k + rng.integers(0, 600, 40)])
+    return (n + 600,) + G.simple_edges(n + 600, np.concatenate([uu, cu]), np.concatenate([vv, cv]))
+
+
+@pytest.mark.parametrize("seed", range(2))
+def test_wide_level_decomposition_matches_oracle(seed):
+    n, u, v = wide_level_graph(seed)
+    P = pkg()
+    arrs = P.Decomposition(P.Graph.from_edges(n, u, v)).arrays()
+    mine = {b["verts"]: b for b in product_bccs(arrs)}
+    theirs, art = _oracle_bccs(n, u, v)
+    assert len(theirs) > 10 and set(mine) == {b["verts"] for b in theirs}
     for b in theirs:
         m = mine[b["verts"]]
         assert m["reach"] == b["reach"] and m["chains"] == b["chains"] and m["free"] == b["free"]
