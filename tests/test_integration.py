@@ -3,7 +3,8 @@ the file centrality-gpu_b200/reference_binding/begin_gpupgm_bcgpu.cpp, and
 the reference's own host pipeline links against it and the in-tree
 libbcgpu.so (oracle/_ref/refbetc, built from the reference's sources when
 they are present). Running it needs a GPU; without one it must stop at its
-first begin_gpu call with libbcgpu's error, not compute anything."""
+first begin_gpu call with libbcgpu's error, not compute anything. On a GPU
+(marked test) it prints what it prints with the oracle behind the binding."""
 import os
 import re
 import subprocess
@@ -144,3 +145,22 @@ def test_reference_betc_without_ears_gives_exact_bc(tmp_path):
     want = O.brandes(8, row, col)
     assert want[1] > 0 and want[0] > 0
     assert np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not REFBETC.exists(), reason="reference sources absent: refbetc not built")
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_reference_betc_on_the_gpu_gives_reference_semantics(tmp_path, name):
+    """The reference's own betc rebuilt on the binding, its begin_gpu calls
+    now computed by libbcgpu on the GPU: the same output as with the oracle
+    behind the binding (the reference's semantics; the exact BC where a BCC
+    has no ears)."""
+    n, u, v, golden, _ = load_case(name)
+    r = subprocess.run([str(REFBETC), str(GOLDEN / f"{name}.txt")], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = _bc_lines(r.stdout, n)
+    want = reference_semantics_bc(n, u, v)
+    assert np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))) < 1e-5  # the reference's float buffers
+    if P().Decomposition(P().Graph.from_edges(n, u, v)).arrays()["n_chains"] == 0:
+        assert np.max(np.abs(got - golden) / np.maximum(1.0, np.abs(golden))) < 1e-5
