@@ -105,6 +105,7 @@ _SIGS = {
     "bc_graph_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_size_t]),
     "bc_graph_csr": (C.c_int, [C.c_void_p, _i32p, _i64p, C.POINTER(_i64p), C.POINTER(_i32p)]),
     "bc_decompose": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bc_decompose_gpu": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "bc_decomp_free": (None, [C.c_void_p]),
     "bc_decomp_view": (C.POINTER(BcBccs), [C.c_void_p]),
     "bc_decomp_get_info": (None, [C.c_void_p, C.POINTER(BcDecompInfo)]),
@@ -202,14 +203,24 @@ def _arr(ptr, count, dtype):
 
 
 class Decomposition:
-    """BCC split + reach + articulation terms + degree-2 chains (bc_decompose)."""
+    """BCC split + reach + articulation terms + degree-2 chains (bc_decompose).
 
-    def __init__(self, graph: Graph):
+    ``gpu_device``: run the BCC split and the arc-to-member pass on that GPU
+    (bc_decompose_gpu; same result); -1 runs those GPU steps as host loops,
+    a check of them without a GPU."""
+
+    def __init__(self, graph: Graph, gpu_device: int | None = None):
         self._graph = graph
         h = C.c_void_p()
-        rc = lib().bc_decompose(graph._h, C.byref(h))
-        if rc:
-            raise BcError(rc, "bc_decompose")
+        if gpu_device is None:
+            rc = lib().bc_decompose(graph._h, C.byref(h))
+            if rc:
+                raise BcError(rc, "bc_decompose")
+        else:
+            err = C.create_string_buffer(512)
+            rc = lib().bc_decompose_gpu(graph._h, int(gpu_device), C.byref(h), err, 512)
+            if rc:
+                raise BcError(rc, "bc_decompose_gpu: " + err.value.decode(errors="replace"))
         self._h = h
         self.view = lib().bc_decomp_view(h)
         info = BcDecompInfo()

@@ -25,6 +25,7 @@
 //    cycle emits none: all its vertices stay free). Here those paths are
 //    walked directly from their endpoints in O(n_b + m_b).
 #include "bchost.h"
+#include "decomp.h"
 
 #include <algorithm>
 #include <chrono>
@@ -38,19 +39,6 @@
 
 #include <omp.h>
 
-struct bc_graph {
-  int32_t n = 0;
-  std::vector<int64_t> row;
-  std::vector<int32_t> col;
-};
-
-struct bc_decomp {
-  bc_bccs view{};
-  bc_decomp_info info{};
-  std::vector<int64_t> vtx_off, row, chain_off;
-  std::vector<int32_t> col, reach, orig, n_plain, chain_start, chain_len, chain_l, chain_r;
-  std::vector<double> art;
-};
 
 namespace {
 
@@ -768,23 +756,22 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   split_bccs(g, SP);
   const int32_t nbcc = SP.nbcc;
   const std::vector<int32_t> &comp = SP.comp, &tbcc = SP.tbcc, &pre = SP.pre, &head = SP.head,
-                             &locid = SP.locid, &members = SP.members;
-  const std::vector<int64_t> &comp_size = SP.comp_size, &below = SP.below, &hang = SP.hang, &sq = SP.sq,
-                             &mem_off = SP.mem_off;
+                             &locid = SP.locid;
+  const std::vector<int64_t> &comp_size = SP.comp_size, &hang = SP.hang, &sq = SP.sq, &mem_off = SP.mem_off;
+  bcg::SplitResult out;
 
   // ---- articulation cross terms: S^2 - sum of squared parts of comp - x
-  D->art.assign((size_t)n, 0.0);
+  out.art.assign((size_t)n, 0.0);
   int32_t n_art = 0;
 #pragma omp parallel for schedule(static) reduction(+ : n_art)
   for (int32_t x = 0; x < n; ++x) {
     const int64_t S = comp_size[comp[x]] - 1, up = S - hang[x];
     const int64_t a = S * S - sq[x] - up * up;
-    D->art[x] = (double)a;
+    out.art[x] = (double)a;
     n_art += a > 0;
   }
 
   // ---- BCC of every arc: the BCC of the tree edge into its endpoint with the larger pre
-  std::vector<int64_t> slot_off(mem_off);  // member slot of (b, local) = mem_off[b] + local
   const int64_t n_slots = mem_off.back();
   auto local_of = [&](int32_t x, int32_t b) -> int32_t {
     return x == head[b] ? (int32_t)(mem_off[b + 1] - mem_off[b] - 1) : locid[x];
@@ -811,6 +798,30 @@ int decompose(const bc_graph *g, bc_decomp *D) {
         sadj[fill[mem_off[b] + local_of(x, b)]++] = local_of(y, b);
       }
   }
+  out.nbcc = nbcc;
+  out.n_art = n_art;
+  out.comp = std::move(SP.comp);
+  out.head = std::move(SP.head);
+  out.members = std::move(SP.members);
+  out.comp_size = std::move(SP.comp_size);
+  out.below = std::move(SP.below);
+  out.hang = std::move(SP.hang);
+  out.mem_off = std::move(SP.mem_off);
+  out.sdeg = std::move(sdeg);
+  out.sadj = std::move(sadj);
+  return bcg::decomp_pack(out, n, D, t0);
+}
+
+}  // namespace
+
+namespace bcg {
+
+int decomp_pack(SplitResult &SR, int32_t n, bc_decomp *D, std::chrono::steady_clock::time_point t0) {
+  const int32_t nbcc = SR.nbcc, n_art = SR.n_art;
+  const std::vector<int32_t> &comp = SR.comp, &head = SR.head, &members = SR.members, &sadj = SR.sadj;
+  const std::vector<int64_t> &comp_size = SR.comp_size, &below = SR.below, &hang = SR.hang, &mem_off = SR.mem_off,
+                             &sdeg = SR.sdeg;
+  D->art = std::move(SR.art);
 
   // ---- pack BCCs with >= 3 vertices, largest first
   std::vector<int32_t> order;
@@ -1049,7 +1060,7 @@ int decompose(const bc_graph *g, bc_decomp *D) {
   return BCGPU_OK;
 }
 
-}  // namespace
+}  // namespace bcg
 
 extern "C" int bc_decompose(const bc_graph *g, bc_decomp **out) {
   if (!g || !out) return BCGPU_EINVAL;

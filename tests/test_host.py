@@ -370,3 +370,26 @@ def test_binary_csr_is_checked(tmp_path):
     assert "loop" in reason(2, [0, 1, 2], [0, 1])
     assert "out of range" in reason(2, [0, 1, 2], [1, 7])
     assert "reverse" in reason(3, [0, 1, 1, 1], [1])
+
+
+def _same_arrays(a, b):
+    return all(np.array_equal(a[k], b[k]) if hasattr(a[k], "shape") else a[k] == b[k] for k in a)
+
+
+@pytest.mark.parametrize("family", ["random", "larger", "wide", "rmat16", "grid"])
+def test_gpu_decomposition_steps_on_host_equal_bc_decompose(family):
+    """bc_decompose_gpu's data-parallel steps (union-find components, BFS
+    forest, level sweeps, union-find over tree edges, member slots), run as
+    host loops (device -1), give exactly bc_decompose's packed arrays."""
+    P = pkg()
+    G = graphs()
+    cases = {
+        "random": lambda: [random_graph(s)[:3] for s in range(0, 40, 3)],
+        "larger": lambda: [larger_random_graph(s) for s in range(12)],
+        "wide": lambda: [wide_level_graph(s) for s in range(2)],
+        "rmat16": lambda: [G.gen_rmat(16, 16, 0.2, 1, 8, seed=2)],
+        "grid": lambda: [G.gen_grid(seed=3)],
+    }[family]()
+    for n, u, v in cases:
+        g = P.Graph.from_edges(n, u, v)
+        assert _same_arrays(P.Decomposition(g).arrays(), P.Decomposition(g, gpu_device=-1).arrays())
