@@ -205,7 +205,7 @@ def _arr(ptr, count, dtype):
 class Decomposition:
     """BCC split + reach + articulation terms + degree-2 chains (bc_decompose).
 
-    ``gpu_device``: run the BCC split and the arc-to-member pass on that GPU
+    ``gpu_device``: run the decomposition on that GPU as data-parallel steps
     (bc_decompose_gpu; same result); -1 runs those GPU steps as host loops,
     a check of them without a GPU."""
 

@@ -41,9 +41,15 @@ struct SplitResult {
 // the start of the whole decomposition, for bc_decomp_info::host_ms.
 int decomp_pack(SplitResult &S, int32_t n, bc_decomp *D, std::chrono::steady_clock::time_point t0);
 
-// The BCC split and the arc-to-member pass as data-parallel steps
-// (decomp_steps.cu): on GPU `device` (>= 0), or, for a check of the same
-// steps without a GPU, as host loops (device < 0).
-int decomp_split_steps(const bc_graph *g, int device, SplitResult &S, char *err, size_t errlen);
+// Points D's view at its arrays and fills its info (D's vtx_off, row,
+// chain_off and chain_len must be final).
+void decomp_finish(bc_decomp *D, int32_t n, int32_t n_components, int32_t nbcc, int32_t n_art, int64_t n_cycle_bccs,
+                   std::chrono::steady_clock::time_point t0);
+
+// The whole decomposition as data-parallel steps (decomp_steps.cu): on GPU
+// `device` (>= 0), or, for a check of the same steps without a GPU, as host
+// loops (device < 0). Same result as bc_decompose.
+int decomp_gpu(const bc_graph *g, int device, bc_decomp *D, std::chrono::steady_clock::time_point t0, char *err,
+               size_t errlen);
 
 }  // namespace bcg

@@ -1,11 +1,13 @@
-// The BCC split and the arc-to-member pass as data-parallel steps, for the
-// GPU (bc_decompose_gpu): Tarjan and Vishkin's method over a BFS forest, the
-// same mathematics as the host split in host_decomp.cpp, written as one
-// functor per step over vertices, frontier positions or BCCs. A backend runs
-// the steps: DevBackend as a grid-stride kernel per step on one GPU,
-// HostBackend as OpenMP loops over the very same functors -- a check of the
-// GPU steps on a machine without one. Prefix sums (a handful, over vertices,
-// roots, BCCs and member slots) are taken on the host in both.
+// The decomposition as data-parallel steps, for the GPU (bc_decompose_gpu):
+// the BCC split (Tarjan and Vishkin's method over a BFS forest, the same
+// mathematics as the host split in host_decomp.cpp), the arc-to-member pass
+// and the packing (exact-order BFS of every BCC at once, chains, packed CSR),
+// written as one functor per step over vertices, frontier positions, member
+// slots or BCCs. A backend runs the steps: DevBackend as a grid-stride kernel
+// per step on one GPU, HostBackend as OpenMP loops over the very same
+// functors -- a check of the GPU steps on a machine without one. Prefix sums
+// are taken on the host in both, as are the stable regrouping of the BFS
+// order by BCC and the sort of rows longer than 32 arcs.
 //
 // Steps (vertex ids int32, counts int64):
 //   components   union-find over the edges, roots the smallest vertices
@@ -24,7 +26,11 @@
 //                vertices under them, hang(x) = sum of below over the BCCs x
 //                heads; articulation terms S^2 - sum of squared parts;
 //   members      per-BCC member lists (head last) and, per member slot, the
-//                member's arcs inside the BCC as local ids in arc order.
+//                member's arcs inside the BCC as local ids in arc order;
+//   packing      as host_decomp.cpp's decomp_pack writes it: BCCs of >= 3
+//                vertices largest first, each in BFS order from its max-degree
+//                vertex (plain vertices first, then chains numbered from the
+//                end met first), adjacency in the new local ids.
 // The split and reach follow Codes/bicc.cpp:81-161 and
 // Codes/modified_apsp.cpp:77-220 in what they compute (not how).
 #include <cuda_runtime.h>
@@ -473,8 +479,17 @@ struct DevBackend {
   }
 };
 
+// The split's results, resident where the backend runs (owned by it).
+struct DevSplit {
+  int32_t n = 0;
+  int64_t arcs = 0, nroots = 0, nbcc = 0, n_slots = 0;
+  int32_t *comp, *head, *members, *sadj, *n_art;
+  int64_t *csize, *below, *hang, *mem_off, *sdeg;
+  double *art;
+};
+
 template <class BE>
-void run(BE &be, const bc_graph *g, SplitResult &S) {
+DevSplit run_split(BE &be, const bc_graph *g) {
   const int32_t n = g->n;
   const int64_t arcs = g->row.empty() ? 0 : g->row[n];
   int64_t *R = be.template alloc<int64_t>((size_t)n + 1);
@@ -566,34 +581,447 @@ void run(BE &be, const bc_graph *g, SplitResult &S) {
   be.each(n_slots, Copy64{cursor, sdeg});
   be.each(n, SlotArcs{R, C, tbcc, pre, head, locid, mem_off, nullptr, cursor, sadj});
 
-  // results to the host
-  S.nbcc = (int32_t)nbcc;
-  be.download(&S.n_art, n_art, 1);
-  S.comp.resize((size_t)n);
-  S.head.resize((size_t)nbcc);
-  S.members.resize((size_t)n_slots);
-  S.sadj.resize((size_t)arcs);
-  S.comp_size.resize((size_t)nroots);
-  S.below.resize((size_t)nbcc);
-  S.hang.resize((size_t)n);
-  S.mem_off.resize((size_t)nbcc + 1);
-  S.sdeg.resize((size_t)n_slots + 1);
-  S.art.resize((size_t)n);
-  be.download(S.comp.data(), comp, (size_t)n);
-  be.download(S.head.data(), head, (size_t)nbcc);
-  be.download(S.members.data(), members, (size_t)n_slots);
-  be.download(S.sadj.data(), sadj, (size_t)arcs);
-  be.download(S.comp_size.data(), csize, (size_t)nroots);
-  be.download(S.below.data(), below, (size_t)nbcc);
-  be.download(S.hang.data(), hang, (size_t)n);
-  be.download(S.mem_off.data(), mem_off, (size_t)nbcc + 1);
-  be.download(S.sdeg.data(), sdeg, (size_t)n_slots + 1);
-  be.download(S.art.data(), art, (size_t)n);
+  DevSplit d;
+  d.n = n;
+  d.arcs = arcs;
+  d.nroots = nroots;
+  d.nbcc = nbcc;
+  d.n_slots = n_slots;
+  d.comp = comp;
+  d.head = head;
+  d.members = members;
+  d.sadj = sadj;
+  d.n_art = n_art;
+  d.csize = csize;
+  d.below = below;
+  d.hang = hang;
+  d.mem_off = mem_off;
+  d.sdeg = sdeg;
+  d.art = art;
+  return d;
+}
+
+// ---- packing on the device: the order, chains and packed CSR that
+// decomp_pack (host_decomp.cpp) writes, as steps. Packed BCC i is BCC
+// pk_bcc[i]; its local ids follow an exact-order BFS from its max-degree
+// vertex (smallest id among equals), plain vertices first, then each chain.
+__host__ __device__ inline void amax64u(uint64_t *p, uint64_t v) {
+#ifdef __CUDA_ARCH__
+  atomicMax((unsigned long long *)p, (unsigned long long)v);
+#else
+  uint64_t c = __atomic_load_n(p, __ATOMIC_RELAXED);
+  while (v > c && !__atomic_compare_exchange_n(p, &c, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+  }
+#endif
+}
+// Largest k in [0, m) with a[k] <= v (a ascending, a[0] <= v).
+__host__ __device__ inline int64_t floor_index(const int64_t *a, int64_t m, int64_t v) {
+  int64_t lo = 0, hi = m - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) / 2;
+    if (a[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Member slots of the packed BCCs, as the packing sees them.
+struct Slots {
+  const int64_t *mem_off, *sdeg;
+  const int32_t *sadj, *slot_b, *pk_of, *members;
+  __host__ __device__ int32_t deg(int32_t s) const { return (int32_t)(sdeg[s + 1] - sdeg[s]); }
+  // slot of the k-th neighbour of slot s
+  __host__ __device__ int32_t nbr(int32_t s, int32_t k) const {
+    return (int32_t)(mem_off[slot_b[s]] + sadj[sdeg[s] + k]);
+  }
+  __host__ __device__ int32_t pk(int32_t s) const { return pk_of[slot_b[s]]; }
+  // Far end of the chain that leaves slot x through its neighbour cur (at
+  // most nb steps; *len > nb when there is no end).
+  __host__ __device__ int32_t walk(int32_t x, int32_t cur, int64_t nb, int64_t *len) const {
+    int32_t prev = x;
+    int64_t k = 0;
+    while (deg(cur) == 2 && k <= nb) {
+      const int32_t a0 = nbr(cur, 0), a1 = nbr(cur, 1);
+      const int32_t nx = a0 == prev ? a1 : a0;
+      prev = cur;
+      cur = nx;
+      ++k;
+    }
+    *len = k;
+    return cur;
+  }
+};
+
+struct SlotBcc {
+  const int64_t *mem_off;
+  int64_t nbcc;
+  int32_t *slot_b;
+  __host__ __device__ void operator()(int64_t s) const { slot_b[s] = (int32_t)floor_index(mem_off, nbcc, s); }
+};
+struct RootKey {  // max over a packed BCC's members of (degree, -vertex id); cycle test
+  Slots S;
+  uint64_t *key;
+  int32_t *cyc;
+  __host__ __device__ void operator()(int64_t s) const {
+    const int32_t i = S.pk((int32_t)s);
+    if (i < 0) return;
+    const int32_t d = S.deg((int32_t)s);
+    if (d != 2) st32(&cyc[i], 0);
+    amax64u(&key[i], ((uint64_t)(uint32_t)d << 32) | (uint64_t)(uint32_t)(INT32_MAX - S.members[s]));
+  }
+};
+struct RootSlot {
+  Slots S;
+  const uint64_t *key;
+  int32_t *bq, *seen;
+  __host__ __device__ void operator()(int64_t s) const {
+    const int32_t i = S.pk((int32_t)s);
+    if (i < 0) return;
+    if (INT32_MAX - (int32_t)(key[i] & 0xffffffffu) == S.members[s]) {
+      bq[i] = (int32_t)s;
+      seen[s] = 1;
+    }
+  }
+};
+// One level of the BFS of every packed BCC at once, in the sequential
+// queue's order: a slot is claimed by the earliest frontier position next to
+// it; counts per position, a prefix sum, then each position writes its own.
+struct PClaim {
+  Slots S;
+  const int32_t *bq, *seen;
+  int32_t *claim;
+  int64_t f0;
+  __host__ __device__ void operator()(int64_t i) const {
+    const int32_t s = bq[f0 + i];
+    for (int32_t k = 0; k < S.deg(s); ++k) {
+      const int32_t t = S.nbr(s, k);
+      if (!seen[t]) min32(&claim[t], (int32_t)i);
+    }
+  }
+};
+struct PCount {
+  Slots S;
+  const int32_t *bq, *seen, *claim;
+  int64_t *cnt;
+  int64_t f0;
+  __host__ __device__ void operator()(int64_t i) const {
+    const int32_t s = bq[f0 + i];
+    int64_t c = 0;
+    for (int32_t k = 0; k < S.deg(s); ++k) {
+      const int32_t t = S.nbr(s, k);
+      c += !seen[t] && ld32(&claim[t]) == (int32_t)i;
+    }
+    cnt[i] = c;
+  }
+};
+struct PEmit {
+  Slots S;
+  const int32_t *seen, *claim;
+  const int64_t *at0;  // exclusive prefix of PCount
+  int32_t *bq;
+  int64_t f0, f1;
+  __host__ __device__ void operator()(int64_t i) const {
+    const int32_t s = bq[f0 + i];
+    int64_t at = f1 + at0[i];
+    for (int32_t k = 0; k < S.deg(s); ++k) {
+      const int32_t t = S.nbr(s, k);
+      if (!seen[t] && ld32(&claim[t]) == (int32_t)i) bq[at++] = t;
+    }
+  }
+};
+struct PMark {
+  const int32_t *bq;
+  int32_t *seen;
+  int64_t f1;
+  __host__ __device__ void operator()(int64_t k) const { seen[bq[f1 + k]] = 1; }
+};
+struct PlainFlag {  // plain = not a chain vertex (every vertex of a cycle BCC is plain)
+  Slots S;
+  const int32_t *q, *cyc;
+  int64_t *flag;
+  __host__ __device__ void operator()(int64_t k) const {
+    const int32_t s = q[k];
+    flag[k] = cyc[S.pk(s)] || S.deg(s) != 2;
+  }
+};
+struct PlainPlace {
+  Slots S;
+  const int32_t *q, *cyc;
+  const int64_t *gidx, *plain_base, *vtx_off;
+  int32_t *nid, *pl, *old;
+  __host__ __device__ void operator()(int64_t k) const {
+    const int32_t s = q[k], i = S.pk(s);
+    if (!(cyc[i] || S.deg(s) != 2)) return;
+    const int32_t f = (int32_t)(gidx[k] - plain_base[i]);
+    nid[s] = f;
+    pl[gidx[k]] = s;
+    old[vtx_off[i] + f] = s;
+  }
+};
+// Chains, numbered from whichever end comes first in the plain order, their
+// vertices from that end: count per plain vertex, then (after prefix sums)
+// write.
+struct Chains {
+  Slots S;
+  const int32_t *pl, *cyc, *nid_plain;
+  const int64_t *plain_base, *vtx_off;
+  int32_t *bad;
+  int64_t *cnt, *vcnt;                      // count pass
+  const int64_t *cidx, *voff, *voff_base;   // write pass
+  const int32_t *n_plain;
+  int32_t *ch_start, *ch_len, *ch_l, *ch_r, *nid, *old;
+  __host__ __device__ void operator()(int64_t g) const {
+    const int32_t x = pl[g], i = S.pk(x);
+    if (cnt) cnt[g] = vcnt[g] = 0;
+    if (cyc[i]) return;
+    const int64_t nb = vtx_off[i + 1] - vtx_off[i];
+    const int32_t f = (int32_t)(g - plain_base[i]);
+    int64_t c = cnt ? 0 : cidx[g];
+    int64_t pos = cnt ? 0 : n_plain[i] + (voff[g] - voff_base[i]);
+    int64_t nc = 0, nv = 0;
+    for (int32_t k = 0; k < S.deg(x); ++k) {
+      const int32_t t = S.nbr(x, k);
+      if (S.deg(t) != 2) continue;
+      int64_t len;
+      const int32_t far = S.walk(x, t, nb, &len);
+      if (len > nb || far == x) {
+        st32(bad, 1);
+        continue;
+      }
+      if (nid_plain[far] < f) continue;  // numbered from its other end
+      if (cnt) {
+        ++nc;
+        nv += len;
+        continue;
+      }
+      ch_start[c] = (int32_t)pos;
+      ch_len[c] = (int32_t)len;
+      ch_l[c] = f;
+      ch_r[c] = nid_plain[far];
+      ++c;
+      int32_t prev = x, cur = t;
+      for (int64_t j = 0; j < len; ++j) {
+        nid[cur] = (int32_t)pos;
+        old[vtx_off[i] + pos] = cur;
+        ++pos;
+        const int32_t a0 = S.nbr(cur, 0), a1 = S.nbr(cur, 1);
+        const int32_t nx = a0 == prev ? a1 : a0;
+        prev = cur;
+        cur = nx;
+      }
+    }
+    if (cnt) {
+      cnt[g] = nc;
+      vcnt[g] = nv;
+    }
+  }
+};
+struct Unset {  // positions no step wrote
+  const int32_t *old;
+  int32_t *bad;
+  __host__ __device__ void operator()(int64_t k) const {
+    if (old[k] < 0) st32(bad, 1);
+  }
+};
+struct Inverse {
+  const int32_t *old;
+  const int64_t *vtx_off;
+  int64_t np;
+  int32_t *inv;
+  __host__ __device__ void operator()(int64_t k) const {
+    inv[old[k]] = (int32_t)(k - vtx_off[floor_index(vtx_off, np, k)]);
+  }
+};
+struct RowLen {
+  Slots S;
+  const int32_t *old;
+  int64_t *row;
+  __host__ __device__ void operator()(int64_t k) const { row[k] = S.deg(old[k]); }
+};
+constexpr int32_t kSmallRow = 32;  // longer rows are sorted on the host
+struct ColFill {
+  Slots S;
+  const int32_t *old, *inv, *head, *comp;
+  const int64_t *row, *csize, *below, *hang;
+  int32_t *col, *orig, *reach;
+  __host__ __device__ void operator()(int64_t k) const {
+    const int32_t s = old[k], b = S.slot_b[s], d = S.deg(s);
+    int32_t *dst = col + row[k];
+    for (int32_t j = 0; j < d; ++j) dst[j] = inv[S.nbr(s, j)];
+    if (d <= kSmallRow)
+      for (int32_t j = 1; j < d; ++j) {
+        const int32_t v = dst[j];
+        int32_t t = j;
+        for (; t > 0 && dst[t - 1] > v; --t) dst[t] = dst[t - 1];
+        dst[t] = v;
+      }
+    const int32_t x = S.members[s];
+    orig[k] = x;
+    reach[k] = x == head[b] ? (int32_t)(csize[comp[x]] - 1 - below[b]) : (int32_t)hang[x];
+  }
+};
+
+template <class BE>
+void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clock::time_point t0) {
+  // packed BCCs: >= 3 members, largest first, equal sizes by BCC id
+  std::vector<int64_t> mem_off((size_t)d.nbcc + 1);
+  be.download(mem_off.data(), d.mem_off, mem_off.size());
+  std::vector<int32_t> pk_bcc, pk_of((size_t)d.nbcc, -1);
+  for (int32_t b = 0; b < (int32_t)d.nbcc; ++b)
+    if (mem_off[b + 1] - mem_off[b] >= 3) pk_bcc.push_back(b);
+  std::stable_sort(pk_bcc.begin(), pk_bcc.end(), [&](int32_t a, int32_t b) {
+    return (mem_off[a + 1] - mem_off[a]) > (mem_off[b + 1] - mem_off[b]);
+  });
+  const int64_t np = (int64_t)pk_bcc.size();
+  D->vtx_off.assign((size_t)np + 1, 0);
+  for (int64_t i = 0; i < np; ++i) {
+    pk_of[pk_bcc[i]] = (int32_t)i;
+    D->vtx_off[i + 1] = D->vtx_off[i] + (mem_off[pk_bcc[i] + 1] - mem_off[pk_bcc[i]]);
+  }
+  const int64_t npk = D->vtx_off[np], ns = d.n_slots;
+  int32_t *slot_b = be.template alloc<int32_t>((size_t)ns), *pkof = be.template alloc<int32_t>((size_t)d.nbcc);
+  int64_t *vtx_off = be.template alloc<int64_t>((size_t)np + 1);
+  be.upload(pkof, pk_of.data(), pk_of.size());
+  be.upload(vtx_off, D->vtx_off.data(), D->vtx_off.size());
+  be.each(ns, SlotBcc{d.mem_off, d.nbcc, slot_b});
+  const Slots S{d.mem_off, d.sdeg, d.sadj, slot_b, pkof, d.members};
+
+  // roots and the BFS of every packed BCC at once
+  uint64_t *key = be.template alloc<uint64_t>((size_t)np);
+  int32_t *cyc = be.template alloc<int32_t>((size_t)np), *seen = be.template alloc<int32_t>((size_t)ns);
+  int32_t *claim = be.template alloc<int32_t>((size_t)ns), *bq = be.template alloc<int32_t>((size_t)npk);
+  int64_t *cnt = be.template alloc<int64_t>((size_t)npk + 1);
+  be.each(np, Fill64{(int64_t *)key, 0});
+  be.each(np, Fill32{cyc, 1});
+  be.each(ns, Fill32{seen, 0});
+  be.each(ns, Fill32{claim, INT32_MAX});
+  be.each(ns, RootKey{S, key, cyc});
+  be.each(ns, RootSlot{S, key, bq, seen});
+  int64_t f0 = 0, f1 = np;
+  while (f1 > f0) {
+    const int64_t fn = f1 - f0;
+    be.each(fn, PClaim{S, bq, seen, claim, f0});
+    be.each(fn, PCount{S, bq, seen, claim, cnt, f0});
+    be.each(1, Fill64{cnt + fn, 0});
+    const int64_t add = be.scan(cnt, fn + 1);
+    if (f1 + add > npk) throw StepError{BCGPU_EINVAL, "packing BFS: inconsistent frontier"};
+    be.each(fn, PEmit{S, seen, claim, cnt, bq, f0, f1});
+    be.each(add, PMark{bq, seen, f1});
+    f0 = f1;
+    f1 += add;
+  }
+  if (f1 != npk) throw StepError{BCGPU_EINVAL, "a BCC is not connected"};
+
+  // each BCC's queue: its subsequence of the level-major order
+  std::vector<int32_t> h_bq((size_t)npk), h_slot_b((size_t)ns), h_q((size_t)npk);
+  be.download(h_bq.data(), bq, (size_t)npk);
+  be.download(h_slot_b.data(), slot_b, (size_t)ns);
+  {
+    std::vector<int64_t> at(D->vtx_off.begin(), D->vtx_off.end() - 1);
+    for (int64_t k = 0; k < npk; ++k) h_q[at[pk_of[h_slot_b[h_bq[k]]]]++] = h_bq[k];
+  }
+  int32_t *q = bq;
+  be.upload(q, h_q.data(), (size_t)npk);
+
+  // plain vertices
+  int64_t *gidx = cnt;
+  be.each(npk, PlainFlag{S, q, cyc, gidx});
+  be.each(1, Fill64{gidx + npk, 0});
+  const int64_t nplain_all = be.scan(gidx, npk + 1);
+  std::vector<int64_t> h_gidx((size_t)npk + 1), plain_base((size_t)np);
+  be.download(h_gidx.data(), gidx, (size_t)npk + 1);
+  D->n_plain.assign((size_t)np, 0);
+  for (int64_t i = 0; i < np; ++i) {
+    plain_base[i] = h_gidx[D->vtx_off[i]];
+    D->n_plain[i] = (int32_t)(h_gidx[D->vtx_off[i + 1]] - plain_base[i]);
+  }
+  int64_t *pbase = be.template alloc<int64_t>((size_t)np);
+  be.upload(pbase, plain_base.data(), (size_t)np);
+  int32_t *nid = claim, *pl = be.template alloc<int32_t>((size_t)nplain_all), *old = seen;
+  be.each(ns, Fill32{nid, -1});
+  be.each(npk, Fill32{old, -1});
+  be.each(npk, PlainPlace{S, q, cyc, gidx, pbase, vtx_off, nid, pl, old});
+
+  // chains: count, prefix sums, write
+  int64_t *ccnt = be.template alloc<int64_t>((size_t)nplain_all + 1), *vcnt = be.template alloc<int64_t>((size_t)nplain_all + 1);
+  int32_t *bad = be.template alloc<int32_t>(1);
+  be.each(1, Fill32{bad, 0});
+  be.each(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, ccnt, vcnt, nullptr, nullptr, nullptr, nullptr,
+                             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr});
+  int32_t h_bad = 0;
+  be.download(&h_bad, bad, 1);
+  if (h_bad) throw StepError{BCGPU_EINVAL, "a chain has no end or returns to its start"};
+  be.each(1, Fill64{ccnt + nplain_all, 0});
+  be.each(1, Fill64{vcnt + nplain_all, 0});
+  const int64_t nchains = be.scan(ccnt, nplain_all + 1);
+  be.scan(vcnt, nplain_all + 1);
+  std::vector<int64_t> h_c((size_t)nplain_all + 1), h_v((size_t)nplain_all + 1), voff_base((size_t)np);
+  be.download(h_c.data(), ccnt, h_c.size());
+  be.download(h_v.data(), vcnt, h_v.size());
+  D->chain_off.assign((size_t)np + 1, 0);
+  for (int64_t i = 0; i < np; ++i) {
+    D->chain_off[i] = h_c[plain_base[i]];
+    voff_base[i] = h_v[plain_base[i]];
+  }
+  D->chain_off[np] = nchains;
+  int64_t *vbase = be.template alloc<int64_t>((size_t)np);
+  int32_t *nplain = be.template alloc<int32_t>((size_t)np);
+  be.upload(vbase, voff_base.data(), (size_t)np);
+  be.upload(nplain, D->n_plain.data(), (size_t)np);
+  int32_t *ch = be.template alloc<int32_t>((size_t)nchains * 4);
+  be.each(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, nullptr, nullptr, ccnt, vcnt, vbase, nplain, ch,
+                             ch + nchains, ch + 2 * nchains, ch + 3 * nchains, nid, old});
+  be.each(npk, Unset{old, bad});
+  be.download(&h_bad, bad, 1);
+  if (h_bad) throw StepError{BCGPU_EINVAL, "packing left a vertex without a place"};
+
+  // packed CSR in the new local ids, orig, reach
+  int32_t *inv = claim;  // nid is no longer needed
+  be.each(npk, Inverse{old, vtx_off, np, inv});
+  int64_t *row = be.template alloc<int64_t>((size_t)npk + 1);
+  be.each(npk, RowLen{S, old, row});
+  be.each(1, Fill64{row + npk, 0});
+  const int64_t parcs = be.scan(row, npk + 1);
+  if (parcs > (int64_t)INT32_MAX * 8) throw StepError{BCGPU_EOVERFLOW, "packed arcs overflow"};
+  int32_t *col = be.template alloc<int32_t>((size_t)parcs), *orig = be.template alloc<int32_t>((size_t)npk);
+  int32_t *reach = be.template alloc<int32_t>((size_t)npk);
+  be.each(npk, ColFill{S, old, inv, d.head, d.comp, row, d.csize, d.below, d.hang, col, orig, reach});
+
+  // to the host; rows longer than kSmallRow are sorted here
+  D->row.resize((size_t)npk + 1);
+  D->col.resize((size_t)parcs);
+  D->orig.resize((size_t)npk);
+  D->reach.resize((size_t)npk);
+  D->chain_start.resize((size_t)nchains);
+  D->chain_len.resize((size_t)nchains);
+  D->chain_l.resize((size_t)nchains);
+  D->chain_r.resize((size_t)nchains);
+  D->art.resize((size_t)d.n);
+  be.download(D->row.data(), row, (size_t)npk + 1);
+  be.download(D->col.data(), col, (size_t)parcs);
+  be.download(D->orig.data(), orig, (size_t)npk);
+  be.download(D->reach.data(), reach, (size_t)npk);
+  be.download(D->chain_start.data(), ch, (size_t)nchains);
+  be.download(D->chain_len.data(), ch + nchains, (size_t)nchains);
+  be.download(D->chain_l.data(), ch + 2 * nchains, (size_t)nchains);
+  be.download(D->chain_r.data(), ch + 3 * nchains, (size_t)nchains);
+  be.download(D->art.data(), d.art, (size_t)d.n);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t k = 0; k < npk; ++k)
+    if (D->row[k + 1] - D->row[k] > kSmallRow) std::sort(D->col.begin() + D->row[k], D->col.begin() + D->row[k + 1]);
+  std::vector<int32_t> h_cyc((size_t)np);
+  be.download(h_cyc.data(), cyc, (size_t)np);
+  int64_t cycles = 0;
+  for (int32_t c : h_cyc) cycles += c;
+  int32_t n_art = 0;
+  be.download(&n_art, d.n_art, 1);
+  decomp_finish(D, d.n, (int32_t)d.nroots, (int32_t)d.nbcc, n_art, cycles, t0);
 }
 
 }  // namespace decomp_steps
 
-int decomp_split_steps(const bc_graph *g, int device, SplitResult &S, char *err, size_t errlen) {
+int decomp_gpu(const bc_graph *g, int device, bc_decomp *D, std::chrono::steady_clock::time_point t0, char *err,
+               size_t errlen) {
   auto fail = [&](int code, const std::string &what) {
     if (err && errlen) std::snprintf(err, errlen, "%s", what.c_str());
     return code;
@@ -601,10 +1029,10 @@ int decomp_split_steps(const bc_graph *g, int device, SplitResult &S, char *err,
   try {
     if (device < 0) {
       decomp_steps::HostBackend be;
-      decomp_steps::run(be, g, S);
+      decomp_steps::pack_steps(be, decomp_steps::run_split(be, g), D, t0);
     } else {
       decomp_steps::DevBackend be(device);
-      decomp_steps::run(be, g, S);
+      decomp_steps::pack_steps(be, decomp_steps::run_split(be, g), D, t0);
     }
   } catch (const decomp_steps::StepError &e) {
     return fail(e.code, e.what);
@@ -621,18 +1049,7 @@ extern "C" int bc_decompose_gpu(const bc_graph *g, int device, bc_decomp **out, 
   const auto t0 = std::chrono::steady_clock::now();
   bc_decomp *D = new (std::nothrow) bc_decomp;
   if (!D) return BCGPU_ENOMEM;
-  int rc;
-  try {
-    bcg::SplitResult S;
-    rc = bcg::decomp_split_steps(g, device, S, err, errlen);
-    if (rc == BCGPU_OK) {
-      rc = bcg::decomp_pack(S, g->n, D, t0);
-      if (rc != BCGPU_OK && err && errlen) std::snprintf(err, errlen, "packing failed (status %d)", rc);
-    }
-  } catch (const std::bad_alloc &) {
-    rc = BCGPU_ENOMEM;
-    if (err && errlen) std::snprintf(err, errlen, "host allocation failed");
-  }
+  const int rc = bcg::decomp_gpu(g, device, D, t0, err, errlen);
   if (rc != BCGPU_OK) {
     delete D;
     return rc;

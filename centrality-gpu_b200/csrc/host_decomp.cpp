@@ -1027,6 +1027,16 @@ int decomp_pack(SplitResult &SR, int32_t n, bc_decomp *D, std::chrono::steady_cl
     D->chain_r.insert(D->chain_r.end(), ch_r[i].begin(), ch_r[i].end());
   }
 
+  int64_t cycles = 0;
+  for (auto c : n_cycle) cycles += c;
+  decomp_finish(D, n, (int32_t)comp_size.size(), nbcc, n_art, cycles, t0);
+  return BCGPU_OK;
+}
+
+void decomp_finish(bc_decomp *D, int32_t n, int32_t n_components, int32_t nbcc, int32_t n_art, int64_t n_cycle_bccs,
+                   std::chrono::steady_clock::time_point t0) {
+  const int32_t np_bcc = (int32_t)D->vtx_off.size() - 1;
+  const int64_t n_packed = D->vtx_off[np_bcc];
   bc_bccs &V = D->view;
   V.n_bcc = np_bcc;
   V.n_orig = n;
@@ -1047,17 +1057,15 @@ int decomp_pack(SplitResult &SR, int32_t n, bc_decomp *D, std::chrono::steady_cl
   V.art = D->art.data();
 
   bc_decomp_info &I = D->info;
-  I.n_components = (int32_t)comp_size.size();
+  I.n_components = n_components;
   I.n_bcc_all = nbcc;
   I.n_bcc_packed = np_bcc;
   I.n_articulation = n_art;
   I.n_chains = V.n_chains;
   I.n_chain_vertices = 0;
   for (auto l : D->chain_len) I.n_chain_vertices += l;
-  I.n_cycle_bccs = 0;
-  for (auto c : n_cycle) I.n_cycle_bccs += c;
+  I.n_cycle_bccs = n_cycle_bccs;
   I.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  return BCGPU_OK;
 }
 
 }  // namespace bcg

@@ -57,12 +57,13 @@ typedef struct bc_decomp_info {
  * to the smallest vertex of the component). The result depends only on g,
  * not on the host thread count. */
 int bc_decompose(const bc_graph *g, bc_decomp **out);
-/* bc_decompose with the BCC split and the arc-to-member pass run on GPU
- * `device` as data-parallel steps (the packing stays on the host); the result
- * is the same as bc_decompose's. device < 0 runs the same steps as host loops
- * instead: a check of the GPU steps on a machine without one, slower than
- * bc_decompose. Writes a message to err on failure (BCGPU_ECUDA without a
- * usable device). */
+/* bc_decompose as data-parallel steps on GPU `device`: the BCC split, the
+ * arc-to-member pass and the packing (BFS order, chains, packed CSR); prefix
+ * sums, the regrouping of the BFS order by BCC and the sort of rows longer
+ * than 32 arcs run on the host. The result is the same as bc_decompose's.
+ * device < 0 runs the same steps as host loops instead: a check of the GPU
+ * steps on a machine without one, slower than bc_decompose. Writes a message
+ * to err on failure (BCGPU_ECUDA without a usable device). */
 int bc_decompose_gpu(const bc_graph *g, int device, bc_decomp **out, char *err, size_t errlen);
 void bc_decomp_free(bc_decomp *d);
 /* Borrowed view, valid until bc_decomp_free. */

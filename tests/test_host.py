@@ -379,8 +379,9 @@ def _same_arrays(a, b):
 @pytest.mark.parametrize("family", ["random", "larger", "wide", "rmat16", "grid"])
 def test_gpu_decomposition_steps_on_host_equal_bc_decompose(family):
     """bc_decompose_gpu's data-parallel steps (union-find components, BFS
-    forest, level sweeps, union-find over tree edges, member slots), run as
-    host loops (device -1), give exactly bc_decompose's packed arrays."""
+    forest, level sweeps, union-find over tree edges, member slots, the
+    exact-order BFS of every BCC at once, chain numbering, packed CSR), run
+    as host loops (device -1), give exactly bc_decompose's packed arrays."""
     P = pkg()
     G = graphs()
     cases = {

@@ -1,6 +1,6 @@
-"""bc_decompose_gpu on the B200: the BCC split and the arc-to-member pass as
-GPU steps give exactly bc_decompose's packed arrays (the same steps run as
-host loops are checked on the CPU in test_host.py)."""
+"""bc_decompose_gpu on the B200: the decomposition as GPU steps (BCC split,
+chains, packing) gives exactly bc_decompose's packed arrays (the same steps
+run as host loops are checked on the CPU in test_host.py)."""
 import numpy as np
 import pytest
 
