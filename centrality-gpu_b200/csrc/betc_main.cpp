@@ -18,8 +18,9 @@
 static void usage() {
   std::fprintf(stderr,
                "usage: betc INPUT_FILE [--out FILE] [--mode plain|batched] [--delta fp64|fp32c]\n"
-               "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE]\n"
-               "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr\n");
+               "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE] [--gpu-decomp]\n"
+               "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr\n"
+               "  --gpu-decomp: run the BCC/chain decomposition on the GPU as well (same result)\n");
 }
 
 int main(int argc, char **argv) {
@@ -27,7 +28,7 @@ int main(int argc, char **argv) {
   const char *input = nullptr, *out_path = nullptr, *save_path = nullptr;
   bc_opts opts;
   bc_default_opts(&opts);
-  bool quiet = false;
+  bool quiet = false, gpu_decomp = false;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     auto next = [&]() -> const char * {
@@ -49,6 +50,7 @@ int main(int argc, char **argv) {
     else if (a == "--device") opts.device = std::atoi(next());
     else if (a == "--quiet") quiet = true;
     else if (a == "--save-csr") save_path = next();
+    else if (a == "--gpu-decomp") gpu_decomp = true;
     else if (a == "-h" || a == "--help") { usage(); return 0; }
     else if (!input) input = argv[i];
     else { usage(); return 1; }
@@ -66,8 +68,15 @@ int main(int argc, char **argv) {
     return 6;
   }
   bc_decomp *d = nullptr;
-  rc = bc_decompose(g, &d);
-  if (rc) { std::fprintf(stderr, "betc: decomposition failed (code %d)\n", rc); bc_graph_free(g); return 3; }
+  if (gpu_decomp) {
+    // on the --device GPU, else device 0
+    rc = bc_decompose_gpu(g, opts.device >= 0 ? opts.device : 0, &d, err, sizeof(err));
+    if (rc == BCGPU_ECUDA) { std::fprintf(stderr, "betc: %s\n", err); bc_graph_free(g); return 4; }
+    if (rc) { std::fprintf(stderr, "betc: GPU decomposition failed (code %d): %s\n", rc, err); bc_graph_free(g); return 3; }
+  } else {
+    rc = bc_decompose(g, &d);
+    if (rc) { std::fprintf(stderr, "betc: decomposition failed (code %d)\n", rc); bc_graph_free(g); return 3; }
+  }
   bc_decomp_info info;
   bc_decomp_get_info(d, &info);
   const bc_bccs *view = bc_decomp_view(d);

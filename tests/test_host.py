@@ -143,8 +143,13 @@ def test_betc_fails_loudly_without_gpu():
     P = pkg()
     r = subprocess.run([str(P.BETC_PATH), str(GOLDEN / "sample1.txt")], capture_output=True, text=True)
     assert r.returncode == 4 and "CUDA" in r.stderr
+    r = subprocess.run([str(P.BETC_PATH), str(GOLDEN / "sample1.txt"), "--gpu-decomp"], capture_output=True, text=True)
+    assert r.returncode == 4 and "CUDA" in r.stderr and not r.stdout
     with pytest.raises(P.BcError) as e:
         P.Context()
+    assert e.value.code == P.ECUDA
+    with pytest.raises(P.BcError) as e:
+        P.Decomposition(P.Graph.load(GOLDEN / "sample1.txt"), gpu_device=0)
     assert e.value.code == P.ECUDA
 
 

@@ -33,3 +33,20 @@ def test_gpu_decomposition_equals_host_at_scale(which):
         "ba64": lambda: G.pack_graphs(G.gen_ba_batch(64, seed=4))[:3],
     }[which]()
     assert _same(P.Graph.from_edges(n, u, v))
+
+
+@pytest.mark.gpu
+def test_betc_with_gpu_decomposition_matches_golden(tmp_path):
+    import json
+    import subprocess
+
+    P = pkg()
+    for name in ("sample4", "rand4", "small2000"):
+        out = tmp_path / f"{name}.out"
+        r = subprocess.run([str(P.BETC_PATH), str(GOLDEN / f"{name}.txt"), "--out", str(out), "--gpu-decomp"],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        vals = np.loadtxt(out, ndmin=2)
+        bc = np.array(json.loads((GOLDEN / f"{name}.bc.json").read_text())["bc"])
+        assert np.array_equal(vals[:, 0], np.arange(len(bc)))
+        assert np.max(np.abs(vals[:, 1] - bc) / np.maximum(1.0, np.abs(bc))) < 1e-6
