@@ -38,6 +38,7 @@
 #include <vector>
 
 #include <omp.h>
+#include <parallel/algorithm>
 
 
 namespace {
@@ -399,23 +400,40 @@ void for_chunks(int64_t k0, int64_t k1, F &&f) {
 }
 
 // Level-synchronous BFS that lists the vertices in exactly the order of the
-// sequential queue BFS from the same sources: the sources in the given order,
-// then level by level the undiscovered neighbours of each frontier vertex in
-// adjacency order, frontier vertices in their own order. On a wide level a
-// vertex is claimed by the earliest frontier position adjacent to it (atomic
-// min), the claims are counted per position and a prefix sum places each
-// position's vertices; a narrow level is one pass of the sequential queue.
+// sequential queue BFS from src: level by level, the undiscovered neighbours
+// of each frontier vertex in adjacency order, frontier vertices in their own
+// order. A narrow level is one pass of the sequential queue. A wide level is
+// expanded top-down -- a vertex is claimed by the earliest frontier position
+// adjacent to it (atomic min), the claims are counted per position and a
+// prefix sum places each position's vertices -- or, when the unvisited
+// vertices have fewer arcs than the frontier, bottom-up: every unvisited
+// vertex finds its earliest adjacent frontier position itself, and the new
+// level is sorted by (that position, key). That needs every adjacency list in
+// increasing key order, key(y) distinct per vertex.
 // adj(x, &ptr) returns the degree of x and points ptr at its neighbours.
 // Returns the visit order (the vertices reached).
-template <class Adj>
-std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
-  std::vector<int32_t> order((size_t)nv), claim;
-  std::vector<char> seen((size_t)nv, 0);
+template <class Adj, class Key>
+std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj, Key key) {
+  std::vector<int32_t> order((size_t)nv), claim, lev((size_t)nv, -1), pos((size_t)nv, 0);
   std::vector<int64_t> cnt;
+  const int nt = omp_get_max_threads();
+  std::vector<std::vector<std::pair<uint64_t, int32_t>>> found((size_t)nt);
+  std::vector<std::pair<uint64_t, int32_t>> all;
+  int64_t unvisited_arcs = 0;
+#pragma omp parallel for schedule(static) reduction(+ : unvisited_arcs)
+  for (int32_t x = 0; x < nv; ++x) {
+    const int32_t *a;
+    unvisited_arcs += adj(x, &a);
+  }
   order[0] = src;
-  seen[src] = 1;
-  int64_t f0 = 0, f1 = 1;
-  while (f1 > f0) {
+  lev[src] = 0;
+  int64_t f0 = 0, f1 = 1, frontier_arcs = 0;
+  {
+    const int32_t *a;
+    frontier_arcs = adj(src, &a);
+    unvisited_arcs -= frontier_arcs;
+  }
+  for (int32_t L = 0; f1 > f0; ++L) {
     const int64_t fn = f1 - f0;
     int64_t f2 = f1;
     if (fn < kParFrontier) {
@@ -423,11 +441,38 @@ std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
         const int32_t *a;
         const int32_t d = adj(order[i], &a);
         for (int32_t j = 0; j < d; ++j)
-          if (!seen[a[j]]) {
-            seen[a[j]] = 1;
+          if (lev[a[j]] < 0) {
+            lev[a[j]] = L + 1;
             order[f2++] = a[j];
           }
       }
+    } else if (unvisited_arcs < frontier_arcs) {
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < fn; ++i) pos[order[f0 + i]] = (int32_t)i;
+#pragma omp parallel
+      {
+        auto &mine = found[(size_t)omp_get_thread_num()];
+        mine.clear();
+#pragma omp for schedule(dynamic, 1024)
+        for (int32_t y = 0; y < nv; ++y) {
+          if (lev[y] >= 0) continue;
+          const int32_t *a;
+          const int32_t d = adj(y, &a);
+          int32_t m = INT32_MAX;
+          for (int32_t j = 0; j < d; ++j)
+            if (lev[a[j]] == L && pos[a[j]] < m) m = pos[a[j]];
+          if (m != INT32_MAX) mine.emplace_back(((uint64_t)(uint32_t)m << 32) | (uint64_t)(uint32_t)key(y), y);
+        }
+      }
+      all.clear();
+      for (auto &v : found) all.insert(all.end(), v.begin(), v.end());
+      __gnu_parallel::sort(all.begin(), all.end());
+#pragma omp parallel for schedule(static)
+      for (int64_t k = 0; k < (int64_t)all.size(); ++k) {
+        order[f1 + k] = all[k].second;
+        lev[all[k].second] = L + 1;
+      }
+      f2 = f1 + (int64_t)all.size();
     } else {
       if (claim.empty()) claim.assign((size_t)nv, INT32_MAX);
       int32_t *cl = claim.data();
@@ -436,7 +481,7 @@ std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
         const int32_t *a;
         const int32_t d = adj(order[f0 + i], &a);
         for (int32_t j = 0; j < d; ++j)
-          if (!seen[a[j]]) amin(&cl[a[j]], (int32_t)i);
+          if (lev[a[j]] < 0) amin(&cl[a[j]], (int32_t)i);
       }
       cnt.assign((size_t)fn + 1, 0);
 #pragma omp parallel for schedule(dynamic, 64)
@@ -444,7 +489,7 @@ std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
         const int32_t *a;
         const int32_t d = adj(order[f0 + i], &a);
         int64_t c = 0;
-        for (int32_t j = 0; j < d; ++j) c += !seen[a[j]] && ald(&cl[a[j]]) == (int32_t)i;
+        for (int32_t j = 0; j < d; ++j) c += lev[a[j]] < 0 && ald(&cl[a[j]]) == (int32_t)i;
         cnt[i + 1] = c;
       }
       for (int64_t i = 0; i < fn; ++i) cnt[i + 1] += cnt[i];
@@ -454,12 +499,19 @@ std::vector<int32_t> bfs_exact_order(int32_t nv, int32_t src, Adj adj) {
         const int32_t d = adj(order[f0 + i], &a);
         int64_t at = f1 + cnt[i];
         for (int32_t j = 0; j < d; ++j)
-          if (!seen[a[j]] && ald(&cl[a[j]]) == (int32_t)i) order[at++] = a[j];
+          if (lev[a[j]] < 0 && ald(&cl[a[j]]) == (int32_t)i) order[at++] = a[j];
       }
       f2 = f1 + cnt[fn];
 #pragma omp parallel for schedule(static)
-      for (int64_t k = f1; k < f2; ++k) seen[order[k]] = 1;
+      for (int64_t k = f1; k < f2; ++k) lev[order[k]] = L + 1;
     }
+    frontier_arcs = 0;
+#pragma omp parallel for schedule(static) reduction(+ : frontier_arcs) if (f2 - f1 >= kParFrontier)
+    for (int64_t k = f1; k < f2; ++k) {
+      const int32_t *a;
+      frontier_arcs += adj(order[k], &a);
+    }
+    unvisited_arcs -= frontier_arcs;
     f0 = f1;
     f1 = f2;
   }
@@ -877,7 +929,9 @@ int decomp_pack(SplitResult &SR, int32_t n, bc_decomp *D, std::chrono::steady_cl
     {
       std::vector<int32_t> q;
       if (par) {
-        q = bfs_exact_order(nb, root, [&](int32_t x, const int32_t **a) { *a = adj(x); return deg(x); });
+        // adjacency lists follow the CSR's arc order, i.e. increasing vertex id
+        q = bfs_exact_order(nb, root, [&](int32_t x, const int32_t **a) { *a = adj(x); return deg(x); },
+                            [&](int32_t x) { return vid[x]; });
       } else {
         std::vector<char> seen((size_t)nb, 0);
         q.reserve((size_t)nb);
