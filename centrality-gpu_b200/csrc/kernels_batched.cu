@@ -1305,27 +1305,30 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
     std::vector<int32_t> order;
     order.reserve((size_t)nb);
     {
-      std::vector<char> done((size_t)nb, 0);
-      std::vector<int32_t> stamp((size_t)nb, -1), q;
+      // mark[y]: the ball that queued y, or kTaken once y is in the order (a
+      // vertex queued by an earlier ball but not taken may join a later one)
+      constexpr int32_t kTaken = INT32_MAX;
+      std::vector<int32_t> mark((size_t)nb, -1), q;
       int32_t ball = 0;
       const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
       for (int32_t seed = 0; seed < nb; ++seed) {
-        if (done[seed]) continue;
+        if (mark[seed] == kTaken) continue;
         q.clear();
         q.push_back(seed);
-        stamp[seed] = ball;
+        mark[seed] = ball;
         int64_t got = 0, scanned = 0;
         for (size_t h = 0; h < q.size() && got < width; ++h) {
           const int32_t x = q[h];
-          done[x] = 1;
+          mark[x] = kTaken;
           order.push_back(x);
           ++got;
           if (scanned >= arc_budget) continue;  // keep draining the queue, stop growing it
           const int64_t e0 = B->row[vo + x], e1 = std::min(B->row[vo + x + 1], e0 + arc_budget - scanned);
           scanned += e1 - e0;
           for (int64_t e = e0; e < e1; ++e) {
+            if (e + 8 < e1) __builtin_prefetch(&mark[B->col[e + 8]]);
             const int32_t y = B->col[e];
-            if (stamp[y] != ball && !done[y]) { stamp[y] = ball; q.push_back(y); }
+            if (mark[y] != ball && mark[y] != kTaken) { mark[y] = ball; q.push_back(y); }
           }
         }
         ++ball;
