@@ -53,6 +53,7 @@
 #include <new>
 #include <numeric>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace bcg {
@@ -604,7 +605,6 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
     const int groups = (words + 3) / 4;
     const int wpad = groups * 4;  // rows are processed in whole 4-word groups
     const int64_t vo = a.vtx_off[bt.bcc];
-    const int32_t nb = (int32_t)(a.vtx_off[bt.bcc + 1] - vo);
     const int32_t n = a.n_plain[bt.bcc];  // core vertices
     const int64_t *HR = a.hrow + a.hvo[bt.bcc];
     const int64_t *HS = a.hsplit + a.hvo[bt.bcc];
@@ -1112,6 +1112,31 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
 
 // ================================================================= host ====
 
+// An allocator whose value-initialising construct leaves trivially
+// constructible elements uninitialised: table vectors that are resized and
+// then fully overwritten by parallel loops skip a sequential zero fill (and
+// their pages are first touched by the parallel writers).
+template <class T>
+struct NoInit : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInit<U>;
+  };
+  NoInit() = default;
+  template <class U>
+  NoInit(const NoInit<U> &) {}
+  template <class U>
+  void construct(U *p) noexcept {
+    ::new ((void *)p) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new ((void *)p) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using HostBuf = std::vector<T, NoInit<T>>;
+
 struct BatchedPlan {
   int width = 0;       // B
   int W = 0;           // words
@@ -1126,7 +1151,7 @@ struct BatchedPlan {
   Args args{};
   std::vector<int64_t> u_src, u_teps, u_bfs, u_aux, u_visits;
   std::vector<Batch> h_batches;
-  std::vector<Slot> h_slots;
+  HostBuf<Slot> h_slots;
   std::vector<int64_t> h_vtx_off;
   int64_t n_batches = 0;
 };
@@ -1175,10 +1200,10 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
 
   // ---- contracted rows, chain prefix sums, heavy chunks, passes
   std::vector<int64_t> hvo, hrow, hsplit, cpre_off;
-  std::vector<int32_t> hcol, hk, hcid;
+  HostBuf<int32_t> hcol, hk, hcid;  // every entry written by the row fill
   std::vector<double> cpre;
-  std::vector<Slot> slots;
-  std::vector<Seed> seeds;
+  HostBuf<Slot> slots;  // every entry written by the pass fill
+  HostBuf<Seed> seeds;
   std::vector<int2> arms;
   std::vector<int64_t> heavy_off{0}, hchunk_off{0}, hchunk_e0, hchunk_e1;
   std::vector<int32_t> heavy, hchunk_v, hfirst;
@@ -1486,7 +1511,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   cudaError_t e = cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(a.redo, 0, (size_t)std::max<int64_t>(P->n_batches, 1) * 4, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
-  P->h_slots = slots;
+  P->h_slots = std::move(slots);
   P->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
   if (e != cudaSuccess) return bail(BCGPU_ECUDA, std::string("batched upload: ") + cudaGetErrorString(e));
   a.reach = reach; a.vtx_off = vtx_off;

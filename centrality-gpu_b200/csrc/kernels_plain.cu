@@ -48,7 +48,7 @@ struct Shared {
   int imax;
   int item;
   int base_a, base_b;  // epochs of rows A and B
-  double red[kBlock / 32];
+  double red[kWarps];
   int wq[kBlock];
   int cq[kBlock];
 };
