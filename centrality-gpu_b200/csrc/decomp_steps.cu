@@ -40,6 +40,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -1038,6 +1039,8 @@ int decomp_gpu(const bc_graph *g, int device, bc_decomp *D, std::chrono::steady_
     return fail(e.code, e.what);
   } catch (const std::bad_alloc &) {
     return fail(BCGPU_ENOMEM, "host allocation failed");
+  } catch (const std::exception &e) {  // nothing else may cross the C ABI
+    return fail(BCGPU_EINVAL, std::string("decomposition steps: ") + e.what());
   }
   return BCGPU_OK;
 }

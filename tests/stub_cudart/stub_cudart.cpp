@@ -1,7 +1,8 @@
 // Test infrastructure only: a stand-in CUDA runtime for exercising libbcgpu's
 // HOST logic on a machine without a GPU. The library's own objects (built by
 // build.py) are linked against this file instead of cudart: "device" memory
-// is host memory, copies and memsets are memcpy/memset, kernel launches do
+// is host memory (filled with a byte pattern when allocated, as cudaMalloc's
+// memory is undefined), copies and memsets are memcpy/memset, kernel launches do
 // nothing but are counted, stream capture records the stream's copies and
 // memsets (and counts its launches) into a replayable list. Eight identical
 // fake sm_100 devices with 148 SMs (one per rank under torchrun); memory is
@@ -158,6 +159,7 @@ cudaError_t cudaMalloc(void **p, size_t bytes) {
   if (g_fail_after.load() > 0) --g_fail_after;
   *p = std::malloc(bytes ? bytes : 1);
   if (!*p) return cudaErrorMemoryAllocation;
+  std::memset(*p, 0xA5, bytes ? bytes : 1);  // device memory starts undefined: never zero here either
   ++g_live;
   return cudaSuccess;
 }

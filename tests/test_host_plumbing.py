@@ -593,3 +593,23 @@ def test_reference_betc_calls_are_accepted(stub_dir, tmp_path):
         art = real_pkg().Decomposition(real_pkg().Graph.from_edges(n, u, v)).arrays()["art"]
         assert [int(a) for a, _ in rows] == list(range(n))
         assert max(abs(g - a) / max(1.0, abs(a)) for g, a in zip(got, art)) < 1e-6, name
+
+
+def test_gpu_decomposition_fails_cleanly_when_its_kernels_do_not_run(stub_dir):
+    """bc_decompose_gpu on the stand-in runtime (kernels counted, not run):
+    its consistency checks turn the missing results into an error status,
+    and every device allocation of the failed call is released."""
+    res = run_stub(stub_dir, """
+L.stub_cudart_live_allocs.restype = C.c_longlong
+before = L.stub_cudart_live_allocs()
+n0 = L.stub_cudart_launches()
+for name in ('sample4', 'small2000'):
+    n, u, v, _, _ = load_case(name)
+    g = P.Graph.from_edges(n, u, v)
+    out[name] = raises(lambda: P.Decomposition(g, gpu_device=0))
+out['live'] = L.stub_cudart_live_allocs() - before
+out['launches'] = L.stub_cudart_launches() - n0
+""")
+    assert res["sample4"] and res["small2000"] and res["sample4"][0] == 1  # EINVAL
+    assert res["live"] == 0 and res["launches"] > 0
+
