@@ -399,3 +399,41 @@ def test_gpu_decomposition_steps_on_host_equal_bc_decompose(family):
     for n, u, v in cases:
         g = P.Graph.from_edges(n, u, v)
         assert _same_arrays(P.Decomposition(g).arrays(), P.Decomposition(g, gpu_device=-1).arrays())
+
+
+@pytest.mark.parametrize("which", ["rmat16", "grid"])
+def test_packed_plain_order_is_the_sequential_bfs(which):
+    """The largest BCC's plain vertices are numbered in the order of a plain
+    sequential queue BFS from its max-degree vertex (smallest vertex id among
+    equals), neighbours visited in increasing vertex id -- recomputed here in
+    Python, independently of the library's level-synchronous, top-down or
+    bottom-up BFS (RMAT-16: 850k vertices, wide levels; the grid: deep)."""
+    from collections import deque
+
+    G = graphs()
+    n, u, v = G.gen_rmat(16, 16, 0.2, 1, 8, seed=2) if which == "rmat16" else G.gen_grid(seed=3)
+    a = decompose(n, u, v).arrays()
+    v0, v1 = int(a["vtx_off"][0]), int(a["vtx_off"][1])
+    nb = v1 - v0
+    R = a["row"][v0:v1 + 1] - a["row"][v0]
+    C = a["col"][a["row"][v0]:a["row"][v1]]
+    o = a["orig"][v0:v1]
+    deg = np.diff(R)
+    rid = np.repeat(np.arange(nb), deg)
+    Cs = C[np.lexsort((o[C], rid))]  # each row by increasing original id
+    cands = np.flatnonzero(deg == deg.max())
+    root = int(cands[np.argmin(o[cands])])
+    seen = np.zeros(nb, bool)
+    seen[root] = True
+    q, order = deque([root]), []
+    Rl, Cl = R.tolist(), Cs.tolist()
+    while q:
+        x = q.popleft()
+        order.append(x)
+        for y in Cl[Rl[x]:Rl[x + 1]]:
+            if not seen[y]:
+                seen[y] = True
+                q.append(y)
+    order = np.array(order)
+    assert len(order) == nb and root == 0
+    assert np.array_equal(order[deg[order] != 2], np.arange(int(a["n_plain"][0])))
