@@ -437,3 +437,46 @@ def test_packed_plain_order_is_the_sequential_bfs(which):
     order = np.array(order)
     assert len(order) == nb and root == 0
     assert np.array_equal(order[deg[order] != 2], np.arange(int(a["n_plain"][0])))
+
+
+def _cactus(count, rng):
+    """count cycles of 3-30 vertices, most hung off a vertex of an earlier cycle."""
+    us, vs, base = [], [], 0
+    for c in range(count):
+        k = int(rng.integers(3, 31))
+        cyc = base + np.arange(k)
+        us.append(cyc)
+        vs.append(np.r_[cyc[1:], cyc[0]])
+        if c and c % 7:
+            us.append([int(rng.integers(0, base))])
+            vs.append([base + int(rng.integers(0, k))])
+        base += k
+    return (base,) + graphs().simple_edges(base, np.concatenate(us), np.concatenate(vs))
+
+
+@pytest.mark.parametrize("which", ["sparse", "ba", "cactus"])
+def test_bccs_and_articulations_match_networkx(which):
+    """BCC vertex sets (>= 3 vertices) and articulation points at sizes that
+    take the split's parallel paths, against networkx's independent
+    biconnected_components / articulation_points."""
+    import networkx as nx
+
+    G = graphs()
+    rng = np.random.default_rng(11)
+    if which == "sparse":  # random sparse core with chains and leaves: many bridges and cut vertices
+        n = 60000
+        u, v = G.simple_edges(n, rng.integers(0, n, int(1.3 * n)), rng.integers(0, n, int(1.3 * n)))
+        n, u, v = G.subdivide(n, u, v, 0.2, 1, 4, rng)
+        n, u, v = G.attach_leaves(n, u, v, 3000, n, rng)
+    elif which == "ba":
+        n, u, v = G.pack_graphs(G.gen_ba_batch(64, 50, 2000, seed=5))[:3]
+    else:
+        n, u, v = _cactus(3000, rng)
+    a = decompose(n, u, v).arrays()
+    g = nx.Graph()
+    g.add_nodes_from(range(n))
+    g.add_edges_from(zip(u.tolist(), v.tolist()))
+    theirs = {frozenset(c) for c in nx.biconnected_components(g) if len(c) >= 3}
+    vo, orig = a["vtx_off"], a["orig"]
+    assert {frozenset(orig[vo[b]:vo[b + 1]].tolist()) for b in range(a["n_bcc"])} == theirs
+    assert set(np.flatnonzero(a["art"] > 0).tolist()) == set(nx.articulation_points(g))
