@@ -480,3 +480,38 @@ def test_bccs_and_articulations_match_networkx(which):
     vo, orig = a["vtx_off"], a["orig"]
     assert {frozenset(orig[vo[b]:vo[b + 1]].tolist()) for b in range(a["n_bcc"])} == theirs
     assert set(np.flatnonzero(a["art"] > 0).tolist()) == set(nx.articulation_points(g))
+
+
+def test_reach_matches_components_of_g_minus_x():
+    """Reach at scale, independently: for sampled members x of the largest
+    BCC b of a sparse graph with chains and leaves, reach_b(x) = the number of
+    vertices in the components of G - x next to x that hold no other vertex
+    of b (scipy's connected components of G without x)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    G = graphs()
+    rng = np.random.default_rng(12)
+    n = 40000
+    u, v = G.simple_edges(n, rng.integers(0, n, int(1.3 * n)), rng.integers(0, n, int(1.3 * n)))
+    n, u, v = G.subdivide(n, u, v, 0.2, 1, 4, rng)
+    n, u, v = G.attach_leaves(n, u, v, 3000, n, rng)
+    a = decompose(n, u, v).arrays()
+    v0, v1 = int(a["vtx_off"][0]), int(a["vtx_off"][1])
+    members, reach = a["orig"][v0:v1], a["reach"][v0:v1]
+    A = csr_matrix((np.ones(2 * len(u)), (np.r_[u, v], np.r_[v, u])), shape=(n, n))
+    cut = np.flatnonzero(a["art"][members] > 0)
+    picks = np.r_[rng.choice(cut, 24, replace=False), rng.choice(np.flatnonzero(a["art"][members] == 0), 6)]
+    for k in picks:
+        x = int(members[k])
+        keep = np.ones(n, bool)
+        keep[x] = False
+        idx = np.flatnonzero(keep)
+        _, lab = connected_components(A[idx][:, idx], directed=False)
+        full = np.full(n, -1)
+        full[idx] = lab
+        sizes = np.bincount(lab)
+        near = set(full[A.indices[A.indptr[x]:A.indptr[x + 1]]].tolist())
+        in_b = set(full[members[members != x]].tolist())
+        assert reach[k] == sum(int(sizes[c]) for c in near - in_b), x
+    assert np.all(reach[cut] > 0)
