@@ -483,10 +483,12 @@ def test_bccs_and_articulations_match_networkx(which):
 
 
 def test_reach_matches_components_of_g_minus_x():
-    """Reach at scale, independently: for sampled members x of the largest
-    BCC b of a sparse graph with chains and leaves, reach_b(x) = the number of
-    vertices in the components of G - x next to x that hold no other vertex
-    of b (scipy's connected components of G without x)."""
+    """Reach and articulation terms at scale, independently: for sampled
+    members x of the largest BCC b of a sparse graph with chains and leaves,
+    reach_b(x) = the number of vertices in the components of G - x next to x
+    that hold no other vertex of b, and art(x) = S^2 - sum(part^2) over those
+    components (S their total) -- scipy's connected components of G
+    without x."""
     from scipy.sparse import csr_matrix
     from scipy.sparse.csgraph import connected_components
 
@@ -514,4 +516,6 @@ def test_reach_matches_components_of_g_minus_x():
         near = set(full[A.indices[A.indptr[x]:A.indptr[x + 1]]].tolist())
         in_b = set(full[members[members != x]].tolist())
         assert reach[k] == sum(int(sizes[c]) for c in near - in_b), x
+        parts = [int(sizes[c]) for c in near]  # the component of x, less x, in pieces
+        assert a["art"][x] == sum(parts) ** 2 - sum(p * p for p in parts), x
     assert np.all(reach[cut] > 0)
