@@ -412,11 +412,14 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     p->ws_n = (p->mode == BCGPU_MODE_PLAIN ? nb_max : nb_plain) + 2;
     const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
     // Four 256-thread CTAs per SM (four sources in flight) when their rows
-    // fit the budget, else two of 512, else one of 1024 per SM.
+    // fit the budget, else two of 512, else one of 1024 per SM; with
+    // plain_ctas_per_sm 8 or 16, CTAs of 128 or 64 threads are tried first.
     int64_t avail = limit - p->device_bytes - 64 * (int64_t)ctx->sms;
     if (avail < 2 * per_slot) return bail(fail(ctx, BCGPU_ENOMEM, "workspace for the largest BCC exceeds the limit"));
     int grid = 0;
-    for (int block : {256, 512, 1024}) {
+    const int first = ctx->opts.plain_ctas_per_sm > 4 ? 1024 / ctx->opts.plain_ctas_per_sm : 256;
+    for (int block : {64, 128, 256, 512, 1024}) {
+      if (block < first) continue;
       const int want = ctx->sms * (1024 / block);
       grid = (int)std::min<int64_t>(want, avail / per_slot - 1);
       p->block = block;
@@ -495,6 +498,8 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
   if (o.delta != BCGPU_DELTA_FP64 && o.delta != BCGPU_DELTA_FP32C) return fail(nullptr, BCGPU_EINVAL, "bad delta");
   if (o.batch_width < 0 || o.batch_width > 1024 || (o.batch_width % 32) != 0)
     return fail(nullptr, BCGPU_EINVAL, "batch_width must be a multiple of 32 in [0, 1024]");
+  if (o.plain_ctas_per_sm != 0 && o.plain_ctas_per_sm != 4 && o.plain_ctas_per_sm != 8 && o.plain_ctas_per_sm != 16)
+    return fail(nullptr, BCGPU_EINVAL, "plain_ctas_per_sm must be 0, 4, 8 or 16");
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0)

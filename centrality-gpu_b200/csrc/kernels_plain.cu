@@ -488,6 +488,8 @@ __global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bc
 
 cudaError_t launch_plain(const PlainArgs &a, int block, int grid, cudaStream_t stream) {
   switch (block) {
+    case 64: plain_kernel<64><<<grid, 64, 0, stream>>>(a); break;
+    case 128: plain_kernel<128><<<grid, 128, 0, stream>>>(a); break;
     case 256: plain_kernel<256><<<grid, 256, 0, stream>>>(a); break;
     case 512: plain_kernel<512><<<grid, 512, 0, stream>>>(a); break;
     case 1024: plain_kernel<1024><<<grid, 1024, 0, stream>>>(a); break;

@@ -62,6 +62,11 @@ typedef struct bc_opts {
                             capture on bc_plan_record or on the range's first run; 0 = enqueue
                             the work directly on every run. The stream must be capturable
                             (not the legacy NULL stream). */
+  int32_t plain_ctas_per_sm; /* per-source schedule: CTAs (sources in flight) per SM; 0 = four
+                            256-thread CTAs, fewer and larger when their rows do not fit the
+                            workspace budget; 8 or 16 = that many CTAs of 128 or 64 threads
+                            (more sources in flight for deep, narrow BCCs), with the same
+                            fallback; other values are rejected */
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;

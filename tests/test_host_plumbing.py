@@ -85,7 +85,8 @@ graphs_ = [("small2000", G.gen_small(1)),
            ("grid30", G.gen_grid(30, leaves=100, seed=3)),
            ("ba12", G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3])]
 graphs_ += [(c, load_case(c)[:3]) for c in GOLDEN_CASES]
-modes = [dict(mode=P.MODE_PLAIN), dict(mode=P.MODE_BATCHED), dict(mode=P.MODE_BATCHED, plain_core=500),
+modes = [dict(mode=P.MODE_PLAIN), dict(mode=P.MODE_PLAIN, plain_ctas_per_sm=16), dict(mode=P.MODE_BATCHED),
+         dict(mode=P.MODE_BATCHED, plain_core=500, plain_ctas_per_sm=8),
          dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=32),
          dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=128),
          dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=1024)]
@@ -612,4 +613,23 @@ out['launches'] = L.stub_cudart_launches() - n0
 """)
     assert res["sample4"] and res["small2000"] and res["sample4"][0] == 1  # EINVAL
     assert res["live"] == 0 and res["launches"] > 0
+
+
+def test_plain_ctas_per_sm_sets_the_sources_in_flight(stub_dir):
+    """bc_opts.plain_ctas_per_sm: the per-source schedule runs that many CTAs
+    per SM (the stand-in device has 148 SMs) while their rows fit, 0 means
+    four; other values are rejected at bc_create."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_small(1)
+d = decomp(n, u, v)
+for k in (0, 4, 8, 16):
+    ctx = P.Context(mode=P.MODE_PLAIN, plain_ctas_per_sm=k)
+    plan = ctx.plan(d)
+    out[str(k)] = plan.concurrency
+    plan.close()
+    ctx.close()
+out['bad'] = [raises(lambda: P.Context(mode=P.MODE_PLAIN, plain_ctas_per_sm=k)) for k in (-1, 2, 3, 32)]
+""")
+    assert [res[k] for k in ("0", "4", "8", "16")] == [148 * 4, 148 * 4, 148 * 8, 148 * 16]
+    assert all(b and b[0] == 1 for b in res["bad"])
 
