@@ -517,10 +517,11 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.each(n, Fill32{par, -2});
   be.each(n, RootScatter{uf, flag, roots, comp, order, par});
 
-  // BFS forest, one launch per level
+  // BFS forest, one launch per level; tail (the end of the listed vertices)
+  // carries over from level to level, so each level costs one read-back
   std::vector<int64_t> lvl{0, nroots};
+  be.upload(tail, &nroots, 1);
   for (int64_t f0 = 0, f1 = nroots; f1 > f0;) {
-    be.upload(tail, &f1, 1);
     be.each(f1 - f0, BfsLevel{R, C, order, par, tail, f0});
     int64_t f2 = 0;
     be.download(&f2, tail, 1);
