@@ -904,8 +904,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
     const int64_t fn = f1 - f0;
     be.each(fn, PClaim{S, bq, seen, claim, f0});
     be.each(fn, PCount{S, bq, seen, claim, cnt, f0});
-    be.each(1, Fill64{cnt + fn, 0});
-    const int64_t add = be.scan(cnt, fn + 1);
+    const int64_t add = be.scan(cnt, fn);  // PEmit reads the starts of positions 0..fn-1 only
     if (f1 + add > npk) throw StepError{BCGPU_EINVAL, "packing BFS: inconsistent frontier"};
     be.each(fn, PEmit{S, seen, claim, cnt, bq, f0, f1});
     be.each(add, PMark{bq, seen, f1});
