@@ -285,6 +285,9 @@ def main():
     ap.add_argument("--plain-ctas", type=int, choices=[0, 4, 8, 16], default=0,
                     help="per-source schedule (and BCCs routed to it): CTAs per SM (bc_opts.plain_ctas_per_sm; "
                          "0 = the library's choice, four of 256 threads)")
+    ap.add_argument("--lazy-tables", action="store_true",
+                    help="e2e steps build the multi-source tables of the passes they run only "
+                         "(bc_opts.lazy_tables)")
     ap.add_argument("--gpu-decomp", action="store_true",
                     help="also time the decomposition on the GPU (bc_decompose_gpu, outside the timed region) "
                          "against the host one, and check that both give the same arrays")
@@ -355,7 +358,7 @@ def main():
             width = int(wt.item())
     ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30), graph=bool(args.graph),
-                    plain_ctas_per_sm=args.plain_ctas)
+                    plain_ctas_per_sm=args.plain_ctas, lazy_tables=args.lazy_tables)
     plan = ctx.plan(d)
     # steps of this many sources, small enough that every rank gets at least one
     total_sources = plan.unit_work(0, plan.n_units)[0]
@@ -496,7 +499,7 @@ def main():
                        "host_decomposition_s": round(host_s, 3), "generator_s": round(gen_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
                        "batch_width": st.get("batch_width"), "autotune_gteps": tuned,
                        "cuda_graph": bool(args.graph), "gpu_decomposition": decomp,
-                       "plain_ctas_per_sm": args.plain_ctas or None,
+                       "plain_ctas_per_sm": args.plain_ctas or None, "lazy_tables": bool(args.lazy_tables),
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "plain": plain,

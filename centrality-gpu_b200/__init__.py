@@ -43,7 +43,8 @@ _f32p = C.POINTER(C.c_float)
 class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
                 ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
-                ("plain_core", C.c_int32), ("graph", C.c_int32), ("plain_ctas_per_sm", C.c_int32)]
+                ("plain_core", C.c_int32), ("graph", C.c_int32), ("plain_ctas_per_sm", C.c_int32),
+                ("lazy_tables", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -259,7 +260,8 @@ class Context:
     _live = weakref.WeakSet()
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
-                 workspace_limit=0, rescale_exp=0, plain_core=0, graph=False, plain_ctas_per_sm=0):
+                 workspace_limit=0, rescale_exp=0, plain_core=0, graph=False, plain_ctas_per_sm=0,
+                 lazy_tables=False):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
@@ -269,6 +271,7 @@ class Context:
         o.plain_core = plain_core
         o.graph = 1 if graph else 0
         o.plain_ctas_per_sm = plain_ctas_per_sm
+        o.lazy_tables = 1 if lazy_tables else 0
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:

@@ -1,6 +1,7 @@
 // Host-visible interface of the BATCHED schedule (kernels_batched.cu).
 #pragma once
 #include <cstdint>
+#include <climits>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -17,6 +18,9 @@ struct BatchedConfig {
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
   const std::vector<char> *bccs_on = nullptr;  // BCCs this plan schedules (null: all)
   const std::vector<int32_t> *ecc0 = nullptr;  // per BCC: eccentricity of local vertex 0 if known (< 0: compute)
+  // Passes (global index) whose slot, seed and arming tables are built; the
+  // others keep their sizes and offsets but no sources, and must not be run.
+  int64_t fill_begin = 0, fill_end = INT64_MAX;
 };
 
 struct BatchedPlan;
@@ -29,6 +33,9 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
                    BatchedPlan **out, std::string *msg);
 void batched_destroy(BatchedPlan *p);
 int64_t batched_device_bytes(const BatchedPlan *p);
+// Digest of what pass `pass` runs from: its descriptor (less the table
+// offsets), its slots, seeds and arming list (tests compare builds with it).
+uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass);
 // Bytes batched_create copied host -> device; bytes batched_failed_batches reads back.
 int64_t batched_h2d_bytes(const BatchedPlan *p);
 int64_t batched_status_bytes(const BatchedPlan *p);

@@ -296,7 +296,10 @@ void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items, const std
 }
 
 // Fills plan p (allocated by create_plan, which releases it on any failure).
-int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan *p) {
+// fill_begin/fill_end: the multi-source passes (units) whose tables are built
+// (a one-shot call that runs only those); default all.
+int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan *p,
+               int64_t fill_begin = 0, int64_t fill_end = INT64_MAX) {
   int rc = BCGPU_OK;
   auto bail = [](int code) { return code; };
   p->n_orig = B->n_orig;
@@ -373,6 +376,8 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     cfg.rescale_exp = ctx->opts.rescale_exp;
     cfg.bccs_on = &on;
     cfg.ecc0 = &ecc0;
+    cfg.fill_begin = fill_begin;
+    cfg.fill_end = fill_end;
     std::string msg;
     rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
@@ -443,7 +448,8 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
 // Validates the input and builds a plan; on any failure -- a status code, or
 // a host allocation that throws -- the partial plan and its device buffers are
 // released and no C++ exception leaves the library.
-int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan **out) {
+int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> *override_items, bc_plan **out,
+                int64_t fill_begin = 0, int64_t fill_end = INT64_MAX) {
   bc_plan *p = nullptr;
   int rc;
   try {
@@ -454,7 +460,7 @@ int create_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem>
       p = new bc_plan;
       p->ctx = ctx;
       p->mode = ctx->opts.mode;
-      rc = build_plan(ctx, B, override_items, p);
+      rc = build_plan(ctx, B, override_items, p, fill_begin, fill_end);
       if (rc == BCGPU_OK) ctx->plans.insert(p);
     }
   } catch (const std::bad_alloc &) {
@@ -500,6 +506,7 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
     return fail(nullptr, BCGPU_EINVAL, "batch_width must be a multiple of 32 in [0, 1024]");
   if (o.plain_ctas_per_sm != 0 && o.plain_ctas_per_sm != 4 && o.plain_ctas_per_sm != 8 && o.plain_ctas_per_sm != 16)
     return fail(nullptr, BCGPU_EINVAL, "plain_ctas_per_sm must be 0, 4, 8 or 16");
+  if (o.lazy_tables != 0 && o.lazy_tables != 1) return fail(nullptr, BCGPU_EINVAL, "lazy_tables must be 0 or 1");
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0)
@@ -829,7 +836,9 @@ int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool
   CK(ctx, cudaEventCreate(&t1));
   CK(ctx, cudaEventRecord(t0, ctx->stream));
   bc_plan *p = nullptr;
-  int rc = create_plan(ctx, bccs, nullptr, &p);
+  // with lazy_tables, only the passes this call runs get their tables built
+  const bool lazy = ctx->opts.lazy_tables && !all;
+  int rc = create_plan(ctx, bccs, nullptr, &p, lazy ? begin : 0, lazy ? end : INT64_MAX);
   bc_stats st{};
   if (!rc && all) { begin = 0; end = bc_plan_num_units(p); }
   if (!rc) rc = bc_plan_run(p, begin, end, &st);

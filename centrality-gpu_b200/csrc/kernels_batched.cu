@@ -1152,6 +1152,8 @@ struct BatchedPlan {
   std::vector<int64_t> u_src, u_teps, u_bfs, u_aux, u_visits;
   std::vector<Batch> h_batches;
   HostBuf<Slot> h_slots;
+  HostBuf<Seed> h_seeds;
+  std::vector<int2> h_arms;
   std::vector<int64_t> h_vtx_off;
   int64_t n_batches = 0;
 };
@@ -1327,16 +1329,23 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
     // levels: few active levels per vertex, dense 32-slot hits. A ball grows
     // only through vertices not yet taken, so each vertex's arcs are scanned
     // once and late balls cost no rescans of finished regions.
+    // Only passes [jf0, jf1) of this BCC are filled (cfg.fill_begin/end); the
+    // source order is then needed up to pass jf1 only, and the greedy below
+    // produces it as a prefix.
+    const int64_t bat0g = (int64_t)P->h_batches.size(), nbat = ((int64_t)nb + width - 1) / width;
+    const int64_t jf0 = std::min(nbat, std::max<int64_t>(0, cfg.fill_begin - bat0g));
+    const int64_t jf1 = std::max(jf0, std::min(nbat, cfg.fill_end - bat0g));
+    const size_t need = (size_t)std::min<int64_t>(nb, jf1 * (int64_t)width);
     std::vector<int32_t> order;
-    order.reserve((size_t)nb);
-    {
+    order.reserve(need);
+    if (need > 0) {
       // mark[y]: the ball that queued y, or kTaken once y is in the order (a
       // vertex queued by an earlier ball but not taken may join a later one)
       constexpr int32_t kTaken = INT32_MAX;
       std::vector<int32_t> mark((size_t)nb, -1), q;
       int32_t ball = 0;
       const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
-      for (int32_t seed = 0; seed < nb; ++seed) {
+      for (int32_t seed = 0; seed < nb && order.size() < need; ++seed) {
         if (mark[seed] == kTaken) continue;
         q.clear();
         q.push_back(seed);
@@ -1363,11 +1372,10 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
     // sized up front (a chain source has two seeds), then every pass fills
     // its own ranges in parallel; the arming lists (variable length after
     // deduplication) are built per pass and concatenated in pass order.
-    const int64_t nbat = ((int64_t)order.size() + width - 1) / width;
     const size_t bat0 = P->h_batches.size(), slot0 = slots.size(), seed0 = seeds.size();
     std::vector<int64_t> seed_at((size_t)nbat + 1, 0);
 #pragma omp parallel for schedule(static)
-    for (int64_t j = 0; j < nbat; ++j) {
+    for (int64_t j = jf0; j < jf1; ++j) {
       const size_t i0 = (size_t)j * width, i1 = std::min(order.size(), i0 + (size_t)width);
       int64_t cnt = 0;
       for (size_t i = i0; i < i1; ++i) cnt += order[i] >= npl ? 2 : 0;
@@ -1375,12 +1383,13 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
     }
     for (int64_t j = 0; j < nbat; ++j) seed_at[j + 1] += seed_at[j];
     P->h_batches.resize(bat0 + (size_t)nbat);
-    slots.resize(slot0 + order.size());
+    slots.resize(slot0 + (size_t)nb);
     seeds.resize(seed0 + (size_t)seed_at[nbat]);
     std::vector<std::vector<int2>> arm_of((size_t)nbat);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t j = 0; j < nbat; ++j) {
-      const size_t i0 = (size_t)j * width, i1 = std::min(order.size(), i0 + (size_t)width);
+      const size_t i0 = (size_t)j * width, i1 = std::min((size_t)nb, i0 + (size_t)width);
+      const bool fill = j >= jf0 && j < jf1;
       Batch bt{};
       bt.bcc = b;
       bt.nslots = (int32_t)(i1 - i0);
@@ -1391,8 +1400,8 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
       bt.seed_off = (int64_t)seed0 + seed_at[j];
       int64_t sd = bt.seed_off;
       std::vector<int2> &arm = arm_of[j];
-      arm.reserve((size_t)bt.nslots * 2);
-      for (size_t i = i0; i < i1; ++i) {
+      if (fill) arm.reserve((size_t)bt.nslots * 2);
+      for (size_t i = i0; fill && i < i1; ++i) {
         const int32_t s = order[i];
         const int32_t slot = (int32_t)(i - i0);
         if (s < npl) {
@@ -1512,6 +1521,8 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   if (e == cudaSuccess) e = cudaMemsetAsync(a.redo, 0, (size_t)std::max<int64_t>(P->n_batches, 1) * 4, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
   P->h_slots = std::move(slots);
+  P->h_seeds = std::move(seeds);
+  P->h_arms = std::move(arms);
   P->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
   if (e != cudaSuccess) return bail(BCGPU_ECUDA, std::string("batched upload: ") + cudaGetErrorString(e));
   a.reach = reach; a.vtx_off = vtx_off;
@@ -1568,6 +1579,22 @@ void batched_destroy(BatchedPlan *p) {
 }
 
 int64_t batched_device_bytes(const BatchedPlan *p) { return p ? p->bytes : 0; }
+
+uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass) {
+  if (!p || pass < 0 || pass >= (int64_t)p->h_batches.size()) return 0;
+  const Batch &b = p->h_batches[(size_t)pass];
+  uint64_t h = 1469598103934665603ull;  // FNV-1a
+  auto mix = [&h](const void *q, size_t n) {
+    const unsigned char *c = (const unsigned char *)q;
+    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+  };
+  const int32_t head[8] = {b.bcc, b.nslots, b.words, b.nseeds, b.max_seed, b.kmax, b.heavy_deg, b.narm};
+  mix(head, sizeof head);
+  mix(p->h_slots.data() + b.slot_off, sizeof(Slot) * (size_t)b.nslots);
+  mix(p->h_seeds.data() + b.seed_off, sizeof(Seed) * (size_t)b.nseeds);
+  mix(p->h_arms.data() + b.arm_off, sizeof(int2) * (size_t)b.narm);
+  return h;
+}
 int64_t batched_h2d_bytes(const BatchedPlan *p) { return p ? p->h2d : 0; }
 int64_t batched_status_bytes(const BatchedPlan *p) {
   return p ? (int64_t)sizeof(int) * std::max<int64_t>(p->n_batches, 1) : 0;

@@ -67,6 +67,9 @@ typedef struct bc_opts {
                             workspace budget; 8 or 16 = that many CTAs of 128 or 64 threads
                             (more sources in flight for deep, narrow BCCs), with the same
                             fallback; other values are rejected */
+  int32_t lazy_tables;   /* 1: a one-shot bc_run_bccs_units call builds the multi-source slot,
+                            seed and arming tables of the passes it runs only (and the source
+                            order up to the last of them); 0 = of every pass */
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;

@@ -633,3 +633,29 @@ out['bad'] = [raises(lambda: P.Context(mode=P.MODE_PLAIN, plain_ctas_per_sm=k)) 
     assert [res[k] for k in ("0", "4", "8", "16")] == [148 * 4, 148 * 4, 148 * 8, 148 * 16]
     assert all(b and b[0] == 1 for b in res["bad"])
 
+
+def test_lazy_tables_build_exactly_the_requested_passes(stub_dir, tmp_path):
+    """bc_opts.lazy_tables restricts a plan's multi-source tables to a pass
+    range (BatchedConfig::fill_begin/fill_end): every pass in the range runs
+    from exactly the slots, seeds and arming list of the full build, and the
+    unit accounting is unchanged (tests/stub_cudart/fill_range_check.cpp,
+    linked against the stand-in runtime's library)."""
+    exe = tmp_path / "fill_range_check"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", str(ROOT / "include"), "-I", str(PKG / "csrc"),
+                    "-I/usr/local/cuda/include", str(STUB / "fill_range_check.cpp"), "-o", str(exe),
+                    "-L", str(stub_dir), "-lbcgpu", "-Wl,-rpath," + str(stub_dir)], check=True)
+    from helpers import graphs
+    G = graphs()
+    cases = {"rmat14": G.gen_rmat(14, 16, 0.2, 1, 8, seed=2), "grid30": G.gen_grid(30, leaves=100, seed=3),
+             "ba12": G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]}
+    ranges = ["0", "1", "3", "7", "-2", "-1", "5", "5", "-3", "1000000000", "0", "1000000000"]
+    for name, (n, u, v) in cases.items():
+        path = tmp_path / f"{name}.txt"
+        G.write_edge_list(path, n, u, v)
+        for width in ("64", "128"):
+            r = subprocess.run([str(exe), str(path), width] + ranges, capture_output=True, text=True, timeout=300)
+            assert r.returncode == 0, r.stdout + r.stderr
+            lines = [ln.split() for ln in r.stdout.splitlines() if ln.startswith("range")]
+            assert len(lines) == len(ranges) // 2 and all(ln[3] == "ok" for ln in lines), (name, width, r.stdout)
+            assert int(r.stdout.split()[1]) > 8  # several passes, so the ranges cut the order
+
