@@ -21,6 +21,7 @@ struct BatchedConfig {
   // Passes (global index) whose slot, seed and arming tables are built; the
   // others keep their sizes and offsets but no sources, and must not be run.
   int64_t fill_begin = 0, fill_end = INT64_MAX;
+  bool keep_host_tables = false;  // keep host copies of seeds and arming lists (batched_pass_digest)
 };
 
 struct BatchedPlan;
@@ -34,7 +35,8 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
 void batched_destroy(BatchedPlan *p);
 int64_t batched_device_bytes(const BatchedPlan *p);
 // Digest of what pass `pass` runs from: its descriptor (less the table
-// offsets), its slots, seeds and arming list (tests compare builds with it).
+// offsets), its slots, seeds and arming list (tests compare builds with it;
+// the plan must have been built with keep_host_tables).
 uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass);
 // Bytes batched_create copied host -> device; bytes batched_failed_batches reads back.
 int64_t batched_h2d_bytes(const BatchedPlan *p);

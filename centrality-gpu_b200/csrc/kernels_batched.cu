@@ -1521,8 +1521,10 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   if (e == cudaSuccess) e = cudaMemsetAsync(a.redo, 0, (size_t)std::max<int64_t>(P->n_batches, 1) * 4, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
   P->h_slots = std::move(slots);
-  P->h_seeds = std::move(seeds);
-  P->h_arms = std::move(arms);
+  if (cfg.keep_host_tables) {
+    P->h_seeds = std::move(seeds);
+    P->h_arms = std::move(arms);
+  }
   P->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
   if (e != cudaSuccess) return bail(BCGPU_ECUDA, std::string("batched upload: ") + cudaGetErrorString(e));
   a.reach = reach; a.vtx_off = vtx_off;
@@ -1583,6 +1585,7 @@ int64_t batched_device_bytes(const BatchedPlan *p) { return p ? p->bytes : 0; }
 uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass) {
   if (!p || pass < 0 || pass >= (int64_t)p->h_batches.size()) return 0;
   const Batch &b = p->h_batches[(size_t)pass];
+  if ((int64_t)p->h_seeds.size() < b.seed_off + b.nseeds || (int64_t)p->h_arms.size() < b.arm_off + b.narm) return 0;
   uint64_t h = 1469598103934665603ull;  // FNV-1a
   auto mix = [&h](const void *q, size_t n) {
     const unsigned char *c = (const unsigned char *)q;

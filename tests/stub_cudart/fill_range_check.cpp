@@ -20,6 +20,7 @@ static bcg::BatchedPlan *build(const bc_bccs *B, int width, int64_t b, int64_t e
   cfg.limit_bytes = (int64_t)1 << 36;
   cfg.fill_begin = b;
   cfg.fill_end = e;
+  cfg.keep_host_tables = true;
   bcg::BatchedPlan *p = nullptr;
   std::string msg;
   if (bcg::batched_create(B, cfg, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -55,7 +56,8 @@ int main(int argc, char **argv) {
     if (s2 != src || t2 != teps) bad = -2;  // the unit accounting never depends on the range
     for (int64_t j = 0; j < npass && bad == -1; ++j) {
       if (j >= b && j < e) {
-        if (bcg::batched_pass_digest(part, j) != bcg::batched_pass_digest(full, j)) bad = j;
+        const uint64_t dp = bcg::batched_pass_digest(part, j), df = bcg::batched_pass_digest(full, j);
+        if (dp == 0 || dp != df) bad = j;  // 0: no host tables to compare
         ++filled;
       }
     }
