@@ -19,8 +19,10 @@ static void usage() {
   std::fprintf(stderr,
                "usage: betc INPUT_FILE [--out FILE] [--mode plain|batched] [--delta fp64|fp32c]\n"
                "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE] [--gpu-decomp]\n"
+               "            [--plain-ctas 4|8|16]\n"
                "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr\n"
-               "  --gpu-decomp: run the BCC/chain decomposition on the GPU as well (same result)\n");
+               "  --gpu-decomp: run the BCC/chain decomposition on the GPU as well (same result)\n"
+               "  --plain-ctas: per-source CTAs per SM (more sources in flight on deep BCCs)\n");
 }
 
 int main(int argc, char **argv) {
@@ -51,6 +53,7 @@ int main(int argc, char **argv) {
     else if (a == "--quiet") quiet = true;
     else if (a == "--save-csr") save_path = next();
     else if (a == "--gpu-decomp") gpu_decomp = true;
+    else if (a == "--plain-ctas") opts.plain_ctas_per_sm = std::atoi(next());
     else if (a == "-h" || a == "--help") { usage(); return 0; }
     else if (!input) input = argv[i];
     else { usage(); return 1; }

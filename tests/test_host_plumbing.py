@@ -391,7 +391,8 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     g = GOLDEN / "sample4.txt"
     n = int(g.read_text().split()[0])
     out = tmp_path / "bc.txt"
-    for extra in ([], ["--mode", "plain"], ["--mode", "batched", "--delta", "fp64", "--batch", "64"]):
+    for extra in ([], ["--mode", "plain"], ["--mode", "batched", "--delta", "fp64", "--batch", "64"],
+                  ["--mode", "plain", "--plain-ctas", "16"]):
         r = run(g, "--out", out, *extra)
         assert r.returncode == 0, r.stderr
         assert "GPU total time is" in r.stderr
@@ -408,6 +409,8 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     assert r.returncode == 2 and "cannot be opened" in r.stderr
     r = run(g, "--batch", "33")
     assert r.returncode == 4 and "multiple of 32" in r.stderr
+    r = run(g, "--plain-ctas", "3")
+    assert r.returncode == 4 and "plain_ctas_per_sm" in r.stderr
     r = run(g, "--out", tmp_path / "no" / "such" / "dir.txt")
     assert r.returncode == 6
 
