@@ -381,7 +381,19 @@ def _same_arrays(a, b):
     return all(np.array_equal(a[k], b[k]) if hasattr(a[k], "shape") else a[k] == b[k] for k in a)
 
 
-@pytest.mark.parametrize("family", ["random", "larger", "wide", "rmat16", "grid"])
+def _deep_cycle():
+    """A 30000-vertex cycle with 12 chords and 200 pendant leaves: BFS levels
+    in the tens of thousands."""
+    G = graphs()
+    rng = np.random.default_rng(21)
+    n = 30000
+    u = np.concatenate([np.arange(n), rng.integers(0, n, 12)])
+    v = np.concatenate([(np.arange(n) + 1) % n, rng.integers(0, n, 12)])
+    uu, vv = G.simple_edges(n, u, v)
+    return G.attach_leaves(n, uu, vv, 200, n, rng)
+
+
+@pytest.mark.parametrize("family", ["random", "larger", "wide", "rmat16", "grid", "deep"])
 def test_gpu_decomposition_steps_on_host_equal_bc_decompose(family):
     """bc_decompose_gpu's data-parallel steps (union-find components, BFS
     forest, level sweeps, union-find over tree edges, member slots, the
@@ -395,6 +407,7 @@ def test_gpu_decomposition_steps_on_host_equal_bc_decompose(family):
         "wide": lambda: [wide_level_graph(s) for s in range(2)],
         "rmat16": lambda: [G.gen_rmat(16, 16, 0.2, 1, 8, seed=2)],
         "grid": lambda: [G.gen_grid(seed=3)],
+        "deep": lambda: [_deep_cycle()],
     }[family]()
     for n, u, v in cases:
         g = P.Graph.from_edges(n, u, v)

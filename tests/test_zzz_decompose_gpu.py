@@ -22,8 +22,19 @@ def test_gpu_decomposition_equals_host_on_fixtures():
         assert _same(P.Graph.from_edges(n, u, v)), name
 
 
+def _deep_cycle():
+    """A 30000-vertex cycle with 12 chords and 200 pendant leaves (deep BFS levels)."""
+    G = graphs()
+    rng = np.random.default_rng(21)
+    n = 30000
+    u = np.concatenate([np.arange(n), rng.integers(0, n, 12)])
+    v = np.concatenate([(np.arange(n) + 1) % n, rng.integers(0, n, 12)])
+    uu, vv = G.simple_edges(n, u, v)
+    return G.attach_leaves(n, uu, vv, 200, n, rng)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("which", ["rmat16", "grid", "ba64"])
+@pytest.mark.parametrize("which", ["rmat16", "grid", "ba64", "deep"])
 def test_gpu_decomposition_equals_host_at_scale(which):
     P = pkg()
     G = graphs()
@@ -31,6 +42,7 @@ def test_gpu_decomposition_equals_host_at_scale(which):
         "rmat16": lambda: G.gen_rmat(16, 16, 0.2, 1, 8, seed=2),
         "grid": lambda: G.gen_grid(seed=3),
         "ba64": lambda: G.pack_graphs(G.gen_ba_batch(64, seed=4))[:3],
+        "deep": _deep_cycle,
     }[which]()
     assert _same(P.Graph.from_edges(n, u, v))
 
