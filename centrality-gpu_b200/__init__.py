@@ -44,7 +44,7 @@ class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
                 ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
                 ("plain_core", C.c_int32), ("graph", C.c_int32), ("plain_ctas_per_sm", C.c_int32),
-                ("lazy_tables", C.c_int32)]
+                ("lazy_tables", C.c_int32), ("wait_limit_ms", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -87,6 +87,7 @@ _SIGS = {
                                         C.c_int32, C.c_void_p, C.c_void_p, _f64p]),
     "bc_begin_active": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, C.c_int32,
                                   _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f64p]),
+    "bc_wait_probe": (C.c_int, [C.c_void_p, C.c_int32, _f64p]),
     "bc_plan_create": (C.c_int, [C.c_void_p, C.POINTER(BcBccs), C.POINTER(C.c_void_p)]),
     "bc_plan_destroy": (None, [C.c_void_p]),
     "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
@@ -261,7 +262,7 @@ class Context:
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
                  workspace_limit=0, rescale_exp=0, plain_core=0, graph=False, plain_ctas_per_sm=0,
-                 lazy_tables=False):
+                 lazy_tables=False, wait_limit_ms=0):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
@@ -272,6 +273,7 @@ class Context:
         o.graph = 1 if graph else 0
         o.plain_ctas_per_sm = plain_ctas_per_sm
         o.lazy_tables = 1 if lazy_tables else 0
+        o.wait_limit_ms = wait_limit_ms
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:
@@ -302,6 +304,13 @@ class Context:
 
     def plan(self, decomp: Decomposition):
         return Plan(self, decomp)
+
+    def wait_probe(self, limit_ms: int):
+        """bc_wait_probe: a device-side wait on a flag nothing sets, bounded by
+        limit_ms. Returns (status code, device milliseconds the probe took)."""
+        ms = C.c_double(0.0)
+        rc = lib().bc_wait_probe(self._h, int(limit_ms), C.byref(ms))
+        return rc, ms.value
 
     def autotune_width(self, decomp: Decomposition, passes: int = 4):
         """Times up to `passes` multi-source passes at widths 128/256/512/1024

@@ -16,6 +16,7 @@ struct BatchedConfig {
   int sms = 148;
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
+  unsigned long long wait_ns = 60ull * 1000 * 1000 * 1000;  // limit of one device-side wait
   const std::vector<char> *bccs_on = nullptr;  // BCCs this plan schedules (null: all)
   const std::vector<int32_t> *ecc0 = nullptr;  // per BCC: eccentricity of local vertex 0 if known (< 0: compute)
   // Passes (global index) whose slot, seed and arming tables are built; the

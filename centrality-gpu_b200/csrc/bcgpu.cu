@@ -54,6 +54,7 @@ struct bc_plan {
   int *err = nullptr;
   unsigned long long *counter = nullptr;
   // PLAIN
+  unsigned long long *acc = nullptr;  // [n_packed][kAccDigits] fixed-point BC counters (folded into bc per launch)
   bcg::PlainItem *items = nullptr;
   int64_t n_items = 0;
   int32_t *ws_i = nullptr, *epochs = nullptr;
@@ -129,23 +130,13 @@ int upload(bc_plan *p, T **ptr, const T *src, int64_t count) {
   return BCGPU_OK;
 }
 
-const char *dev_err_text(int code) {
-  switch (code) {
-    case bcg::kDevDisconnected: return "a BCC is not connected (row did not reach every vertex)";
-    case bcg::kDevWorkspace: return "BCC larger than the kernel workspace";
-    case bcg::kDevTimeout: return "device-side wait exceeded its iteration limit";
-    case bcg::kDevBadItem: return "work item references data out of range";
-    default: return "unknown device error";
-  }
-}
-
 int check_dev_err(bc_plan *p) {
   int h = 0;
   CK(p->ctx, cudaMemcpyAsync(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream));
   CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
   p->d2h_bytes += (int64_t)sizeof(int);
   if (h != bcg::kDevOk)
-    return fail(p->ctx, h == bcg::kDevTimeout ? BCGPU_ETIMEOUT : BCGPU_EINVAL, dev_err_text(h));
+    return fail(p->ctx, bcg::dev_err_status(h), bcg::dev_err_text(h));
   if (p->bp) {
     int64_t bad = 0;
     if (bcg::batched_failed_batches(p->bp, p->ctx->stream, &bad) != BCGPU_OK)
@@ -211,6 +202,11 @@ int validate(bc_ctx *ctx, const bc_bccs *B) {
     if (out) return fail(ctx, BCGPU_EINVAL, kWhat[9]);
   }
   return BCGPU_OK;
+}
+
+// Limit of one device-side wait, from bc_opts.wait_limit_ms.
+unsigned long long wait_ns(const bc_ctx *ctx) {
+  return ctx->opts.wait_limit_ms > 0 ? (unsigned long long)ctx->opts.wait_limit_ms * 1000000ull : bcg::kDefaultWaitNs;
 }
 
 // Chain vertices per PLAIN work item: bounds the longest item so the dynamic
@@ -374,6 +370,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     cfg.sms = ctx->sms;
     cfg.limit_bytes = limit - p->device_bytes;
     cfg.rescale_exp = ctx->opts.rescale_exp;
+    cfg.wait_ns = wait_ns(ctx);
     cfg.bccs_on = &on;
     cfg.ecc0 = &ecc0;
     cfg.fill_begin = fill_begin;
@@ -415,7 +412,11 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
     p->h_items = items;
     p->ws_n = (p->mode == BCGPU_MODE_PLAIN ? nb_max : nb_plain) + 2;
-    const int64_t per_slot = p->ws_n * (7 * 4 + 4 * 8);
+    if ((rc = dalloc(p, &p->acc, bcg::kAccDigits * B->n_packed))) return bail(rc);
+    if (cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * bcg::kAccDigits * (size_t)std::max<int64_t>(B->n_packed, 1),
+                        ctx->stream) != cudaSuccess)
+      return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
+    const int64_t per_slot = p->ws_n * (bcg::kWsIntRows * 4 + bcg::kWsDblRows * 8);
     // Four 256-thread CTAs per SM (four sources in flight) when their rows
     // fit the budget, else two of 512, else one of 1024 per SM; with
     // plain_ctas_per_sm 8 or 16, CTAs of 128 or 64 threads are tried first.
@@ -432,10 +433,11 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     }
     p->grid = std::max(1, grid);
     const int64_t slots = p->grid + 1;  // + the row-export slot
-    if ((rc = dalloc(p, &p->ws_i, slots * 7 * p->ws_n)) || (rc = dalloc(p, &p->ws_f, slots * 4 * p->ws_n)) ||
-        (rc = dalloc(p, &p->epochs, 2 * slots)))
+    if ((rc = dalloc(p, &p->ws_i, slots * bcg::kWsIntRows * p->ws_n)) ||
+        (rc = dalloc(p, &p->ws_f, slots * bcg::kWsDblRows * p->ws_n)) || (rc = dalloc(p, &p->epochs, 2 * slots)))
       return bail(rc);
-    if (cudaMemsetAsync(p->ws_i, 0, sizeof(int32_t) * (size_t)(slots * 7 * p->ws_n), ctx->stream) != cudaSuccess)
+    if (cudaMemsetAsync(p->ws_i, 0, sizeof(int32_t) * (size_t)(slots * bcg::kWsIntRows * p->ws_n), ctx->stream) !=
+        cudaSuccess)
       return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
     std::vector<int32_t> ep((size_t)(2 * slots), 1);
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -484,6 +486,23 @@ void ctx_device_stream(const bc_ctx *ctx, int *device, cudaStream_t *stream, cud
   *ev1 = ctx->ev1;
 }
 void ctx_set_error(bc_ctx *ctx, const char *msg) { ctx->err = msg; }
+const char *dev_err_text(int code) {
+  switch (code) {
+    case kDevDisconnected: return "a BCC is not connected (row did not reach every vertex)";
+    case kDevWorkspace: return "BCC larger than the kernel workspace";
+    case kDevTimeout: return "device-side wait exceeded its iteration limit";
+    case kDevBadItem: return "work item references data out of range";
+    case kDevOverflow:
+      return "a path count or dependency left FP64's range despite per-level power-of-two scaling, or a BC "
+             "contribution exceeded the fixed-point accumulator";
+    default: return "unknown device error";
+  }
+}
+
+int dev_err_status(int code) {
+  return code == kDevTimeout ? BCGPU_ETIMEOUT : code == kDevOverflow ? BCGPU_EOVERFLOW : BCGPU_EINVAL;
+}
+
 }  // namespace bcg
 
 extern "C" void bc_default_opts(bc_opts *o) {
@@ -507,6 +526,7 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
   if (o.plain_ctas_per_sm != 0 && o.plain_ctas_per_sm != 4 && o.plain_ctas_per_sm != 8 && o.plain_ctas_per_sm != 16)
     return fail(nullptr, BCGPU_EINVAL, "plain_ctas_per_sm must be 0, 4, 8 or 16");
   if (o.lazy_tables != 0 && o.lazy_tables != 1) return fail(nullptr, BCGPU_EINVAL, "lazy_tables must be 0 or 1");
+  if (o.wait_limit_ms < 0) return fail(nullptr, BCGPU_EINVAL, "wait_limit_ms must be >= 0");
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0)
@@ -599,6 +619,41 @@ extern "C" int bc_autotune_width(bc_ctx *ctx, const bc_bccs *bccs, int32_t passe
   return BCGPU_OK;
 }
 
+namespace {
+
+// One thread waits on *flag (which nothing sets) with the library's bounded wait.
+__global__ void wait_probe_kernel(const unsigned int *flag, int *err, unsigned long long limit_ns) {
+  if (threadIdx.x == 0) bcg::wait_while_equal_probe(flag, err, limit_ns);
+}
+
+}  // namespace
+
+extern "C" int bc_wait_probe(bc_ctx *ctx, int32_t limit_ms, double *waited_ms) {
+  if (!ctx) return fail(ctx, BCGPU_EINVAL, "null context");
+  if (limit_ms <= 0) return fail(ctx, BCGPU_EINVAL, "limit_ms must be > 0");
+  CK(ctx, cudaSetDevice(ctx->device));
+  unsigned int *buf = nullptr;  // [0]: the flag, [1]: the error word
+  CK(ctx, cudaMalloc((void **)&buf, 2 * sizeof(unsigned int)));
+  cudaError_t e = cudaMemsetAsync(buf, 0, 2 * sizeof(unsigned int), ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, ctx->stream);
+  if (e == cudaSuccess) {
+    wait_probe_kernel<<<1, 32, 0, ctx->stream>>>(buf, reinterpret_cast<int *>(buf + 1),
+                                                 (unsigned long long)limit_ms * 1000000ull);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, ctx->stream);
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, buf + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  cudaFree(buf);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "wait probe");
+  if (waited_ms) *waited_ms = ms;
+  if (h != bcg::kDevOk) return fail(ctx, bcg::dev_err_status(h), bcg::dev_err_text(h));
+  return BCGPU_OK;
+}
+
 extern "C" void bc_plan_destroy(bc_plan *p) {
   if (!p) return;
   p->ctx->plans.erase(p);
@@ -653,11 +708,26 @@ extern "C" int bc_plan_reset(bc_plan *p) {
   if (!p) return BCGPU_EINVAL;
   CK(p->ctx, cudaSetDevice(p->ctx->device));
   CK(p->ctx, cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(p->n_packed, 1), p->ctx->stream));
+  if (p->acc)  // folded after every launch, so normally zero already; cleared after a failed run
+    CK(p->ctx, cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * bcg::kAccDigits * (size_t)std::max<int64_t>(p->n_packed, 1),
+                               p->ctx->stream));
   CK(p->ctx, cudaMemsetAsync(p->err, 0, sizeof(int), p->ctx->stream));
   return BCGPU_OK;
 }
 
 namespace {
+
+// Arguments of the per-source kernel over this plan's buffers (item range unset).
+bcg::PlainArgs plain_args(const bc_plan *p) {
+  bcg::PlainArgs a{};
+  a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
+  a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
+  a.items = p->items; a.next_item = p->counter; a.acc = p->acc;
+  a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
+  a.rescale_exp = p->ctx->opts.rescale_exp > 0 ? p->ctx->opts.rescale_exp : 900;
+  a.err = p->err;
+  return a;
+}
 
 // The device work of units [begin, end) (range already checked), enqueued on
 // the context's stream: the multi-source passes, then the per-source items.
@@ -669,17 +739,26 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
     if (rc) return fail(ctx, rc, "batched run: " + msg);
   }
   const int64_t i0 = std::max(begin, p->n_bat) - p->n_bat, i1 = end - p->n_bat;
-  if (i1 > i0) {  // per-source items
+  // per-source items, in launches of at most kAccMaxAdds sources (the adds one
+  // fixed-point counter takes between folds); each launch is followed by the
+  // fold of the counters of the BCCs it touched
+  for (int64_t j0 = i0; j0 < i1;) {
+    const int64_t *us = p->unit_sources.data() + p->n_bat;
+    int64_t j1 = j0 + 1;
+    while (j1 < i1 && us[j1 + 1] - us[j0] <= bcg::kAccMaxAdds) ++j1;
+    int32_t b0 = INT32_MAX, b1 = -1;
+    for (int64_t j = j0; j < j1; ++j) {
+      b0 = std::min(b0, p->h_items[j].bcc);
+      b1 = std::max(b1, p->h_items[j].bcc);
+    }
     CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
-    bcg::PlainArgs a{};
-    a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
-    a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
-    a.items = p->items; a.item_begin = i0; a.item_end = i1; a.next_item = p->counter; a.bc = p->bc;
-    a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid;
-    a.err = p->err;
-    const int grid = (int)std::min<int64_t>(p->grid, i1 - i0);
+    bcg::PlainArgs a = plain_args(p);
+    a.item_begin = j0; a.item_end = j1;
+    const int grid = (int)std::min<int64_t>(p->grid, j1 - j0);
     CK(ctx, bcg::launch_plain(a, p->block, grid, ctx->stream));
-    ++*launches;
+    CK(ctx, bcg::launch_fold(p->acc, p->bc, p->h_vtx_off[b0], p->h_vtx_off[b1 + 1], ctx->stream));
+    *launches += 2;
+    j0 = j1;
   }
   return BCGPU_OK;
 }
@@ -812,10 +891,7 @@ extern "C" int bc_plan_source_rows(bc_plan *p, int64_t packed, int32_t *d_out, d
   double *ds = nullptr;
   CK(ctx, cudaMallocAsync((void **)&dd, sizeof(int32_t) * (size_t)nb, ctx->stream));
   CK(ctx, cudaMallocAsync((void **)&ds, sizeof(double) * (size_t)nb, ctx->stream));
-  bcg::PlainArgs a{};
-  a.row = p->row; a.col = p->col; a.reach = p->reach; a.vtx_off = p->vtx_off;
-  a.chain_start = p->chain_start; a.chain_len = p->chain_len; a.chain_l = p->chain_l; a.chain_r = p->chain_r;
-  a.ws_i = p->ws_i; a.ws_f = p->ws_f; a.ws_n = p->ws_n; a.epochs = p->epochs; a.rows_slot = p->grid; a.err = p->err;
+  const bcg::PlainArgs a = plain_args(p);
   cudaError_t e = bcg::launch_rows(a, b, local, chain, dd, ds, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, dd, sizeof(int32_t) * (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_out, ds, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream);

@@ -20,7 +20,10 @@ static void usage() {
                "usage: betc INPUT_FILE [--out FILE] [--mode plain|batched] [--delta fp64|fp32c]\n"
                "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE] [--gpu-decomp]\n"
                "            [--plain-ctas 4|8|16]\n"
-               "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr\n"
+               "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr;\n"
+               "    the graph is taken as simple and unweighted: repeated edges count once and\n"
+               "    self-loops are dropped (the reference keeps repeated edges as parallel arcs,\n"
+               "    which multiplies path counts)\n"
                "  --gpu-decomp: run the BCC/chain decomposition on the GPU as well (same result)\n"
                "  --plain-ctas: per-source CTAs per SM (more sources in flight on deep BCCs)\n");
 }

@@ -10,5 +10,9 @@ namespace bcg {
 void ctx_device_stream(const bc_ctx *ctx, int *device, cudaStream_t *stream, cudaEvent_t *ev0, cudaEvent_t *ev1);
 // Records msg as the context's last error (read back by bc_last_error).
 void ctx_set_error(bc_ctx *ctx, const char *msg);
+// The text and the BCGPU_* status of a device error code (common.cuh DevErr),
+// shared by every entry point that reads a kernel's error flag.
+const char *dev_err_text(int code);
+int dev_err_status(int code);
 
 }  // namespace bcg

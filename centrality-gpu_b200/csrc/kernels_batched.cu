@@ -66,7 +66,6 @@ constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in 
 constexpr int kHeavyDegSmall = 32; // ... or than this, on cores small enough that one row is a level's critical path
 constexpr int kSmallCore = 16384;  // cores below this many vertices use kHeavyDegSmall
 constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
-constexpr long long kSpinLimit = 1ll << 28;  // ~1 min of polling before giving up
 constexpr int kHalf = 4;           // words per pass over a vertex row
 
 // One source of a pass. chain < 0: the core vertex src (level 0). Otherwise
@@ -152,6 +151,7 @@ struct Args {
   int32_t W;        // words per row (row stride)
   int32_t tcap;     // levels allocated
   int32_t rescale_exp;
+  unsigned long long wait_ns;  // limit of one grid-barrier wait
   int32_t pad;
   double *bc;
   Ctrl *ctrl;
@@ -171,8 +171,9 @@ __device__ __forceinline__ bool cta_failed(const Args &a) {
 }
 
 // Grid-wide barrier for a cooperative launch. Waits are bounded: after
-// kSpinLimit polls the CTA records kDevTimeout and continues; once any error
-// is flagged every barrier returns at once so the kernel drains quickly.
+// a.wait_ns of device time the CTA records kDevTimeout and continues; once
+// any error is flagged every barrier returns at once so the kernel drains
+// quickly.
 __device__ void grid_sync(const Args &a) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -185,12 +186,7 @@ __device__ void grid_sync(const Args &a) {
       __threadfence();
       atomicAdd(&a.ctrl->bar_gen, 1u);
     } else {
-      long long it = 0;
-      while (*gen == g) {
-        if (failed(a)) break;
-        if (++it > kSpinLimit) { set_err(a.err, kDevTimeout); break; }
-        __nanosleep(128);
-      }
+      wait_while_equal(gen, g, a.wait_ns, a.err, [&] { return failed(a); });
     }
     __threadfence();
   }
@@ -1531,6 +1527,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   a.chain_start = chain_start; a.chain_len = chain_len; a.chain_l = chain_l; a.chain_r = chain_r;
   a.n_cap = P->n_cap; a.W = W; a.tcap = tcap; a.bc = bc; a.err = err;
   a.rescale_exp = cfg.rescale_exp > 0 ? cfg.rescale_exp : 900;
+  a.wait_ns = cfg.wait_ns;
 
   // cooperative grid: every CTA resident
   int dev = 0, sms = 0, per_sm = 0, coop = 0;

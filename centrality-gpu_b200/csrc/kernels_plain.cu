@@ -1,5 +1,7 @@
-// PLAIN schedule: one source per CTA at a time, FP64 path counts and
-// dependencies, FP64 atomics into the per-vertex BC accumulator.
+// PLAIN schedule: one source per CTA at a time, FP64 path counts (with
+// per-level power-of-two scaling) and dependencies; BC accumulated in
+// fixed-point integer counters, so the result does not depend on the order
+// in which CTAs finish their sources.
 //
 // Follows the reference's per-source Brandes (bc_kgpu_free / bc_kgpu_active,
 // Codes/kernels_free.cu:154-473, Codes/kernels_active.cu:263-602) and its
@@ -17,6 +19,17 @@
 //  * the dependency sweep stores q(w) = (reach(w)+1+delta(w)) / sigma(w) so a
 //    predecessor reads one value per successor: delta(v) = sigma(v) * sum q(w)
 //    (same quantity as Codes/kernels_free.cu:391,409);
+//  * path counts are stored per level relative to a power of two 2^X(level):
+//    a level whose largest count passes 2^rescale_exp is divided by a power
+//    of two (exact), so deep, high-diameter BCCs do not overflow FP64 (the
+//    reference keeps sigma in uint64 / int32, Codes/kernels_free.cu:161,
+//    Codes/kernels_active.cu:274, and overflows silently); the backward
+//    sweep rescales by 2^(X(l) - X(l+1)) between levels. Counts or
+//    dependencies that still leave FP64's range flag kDevOverflow;
+//  * BC: the reference adds FP32 dependencies with atomicAdd
+//    (Codes/kernels_free.cu:423-426), whose result depends on the order of
+//    the adds; here each contribution goes into fixed-point integer counters
+//    (see PlainArgs::acc) that launch_fold turns into FP64;
 //  * a chain vertex's rows are the merge of its endpoints' rows
 //    (Codes/postprocesses.cu:329-351) and its dependency sweep walks the
 //    endpoints' level buckets directly instead of radix-sorting n distance
@@ -28,6 +41,7 @@
 #include "common.cuh"
 #include "plain.h"
 
+#include <algorithm>
 #include <cooperative_groups.h>
 
 namespace cg = cooperative_groups;
@@ -48,26 +62,87 @@ struct Shared {
   int imax;
   int item;
   int base_a, base_b;  // epochs of rows A and B
+  int emax[2];         // largest biased FP64 exponent of the path counts of a level (by level parity)
   double red[kWarps];
   int wq[kBlock];
   int cq[kBlock];
 };
 
-// Per-CTA workspace rows (capacity ws_n each).
+// Per-CTA workspace rows (capacity ws_n each), addressed from two base
+// pointers so that the row pointers are recomputed where used instead of
+// being held in registers. lxA/lxB: the power-of-two exponent X of each level
+// of rows A/B (path count = stored value * 2^X); lxM: the same for the merged
+// row of a chain vertex.
 struct Rows {
-  int32_t *dA, *SA, *lvA, *dB, *SB, *lvB, *dM;
-  double *sA, *sB, *sM, *q;
+  int32_t *wi;
+  double *wf;
+  int64_t n;
+  __device__ __forceinline__ int32_t *dA() const { return wi; }
+  __device__ __forceinline__ int32_t *SA() const { return wi + n; }
+  __device__ __forceinline__ int32_t *lvA() const { return wi + 2 * n; }
+  __device__ __forceinline__ int32_t *dB() const { return wi + 3 * n; }
+  __device__ __forceinline__ int32_t *SB() const { return wi + 4 * n; }
+  __device__ __forceinline__ int32_t *lvB() const { return wi + 5 * n; }
+  __device__ __forceinline__ int32_t *dM() const { return wi + 6 * n; }
+  __device__ __forceinline__ int32_t *lxA() const { return wi + 7 * n; }
+  __device__ __forceinline__ int32_t *lxB() const { return wi + 8 * n; }
+  __device__ __forceinline__ int32_t *lxM() const { return wi + 9 * n; }
+  __device__ __forceinline__ double *sA() const { return wf; }
+  __device__ __forceinline__ double *sB() const { return wf + n; }
+  __device__ __forceinline__ double *sM() const { return wf + 2 * n; }
+  __device__ __forceinline__ double *q() const { return wf + 3 * n; }
 };
 
 __device__ __forceinline__ Rows rows_of(const PlainArgs &a, int64_t slot) {
-  Rows r;
-  const int64_t n = a.ws_n;
-  int32_t *wi = a.ws_i + slot * 7 * n;
-  double *wf = a.ws_f + slot * 4 * n;
-  r.dA = wi; r.SA = wi + n; r.lvA = wi + 2 * n; r.dB = wi + 3 * n; r.SB = wi + 4 * n; r.lvB = wi + 5 * n;
-  r.dM = wi + 6 * n;
-  r.sA = wf; r.sB = wf + n; r.sM = wf + 2 * n; r.q = wf + 3 * n;
-  return r;
+  return Rows{a.ws_i + slot * kWsIntRows * a.ws_n, a.ws_f + slot * kWsDblRows * a.ws_n, a.ws_n};
+}
+
+// Biased IEEE-754 exponent field of a double (0: zero or subnormal, 2047: inf or NaN).
+__device__ __forceinline__ int exp_bits(double v) {
+  return (int)((unsigned long long)__double_as_longlong(v) >> 52) & 0x7ff;
+}
+
+// 2^e for -1022 <= e <= 1023, built from its IEEE-754 exponent field.
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// v * 2^e: a multiplication by an exact power of two (exact unless the result
+// leaves the normal range); |e| beyond one factor's range takes two factors.
+// e == 0 leaves v untouched.
+__device__ __forceinline__ double scale2(double v, int e) {
+  if (e == 0) return v;
+  if (e >= -1022 && e <= 1023) return v * pow2(e);
+  const int h = max(-1022, min(1023, e / 2));
+  return v * pow2(h) * pow2(max(-1022, min(1023, e - h)));
+}
+
+// Adds contribution c >= 0 to a vertex's fixed-point counters a4[0..kAccDigits):
+// floor(c * 2^kAccFrac) split into kAccDigitBits-bit digits. The double's
+// fields are read directly (IEEE-754 binary64: c = m * 2^(E - 1075) with the
+// 53-bit integer m = mantissa | 2^52 for a normal number); a value below
+// 2^-kAccFrac contributes nothing, one too large for the counters (or not
+// finite) flags kDevOverflow.
+__device__ __forceinline__ void acc_add(unsigned long long *a4, double c, int *err) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(c);
+  const int E = (int)(bits >> 52) & 0x7ff;
+  if (bits >> 63 || E == 0x7ff) { set_err(err, kDevOverflow); return; }  // negative, inf or NaN
+  if (E == 0) return;                                                  // zero or subnormal: below 2^-kAccFrac
+  unsigned long long m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+  int s = E - 1075 + kAccFrac;  // c * 2^kAccFrac = m * 2^s
+  if (s < 0) {
+    if (s <= -53) return;
+    m >>= -s;
+    s = 0;
+  }
+  if (s + 53 > kAccDigits * kAccDigitBits) { set_err(err, kDevOverflow); return; }
+  constexpr unsigned long long kMask = (1ull << kAccDigitBits) - 1;
+  const int di = s / kAccDigitBits, off = s % kAccDigitBits;  // m * 2^off spans digits di .. di+2
+  const unsigned long long d0 = (m << off) & kMask;
+  const unsigned long long d1 = (m >> (kAccDigitBits - off)) & kMask;
+  const int sh2 = 2 * kAccDigitBits - off;
+  const unsigned long long d2 = sh2 < 53 ? m >> sh2 : 0ull;
+  if (d0) atomicAdd(a4 + di, d0);
+  if (d1) atomicAdd(a4 + di + 1, d1);  // nonzero only when digit di+1 exists (s + 53 <= digits * bits)
+  if (d2) atomicAdd(a4 + di + 2, d2);
 }
 
 // Appends x to S (warp-aggregated atomic on the shared tail).
@@ -146,11 +221,13 @@ __device__ __forceinline__ double block_sum(Shared<kBlock> &sh, double v) {
   return t;
 }
 
-// CTA-wide BFS from s over one BCC: fills d (epoch base), sigma, the level
-// order S and level offsets lv[0..nlev]. Returns nlev (number of levels).
+// CTA-wide BFS from s over one BCC: fills d (epoch base), the scaled path
+// counts sig, the level order S, level offsets lv[0..nlev] and the level
+// exponents lx[0..nlev) (path count of a vertex on level l = sig * 2^lx[l]).
+// Returns nlev (number of levels).
 template <int kBlock>
-__device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, int32_t nb, int32_t s, int32_t *d, double *sig,
-                       int32_t *S, int32_t *lv, int base) {
+__device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, int32_t s, int32_t *d, double *sig,
+                       int32_t *S, int32_t *lv, int32_t *lx, int base, int rescale_exp, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
@@ -159,13 +236,16 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
     lv[0] = 0;
     lv[1] = 1;
     sh.tail = 1;
+    sh.emax[0] = 0;
+    sh.emax[1] = 0;
   }
   __syncthreads();
-  int lev = 0;
+  int lev = 0, xprev = 0;
   while (true) {
     const int f0 = lv[lev], f1 = lv[lev + 1];
     // the source has no predecessors; stale stamps are < base so they never match base+lev-1
     const int dprev = lev == 0 ? INT_MIN : base + lev - 1, dnext = base + lev + 1;
+    int emax = 0;  // largest exponent field among the path counts this thread writes on this level
     for (int c0 = f0; c0 < f1; c0 += kBlock) {
       if (tid == 0) { sh.nwq = 0; sh.ncq = 0; }
       __syncthreads();
@@ -176,7 +256,9 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         const int64_t deg = e1 - e0;
         if (deg <= kSmallDeg) {
           const double acc = fwd_small(sh, C + e0, (int)deg, d, sig, S, dprev, dnext, base);
-          sig[w] = lev == 0 ? 1.0 : acc;
+          const double v = lev == 0 ? 1.0 : acc;
+          sig[w] = v;
+          emax = max(emax, exp_bits(v));
         } else if (deg <= kWarpDeg) {
           sh.wq[atomicAdd(&sh.nwq, 1)] = w;
         } else {
@@ -190,7 +272,11 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         double acc = 0.0;
         for (int64_t e = e0 + lane; e < e1; e += 32) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
         acc = warp_sum(acc);
-        if (lane == 0) sig[w] = lev == 0 ? 1.0 : acc;
+        if (lane == 0) {
+          const double v = lev == 0 ? 1.0 : acc;
+          sig[w] = v;
+          emax = max(emax, exp_bits(v));
+        }
       }
       const int ncq = sh.ncq;
       for (int k = 0; k < ncq; ++k) {
@@ -199,17 +285,45 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         double acc = 0.0;
         for (int64_t e = e0 + tid; e < e1; e += kBlock) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
         acc = block_sum(sh, acc);
-        if (tid == 0) sig[w] = lev == 0 ? 1.0 : acc;
+        if (tid == 0) {
+          const double v = lev == 0 ? 1.0 : acc;
+          sig[w] = v;
+          emax = max(emax, exp_bits(v));
+        }
       }
+      emax = __reduce_max_sync(0xffffffffu, emax);
+      if (lane == 0) atomicMax(&sh.emax[lev & 1], emax);
       __syncthreads();
     }
+    // the level's path counts are final: rescale them if the largest passed 2^rescale_exp
+    const int ebig = sh.emax[lev & 1];
+    int x = xprev;
+    if (ebig == 0x7ff) {
+      set_err(err, kDevOverflow);
+    } else if (rescale_exp > 0 && ebig - 1023 > rescale_exp) {
+      const int k = ebig - 1023;  // brings the largest count to [1, 2)
+      x += k;
+      bool lost = false;
+      for (int i = f0 + tid; i < f1; i += kBlock) {
+        const int32_t w = S[i];
+        const double v = scale2(sig[w], -k);
+        lost |= exp_bits(v) == 0;  // a count of this level fell out of the normal range
+        sig[w] = v;
+      }
+      if (lost) set_err(err, kDevOverflow);
+    }
+    if (tid == 0) {
+      lx[lev] = x;
+      sh.emax[(lev + 1) & 1] = 0;
+    }
+    xprev = x;
     const int tail = sh.tail;
     if (tail == f1) break;
     if (tid == 0) lv[lev + 2] = tail;
     ++lev;
     __syncthreads();
   }
-  (void)nb;
+  __syncthreads();  // rescaled counts and lx visible to the caller's next phase
   return lev + 1;
 }
 
@@ -239,12 +353,18 @@ __device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_
   return acc;
 }
 
-__device__ __forceinline__ void finish_vertex(int32_t w, double acc, const int32_t *rch, const double *sig, double *q,
-                                              double *bcb, double wsrc) {
+// Successor sums arrive in the scale of the next level: 2^sdiff =
+// 2^(X(level) - X(level+1)) brings them to this level's, so that
+// delta = sig * sum is the unscaled dependency and q = (reach+1+delta)/sig is
+// in this level's scale.
+__device__ __forceinline__ void finish_vertex(int32_t w, double acc, int sdiff, const int32_t *rch, const double *sig,
+                                              double *q, unsigned long long *accb, double wsrc, int *err) {
   const double sw = sig[w];
-  const double delta = sw * acc;
-  q[w] = ((double)rch[w] + 1.0 + delta) / sw;
-  if (delta != 0.0) atomicAdd(bcb + w, delta * wsrc);
+  const double delta = sw * scale2(acc, sdiff);
+  const double qw = ((double)rch[w] + 1.0 + delta) / sw;
+  q[w] = qw;
+  if (exp_bits(qw) == 0x7ff || exp_bits(delta) == 0x7ff) set_err(err, kDevOverflow);
+  if (delta != 0.0) acc_add(accb + (int64_t)kAccDigits * w, delta * wsrc, err);
 }
 
 // Vertex list of one backward level: up to three index ranges with filters.
@@ -275,8 +395,8 @@ __device__ __forceinline__ bool keep_vertex(int mode, int list, int32_t w, int l
 
 template <int kBlock>
 __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, const int32_t *d, const double *sig,
-                              double *q, const int32_t *rch, double *bcb, double wsrc, int dsucc, int lev, int mode,
-                              const LevelList &L, const MergeFilter &mf) {
+                              double *q, const int32_t *rch, unsigned long long *accb, double wsrc, int dsucc, int lev,
+                              int sdiff, int mode, const LevelList &L, const MergeFilter &mf, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int list = 0; list < 3; ++list) {
@@ -293,7 +413,7 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
         if (keep_vertex(mode, list, w, lev, d, mf)) {
           const int64_t deg = R[w + 1] - R[w];
           if (deg <= kSmallDeg) {
-            finish_vertex(w, bwd_arcs_thread(R, C, d, q, w, dsucc), rch, sig, q, bcb, wsrc);
+            finish_vertex(w, bwd_arcs_thread(R, C, d, q, w, dsucc), sdiff, rch, sig, q, accb, wsrc, err);
           } else if (deg <= kWarpDeg) {
             sh.wq[atomicAdd(&sh.nwq, 1)] = w;
           } else {
@@ -310,7 +430,7 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
           if (d[x] == dsucc) acc += q[x];
         }
         acc = warp_sum(acc);
-        if (lane == 0) finish_vertex(w, acc, rch, sig, q, bcb, wsrc);
+        if (lane == 0) finish_vertex(w, acc, sdiff, rch, sig, q, accb, wsrc, err);
       }
       const int ncq = sh.ncq;
       for (int k = 0; k < ncq; ++k) {
@@ -321,7 +441,7 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
           if (d[x] == dsucc) acc += q[x];
         }
         acc = block_sum(sh, acc);
-        if (tid == 0) finish_vertex(w, acc, rch, sig, q, bcb, wsrc);
+        if (tid == 0) finish_vertex(w, acc, sdiff, rch, sig, q, accb, wsrc, err);
       }
       __syncthreads();
     }
@@ -337,27 +457,50 @@ __device__ void ensure_epoch(int32_t *d, int64_t cap, int &base, int span) {
   base = 1;
 }
 
+// Level exponents of a merged row: level l of the merged row holds vertices
+// from level l-ld of row A and level l-rd of row B; its exponent is the larger
+// of theirs (0 when neither exists: chain vertices only).
+struct MergedExp {
+  const int32_t *lxA, *lxB;
+  int nlevA, nlevB, ld, rd;
+  __device__ __forceinline__ int operator()(int l) const {
+    int x = 0;
+    const int a = l - ld, b = l - rd;
+    if (a >= 0 && a < nlevA) x = max(x, lxA[a]);
+    if (b >= 0 && b < nlevB) x = max(x, lxB[b]);
+    return x;
+  }
+};
+
 // Rows of chain vertex (start+pos) from the endpoint rows A (left) and B
 // (right): d = min(dA+ld, dB+rd), sigma from the strictly shorter side or the
-// sum on ties (Codes/postprocesses.cu:334-350); then the chain's own vertices
-// are fixed along the chain (Codes/postprocesses.cu:205-274). Returns max level.
+// sum on ties (Codes/postprocesses.cu:334-350), each brought to the merged
+// level's exponent; then the chain's own vertices are fixed along the chain
+// (Codes/postprocesses.cu:205-274). Returns max level.
 template <int kBlock>
 __device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int baseB, int32_t nb, int32_t start, int32_t len,
-                          int32_t pos, int *err) {
+                          int32_t pos, const MergedExp &xm, int *err) {
   const int ld = pos + 1, rd = len - pos;
   int mx = 0;
   bool bad = false;
   for (int k = threadIdx.x; k < nb; k += kBlock) {
-    const int la = __ldcg(r.dA + k) - baseA, lb = __ldcg(r.dB + k) - baseB;
-    bad |= (la < 0) | (lb < 0);
+    const int la = __ldcg(r.dA() + k) - baseA, lb = __ldcg(r.dB() + k) - baseB;
+    if ((la < 0) | (lb < 0) | (la >= xm.nlevA) | (lb >= xm.nlevB)) {
+      bad = true;
+      continue;
+    }
     const int a = la + ld, b = lb + rd;
     int dm;
     double sm;
-    if (a < b) { dm = a; sm = r.sA[k]; }
-    else if (a > b) { dm = b; sm = r.sB[k]; }
-    else { dm = b; sm = r.sA[k] + r.sB[k]; }
-    r.dM[k] = dm;
-    r.sM[k] = sm;
+    if (a < b) { dm = a; sm = scale2(r.sA()[k], xm.lxA[la] - xm(a)); }
+    else if (a > b) { dm = b; sm = scale2(r.sB()[k], xm.lxB[lb] - xm(b)); }
+    else {
+      dm = b;
+      const int x = xm(b);
+      sm = scale2(r.sA()[k], xm.lxA[la] - x) + scale2(r.sB()[k], xm.lxB[lb] - x);
+    }
+    r.dM()[k] = dm;
+    r.sM()[k] = sm;
     mx = max(mx, dm);
   }
   if (bad) set_err(err, kDevDisconnected);
@@ -366,16 +509,19 @@ __device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int base
   __syncthreads();
   if ((threadIdx.x & 31) == 0) atomicMax(&sh.imax, mx);
   __syncthreads();
+  const int maxlev = sh.imax;
   if (threadIdx.x == 0) {
     for (int j = 0; j < len; ++j) {
       const int k = start + j;
       const int dist = j > pos ? j - pos : pos - j;
-      if (r.dM[k] > dist) { r.dM[k] = dist; r.sM[k] = 1.0; }
-      else if (r.dM[k] == dist) r.sM[k] += 1.0;
+      const double one = scale2(1.0, -xm(dist));  // one path, in the merged level's scale
+      if (r.dM()[k] > dist) { r.dM()[k] = dist; r.sM()[k] = one; }
+      else if (r.dM()[k] == dist) r.sM()[k] += one;
     }
   }
+  for (int l = threadIdx.x; l <= maxlev; l += kBlock) r.lxM()[l] = xm(l);
   __syncthreads();
-  return sh.imax;
+  return maxlev;
 }
 
 template <int kBlock>
@@ -386,17 +532,18 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
   if ((int64_t)nb + 2 > a.ws_n) { set_err(a.err, kDevWorkspace); return; }
   const int64_t *R = a.row + vo;
   const int32_t *rch = a.reach + vo;
-  double *bcb = a.bc + vo;
+  unsigned long long *accb = a.acc + (int64_t)kAccDigits * vo;
   const MergeFilter none{nullptr, 0, 0, nullptr, 0, 0};
 
   // own source: BFS into row A, then its dependency sweep
   int baseA = sh.base_a;
-  ensure_epoch(r.dA, a.ws_n, baseA, nb);
-  const int nlevA = cta_bfs(sh, R, a.col, nb, it.src, r.dA, r.sA, r.SA, r.lvA, baseA);
+  ensure_epoch(r.dA(), a.ws_n, baseA, nb);
+  const int nlevA = cta_bfs(sh, R, a.col, it.src, r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), baseA, a.rescale_exp, a.err);
   const double wsrc = (double)rch[it.src] + 1.0;
   for (int lev = it.own ? nlevA - 1 : 0; lev >= 1; --lev) {
-    LevelList L{r.SA, r.lvA[lev], r.lvA[lev + 1], nullptr, 0, 0, -1, -1};
-    cta_bwd_level(sh, R, a.col, r.dA, r.sA, r.q, rch, bcb, wsrc, baseA + lev + 1, lev, 0, L, none);
+    LevelList L{r.SA(), r.lvA()[lev], r.lvA()[lev + 1], nullptr, 0, 0, -1, -1};
+    const int sdiff = lev + 1 < nlevA ? r.lxA()[lev] - r.lxA()[lev + 1] : 0;  // the deepest level has no successors
+    cta_bwd_level(sh, R, a.col, r.dA(), r.sA(), r.q(), rch, accb, wsrc, baseA + lev + 1, lev, sdiff, 0, L, none, a.err);
   }
 
   int baseB = sh.base_b, nlevB = 0, prevR = -1;
@@ -405,24 +552,26 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
     if (a.chain_l[c] != it.src || start < 0 || start + len > nb) { set_err(a.err, kDevBadItem); break; }
     if (cr != prevR) {
       if (prevR >= 0) baseB += nlevB + 1;
-      ensure_epoch(r.dB, a.ws_n, baseB, nb);
-      nlevB = cta_bfs(sh, R, a.col, nb, cr, r.dB, r.sB, r.SB, r.lvB, baseB);
+      ensure_epoch(r.dB(), a.ws_n, baseB, nb);
+      nlevB = cta_bfs(sh, R, a.col, cr, r.dB(), r.sB(), r.SB(), r.lvB(), r.lxB(), baseB, a.rescale_exp, a.err);
       prevR = cr;
     }
     for (int32_t pos = 0; pos < len; ++pos) {
       const int32_t z = start + pos;
       const int ld = pos + 1, rd = len - pos;
-      const int maxlev = merge_rows(sh, r, baseA, baseB, nb, start, len, pos, a.err);
+      const MergedExp xm{r.lxA(), r.lxB(), nlevA, nlevB, ld, rd};
+      const int maxlev = merge_rows(sh, r, baseA, baseB, nb, start, len, pos, xm, a.err);
       const double wz = (double)rch[z] + 1.0;
-      const MergeFilter mf{r.dA, baseA, ld, r.dB, baseB, rd};
+      const MergeFilter mf{r.dA(), baseA, ld, r.dB(), baseB, rd};
       for (int lev = maxlev; lev >= 1; --lev) {
-        LevelList L{r.SA, 0, 0, r.SB, 0, 0, -1, -1};
+        LevelList L{r.SA(), 0, 0, r.SB(), 0, 0, -1, -1};
         const int la = lev - ld, lb = lev - rd;
-        if (la >= 0 && la < nlevA) { L.a0 = r.lvA[la]; L.b0 = r.lvA[la + 1]; }
-        if (lb >= 0 && lb < nlevB) { L.a1 = r.lvB[lb]; L.b1 = r.lvB[lb + 1]; }
+        if (la >= 0 && la < nlevA) { L.a0 = r.lvA()[la]; L.b0 = r.lvA()[la + 1]; }
+        if (lb >= 0 && lb < nlevB) { L.a1 = r.lvB()[lb]; L.b1 = r.lvB()[lb + 1]; }
         if (pos - lev >= 0) L.ck0 = start + pos - lev;
         if (pos + lev < len) L.ck1 = start + pos + lev;
-        cta_bwd_level(sh, R, a.col, r.dM, r.sM, r.q, rch, bcb, wz, lev + 1, lev, 1, L, mf);
+        const int sdiff = lev < maxlev ? r.lxM()[lev] - r.lxM()[lev + 1] : 0;
+        cta_bwd_level(sh, R, a.col, r.dM(), r.sM(), r.q(), rch, accb, wz, lev + 1, lev, sdiff, 1, L, mf, a.err);
       }
     }
   }
@@ -470,21 +619,62 @@ __global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bc
   const int32_t nb = (int32_t)(a.vtx_off[bcc + 1] - vo);
   if ((int64_t)nb + 2 > a.ws_n) { set_err(a.err, kDevWorkspace); return; }
   const int64_t *R = a.row + vo;
-  for (int k = threadIdx.x; k < nb; k += kBlock) { r.dA[k] = 0; r.dB[k] = 0; }
+  for (int k = threadIdx.x; k < nb; k += kBlock) { r.dA()[k] = 0; r.dB()[k] = 0; }
   __syncthreads();
   if (chain < 0) {
-    cta_bfs(sh, R, a.col, nb, src, r.dA, r.sA, r.SA, r.lvA, 1);
-    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dA[k] - 1; s_out[k] = r.sA[k]; }
+    cta_bfs(sh, R, a.col, src, r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
+    for (int k = threadIdx.x; k < nb; k += kBlock) {
+      const int l = r.dA()[k] - 1;
+      d_out[k] = l;
+      s_out[k] = l >= 0 ? scale2(r.sA()[k], r.lxA()[l]) : 0.0;
+    }
   } else {
-    const int32_t start = a.chain_start[chain], len = a.chain_len[chain];
-    cta_bfs(sh, R, a.col, nb, a.chain_l[chain], r.dA, r.sA, r.SA, r.lvA, 1);
-    cta_bfs(sh, R, a.col, nb, a.chain_r[chain], r.dB, r.sB, r.SB, r.lvB, 1);
-    merge_rows(sh, r, 1, 1, nb, start, len, src - start, a.err);
-    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dM[k]; s_out[k] = r.sM[k]; }
+    const int32_t start = a.chain_start[chain], len = a.chain_len[chain], pos = src - start;
+    const int nlevA = cta_bfs(sh, R, a.col, a.chain_l[chain], r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
+    const int nlevB = cta_bfs(sh, R, a.col, a.chain_r[chain], r.dB(), r.sB(), r.SB(), r.lvB(), r.lxB(), 1, a.rescale_exp, a.err);
+    const MergedExp xm{r.lxA(), r.lxB(), nlevA, nlevB, pos + 1, len - pos};
+    merge_rows(sh, r, 1, 1, nb, start, len, pos, xm, a.err);
+    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dM()[k]; s_out[k] = scale2(r.sM()[k], xm(r.dM()[k])); }
+  }
+}
+
+// Counters -> FP64, one vertex per thread: carries propagated exactly (each
+// counter is below 2^64 - 2^(64-kAccDigitBits), so counter + carry fits), then
+// the digits summed from the most significant down; the order of the FP64
+// operations is fixed, so equal counters give equal values.
+__global__ void __launch_bounds__(256) fold_kernel(unsigned long long *acc, double *bc, int64_t v0, int64_t v1) {
+  static_assert(kAccDigits == 4, "fold_kernel reads four counters per vertex");
+  constexpr unsigned long long kMask = (1ull << kAccDigitBits) - 1;
+  for (int64_t v = v0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x) {
+    ulonglong2 *p = reinterpret_cast<ulonglong2 *>(acc + kAccDigits * v);
+    const ulonglong2 lo = p[0], hi = p[1];
+    if ((lo.x | lo.y | hi.x | hi.y) == 0) continue;
+    const unsigned long long c[4] = {lo.x, lo.y, hi.x, hi.y};
+    unsigned long long dg[5], carry = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const unsigned long long t = c[i] + carry;
+      dg[i] = t & kMask;
+      carry = t >> kAccDigitBits;
+    }
+    dg[4] = carry;
+    double r = 0.0;
+#pragma unroll
+    for (int i = 4; i >= 0; --i) r += (double)dg[i] * pow2(i * kAccDigitBits - kAccFrac);
+    bc[v] += r;
+    p[0] = make_ulonglong2(0, 0);
+    p[1] = make_ulonglong2(0, 0);
   }
 }
 
 }  // namespace
+
+cudaError_t launch_fold(unsigned long long *acc, double *bc, int64_t v0, int64_t v1, cudaStream_t stream) {
+  if (v1 <= v0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((v1 - v0 + 255) / 256, 148 * 8);
+  fold_kernel<<<(int)blocks, 256, 0, stream>>>(acc, bc, v0, v1);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_plain(const PlainArgs &a, int block, int grid, cudaStream_t stream) {
   switch (block) {

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
+#include <string>
 
 namespace bcg {
 namespace {
@@ -23,16 +24,19 @@ constexpr int64_t kRowCap = kMaxVertices + 2;  // per-slot row capacity the kern
 
 constexpr int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
 constexpr int64_t kOffWsI = 0;
-constexpr int64_t kBytesWsI = align256(kSlots * 7 * kRowCap * 4);
+constexpr int64_t kBytesWsI = align256(kSlots * kWsIntRows * kRowCap * 4);
 constexpr int64_t kOffWsF = kOffWsI + kBytesWsI;
-constexpr int64_t kBytesWsF = align256(kSlots * 4 * kRowCap * 8);
+constexpr int64_t kBytesWsF = align256(kSlots * kWsDblRows * kRowCap * 8);
 constexpr int64_t kOffRow = kOffWsF + kBytesWsF;
 constexpr int64_t kBytesRow = align256((kMaxVertices + 1) * 8);
 constexpr int64_t kOffItems = kOffRow + kBytesRow;
 constexpr int64_t kBytesItems = align256(kMaxVertices * (int64_t)sizeof(PlainItem));
-constexpr int64_t kOffCtl = kOffItems + kBytesItems;  // vtx_off[2], counter, epochs[2*kSlots], err
+constexpr int64_t kOffAcc = kOffItems + kBytesItems;  // fixed-point BC counters, kAccDigits per vertex
+constexpr int64_t kBytesAcc = align256(kMaxVertices * kAccDigits * 8);
+constexpr int64_t kOffCtl = kOffAcc + kBytesAcc;  // vtx_off[2], counter, epochs[2*kSlots], err
 constexpr int64_t kBytesCtl = align256(16 + 8 + 8 * kSlots + 4);
-constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // about 16 MiB
+constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // about 18 MiB
+static_assert(kMaxVertices <= kAccMaxAdds, "one call's sources must fit the fixed-point counters' headroom");
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -41,6 +45,7 @@ struct Layout {
   double *ws_f;
   int64_t *row;
   PlainItem *items;
+  unsigned long long *acc;
   int64_t *vtx_off;
   unsigned long long *counter;
   int32_t *epochs;
@@ -53,6 +58,7 @@ Layout layout(unsigned char *base) {
   L.ws_f = reinterpret_cast<double *>(base + kOffWsF);
   L.row = reinterpret_cast<int64_t *>(base + kOffRow);
   L.items = reinterpret_cast<PlainItem *>(base + kOffItems);
+  L.acc = reinterpret_cast<unsigned long long *>(base + kOffAcc);
   L.vtx_off = reinterpret_cast<int64_t *>(base + kOffCtl);
   L.counter = reinterpret_cast<unsigned long long *>(base + kOffCtl + 16);
   L.epochs = reinterpret_cast<int32_t *>(base + kOffCtl + 24);
@@ -60,12 +66,16 @@ Layout layout(unsigned char *base) {
   return L;
 }
 
-// Resets the per-call state held in the scratch array and builds the work
-// items: row offsets widened to int64, one item per source, epochs back to 1.
-// Malformed input (offsets, neighbour ids, sources) sets the error flag, and
-// the BC kernel then takes no work.
+// Builds the work items of one call: row offsets widened to int64, one item
+// per source. Malformed input (offsets, neighbour ids, sources) sets the error
+// flag, and the BC kernel then takes no work. On the first call on a device
+// (first != 0) it also sets the level-stamp epochs to 1; the workspace rows
+// and the fixed-point counters were cleared just before. Later calls keep the
+// epochs and stamps the previous call left (every stamp is below its row's
+// epoch, and the kernel wraps a row back to zero before an epoch could
+// overflow) and find the counters cleared by the previous call's fold.
 __global__ void setup_kernel(Layout L, const int32_t *R, const int32_t *C, int32_t n, int32_t m, const int32_t *src,
-                             int32_t nsrc) {
+                             int32_t nsrc, int first) {
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = tid; i <= n; i += stride) {
@@ -84,7 +94,7 @@ __global__ void setup_kernel(Layout L, const int32_t *R, const int32_t *C, int32
     }
     L.items[i] = PlainItem{0, s, 0, 0, 1};
   }
-  if (tid < 2 * kSlots) L.epochs[tid] = 1;
+  if (first && tid < 2 * kSlots) L.epochs[tid] = 1;
   if (tid == 0) {
     L.vtx_off[0] = 0;
     L.vtx_off[1] = n;
@@ -92,9 +102,13 @@ __global__ void setup_kernel(Layout L, const int32_t *R, const int32_t *C, int32
   }
 }
 
-// Device address of g_scratch per device, looked up once with that device current.
+// Device address of g_scratch per device, looked up once with that device
+// current; g_ready: the array's rows, epochs and counters are in the state a
+// finished call leaves (false before the first call and after a failed one,
+// which then clears them again).
 std::mutex g_mu;
 unsigned char *g_addr[64] = {nullptr};
+bool g_ready[64] = {false};
 
 }  // namespace
 }  // namespace bcg
@@ -119,6 +133,7 @@ extern "C" int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_
   ctx_device_stream(ctx, &dev, &stream, &e0, &e1);
   if (dev < 0 || dev >= 64 || cudaSetDevice(dev) != cudaSuccess) return BCGPU_ECUDA;
   unsigned char *base = nullptr;
+  bool first = false;
   {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_addr[dev]) {
@@ -131,16 +146,20 @@ extern "C" int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_
       g_addr[dev] = static_cast<unsigned char *>(p);
     }
     base = g_addr[dev];
+    first = !g_ready[dev];
+    g_ready[dev] = false;  // set again once this call has finished cleanly
   }
   const Layout L = layout(base);
   const bool timing = time_s != nullptr;
   if (timing) cudaEventRecord(e0, stream);
-  // the previous call's rows, stamps and error flag are still in the array: clear them
-  cudaError_t e = cudaMemsetAsync(L.ws_i, 0, (size_t)kBytesWsI, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(L.err, 0, sizeof(int), stream);
+  // the previous call's error flag is still in the array: clear it (and, on a
+  // device's first call or after a failed one, the rows and the counters)
+  cudaError_t e = cudaMemsetAsync(L.err, 0, sizeof(int), stream);
+  if (e == cudaSuccess && first) e = cudaMemsetAsync(L.ws_i, 0, (size_t)kBytesWsI, stream);
+  if (e == cudaSuccess && first) e = cudaMemsetAsync(L.acc, 0, (size_t)kBytesAcc, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(bc, 0, sizeof(double) * (size_t)n, stream);
   if (e == cudaSuccess) {
-    setup_kernel<<<64, 256, 0, stream>>>(L, R, C, n, m, req_nodes, n_req);
+    setup_kernel<<<64, 256, 0, stream>>>(L, R, C, n, m, req_nodes, n_req, first ? 1 : 0);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && n_req > 0) {
@@ -153,14 +172,16 @@ extern "C" int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_
     a.item_begin = 0;
     a.item_end = n_req;
     a.next_item = L.counter;
-    a.bc = bc;
+    a.acc = L.acc;
     a.ws_i = L.ws_i;
     a.ws_f = L.ws_f;
     a.ws_n = kRowCap;
     a.epochs = L.epochs;
-    a.rows_slot = kSlots - 1;
+    a.rows_slot = -1;  // no row export on this path (launch_rows is never called with these arguments)
+    a.rescale_exp = 900;
     a.err = L.err;
     e = launch_plain(a, 256, (int)std::min<int64_t>(kSlots, n_req), stream);
+    if (e == cudaSuccess) e = launch_fold(L.acc, bc, 0, n, stream);  // counters -> bc, counters cleared
   }
   int h_err = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -175,8 +196,13 @@ extern "C" int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_
     return BCGPU_ECUDA;
   }
   if (h_err != kDevOk) {
-    ctx_set_error(ctx, "bc_begin_free_noalloc: malformed CSR or source list (offsets, neighbour or source ids)");
-    return BCGPU_EINVAL;
+    const std::string msg = std::string("bc_begin_free_noalloc: ") +
+                            (h_err == kDevBadItem ? "malformed CSR or source list (offsets, neighbour or source ids)"
+                                                  : dev_err_text(h_err));
+    ctx_set_error(ctx, msg.c_str());
+    return dev_err_status(h_err);
   }
+  std::lock_guard<std::mutex> lock(g_mu);
+  g_ready[dev] = true;
   return BCGPU_OK;
 }

@@ -70,6 +70,11 @@ typedef struct bc_opts {
   int32_t lazy_tables;   /* 1: a one-shot bc_run_bccs_units call builds the multi-source slot,
                             seed and arming tables of the passes it runs only (and the source
                             order up to the last of them); 0 = of every pass */
+  int32_t wait_limit_ms; /* limit of one device-side wait (the multi-source kernel's grid
+                            barrier), in milliseconds of device time; a wait that runs out
+                            records an error and the run returns BCGPU_ETIMEOUT. 0 = 60000.
+                            No reference counterpart: the reference has no device-side
+                            waits and exit()s on any CUDA error (Codes/kernels.cuh:25-32). */
 } bc_opts;
 
 typedef struct bc_ctx bc_ctx;
@@ -181,6 +186,15 @@ int bc_begin_active(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, 
                     int32_t n_active, int32_t n_ears, const int32_t *lnode, const int32_t *rnode, const int32_t *cnt,
                     const int32_t *off, const int32_t *nodes, const int32_t *ld, const int32_t *rd,
                     const int32_t *reach, float *bc, double *time_s);
+
+/* Self-check of the bounded device-side wait (no reference counterpart): runs
+ * a one-CTA kernel whose thread 0 waits, with the same wait primitive as the
+ * multi-source kernel's grid barrier, on a device flag that nothing sets,
+ * with a limit of limit_ms (> 0) milliseconds. The wait runs out, so the call
+ * returns BCGPU_ETIMEOUT (the status a plan run returns when one of its waits
+ * runs out) and the context stays usable. *waited_ms (may be NULL) receives
+ * the device time the kernel took. */
+int bc_wait_probe(bc_ctx *ctx, int32_t limit_ms, double *waited_ms);
 
 /* ------------------------------------ device-resident plans (benchmark) -- */
 /* A plan uploads the packed BCCs once and keeps the BC accumulator on the

@@ -1,7 +1,7 @@
 // Test infrastructure only: the reference's own host pipeline driving libbcgpu
 // through centrality-gpu_b200/reference_binding/begin_gpupgm_bcgpu.cpp, i.e.
-// the reference's `betc` with its GPU files replaced as INTEGRATION.md
-// describes. Mirrors Codes/main.cpp:26-72 (same run_modified_apsp flags,
+// the reference's `betc` with its GPU files replaced by the binding to
+// libbcgpu. Mirrors Codes/main.cpp:26-72 (same run_modified_apsp flags,
 // :65) and prints the per-vertex BC that it leaves commented out (:45-49),
 // then the "GPU total time" line it prints (:70).
 #include "graph.h"

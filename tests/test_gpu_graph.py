@@ -62,7 +62,7 @@ def test_graph_replay_matches_oracle_on_grid(mode, delta, plain_core):
     for r0, r1 in parts:
         st = plan.run(r0, r1, stats=True)
         launches += st["kernel_launches"]
-    assert 1 <= launches <= 2 * len(parts)
+    assert 1 <= launches <= 3 * len(parts)  # multi-source kernel, per-source kernel, fold
     got = plan.read()
     assert rel_err(got, want) < TOL[delta]
     for r0, r1 in parts:  # second replay of the same graphs

@@ -119,7 +119,8 @@ def test_routing_between_the_schedules(stub_dir):
     """Twelve BA graphs with the core threshold at 500: the multi-source
     passes come first and hold exactly the sources of the five BCCs whose
     cores reach it; the per-source items hold the seven others; one run over
-    all units launches each schedule once. A deep BCC is routed
+    all units launches each schedule once, plus the fold of the per-source
+    schedule's fixed-point counters. A deep BCC is routed
     per-source by its depth alone (60x60 grid); forcing multi-source passes
     overrides it."""
     res = run_stub(stub_dir, """
@@ -156,7 +157,7 @@ out["grid_units"] = units
 """)
     assert res["big"] == 5 and res["passes_first"]
     assert res["pass_sources"] == res["big_vertices"]
-    assert res["launches"] == [2, 2]
+    assert res["launches"] == [3, 3]
     assert res["grid_core"] >= 100  # above the threshold given: only the depth routes it
     assert res["grid_units"]["auto"] == res["grid_units"]["plain"]
     assert res["grid_units"]["multi"] == -(-3600 // 128)
@@ -190,8 +191,8 @@ plan.close()
 c.close()
 """)
     assert res["after_record"] == 0
-    assert res["replays"] == [2, 2, 2]
-    assert res["fresh"] == 2
+    assert res["replays"] == [3, 3, 3]
+    assert res["fresh"] == 3
     assert res["refused"] is not None and res["refused"][0] == 1
 
 
