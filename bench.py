@@ -189,10 +189,11 @@ def traffic_per_source(mode, workload):
     return (float(m.group(1)), f"profiles/{name}") if m else (None, None)
 
 
-def plain_sample(P, d, device, stream, waves, batched_gteps):
+def plain_sample(P, d, device, stream, waves, batched_gteps, whole=False):
     """Times the plain FP64 schedule (one source per CTA) on `waves` full
     waves of its work items, taken from two places in the largest BCC's item
-    list, with CUDA events; returns its TEPS and the batched/plain ratio."""
+    list (or on all its items when `whole`), with CUDA events; returns its TEPS
+    and the batched/plain ratio."""
     import torch
     pctx = P.Context(mode=P.MODE_PLAIN, device=device, stream=stream.cuda_stream)
     pplan = pctx.plan(d)
@@ -201,6 +202,8 @@ def plain_sample(P, d, device, stream, waves, batched_gteps):
     n = pplan.n_units
     picks = [(max(0, int(f * n) - per // 2), max(0, int(f * n) - per // 2) + per) for f in (0.25, 0.75)]
     picks = [(a, min(n, b)) for a, b in picks]
+    if whole:
+        picks = [(0, n)]
     pplan.run(picks[0][0], min(picks[0][1], picks[0][0] + slots), stats=False)  # warm-up wave
     torch.cuda.synchronize()
     ms = teps = src = 0.0
@@ -219,7 +222,8 @@ def plain_sample(P, d, device, stream, waves, batched_gteps):
     g = teps / (ms * 1e-3) / 1e9
     return {"value": g, "unit": "GTEPS", "dtype": "f64", "items": sum(b - a for a, b in picks), "sources": int(src),
             "ms": ms, "resident_ctas": slots, "batched_over_plain": batched_gteps / g,
-            "sample": f"{waves} full waves of plain work items ({slots} resident CTAs) at 25% and 75% of the item list"}
+            "sample": "every plain work item (the whole workload)" if whole else
+                      f"{waves} full waves of plain work items ({slots} resident CTAs) at 25% and 75% of the item list"}
 
 
 def run_reference(args):
@@ -265,12 +269,12 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="sources per multi-source pass (0 = autotune)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat20")
     ap.add_argument("--step-sources", type=int, default=0, help="sources per step (0 = by workload and mode)")
-    ap.add_argument("--e2e-steps", type=int, default=2,
+    ap.add_argument("--e2e-steps", type=int, default=5,
                     help="steps timed end to end through bc_run_bccs_units with host buffers (0 = skip)")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="--impl reference: seconds of CPU work per step (its sources are sized to it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plain-waves", type=int, default=2,
+    ap.add_argument("--plain-waves", type=int, default=6,
                     help="batched runs: also time the plain FP64 schedule on this many full waves of its work "
                          "items (one item per resident CTA), the denominator of batched vs plain (0 = skip)")
     ap.add_argument("--graph", type=int, choices=[0, 1], default=1,
@@ -282,6 +286,9 @@ def main():
                          "BCGPU_LIB_DIR=centrality-gpu_b200/lib_phase)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
+    ap.add_argument("--tile-max", type=int, default=0,
+                    help="small-BCC schedule: largest BCC it takes (bc_opts.tile_max; 0 = as large as shared "
+                         "memory allows, -1 = off)")
     ap.add_argument("--plain-ctas", type=int, choices=[0, 4, 8, 16], default=0,
                     help="per-source schedule (and BCCs routed to it): CTAs per SM (bc_opts.plain_ctas_per_sm; "
                          "0 = the library's choice, four of 256 threads)")
@@ -358,11 +365,13 @@ def main():
             width = int(wt.item())
     ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30), graph=bool(args.graph),
-                    plain_ctas_per_sm=args.plain_ctas, lazy_tables=args.lazy_tables)
+                    plain_ctas_per_sm=args.plain_ctas, lazy_tables=args.lazy_tables, tile_max=args.tile_max)
     plan = ctx.plan(d)
     # steps of this many sources, small enough that every rank gets at least one
     total_sources = plan.unit_work(0, plan.n_units)[0]
-    target = args.step_sources or (8192 if mode == P.MODE_BATCHED else 512)
+    # the batch of independent graphs runs whole, in one launch per schedule
+    whole = args.workload == "ba"
+    target = args.step_sources or (total_sources if whole else 8192 if mode == P.MODE_BATCHED else 512)
     target = max(1, min(target, total_sources // world))
     ranges = step_ranges(plan, target)
     if len(ranges) < world:  # the same on every rank (same plan): all stop here, before any collective
@@ -470,7 +479,7 @@ def main():
 
     plain = None
     if rank == 0 and world == 1 and mode == P.MODE_BATCHED and args.plain_waves > 0:
-        plain = plain_sample(P, d, local, stream, args.plain_waves, value)
+        plain = plain_sample(P, d, local, stream, args.plain_waves, value, whole=whole)
 
     cpu = None
     accuracy = None
@@ -500,6 +509,7 @@ def main():
                        "batch_width": st.get("batch_width"), "autotune_gteps": tuned,
                        "cuda_graph": bool(args.graph), "gpu_decomposition": decomp,
                        "plain_ctas_per_sm": args.plain_ctas or None, "lazy_tables": bool(args.lazy_tables),
+                       "tile_max": args.tile_max,
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "plain": plain,

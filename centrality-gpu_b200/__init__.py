@@ -44,7 +44,7 @@ class BcOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("delta", C.c_int32), ("batch_width", C.c_int32),
                 ("stream", C.c_void_p), ("workspace_limit", C.c_int64), ("rescale_exp", C.c_int32),
                 ("plain_core", C.c_int32), ("graph", C.c_int32), ("plain_ctas_per_sm", C.c_int32),
-                ("lazy_tables", C.c_int32), ("wait_limit_ms", C.c_int32)]
+                ("lazy_tables", C.c_int32), ("tile_max", C.c_int32), ("wait_limit_ms", C.c_int32)]
 
 
 class BcBccs(C.Structure):
@@ -262,7 +262,7 @@ class Context:
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
                  workspace_limit=0, rescale_exp=0, plain_core=0, graph=False, plain_ctas_per_sm=0,
-                 lazy_tables=False, wait_limit_ms=0):
+                 lazy_tables=False, tile_max=0, wait_limit_ms=0):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device
@@ -274,6 +274,7 @@ class Context:
         o.plain_ctas_per_sm = plain_ctas_per_sm
         o.lazy_tables = 1 if lazy_tables else 0
         o.wait_limit_ms = wait_limit_ms
+        o.tile_max = tile_max
         h = C.c_void_p()
         rc = lib().bc_create(C.byref(o), C.byref(h))
         if rc:

@@ -27,7 +27,7 @@ CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopen
                    "-ccbin", HOSTCXX, "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-I" + str(INC), "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["kernels_plain.cu", "kernels_batched.cu", "bcgpu.cu", "noalloc.cu", "decomp_steps.cu"]
+CU_SOURCES = ["kernels_plain.cu", "kernels_batched.cu", "kernels_tile.cu", "bcgpu.cu", "noalloc.cu", "decomp_steps.cu"]
 CXX_SOURCES = ["host_decomp.cpp"]
 
 

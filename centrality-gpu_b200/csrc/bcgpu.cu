@@ -11,8 +11,10 @@
 #include "common.cuh"
 #include "internal.h"
 #include "plain.h"
+#include "tile.h"
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -61,6 +63,19 @@ struct bc_plan {
   double *ws_f = nullptr;
   int64_t ws_n = 0;
   int grid = 0, block = 1024;
+  // small-BCC schedule (BATCHED plans): units [n_bat + n_items, ...) are its items
+  bcg::TileItem *titems = nullptr;
+  std::vector<bcg::TileItem> h_titems;
+  int64_t n_titems = 0;
+  unsigned char *slices = nullptr;
+  int64_t *slice_off = nullptr;
+  int32_t *slice_bytes = nullptr;
+  int32_t *tws_S = nullptr, *tws_lv = nullptr;
+  double *tws_sq = nullptr;
+  int64_t tcap = 0;
+  int32_t tnmax = 0, tslice_max = 0;
+  size_t tsmem = 0;
+  int tgrid = 0;
   // BATCHED: multi-source passes are units [0, n_bat); the BCCs routed to
   // the per-source schedule follow as PLAIN items
   bcg::BatchedPlan *bp = nullptr;
@@ -204,6 +219,11 @@ int validate(bc_ctx *ctx, const bc_bccs *B) {
   return BCGPU_OK;
 }
 
+// Bytes of the fixed-point BC counters of n packed vertices, as dalloc sizes them.
+size_t acc_bytes(int64_t n) {
+  return sizeof(unsigned long long) * (size_t)std::max<int64_t>(bcg::kAccDigits * n, 1);
+}
+
 // Limit of one device-side wait, from bc_opts.wait_limit_ms.
 unsigned long long wait_ns(const bc_ctx *ctx) {
   return ctx->opts.wait_limit_ms > 0 ? (unsigned long long)ctx->opts.wait_limit_ms * 1000000ull : bcg::kDefaultWaitNs;
@@ -291,6 +311,128 @@ void plain_items(const bc_bccs *B, std::vector<bcg::PlainItem> &items, const std
   }
 }
 
+// The fixed-point BC counters (once per plan), cleared.
+int alloc_acc(bc_plan *p, int64_t n_packed) {
+  if (p->acc) return BCGPU_OK;
+  int rc = dalloc(p, &p->acc, bcg::kAccDigits * n_packed);
+  if (rc) return rc;
+  if (cudaMemsetAsync(p->acc, 0, acc_bytes(n_packed), p->ctx->stream) != cudaSuccess)
+    return cuda_fail(p->ctx, cudaGetLastError(), "cudaMemsetAsync");
+  return BCGPU_OK;
+}
+
+// Sources per small-BCC work item: a CTA's warps take them one at a time, so
+// an item is several rounds of kTileWarps sources (larger BCCs are split so
+// that many CTAs share them).
+constexpr int32_t kTileItemSources = 128;
+
+// Which BCCs (of those not in multi-source passes) take the small-BCC
+// schedule: at most opts.tile_max vertices, shared memory for the CTA's
+// counters, level rows and slice within the device's per-CTA limit, and no
+// FP64 overflow possible without per-level scaling -- a BFS from any vertex
+// has at most 2 ecc(0) + 1 levels and a path count on level l is at most
+// maxdeg^l, so (2 ecc(0) + 1) log2(maxdeg) <= 1000 keeps every count below
+// 2^1000. Candidates are taken smallest first while the launch's shared
+// memory (sized by the largest BCC and the largest slice) still fits.
+void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std::vector<char> &tile) {
+  tile.assign((size_t)B->n_bcc, 0);
+  const size_t lim = bcg::tile_smem_limit(ctx->device);
+  if (lim == 0) return;
+  const int64_t cap = ctx->opts.tile_max > 0 ? ctx->opts.tile_max : INT32_MAX;
+  std::vector<int64_t> bytes((size_t)B->n_bcc, 0);
+  std::vector<char> ok((size_t)B->n_bcc, 0);
+#pragma omp parallel
+  {
+    std::vector<int32_t> dist, queue;
+#pragma omp for schedule(dynamic, 16)
+    for (int32_t b = 0; b < B->n_bcc; ++b) {
+      if (on[b]) continue;
+      const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
+      const int64_t arcs = B->row[vo + nb] - B->row[vo];
+      bytes[b] = bcg::TileSlice::bytes(nb, arcs);
+      if (nb > cap || bcg::tile_smem_bytes(nb, bytes[b]) > lim) continue;
+      int64_t maxdeg = 1;
+      for (int64_t k = vo; k < vo + nb; ++k) maxdeg = std::max(maxdeg, B->row[k + 1] - B->row[k]);
+      const int ecc = bcc_ecc0(B, b, dist, queue, false);
+      ok[b] = (2.0 * ecc + 1.0) * std::log2((double)std::max<int64_t>(maxdeg, 2)) <= 1000.0;
+    }
+  }
+  std::vector<int32_t> cand;
+  for (int32_t b = 0; b < B->n_bcc; ++b)
+    if (ok[b]) cand.push_back(b);
+  std::stable_sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) {
+    return B->vtx_off[x + 1] - B->vtx_off[x] < B->vtx_off[y + 1] - B->vtx_off[y];
+  });
+  int64_t nmax = 0, smax = 0;
+  for (int32_t b : cand) {
+    const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+    if (bcg::tile_smem_bytes(std::max(nmax, nb), std::max(smax, bytes[b])) > lim) break;
+    nmax = std::max(nmax, nb);
+    smax = std::max(smax, bytes[b]);
+    tile[b] = 1;
+  }
+}
+
+// Work items, staged slices and warp workspace of the small-BCC schedule.
+int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &tile, bc_plan *p) {
+  int rc = BCGPU_OK;
+  std::vector<int64_t> off((size_t)B->n_bcc, -1);
+  std::vector<int32_t> size((size_t)B->n_bcc, 0);
+  int64_t total = 0, nmax = 0, smax = 0;
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    if (!tile[b]) continue;
+    const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
+    const int64_t arcs = B->row[vo + nb] - B->row[vo];
+    off[b] = total;
+    size[b] = (int32_t)bcg::TileSlice::bytes(nb, arcs);
+    total += size[b];
+    nmax = std::max(nmax, nb);
+    smax = std::max<int64_t>(smax, size[b]);
+    for (int32_t s0 = 0; s0 < nb; s0 += kTileItemSources)
+      p->h_titems.push_back({b, s0, (int32_t)std::min<int64_t>(nb, s0 + kTileItemSources), 0});
+  }
+  // slices: local row offsets, neighbours, reach (int32, 16-byte aligned parts)
+  std::vector<unsigned char> blob((size_t)std::max<int64_t>(total, 16), 0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    if (!tile[b]) continue;
+    const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo, e0 = B->row[vo];
+    const int64_t arcs = B->row[vo + nb] - e0;
+    int32_t *R = reinterpret_cast<int32_t *>(blob.data() + off[b]);
+    int32_t *C = reinterpret_cast<int32_t *>(blob.data() + off[b] + bcg::TileSlice::col_at(nb));
+    int32_t *W = reinterpret_cast<int32_t *>(blob.data() + off[b] + bcg::TileSlice::reach_at(nb, arcs));
+    for (int64_t v = 0; v <= nb; ++v) R[v] = (int32_t)(B->row[vo + v] - e0);
+    for (int64_t e = 0; e < arcs; ++e) C[e] = B->col[e0 + e];
+    for (int64_t v = 0; v < nb; ++v) W[v] = B->reach[vo + v];
+  }
+  p->n_titems = (int64_t)p->h_titems.size();
+  p->tnmax = (int32_t)nmax;
+  p->tslice_max = (int32_t)smax;
+  p->tsmem = bcg::tile_smem_bytes(nmax, smax);
+  const int per_sm = bcg::tile_ctas_per_sm(p->tsmem);
+  if (per_sm < 1) return fail(ctx, BCGPU_ECUDA, "small-BCC schedule: no CTA fits an SM");
+  p->tgrid = ctx->sms * per_sm;
+  p->tcap = nmax + 2;
+  const int64_t slots = (int64_t)p->tgrid * bcg::kTileWarps;
+  if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) || (rc = upload(p, &p->slice_off, off.data(), B->n_bcc)) ||
+      (rc = upload(p, &p->slice_bytes, size.data(), B->n_bcc)) ||
+      (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) ||
+      (rc = dalloc(p, &p->tws_S, slots * p->tcap)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
+      (rc = dalloc(p, &p->tws_sq, slots * p->tcap)) || (rc = alloc_acc(p, B->n_packed)))
+    return rc;
+  for (const auto &it : p->h_titems) {
+    const int64_t vo = B->vtx_off[it.bcc], nb = B->vtx_off[it.bcc + 1] - vo;
+    const int64_t arcs = B->row[vo + nb] - B->row[vo];
+    const int64_t src = it.s1 - it.s0;
+    p->unit_sources.push_back(p->unit_sources.back() + src);
+    p->unit_teps.push_back(p->unit_teps.back() + src * arcs);
+    p->unit_bfs.push_back(p->unit_bfs.back() + src);
+    p->unit_aux.push_back(p->unit_aux.back());
+    p->unit_visits.push_back(p->unit_visits.back() + src * nb);
+  }
+  return BCGPU_OK;
+}
+
 // Fills plan p (allocated by create_plan, which releases it on any failure).
 // fill_begin/fill_end: the multi-source passes (units) whose tables are built
 // (a one-shot call that runs only those); default all.
@@ -356,12 +498,21 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     }
     for (char x : on) n_on += x;
   }
+  // BATCHED: BCCs off the multi-source passes that fit the small-BCC schedule
+  std::vector<char> tile;
+  int64_t n_tile = 0;
+  if (p->mode == BCGPU_MODE_BATCHED && ctx->opts.tile_max >= 0 && n_on < B->n_bcc) {
+    route_tiles(ctx, B, on, tile);
+    for (char x : tile) n_tile += x;
+  }
   std::vector<bcg::PlainItem> items;
   if (p->mode == BCGPU_MODE_PLAIN) {
     if (override_items) items = *override_items;
     else plain_items(B, items);
-  } else if (n_on < B->n_bcc) {
-    plain_items(B, items, &on);
+  } else if (n_on + n_tile < B->n_bcc) {
+    std::vector<char> skip(on);
+    for (int32_t b = 0; b < B->n_bcc; ++b) skip[b] |= n_tile ? tile[b] : 0;
+    plain_items(B, items, &skip);
   }
   if (p->mode == BCGPU_MODE_BATCHED && n_on > 0) {
     bcg::BatchedConfig cfg;
@@ -412,10 +563,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     if ((rc = upload(p, &p->items, items.data(), (int64_t)items.size()))) return bail(rc);
     p->h_items = items;
     p->ws_n = (p->mode == BCGPU_MODE_PLAIN ? nb_max : nb_plain) + 2;
-    if ((rc = dalloc(p, &p->acc, bcg::kAccDigits * B->n_packed))) return bail(rc);
-    if (cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * bcg::kAccDigits * (size_t)std::max<int64_t>(B->n_packed, 1),
-                        ctx->stream) != cudaSuccess)
-      return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
+    if ((rc = alloc_acc(p, B->n_packed))) return bail(rc);
     const int64_t per_slot = p->ws_n * (bcg::kWsIntRows * 4 + bcg::kWsDblRows * 8);
     // Four 256-thread CTAs per SM (four sources in flight) when their rows
     // fit the budget, else two of 512, else one of 1024 per SM; with
@@ -443,6 +591,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
     p->h2d_bytes += (int64_t)(sizeof(int32_t) * ep.size());
   }
+  if (n_tile && (rc = build_tiles(ctx, B, tile, p))) return bail(rc);
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return BCGPU_OK;
 }
@@ -690,12 +839,17 @@ extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t
   std::vector<int64_t> ids;
   try {
     if (p->bp && begin < p->n_bat) bcg::batched_unit_sources(p->bp, begin, std::min(end, p->n_bat), ids);
-    for (int64_t i = std::max(begin, p->n_bat) - p->n_bat; i < end - p->n_bat; ++i) {  // per-source items
-      const auto &it = p->h_items[i];
+    for (int64_t i = std::max(begin, p->n_bat) - p->n_bat; i < std::min(end - p->n_bat, p->n_items); ++i) {
+      const auto &it = p->h_items[i];  // per-source items
       const int64_t vo = p->h_vtx_off[it.bcc];
       if (it.own) ids.push_back(vo + it.src);
       for (int32_t c = it.c0; c < it.c1; ++c)
         for (int32_t k = 0; k < p->h_chain_len[c]; ++k) ids.push_back(vo + p->h_chain_start[c] + k);
+    }
+    for (int64_t i = std::max(begin, p->n_bat + p->n_items) - p->n_bat - p->n_items;
+         i < end - p->n_bat - p->n_items; ++i) {  // small-BCC items
+      const auto &it = p->h_titems[i];
+      for (int32_t s = it.s0; s < it.s1; ++s) ids.push_back(p->h_vtx_off[it.bcc] + s);
     }
   } catch (const std::bad_alloc &) {
     return -BCGPU_ENOMEM;
@@ -709,8 +863,7 @@ extern "C" int bc_plan_reset(bc_plan *p) {
   CK(p->ctx, cudaSetDevice(p->ctx->device));
   CK(p->ctx, cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(p->n_packed, 1), p->ctx->stream));
   if (p->acc)  // folded after every launch, so normally zero already; cleared after a failed run
-    CK(p->ctx, cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * bcg::kAccDigits * (size_t)std::max<int64_t>(p->n_packed, 1),
-                               p->ctx->stream));
+    CK(p->ctx, cudaMemsetAsync(p->acc, 0, acc_bytes(p->n_packed), p->ctx->stream));
   CK(p->ctx, cudaMemsetAsync(p->err, 0, sizeof(int), p->ctx->stream));
   return BCGPU_OK;
 }
@@ -738,7 +891,7 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
     int rc = bcg::batched_run(p->bp, begin, std::min(end, p->n_bat), ctx->stream, launches, &msg);
     if (rc) return fail(ctx, rc, "batched run: " + msg);
   }
-  const int64_t i0 = std::max(begin, p->n_bat) - p->n_bat, i1 = end - p->n_bat;
+  const int64_t i0 = std::max(begin, p->n_bat) - p->n_bat, i1 = std::min(end - p->n_bat, p->n_items);
   // per-source items, in launches of at most kAccMaxAdds sources (the adds one
   // fixed-point counter takes between folds); each launch is followed by the
   // fold of the counters of the BCCs it touched
@@ -759,6 +912,27 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
     CK(ctx, bcg::launch_fold(p->acc, p->bc, p->h_vtx_off[b0], p->h_vtx_off[b1 + 1], ctx->stream));
     *launches += 2;
     j0 = j1;
+  }
+  // small-BCC items: one launch (each BCC's sources are far fewer than
+  // kAccMaxAdds), then the fold of the BCCs it touched
+  const int64_t t0 = std::max(begin, p->n_bat + p->n_items) - p->n_bat - p->n_items;
+  const int64_t t1 = end - p->n_bat - p->n_items;
+  if (t1 > t0) {
+    int32_t b0 = INT32_MAX, b1 = -1;
+    for (int64_t j = t0; j < t1; ++j) {
+      b0 = std::min(b0, p->h_titems[j].bcc);
+      b1 = std::max(b1, p->h_titems[j].bcc);
+    }
+    CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
+    bcg::TileArgs a{};
+    a.vtx_off = p->vtx_off; a.slices = p->slices; a.slice_off = p->slice_off; a.slice_bytes = p->slice_bytes;
+    a.items = p->titems; a.item_begin = t0; a.item_end = t1; a.next_item = p->counter; a.acc = p->acc;
+    a.ws_S = p->tws_S; a.ws_lv = p->tws_lv; a.ws_sq = p->tws_sq; a.cap = p->tcap; a.nmax = p->tnmax;
+    a.slice_max = p->tslice_max; a.wait_ns = wait_ns(ctx); a.err = p->err;
+    const int grid = (int)std::min<int64_t>(p->tgrid, t1 - t0);
+    CK(ctx, bcg::launch_tile(a, grid, p->tsmem, ctx->stream));
+    CK(ctx, bcg::launch_fold(p->acc, p->bc, p->h_vtx_off[b0], p->h_vtx_off[b1 + 1], ctx->stream));
+    *launches += 2;
   }
   return BCGPU_OK;
 }

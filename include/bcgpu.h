@@ -70,6 +70,14 @@ typedef struct bc_opts {
   int32_t lazy_tables;   /* 1: a one-shot bc_run_bccs_units call builds the multi-source slot,
                             seed and arming tables of the passes it runs only (and the source
                             order up to the last of them); 0 = of every pass */
+  int32_t tile_max;      /* BATCHED: BCCs routed away from multi-source passes run on the
+                            small-BCC schedule (a CTA per range of sources of one BCC, its CSR
+                            slice staged in shared memory by a bulk copy, one warp per source)
+                            when they have at most tile_max vertices, fit shared memory and
+                            cannot overflow FP64 path counts; the others use the per-source
+                            schedule. 0 = as large as shared memory allows, -1 = off.
+                            No reference counterpart (one source per CTA for every BCC,
+                            Codes/begin_gpupgm.cu:52-65). */
   int32_t wait_limit_ms; /* limit of one device-side wait (the multi-source kernel's grid
                             barrier), in milliseconds of device time; a wait that runs out
                             records an error and the run returns BCGPU_ETIMEOUT. 0 = 60000.

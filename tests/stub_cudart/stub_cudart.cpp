@@ -131,7 +131,10 @@ cudaError_t cudaGetDeviceProperties_v2(cudaDeviceProp *prop, int device) {
   return cudaSuccess;
 }
 cudaError_t cudaDeviceGetAttribute(int *value, cudaDeviceAttr attr, int) {
-  *value = attr == cudaDevAttrMultiProcessorCount ? 148 : attr == cudaDevAttrCooperativeLaunch ? 1 : 0;
+  *value = attr == cudaDevAttrMultiProcessorCount        ? 148
+           : attr == cudaDevAttrCooperativeLaunch        ? 1
+           : attr == cudaDevAttrMaxSharedMemoryPerBlockOptin ? 232448  // B200: 227 KB per CTA
+                                                         : 0;
   return cudaSuccess;
 }
 cudaError_t cudaFuncSetAttribute(const void *, cudaFuncAttribute, int) { return cudaSuccess; }

@@ -86,6 +86,7 @@ graphs_ = [("small2000", G.gen_small(1)),
            ("ba12", G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3])]
 graphs_ += [(c, load_case(c)[:3]) for c in GOLDEN_CASES]
 modes = [dict(mode=P.MODE_PLAIN), dict(mode=P.MODE_PLAIN, plain_ctas_per_sm=16), dict(mode=P.MODE_BATCHED),
+         dict(mode=P.MODE_BATCHED, tile_max=-1), dict(mode=P.MODE_BATCHED, tile_max=300),
          dict(mode=P.MODE_BATCHED, plain_core=500, plain_ctas_per_sm=8),
          dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=32),
          dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=128),
@@ -122,14 +123,14 @@ def test_routing_between_the_schedules(stub_dir):
     all units launches each schedule once, plus the fold of the per-source
     schedule's fixed-point counters. A deep BCC is routed
     per-source by its depth alone (60x60 grid); forcing multi-source passes
-    overrides it."""
+    overrides it. (The small-BCC schedule is off here: tile_max -1.)"""
     res = run_stub(stub_dir, """
 n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
 d = decomp(n, u, v)
 a = d.arrays()
 big = [b for b in range(a["n_bcc"]) if a["n_plain"][b] >= 500]
 owner = np.repeat(np.arange(a["n_bcc"]), np.diff(a["vtx_off"]))
-ctx = P.Context(mode=P.MODE_BATCHED, plain_core=500)
+ctx = P.Context(mode=P.MODE_BATCHED, plain_core=500, tile_max=-1)
 plan = ctx.plan(d)
 kinds = [bool(np.isin(owner[plan.unit_sources(k, k + 1)], big).all()) for k in range(plan.n_units)]
 first_item = kinds.index(False)
@@ -145,7 +146,7 @@ ctx.close()
 g = decomp(*G.gen_grid(60, delete_frac=0.0, sub_p=0.0, leaves=0, seed=9))  # levels deeper than 96 from any vertex
 ga = g.arrays()
 units = {}
-for name, opts in (("plain", dict(mode=P.MODE_PLAIN)), ("auto", dict(mode=P.MODE_BATCHED, plain_core=100)),
+for name, opts in (("plain", dict(mode=P.MODE_PLAIN)), ("auto", dict(mode=P.MODE_BATCHED, plain_core=100, tile_max=-1)),
                    ("multi", dict(mode=P.MODE_BATCHED, plain_core=-1, batch_width=128))):
     c = P.Context(**opts)
     p = c.plan(g)
@@ -163,6 +164,49 @@ out["grid_units"] = units
     assert res["grid_units"]["multi"] == -(-3600 // 128)
 
 
+def test_small_bccs_take_the_tile_schedule(stub_dir):
+    """BATCHED plan of twelve BA graphs (every core under the multi-source
+    threshold): with tile_max 600 the BCCs of at most 600 vertices become
+    small-BCC items of at most 128 sources each, listed after the per-source
+    items of the larger BCCs; one run over all units launches the per-source
+    kernel, the tile kernel and one counter fold after each; with tile_max -1
+    every BCC stays per-source."""
+    res = run_stub(stub_dir, """
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
+d = decomp(n, u, v)
+a = d.arrays()
+nb = np.diff(a["vtx_off"])
+owner = np.repeat(np.arange(a["n_bcc"]), nb)
+ctx = P.Context(mode=P.MODE_BATCHED, tile_max=600)
+plan = ctx.plan(d)
+sizes = [int(nb[owner[plan.unit_sources(k, k + 1)]].max()) for k in range(plan.n_units)]
+counts = [int(plan.unit_work(k, k + 1)[0]) for k in range(plan.n_units)]
+small = [s <= 600 for s in sizes]
+first = small.index(True) if True in small else len(small)
+out["order"] = all(not x for x in small[:first]) and all(small[first:])
+out["small_units"] = len(small) - first
+out["small_bccs"] = int((nb <= 600).sum())
+out["max_small_unit"] = max(counts[first:]) if first < len(counts) else 0
+l0 = L.stub_cudart_launches()
+st = plan.run()
+out["launches"] = [st["kernel_launches"], L.stub_cudart_launches() - l0]
+plan.close()
+ctx.close()
+ctx = P.Context(mode=P.MODE_BATCHED, tile_max=-1)
+plan = ctx.plan(d)
+out["off_units"] = plan.n_units
+out["off_launches"] = plan.run()["kernel_launches"]
+plan.close()
+ctx.close()
+out["n_bcc"] = int(a["n_bcc"])
+out["n_packed"] = int(a["n_packed"])
+""")
+    assert res["order"] and res["small_bccs"] > 0 and res["small_units"] >= res["small_bccs"]
+    assert 0 < res["max_small_unit"] <= 128
+    assert res["launches"] == [4, 4]  # per-source kernel + fold, tile kernel + fold
+    assert res["off_launches"] == 2 and res["off_units"] < res["n_packed"]
+
+
 def test_graph_mode_records_then_replays(stub_dir):
     """Recording enqueues nothing; each replay of a recorded range launches
     what the range holds; a range run without recording is recorded on its
@@ -170,7 +214,7 @@ def test_graph_mode_records_then_replays(stub_dir):
     res = run_stub(stub_dir, """
 n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]  # both schedules at this threshold
 d = decomp(n, u, v)
-c = P.Context(mode=P.MODE_BATCHED, plain_core=500, graph=True)
+c = P.Context(mode=P.MODE_BATCHED, plain_core=500, graph=True, tile_max=-1)
 plan = c.plan(d)
 k = plan.n_units
 l0 = L.stub_cudart_launches()
