@@ -63,19 +63,27 @@ struct bc_plan {
   double *ws_f = nullptr;
   int64_t ws_n = 0;
   int grid = 0, block = 1024;
-  // small-BCC schedule (BATCHED plans): units [n_bat + n_items, ...) are its items
+  // small-BCC schedule (BATCHED plans): units [n_bat + n_items, ...) are its
+  // items, those of the warp class first, then those of the CTA class
   bcg::TileItem *titems = nullptr;
   std::vector<bcg::TileItem> h_titems;
   int64_t n_titems = 0;
   unsigned char *slices = nullptr;
   int64_t *slice_off = nullptr;
   int32_t *slice_bytes = nullptr;
-  int32_t *tws_S = nullptr, *tws_lv = nullptr;
-  double *tws_sq = nullptr;
+  int32_t *tws_lv = nullptr;  // warp class: level offsets per warp slot
+  // one launch per class and shared-memory bucket (the CTA class in buckets
+  // by resident CTAs per SM, so that small BCCs are not run at the
+  // occupancy of the largest)
+  struct TileLaunch {
+    int cls = 0;
+    int64_t i0 = 0, i1 = 0;  // its items in h_titems
+    int32_t nmax = 0, slice_max = 0;
+    size_t smem = 0;
+    int grid = 0;
+  };
+  std::vector<TileLaunch> tl;
   int64_t tcap = 0;
-  int32_t tnmax = 0, tslice_max = 0;
-  size_t tsmem = 0;
-  int tgrid = 0;
   // BATCHED: multi-source passes are units [0, n_bat); the BCCs routed to
   // the per-source schedule follow as PLAIN items
   bcg::BatchedPlan *bp = nullptr;
@@ -321,26 +329,34 @@ int alloc_acc(bc_plan *p, int64_t n_packed) {
   return BCGPU_OK;
 }
 
-// Sources per small-BCC work item: a CTA's warps take them one at a time, so
-// an item is several rounds of kTileWarps sources (larger BCCs are split so
-// that many CTAs share them).
+// Sources per small-BCC work item: the CTA runs them (a warp each, or one
+// after another) from one staged slice; larger BCCs are split so that many
+// CTAs share them.
 constexpr int32_t kTileItemSources = 128;
+// BCCs of up to this many vertices take the warp class (a warp per source,
+// eight per CTA); larger ones the CTA class (the CTA on one source).
+constexpr int64_t kTileWarpMaxVertices = 640;
 
-// Which BCCs (of those not in multi-source passes) take the small-BCC
-// schedule: at most opts.tile_max vertices, shared memory for the CTA's
-// counters, level rows and slice within the device's per-CTA limit, and no
-// FP64 overflow possible without per-level scaling -- a BFS from any vertex
-// has at most 2 ecc(0) + 1 levels and a path count on level l is at most
-// maxdeg^l, so (2 ecc(0) + 1) log2(maxdeg) <= 1000 keeps every count below
-// 2^1000. Candidates are taken smallest first while the launch's shared
-// memory (sized by the largest BCC and the largest slice) still fits.
-void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std::vector<char> &tile) {
-  tile.assign((size_t)B->n_bcc, 0);
+// Small-BCC class of each BCC (-1: not in the schedule): BCCs off the
+// multi-source passes with at most opts.tile_max vertices whose CTA fits the
+// device's shared memory and whose path counts cannot overflow FP64 without
+// per-level scaling -- a BFS from any vertex has at most 2 ecc(0) + 1 levels
+// and a path count on level l is at most maxdeg^l, so
+// (2 ecc(0) + 1) log2(maxdeg) <= 1000 keeps every count below 2^1000 (and the
+// levels below the CTA class's level table). Within a class, candidates are
+// taken smallest first while the launch's shared memory (sized by the class's
+// largest BCC and largest slice) still fits.
+// The variant whose shared memory bounds a class's (the CTA class's largest
+// block has the largest work queue).
+int fit_cls(int c) { return c == bcg::kTileWarp ? c : bcg::kTileCta1024; }
+
+void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std::vector<int8_t> &cls) {
+  cls.assign((size_t)B->n_bcc, -1);
   const size_t lim = bcg::tile_smem_limit(ctx->device);
   if (lim == 0) return;
-  const int64_t cap = ctx->opts.tile_max > 0 ? ctx->opts.tile_max : INT32_MAX;
+  const int64_t cap = std::min<int64_t>(ctx->opts.tile_max > 0 ? ctx->opts.tile_max : INT32_MAX, bcg::kTileMaxVertices);
   std::vector<int64_t> bytes((size_t)B->n_bcc, 0);
-  std::vector<char> ok((size_t)B->n_bcc, 0);
+  std::vector<int8_t> want((size_t)B->n_bcc, -1);
 #pragma omp parallel
   {
     std::vector<int32_t> dist, queue;
@@ -350,75 +366,100 @@ void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std
       const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
       const int64_t arcs = B->row[vo + nb] - B->row[vo];
       bytes[b] = bcg::TileSlice::bytes(nb, arcs);
-      if (nb > cap || bcg::tile_smem_bytes(nb, bytes[b]) > lim) continue;
+      if (nb > cap) continue;
+      const int c = nb <= kTileWarpMaxVertices ? bcg::kTileWarp : bcg::kTileCta;
+      if (bcg::tile_smem_bytes(fit_cls(c), nb, bytes[b]) > lim) continue;
       int64_t maxdeg = 1;
       for (int64_t k = vo; k < vo + nb; ++k) maxdeg = std::max(maxdeg, B->row[k + 1] - B->row[k]);
       const int ecc = bcc_ecc0(B, b, dist, queue, false);
-      ok[b] = (2.0 * ecc + 1.0) * std::log2((double)std::max<int64_t>(maxdeg, 2)) <= 1000.0;
+      if ((2.0 * ecc + 1.0) * std::log2((double)std::max<int64_t>(maxdeg, 2)) <= 1000.0) want[b] = (int8_t)c;
     }
   }
-  std::vector<int32_t> cand;
-  for (int32_t b = 0; b < B->n_bcc; ++b)
-    if (ok[b]) cand.push_back(b);
-  std::stable_sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) {
-    return B->vtx_off[x + 1] - B->vtx_off[x] < B->vtx_off[y + 1] - B->vtx_off[y];
-  });
-  int64_t nmax = 0, smax = 0;
-  for (int32_t b : cand) {
-    const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
-    if (bcg::tile_smem_bytes(std::max(nmax, nb), std::max(smax, bytes[b])) > lim) break;
-    nmax = std::max(nmax, nb);
-    smax = std::max(smax, bytes[b]);
-    tile[b] = 1;
+  for (int c : {bcg::kTileWarp, bcg::kTileCta}) {
+    std::vector<int32_t> cand;
+    for (int32_t b = 0; b < B->n_bcc; ++b)
+      if (want[b] == c) cand.push_back(b);
+    std::stable_sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) {
+      return B->vtx_off[x + 1] - B->vtx_off[x] < B->vtx_off[y + 1] - B->vtx_off[y];
+    });
+    int64_t nmax = 0, smax = 0;
+    for (int32_t b : cand) {
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+      if (bcg::tile_smem_bytes(fit_cls(c), std::max(nmax, nb), std::max(smax, bytes[b])) > lim) break;
+      nmax = std::max(nmax, nb);
+      smax = std::max(smax, bytes[b]);
+      cls[b] = (int8_t)c;
+    }
   }
 }
 
 // Work items, staged slices and warp workspace of the small-BCC schedule.
-int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &tile, bc_plan *p) {
+// Launches: the warp class, then the CTA class in buckets of resident CTAs
+// per SM (4 or more, 3, 2, 1 -- from each BCC's own shared-memory need), the
+// items of each launch contiguous.
+int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, bc_plan *p) {
   int rc = BCGPU_OK;
   std::vector<int64_t> off((size_t)B->n_bcc, -1);
   std::vector<int32_t> size((size_t)B->n_bcc, 0);
-  int64_t total = 0, nmax = 0, smax = 0;
+  std::vector<int8_t> bucket((size_t)B->n_bcc, -1);
+  constexpr int64_t kSmPerSm = 228 * 1024, kReserved = 1024;  // shared memory per SM, per-CTA reserve
   for (int32_t b = 0; b < B->n_bcc; ++b) {
-    if (!tile[b]) continue;
+    if (cls[b] < 0) continue;
     const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
-    const int64_t arcs = B->row[vo + nb] - B->row[vo];
-    off[b] = total;
-    size[b] = (int32_t)bcg::TileSlice::bytes(nb, arcs);
-    total += size[b];
-    nmax = std::max(nmax, nb);
-    smax = std::max<int64_t>(smax, size[b]);
-    for (int32_t s0 = 0; s0 < nb; s0 += kTileItemSources)
-      p->h_titems.push_back({b, s0, (int32_t)std::min<int64_t>(nb, s0 + kTileItemSources), 0});
+    size[b] = (int32_t)bcg::TileSlice::bytes(nb, B->row[vo + nb] - B->row[vo]);
+    if (cls[b] == bcg::kTileWarp) { bucket[b] = 0; continue; }
+    const int64_t per = kSmPerSm / ((int64_t)bcg::tile_smem_bytes(bcg::kTileCta, nb, size[b]) + kReserved);
+    bucket[b] = (int8_t)(per >= 4 ? 1 : per == 3 ? 2 : per == 2 ? 3 : 4);
   }
-  // slices: local row offsets, neighbours, reach (int32, 16-byte aligned parts)
+  int64_t total = 0;
+  for (int k = 0; k <= 4; ++k) {
+    bc_plan::TileLaunch T;
+    T.cls = k == 0 ? bcg::kTileWarp : k <= 2 ? bcg::kTileCta : k == 3 ? bcg::kTileCta512 : bcg::kTileCta1024;
+    T.i0 = (int64_t)p->h_titems.size();
+    int64_t nmax = 0, smax = 0;
+    for (int32_t b = 0; b < B->n_bcc; ++b) {
+      if (bucket[b] != k) continue;
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+      off[b] = total;
+      total += size[b];
+      nmax = std::max(nmax, nb);
+      smax = std::max<int64_t>(smax, size[b]);
+      for (int32_t s0 = 0; s0 < nb; s0 += kTileItemSources)
+        p->h_titems.push_back({b, s0, (int32_t)std::min<int64_t>(nb, s0 + kTileItemSources), 0});
+    }
+    T.i1 = (int64_t)p->h_titems.size();
+    if (T.i1 == T.i0) continue;
+    T.nmax = (int32_t)nmax;
+    T.slice_max = (int32_t)smax;
+    T.smem = bcg::tile_smem_bytes(T.cls, nmax, smax);
+    const int per_sm = bcg::tile_ctas_per_sm(T.cls, T.smem);
+    if (per_sm < 1) return fail(ctx, BCGPU_ECUDA, "small-BCC schedule: no CTA fits an SM");
+    T.grid = ctx->sms * per_sm;
+    if (T.cls == bcg::kTileWarp) p->tcap = nmax + 2;
+    p->tl.push_back(T);
+  }
+  // slices: local row offsets (int32), neighbours (uint16), 16-byte aligned parts
   std::vector<unsigned char> blob((size_t)std::max<int64_t>(total, 16), 0);
 #pragma omp parallel for schedule(dynamic, 16)
   for (int32_t b = 0; b < B->n_bcc; ++b) {
-    if (!tile[b]) continue;
+    if (cls[b] < 0) continue;
     const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo, e0 = B->row[vo];
     const int64_t arcs = B->row[vo + nb] - e0;
     int32_t *R = reinterpret_cast<int32_t *>(blob.data() + off[b]);
-    int32_t *C = reinterpret_cast<int32_t *>(blob.data() + off[b] + bcg::TileSlice::col_at(nb));
-    int32_t *W = reinterpret_cast<int32_t *>(blob.data() + off[b] + bcg::TileSlice::reach_at(nb, arcs));
+    uint16_t *C = reinterpret_cast<uint16_t *>(blob.data() + off[b] + bcg::TileSlice::col_at(nb));
     for (int64_t v = 0; v <= nb; ++v) R[v] = (int32_t)(B->row[vo + v] - e0);
-    for (int64_t e = 0; e < arcs; ++e) C[e] = B->col[e0 + e];
-    for (int64_t v = 0; v < nb; ++v) W[v] = B->reach[vo + v];
+    for (int64_t e = 0; e < arcs; ++e) C[e] = (uint16_t)B->col[e0 + e];
   }
   p->n_titems = (int64_t)p->h_titems.size();
-  p->tnmax = (int32_t)nmax;
-  p->tslice_max = (int32_t)smax;
-  p->tsmem = bcg::tile_smem_bytes(nmax, smax);
-  const int per_sm = bcg::tile_ctas_per_sm(p->tsmem);
-  if (per_sm < 1) return fail(ctx, BCGPU_ECUDA, "small-BCC schedule: no CTA fits an SM");
-  p->tgrid = ctx->sms * per_sm;
-  p->tcap = nmax + 2;
-  const int64_t slots = (int64_t)p->tgrid * bcg::kTileWarps;
+  int warp_grid = 1;
+  for (const auto &T : p->tl)
+    if (T.cls == bcg::kTileWarp) warp_grid = T.grid;
+  const int64_t slots = (int64_t)warp_grid * bcg::kTileWarps;
+  p->tcap = std::max<int64_t>(p->tcap, 2);
   if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) || (rc = upload(p, &p->slice_off, off.data(), B->n_bcc)) ||
       (rc = upload(p, &p->slice_bytes, size.data(), B->n_bcc)) ||
-      (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) ||
-      (rc = dalloc(p, &p->tws_S, slots * p->tcap)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
-      (rc = dalloc(p, &p->tws_sq, slots * p->tcap)) || (rc = alloc_acc(p, B->n_packed)))
+      (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
+      (rc = alloc_acc(p, B->n_packed)))
     return rc;
   for (const auto &it : p->h_titems) {
     const int64_t vo = B->vtx_off[it.bcc], nb = B->vtx_off[it.bcc + 1] - vo;
@@ -499,11 +540,11 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     for (char x : on) n_on += x;
   }
   // BATCHED: BCCs off the multi-source passes that fit the small-BCC schedule
-  std::vector<char> tile;
+  std::vector<int8_t> tile;
   int64_t n_tile = 0;
   if (p->mode == BCGPU_MODE_BATCHED && ctx->opts.tile_max >= 0 && n_on < B->n_bcc) {
     route_tiles(ctx, B, on, tile);
-    for (char x : tile) n_tile += x;
+    for (int8_t x : tile) n_tile += x >= 0;
   }
   std::vector<bcg::PlainItem> items;
   if (p->mode == BCGPU_MODE_PLAIN) {
@@ -511,7 +552,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     else plain_items(B, items);
   } else if (n_on + n_tile < B->n_bcc) {
     std::vector<char> skip(on);
-    for (int32_t b = 0; b < B->n_bcc; ++b) skip[b] |= n_tile ? tile[b] : 0;
+    for (int32_t b = 0; b < B->n_bcc; ++b) skip[b] |= n_tile ? tile[b] >= 0 : 0;
     plain_items(B, items, &skip);
   }
   if (p->mode == BCGPU_MODE_BATCHED && n_on > 0) {
@@ -913,8 +954,8 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
     *launches += 2;
     j0 = j1;
   }
-  // small-BCC items: one launch (each BCC's sources are far fewer than
-  // kAccMaxAdds), then the fold of the BCCs it touched
+  // small-BCC items: one launch per class (each BCC's sources are far fewer
+  // than kAccMaxAdds), then one fold over the BCCs they touched
   const int64_t t0 = std::max(begin, p->n_bat + p->n_items) - p->n_bat - p->n_items;
   const int64_t t1 = end - p->n_bat - p->n_items;
   if (t1 > t0) {
@@ -923,16 +964,20 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
       b0 = std::min(b0, p->h_titems[j].bcc);
       b1 = std::max(b1, p->h_titems[j].bcc);
     }
-    CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
-    bcg::TileArgs a{};
-    a.vtx_off = p->vtx_off; a.slices = p->slices; a.slice_off = p->slice_off; a.slice_bytes = p->slice_bytes;
-    a.items = p->titems; a.item_begin = t0; a.item_end = t1; a.next_item = p->counter; a.acc = p->acc;
-    a.ws_S = p->tws_S; a.ws_lv = p->tws_lv; a.ws_sq = p->tws_sq; a.cap = p->tcap; a.nmax = p->tnmax;
-    a.slice_max = p->tslice_max; a.wait_ns = wait_ns(ctx); a.err = p->err;
-    const int grid = (int)std::min<int64_t>(p->tgrid, t1 - t0);
-    CK(ctx, bcg::launch_tile(a, grid, p->tsmem, ctx->stream));
+    for (const bc_plan::TileLaunch &T : p->tl) {
+      const int64_t j0 = std::max(t0, T.i0), j1 = std::min(t1, T.i1);
+      if (j1 <= j0) continue;
+      CK(ctx, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), ctx->stream));
+      bcg::TileArgs a{};
+      a.vtx_off = p->vtx_off; a.reach = p->reach; a.slices = p->slices; a.slice_off = p->slice_off;
+      a.slice_bytes = p->slice_bytes; a.items = p->titems; a.item_begin = j0; a.item_end = j1;
+      a.next_item = p->counter; a.acc = p->acc; a.ws_lv = p->tws_lv; a.cap = p->tcap; a.nmax = T.nmax;
+      a.slice_max = T.slice_max; a.wait_ns = wait_ns(ctx); a.err = p->err;
+      CK(ctx, bcg::launch_tile(T.cls, a, (int)std::min<int64_t>(T.grid, j1 - j0), T.smem, ctx->stream));
+      ++*launches;
+    }
     CK(ctx, bcg::launch_fold(p->acc, p->bc, p->h_vtx_off[b0], p->h_vtx_off[b1 + 1], ctx->stream));
-    *launches += 2;
+    ++*launches;
   }
   return BCGPU_OK;
 }

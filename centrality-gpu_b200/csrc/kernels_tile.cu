@@ -1,29 +1,34 @@
-// Small-BCC schedule: one CTA per range of sources of one BCC, one warp per
-// source, the BCC's CSR slice in shared memory.
+// Small-BCC schedule: one CTA per range of sources of one BCC, every array a
+// source touches in shared memory.
 //
 // The reference runs every BCC through the same per-source kernel, one
 // source per CTA (Codes/kernels_free.cu:154-473, launch shape
-// Codes/begin_gpupgm.cu:52-65), whatever its size; on a batch of thousands of
-// small graphs most of a CTA then waits at its per-level barriers. Here a
-// BCC that fits shared memory is run warp-synchronously:
-//  * the slice (local row offsets, neighbours, reach; tile.h TileSlice) is
-//    brought into shared memory by one cp.async.bulk (a plain bulk copy from
-//    this GPU's global memory into this CTA's shared memory, completion on an
-//    mbarrier whose wait is bounded) and serves every source of the range;
-//  * each warp runs one source at a time: a level-synchronous BFS whose levels
-//    live in shared memory (one int32 row per warp), each frontier vertex
-//    pulling sigma from its predecessors and claiming its successors in one
-//    scan of its row (lane per vertex; a vertex of more than 32 arcs is
-//    scanned by the whole warp), then the successor-form dependency sweep
-//    q(w) = (reach(w)+1+delta(w))/sigma(w), delta(v) = sigma(v) * sum q
-//    (Codes/kernels_free.cu:391,409), q overwriting sigma in place;
-//  * chain (degree-2) vertices are ordinary vertices and sources here: their
-//    BFS costs no more than the endpoint merge of the per-source schedule on
-//    a BCC this small;
-//  * BC: each contribution delta * (reach(s)+1) (Codes/kernels_free.cu:425) is
-//    added to the CTA's fixed-point counters in shared memory (integer
-//    atomics: the result does not depend on the order of the warps), which
-//    are added to the global counters once per work item.
+// Codes/begin_gpupgm.cu:52-65), with its rows in global memory, whatever the
+// BCC's size; on a batch of thousands of small graphs the CTAs then wait on
+// global-memory latency at every arc. Here a BCC that fits shared memory is
+// run from shared memory only:
+//  * the slice (local row offsets, 16-bit neighbour ids; tile.h TileSlice) is
+//    brought in by one cp.async.bulk (a plain bulk copy from this GPU's global
+//    memory into this CTA's shared memory, completion on an mbarrier whose wait
+//    is bounded) and serves every source of the item;
+//  * levels, path counts (then q in place) and the visit order of each source
+//    live in shared memory: one set per warp in the warp class (a warp per
+//    source, eight in flight), one per CTA in the CTA class;
+//  * forward: level-synchronous, each frontier vertex pulls sigma from its
+//    predecessors and claims its successors in one scan of its row -- a row of
+//    up to kLaneDeg arcs by one lane (four arcs' loads in flight), a longer one
+//    by a whole warp (lanes over arcs, then a fixed-order warp sum);
+//  * backward: successor form, q(w) = (reach(w)+1+delta(w))/sigma(w) and
+//    delta(v) = sigma(v) * sum q (Codes/kernels_free.cu:391,409), q
+//    overwriting sigma in place;
+//  * chain (degree-2) vertices are ordinary vertices and sources here: on a
+//    BCC this small their BFS costs about what the endpoint merge of the
+//    per-source schedule does;
+//  * BC: contributions delta * (reach(s)+1) (Codes/kernels_free.cu:425) go to
+//    shared-memory fixed-point counters (warp class: integer atomics, any
+//    order) or to an FP64 partial row (CTA class: the CTA's sources run one
+//    after another, each vertex written by one thread, so the order is fixed),
+//    then once per item into the global fixed-point counters.
 // Path counts are FP64 without per-level scaling: the plan routes a BCC here
 // only when no path count can pass 2^1000 ((2 ecc + 1) levels of at most
 // maxdeg predecessors each); a non-finite value still flags kDevOverflow.
@@ -31,45 +36,44 @@
 #include "common.cuh"
 #include "tile.h"
 
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
 namespace bcg {
 
 namespace {
 
 constexpr int kThreads = kTileWarps * 32;
-constexpr int kWarpScan = 32;  // rows longer than this are scanned by the whole warp
+constexpr int kLaneDeg = 8;  // rows up to this many arcs: one lane; longer rows: a whole warp
 
-// Shared memory: control words, then the counters, the per-warp level rows
-// and the staged slice, each on a 16-byte boundary.
 struct Ctl {
   unsigned long long bar;  // mbarrier of the slice copy
-  int item, next, bcc, pad;
-  int tail[kTileWarps];
+  int item, next, bcc, nq, tail, pad;
+  int tails[kTileWarps];
 };
 
 __host__ __device__ constexpr int64_t align16(int64_t x) { return (x + 15) / 16 * 16; }
 
-struct Smem {
-  Ctl *ctl;
-  unsigned long long *cnt;  // [nmax][kAccDigits]
-  int32_t *lev;             // [kTileWarps][nmax]
-  unsigned char *slice;
+// ---- shared-memory layouts (host and device agree through these)
+struct WarpLayout {  // ctl | counters [nmax][kAccDigits] | per warp: d [nmax], S [nmax], sq [nmax] | slice
+  __host__ __device__ static int64_t cnt() { return align16(sizeof(Ctl)); }
+  __host__ __device__ static int64_t per_warp(int64_t nmax) { return align16(8 * nmax) + 2 * align16(4 * nmax); }
+  __host__ __device__ static int64_t warps(int64_t nmax) { return cnt() + align16(nmax * kAccDigits * 8); }
+  __host__ __device__ static int64_t slice(int64_t nmax) { return warps(nmax) + kTileWarps * per_warp(nmax); }
+};
+template <int kBlock>
+struct CtaLayout {  // ctl | P [nmax] | sq [nmax] | d [nmax] | S [nmax] | lv [kTileMaxLevels] | queue [kBlock] | slice
+  __host__ __device__ static int64_t P() { return align16(sizeof(Ctl)); }
+  __host__ __device__ static int64_t sq(int64_t nmax) { return P() + align16(8 * nmax); }
+  __host__ __device__ static int64_t d(int64_t nmax) { return sq(nmax) + align16(8 * nmax); }
+  __host__ __device__ static int64_t S(int64_t nmax) { return d(nmax) + align16(4 * nmax); }
+  __host__ __device__ static int64_t lv(int64_t nmax) { return S(nmax) + align16(4 * nmax); }
+  __host__ __device__ static int64_t q(int64_t nmax) { return lv(nmax) + align16(4 * kTileMaxLevels); }
+  __host__ __device__ static int64_t slice(int64_t nmax) { return q(nmax) + align16(4 * kBlock); }
 };
 
-__device__ __forceinline__ Smem smem_of(unsigned char *base, int nmax) {
-  Smem s;
-  s.ctl = reinterpret_cast<Ctl *>(base);
-  int64_t off = align16(sizeof(Ctl));
-  s.cnt = reinterpret_cast<unsigned long long *>(base + off);
-  off += align16((int64_t)nmax * kAccDigits * 8);
-  s.lev = reinterpret_cast<int32_t *>(base + off);
-  off += align16((int64_t)kTileWarps * nmax * 4);
-  s.slice = base + off;
-  return s;
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // mbarrier and bulk-copy primitives (PTX ISA: mbarrier, cp.async.bulk).
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
@@ -90,7 +94,7 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
       : "memory");
   return done != 0;
 }
-// Global -> this CTA's shared memory, bytes a multiple of 16, both ends 16-byte aligned.
+// Global -> this CTA's shared memory; bytes a multiple of 16, both ends 16-byte aligned.
 __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of dst before the copy's writes
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -98,7 +102,6 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
                "l"(src), "r"(bytes), "r"(smem_addr(bar))
                : "memory");
 }
-
 // Waits for phase `parity` of the barrier, at most limit_ns; false on timeout.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned long long limit_ns) {
   const unsigned long long t0 = global_ns();
@@ -108,15 +111,150 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
   return true;
 }
 
-// One BCC as the kernel reads it: local row offsets, neighbours, reach.
+// One BCC as the kernels read it: local row offsets and neighbours (shared
+// memory), reach (global).
 struct View {
-  const int32_t *R, *C, *rch;
+  const int32_t *R;
+  const uint16_t *C;
+  const int32_t *rch;
 };
 
-// Forward BFS of one warp from s: levels in d (-1 = unvisited), path counts in
-// sq, visit order in S, level offsets lv[0..nlev]. Returns nlev.
+// Pulls the next item for the CTA (thread 0) and stages its BCC's slice if
+// the CTA does not hold it already. Returns false when the CTA is done (no
+// item left, an error flagged, or the slice did not arrive in time).
+__device__ bool next_item(const TileArgs &a, Ctl &ctl, unsigned char *slice, unsigned &phase, TileItem &it,
+                          int64_t &vo, int32_t &nb) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    const int64_t k = (int64_t)atomicAdd(a.next_item, 1ull);
+    ctl.item = (*(volatile int *)a.err != kDevOk || a.item_begin + k >= a.item_end) ? -1 : (int)k;
+    ctl.next = 0;
+  }
+  __syncthreads();  // also: every thread is done with the previous item's slice and rows
+  if (ctl.item < 0) return false;
+  it = a.items[a.item_begin + ctl.item];
+  vo = a.vtx_off[it.bcc];
+  nb = (int32_t)(a.vtx_off[it.bcc + 1] - vo);
+  const int64_t soff = a.slice_off[it.bcc];
+  if (nb > a.nmax || soff < 0 || it.s0 < 0 || it.s1 > nb) {  // uniform over the CTA
+    if (tid == 0) set_err(a.err, kDevBadItem);
+    return false;
+  }
+  if (ctl.bcc != it.bcc) {  // uniform: ctl.bcc was last written before a barrier
+    if (tid == 0) {
+      const unsigned bytes = (unsigned)a.slice_bytes[it.bcc];
+      mbar_expect_tx(&ctl.bar, bytes);
+      bulk_copy(slice, a.slices + soff, bytes, &ctl.bar);
+    }
+    if (!mbar_wait(&ctl.bar, phase, a.wait_ns)) {
+      // the copy did not complete in time: record it, wait (again bounded)
+      // for the copy in flight to land in this CTA's shared memory, stop
+      set_err(a.err, kDevTimeout);
+      mbar_wait(&ctl.bar, phase, a.wait_ns);
+      return false;
+    }
+    phase ^= 1u;
+  }
+  return true;
+}
+
+__device__ __forceinline__ View view_of(const TileArgs &a, const unsigned char *slice, int32_t nb, int64_t vo) {
+  const int32_t *R = reinterpret_cast<const int32_t *>(slice);
+  return View{R, reinterpret_cast<const uint16_t *>(slice + TileSlice::col_at(nb)), a.reach + vo};
+}
+
+// Appends x to the visit order S: one atomic per group of lanes appending at
+// once (the lanes that reach this call together), not one per lane.
+__device__ __forceinline__ void append(int32_t *S, int *tail, int32_t x) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int pos = 0;
+  if (g.thread_rank() == 0) pos = atomicAdd(tail, (int)g.size());
+  S[g.shfl(pos, 0) + (int)g.thread_rank()] = x;
+}
+
+// Forward scan of one row by one thread (four arcs' loads in flight, sums in
+// arc order): pulls sigma from level dprev, claims unvisited vertices for
+// dnext (appended to S at *tail).
+__device__ __forceinline__ double pull_row(const View &g, int e0, int e1, int32_t *d, const double *sq, int32_t *S,
+                                           int *tail, int dprev, int dnext) {
+  double acc = 0.0;
+  for (int e = e0; e < e1; e += 4) {
+    int32_t x[4], dx[4];
+    double sv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? (int32_t)g.C[e + j] : -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dx[j] = x[j] >= 0 ? d[x[j]] : INT_MAX;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sv[j] = dx[j] == dprev ? sq[x[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (dx[j] == dprev) acc += sv[j];
+      else if (dx[j] == -1 && atomicCAS(d + x[j], -1, dnext) == -1) append(S, tail, x[j]);
+    }
+  }
+  return acc;
+}
+
+// The same for a long row, by a whole warp (lanes over arcs, fixed-order sum).
+__device__ __forceinline__ double pull_row_warp(const View &g, int e0, int e1, int32_t *d, const double *sq, int32_t *S,
+                                                int *tail, int dprev, int dnext, int lane) {
+  double acc = 0.0;
+  for (int e = e0 + lane; e < e1; e += 32) {
+    const int32_t x = g.C[e];
+    const int dx = d[x];
+    if (dx == dprev) acc += sq[x];
+    else if (dx == -1 && atomicCAS(d + x, -1, dnext) == -1) append(S, tail, x);
+  }
+  return warp_sum(acc);
+}
+
+// Sum of q over the successors (level dsucc) of one row, by one thread.
+__device__ __forceinline__ double push_row(const View &g, int e0, int e1, const int32_t *d, const double *sq, int dsucc) {
+  double acc = 0.0;
+  for (int e = e0; e < e1; e += 4) {
+    int32_t x[4];
+    bool hit[4];
+    double qv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? (int32_t)g.C[e + j] : -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) hit[j] = x[j] >= 0 && d[x[j]] == dsucc;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) qv[j] = hit[j] ? sq[x[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (hit[j]) acc += qv[j];
+  }
+  return acc;
+}
+
+__device__ __forceinline__ double push_row_warp(const View &g, int e0, int e1, const int32_t *d, const double *sq,
+                                                int dsucc, int lane) {
+  double acc = 0.0;
+  for (int e = e0 + lane; e < e1; e += 32) {
+    const int32_t x = g.C[e];
+    if (d[x] == dsucc) acc += sq[x];
+  }
+  return warp_sum(acc);
+}
+
+// delta and q of w from the successors' sum; returns delta (q overwrites sigma).
+__device__ __forceinline__ double finish(const View &g, int32_t w, double sum, double *sq, int *err) {
+  const double sw = sq[w];
+  const double delta = sw * sum;
+  const double qw = ((double)__ldg(g.rch + w) + 1.0 + delta) / sw;
+  if (exp_bits(qw) == 0x7ff || exp_bits(delta) == 0x7ff || exp_bits(sw) == 0) set_err(err, kDevOverflow);
+  sq[w] = qw;
+  return delta;
+}
+
+// ======================================================= warp per source ===
+
+// BFS of one warp from s (rows in this warp's shared memory, level offsets lv
+// in global memory). Returns the number of levels.
 __device__ int warp_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double *sq, int32_t *S, int32_t *lv,
-                        int *tail, int lane, int *err) {
+                        int *tail, int lane) {
   for (int v = lane; v < nb; v += 32) d[v] = -1;
   __syncwarp();
   if (lane == 0) {
@@ -139,43 +277,18 @@ __device__ int warp_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double
         e0 = g.R[w];
         e1 = g.R[w + 1];
       }
-      const bool big = e1 - e0 > kWarpScan;
+      const bool big = e1 - e0 > kLaneDeg;
       if (w >= 0 && !big) {
-        double acc = 0.0;
-        for (int e = e0; e < e1; e += 4) {  // four arcs' loads in flight; sums in arc order
-          int32_t x[4], dx[4];
-          double sv[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? g.C[e + j] : -1;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) dx[j] = x[j] >= 0 ? d[x[j]] : INT_MAX;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sv[j] = dx[j] == dprev ? __ldcg(sq + x[j]) : 0.0;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (dx[j] == dprev) {
-              acc += sv[j];
-            } else if (dx[j] == -1 && atomicCAS(d + x[j], -1, dnext) == -1) {
-              S[atomicAdd(tail, 1)] = x[j];
-            }
-          }
-        }
+        const double acc = pull_row(g, e0, e1, d, sq, S, tail, dprev, dnext);
         if (lev > 0) sq[w] = acc;
       }
       uint32_t bigs = __ballot_sync(0xffffffffu, w >= 0 && big);
-      while (bigs) {  // rows longer than kWarpScan: the whole warp, lanes over arcs
+      while (bigs) {
         const int j = __ffs(bigs) - 1;
         bigs &= bigs - 1;
         const int32_t wj = __shfl_sync(0xffffffffu, w, j);
-        const int32_t a0 = __shfl_sync(0xffffffffu, e0, j), a1 = __shfl_sync(0xffffffffu, e1, j);
-        double acc = 0.0;
-        for (int e = a0 + lane; e < a1; e += 32) {
-          const int32_t x = g.C[e];
-          const int dx = d[x];
-          if (dx == dprev) acc += __ldcg(sq + x);
-          else if (dx == -1 && atomicCAS(d + x, -1, dnext) == -1) S[atomicAdd(tail, 1)] = x;
-        }
-        acc = warp_sum(acc);
+        const int a0 = __shfl_sync(0xffffffffu, e0, j), a1 = __shfl_sync(0xffffffffu, e1, j);
+        const double acc = pull_row_warp(g, a0, a1, d, sq, S, tail, dprev, dnext, lane);
         if (lane == 0 && lev > 0) sq[wj] = acc;
       }
     }
@@ -188,14 +301,11 @@ __device__ int warp_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double
     ++lev;
     __syncwarp();
   }
-  (void)err;
   return lev + 1;
 }
 
-// Dependency sweep of one warp, deepest level first; q overwrites sigma in
-// sq; contributions delta * wsrc go to the shared-memory counters.
-__device__ void warp_sweep(const View &g, int32_t nlev, const int32_t *d, double *sq, const int32_t *S,
-                           const int32_t *lv, double wsrc, unsigned long long *cnt, int lane, int *err) {
+__device__ void warp_sweep(const View &g, int nlev, const int32_t *d, double *sq, const int32_t *S, const int32_t *lv,
+                           double wsrc, unsigned long long *cnt, int lane, int *err) {
   for (int lev = nlev - 1; lev >= 1; --lev) {
     const int dsucc = lev + 1, a0 = lv[lev], a1 = lv[lev + 1];
     for (int c0 = a0; c0 < a1; c0 += 32) {
@@ -206,43 +316,19 @@ __device__ void warp_sweep(const View &g, int32_t nlev, const int32_t *d, double
         e0 = g.R[w];
         e1 = g.R[w + 1];
       }
-      const bool big = e1 - e0 > kWarpScan;
-      double acc = 0.0;
-      if (w >= 0 && !big) {
-        for (int e = e0; e < e1; e += 4) {
-          int32_t x[4];
-          bool hit[4];
-          double qv[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? g.C[e + j] : -1;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) hit[j] = x[j] >= 0 && d[x[j]] == dsucc;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) qv[j] = hit[j] ? __ldcg(sq + x[j]) : 0.0;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (hit[j]) acc += qv[j];
-        }
-      }
+      const bool big = e1 - e0 > kLaneDeg;
+      double sum = 0.0;
+      if (w >= 0 && !big) sum = push_row(g, e0, e1, d, sq, dsucc);
       uint32_t bigs = __ballot_sync(0xffffffffu, w >= 0 && big);
       while (bigs) {
         const int j = __ffs(bigs) - 1;
         bigs &= bigs - 1;
-        const int32_t a0j = __shfl_sync(0xffffffffu, e0, j), a1j = __shfl_sync(0xffffffffu, e1, j);
-        double part = 0.0;
-        for (int e = a0j + lane; e < a1j; e += 32) {
-          const int32_t x = g.C[e];
-          if (d[x] == dsucc) part += __ldcg(sq + x);
-        }
-        part = warp_sum(part);
-        if (lane == j) acc = part;
+        const int b0 = __shfl_sync(0xffffffffu, e0, j), b1 = __shfl_sync(0xffffffffu, e1, j);
+        const double part = push_row_warp(g, b0, b1, d, sq, dsucc, lane);
+        if (lane == j) sum = part;
       }
       if (w >= 0) {
-        const double sw = __ldcg(sq + w);
-        const double delta = sw * acc;
-        const double qw = ((double)g.rch[w] + 1.0 + delta) / sw;
-        if (exp_bits(qw) == 0x7ff || exp_bits(delta) == 0x7ff || exp_bits(sw) == 0) set_err(err, kDevOverflow);
-        sq[w] = qw;  // this level's q: read only by the level above (after the warp barrier)
+        const double delta = finish(g, w, sum, sq, err);  // this level's q: read by the level above only
         if (delta != 0.0) acc_add(cnt + (int64_t)kAccDigits * w, delta * wsrc, err);
       }
     }
@@ -250,87 +336,184 @@ __device__ void warp_sweep(const View &g, int32_t nlev, const int32_t *d, double
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) tile_kernel(TileArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) tile_warp_kernel(TileArgs a) {
   extern __shared__ __align__(16) unsigned char s_raw[];
-  const Smem sm = smem_of(s_raw, a.nmax);
-  Ctl &ctl = *sm.ctl;
+  Ctl &ctl = *reinterpret_cast<Ctl *>(s_raw);
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(s_raw + WarpLayout::cnt());
+  unsigned char *slice = s_raw + WarpLayout::slice(a.nmax);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t slot = (int64_t)blockIdx.x * kTileWarps + warp;
-  int32_t *S = a.ws_S + slot * a.cap, *lv = a.ws_lv + slot * a.cap;
-  double *sq = a.ws_sq + slot * a.cap;
-  int32_t *dl = sm.lev + (int64_t)warp * a.nmax;
+  unsigned char *mine = s_raw + WarpLayout::warps(a.nmax) + (int64_t)warp * WarpLayout::per_warp(a.nmax);
+  double *sq = reinterpret_cast<double *>(mine);
+  int32_t *d = reinterpret_cast<int32_t *>(mine + align16(8 * (int64_t)a.nmax));
+  int32_t *S = d + align16(4 * (int64_t)a.nmax) / 4;
+  int32_t *lv = a.ws_lv + ((int64_t)blockIdx.x * kTileWarps + warp) * a.cap;
   if (tid == 0) {
     mbar_init(&ctl.bar, 1);
     ctl.bcc = -1;
   }
   __syncthreads();
   unsigned phase = 0;
-  while (true) {
-    if (tid == 0) {
-      const int64_t k = (int64_t)atomicAdd(a.next_item, 1ull);
-      ctl.item = (*(volatile int *)a.err != kDevOk || a.item_begin + k >= a.item_end) ? -1 : (int)k;
-      ctl.next = 0;
-    }
-    __syncthreads();  // also: every warp is done with the previous item's slice and counters
-    if (ctl.item < 0) break;
-    const TileItem it = a.items[a.item_begin + ctl.item];
-    const int64_t vo = a.vtx_off[it.bcc];
-    const int32_t nb = (int32_t)(a.vtx_off[it.bcc + 1] - vo);
-    const int64_t soff = a.slice_off[it.bcc];
-    if (nb > a.nmax || soff < 0) {  // uniform over the CTA
-      set_err(a.err, kDevBadItem);
-      continue;
-    }
-    if (ctl.bcc != it.bcc) {  // stage the BCC's slice (uniform: ctl.bcc was last written before a barrier)
-      if (tid == 0) {
-        const unsigned bytes = (unsigned)a.slice_bytes[it.bcc];
-        mbar_expect_tx(&ctl.bar, bytes);
-        bulk_copy(sm.slice, a.slices + soff, bytes, &ctl.bar);
-      }
-      const bool ok = mbar_wait(&ctl.bar, phase, a.wait_ns);
-      if (!ok) {
-        // the copy did not complete in time: record it, wait (again bounded)
-        // for the copy in flight to land in this CTA's shared memory, stop
-        set_err(a.err, kDevTimeout);
-        mbar_wait(&ctl.bar, phase, a.wait_ns);
-        break;
-      }
-      phase ^= 1u;
-    }
-    for (int64_t k = tid; k < (int64_t)kAccDigits * nb; k += kThreads) sm.cnt[k] = 0ull;
+  TileItem it;
+  int64_t vo;
+  int32_t nb;
+  while (next_item(a, ctl, slice, phase, it, vo, nb)) {
+    for (int64_t k = tid; k < (int64_t)kAccDigits * nb; k += kThreads) cnt[k] = 0ull;
     __syncthreads();
-    if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next top-of-loop barrier
-    const int32_t *sl = reinterpret_cast<const int32_t *>(sm.slice);
-    const View g{sl, sl + TileSlice::col_at(nb) / 4,
-                 reinterpret_cast<const int32_t *>(sm.slice + TileSlice::reach_at(nb, sl[nb]))};
-    while (true) {  // warps take the item's sources one at a time
+    if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
+    const View g = view_of(a, slice, nb, vo);
+    while (true) {  // the warps take the item's sources one at a time
       int k = 0;
       if (lane == 0) k = atomicAdd(&ctl.next, 1);
       k = __shfl_sync(0xffffffffu, k, 0);
       const int32_t s = it.s0 + k;
       if (s >= it.s1) break;
-      if (s < 0 || s >= nb) {
-        set_err(a.err, kDevBadItem);
-        break;
-      }
-      const int nlev = warp_bfs(g, nb, s, dl, sq, S, lv, &ctl.tail[warp], lane, a.err);
-      warp_sweep(g, nlev, dl, sq, S, lv, (double)g.rch[s] + 1.0, sm.cnt, lane, a.err);
+      const int nlev = warp_bfs(g, nb, s, d, sq, S, lv, &ctl.tails[warp], lane);
+      warp_sweep(g, nlev, d, sq, S, lv, (double)__ldg(g.rch + s) + 1.0, cnt, lane, a.err);
     }
     __syncthreads();
-    // the item's contributions into the global counters (integer adds: any order)
-    unsigned long long *acc = a.acc + (int64_t)kAccDigits * vo;
+    unsigned long long *acc = a.acc + (int64_t)kAccDigits * vo;  // integer adds: any order
     for (int64_t k = tid; k < (int64_t)kAccDigits * nb; k += kThreads) {
-      const unsigned long long c = sm.cnt[k];
+      const unsigned long long c = cnt[k];
       if (c) atomicAdd(acc + k, c);
     }
   }
 }
 
+// ======================================================== CTA per source ===
+
+template <int kBlock>
+__device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double *sq, int32_t *S, int32_t *lv, int32_t *q,
+                       Ctl &ctl, int *err) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int v = tid; v < nb; v += kBlock) d[v] = -1;
+  __syncthreads();
+  if (tid == 0) {
+    d[s] = 0;
+    S[0] = s;
+    sq[s] = 1.0;
+    lv[0] = 0;
+    lv[1] = 1;
+    ctl.tail = 1;
+  }
+  __syncthreads();
+  int lev = 0, f0 = 0, f1 = 1;
+  while (true) {
+    const int dprev = lev == 0 ? INT_MIN : lev - 1, dnext = lev + 1;
+    for (int c0 = f0; c0 < f1; c0 += kBlock) {
+      if (tid == 0) ctl.nq = 0;
+      __syncthreads();
+      const int i = c0 + tid;
+      if (i < f1) {
+        const int32_t w = S[i];
+        const int e0 = g.R[w], e1 = g.R[w + 1];
+        if (e1 - e0 <= kLaneDeg) {
+          const double acc = pull_row(g, e0, e1, d, sq, S, &ctl.tail, dprev, dnext);
+          if (lev > 0) sq[w] = acc;
+        } else {
+          q[atomicAdd(&ctl.nq, 1)] = w;
+        }
+      }
+      __syncthreads();
+      for (int k = warp; k < ctl.nq; k += kBlock / 32) {
+        const int32_t w = q[k];
+        const double acc = pull_row_warp(g, g.R[w], g.R[w + 1], d, sq, S, &ctl.tail, dprev, dnext, lane);
+        if (lane == 0 && lev > 0) sq[w] = acc;
+      }
+      __syncthreads();
+    }
+    const int t = ctl.tail;
+    if (t == f1) break;
+    if (lev + 2 >= kTileMaxLevels) {  // uniform; routing keeps BCCs below this depth
+      if (tid == 0) set_err(err, kDevWorkspace);
+      return -1;
+    }
+    if (tid == 0) lv[lev + 2] = t;
+    f0 = f1;
+    f1 = t;
+    ++lev;
+  }
+  return lev + 1;
+}
+
+template <int kBlock>
+__device__ void cta_sweep(const View &g, int nlev, const int32_t *d, double *sq, const int32_t *S, const int32_t *lv,
+                          int32_t *q, Ctl &ctl, double wsrc, double *P, int *err) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int lev = nlev - 1; lev >= 1; --lev) {
+    const int dsucc = lev + 1, a0 = lv[lev], a1 = lv[lev + 1];
+    for (int c0 = a0; c0 < a1; c0 += kBlock) {
+      if (tid == 0) ctl.nq = 0;
+      __syncthreads();
+      const int i = c0 + tid;
+      if (i < a1) {
+        const int32_t w = S[i];
+        const int e0 = g.R[w], e1 = g.R[w + 1];
+        if (e1 - e0 <= kLaneDeg) {
+          P[w] += finish(g, w, push_row(g, e0, e1, d, sq, dsucc), sq, err) * wsrc;
+        } else {
+          q[atomicAdd(&ctl.nq, 1)] = w;
+        }
+      }
+      __syncthreads();
+      for (int k = warp; k < ctl.nq; k += kBlock / 32) {
+        const int32_t w = q[k];
+        const double sum = push_row_warp(g, g.R[w], g.R[w + 1], d, sq, dsucc, lane);
+        if (lane == 0) P[w] += finish(g, w, sum, sq, err) * wsrc;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock, 1) tile_cta_kernel(TileArgs a) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  const int64_t nmax = a.nmax;
+  Ctl &ctl = *reinterpret_cast<Ctl *>(s_raw);
+  double *P = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::P());
+  double *sq = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::sq(nmax));
+  int32_t *d = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::d(nmax));
+  int32_t *S = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::S(nmax));
+  int32_t *lv = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::lv(nmax));
+  int32_t *q = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::q(nmax));
+  unsigned char *slice = s_raw + CtaLayout<kBlock>::slice(nmax);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&ctl.bar, 1);
+    ctl.bcc = -1;
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  TileItem it;
+  int64_t vo;
+  int32_t nb;
+  while (next_item(a, ctl, slice, phase, it, vo, nb)) {
+    for (int v = tid; v < nb; v += kBlock) P[v] = 0.0;
+    __syncthreads();
+    if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
+    const View g = view_of(a, slice, nb, vo);
+    for (int32_t s = it.s0; s < it.s1; ++s) {  // one source at a time: P is summed in source order
+      const int nlev = cta_bfs<kBlock>(g, nb, s, d, sq, S, lv, q, ctl, a.err);
+      if (nlev < 0) break;
+      cta_sweep<kBlock>(g, nlev, d, sq, S, lv, q, ctl, (double)__ldg(g.rch + s) + 1.0, P, a.err);
+    }
+    __syncthreads();
+    unsigned long long *acc = a.acc + (int64_t)kAccDigits * vo;
+    for (int v = tid; v < nb; v += kBlock)
+      if (P[v] != 0.0) acc_add(acc + (int64_t)kAccDigits * v, P[v], a.err);
+  }
+}
+
 }  // namespace
 
-size_t tile_smem_bytes(int64_t nmax, int64_t slice_max) {
-  return (size_t)(align16(sizeof(Ctl)) + align16(nmax * kAccDigits * 8) + align16((int64_t)kTileWarps * nmax * 4) +
-                  align16(slice_max));
+int block_of(int cls) { return cls == kTileCta1024 ? 1024 : cls == kTileCta512 ? 512 : kThreads; }
+
+size_t tile_smem_bytes(int cls, int64_t nmax, int64_t slice_max) {
+  const int64_t head = cls == kTileWarp     ? WarpLayout::slice(nmax)
+                       : cls == kTileCta    ? CtaLayout<256>::slice(nmax)
+                       : cls == kTileCta512 ? CtaLayout<512>::slice(nmax)
+                                            : CtaLayout<1024>::slice(nmax);
+  return (size_t)(head + align16(slice_max));
 }
 
 size_t tile_smem_limit(int device) {
@@ -339,18 +522,32 @@ size_t tile_smem_limit(int device) {
   return (size_t)v;
 }
 
-int tile_ctas_per_sm(size_t smem) {
+namespace {
+const void *tile_fn(int cls) {
+  return cls == kTileWarp     ? reinterpret_cast<const void *>(tile_warp_kernel)
+         : cls == kTileCta    ? reinterpret_cast<const void *>(tile_cta_kernel<256>)
+         : cls == kTileCta512 ? reinterpret_cast<const void *>(tile_cta_kernel<512>)
+                              : reinterpret_cast<const void *>(tile_cta_kernel<1024>);
+}
+}  // namespace
+
+int tile_ctas_per_sm(int cls, size_t smem) {
   int n = 0;
-  if (cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(tile_fn(cls), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tile_kernel, kThreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tile_fn(cls), block_of(cls), smem) != cudaSuccess) return 0;
   return n;
 }
 
-cudaError_t launch_tile(const TileArgs &a, int grid, size_t smem, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t launch_tile(int cls, const TileArgs &a, int grid, size_t smem, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(tile_fn(cls), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tile_kernel<<<grid, kThreads, smem, stream>>>(a);
+  switch (cls) {
+    case kTileWarp: tile_warp_kernel<<<grid, kThreads, smem, stream>>>(a); break;
+    case kTileCta: tile_cta_kernel<256><<<grid, 256, smem, stream>>>(a); break;
+    case kTileCta512: tile_cta_kernel<512><<<grid, 512, smem, stream>>>(a); break;
+    default: tile_cta_kernel<1024><<<grid, 1024, smem, stream>>>(a); break;
+  }
   return cudaGetLastError();
 }
 

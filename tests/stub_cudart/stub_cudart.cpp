@@ -142,6 +142,10 @@ cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(int *n, const
   *n = 4;
   return cudaSuccess;
 }
+cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessor(int *n, const void *, int, size_t) {
+  *n = 4;
+  return cudaSuccess;
+}
 cudaError_t cudaGetLastError() { return cudaSuccess; }
 const char *cudaGetErrorName(cudaError_t e) { return e == cudaSuccess ? "cudaSuccess" : "cudaErrorStub"; }
 const char *cudaGetErrorString(cudaError_t e) { return e == cudaSuccess ? "no error" : "stub runtime error"; }

@@ -178,7 +178,8 @@ def test_routing_mixes_both_schedules():
     """Twelve BA graphs of mixed sizes: with the core threshold at 500, the
     five BCCs whose cores reach it take multi-source passes and the seven
     smaller ones per-source items, in one plan (three launches: the
-    multi-source kernel, the per-source kernel and the fold of its counters)."""
+    multi-source kernel, the per-source kernel and the fold of its counters;
+    the small-BCC schedule is off here)."""
     G = graphs()
     n, u, v, _ = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))
     d = decomp(n, u, v)
@@ -187,7 +188,8 @@ def test_routing_mixes_both_schedules():
     assert sum(c >= 500 for c in cores) == 5 and sum(c < 500 for c in cores) == 7
     P = pkg()
     for delta in ("fp64", "fp32c"):
-        c = P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C, plain_core=500)
+        c = P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C, plain_core=500,
+                      tile_max=-1)  # the small-BCC schedule off: test_gpu_tile.py mixes all three
         plan = c.plan(d)
         st = plan.run(0, plan.n_units)
         assert st["kernel_launches"] == 3

@@ -53,20 +53,20 @@ def test_tile_bc_matches_the_oracle(name):
 @pytest.mark.parametrize("delta", ["fp64", "fp32c"])
 def test_three_schedules_in_one_plan(delta):
     """BA graphs with the multi-source threshold at 500 core vertices and the
-    small-BCC limit at 800 vertices: the largest BCCs take multi-source
+    small-BCC limit at 600 vertices: the largest BCCs take multi-source
     passes, the middle ones per-source items, the smallest tile items."""
     P = pkg()
     n, u, v = ba(16, seed=12)
     d = decomp(n, u, v)
     arrs = d.arrays()
     nb = np.diff(arrs["vtx_off"])
-    assert (nb <= 800).any() and (arrs["n_plain"] >= 500).any() and ((nb > 800) & (arrs["n_plain"] < 500)).any()
+    assert (nb <= 600).any() and (arrs["n_plain"] >= 500).any() and ((nb > 600) & (arrs["n_plain"] < 500)).any()
     ctx = P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64 if delta == "fp64" else P.DELTA_FP32C, plain_core=500,
-                    tile_max=800)
+                    tile_max=600)
     plan = ctx.plan(d)
     st = plan.run()
     got = plan.read()
-    assert st["kernel_launches"] == 5  # multi-source, per-source + fold, tile + fold
+    assert st["kernel_launches"] == 5  # multi-source, per-source + fold, tile (warp class) + fold
     assert rel_err(got, oracle_bc(n, u, v)) < TOL[delta]
     plan.close()
     ctx.close()
