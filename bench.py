@@ -36,6 +36,14 @@ FALLBACK_HBM_GBS = 6650.0
 METRIC = "exact-BC TEPS on 1 B200, batched vs plain, at FP64-oracle rel err \u22641e-6"
 
 
+def load_graphs():
+    """The seeded workload generators (numpy only; loads no native library)."""
+    spec = importlib.util.spec_from_file_location("bench_graphs", PKG_DIR / "graphs.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def load_pkg():
     name = "centrality_gpu_b200"
     if name in sys.modules:
@@ -128,9 +136,21 @@ def step_ranges(plan, target_sources):
     return list(zip(bounds[:-1], bounds[1:]))
 
 
-def cpu_sample(P, arrs, budget_s, threads):
+def oracle_largest_bcc(n, u, v):
+    """The largest BCC (by edges) as the oracle alone decomposes and packs it
+    (linear-time BCC split, reach and chains in oracle/bc_oracle.c), with the
+    oracle's articulation terms: the CPU legs use no part of the product."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O  # the checker: CPU legs only
+    nbcc, eb, art = O.decompose_linear(n, u, v)
+    big = int(np.argmax(np.bincount(eb, minlength=max(nbcc, 1))))
+    return O.pack_bcc(n, u, v, eb, big), art
+
+
+def cpu_sample(arrs, budget_s, threads):
     """Times the oracle's per-BCC kernel (CPU restatement of the method) on an
-    evenly spaced sample of the largest BCC's sources, sized to ~budget_s."""
+    evenly spaced sample of the sources of the BCC in arrs (the oracle's own
+    packing of the largest BCC), sized to ~budget_s."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O  # the checker: CPU-baseline leg only
     nb = int(arrs["vtx_off"][1] - arrs["vtx_off"][0])
@@ -147,11 +167,13 @@ def cpu_sample(P, arrs, budget_s, threads):
     return {"sources": count, "arcs": arcs, "vertices": nb, "seconds": dt, "gteps": count * arcs / dt / 1e9}
 
 
-def cpu_unit_check(P, plan, arrs, threads):
-    """CPU-baseline leg: times the oracle's per-BCC kernel (the method's CPU
-    restatement) on exactly the sources of one GPU work unit of the largest
-    BCC, on all host threads, and reports the max relative BC error of that
-    unit's GPU result against it."""
+def cpu_unit_check(plan, arrs, oarrs, oart, threads):
+    """CPU-baseline and accuracy leg: times the oracle's per-BCC kernel (the
+    method's CPU restatement) on exactly the sources of one GPU work unit of
+    the largest BCC, on all host threads, on the oracle's own decomposition
+    and packing of that BCC (oarrs, oart), and reports the max relative BC
+    error of the unit's GPU result (plus the GPU's articulation terms) against
+    the oracle's (plus the oracle's articulation terms)."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O  # the checker: CPU-baseline leg only
     v0, v1 = int(arrs["vtx_off"][0]), int(arrs["vtx_off"][1])
@@ -165,16 +187,48 @@ def cpu_unit_check(P, plan, arrs, threads):
     plan.reset()
     plan.run(k0, k0 + 1, stats=False)
     got = plan.read()
-    local = (ids - v0).astype(np.int32)
+    n = len(got)
+    onb = int(oarrs["n_packed"])
+    if onb != v1 - v0:
+        raise RuntimeError(f"oracle's largest BCC has {onb} vertices, the product's {v1 - v0}")
+    to_local = np.full(n, -1, dtype=np.int64)
+    to_local[oarrs["orig"]] = np.arange(onb)
+    local = to_local[arrs["orig"][ids]].astype(np.int32)  # the unit's sources in the oracle's packing
+    if (local < 0).any():
+        raise RuntimeError("a GPU source is not in the oracle's largest BCC")
     t = time.perf_counter()
-    contrib = O.bcc_sources(arrs, 0, local, threads)
+    contrib = O.bcc_sources(oarrs, 0, local, threads)
     dt = time.perf_counter() - t
-    want = np.array(arrs["art"], dtype=np.float64)
-    np.add.at(want, arrs["orig"][v0:v1], contrib)
+    want = np.array(oart, dtype=np.float64)
+    np.add.at(want, oarrs["orig"], contrib)
     err = float(np.max(np.abs(got - want) / np.maximum(1.0, np.abs(want))))
     arcs = int(arrs["row"][v1] - arrs["row"][v0])
     return {"unit": k0, "sources": len(ids), "arcs": arcs, "vertices": v1 - v0, "seconds": dt,
             "gteps": len(ids) * arcs / dt / 1e9, "max_rel_err": err}
+
+
+def batch_graph_check(P, plan, G, threads, count=16):
+    """Accuracy of a whole run of the batch of independent graphs: the GPU's BC
+    of every vertex of a seeded sample of `count` graphs against the oracle's
+    restatement of the method (its own decomposition) run on each graph alone."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O  # the checker
+    batch = G.gen_ba_batch(4096, seed=4)
+    offs = np.concatenate(([0], np.cumsum([g[0] for g in batch])))
+    plan.reset()
+    plan.run(stats=False)
+    got = plan.read()
+    pick = np.sort(np.random.default_rng(2024).choice(len(batch), size=count, replace=False))
+    err, verts = 0.0, 0
+    for i in pick:
+        n, u, v = batch[i]
+        want = O.method_bc(n, u, v, threads)
+        mine = got[offs[i]:offs[i] + n]
+        err = max(err, float(np.max(np.abs(mine - want) / np.maximum(1.0, np.abs(want)))))
+        verts += n
+    return {"max_rel_err": err, "vs": "FP64 CPU oracle (the method restated, its own decomposition), per graph",
+            "graphs": int(count), "vertices": int(verts), "sample": f"seeded {count} of {len(batch)} graphs, every vertex",
+            "bar": 1e-6}
 
 
 def traffic_per_source(mode, workload):
@@ -230,16 +284,14 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    P = load_pkg()
-    from centrality_gpu_b200 import graphs as G
+    G = load_graphs()  # the seeded generators only: nothing of libbcgpu is loaded on this arm
     desc, gen = WORKLOADS[args.workload]
     n, u, v = gen(G)
-    d = P.Decomposition(P.Graph.from_edges(n, u, v))
-    arrs = d.arrays()
+    arrs, _ = oracle_largest_bcc(n, u, v)
     threads = len(os.sched_getaffinity(0))
     for _ in range(args.warmup):
-        cpu_sample(P, arrs, 0.5, threads)
-    res = [cpu_sample(P, arrs, args.ref_step_s, threads) for _ in range(args.steps)]
+        cpu_sample(arrs, 0.5, threads)
+    res = [cpu_sample(arrs, args.ref_step_s, threads) for _ in range(args.steps)]
     secs = sum(r["seconds"] for r in res)
     value = sum(r["sources"] * r["arcs"] for r in res) / secs / 1e9
     line = {
@@ -247,7 +299,8 @@ def run_reference(args):
         "unit": "GTEPS", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{args.workload}: {desc}", "sample": "evenly spaced sources of the largest BCC"},
+        "config": {"workload": f"{args.workload}: {desc}",
+                   "sample": "evenly spaced sources of the largest BCC, decomposed and packed by the oracle"},
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
                          "sample": f"{res[0]['sources']} sources/step of the largest BCC "
                                    f"({res[0]['vertices']} vertices, {res[0]['arcs']} arcs)"},
@@ -485,12 +538,18 @@ def main():
     accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
-        s = cpu_unit_check(P, plan, arrs, threads)
+        oarrs, oart = oracle_largest_bcc(n, u, v)
+        s = cpu_unit_check(plan, arrs, oarrs, oart, threads)
         cpu = {"value": s["gteps"], "unit": "GTEPS", "cores": threads, "kind": "port",
                "sample": f"the {s['sources']} sources of GPU unit {s['unit']} (largest BCC: {s['vertices']} vertices, "
                          f"{s['arcs']} arcs), oracle per-BCC kernel, {s['seconds']:.1f} s"}
-        accuracy = {"max_rel_err": s["max_rel_err"], "vs": "FP64 CPU oracle on the same sources",
+        accuracy = {"max_rel_err": s["max_rel_err"],
+                    "vs": "FP64 CPU oracle on the same sources, on the oracle's own decomposition",
                     "sources": s["sources"], "bar": 1e-6}
+        if whole:  # the batch of graphs: every vertex of sampled graphs, after one whole run
+            unit_err = accuracy["max_rel_err"]
+            accuracy = batch_graph_check(P, plan, G, threads)
+            accuracy["unit_check_max_rel_err"] = unit_err
 
     if rank == 0:
         info = d.info

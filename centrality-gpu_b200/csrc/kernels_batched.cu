@@ -42,6 +42,7 @@
 // deterministic (the reference uses FP32 atomics, Codes/kernels_free.cu:423-426).
 // The whole GPU works on one batch at a time: a cooperative persistent kernel
 // with a grid barrier whose waits are bounded (error flag, no hang).
+#include "accum.cuh"
 #include "batched.h"
 #include "common.cuh"
 
@@ -67,6 +68,17 @@ constexpr int kHeavyDegSmall = 32; // ... or than this, on cores small enough th
 constexpr int kSmallCore = 16384;  // cores below this many vertices use kHeavyDegSmall
 constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr int kHalf = 4;           // words per pass over a vertex row
+// Resident CTAs per SM the kernel is compiled for (registers per thread =
+// 65536 / (kThreads * kMinCtas)) and hit values gathered at once per lane in
+// a row pass; profiling builds may override both.
+#ifndef BCGPU_BATCHED_MIN_CTAS
+#define BCGPU_BATCHED_MIN_CTAS 4
+#endif
+#ifndef BCGPU_BATCHED_GATHER
+#define BCGPU_BATCHED_GATHER 4
+#endif
+constexpr int kMinCtas = BCGPU_BATCHED_MIN_CTAS;
+constexpr int kGatherHits = BCGPU_BATCHED_GATHER;
 
 // One source of a pass. chain < 0: the core vertex src (level 0). Otherwise
 // src is the chain vertex at position pos of chain `chain` (global index).
@@ -271,9 +283,9 @@ template <bool kTail>
 __device__ __forceinline__ double fed_dep(const Stretch &s, int i, const End &A, const End &B, int D) {
   const int m = s.m();
   const int P = min(m - 1, D / 2);  // last vertex fed from A
-  if ((D & 1) == 0 && D / 2 <= m - 1) return s.pre(P) - s.pre(i + 1) + s.wt(P) / (1.0 + ldexp(B.s / A.s, B.x - A.x));
+  if ((D & 1) == 0 && D / 2 <= m - 1) return s.pre(P) - s.pre(i + 1) + s.wt(P) / (1.0 + scale2(B.s / A.s, B.x - A.x));
   double v = s.pre(P + 1) - s.pre(i + 1);
-  if (kTail && P == m - 1 && B.d == A.d + m + 1) v += ldexp(A.s * B.qs, A.x - B.x);
+  if (kTail && P == m - 1 && B.d == A.d + m + 1) v += scale2(A.s * B.qs, A.x - B.x);
   return v;
 }
 
@@ -392,9 +404,9 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
       const int32_t *xb = kLev ? a.X + (int64_t)((w0 + k) * 32 + lane) * (a.tcap + 2) : nullptr;
       const int xt = kLev ? __ldcg(xb + t) : 0;
       while (hits) {  // uniform
-        T x[4];
+        T x[kGatherHits];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < kGatherHits; ++r) {
           x[r] = (T)0;
           if (hits) {  // uniform
             const int j = __ffs(hits) - 1;
@@ -404,12 +416,12 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
             const int lj = kLev ? __shfl_sync(0xffffffffu, lvl, j) : 0;
             if ((fj >> lane) & 1u) {
               x[r] = __ldcg(vk + (int64_t)uj * W * 32);
-              if (kLev) x[r] = (T)ldexp((double)x[r], kLev == 1 ? __ldcg(xb + lj) - xt : xt - __ldcg(xb + lj));
+              if (kLev) x[r] = (T)scale2((double)x[r], kLev == 1 ? __ldcg(xb + lj) - xt : xt - __ldcg(xb + lj));
             }
           }
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) acc[k].add((double)x[r]);
+        for (int r = 0; r < kGatherHits; ++r) acc[k].add((double)x[r]);
       }
     }
   }
@@ -426,8 +438,8 @@ __device__ __forceinline__ int finish_pull(const Args &a, int32_t v, int w, int 
   if ((newm >> lane) & 1u) {
     a.d[idx] = t + 1;
     a.sig[idx] = acc;
-    if (acc > ldexp(1.0, a.rescale_exp)) {
-      atomicMax(a.rexp + w * 32 + lane, ilogb(acc));
+    if (exp_bits(acc) - 1023 >= a.rescale_exp && acc > pow2(a.rescale_exp)) {  // acc > 2^rescale_exp, acc normal
+      atomicMax(a.rexp + w * 32 + lane, exp_bits(acc) - 1023);
       a.ctrl->rescale[t & 1] = 1;
     }
   }
@@ -511,7 +523,7 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
             }
             const double sb = __ldcg(a.sig + ib);
             const int xbb = __ldcg(xb + dB[r]);
-            sum += (double)P + 1.0 / (1.0 + ldexp(sb / A.s, xbb - A.x));
+            sum += (double)P + 1.0 / (1.0 + scale2(sb / A.s, xbb - A.x));
           } else {
             sum += (double)(min(kj[r] - 1, P) + 1);
           }
@@ -556,7 +568,7 @@ __device__ __forceinline__ void finish_dep(const Args &a, const Slot *slots, con
     const int64_t idx = ((int64_t)v * W + w) * 32 + lane;
     const double sv = a.sig[idx];
     const int xd = a.X[(int64_t)b * (a.tcap + 2) + lev] - a.X[(int64_t)b * (a.tcap + 2) + lev + 1];
-    const double delta = ldexp(sv * sum, xd) + (chains ? __ldcg(a.cdep + idx) : 0.0);
+    const double delta = scale2(sv * sum, xd) + (chains ? __ldcg(a.cdep + idx) : 0.0);
     const double qv = ((double)rch[v] + 1.0 + delta) / sv;
     if (kF32) {
       const double aq = fabs(qv);
@@ -583,7 +595,7 @@ __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
 // --------------------------------------------------------------- kernel ----
 
 template <typename QT>
-__global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   WarpScratch *scratch = reinterpret_cast<WarpScratch *>(s_raw);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -802,7 +814,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int b = s.slot, w = b >> 5;
           const uint32_t bit = 1u << (b & 31);
           const int64_t idx = ((int64_t)s.v * W + w) * 32 + (b & 31);
-          const double one = ldexp(1.0, -a.X[(int64_t)b * (a.tcap + 2) + t]);
+          const double one = scale2(1.0, -a.X[(int64_t)b * (a.tcap + 2) + t]);
           const uint32_t old = atomicOr(a.seen + (int64_t)s.v * W + w, bit);
           if (!(old & bit)) {
             a.d[idx] = t + 1;
@@ -837,7 +849,7 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
           const int re = __ldcg(a.rexp + w * 32 + lane);
           if (((m >> lane) & 1u) && re > a.rescale_exp) {
             const int64_t idx = ((int64_t)v * W + w) * 32 + lane;
-            a.sig[idx] = ldexp(a.sig[idx], -re);
+            a.sig[idx] = scale2(a.sig[idx], -re);
           }
         }
       }
@@ -1046,13 +1058,13 @@ __global__ void __launch_bounds__(kThreads, 4) batched_kernel(Args a) {
             if (D >= 0 && (D & 1) == 0 && D / 2 <= k - 1) {
               tv = D / 2;
               const double p0 = chain_pre(P, tv), p1 = chain_pre(P, tv + 1), wt = p1 - p0;
-              fL = p0 + wt / (1.0 + ldexp(eR.s / eL.s, eR.x - eL.x));
-              fR = -p1 + wt / (1.0 + ldexp(eL.s / eR.s, eL.x - eR.x));
+              fL = p0 + wt / (1.0 + scale2(eR.s / eL.s, eR.x - eL.x));
+              fR = -p1 + wt / (1.0 + scale2(eL.s / eR.s, eL.x - eR.x));
             } else {
               pl = D >= 0 ? min(k - 1, D / 2) : -1;
               const double p1 = chain_pre(P, pl + 1);
-              fL = p1 + (eR.d == eL.d + k + 1 ? ldexp(eL.s * eR.qs, eL.x - eR.x) : 0.0);
-              fR = -p1 + (eL.d == eR.d + k + 1 ? ldexp(eR.s * eL.qs, eR.x - eL.x) : 0.0);
+              fL = p1 + (eR.d == eL.d + k + 1 ? scale2(eL.s * eR.qs, eL.x - eR.x) : 0.0);
+              fR = -p1 + (eL.d == eR.d + k + 1 ? scale2(eR.s * eL.qs, eR.x - eL.x) : 0.0);
             }
           }
           auto dep_of = [&](int j) -> double {

@@ -411,3 +411,211 @@ int32_t orc_method_bc(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev
   free(edge_bcc); free(art); free(reach); free(loc); free(deg);
   return nbcc;
 }
+
+/* ------------------------------------------------- linear decomposition --- */
+
+/* Depth-first search state of the whole graph (iterative, explicit stacks). */
+typedef struct {
+  int32_t n, nbcc;
+  int64_t *R;          /* adjacency CSR with edge ids */
+  int32_t *C, *E;
+  int32_t *disc, *low, *parent, *pe, *sub, *root;
+  int64_t *sep, *sep_sq; /* per vertex: sum (and sum of squares) of the subtree sizes of its separating children */
+} Dfs;
+
+static void dfs_free(Dfs *g) {
+  free(g->R); free(g->C); free(g->E); free(g->disc); free(g->low); free(g->parent); free(g->pe); free(g->sub);
+  free(g->root); free(g->sep); free(g->sep_sq);
+}
+
+/* Hopcroft-Tarjan: edge_bcc[e] gets a BCC id in order of discovery. */
+static void dfs_run(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev, Dfs *g, int32_t *edge_bcc) {
+  g->n = n;
+  g->R = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+  g->C = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(2 * m + 1));
+  g->E = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(2 * m + 1));
+  for (int64_t e = 0; e < m; ++e) { g->R[eu[e] + 1]++; g->R[ev[e] + 1]++; }
+  for (int32_t v = 0; v < n; ++v) g->R[v + 1] += g->R[v];
+  int64_t *fill = (int64_t *)xmalloc(sizeof(int64_t) * (size_t)(n + 1));
+  memcpy(fill, g->R, sizeof(int64_t) * (size_t)(n + 1));
+  for (int64_t e = 0; e < m; ++e) {
+    g->C[fill[eu[e]]] = ev[e]; g->E[fill[eu[e]]++] = (int32_t)e;
+    g->C[fill[ev[e]]] = eu[e]; g->E[fill[ev[e]]++] = (int32_t)e;
+  }
+  size_t nn = (size_t)(n > 0 ? n : 1);
+  g->disc = (int32_t *)xmalloc(sizeof(int32_t) * nn); g->low = (int32_t *)xmalloc(sizeof(int32_t) * nn);
+  g->parent = (int32_t *)xmalloc(sizeof(int32_t) * nn); g->pe = (int32_t *)xmalloc(sizeof(int32_t) * nn);
+  g->sub = (int32_t *)xmalloc(sizeof(int32_t) * nn); g->root = (int32_t *)xmalloc(sizeof(int32_t) * nn);
+  g->sep = (int64_t *)calloc(nn, sizeof(int64_t)); g->sep_sq = (int64_t *)calloc(nn, sizeof(int64_t));
+  int64_t *it = fill; /* reused as the per-vertex adjacency cursor */
+  int32_t *vs = (int32_t *)xmalloc(sizeof(int32_t) * nn);
+  int32_t *es = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+  for (int32_t v = 0; v < n; ++v) { g->disc[v] = -1; it[v] = g->R[v]; }
+  int32_t t = 0, nbcc = 0;
+  for (int32_t r = 0; r < n; ++r) {
+    if (g->disc[r] >= 0) continue;
+    int32_t top = 0;
+    int64_t etop = 0;
+    vs[top++] = r;
+    g->disc[r] = g->low[r] = t++; g->parent[r] = -1; g->pe[r] = -1; g->sub[r] = 1; g->root[r] = r;
+    while (top > 0) {
+      const int32_t v = vs[top - 1];
+      if (it[v] < g->R[v + 1]) {
+        const int32_t w = g->C[it[v]], e = g->E[it[v]];
+        ++it[v];
+        if (e == g->pe[v]) continue;
+        if (g->disc[w] < 0) {
+          es[etop++] = e;
+          g->parent[w] = v; g->pe[w] = e; g->disc[w] = g->low[w] = t++; g->sub[w] = 1; g->root[w] = r;
+          vs[top++] = w;
+        } else if (g->disc[w] < g->disc[v]) { /* back edge to an ancestor */
+          es[etop++] = e;
+          if (g->disc[w] < g->low[v]) g->low[v] = g->disc[w];
+        }
+      } else {
+        --top;
+        const int32_t p = g->parent[v];
+        if (p < 0) continue;
+        if (g->low[v] < g->low[p]) g->low[p] = g->low[v];
+        g->sub[p] += g->sub[v];
+        if (g->low[v] >= g->disc[p]) { /* p separates v's subtree: the edges above it on the stack form a BCC */
+          g->sep[p] += g->sub[v];
+          g->sep_sq[p] += (int64_t)g->sub[v] * g->sub[v];
+          int32_t e;
+          do { e = es[--etop]; edge_bcc[e] = nbcc; } while (e != g->pe[v]);
+          ++nbcc;
+        }
+      }
+    }
+  }
+  g->nbcc = nbcc;
+  free(fill); free(vs); free(es);
+}
+
+int32_t orc_decompose_linear(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev, int32_t *edge_bcc,
+                             double *art_term) {
+  Dfs g;
+  dfs_run(n, m, eu, ev, &g, edge_bcc);
+  /* renumber by smallest edge index (orc_decompose's numbering) */
+  int32_t *first = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(g.nbcc > 0 ? g.nbcc : 1));
+  int32_t *map = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(g.nbcc > 0 ? g.nbcc : 1));
+  for (int32_t b = 0; b < g.nbcc; ++b) first[b] = -1;
+  int32_t next = 0;
+  for (int64_t e = 0; e < m; ++e)
+    if (first[edge_bcc[e]] < 0) { first[edge_bcc[e]] = (int32_t)e; map[edge_bcc[e]] = next++; }
+  for (int64_t e = 0; e < m; ++e) edge_bcc[e] = map[edge_bcc[e]];
+  /* articulation cross terms: S^2 - sum of squared part sizes, the parts being
+   * the separating children's subtrees and (below the root) the rest of the
+   * component (Codes/modified_apsp.cpp:157-220) */
+  for (int32_t v = 0; v < n; ++v) {
+    const int64_t S = (int64_t)g.sub[g.root[v]] - 1;
+    int64_t sq = g.sep_sq[v];
+    if (g.parent[v] >= 0) {
+      const int64_t rest = S - g.sep[v];
+      sq += rest * rest;
+    }
+    art_term[v] = (double)(S * S - sq);
+  }
+  const int32_t nb = g.nbcc;
+  free(first); free(map); dfs_free(&g);
+  return nb;
+}
+
+/* Vertex count and edge count of BCC b. */
+void orc_bcc_size(int64_t m, const int32_t *eu, const int32_t *ev, const int32_t *edge_bcc, int32_t n, int32_t b,
+                  int32_t *nb_out, int64_t *mb_out) {
+  char *in = (char *)calloc((size_t)(n > 0 ? n : 1), 1);
+  int32_t nb = 0;
+  int64_t mb = 0;
+  for (int64_t e = 0; e < m; ++e) {
+    if (edge_bcc[e] != b) continue;
+    ++mb;
+    if (!in[eu[e]]) { in[eu[e]] = 1; ++nb; }
+    if (!in[ev[e]]) { in[ev[e]] = 1; ++nb; }
+  }
+  free(in);
+  *nb_out = nb;
+  *mb_out = mb;
+}
+
+int32_t orc_pack_bcc(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev, const int32_t *edge_bcc, int32_t b,
+                     int32_t *vert_out, int64_t *R, int32_t *C, int32_t *reach_out, int32_t *chain_start,
+                     int32_t *chain_len, int32_t *chain_l, int32_t *chain_r) {
+  /* a fresh DFS for subtree sizes (the BCC partition does not depend on the DFS) */
+  int32_t *eb2 = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+  Dfs g;
+  dfs_run(n, m, eu, ev, &g, eb2);
+  free(eb2);
+  int32_t *loc = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  int32_t *deg = (int32_t *)calloc((size_t)(n > 0 ? n : 1), sizeof(int32_t));
+  for (int32_t v = 0; v < n; ++v) loc[v] = -1;
+  int32_t nb = 0;
+  int64_t mb = 0;
+  for (int64_t e = 0; e < m; ++e) {
+    if (edge_bcc[e] != b) continue;
+    ++mb; deg[eu[e]]++; deg[ev[e]]++;
+    if (loc[eu[e]] < 0) loc[eu[e]] = nb++;
+    if (loc[ev[e]] < 0) loc[ev[e]] = nb++;
+  }
+  int32_t *vert = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(nb > 0 ? nb : 1));
+  for (int32_t v = 0; v < n; ++v) if (loc[v] >= 0) vert[loc[v]] = v;
+  /* reach: the head (smallest discovery time) loses everything but the
+   * subtree of its child in this BCC; any other vertex keeps exactly the
+   * subtrees of its separating children */
+  int32_t head = vert[0];
+  for (int32_t i = 1; i < nb; ++i) if (g.disc[vert[i]] < g.disc[head]) head = vert[i];
+  int32_t cb = -1;
+  for (int64_t e = g.R[head]; e < g.R[head + 1]; ++e)
+    if (edge_bcc[g.E[e]] == b && g.parent[g.C[e]] == head && g.pe[g.C[e]] == g.E[e]) cb = g.C[e];
+  int is_cycle = 1;
+  for (int32_t i = 0; i < nb; ++i) if (deg[vert[i]] != 2) { is_cycle = 0; break; }
+  int64_t *R0 = (int64_t *)calloc((size_t)nb + 1, sizeof(int64_t));
+  int32_t *C0 = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(2 * mb + 1));
+  for (int32_t i = 0; i < nb; ++i) R0[i + 1] = R0[i] + deg[vert[i]];
+  int64_t *fill = (int64_t *)xmalloc(sizeof(int64_t) * (size_t)(nb > 0 ? nb : 1));
+  memcpy(fill, R0, sizeof(int64_t) * (size_t)nb);
+  for (int64_t e = 0; e < m; ++e) {
+    if (edge_bcc[e] != b) continue;
+    const int32_t a = loc[eu[e]], c = loc[ev[e]];
+    C0[fill[a]++] = c; C0[fill[c]++] = a;
+  }
+  /* new ids: non-chain vertices first, then each maximal degree-2 path
+   * contiguous from chain_l to chain_r (a cycle BCC has none) */
+  int32_t *nid = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(nb > 0 ? nb : 1));
+  int32_t *old = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(nb > 0 ? nb : 1));
+  for (int32_t i = 0; i < nb; ++i) nid[i] = -1;
+  int32_t next = 0, nch = 0;
+  for (int32_t i = 0; i < nb; ++i)
+    if (is_cycle || deg[vert[i]] != 2) { nid[i] = next; old[next] = i; ++next; }
+  if (!is_cycle) {
+    for (int32_t i = 0; i < nb; ++i) {
+      if (deg[vert[i]] == 2) continue;
+      for (int64_t e = R0[i]; e < R0[i + 1]; ++e) {
+        int32_t prev = i, cur = C0[e];
+        if (deg[vert[cur]] != 2 || nid[cur] >= 0) continue;
+        const int32_t start = next;
+        while (deg[vert[cur]] == 2) {
+          nid[cur] = next; old[next] = cur; ++next;
+          const int32_t a = C0[R0[cur]], c = C0[R0[cur] + 1];
+          const int32_t nx = (a == prev) ? c : a;
+          prev = cur; cur = nx;
+        }
+        chain_start[nch] = start; chain_len[nch] = next - start; chain_l[nch] = nid[i]; chain_r[nch] = cur;
+        ++nch;
+      }
+    }
+    for (int32_t c = 0; c < nch; ++c) chain_r[c] = nid[chain_r[c]];
+  }
+  R[0] = 0;
+  for (int32_t k = 0; k < nb; ++k) R[k + 1] = R[k] + (R0[old[k] + 1] - R0[old[k]]);
+  for (int32_t k = 0; k < nb; ++k) {
+    int64_t o = R[k];
+    for (int64_t e = R0[old[k]]; e < R0[old[k] + 1]; ++e) C[o++] = nid[C0[e]];
+    const int32_t x = vert[old[k]];
+    vert_out[k] = x;
+    reach_out[k] = x == head ? (cb >= 0 ? g.sub[g.root[x]] - 1 - g.sub[cb] : 0) : (int32_t)g.sep[x];
+  }
+  free(loc); free(deg); free(vert); free(R0); free(C0); free(fill); free(nid); free(old);
+  dfs_free(&g);
+  return nch;
+}

@@ -74,6 +74,27 @@ void orc_bcc_source_rows(int32_t nb, const int64_t *R, const int32_t *C, int32_t
                          const int32_t *chain_start, const int32_t *chain_len, const int32_t *chain_l,
                          const int32_t *chain_r, int32_t s, int32_t *d, double *sigma);
 
+/* The same decomposition in linear time (iterative Hopcroft-Tarjan over an
+ * explicit edge stack; articulation terms from the DFS subtree sizes), with
+ * orc_decompose's outputs and numbering. For graphs beyond the brute force's
+ * reach (the RMAT workloads); pinned against orc_decompose by the tests. */
+int32_t orc_decompose_linear(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev, int32_t *edge_bcc,
+                             double *art_term);
+
+/* Vertices and edges of BCC b (edge_bcc from either decomposition). */
+void orc_bcc_size(int64_t m, const int32_t *eu, const int32_t *ev, const int32_t *edge_bcc, int32_t n, int32_t b,
+                  int32_t *nb_out, int64_t *mb_out);
+
+/* BCC b in the packed per-BCC format of orc_bcc_sources, built by the
+ * oracle alone: vert_out[k] original id of local vertex k (non-chain vertices
+ * first, then each maximal degree-2 path from chain_l to chain_r), R [nb+1],
+ * C [2 mb] local ids, reach_out [nb] (vertices outside the BCC hanging off
+ * the vertex, from DFS subtree sizes), chains (arrays of nb entries).
+ * Returns the number of chains. */
+int32_t orc_pack_bcc(int32_t n, int64_t m, const int32_t *eu, const int32_t *ev, const int32_t *edge_bcc, int32_t b,
+                     int32_t *vert_out, int64_t *R, int32_t *C, int32_t *reach_out, int32_t *chain_start,
+                     int32_t *chain_len, int32_t *chain_l, int32_t *chain_r);
+
 #ifdef __cplusplus
 }
 #endif

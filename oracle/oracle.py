@@ -46,6 +46,12 @@ def lib():
                                       C.c_int64, C.c_int, _f64p]
         L.orc_bcc_source_rows.argtypes = [C.c_int32, _i64p, _i32p, C.c_int32, _i32p, _i32p, _i32p, _i32p, C.c_int32,
                                           _i32p, _f64p]
+        L.orc_decompose_linear.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, _i32p, _f64p]
+        L.orc_decompose_linear.restype = C.c_int32
+        L.orc_bcc_size.argtypes = [C.c_int64, _i32p, _i32p, _i32p, C.c_int32, C.c_int32, _i32p, _i64p]
+        L.orc_pack_bcc.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, _i32p, C.c_int32, _i32p, _i64p, _i32p, _i32p,
+                                   _i32p, _i32p, _i32p, _i32p]
+        L.orc_pack_bcc.restype = C.c_int32
         _lib = L
     return _lib
 
@@ -96,6 +102,41 @@ def decompose(n, u, v):
     art = np.zeros(n, dtype=np.float64)
     nb = lib().orc_decompose(n, len(u), _p(u, _i32p), _p(v, _i32p), _p(eb, _i32p), _p(art, _f64p))
     return nb, eb, art
+
+
+def decompose_linear(n, u, v):
+    """Linear-time BCC split with decompose()'s outputs: (n_bcc, edge_bcc, art_term)."""
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    eb = np.zeros(len(u), dtype=np.int32)
+    art = np.zeros(n, dtype=np.float64)
+    nb = lib().orc_decompose_linear(n, len(u), _p(u, _i32p), _p(v, _i32p), _p(eb, _i32p), _p(art, _f64p))
+    return nb, eb, art
+
+
+def pack_bcc(n, u, v, edge_bcc, b):
+    """BCC b packed by the oracle alone, as a one-BCC arrays dict that
+    bcc_sources(arrs, 0, ...) takes: orig (original ids), row, col, reach,
+    n_plain and the chain table."""
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    eb = np.ascontiguousarray(edge_bcc, dtype=np.int32)
+    nb = C.c_int32()
+    mb = C.c_int64()
+    lib().orc_bcc_size(len(u), _p(u, _i32p), _p(v, _i32p), _p(eb, _i32p), n, int(b), C.byref(nb), C.byref(mb))
+    k, m2 = nb.value, 2 * mb.value
+    vert = np.zeros(max(k, 1), np.int32)
+    row = np.zeros(k + 1, np.int64)
+    col = np.zeros(max(m2, 1), np.int32)
+    rch = np.zeros(max(k, 1), np.int32)
+    ch = [np.zeros(max(k, 1), np.int32) for _ in range(4)]
+    nch = lib().orc_pack_bcc(n, len(u), _p(u, _i32p), _p(v, _i32p), _p(eb, _i32p), int(b), _p(vert, _i32p),
+                             _p(row, _i64p), _p(col, _i32p), _p(rch, _i32p), *[_p(c, _i32p) for c in ch])
+    plain = k - int(ch[1][:nch].sum())
+    return {"n_bcc": 1, "n_packed": k, "vtx_off": np.array([0, k], np.int64), "row": row, "col": col[:m2],
+            "reach": rch[:k], "orig": vert[:k], "n_plain": np.array([plain], np.int32),
+            "chain_off": np.array([0, nch], np.int64), "chain_start": ch[0][:nch], "chain_len": ch[1][:nch],
+            "chain_l": ch[2][:nch], "chain_r": ch[3][:nch]}
 
 
 def reach(n, u, v, edge_bcc, bcc):

@@ -5,7 +5,7 @@ sets). CPU only."""
 import numpy as np
 import pytest
 
-from helpers import GOLDEN_CASES, canonical_chains, graphs, load_case, oracle, rel_err
+from helpers import GOLDEN_CASES, canonical_chains, graphs, load_case, oracle, pkg, rel_err
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -144,3 +144,54 @@ def test_rows_of_chain_vertex_equal_bfs():
         db, sb = O.bfs_rows(v1 - v0, row, col, s)
         assert np.array_equal(dm, db)
         assert np.array_equal(sm, sb)
+
+
+def test_linear_decomposition_equals_brute_force():
+    """orc_decompose_linear (Hopcroft-Tarjan, DFS subtree sizes) gives
+    orc_decompose's BCC ids and articulation terms, and orc_pack_bcc the
+    reach of orc_reach, on random graphs with chains, leaves, isolated
+    vertices and several components; BC through the linear packing equals
+    Brandes."""
+    G = graphs()
+    O = oracle()
+    rng = np.random.default_rng(7)
+    for t in range(150):
+        n = int(rng.integers(1, 70))
+        m = int(rng.integers(0, 3 * n + 1))
+        u, v = G.simple_edges(n, rng.integers(0, n, m), rng.integers(0, n, m))
+        if len(u) and t % 2 == 0:
+            n, u, v = G.subdivide(n, u, v, 0.3, 1, 4, rng)
+            n, u, v = G.attach_leaves(n, u, v, int(rng.integers(0, 10)), n, rng)
+        nb, eb, art = O.decompose(n, u, v)
+        nl, el, artl = O.decompose_linear(n, u, v)
+        assert nb == nl and np.array_equal(eb, el) and np.array_equal(art, artl), t
+        bc = artl.copy()
+        for b in range(nl):
+            pk = O.pack_bcc(n, u, v, el, b)
+            r = np.full(n, -1)
+            r[pk["orig"]] = pk["reach"]
+            assert np.array_equal(r, O.reach(n, u, v, eb, b)), (t, b)
+            if pk["n_packed"] >= 3:
+                np.add.at(bc, pk["orig"], O.bcc_sources(pk, 0, np.arange(pk["n_packed"], dtype=np.int32)))
+        row, col = O.csr(n, u, v)
+        want = O.brandes(n, row, col)
+        assert np.max(np.abs(bc - want) / np.maximum(1.0, np.abs(want)), initial=0.0) < 1e-12, t
+
+
+def test_linear_packing_of_the_largest_bcc_matches_the_product():
+    """RMAT scale 14 with chains: the oracle's own packing of the largest BCC
+    has the product's vertex set, core size, chain count and per-vertex
+    reach."""
+    G = graphs()
+    O = oracle()
+    P = pkg()
+    n, u, v = G.gen_rmat(14, 16, 0.2, 1, 8, seed=3)
+    nbcc, eb, _ = O.decompose_linear(n, u, v)
+    pk = O.pack_bcc(n, u, v, eb, int(np.argmax(np.bincount(eb))))
+    a = P.Decomposition(P.Graph.from_edges(n, u, v)).arrays()
+    v1 = int(a["vtx_off"][1])
+    assert int(pk["n_packed"]) == v1 and int(pk["n_plain"][0]) == int(a["n_plain"][0])
+    assert len(pk["chain_len"]) == int(a["chain_off"][1])
+    assert np.array_equal(np.sort(pk["orig"]), np.sort(a["orig"][:v1]))
+    mine = dict(zip(a["orig"][:v1].tolist(), a["reach"][:v1].tolist()))
+    assert all(mine[int(x)] == int(r) for x, r in zip(pk["orig"], pk["reach"]))
