@@ -207,17 +207,18 @@ def cpu_unit_check(plan, arrs, oarrs, oart, threads):
             "gteps": len(ids) * arcs / dt / 1e9, "max_rel_err": err}
 
 
-def batch_graph_check(P, plan, G, threads, count=16):
+def batch_graph_check(P, plan, G, threads, count=16, graphs=4096):
     """Accuracy of a whole run of the batch of independent graphs: the GPU's BC
     of every vertex of a seeded sample of `count` graphs against the oracle's
     restatement of the method (its own decomposition) run on each graph alone."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O  # the checker
-    batch = G.gen_ba_batch(4096, seed=4)
+    batch = G.gen_ba_batch(graphs, seed=4)
     offs = np.concatenate(([0], np.cumsum([g[0] for g in batch])))
     plan.reset()
     plan.run(stats=False)
     got = plan.read()
+    count = min(count, len(batch))
     pick = np.sort(np.random.default_rng(2024).choice(len(batch), size=count, replace=False))
     err, verts = 0.0, 0
     for i in pick:
@@ -339,6 +340,8 @@ def main():
                          "BCGPU_LIB_DIR=centrality-gpu_b200/lib_phase)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
+    ap.add_argument("--ba-graphs", type=int, default=4096,
+                    help="ba workload: graphs in the batch (fewer only for small profiler captures)")
     ap.add_argument("--tile-max", type=int, default=0,
                     help="small-BCC schedule: largest BCC it takes (bc_opts.tile_max; 0 = as large as shared "
                          "memory allows, -1 = off)")
@@ -373,6 +376,9 @@ def main():
     P = load_pkg()
     from centrality_gpu_b200 import graphs as G
     desc, gen = WORKLOADS[args.workload]
+    if args.workload == "ba" and args.ba_graphs != 4096:
+        desc = desc.replace("4096", str(args.ba_graphs))
+        gen = lambda G: G.pack_graphs(G.gen_ba_batch(args.ba_graphs, seed=4))[:3]  # noqa: E731
     t0 = time.perf_counter()
     n, u, v = gen(G)
     gen_s = time.perf_counter() - t0  # the seeded workload generator (Python): not the product
@@ -548,7 +554,7 @@ def main():
                     "sources": s["sources"], "bar": 1e-6}
         if whole:  # the batch of graphs: every vertex of sampled graphs, after one whole run
             unit_err = accuracy["max_rel_err"]
-            accuracy = batch_graph_check(P, plan, G, threads)
+            accuracy = batch_graph_check(P, plan, G, threads, graphs=args.ba_graphs)
             accuracy["unit_check_max_rel_err"] = unit_err
 
     if rank == 0:

@@ -329,10 +329,12 @@ int alloc_acc(bc_plan *p, int64_t n_packed) {
   return BCGPU_OK;
 }
 
-// Sources per small-BCC work item: the CTA runs them (a warp each, or one
-// after another) from one staged slice; larger BCCs are split so that many
-// CTAs share them.
+// Sources per small-BCC work item, at most: the CTA runs them (a warp each,
+// or one after another) from one staged slice; larger BCCs are split so that
+// many CTAs share them, and a class with few sources in all gets smaller
+// items, so that it still has several items per resident CTA.
 constexpr int32_t kTileItemSources = 128;
+constexpr int64_t kTileItemsPerCta = 4;
 // BCCs of up to this many vertices take the warp class (a warp per source,
 // eight per CTA); larger ones the CTA class (the CTA on one source).
 constexpr int64_t kTileWarpMaxVertices = 640;
@@ -416,25 +418,33 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, b
     bc_plan::TileLaunch T;
     T.cls = k == 0 ? bcg::kTileWarp : k <= 2 ? bcg::kTileCta : k == 3 ? bcg::kTileCta512 : bcg::kTileCta1024;
     T.i0 = (int64_t)p->h_titems.size();
-    int64_t nmax = 0, smax = 0;
+    int64_t nmax = 0, smax = 0, sources = 0;
     for (int32_t b = 0; b < B->n_bcc; ++b) {
       if (bucket[b] != k) continue;
       const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
-      off[b] = total;
-      total += size[b];
       nmax = std::max(nmax, nb);
       smax = std::max<int64_t>(smax, size[b]);
-      for (int32_t s0 = 0; s0 < nb; s0 += kTileItemSources)
-        p->h_titems.push_back({b, s0, (int32_t)std::min<int64_t>(nb, s0 + kTileItemSources), 0});
+      sources += nb;
     }
-    T.i1 = (int64_t)p->h_titems.size();
-    if (T.i1 == T.i0) continue;
+    if (sources == 0) continue;
     T.nmax = (int32_t)nmax;
     T.slice_max = (int32_t)smax;
     T.smem = bcg::tile_smem_bytes(T.cls, nmax, smax);
     const int per_sm = bcg::tile_ctas_per_sm(T.cls, T.smem);
     if (per_sm < 1) return fail(ctx, BCGPU_ECUDA, "small-BCC schedule: no CTA fits an SM");
     T.grid = ctx->sms * per_sm;
+    const int64_t floor_items = T.cls == bcg::kTileWarp ? bcg::kTileWarps : 1;  // a warp-class item feeds 8 warps
+    const int32_t per_item = (int32_t)std::max<int64_t>(
+        floor_items, std::min<int64_t>(kTileItemSources, sources / ((int64_t)T.grid * kTileItemsPerCta)));
+    for (int32_t b = 0; b < B->n_bcc; ++b) {
+      if (bucket[b] != k) continue;
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+      off[b] = total;
+      total += size[b];
+      for (int32_t s0 = 0; s0 < nb; s0 += per_item)
+        p->h_titems.push_back({b, s0, (int32_t)std::min<int64_t>(nb, s0 + per_item), 0});
+    }
+    T.i1 = (int64_t)p->h_titems.size();
     if (T.cls == bcg::kTileWarp) p->tcap = nmax + 2;
     p->tl.push_back(T);
   }

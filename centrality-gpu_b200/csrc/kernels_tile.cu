@@ -46,10 +46,14 @@ namespace {
 
 constexpr int kThreads = kTileWarps * 32;
 constexpr int kLaneDeg = 8;  // rows up to this many arcs: one lane; longer rows: a whole warp
+// CTA class: long rows of a level queued for the whole CTA (a row beyond the
+// queue's room is scanned at once by the warp that found it).
+constexpr int kLongQueue = 1024;
 
 struct Ctl {
   unsigned long long bar;  // mbarrier of the slice copy
-  int item, next, bcc, nq, tail, pad;
+  int item, next, bcc, pad;
+  int cnt[4], nq[4];  // CTA class: queue tails and long-row queue lengths of three consecutive levels
   int tails[kTileWarps];
 };
 
@@ -63,14 +67,14 @@ struct WarpLayout {  // ctl | counters [nmax][kAccDigits] | per warp: d [nmax], 
   __host__ __device__ static int64_t slice(int64_t nmax) { return warps(nmax) + kTileWarps * per_warp(nmax); }
 };
 template <int kBlock>
-struct CtaLayout {  // ctl | P [nmax] | sq [nmax] | d [nmax] | S [nmax] | lv [kTileMaxLevels] | queue [kBlock] | slice
+struct CtaLayout {  // ctl | P [nmax] | sq [nmax] | d [nmax] | S [nmax] | lv [kTileMaxLevels] | q [kLongQueue] | slice
   __host__ __device__ static int64_t P() { return align16(sizeof(Ctl)); }
   __host__ __device__ static int64_t sq(int64_t nmax) { return P() + align16(8 * nmax); }
   __host__ __device__ static int64_t d(int64_t nmax) { return sq(nmax) + align16(8 * nmax); }
   __host__ __device__ static int64_t S(int64_t nmax) { return d(nmax) + align16(4 * nmax); }
   __host__ __device__ static int64_t lv(int64_t nmax) { return S(nmax) + align16(4 * nmax); }
   __host__ __device__ static int64_t q(int64_t nmax) { return lv(nmax) + align16(4 * kTileMaxLevels); }
-  __host__ __device__ static int64_t slice(int64_t nmax) { return q(nmax) + align16(4 * kBlock); }
+  __host__ __device__ static int64_t slice(int64_t nmax) { return q(nmax) + align16(4 * kLongQueue); }
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -381,11 +385,25 @@ __global__ void __launch_bounds__(kThreads, 1) tile_warp_kernel(TileArgs a) {
 
 // ======================================================== CTA per source ===
 
+// BFS of the whole CTA from s, two barriers per level: the frontier's rows of
+// up to kLaneDeg arcs are scanned by one thread each (chunks of a level are
+// independent: they read the previous level only) while longer rows are
+// queued; after a barrier the warps share the queued rows; a second barrier
+// ends the level. Queue and tail counters of level l are cnt[l % 3] and
+// nq[l % 3]; those of level l+1 are cleared at the start of level l, two
+// barriers after their last reader.
 template <int kBlock>
 __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double *sq, int32_t *S, int32_t *lv, int32_t *q,
-                       Ctl &ctl, int *err) {
+                       int *cnt, int *nq, int *err) {
+  constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int v = tid; v < nb; v += kBlock) d[v] = -1;
+  if (tid == 0) {
+    cnt[0] = 0;
+    cnt[1] = 0;
+    nq[0] = 0;
+    nq[1] = 0;
+  }
   __syncthreads();
   if (tid == 0) {
     d[s] = 0;
@@ -393,35 +411,53 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double 
     sq[s] = 1.0;
     lv[0] = 0;
     lv[1] = 1;
-    ctl.tail = 1;
   }
   __syncthreads();
   int lev = 0, f0 = 0, f1 = 1;
   while (true) {
     const int dprev = lev == 0 ? INT_MIN : lev - 1, dnext = lev + 1;
-    for (int c0 = f0; c0 < f1; c0 += kBlock) {
-      if (tid == 0) ctl.nq = 0;
-      __syncthreads();
-      const int i = c0 + tid;
-      if (i < f1) {
-        const int32_t w = S[i];
-        const int e0 = g.R[w], e1 = g.R[w + 1];
-        if (e1 - e0 <= kLaneDeg) {
-          const double acc = pull_row(g, e0, e1, d, sq, S, &ctl.tail, dprev, dnext);
-          if (lev > 0) sq[w] = acc;
-        } else {
-          q[atomicAdd(&ctl.nq, 1)] = w;
-        }
-      }
-      __syncthreads();
-      for (int k = warp; k < ctl.nq; k += kBlock / 32) {
-        const int32_t w = q[k];
-        const double acc = pull_row_warp(g, g.R[w], g.R[w + 1], d, sq, S, &ctl.tail, dprev, dnext, lane);
-        if (lane == 0 && lev > 0) sq[w] = acc;
-      }
-      __syncthreads();
+    int *tail = cnt + lev % 3, *nql = nq + lev % 3;
+    if (tid == 0) {
+      cnt[(lev + 1) % 3] = 0;
+      nq[(lev + 1) % 3] = 0;
     }
-    const int t = ctl.tail;
+    for (int c0 = f0; c0 < f1; c0 += kBlock) {  // uniform
+      const int i = c0 + tid;
+      int32_t w = -1, e0 = 0, e1 = 0;
+      if (i < f1) {
+        w = S[i];
+        e0 = g.R[w];
+        e1 = g.R[w + 1];
+      }
+      const bool big = e1 - e0 > kLaneDeg;
+      if (w >= 0 && !big) {
+        const double acc = pull_row(g, e0, e1, d, sq, S + f1, tail, dprev, dnext);
+        if (lev > 0) sq[w] = acc;
+      }
+      bool mine = false;  // a long row the queue had no room for
+      if (w >= 0 && big) {
+        const int pos = atomicAdd(nql, 1);
+        if (pos < kLongQueue) q[pos] = w;
+        else mine = true;
+      }
+      uint32_t over = __ballot_sync(0xffffffffu, mine);
+      while (over) {
+        const int j = __ffs(over) - 1;
+        over &= over - 1;
+        const int32_t wj = __shfl_sync(0xffffffffu, w, j);
+        const double acc = pull_row_warp(g, g.R[wj], g.R[wj + 1], d, sq, S + f1, tail, dprev, dnext, lane);
+        if (lane == 0 && lev > 0) sq[wj] = acc;
+      }
+    }
+    __syncthreads();
+    const int nlong = min(*(volatile int *)nql, kLongQueue);
+    for (int k = warp; k < nlong; k += kWarps) {
+      const int32_t w = q[k];
+      const double acc = pull_row_warp(g, g.R[w], g.R[w + 1], d, sq, S + f1, tail, dprev, dnext, lane);
+      if (lane == 0 && lev > 0) sq[w] = acc;
+    }
+    __syncthreads();
+    const int t = f1 + *(volatile int *)tail;
     if (t == f1) break;
     if (lev + 2 >= kTileMaxLevels) {  // uniform; routing keeps BCCs below this depth
       if (tid == 0) set_err(err, kDevWorkspace);
@@ -435,33 +471,55 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double 
   return lev + 1;
 }
 
+// Dependency sweep of the whole CTA, two barriers per level as in cta_bfs;
+// contributions go to the FP64 row P, each vertex written by one thread.
 template <int kBlock>
 __device__ void cta_sweep(const View &g, int nlev, const int32_t *d, double *sq, const int32_t *S, const int32_t *lv,
-                          int32_t *q, Ctl &ctl, double wsrc, double *P, int *err) {
+                          int32_t *q, int *nq, double wsrc, double *P, int *err) {
+  constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int lev = nlev - 1; lev >= 1; --lev) {
+  if (tid == 0) {
+    nq[0] = 0;
+    nq[1] = 0;
+  }
+  __syncthreads();
+  for (int lev = nlev - 1, k3 = 0; lev >= 1; --lev, k3 = (k3 + 1) % 3) {
     const int dsucc = lev + 1, a0 = lv[lev], a1 = lv[lev + 1];
-    for (int c0 = a0; c0 < a1; c0 += kBlock) {
-      if (tid == 0) ctl.nq = 0;
-      __syncthreads();
+    int *nql = nq + k3;
+    if (tid == 0) nq[(k3 + 1) % 3] = 0;
+    for (int c0 = a0; c0 < a1; c0 += kBlock) {  // uniform
       const int i = c0 + tid;
+      int32_t w = -1, e0 = 0, e1 = 0;
       if (i < a1) {
-        const int32_t w = S[i];
-        const int e0 = g.R[w], e1 = g.R[w + 1];
-        if (e1 - e0 <= kLaneDeg) {
-          P[w] += finish(g, w, push_row(g, e0, e1, d, sq, dsucc), sq, err) * wsrc;
-        } else {
-          q[atomicAdd(&ctl.nq, 1)] = w;
-        }
+        w = S[i];
+        e0 = g.R[w];
+        e1 = g.R[w + 1];
       }
-      __syncthreads();
-      for (int k = warp; k < ctl.nq; k += kBlock / 32) {
-        const int32_t w = q[k];
-        const double sum = push_row_warp(g, g.R[w], g.R[w + 1], d, sq, dsucc, lane);
-        if (lane == 0) P[w] += finish(g, w, sum, sq, err) * wsrc;
+      const bool big = e1 - e0 > kLaneDeg;
+      if (w >= 0 && !big) P[w] += finish(g, w, push_row(g, e0, e1, d, sq, dsucc), sq, err) * wsrc;
+      bool mine = false;
+      if (w >= 0 && big) {
+        const int pos = atomicAdd(nql, 1);
+        if (pos < kLongQueue) q[pos] = w;
+        else mine = true;
       }
-      __syncthreads();
+      uint32_t over = __ballot_sync(0xffffffffu, mine);
+      while (over) {
+        const int j = __ffs(over) - 1;
+        over &= over - 1;
+        const int32_t wj = __shfl_sync(0xffffffffu, w, j);
+        const double sum = push_row_warp(g, g.R[wj], g.R[wj + 1], d, sq, dsucc, lane);
+        if (lane == 0) P[wj] += finish(g, wj, sum, sq, err) * wsrc;
+      }
     }
+    __syncthreads();
+    const int nlong = min(*(volatile int *)nql, kLongQueue);
+    for (int k = warp; k < nlong; k += kWarps) {
+      const int32_t w = q[k];
+      const double sum = push_row_warp(g, g.R[w], g.R[w + 1], d, sq, dsucc, lane);
+      if (lane == 0) P[w] += finish(g, w, sum, sq, err) * wsrc;
+    }
+    __syncthreads();
   }
 }
 
@@ -493,9 +551,9 @@ __global__ void __launch_bounds__(kBlock, 1) tile_cta_kernel(TileArgs a) {
     if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
     const View g = view_of(a, slice, nb, vo);
     for (int32_t s = it.s0; s < it.s1; ++s) {  // one source at a time: P is summed in source order
-      const int nlev = cta_bfs<kBlock>(g, nb, s, d, sq, S, lv, q, ctl, a.err);
+      const int nlev = cta_bfs<kBlock>(g, nb, s, d, sq, S, lv, q, ctl.cnt, ctl.nq, a.err);
       if (nlev < 0) break;
-      cta_sweep<kBlock>(g, nlev, d, sq, S, lv, q, ctl, (double)__ldg(g.rch + s) + 1.0, P, a.err);
+      cta_sweep<kBlock>(g, nlev, d, sq, S, lv, q, ctl.nq, (double)__ldg(g.rch + s) + 1.0, P, a.err);
     }
     __syncthreads();
     unsigned long long *acc = a.acc + (int64_t)kAccDigits * vo;
