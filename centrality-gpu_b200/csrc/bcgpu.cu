@@ -72,6 +72,8 @@ struct bc_plan {
   int64_t *slice_off = nullptr;
   int32_t *slice_bytes = nullptr;
   int32_t *tws_lv = nullptr;  // warp class: level offsets per warp slot
+  double *tws_P = nullptr;    // CTA class: FP64 partial BC row per CTA
+  int64_t tcap_P = 0;
   // one launch per class and shared-memory bucket (the CTA class in buckets
   // by resident CTAs per SM, so that small BCCs are not run at the
   // occupancy of the largest)
@@ -461,14 +463,20 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, b
     for (int64_t e = 0; e < arcs; ++e) C[e] = (uint16_t)B->col[e0 + e];
   }
   p->n_titems = (int64_t)p->h_titems.size();
-  int warp_grid = 1;
-  for (const auto &T : p->tl)
+  int warp_grid = 1, cta_grid = 1;
+  for (const auto &T : p->tl) {
     if (T.cls == bcg::kTileWarp) warp_grid = T.grid;
+    else {
+      cta_grid = std::max(cta_grid, T.grid);
+      p->tcap_P = std::max<int64_t>(p->tcap_P, T.nmax);
+    }
+  }
   const int64_t slots = (int64_t)warp_grid * bcg::kTileWarps;
   p->tcap = std::max<int64_t>(p->tcap, 2);
   if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) || (rc = upload(p, &p->slice_off, off.data(), B->n_bcc)) ||
       (rc = upload(p, &p->slice_bytes, size.data(), B->n_bcc)) ||
       (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
+      (rc = dalloc(p, &p->tws_P, (int64_t)cta_grid * std::max<int64_t>(p->tcap_P, 1))) ||
       (rc = alloc_acc(p, B->n_packed)))
     return rc;
   for (const auto &it : p->h_titems) {
@@ -982,6 +990,7 @@ int enqueue_units(bc_plan *p, int64_t begin, int64_t end, int *launches) {
       a.vtx_off = p->vtx_off; a.reach = p->reach; a.slices = p->slices; a.slice_off = p->slice_off;
       a.slice_bytes = p->slice_bytes; a.items = p->titems; a.item_begin = j0; a.item_end = j1;
       a.next_item = p->counter; a.acc = p->acc; a.ws_lv = p->tws_lv; a.cap = p->tcap; a.nmax = T.nmax;
+      a.ws_P = p->tws_P; a.cap_P = p->tcap_P;
       a.slice_max = T.slice_max; a.wait_ns = wait_ns(ctx); a.err = p->err;
       CK(ctx, bcg::launch_tile(T.cls, a, (int)std::min<int64_t>(T.grid, j1 - j0), T.smem, ctx->stream));
       ++*launches;

@@ -67,12 +67,11 @@ struct WarpLayout {  // ctl | counters [nmax][kAccDigits] | per warp: d [nmax], 
   __host__ __device__ static int64_t slice(int64_t nmax) { return warps(nmax) + kTileWarps * per_warp(nmax); }
 };
 template <int kBlock>
-struct CtaLayout {  // ctl | P [nmax] | sq [nmax] | d [nmax] | S [nmax] | lv [kTileMaxLevels] | q [kLongQueue] | slice
-  __host__ __device__ static int64_t P() { return align16(sizeof(Ctl)); }
-  __host__ __device__ static int64_t sq(int64_t nmax) { return P() + align16(8 * nmax); }
-  __host__ __device__ static int64_t d(int64_t nmax) { return sq(nmax) + align16(8 * nmax); }
-  __host__ __device__ static int64_t S(int64_t nmax) { return d(nmax) + align16(4 * nmax); }
-  __host__ __device__ static int64_t lv(int64_t nmax) { return S(nmax) + align16(4 * nmax); }
+struct CtaLayout {  // ctl | sq [nmax] | d int16 [nmax] | S uint16 [nmax] | lv [kTileMaxLevels] | q [kLongQueue] | slice
+  __host__ __device__ static int64_t sq() { return align16(sizeof(Ctl)); }
+  __host__ __device__ static int64_t d(int64_t nmax) { return sq() + align16(8 * nmax); }
+  __host__ __device__ static int64_t S(int64_t nmax) { return d(nmax) + align16(2 * nmax); }
+  __host__ __device__ static int64_t lv(int64_t nmax) { return S(nmax) + align16(2 * nmax); }
   __host__ __device__ static int64_t q(int64_t nmax) { return lv(nmax) + align16(4 * kTileMaxLevels); }
   __host__ __device__ static int64_t slice(int64_t nmax) { return q(nmax) + align16(4 * kLongQueue); }
 };
@@ -169,18 +168,27 @@ __device__ __forceinline__ View view_of(const TileArgs &a, const unsigned char *
 
 // Appends x to the visit order S: one atomic per group of lanes appending at
 // once (the lanes that reach this call together), not one per lane.
-__device__ __forceinline__ void append(int32_t *S, int *tail, int32_t x) {
+template <typename ST>
+__device__ __forceinline__ void append(ST *S, int *tail, int32_t x) {
   cg::coalesced_group g = cg::coalesced_threads();
   int pos = 0;
   if (g.thread_rank() == 0) pos = atomicAdd(tail, (int)g.size());
-  S[g.shfl(pos, 0) + (int)g.thread_rank()] = x;
+  S[g.shfl(pos, 0) + (int)g.thread_rank()] = (ST)x;
+}
+
+// Claims unvisited vertex x (level -1) for level lev; true for the one claim
+// that wins. Levels are int32 (warp class) or int16 (CTA class).
+__device__ __forceinline__ bool claim(int32_t *d, int32_t x, int lev) { return atomicCAS(d + x, -1, lev) == -1; }
+__device__ __forceinline__ bool claim(int16_t *d, int32_t x, int lev) {
+  return atomicCAS(reinterpret_cast<unsigned short *>(d + x), (unsigned short)0xffffu, (unsigned short)lev) == 0xffffu;
 }
 
 // Forward scan of one row by one thread (four arcs' loads in flight, sums in
 // arc order): pulls sigma from level dprev, claims unvisited vertices for
 // dnext (appended to S at *tail).
-__device__ __forceinline__ double pull_row(const View &g, int e0, int e1, int32_t *d, const double *sq, int32_t *S,
-                                           int *tail, int dprev, int dnext) {
+template <typename DT, typename ST>
+__device__ __forceinline__ double pull_row(const View &g, int e0, int e1, DT *d, const double *sq, ST *S, int *tail,
+                                           int dprev, int dnext) {
   double acc = 0.0;
   for (int e = e0; e < e1; e += 4) {
     int32_t x[4], dx[4];
@@ -188,33 +196,35 @@ __device__ __forceinline__ double pull_row(const View &g, int e0, int e1, int32_
 #pragma unroll
     for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? (int32_t)g.C[e + j] : -1;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) dx[j] = x[j] >= 0 ? d[x[j]] : INT_MAX;
+    for (int j = 0; j < 4; ++j) dx[j] = x[j] >= 0 ? (int)d[x[j]] : INT_MAX;
 #pragma unroll
     for (int j = 0; j < 4; ++j) sv[j] = dx[j] == dprev ? sq[x[j]] : 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       if (dx[j] == dprev) acc += sv[j];
-      else if (dx[j] == -1 && atomicCAS(d + x[j], -1, dnext) == -1) append(S, tail, x[j]);
+      else if (dx[j] == -1 && claim(d, x[j], dnext)) append(S, tail, x[j]);
     }
   }
   return acc;
 }
 
 // The same for a long row, by a whole warp (lanes over arcs, fixed-order sum).
-__device__ __forceinline__ double pull_row_warp(const View &g, int e0, int e1, int32_t *d, const double *sq, int32_t *S,
-                                                int *tail, int dprev, int dnext, int lane) {
+template <typename DT, typename ST>
+__device__ __forceinline__ double pull_row_warp(const View &g, int e0, int e1, DT *d, const double *sq, ST *S, int *tail,
+                                                int dprev, int dnext, int lane) {
   double acc = 0.0;
   for (int e = e0 + lane; e < e1; e += 32) {
     const int32_t x = g.C[e];
     const int dx = d[x];
     if (dx == dprev) acc += sq[x];
-    else if (dx == -1 && atomicCAS(d + x, -1, dnext) == -1) append(S, tail, x);
+    else if (dx == -1 && claim(d, x, dnext)) append(S, tail, x);
   }
   return warp_sum(acc);
 }
 
 // Sum of q over the successors (level dsucc) of one row, by one thread.
-__device__ __forceinline__ double push_row(const View &g, int e0, int e1, const int32_t *d, const double *sq, int dsucc) {
+template <typename DT>
+__device__ __forceinline__ double push_row(const View &g, int e0, int e1, const DT *d, const double *sq, int dsucc) {
   double acc = 0.0;
   for (int e = e0; e < e1; e += 4) {
     int32_t x[4];
@@ -223,7 +233,7 @@ __device__ __forceinline__ double push_row(const View &g, int e0, int e1, const 
 #pragma unroll
     for (int j = 0; j < 4; ++j) x[j] = e + j < e1 ? (int32_t)g.C[e + j] : -1;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) hit[j] = x[j] >= 0 && d[x[j]] == dsucc;
+    for (int j = 0; j < 4; ++j) hit[j] = x[j] >= 0 && (int)d[x[j]] == dsucc;
 #pragma unroll
     for (int j = 0; j < 4; ++j) qv[j] = hit[j] ? sq[x[j]] : 0.0;
 #pragma unroll
@@ -233,12 +243,13 @@ __device__ __forceinline__ double push_row(const View &g, int e0, int e1, const 
   return acc;
 }
 
-__device__ __forceinline__ double push_row_warp(const View &g, int e0, int e1, const int32_t *d, const double *sq,
-                                                int dsucc, int lane) {
+template <typename DT>
+__device__ __forceinline__ double push_row_warp(const View &g, int e0, int e1, const DT *d, const double *sq, int dsucc,
+                                                int lane) {
   double acc = 0.0;
   for (int e = e0 + lane; e < e1; e += 32) {
     const int32_t x = g.C[e];
-    if (d[x] == dsucc) acc += sq[x];
+    if ((int)d[x] == dsucc) acc += sq[x];
   }
   return warp_sum(acc);
 }
@@ -393,8 +404,8 @@ __global__ void __launch_bounds__(kThreads, 1) tile_warp_kernel(TileArgs a) {
 // nq[l % 3]; those of level l+1 are cleared at the start of level l, two
 // barriers after their last reader.
 template <int kBlock>
-__device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double *sq, int32_t *S, int32_t *lv, int32_t *q,
-                       int *cnt, int *nq, int *err) {
+__device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double *sq, uint16_t *S, int32_t *lv,
+                       int32_t *q, int *cnt, int *nq, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int v = tid; v < nb; v += kBlock) d[v] = -1;
@@ -407,7 +418,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double 
   __syncthreads();
   if (tid == 0) {
     d[s] = 0;
-    S[0] = s;
+    S[0] = (uint16_t)s;
     sq[s] = 1.0;
     lv[0] = 0;
     lv[1] = 1;
@@ -474,7 +485,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double 
 // Dependency sweep of the whole CTA, two barriers per level as in cta_bfs;
 // contributions go to the FP64 row P, each vertex written by one thread.
 template <int kBlock>
-__device__ void cta_sweep(const View &g, int nlev, const int32_t *d, double *sq, const int32_t *S, const int32_t *lv,
+__device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq, const uint16_t *S, const int32_t *lv,
                           int32_t *q, int *nq, double wsrc, double *P, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -523,15 +534,17 @@ __device__ void cta_sweep(const View &g, int nlev, const int32_t *d, double *sq,
   }
 }
 
+// 1024 / kBlock CTAs per SM at most (the shared-memory buckets), so 64
+// registers per thread whatever the block size.
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock, 1) tile_cta_kernel(TileArgs a) {
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) tile_cta_kernel(TileArgs a) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   const int64_t nmax = a.nmax;
   Ctl &ctl = *reinterpret_cast<Ctl *>(s_raw);
-  double *P = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::P());
-  double *sq = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::sq(nmax));
-  int32_t *d = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::d(nmax));
-  int32_t *S = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::S(nmax));
+  double *P = a.ws_P + (int64_t)blockIdx.x * a.cap_P;  // this CTA's FP64 partial row (global, L2-resident)
+  double *sq = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::sq());
+  int16_t *d = reinterpret_cast<int16_t *>(s_raw + CtaLayout<kBlock>::d(nmax));
+  uint16_t *S = reinterpret_cast<uint16_t *>(s_raw + CtaLayout<kBlock>::S(nmax));
   int32_t *lv = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::lv(nmax));
   int32_t *q = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::q(nmax));
   unsigned char *slice = s_raw + CtaLayout<kBlock>::slice(nmax);

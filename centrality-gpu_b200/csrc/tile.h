@@ -46,6 +46,8 @@ struct TileArgs {
   unsigned long long *acc;        // [n_packed][kAccDigits] fixed-point BC counters (plain.h)
   int32_t *ws_lv;                 // warp class: level offsets per warp slot ([slots][cap])
   int64_t cap;                    // per-slot row capacity (>= largest BCC of the class + 2)
+  double *ws_P;                   // CTA class: FP64 partial BC row per CTA ([grid][cap_P])
+  int64_t cap_P;
   int32_t nmax;                   // largest BCC of the launch (shared-memory rows are sized for it)
   int32_t slice_max;              // largest slice in bytes
   unsigned long long wait_ns;     // limit of the wait for a staged slice
