@@ -136,14 +136,24 @@ def step_ranges(plan, target_sources):
     return list(zip(bounds[:-1], bounds[1:]))
 
 
-def oracle_largest_bcc(n, u, v):
-    """The largest BCC (by edges) as the oracle alone decomposes and packs it
-    (linear-time BCC split, reach and chains in oracle/bc_oracle.c), with the
-    oracle's articulation terms: the CPU legs use no part of the product."""
+def oracle_largest_bcc(n, u, v, edge=None):
+    """A BCC as the oracle alone decomposes and packs it (linear-time BCC
+    split, reach and chains in oracle/bc_oracle.c), with the oracle's
+    articulation terms: the CPU legs compute with no part of the product.
+    Which BCC: the one holding `edge` (a pair of original vertex ids, e.g. an
+    edge of the GPU plan's largest BCC, so that both sides name the same
+    one), else the one with the most edges."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O  # the checker: CPU legs only
     nbcc, eb, art = O.decompose_linear(n, u, v)
-    big = int(np.argmax(np.bincount(eb, minlength=max(nbcc, 1))))
+    if edge is None:
+        big = int(np.argmax(np.bincount(eb, minlength=max(nbcc, 1))))
+    else:
+        a, b = edge
+        hit = np.nonzero(((u == a) & (v == b)) | ((u == b) & (v == a)))[0]
+        if len(hit) == 0:
+            raise RuntimeError("the edge naming the BCC is not in the graph")
+        big = int(eb[hit[0]])
     return O.pack_bcc(n, u, v, eb, big), art
 
 
@@ -340,6 +350,10 @@ def main():
                          "BCGPU_LIB_DIR=centrality-gpu_b200/lib_phase)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="cap the device workspace (0 = library default); used to keep profiler captures small")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="take --batch / --tile-max as given (0 = the library's defaults) instead of measuring them")
+    ap.add_argument("--tune-cache", default="",
+                    help="JSON file the autotuner reads its choice from, or writes it to (keyed by graph shape and GPU)")
     ap.add_argument("--ba-graphs", type=int, default=4096,
                     help="ba workload: graphs in the batch (fewer only for small profiler captures)")
     ap.add_argument("--tile-max", type=int, default=0,
@@ -348,9 +362,9 @@ def main():
     ap.add_argument("--plain-ctas", type=int, choices=[0, 4, 8, 16], default=0,
                     help="per-source schedule (and BCCs routed to it): CTAs per SM (bc_opts.plain_ctas_per_sm; "
                          "0 = the library's choice, four of 256 threads)")
-    ap.add_argument("--lazy-tables", action="store_true",
-                    help="e2e steps build the multi-source tables of the passes they run only "
-                         "(bc_opts.lazy_tables)")
+    ap.add_argument("--full-tables", action="store_true",
+                    help="e2e steps build the multi-source tables of every pass, not only of the passes "
+                         "they run (bc_opts.lazy_tables = 0; lazy tables are the library's default)")
     ap.add_argument("--gpu-decomp", action="store_true",
                     help="also time the decomposition on the GPU (bc_decompose_gpu, outside the timed region) "
                          "against the host one, and check that both give the same arrays")
@@ -410,21 +424,29 @@ def main():
     # library reads as "use your own stream"
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    width, tuned = args.batch, None
-    if mode == P.MODE_BATCHED and args.batch == 0:  # the library's autotuner, outside the timed region
-        if rank == 0:  # every rank must build the same plan: rank 0 tunes, the others take its width
-            tctx = P.Context(mode=mode, delta=delta, device=local, stream=stream.cuda_stream,
-                             workspace_limit=int(args.workspace_gb * 2**30))
-            width, per = tctx.autotune_width(d, passes=4)
-            tctx.close()
-            tuned = {str(k): round(v, 2) for k, v in per.items()}
+    width, tile_max, tuned = args.batch, args.tile_max, None
+    if mode == P.MODE_BATCHED and (args.batch == 0 or args.tile_max == 0) and not args.no_autotune:
+        # the project autotuner, outside the timed region: pass width and the
+        # small-BCC size limit, measured on this graph (or read from --tune-cache)
+        if rank == 0:  # every rank must build the same plan: rank 0 tunes, the others take its shapes
+            from centrality_gpu_b200 import autotune
+            res = autotune.tune(P, d, dict(delta=delta, device=local, stream=stream.cuda_stream,
+                                           workspace_limit=int(args.workspace_gb * 2**30)),
+                                cache_path=args.tune_cache or None, device_name=torch.cuda.get_device_name(local))
+            width = res["batch_width"] if args.batch == 0 else width
+            tile_max = res["tile_max"] if args.tile_max == 0 else tile_max
+            tuned = {"cached": res["cached"], "batch_width": res["batch_width"], "tile_max": res["tile_max"],
+                     "width_gteps": {k: round(v, 2) for k, v in res["width_gteps"].items()},
+                     "bands": [{"vertices": f"{b['lo']}-{b['hi']}", "bccs": b["bccs"], "sampled": b["sampled"],
+                                "per_source_ms": round(b["per_source_ms"], 3), "tile_ms": round(b["tile_ms"], 3)}
+                               for b in res["bands"]]}
         if dist:
-            wt = torch.tensor([width], dtype=torch.int64, device=rdev)
+            wt = torch.tensor([width, tile_max], dtype=torch.int64, device=rdev)
             dist.broadcast(wt, src=0)
-            width = int(wt.item())
+            width, tile_max = int(wt[0].item()), int(wt[1].item())
     ctx = P.Context(mode=mode, delta=delta, batch_width=width, device=local, stream=stream.cuda_stream,
                     workspace_limit=int(args.workspace_gb * 2**30), graph=bool(args.graph),
-                    plain_ctas_per_sm=args.plain_ctas, lazy_tables=args.lazy_tables, tile_max=args.tile_max)
+                    plain_ctas_per_sm=args.plain_ctas, lazy_tables=not args.full_tables, tile_max=tile_max)
     plan = ctx.plan(d)
     # steps of this many sources, small enough that every rank gets at least one
     total_sources = plan.unit_work(0, plan.n_units)[0]
@@ -544,7 +566,10 @@ def main():
     accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
-        oarrs, oart = oracle_largest_bcc(n, u, v)
+        # the GPU plan's largest BCC, named for the oracle by its first arc's original end points
+        e0 = int(arrs["row"][0])
+        first_edge = (int(arrs["orig"][0]), int(arrs["orig"][arrs["col"][e0]]))
+        oarrs, oart = oracle_largest_bcc(n, u, v, first_edge)
         s = cpu_unit_check(plan, arrs, oarrs, oart, threads)
         cpu = {"value": s["gteps"], "unit": "GTEPS", "cores": threads, "kind": "port",
                "sample": f"the {s['sources']} sources of GPU unit {s['unit']} (largest BCC: {s['vertices']} vertices, "
@@ -571,10 +596,10 @@ def main():
                        "chain_vertices": info["n_chain_vertices"], "sources_per_step": sources_all / args.steps / world,
                        "units_per_step": float(np.mean([r1 - r0 for r0, r1 in sel])),
                        "host_decomposition_s": round(host_s, 3), "generator_s": round(gen_s, 3), "l2": "inputs larger than L2 (CSR + per-CTA rows)",
-                       "batch_width": st.get("batch_width"), "autotune_gteps": tuned,
+                       "batch_width": st.get("batch_width"), "tile_max": tile_max, "autotune": tuned,
                        "cuda_graph": bool(args.graph), "gpu_decomposition": decomp,
-                       "plain_ctas_per_sm": args.plain_ctas or None, "lazy_tables": bool(args.lazy_tables),
-                       "tile_max": args.tile_max,
+                       "plain_ctas_per_sm": args.plain_ctas or None, "lazy_tables": not args.full_tables,
+
                        "parallelism": f"sources sharded over {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "e2e": e2e, "clocks": clocks,
             "plain": plain,

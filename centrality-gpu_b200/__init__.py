@@ -262,7 +262,7 @@ class Context:
 
     def __init__(self, mode=MODE_PLAIN, delta=DELTA_FP32C, batch_width=0, device=-1, stream=None,
                  workspace_limit=0, rescale_exp=0, plain_core=0, graph=False, plain_ctas_per_sm=0,
-                 lazy_tables=False, tile_max=0, wait_limit_ms=0):
+                 lazy_tables=True, tile_max=0, wait_limit_ms=0):
         o = BcOpts()
         lib().bc_default_opts(C.byref(o))
         o.mode, o.delta, o.batch_width, o.device = mode, delta, batch_width, device

@@ -720,6 +720,7 @@ extern "C" void bc_default_opts(bc_opts *o) {
   o->mode = BCGPU_MODE_BATCHED;
   o->delta = BCGPU_DELTA_FP32C;
   o->batch_width = 0;
+  o->lazy_tables = 1;
 }
 
 extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {

@@ -35,7 +35,7 @@ constexpr int64_t kOffAcc = kOffItems + kBytesItems;  // fixed-point BC counters
 constexpr int64_t kBytesAcc = align256(kMaxVertices * kAccDigits * 8);
 constexpr int64_t kOffCtl = kOffAcc + kBytesAcc;  // vtx_off[2], counter, epochs[2*kSlots], err
 constexpr int64_t kBytesCtl = align256(16 + 8 + 8 * kSlots + 4);
-constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // about 18 MiB
+constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // 19,860,224 bytes (about 19 MiB)
 static_assert(kMaxVertices <= kAccMaxAdds, "one call's sources must fit the fixed-point counters' headroom");
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];

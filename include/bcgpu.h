@@ -67,9 +67,10 @@ typedef struct bc_opts {
                             workspace budget; 8 or 16 = that many CTAs of 128 or 64 threads
                             (more sources in flight for deep, narrow BCCs), with the same
                             fallback; other values are rejected */
-  int32_t lazy_tables;   /* 1: a one-shot bc_run_bccs_units call builds the multi-source slot,
-                            seed and arming tables of the passes it runs only (and the source
-                            order up to the last of them); 0 = of every pass */
+  int32_t lazy_tables;   /* 1 (default): a one-shot bc_run_bccs_units call builds the multi-source
+                            slot, seed and arming tables of the passes it runs only (and the
+                            source order up to the last of them); 0 = of every pass (the same
+                            BC, bit for bit) */
   int32_t tile_max;      /* BATCHED: BCCs routed away from multi-source passes run on the
                             small-BCC schedule (a CTA per range of sources of one BCC, its CSR
                             slice staged in shared memory by a bulk copy, one warp per source)
@@ -87,7 +88,7 @@ typedef struct bc_opts {
 
 typedef struct bc_ctx bc_ctx;
 
-/* Fills opts with defaults (device -1, BATCHED, FP32C, width 0 = 512, graph off). */
+/* Fills opts with defaults (device -1, BATCHED, FP32C, width 0 = 512, lazy tables on, graph off). */
 void bc_default_opts(bc_opts *opts);
 int bc_create(const bc_opts *opts, bc_ctx **out);
 /* Releases the context and every plan still alive on it. */
@@ -162,13 +163,17 @@ int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, in
                   int32_t n_req, const int32_t *reach, float *bc, double *time_s);
 
 /* Variant of bc_begin_free that allocates nothing (no reference counterpart).
+ * BC is accumulated like the per-source schedule's (fixed-point counters
+ * folded to FP64: the same result on every call, whatever the order in which
+ * the CTAs finish their sources); the first call on a device clears the
+ * array's rows and counters, later calls reuse what the previous call left.
  * For callers that cannot create device allocations of their own -- their
  * device memory belongs to another allocator (a framework's caching pool, an
  * arena budgeted up front), so a cudaMalloc/cudaFree here would break that
  * accounting or stall the device. Inputs and the output are the CALLER's
  * DEVICE buffers: R[n+1], C[m] (m = arcs), req_nodes[n_req], reach[n], and
  * bc[n] (FP64, overwritten). All other working memory is one file-scope
- * __device__ array of about 16 MiB that every GPU loading this library holds
+ * __device__ array of about 19 MiB that every GPU loading this library holds
  * until the process exits. Limits: n <= 16384 and n_req <= 16384
  * (BCGPU_EOVERFLOW beyond, with the reason in bc_last_error).
  * The first call on a device looks up that array's device address

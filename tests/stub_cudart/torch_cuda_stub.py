@@ -35,4 +35,5 @@ torch.cuda.Stream = lambda *args, **kwargs: _Stream()
 torch.cuda.set_stream = lambda stream: None
 torch.cuda.synchronize = lambda *args, **kwargs: None
 torch.cuda.Event = _Event
+torch.cuda.get_device_name = lambda *args, **kwargs: "stub sm_100 (no GPU)"
 torch.tensor = _tensor_on_cpu

@@ -207,6 +207,51 @@ out["n_packed"] = int(a["n_packed"])
     assert res["off_launches"] == 2 and res["off_units"] < res["n_packed"]
 
 
+def test_autotuner_measures_caches_and_rereads(stub_dir, tmp_path):
+    """The shape autotuner (centrality-gpu_b200/autotune.py) on the stand-in
+    runtime: it returns a batch width and a tile_max from the candidates,
+    reports the size bands it sampled, writes its choice to the JSON cache
+    under a key of the graph's shape and device, reads it back on a second
+    call without measuring, and measures again for another graph. The
+    sub-batches it times are exact: a subset of BCCs packed on its own holds
+    their sources and work."""
+    cache = tmp_path / "tune.json"
+    res = run_stub(stub_dir, f"""
+from centrality_gpu_b200 import autotune as A
+n, u, v = G.pack_graphs(G.gen_ba_batch(24, 40, 3000, seed=7))[:3]
+d = decomp(n, u, v)
+a = d.arrays()
+l0 = L.stub_cudart_launches()
+r1 = A.tune(P, d, cache_path="{cache}", device_name="stub")
+out["launches_first"] = L.stub_cudart_launches() - l0
+l1 = L.stub_cudart_launches()
+r2 = A.tune(P, d, cache_path="{cache}", device_name="stub")
+out["launches_second"] = L.stub_cudart_launches() - l1
+out["r1"] = r1
+out["r2"] = r2
+g = decomp(*G.gen_grid(30, leaves=100, seed=3))
+out["r3_cached"] = A.tune(P, g, cache_path="{cache}", device_name="stub")["cached"]
+out["keys"] = len(__import__("json").load(open("{cache}")))
+pick = [1, 4, 9]
+sub = A.PackedBccs(A.subset(a, pick))
+ctx = P.Context(mode=P.MODE_BATCHED)
+plan = ctx.plan(sub)
+nb = np.diff(a["vtx_off"])[pick]
+arcs = (a["row"][a["vtx_off"][1:]] - a["row"][a["vtx_off"][:-1]])[pick]
+out["sub"] = [list(plan.unit_work()), [int(nb.sum()), int((nb * arcs).sum()), int((nb * nb).sum())]]
+plan.close()
+ctx.close()
+""")
+    r1, r2 = res["r1"], res["r2"]
+    assert r1["batch_width"] in (0, 128, 256, 512, 1024) and not r1["cached"]
+    assert r1["tile_max"] in [-1] + [b["hi"] for b in r1["bands"]] and len(r1["bands"]) >= 2
+    assert all(b["sampled"] <= b["bccs"] for b in r1["bands"])
+    assert res["launches_first"] > 0 and res["launches_second"] == 0
+    assert r2["cached"] and r2["batch_width"] == r1["batch_width"] and r2["tile_max"] == r1["tile_max"]
+    assert res["r3_cached"] is False and res["keys"] == 2
+    assert res["sub"][0] == res["sub"][1]
+
+
 def test_graph_mode_records_then_replays(stub_dir):
     """Recording enqueues nothing; each replay of a recorded range launches
     what the range holds; a range run without recording is recorded on its

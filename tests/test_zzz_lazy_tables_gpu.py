@@ -23,7 +23,7 @@ def test_lazy_tables_give_the_same_bc(route):
     n, u, v = G.pack_graphs(G.gen_ba_batch(12, 40, 3000, seed=7))[:3]
     d = P.Decomposition(P.Graph.from_edges(n, u, v))
     opts = dict(mode=P.MODE_BATCHED, delta=P.DELTA_FP32C, batch_width=64, plain_core=-1 if route == "multi" else 500)
-    full, lazy = P.Context(**opts), P.Context(lazy_tables=True, **opts)
+    full, lazy = P.Context(lazy_tables=False, **opts), P.Context(lazy_tables=True, **opts)
     plan = full.plan(d)
     units = plan.n_units
     arrs = d.arrays()
