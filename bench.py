@@ -187,12 +187,13 @@ def cpu_unit_check(plan, arrs, oarrs, oart, threads):
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O  # the checker: CPU-baseline leg only
     v0, v1 = int(arrs["vtx_off"][0]), int(arrs["vtx_off"][1])
-    k0 = plan.n_units // 2
-    while k0 > 0:
-        ids = plan.unit_sources(k0, k0 + 1)
-        if len(ids) and ids.min() >= v0 and ids.max() < v1:
-            break
-        k0 -= 1
+    # a unit of the largest BCC, the one nearest the middle of the unit list
+    # (its units may sit anywhere: passes first, small-BCC items last)
+    inside = [k for k in range(plan.n_units)
+              if len(ids := plan.unit_sources(k, k + 1)) and ids.min() >= v0 and ids.max() < v1]
+    if not inside:
+        raise RuntimeError("no unit lies in the largest BCC")
+    k0 = min(inside, key=lambda k: abs(k - plan.n_units // 2))
     ids = plan.unit_sources(k0, k0 + 1)
     plan.reset()
     plan.run(k0, k0 + 1, stats=False)
@@ -240,6 +241,30 @@ def batch_graph_check(P, plan, G, threads, count=16, graphs=4096):
     return {"max_rel_err": err, "vs": "FP64 CPU oracle (the method restated, its own decomposition), per graph",
             "graphs": int(count), "vertices": int(verts), "sample": f"seeded {count} of {len(batch)} graphs, every vertex",
             "bar": 1e-6}
+
+
+def save_sample(P, d, arrs, plan, args, device, stream, width, tile_max):
+    """Runs `args.sample_units` seeded random units of the plan's largest BCC
+    (outside the timed region) in FP32C and in FP64, and saves their BC
+    contributions (original ids, articulation terms excluded) with the original
+    ids of their sources to args.save_bc."""
+    v1 = int(arrs["vtx_off"][1])  # the largest BCC: the units whose sources all lie in it
+    inside = [k for k in range(plan.n_units) if plan.unit_sources(k, k + 1).max(initial=-1) < v1]
+    rng = np.random.default_rng(2025)
+    units = np.sort(rng.choice(inside, size=min(args.sample_units, len(inside)), replace=False))
+    srcs = np.concatenate([plan.unit_sources(int(k), int(k) + 1) for k in units])
+    out = {"units": units, "sources_orig": arrs["orig"][srcs], "sources_packed": srcs,
+           "workload": np.array(args.workload)}
+    for name, dl in (("fp32c", P.DELTA_FP32C), ("fp64", P.DELTA_FP64)):
+        c = P.Context(mode=P.MODE_BATCHED, delta=dl, batch_width=width, device=device, stream=stream.cuda_stream,
+                      tile_max=tile_max, workspace_limit=int(args.workspace_gb * 2**30))
+        pl = c.plan(d)
+        for k in units:
+            pl.run(int(k), int(k) + 1, stats=False)
+        out["bc_" + name] = pl.read() - arrs["art"]
+        pl.close()
+        c.close()
+    np.savez_compressed(args.save_bc, **out)
 
 
 def traffic_per_source(mode, workload):
@@ -354,6 +379,11 @@ def main():
                     help="take --batch / --tile-max as given (0 = the library's defaults) instead of measuring them")
     ap.add_argument("--tune-cache", default="",
                     help="JSON file the autotuner reads its choice from, or writes it to (keyed by graph shape and GPU)")
+    ap.add_argument("--sample-units", type=int, default=0,
+                    help="after the timed region: run this many seeded random units of the plan in the line's "
+                         "delta mode and in FP64 and save their BC contributions to --save-bc (for "
+                         "tests/sample_accuracy.py, which checks them against the oracle on the CPU)")
+    ap.add_argument("--save-bc", default="", help="npz file for --sample-units")
     ap.add_argument("--ba-graphs", type=int, default=4096,
                     help="ba workload: graphs in the batch (fewer only for small profiler captures)")
     ap.add_argument("--tile-max", type=int, default=0,
@@ -557,6 +587,9 @@ def main():
         total = multigpu.combine_bc(plan.read() - arrs["art"], arrs["art"], dist, device=rdev)
         if rank == 0:
             print(f"combined BC over {world} ranks: sum {float(total.sum()):.6e}", file=sys.stderr)
+
+    if rank == 0 and world == 1 and args.sample_units > 0 and args.save_bc:
+        save_sample(P, d, arrs, plan, args, local, stream, width, tile_max)
 
     plain = None
     if rank == 0 and world == 1 and mode == P.MODE_BATCHED and args.plain_waves > 0:
