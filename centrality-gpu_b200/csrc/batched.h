@@ -39,8 +39,10 @@ int64_t batched_device_bytes(const BatchedPlan *p);
 // offsets), its slots, seeds and arming list (tests compare builds with it;
 // the plan must have been built with keep_host_tables).
 uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass);
-// Bytes batched_create copied host -> device; bytes batched_failed_batches reads back.
+// Bytes batched_create copied host -> device and read back (its row checks' flag);
+// bytes batched_failed_batches reads back.
 int64_t batched_h2d_bytes(const BatchedPlan *p);
+int64_t batched_d2h_bytes(const BatchedPlan *p);
 int64_t batched_status_bytes(const BatchedPlan *p);
 int batched_width(const BatchedPlan *p);
 // Packed ids of the own sources (own BFS + chain slots) of batches [begin, end).

@@ -590,6 +590,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
     if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
     p->device_bytes += bcg::batched_device_bytes(p->bp);
+    p->d2h_bytes += bcg::batched_d2h_bytes(p->bp);
     bcg::batched_unit_work(p->bp, p->unit_sources, p->unit_teps, p->unit_bfs, p->unit_aux, p->unit_visits);
     p->n_bat = (int64_t)p->unit_sources.size() - 1;
   } else {

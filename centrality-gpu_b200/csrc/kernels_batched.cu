@@ -1155,6 +1155,7 @@ struct BatchedPlan {
   size_t smem = 0;
   int64_t bytes = 0;
   int64_t h2d = 0;  // bytes uploaded by batched_create
+  int64_t d2h = 0;  // bytes batched_create read back (the row checks' flag)
   std::vector<void *> allocs;
   Args args{};
   std::vector<int64_t> u_src, u_teps, u_bfs, u_aux, u_visits;
@@ -1193,10 +1194,68 @@ int bcc_ecc(const int64_t *row, const int32_t *col, int64_t vo, int32_t nb, std:
 
 namespace {
 
+// The contracted rows of the core vertices of the BCCs in multi-source
+// passes, built on the device from the packed CSR already there (the host
+// computes only the row offsets hrow and, per packed chain vertex, its chain
+// and position): one thread per row writes the row's unit arcs, then its chain
+// arcs, each in the order of the vertex's CSR row -- so the rows are those a
+// sequential fill gives. Entries of rbcc < 0 are a BCC's end offsets. A
+// non-core neighbour outside every chain sets bit 1 of *bad, a core vertex
+// next to the inside of a chain bit 2.
+__global__ void contract_rows_kernel(const int64_t *row, const int32_t *col, const int64_t *vtx_off,
+                                     const int32_t *n_plain, const int32_t *rbcc, const int64_t *hvo,
+                                     const int64_t *hrow, int64_t nrows, const int32_t *gcof, const int32_t *gcpos,
+                                     const int32_t *chain_len, const int32_t *chain_l, const int32_t *chain_r,
+                                     int64_t *hsplit, int32_t *hcol, int32_t *hk, int32_t *hcid, int *bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t b = rbcc[i];
+    if (b < 0) {
+      hsplit[i] = hrow[i];
+      continue;
+    }
+    const int64_t vo = vtx_off[b];
+    const int32_t npl = n_plain[b], x = (int32_t)(i - hvo[b]);
+    const int64_t e0 = row[vo + x], e1 = row[vo + x + 1];
+    int64_t o = hrow[i];
+    for (int64_t e = e0; e < e1; ++e) {
+      const int32_t y = col[e];
+      if (y < npl) {
+        hcol[o] = y;
+        hk[o] = 0;
+        hcid[o] = -1;
+        ++o;
+      }
+    }
+    hsplit[i] = o;
+    for (int64_t e = e0; e < e1; ++e) {
+      const int32_t y = col[e];
+      if (y < npl) continue;
+      const int32_t c = gcof[vo + y];
+      if (c < 0) {
+        atomicOr(bad, 1);
+        continue;
+      }
+      const int32_t k = chain_len[c], pos = gcpos[vo + y];
+      int right;
+      if (x == chain_l[c] && pos == 0) right = 0;
+      else if (x == chain_r[c] && pos == k - 1) right = 1;
+      else {
+        atomicOr(bad, 2);
+        continue;
+      }
+      hcol[o] = right ? chain_l[c] : chain_r[c];
+      hk[o] = k;
+      hcid[o] = c * 2 + right;
+      ++o;
+    }
+  }
+}
+
 // Fills P (allocated by batched_create, which releases it on any failure).
-int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *reach, const int64_t *vtx_off,
-                  const int32_t *chain_start, const int32_t *chain_len, const int32_t *chain_l, const int32_t *chain_r,
-                  double *bc, int *err, cudaStream_t stream, BatchedPlan *P, std::string *msg) {
+int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row, const int32_t *col,
+                  const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
+                  const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
+                  BatchedPlan *P, std::string *msg) {
   auto bail = [&](int code, const std::string &m) {
     if (msg) *msg = m;
     return code;
@@ -1209,8 +1268,10 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   const int W = P->W;
 
   // ---- contracted rows, chain prefix sums, heavy chunks, passes
-  std::vector<int64_t> hvo, hrow, hsplit, cpre_off;
-  HostBuf<int32_t> hcol, hk, hcid;  // every entry written by the row fill
+  std::vector<int64_t> hvo, hrow, cpre_off;
+  std::vector<int32_t> rbcc;          // per hrow entry: its BCC, -1 for a BCC's end offset
+  HostBuf<int32_t> gcof, gcpos;       // per packed vertex of a BCC in passes: chain (global, -1: core), position
+  int64_t narcs = 0;                  // contracted arcs so far
   std::vector<double> cpre;
   HostBuf<Slot> slots;  // every entry written by the pass fill
   HostBuf<Seed> seeds;
@@ -1222,6 +1283,8 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   int64_t ncap = 1;
   int tcap = 2;
   cpre_off.resize((size_t)B->n_chains);
+  gcof.resize((size_t)std::max<int64_t>(B->n_packed, 1));
+  gcpos.resize(gcof.size());
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     const int64_t vo = B->vtx_off[b];
     const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
@@ -1250,6 +1313,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
         cof[s + j] = (int32_t)c;
         cpos[s + j] = j;
       }
+
       for (int32_t j = 0; j < k; ++j) {
         const int32_t x = s + j, prev = j == 0 ? L : x - 1, next = j == k - 1 ? R : x + 1;
         const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
@@ -1274,46 +1338,18 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
     // Every arc of a core vertex becomes one contracted arc (a unit arc, or
     // the chain arc of the chain vertex it leads to), so the contracted rows
     // have the original degrees: offsets first, then the rows in parallel.
+    std::copy(cof.begin(), cof.end(), gcof.begin() + vo);  // the device fill reads them per packed vertex
+    std::copy(cpos.begin(), cpos.end(), gcpos.begin() + vo);
     const size_t rb = hrow.size();
     hrow.resize(rb + (size_t)npl + 1);
-    hsplit.resize(rb + (size_t)npl + 1);
-    hrow[rb] = (int64_t)hcol.size();
+    hrow[rb] = narcs;
     for (int32_t x = 0; x < npl; ++x) hrow[rb + x + 1] = hrow[rb + x] + (B->row[vo + x + 1] - B->row[vo + x]);
-    hsplit[rb + npl] = hrow[rb + npl];
-    hcol.resize((size_t)hrow[rb + npl]);
-    hk.resize(hcol.size());
-    hcid.resize(hcol.size());
-    int row_bad = 0;
-#pragma omp parallel for schedule(dynamic, 2048) reduction(| : row_bad)
-    for (int32_t x = 0; x < npl; ++x) {
-      const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
-      int64_t o = hrow[rb + x];
-      for (int64_t e = e0; e < e1; ++e)
-        if (B->col[e] < npl) { hcol[o] = B->col[e]; hk[o] = 0; hcid[o] = -1; ++o; }
-      hsplit[rb + x] = o;
-      for (int64_t e = e0; e < e1; ++e) {
-        const int32_t y = B->col[e];
-        if (y < npl) continue;
-        const int64_t c = cof[y];
-        if (c < 0) { row_bad |= 1; continue; }
-        const int32_t k = B->chain_len[c];
-        int right;
-        if (x == B->chain_l[c] && cpos[y] == 0) right = 0;
-        else if (x == B->chain_r[c] && cpos[y] == k - 1) right = 1;
-        else { row_bad |= 2; continue; }
-        hcol[o] = right ? B->chain_l[c] : B->chain_r[c];
-        hk[o] = k;
-        hcid[o] = (int32_t)(c * 2 + right);
-        ++o;
-      }
-    }
-    if (row_bad & 1) return bail(BCGPU_EINVAL, "a non-core vertex outside every chain");
-    if (row_bad & 2) return bail(BCGPU_EINVAL, "a core vertex adjacent to the inside of a chain");
+    narcs = hrow[rb + npl];
+    rbcc.resize(rb + (size_t)npl, b);
     hrow.pop_back();  // the BCC's end offset is pushed below, after its heavy rows
-    hsplit.pop_back();
     int32_t hidx = 0;
     for (int32_t x = 0; x < npl; ++x) {
-      const int64_t r0 = hrow[rb + x], r1 = x + 1 < npl ? hrow[rb + x + 1] : (int64_t)hcol.size();
+      const int64_t r0 = hrow[rb + x], r1 = x + 1 < npl ? hrow[rb + x + 1] : narcs;
       if (r1 - r0 <= heavy_deg) continue;
       heavy.push_back(x);
       hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
@@ -1324,8 +1360,8 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
       }
       ++hidx;
     }
-    hrow.push_back((int64_t)hcol.size());
-    hsplit.push_back((int64_t)hcol.size());
+    hrow.push_back(narcs);
+    rbcc.push_back(-1);
     hfirst.push_back((int32_t)((int64_t)hchunk_v.size() - hchunk_off.back()));
     heavy_off.push_back((int64_t)heavy.size());
     hchunk_off.push_back((int64_t)hchunk_v.size());
@@ -1503,11 +1539,29 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   };
   ok = ok && upload((const void **)&a.hvo, hvo.data(), (int64_t)hvo.size() * 8);
   ok = ok && upload((const void **)&a.hrow, hrow.data(), (int64_t)hrow.size() * 8);
-  ok = ok && upload((const void **)&a.hsplit, hsplit.data(), (int64_t)hsplit.size() * 8);
-  ok = ok && upload((const void **)&a.hcol, hcol.data(), (int64_t)hcol.size() * 4);
-  ok = ok && upload((const void **)&a.hk, hk.data(), (int64_t)hk.size() * 4);
-  ok = ok && upload((const void **)&a.hcid, hcid.data(), (int64_t)hcid.size() * 4);
   ok = ok && upload((const void **)&a.n_plain, B->n_plain, (int64_t)B->n_bcc * 4);
+  // the contracted rows themselves: filled on the device from the packed CSR
+  const int32_t *d_rbcc = nullptr, *d_gcof = nullptr, *d_gcpos = nullptr;
+  int *d_bad = nullptr;
+  ok = ok && upload((const void **)&d_rbcc, rbcc.data(), (int64_t)rbcc.size() * 4);
+  ok = ok && upload((const void **)&d_gcof, gcof.data(), (int64_t)gcof.size() * 4);
+  ok = ok && upload((const void **)&d_gcpos, gcpos.data(), (int64_t)gcpos.size() * 4);
+  ok = ok && alloc(&p, (int64_t)hrow.size() * 8); a.hsplit = (const int64_t *)p;
+  ok = ok && alloc(&p, narcs * 4); a.hcol = (const int32_t *)p;
+  ok = ok && alloc(&p, narcs * 4); a.hk = (const int32_t *)p;
+  ok = ok && alloc(&p, narcs * 4); a.hcid = (const int32_t *)p;
+  ok = ok && alloc(&p, 4); d_bad = (int *)p;
+  if (ok && !hrow.empty()) {
+    ok = cudaMemsetAsync(d_bad, 0, sizeof(int), stream) == cudaSuccess;
+    const int64_t nr = (int64_t)hrow.size();
+    const int blocks = (int)std::min<int64_t>((nr + 255) / 256, 148 * 16);
+    if (ok) {
+      contract_rows_kernel<<<blocks, 256, 0, stream>>>(row, col, vtx_off, a.n_plain, d_rbcc, a.hvo, a.hrow, nr, d_gcof,
+                                                       d_gcpos, chain_len, chain_l, chain_r, (int64_t *)a.hsplit,
+                                                       (int32_t *)a.hcol, (int32_t *)a.hk, (int32_t *)a.hcid, d_bad);
+      ok = cudaGetLastError() == cudaSuccess;
+    }
+  }
   ok = ok && upload((const void **)&a.chain_off, B->chain_off, (int64_t)(B->n_bcc + 1) * 8);
   ok = ok && upload((const void **)&a.cpre_off, cpre_off.data(), (int64_t)cpre_off.size() * 8);
   ok = ok && upload((const void **)&a.cpre, cpre.data(), (int64_t)cpre.size() * 8);
@@ -1527,6 +1581,11 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   if (!ok) return bail(BCGPU_ENOMEM, "cudaMalloc or upload of the batched workspace failed");
   cudaError_t e = cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(a.redo, 0, (size_t)std::max<int64_t>(P->n_batches, 1) * 4, stream);
+  int h_bad = 0;
+  if (e == cudaSuccess && !hrow.empty()) {
+    e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    P->d2h += (int64_t)sizeof(int);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
   P->h_slots = std::move(slots);
   if (cfg.keep_host_tables) {
@@ -1535,6 +1594,8 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int32_t *rea
   }
   P->h_vtx_off.assign(B->vtx_off, B->vtx_off + B->n_bcc + 1);
   if (e != cudaSuccess) return bail(BCGPU_ECUDA, std::string("batched upload: ") + cudaGetErrorString(e));
+  if (h_bad & 1) return bail(BCGPU_EINVAL, "a non-core vertex outside every chain");
+  if (h_bad & 2) return bail(BCGPU_EINVAL, "a core vertex adjacent to the inside of a chain");
   a.reach = reach; a.vtx_off = vtx_off;
   a.chain_start = chain_start; a.chain_len = chain_len; a.chain_l = chain_l; a.chain_r = chain_r;
   a.n_cap = P->n_cap; a.W = W; a.tcap = tcap; a.bc = bc; a.err = err;
@@ -1565,12 +1626,12 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
                    const int32_t *reach, const int64_t *vtx_off, const int32_t *chain_start, const int32_t *chain_len,
                    const int32_t *chain_l, const int32_t *chain_r, double *bc, int *err, cudaStream_t stream,
                    BatchedPlan **out, std::string *msg) {
-  (void)row; (void)col;
   BatchedPlan *P = nullptr;
   int rc;
   try {  // a host allocation that throws releases the partial plan like any other failure
     P = new BatchedPlan;
-    rc = batched_build(B, cfg, reach, vtx_off, chain_start, chain_len, chain_l, chain_r, bc, err, stream, P, msg);
+    rc = batched_build(B, cfg, row, col, reach, vtx_off, chain_start, chain_len, chain_l, chain_r, bc, err, stream, P,
+                       msg);
   } catch (const std::bad_alloc &) {
     if (msg) *msg = "host allocation failed while building the passes";
     rc = BCGPU_ENOMEM;
@@ -1608,6 +1669,7 @@ uint64_t batched_pass_digest(const BatchedPlan *p, int64_t pass) {
   return h;
 }
 int64_t batched_h2d_bytes(const BatchedPlan *p) { return p ? p->h2d : 0; }
+int64_t batched_d2h_bytes(const BatchedPlan *p) { return p ? p->d2h : 0; }
 int64_t batched_status_bytes(const BatchedPlan *p) {
   return p ? (int64_t)sizeof(int) * std::max<int64_t>(p->n_batches, 1) : 0;
 }
