@@ -4,6 +4,9 @@
     python centrality-gpu_b200/build.py --variant phase -DBCGPU_PHASE_TIMERS
         # an instrumented copy in lib_phase/ (objects in _build_phase/); load it
         # with BCGPU_LIB_DIR=<package>/lib_phase. The default build is unaffected.
+    python centrality-gpu_b200/build.py --variant ht -DBCGPU_HOST_TIMERS
+        # the same for the host side of plan builds: each stage's wall time
+        # ("[host] route", "[host] uploads", ...) printed to stderr.
 """
 from __future__ import annotations
 

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <climits>
+#include <functional>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -17,13 +18,24 @@ struct BatchedConfig {
   int64_t limit_bytes = 0;  // device bytes available to the plan's workspace
   int rescale_exp = 900;    // rescale a level's path counts above 2^rescale_exp
   unsigned long long wait_ns = 60ull * 1000 * 1000 * 1000;  // limit of one device-side wait
+  cudaMemPool_t pool = nullptr;  // device memory from this pool, ordered on the plan's stream (null: cudaMalloc)
   const std::vector<char> *bccs_on = nullptr;  // BCCs this plan schedules (null: all)
   const std::vector<int32_t> *ecc0 = nullptr;  // per BCC: eccentricity of local vertex 0 if known (< 0: compute)
   // Passes (global index) whose slot, seed and arming tables are built; the
   // others keep their sizes and offsets but no sources, and must not be run.
   int64_t fill_begin = 0, fill_end = INT64_MAX;
   bool keep_host_tables = false;  // keep host copies of seeds and arming lists (batched_pass_digest)
+  // Source order of BCC b (batched_source_order with at least the length the
+  // filled passes need), computed by the caller (e.g. alongside its uploads);
+  // empty: batched_create computes it.
+  std::function<const std::vector<int32_t> &(int32_t b)> order_of;
 };
+
+// Sources per pass for a requested width (0: the default).
+int batched_width(int requested);
+// The source order of BCC b's passes, at least its first `need` entries (a
+// prefix of the full order).
+void batched_source_order(const bc_bccs *B, int32_t b, int width, int64_t need, std::vector<int32_t> &order);
 
 struct BatchedPlan;
 

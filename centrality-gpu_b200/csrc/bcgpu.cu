@@ -22,6 +22,7 @@
 #include <new>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 struct bc_plan;
@@ -34,6 +35,12 @@ struct bc_ctx {
   bool own_stream = false;
   std::string err;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Stream-ordered pool of the plans' device memory: a destroyed plan's
+  // buffers go back to the pool (cudaFreeAsync) and stay reserved for the
+  // next plan of this context instead of returning to the device (a plan of
+  // RMAT-20 holds ~5 GB; cudaFree of that took ~0.2 s per plan). Released
+  // to the device by bc_destroy.
+  cudaMemPool_t pool = nullptr;
   std::set<bc_plan *> plans;  // live plans: bc_destroy releases them first
 };
 
@@ -103,6 +110,16 @@ struct bc_plan {
   std::map<std::pair<int64_t, int64_t>, Recorded> graphs;
 };
 
+#ifdef BCGPU_HOST_TIMERS
+namespace bcg {
+void host_mark(const char *name) {
+  static auto last = std::chrono::steady_clock::now();
+  auto now = std::chrono::steady_clock::now();
+  fprintf(stderr, "[host] %-28s %9.2f ms\n", name, std::chrono::duration<double, std::milli>(now - last).count());
+  last = now;
+}
+}
+#endif
 namespace {
 
 thread_local std::string g_create_err;
@@ -136,11 +153,34 @@ int guard(bc_ctx *ctx, F &&body) {
   }
 }
 
+// Device memory from the context's pool, ordered on its stream. When the
+// pool cannot grow, its unused reserve is trimmed once and the allocation
+// retried (fragments a larger earlier plan left behind).
+cudaError_t pool_alloc(bc_ctx *ctx, void **ptr, size_t bytes) {
+  cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, ctx->pool, ctx->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    if (cudaStreamSynchronize(ctx->stream) == cudaSuccess && cudaMemPoolTrimTo(ctx->pool, 0) == cudaSuccess)
+      e = cudaMallocFromPoolAsync(ptr, bytes, ctx->pool, ctx->stream);
+  }
+  return e;
+}
+
+// Bytes the context's pool holds in reserve (freed by earlier plans, not
+// yet returned to the device): available to a new plan of this context.
+int64_t pool_spare(const bc_ctx *ctx) {
+  uint64_t reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    return 0;
+  return reserved > used ? (int64_t)(reserved - used) : 0;
+}
+
 template <typename T>
 int dalloc(bc_plan *p, T **ptr, int64_t count) {
   size_t bytes = sizeof(T) * (size_t)std::max<int64_t>(count, 1);
-  cudaError_t e = cudaMalloc((void **)ptr, bytes);
-  if (e != cudaSuccess) return cuda_fail(p->ctx, e, "cudaMalloc");
+  cudaError_t e = pool_alloc(p->ctx, (void **)ptr, bytes);
+  if (e != cudaSuccess) return cuda_fail(p->ctx, e, "cudaMallocFromPoolAsync");
   p->allocs.push_back(*ptr);
   p->device_bytes += (int64_t)bytes;
   return BCGPU_OK;
@@ -492,6 +532,52 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, b
   return BCGPU_OK;
 }
 
+// Source orders of the BCCs in multi-source passes, computed on one host
+// thread (each BCC up to the passes the plan fills, as batched_create would).
+// get() waits for the thread; a host allocation that failed there is
+// rethrown as std::bad_alloc. The destructor waits too, so no exit path
+// leaves the thread running.
+struct SourceOrders {
+  std::vector<std::vector<int32_t>> by_bcc;
+  std::thread th;
+  bool failed = false;
+  void start(const bc_bccs *B, const std::vector<char> &on, int width, int64_t fill_begin, int64_t fill_end) {
+    by_bcc.resize((size_t)B->n_bcc);
+    std::vector<std::pair<int32_t, int64_t>> jobs;  // (BCC, entries needed), as batched_build counts passes
+    int64_t bat0 = 0;
+    for (int32_t b = 0; b < B->n_bcc; ++b) {
+      if (!on[b]) continue;
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b], nbat = (nb + width - 1) / width;
+      const int64_t jf0 = std::min(nbat, std::max<int64_t>(0, fill_begin - bat0));
+      const int64_t jf1 = std::max(jf0, std::min(nbat, fill_end - bat0));
+      if (jf1 > 0) jobs.emplace_back(b, std::min<int64_t>(nb, jf1 * width));
+      bat0 += nbat;
+    }
+    th = std::thread([this, B, width, jobs = std::move(jobs)] {
+      try {
+#ifdef BCGPU_HOST_TIMERS
+        auto t0 = std::chrono::steady_clock::now();
+#endif
+        for (const auto &j : jobs) bcg::batched_source_order(B, j.first, width, j.second, by_bcc[(size_t)j.first]);
+#ifdef BCGPU_HOST_TIMERS
+        fprintf(stderr, "[host] order thread %.2f ms\n",
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+#endif
+      } catch (const std::bad_alloc &) {
+        failed = true;
+      }
+    });
+  }
+  const std::vector<int32_t> &get(int32_t b) {
+    if (th.joinable()) th.join();
+    if (failed) throw std::bad_alloc();
+    return by_bcc[(size_t)b];
+  }
+  ~SourceOrders() {
+    if (th.joinable()) th.join();
+  }
+};
+
 // Fills plan p (allocated by create_plan, which releases it on any failure).
 // fill_begin/fill_end: the multi-source passes (units) whose tables are built
 // (a one-shot call that runs only those); default all.
@@ -508,22 +594,8 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
   p->h_n_plain.assign(B->n_plain, B->n_plain + B->n_bcc);
   p->h_chain_start.assign(B->chain_start, B->chain_start + B->n_chains);
   p->h_chain_len.assign(B->chain_len, B->chain_len + B->n_chains);
-  if ((rc = upload(p, &p->row, B->row, B->n_packed + 1)) || (rc = upload(p, &p->vtx_off, B->vtx_off, B->n_bcc + 1)) ||
-      (rc = upload(p, &p->col, B->col, B->n_arcs)) || (rc = upload(p, &p->reach, B->reach, B->n_packed)) ||
-      (rc = upload(p, &p->chain_start, B->chain_start, B->n_chains)) ||
-      (rc = upload(p, &p->chain_len, B->chain_len, B->n_chains)) ||
-      (rc = upload(p, &p->chain_l, B->chain_l, B->n_chains)) || (rc = upload(p, &p->chain_r, B->chain_r, B->n_chains)) ||
-      (rc = dalloc(p, &p->bc, B->n_packed)) || (rc = dalloc(p, &p->err, 1)) || (rc = dalloc(p, &p->counter, 1)))
-    return bail(rc);
-  if (cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(B->n_packed, 1), ctx->stream) != cudaSuccess ||
-      cudaMemsetAsync(p->err, 0, sizeof(int), ctx->stream) != cudaSuccess)
-    return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
   int64_t nb_max = 0;
   for (int32_t b = 0; b < B->n_bcc; ++b) nb_max = std::max(nb_max, B->vtx_off[b + 1] - B->vtx_off[b]);
-
-  size_t free_b = 0, total_b = 0;
-  CK(ctx, cudaMemGetInfo(&free_b, &total_b));
-  int64_t limit = ctx->opts.workspace_limit > 0 ? ctx->opts.workspace_limit : (int64_t)(0.8 * (double)free_b);
 
   // BATCHED: which BCCs take multi-source passes (the others: per-source items)
   std::vector<char> on;
@@ -557,6 +629,29 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     }
     for (char x : on) n_on += x;
   }
+  HOST_MARK("route");
+  // The multi-source passes' source orders (a sequential greedy over each
+  // BCC's arcs) are computed on a host thread while the graph is uploaded
+  // and the rest of the plan is built; batched_create waits for them.
+  SourceOrders orders;
+  if (p->mode == BCGPU_MODE_BATCHED && n_on > 0) orders.start(B, on, bcg::batched_width(ctx->opts.batch_width),
+                                                              fill_begin, fill_end);
+  if ((rc = upload(p, &p->row, B->row, B->n_packed + 1)) || (rc = upload(p, &p->vtx_off, B->vtx_off, B->n_bcc + 1)) ||
+      (rc = upload(p, &p->col, B->col, B->n_arcs)) || (rc = upload(p, &p->reach, B->reach, B->n_packed)) ||
+      (rc = upload(p, &p->chain_start, B->chain_start, B->n_chains)) ||
+      (rc = upload(p, &p->chain_len, B->chain_len, B->n_chains)) ||
+      (rc = upload(p, &p->chain_l, B->chain_l, B->n_chains)) || (rc = upload(p, &p->chain_r, B->chain_r, B->n_chains)) ||
+      (rc = dalloc(p, &p->bc, B->n_packed)) || (rc = dalloc(p, &p->err, 1)) || (rc = dalloc(p, &p->counter, 1)))
+    return bail(rc);
+  if (cudaMemsetAsync(p->bc, 0, sizeof(double) * (size_t)std::max<int64_t>(B->n_packed, 1), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(p->err, 0, sizeof(int), ctx->stream) != cudaSuccess)
+    return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
+  HOST_MARK("uploads");
+
+  size_t free_b = 0, total_b = 0;
+  CK(ctx, cudaMemGetInfo(&free_b, &total_b));
+  const double avail_b = (double)free_b + (double)pool_spare(ctx);
+  int64_t limit = ctx->opts.workspace_limit > 0 ? ctx->opts.workspace_limit : (int64_t)(0.8 * avail_b);
   // BATCHED: BCCs off the multi-source passes that fit the small-BCC schedule
   std::vector<int8_t> tile;
   int64_t n_tile = 0;
@@ -564,6 +659,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     route_tiles(ctx, B, on, tile);
     for (int8_t x : tile) n_tile += x >= 0;
   }
+  HOST_MARK("route_tiles");
   std::vector<bcg::PlainItem> items;
   if (p->mode == BCGPU_MODE_PLAIN) {
     if (override_items) items = *override_items;
@@ -581,6 +677,8 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     cfg.limit_bytes = limit - p->device_bytes;
     cfg.rescale_exp = ctx->opts.rescale_exp;
     cfg.wait_ns = wait_ns(ctx);
+    cfg.pool = ctx->pool;
+    cfg.order_of = [&orders](int32_t b) -> const std::vector<int32_t> & { return orders.get(b); };
     cfg.bccs_on = &on;
     cfg.ecc0 = &ecc0;
     cfg.fill_begin = fill_begin;
@@ -588,6 +686,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     std::string msg;
     rc = bcg::batched_create(B, cfg, p->row, p->col, p->reach, p->vtx_off, p->chain_start, p->chain_len, p->chain_l,
                              p->chain_r, p->bc, p->err, ctx->stream, &p->bp, &msg);
+    HOST_MARK("batched_create");
     if (rc) return bail(fail(ctx, rc, "batched plan: " + msg));
     p->device_bytes += bcg::batched_device_bytes(p->bp);
     p->d2h_bytes += bcg::batched_d2h_bytes(p->bp);
@@ -651,8 +750,10 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));
     p->h2d_bytes += (int64_t)(sizeof(int32_t) * ep.size());
   }
+  HOST_MARK("plain items+ws");
   if (n_tile && (rc = build_tiles(ctx, B, tile, p))) return bail(rc);
   CK(ctx, cudaStreamSynchronize(ctx->stream));
+  HOST_MARK("tiles+sync");
   return BCGPU_OK;
 }
 
@@ -778,6 +879,14 @@ extern "C" int bc_create(const bc_opts *opts, bc_ctx **out) {
   }
   if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess)
     return bad(e, "cudaEventCreate");
+  cudaMemPoolProps pp{};
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = dev;
+  if ((e = cudaMemPoolCreate(&ctx->pool, &pp)) != cudaSuccess) return bad(e, "cudaMemPoolCreate");
+  uint64_t keep = ~(uint64_t)0;  // never release reserve at a synchronisation: plans reuse it
+  if ((e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+    return bad(e, "cudaMemPoolSetAttribute");
   *out = ctx;
   return BCGPU_OK;
 }
@@ -786,6 +895,10 @@ extern "C" void bc_destroy(bc_ctx *ctx) {
   if (!ctx) return;
   while (!ctx->plans.empty()) bc_plan_destroy(*ctx->plans.begin());
   cudaSetDevice(ctx->device);
+  if (ctx->pool) {
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // frees ordered on the stream have completed
+    cudaMemPoolDestroy(ctx->pool);
+  }
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -871,7 +984,7 @@ extern "C" void bc_plan_destroy(bc_plan *p) {
   cudaStreamSynchronize(p->ctx->stream);
   for (auto &g : p->graphs) cudaGraphExecDestroy(g.second.exec);
   if (p->bp) bcg::batched_destroy(p->bp);
-  for (void *a : p->allocs) cudaFree(a);
+  for (void *a : p->allocs) cudaFreeAsync(a, p->ctx->stream);  // back to the context's pool
   delete p;
 }
 
@@ -1154,11 +1267,14 @@ int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool
   bc_plan *p = nullptr;
   // with lazy_tables, only the passes this call runs get their tables built
   const bool lazy = ctx->opts.lazy_tables && !all;
+  HOST_MARK("run_units start");
   int rc = create_plan(ctx, bccs, nullptr, &p, lazy ? begin : 0, lazy ? end : INT64_MAX);
   bc_stats st{};
   if (!rc && all) { begin = 0; end = bc_plan_num_units(p); }
   if (!rc) rc = bc_plan_run(p, begin, end, &st);
+  HOST_MARK("run");
   if (!rc) rc = bc_plan_read(p, bc_out);
+  HOST_MARK("read");
   if (!rc && !with_art && !p->art.empty())
     for (int32_t v = 0; v < p->n_orig; ++v) bc_out[v] -= p->art[v];
   if (!rc) {
@@ -1173,6 +1289,7 @@ int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool
     if (stats) *stats = st;
   }
   bc_plan_destroy(p);
+  HOST_MARK("destroy");
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   return rc;

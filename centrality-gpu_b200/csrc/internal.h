@@ -15,4 +15,12 @@ void ctx_set_error(bc_ctx *ctx, const char *msg);
 const char *dev_err_text(int code);
 int dev_err_status(int code);
 
+// Profiling builds only (-DBCGPU_HOST_TIMERS): prints the wall time since
+// the previous mark under `name` to stderr (one plan build at a time).
+#ifdef BCGPU_HOST_TIMERS
+void host_mark(const char *name);
+#define HOST_MARK(n) ::bcg::host_mark(n)
+#else
+#define HOST_MARK(n) do {} while (0)
+#endif
 }  // namespace bcg

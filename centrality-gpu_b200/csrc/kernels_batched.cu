@@ -45,6 +45,7 @@
 #include "accum.cuh"
 #include "batched.h"
 #include "common.cuh"
+#include "internal.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -299,13 +300,6 @@ __device__ __noinline__ double stretch_dep(const Stretch &s, int i, const End &A
   return 0.0;  // fed from both ends: no successor on the chain
 }
 
-// Whether what A receives from the stretch needs B's path count (the vertex
-// where the two sides meet ties).
-__device__ __forceinline__ bool end_needs_sigma(int m, int dA, int dB) {
-  const int D = dB + m - dA - 1;
-  return m > 0 && D >= 0 && (D & 1) == 0 && D / 2 <= m - 1;
-}
-
 // What end A receives from the stretch's vertices (its neighbour on the
 // stretch is its successor iff that neighbour is fed from A: D >= 0), less
 // the term through B (sigma_A * q(B) when B's paths run through the
@@ -463,9 +457,13 @@ __device__ __forceinline__ void arm_arcs(const Args &a, int64_t e0, int64_t e1, 
 
 // What core vertex v receives from the vertices of its chains, for the 32
 // slots of word w (the part that needs only forward results): cdep[v][w][.].
-// Chain-arc data are loaded lane-parallel, 32 arcs at a time; the far ends'
-// levels four arcs at a time, then the path counts the ties need.
+// Chain-arc data are loaded lane-parallel, 32 arcs at a time; then, four arcs
+// at a time, the far ends' levels and path counts in one batch of loads (a
+// tie needs the path counts on about half the slots, so a warp nearly always
+// needs them: loading them with the levels takes one memory round trip per
+// group instead of one more per tying arc), then their level exponents.
 constexpr int kArcGroup = 4;
+__device__ __forceinline__ int level_index(const Args &a, int d) { return min(max(d, 0), a.tcap + 1); }
 __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int nslots, int32_t v, int w, int64_t c0,
                                          int64_t c1, int lane) {
   const int W = a.W;
@@ -477,9 +475,10 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
   Slot sl{0, -1, 0, 0};
   if (live) {
     A.d = __ldcg(a.d + iv);
+    A.s = __ldcg(a.sig + iv);
     sl = slots[b];
+    A.x = __ldcg(xb + level_index(a, A.d));
   }
-  bool have_a = false;  // A's path count, loaded on the first tie
   double sum = 0.0;
   for (int64_t base = c0; base < c1; base += 32) {
     const int64_t e = base + lane;
@@ -493,60 +492,46 @@ __device__ __forceinline__ void chain_in(const Args &a, const Slot *slots, int n
     }
     const int cnt = (int)min((int64_t)32, c1 - base);
     for (int j0 = 0; j0 < cnt; j0 += kArcGroup) {
-      int32_t uj[kArcGroup], cj[kArcGroup], kj[kArcGroup], dB[kArcGroup];
+      int32_t uj[kArcGroup], cj[kArcGroup], kj[kArcGroup], dB[kArcGroup], xB[kArcGroup];
       int64_t pj[kArcGroup];
+      double sB[kArcGroup];
 #pragma unroll
-      for (int r = 0; r < kArcGroup; ++r) {  // the far ends' levels, all in flight
+      for (int r = 0; r < kArcGroup; ++r) {  // the far ends' levels and path counts, all in flight
         const int j = (j0 + r) & 31;
         uj[r] = __shfl_sync(0xffffffffu, u, j);
         cj[r] = __shfl_sync(0xffffffffu, cid, j);
         kj[r] = __shfl_sync(0xffffffffu, k, j);
         pj[r] = __shfl_sync(0xffffffffu, poff, j);
-        dB[r] = (live && j0 + r < cnt) ? __ldcg(a.d + ((int64_t)uj[r] * W + w) * 32 + lane) : 0;
+        const int64_t ib = ((int64_t)uj[r] * W + w) * 32 + lane;
+        const bool ld = live && j0 + r < cnt;
+        dB[r] = ld ? __ldcg(a.d + ib) : 0;
+        sB[r] = ld ? __ldcg(a.sig + ib) : 1.0;
       }
+#pragma unroll
+      for (int r = 0; r < kArcGroup; ++r) xB[r] = (live && j0 + r < cnt) ? __ldcg(xb + level_index(a, dB[r])) : 0;
 #pragma unroll
       for (int r = 0; r < kArcGroup; ++r) {
         if (!live || j0 + r >= cnt) continue;
         const bool same = sl.chain == (cj[r] >> 1);  // the source sits on this chain
-        const int64_t ib = ((int64_t)uj[r] * W + w) * 32 + lane;
         if (pj[r] < 0 && !same) {
           // nothing hangs off the chain: prefix sums are positions; the
           // vertices up to P = D/2 are fed from A, the one at D/2 ties when D is even
           const int D = dB[r] + kj[r] - A.d - 1;
           if (D < 0) continue;
           const int P = D >> 1;
-          if ((D & 1) == 0 && P <= kj[r] - 1) {
-            if (!have_a) {
-              A.s = __ldcg(a.sig + iv);
-              A.x = __ldcg(xb + A.d);
-              have_a = true;
-            }
-            const double sb = __ldcg(a.sig + ib);
-            const int xbb = __ldcg(xb + dB[r]);
-            sum += (double)P + 1.0 / (1.0 + scale2(sb / A.s, xbb - A.x));
-          } else {
+          if ((D & 1) == 0 && P <= kj[r] - 1)
+            sum += (double)P + 1.0 / (1.0 + scale2(sB[r] / A.s, xB[r] - A.x));
+          else
             sum += (double)(min(kj[r] - 1, P) + 1);
-          }
           continue;
         }
         const bool right = cj[r] & 1;
         const double *Pj = pj[r] < 0 ? nullptr : a.cpre + pj[r];
         Stretch st{Pj, 0, kj[r], right};
-        End B{dB[r], 0, 1.0, 0.0};
+        End B{dB[r], xB[r], sB[r], 0.0};
         if (same) {  // the stretch ends at the source
           B = source_end();
           st = right ? Stretch{Pj, sl.pos + 1, kj[r], true} : Stretch{Pj, 0, sl.pos, false};
-        }
-        if (end_needs_sigma(st.m(), A.d, B.d)) {
-          if (!same) {
-            B.s = __ldcg(a.sig + ib);
-            B.x = __ldcg(xb + B.d);
-          }
-          if (!have_a) {
-            A.s = __ldcg(a.sig + iv);
-            A.x = __ldcg(xb + A.d);
-            have_a = true;
-          }
         }
         sum += end_dep(st, A, B);
       }
@@ -1032,17 +1017,17 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
             const bool sig = tieL || tieR || viaL || viaR;
             if (sig) {
               eL.s = __ldcg(a.sig + iL);
-              eL.x = __ldcg(xb + eL.d);
+              eL.x = __ldcg(xb + level_index(a, eL.d));
               eR.s = __ldcg(a.sig + iR);
-              eR.x = __ldcg(xb + eR.d);
+              eR.x = __ldcg(xb + level_index(a, eR.d));
             }
             if (viaR || srcL) {
               eL.qs = (double)__ldcg(qq + iL);
-              if (!sig) eL.x = __ldcg(xb + eL.d);
+              if (!sig) eL.x = __ldcg(xb + level_index(a, eL.d));
             }
             if (viaL || srcR) {
               eR.qs = (double)__ldcg(qq + iR);
-              if (!sig) eR.x = __ldcg(xb + eR.d);
+              if (!sig) eR.x = __ldcg(xb + level_index(a, eR.d));
             }
           }
           const double wsrc = live ? a.wsrc[b] : 0.0;
@@ -1156,6 +1141,8 @@ struct BatchedPlan {
   int64_t bytes = 0;
   int64_t h2d = 0;  // bytes uploaded by batched_create
   int64_t d2h = 0;  // bytes batched_create read back (the row checks' flag)
+  cudaMemPool_t pool = nullptr;  // allocs come from this pool on `stream` (null: cudaMalloc)
+  cudaStream_t stream = nullptr;
   std::vector<void *> allocs;
   Args args{};
   std::vector<int64_t> u_src, u_teps, u_bfs, u_aux, u_visits;
@@ -1191,6 +1178,61 @@ int bcc_ecc(const int64_t *row, const int32_t *col, int64_t vo, int32_t nb, std:
 }
 
 }  // namespace
+
+int batched_width(int requested) {
+  const int width = requested > 0 ? requested : 512;
+  return std::max(32, std::min(1024, (width + 31) / 32 * 32));
+}
+
+// Source order of BCC b: bounded BFS balls of nearby vertices (chain vertices
+// included), so a pass's sources see every vertex within a narrow band of
+// levels: few active levels per vertex, dense 32-slot hits. A ball grows only
+// through vertices not yet taken, so each vertex's arcs are scanned once and
+// late balls cost no rescans of finished regions. The greedy stops at the
+// first ball boundary at or after `need` vertices: the order of a larger
+// `need` extends it (a lazy plan that fills only some passes needs a prefix).
+void batched_source_order(const bc_bccs *B, int32_t b, int width, int64_t need, std::vector<int32_t> &order) {
+  const int64_t vo = B->vtx_off[b];
+  const int32_t nb = (int32_t)(B->vtx_off[b + 1] - vo);
+  order.clear();
+  need = std::min<int64_t>(need, nb);
+  if (need <= 0) return;
+  order.reserve((size_t)need + (size_t)width);
+  // taken: one bit per vertex (small enough to stay in the host's caches).
+  // A ball's queue may list a vertex more than once (every taken vertex
+  // queues its untaken neighbours); it is taken at its first listing and
+  // skipped at the later ones, so the order is that of a queue holding each
+  // vertex once. A vertex queued by an earlier ball but not taken may join
+  // a later one.
+  std::vector<uint64_t> taken(((size_t)nb + 63) / 64, 0);
+  auto is_taken = [&](int32_t y) { return (taken[(size_t)y >> 6] >> (y & 63)) & 1u; };
+  std::vector<int32_t> q;
+  const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
+  for (int32_t seed = 0; seed < nb && (int64_t)order.size() < need; ++seed) {
+    if (is_taken(seed)) continue;
+    q.clear();
+    q.push_back(seed);
+    int64_t got = 0, scanned = 0;
+    for (size_t h = 0; h < q.size() && got < width; ++h) {
+      // software pipeline over the queue: row offsets 16 entries ahead, the
+      // row's arcs 8 ahead (rows are short: ~9 arcs on RMAT)
+      if (h + 16 < q.size()) __builtin_prefetch(&B->row[vo + q[h + 16]]);
+      if (h + 8 < q.size()) __builtin_prefetch(&B->col[B->row[vo + q[h + 8]]]);
+      const int32_t x = q[h];
+      if (is_taken(x)) continue;
+      taken[(size_t)x >> 6] |= 1ull << (x & 63);
+      order.push_back(x);
+      ++got;
+      if (scanned >= arc_budget) continue;  // keep draining the queue, stop growing it
+      const int64_t e0 = B->row[vo + x], e1 = std::min(B->row[vo + x + 1], e0 + arc_budget - scanned);
+      scanned += e1 - e0;
+      for (int64_t e = e0; e < e1; ++e) {
+        const int32_t y = B->col[e];
+        if (!is_taken(y)) q.push_back(y);
+      }
+    }
+  }
+}
 
 namespace {
 
@@ -1261,8 +1303,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
     return code;
   };
   P->f32 = cfg.delta_fp32c;
-  int width = cfg.width > 0 ? cfg.width : 512;
-  width = std::max(32, std::min(1024, (width + 31) / 32 * 32));
+  const int width = batched_width(cfg.width);
   P->width = width;
   P->W = (width / 32 + 3) / 4 * 4;  // row stride: whole 4-word groups (16-byte mask loads)
   const int W = P->W;
@@ -1300,38 +1341,76 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
     ncap = std::max<int64_t>(ncap, npl);
     const int64_t arcs = B->row[vo + nb] - B->row[vo];
     // chain membership, and the shape the closed forms rely on: each chain
-    // vertex has exactly its two chain neighbours, the ends are distinct core vertices
-    cof.assign((size_t)nb, -1);
-    cpos.assign((size_t)nb, -1);
+    // vertex has exactly its two chain neighbours, the ends are distinct core
+    // vertices. Checked in parallel; the error reported is the one a pass in
+    // chain order meets first (per chain: equal ends, then a vertex an
+    // earlier chain holds, then the neighbours).
+    const int64_t nchb = ce1 - ce0;
+    std::vector<int32_t> first((size_t)nb, INT32_MAX);  // smallest chain (BCC-relative) holding each vertex
+    std::vector<int32_t> csize((size_t)nchb + 1, 0);     // prefix-sum entries of each chain (0: nothing hangs off it)
+    std::vector<uint8_t> cerr((size_t)nchb, 0);          // 1 equal ends, 3 bad neighbours (2 = overlap, below)
     int kmax = 0;
-    for (int64_t c = ce0; c < ce1; ++c) {
-      const int32_t s = B->chain_start[c], k = B->chain_len[c], L = B->chain_l[c], R = B->chain_r[c];
-      if (L == R) return bail(BCGPU_EINVAL, "a chain whose two ends are the same vertex");
+#pragma omp parallel for schedule(static) reduction(max : kmax)
+    for (int64_t i = 0; i < nchb; ++i) {
+      const int64_t c = ce0 + i;
+      const int32_t st = B->chain_start[c], k = B->chain_len[c], L = B->chain_l[c], R = B->chain_r[c];
       kmax = std::max(kmax, k);
+      if (L == R) { cerr[(size_t)i] = 1; continue; }
+      bool flat = true;
       for (int32_t j = 0; j < k; ++j) {
-        if (cof[s + j] >= 0) return bail(BCGPU_EINVAL, "chains overlap");
-        cof[s + j] = (int32_t)c;
-        cpos[s + j] = j;
-      }
-
-      for (int32_t j = 0; j < k; ++j) {
-        const int32_t x = s + j, prev = j == 0 ? L : x - 1, next = j == k - 1 ? R : x + 1;
+        int32_t *f = &first[(size_t)(st + j)];
+        int32_t cur = __atomic_load_n(f, __ATOMIC_RELAXED);
+        while ((int32_t)i < cur && !__atomic_compare_exchange_n(f, &cur, (int32_t)i, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+        }
+        const int32_t x = st + j, prev = j == 0 ? L : x - 1, next = j == k - 1 ? R : x + 1;
         const int64_t e0 = B->row[vo + x], e1 = B->row[vo + x + 1];
         if (e1 - e0 != 2 || !((B->col[e0] == prev && B->col[e0 + 1] == next) || (B->col[e0] == next && B->col[e0 + 1] == prev)))
-          return bail(BCGPU_EINVAL, "a chain vertex whose neighbours are not its chain neighbours");
+          cerr[(size_t)i] = 3;
+        flat = flat && B->reach[vo + x] == 0;
       }
-      bool flat = true;
-      for (int32_t j = 0; j < k; ++j) flat = flat && B->reach[vo + s + j] == 0;
-      cpre_off[c] = flat ? -1 : (int64_t)cpre.size();
+      csize[(size_t)i + 1] = flat ? 0 : k + 1;
+    }
+    int64_t bad_chain = nchb;  // the first chain with an error
+#pragma omp parallel for schedule(static) reduction(min : bad_chain)
+    for (int64_t i = 0; i < nchb; ++i) {
+      if (cerr[(size_t)i] != 1) {
+        const int32_t st = B->chain_start[ce0 + i], k = B->chain_len[ce0 + i];
+        for (int32_t j = 0; j < k; ++j)
+          if (first[(size_t)(st + j)] < (int32_t)i) cerr[(size_t)i] = 2;  // an earlier chain holds the vertex
+      }
+      if (cerr[(size_t)i]) bad_chain = std::min(bad_chain, i);
+    }
+    if (bad_chain < nchb) {
+      const int e = cerr[(size_t)bad_chain];
+      return bail(BCGPU_EINVAL, e == 1 ? "a chain whose two ends are the same vertex"
+                                 : e == 2 ? "chains overlap"
+                                          : "a chain vertex whose neighbours are not its chain neighbours");
+    }
+    for (int64_t i = 0; i < nchb; ++i) csize[(size_t)i + 1] += csize[(size_t)i];
+    const int64_t cpre0 = (int64_t)cpre.size();
+    cpre.resize((size_t)(cpre0 + csize[(size_t)nchb]));
+    cof.assign((size_t)nb, -1);
+    cpos.assign((size_t)nb, -1);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nchb; ++i) {
+      const int64_t c = ce0 + i;
+      const int32_t st = B->chain_start[c], k = B->chain_len[c];
+      for (int32_t j = 0; j < k; ++j) {
+        cof[(size_t)(st + j)] = (int32_t)c;
+        cpos[(size_t)(st + j)] = j;
+      }
+      const bool flat = csize[(size_t)i + 1] == csize[(size_t)i];
+      cpre_off[c] = flat ? -1 : cpre0 + csize[(size_t)i];
       if (!flat) {
-        double acc = 0.0;
-        cpre.push_back(0.0);
+        double *P = cpre.data() + cpre0 + csize[(size_t)i], acc = 0.0;
+        P[0] = 0.0;
         for (int32_t j = 0; j < k; ++j) {
-          acc += (double)B->reach[vo + s + j] + 1.0;
-          cpre.push_back(acc);
+          acc += (double)B->reach[vo + st + j] + 1.0;
+          P[j + 1] = acc;
         }
       }
     }
+    HOST_MARK("b: chains");
     // contracted rows: unit arcs first, then chain arcs
     hvo.push_back((int64_t)hrow.size());
     const int heavy_deg = npl < kSmallCore ? kHeavyDegSmall : kHeavyDeg;
@@ -1368,50 +1447,19 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
     const int32_t ecc = cfg.ecc0 && (*cfg.ecc0)[b] >= 0 ? (*cfg.ecc0)[b] : bcc_ecc(B->row, B->col, vo, nb, dist, queue);
     tcap = std::max(tcap, 2 * ecc + kmax + 3);
 
-    // Source order: bounded BFS balls of nearby vertices (chain vertices
-    // included), so a pass's sources see every vertex within a narrow band of
-    // levels: few active levels per vertex, dense 32-slot hits. A ball grows
-    // only through vertices not yet taken, so each vertex's arcs are scanned
-    // once and late balls cost no rescans of finished regions.
-    // Only passes [jf0, jf1) of this BCC are filled (cfg.fill_begin/end); the
-    // source order is then needed up to pass jf1 only, and the greedy below
-    // produces it as a prefix.
     const int64_t bat0g = (int64_t)P->h_batches.size(), nbat = ((int64_t)nb + width - 1) / width;
     const int64_t jf0 = std::min(nbat, std::max<int64_t>(0, cfg.fill_begin - bat0g));
     const int64_t jf1 = std::max(jf0, std::min(nbat, cfg.fill_end - bat0g));
     const size_t need = (size_t)std::min<int64_t>(nb, jf1 * (int64_t)width);
-    std::vector<int32_t> order;
-    order.reserve(need);
-    if (need > 0) {
-      // mark[y]: the ball that queued y, or kTaken once y is in the order (a
-      // vertex queued by an earlier ball but not taken may join a later one)
-      constexpr int32_t kTaken = INT32_MAX;
-      std::vector<int32_t> mark((size_t)nb, -1), q;
-      int32_t ball = 0;
-      const int64_t arc_budget = 16 * (int64_t)width;  // bounds the host work per ball
-      for (int32_t seed = 0; seed < nb && order.size() < need; ++seed) {
-        if (mark[seed] == kTaken) continue;
-        q.clear();
-        q.push_back(seed);
-        mark[seed] = ball;
-        int64_t got = 0, scanned = 0;
-        for (size_t h = 0; h < q.size() && got < width; ++h) {
-          const int32_t x = q[h];
-          mark[x] = kTaken;
-          order.push_back(x);
-          ++got;
-          if (scanned >= arc_budget) continue;  // keep draining the queue, stop growing it
-          const int64_t e0 = B->row[vo + x], e1 = std::min(B->row[vo + x + 1], e0 + arc_budget - scanned);
-          scanned += e1 - e0;
-          for (int64_t e = e0; e < e1; ++e) {
-            if (e + 8 < e1) __builtin_prefetch(&mark[B->col[e + 8]]);
-            const int32_t y = B->col[e];
-            if (mark[y] != ball && mark[y] != kTaken) { mark[y] = ball; q.push_back(y); }
-          }
-        }
-        ++ball;
-      }
+    std::vector<int32_t> own_order;
+    const std::vector<int32_t> *order_p = cfg.order_of ? &cfg.order_of(b) : nullptr;
+    if (!order_p) {
+      batched_source_order(B, b, width, (int64_t)need, own_order);
+      order_p = &own_order;
     }
+    const std::vector<int32_t> &order = *order_p;
+    if (order.size() < need) return bail(BCGPU_EINVAL, "source order shorter than the passes need");
+    HOST_MARK("b: order");
     // Passes of `width` consecutive sources of the order. Slots and seeds are
     // sized up front (a chain source has two seeds), then every pass fills
     // its own ranges in parallel; the arming lists (variable length after
@@ -1483,6 +1531,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
       P->u_visits.push_back((int64_t)bt.nslots * nb);
     }
   }
+  HOST_MARK("b: passes");
   P->tcap = tcap;
   P->n_cap = ncap;
   P->n_batches = (int64_t)P->h_batches.size();
@@ -1502,8 +1551,17 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   if (need > cfg.limit_bytes)
     return bail(BCGPU_ENOMEM, "batched workspace " + std::to_string(need >> 20) + " MiB exceeds the limit " +
                                   std::to_string(cfg.limit_bytes >> 20) + " MiB (lower the batch width)");
+  P->pool = cfg.pool;
+  P->stream = stream;
   auto alloc = [&](void **p, int64_t bytes) -> bool {
-    if (cudaMalloc(p, (size_t)std::max<int64_t>(bytes, 16)) != cudaSuccess) return false;
+    const size_t sz = (size_t)std::max<int64_t>(bytes, 16);
+    cudaError_t e = P->pool ? cudaMallocFromPoolAsync(p, sz, P->pool, stream) : cudaMalloc(p, sz);
+    if (e == cudaErrorMemoryAllocation && P->pool) {  // trim the pool's unused reserve once and retry
+      cudaGetLastError();
+      if (cudaStreamSynchronize(stream) == cudaSuccess && cudaMemPoolTrimTo(P->pool, 0) == cudaSuccess)
+        e = cudaMallocFromPoolAsync(p, sz, P->pool, stream);
+    }
+    if (e != cudaSuccess) return false;
     P->allocs.push_back(*p);
     P->bytes += bytes;
     return true;
@@ -1528,6 +1586,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   ok &= ok && alloc(&p, (int64_t)W * 32 * 4); a.rexp = (int32_t *)p;
   ok &= ok && alloc(&p, sizeof(Ctrl)); a.ctrl = (Ctrl *)p;
   ok &= ok && alloc(&p, (int64_t)std::max<int64_t>(P->n_batches, 1) * 4); a.redo = (int *)p;
+  HOST_MARK("b: ws alloc");
   // tables
   auto upload = [&](const void **dst, const void *src, int64_t bytes) -> bool {
     if (!alloc(&p, bytes)) return false;
@@ -1573,7 +1632,20 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   ok = ok && upload((const void **)&a.hchunk_e1, hchunk_e1.data(), nch * 8);
   ok = ok && upload((const void **)&a.hfirst, hfirst.data(), (int64_t)hfirst.size() * 4);
   ok = ok && upload((const void **)&a.batches, P->h_batches.data(), (int64_t)P->h_batches.size() * (int64_t)sizeof(Batch));
-  ok = ok && upload((const void **)&a.slots, slots.data(), (int64_t)slots.size() * (int64_t)sizeof(Slot));
+  {  // slots: only those of the filled passes are copied (the rest are never read)
+    int64_t s0 = (int64_t)slots.size(), s1 = 0;
+    for (int64_t j = std::max<int64_t>(0, cfg.fill_begin); j < std::min(P->n_batches, cfg.fill_end); ++j) {
+      s0 = std::min(s0, P->h_batches[(size_t)j].slot_off);
+      s1 = std::max(s1, P->h_batches[(size_t)j].slot_off + P->h_batches[(size_t)j].nslots);
+    }
+    ok = ok && alloc(&p, (int64_t)slots.size() * (int64_t)sizeof(Slot));
+    a.slots = (const Slot *)p;
+    if (ok && s1 > s0) {
+      const size_t bytes = (size_t)(s1 - s0) * sizeof(Slot);
+      ok = cudaMemcpyAsync((Slot *)p + s0, slots.data() + s0, bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess;
+      P->h2d += (int64_t)bytes;
+    }
+  }
   ok = ok && upload((const void **)&a.seeds, seeds.data(), (int64_t)seeds.size() * (int64_t)sizeof(Seed));
   ok = ok && upload((const void **)&a.arms, arms.data(), (int64_t)arms.size() * (int64_t)sizeof(int2));
   ok = ok && alloc(&p, std::max<int64_t>(nch, 1) * W * 32 * 8); a.hacc = (double *)p;
@@ -1587,6 +1659,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
     P->d2h += (int64_t)sizeof(int);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the host vectors go out of scope
+  HOST_MARK("b: uploads+sync");
   P->h_slots = std::move(slots);
   if (cfg.keep_host_tables) {
     P->h_seeds = std::move(seeds);
@@ -1646,7 +1719,10 @@ int batched_create(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *ro
 
 void batched_destroy(BatchedPlan *p) {
   if (!p) return;
-  for (void *a : p->allocs) cudaFree(a);
+  for (void *a : p->allocs) {
+    if (p->pool) cudaFreeAsync(a, p->stream);
+    else cudaFree(a);
+  }
   delete p;
 }
 

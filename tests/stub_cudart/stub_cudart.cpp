@@ -177,6 +177,36 @@ cudaError_t cudaFree(void *p) {
 }
 cudaError_t cudaMallocAsync(void **p, size_t bytes, cudaStream_t) { return cudaMalloc(p, bytes); }
 cudaError_t cudaFreeAsync(void *p, cudaStream_t) { return cudaFree(p); }
+// Memory pools: a pool is a tag; its allocations are ordinary stand-in
+// allocations. An injected failure of a pool allocation also fails the
+// allocation that follows it (the library retries once after trimming the
+// pool), so that every allocation can still be made to fail.
+struct StubPool { int id; };
+static bool g_pool_refail = false;
+cudaError_t cudaMemPoolCreate(cudaMemPool_t *pool, const cudaMemPoolProps *) {
+  *pool = reinterpret_cast<cudaMemPool_t>(new StubPool{0});
+  return cudaSuccess;
+}
+cudaError_t cudaMemPoolDestroy(cudaMemPool_t pool) {
+  delete reinterpret_cast<StubPool *>(pool);
+  return cudaSuccess;
+}
+cudaError_t cudaMemPoolSetAttribute(cudaMemPool_t, cudaMemPoolAttr, void *) { return cudaSuccess; }
+cudaError_t cudaMemPoolGetAttribute(cudaMemPool_t, cudaMemPoolAttr, void *value) {
+  *static_cast<uint64_t *>(value) = 0;  // nothing held in reserve
+  return cudaSuccess;
+}
+cudaError_t cudaMemPoolTrimTo(cudaMemPool_t, size_t) { return cudaSuccess; }
+cudaError_t cudaMallocFromPoolAsync(void **p, size_t bytes, cudaMemPool_t, cudaStream_t) {
+  if (g_pool_refail) {
+    g_pool_refail = false;
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  const cudaError_t e = cudaMalloc(p, bytes);
+  g_pool_refail = e == cudaErrorMemoryAllocation;
+  return e;
+}
 cudaError_t cudaMemcpyAsync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
   return on_stream(s, [=] {
     std::memcpy(dst, src, bytes);

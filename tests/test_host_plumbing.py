@@ -361,6 +361,61 @@ small.close()
     assert res["limit"][0] == 3 and "exceeds the limit" in res["limit"][1]
 
 
+def test_chain_shape_errors(stub_dir):
+    """The multi-source builder's chain checks (run in parallel) report the
+    error a pass in chain order meets first: equal ends, a vertex an earlier
+    chain holds, a chain vertex whose neighbours are not its chain
+    neighbours; with two faulty chains, the earlier one's error."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_small(1)
+d = decomp(n, u, v)
+a = d.arrays()
+ctx = P.Context(mode=P.MODE_BATCHED, plain_core=-1)
+b = int(np.argmax(np.diff(a["chain_off"])))
+c0 = int(a["chain_off"][b])
+out["chains"] = int(a["chain_off"][b + 1]) - c0
+
+def packed(**change):
+    arr = {k: np.array(x, copy=True) for k, x in a.items() if isinstance(x, np.ndarray)}
+    for k, f in change.items():
+        f(arr[k])
+    from centrality_gpu_b200 import autotune as A
+    return A.PackedBccs(dict(a, **arr))
+
+def put(i, val):
+    def f(x):
+        x[i] = val
+    return f
+
+def foreign(c):  # the first arc of chain c's first vertex leads to a core vertex off the chain
+    e0 = int(a["row"][int(a["vtx_off"][b]) + int(a["chain_start"][c])])
+    L, R = int(a["chain_l"][c]), int(a["chain_r"][c])
+    w = next(x for x in range(int(a["n_plain"][b])) if x not in (L, R))
+    return put(e0, w)
+
+cases = {
+    "ok": packed(),
+    "same": packed(chain_r=put(c0 + 3, int(a["chain_l"][c0 + 3]))),
+    "overlap": packed(chain_start=put(c0 + 6, int(a["chain_start"][c0 + 2]))),
+    "neigh": packed(col=foreign(c0 + 3)),
+    # chain 3 with foreign neighbours before chain 6 overlapping chain 2: chain 3's error
+    "first": packed(col=foreign(c0 + 3), chain_start=put(c0 + 6, int(a["chain_start"][c0 + 2]))),
+    # chain 2 with equal ends before chain 4 with foreign neighbours: chain 2's error
+    "first2": packed(chain_r=put(c0 + 2, int(a["chain_l"][c0 + 2])), col=foreign(c0 + 4)),
+}
+out["res"] = {k: raises(lambda: ctx.run(pk)) for k, pk in cases.items()}
+ctx.close()
+""")
+    r = res["res"]
+    assert res["chains"] >= 10
+    assert r["ok"] is None
+    want = {"same": "two ends are the same vertex", "overlap": "chains overlap",
+            "neigh": "neighbours are not its chain neighbours", "first": "neighbours are not its chain neighbours",
+            "first2": "two ends are the same vertex"}
+    for name, msg in want.items():
+        assert r[name] is not None and r[name][0] == 1 and msg in r[name][1], (name, r[name])
+
+
 def test_failed_plan_builds_release_everything(stub_dir):
     """A device allocation failing at any point of a plan build (PLAIN, and
     multi-source with per-source items) returns BCGPU_ENOMEM (3) and leaves
