@@ -93,6 +93,7 @@ _SIGS = {
     "bc_plan_num_units": (C.c_int64, [C.c_void_p]),
     "bc_plan_unit_work": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _i64p, _i64p, _i64p]),
     "bc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "bc_plan_tile_launches": (C.c_int, [C.c_void_p, _i32p, _i32p, C.c_int32]),
     "bc_plan_concurrency": (C.c_int, [C.c_void_p]),
     "bc_autotune_width": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "bc_plan_unit_sources": (C.c_int64, [C.c_void_p, C.c_int64, C.c_int64, _i64p, C.c_int64]),
@@ -368,6 +369,18 @@ class Plan:
         w = C.c_int64()
         self.ctx._check(lib().bc_plan_unit_work(self._h, begin, end, C.byref(s), C.byref(t), C.byref(w)))
         return s.value, t.value, w.value
+
+    def tile_launches(self):
+        """[(class, grid)] of the small-BCC schedule's launches, in launch order
+        (class: 0 warp per source; 1, 2, 3 one source per 256-, 512-, 1024-thread
+        CTA; 4, 5 a 1024-thread CTA of two / four source groups)."""
+        n = lib().bc_plan_tile_launches(self._h, None, None, 0)
+        if n < 0:
+            raise BcError(-n, "bc_plan_tile_launches")
+        cls = np.zeros(max(n, 1), dtype=np.int32)
+        grid = np.zeros(max(n, 1), dtype=np.int32)
+        lib().bc_plan_tile_launches(self._h, _ptr(cls, _i32p), _ptr(grid, _i32p), n)
+        return [(int(cls[i]), int(grid[i])) for i in range(n)]
 
     def unit_sources(self, begin=0, end=None):
         """Packed ids of the sources units [begin, end) accumulate."""

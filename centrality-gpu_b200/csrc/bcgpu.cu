@@ -394,8 +394,10 @@ constexpr int64_t kTileWarpMaxVertices = 640;
 // block has the largest work queue).
 int fit_cls(int c) { return c == bcg::kTileWarp ? c : bcg::kTileCta1024; }
 
-void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std::vector<int8_t> &cls) {
+void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std::vector<int8_t> &cls,
+                 std::vector<int32_t> &ecc_of) {
   cls.assign((size_t)B->n_bcc, -1);
+  ecc_of.assign((size_t)B->n_bcc, -1);
   const size_t lim = bcg::tile_smem_limit(ctx->device);
   if (lim == 0) return;
   const int64_t cap = std::min<int64_t>(ctx->opts.tile_max > 0 ? ctx->opts.tile_max : INT32_MAX, bcg::kTileMaxVertices);
@@ -416,6 +418,7 @@ void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std
       int64_t maxdeg = 1;
       for (int64_t k = vo; k < vo + nb; ++k) maxdeg = std::max(maxdeg, B->row[k + 1] - B->row[k]);
       const int ecc = bcc_ecc0(B, b, dist, queue, false);
+      ecc_of[b] = ecc;
       if ((2.0 * ecc + 1.0) * std::log2((double)std::max<int64_t>(maxdeg, 2)) <= 1000.0) want[b] = (int8_t)c;
     }
   }
@@ -438,27 +441,62 @@ void route_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<char> &on, std
 }
 
 // Work items, staged slices and warp workspace of the small-BCC schedule.
-// Launches: the warp class, then the CTA class in buckets of resident CTAs
-// per SM (4 or more, 3, 2, 1 -- from each BCC's own shared-memory need), the
-// items of each launch contiguous.
-int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, bc_plan *p) {
+// Launches: the warp class, then the CTA class in buckets by sources in
+// flight per SM (from each BCC's own shared-memory need): 256-thread CTAs at
+// 4 or more / 3 per SM; a 1024-thread CTA of four source groups (when four
+// groups' arrays and the slice fit, and the BCC fits that class's level
+// table); 512-thread CTAs at 2 per SM; a 1024-thread CTA of two groups; one
+// 1024-thread CTA per SM. Each bucket's items are contiguous.
+int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, const std::vector<int32_t> &ecc_of,
+                bc_plan *p) {
   int rc = BCGPU_OK;
   std::vector<int64_t> off((size_t)B->n_bcc, -1);
   std::vector<int32_t> size((size_t)B->n_bcc, 0);
   std::vector<int8_t> bucket((size_t)B->n_bcc, -1);
   constexpr int64_t kSmPerSm = 228 * 1024, kReserved = 1024;  // shared memory per SM, per-CTA reserve
+  // bucket k -> class: 0 warp, 1 / 2 CTA (4+ / 3 per SM), 3 four groups, 4 CTA-512, 5 two groups, 6 CTA-1024
+  constexpr int kBucketCls[7] = {bcg::kTileWarp,    bcg::kTileCta,       bcg::kTileCta,      bcg::kTileCta1024x4,
+                                 bcg::kTileCta512, bcg::kTileCta1024x2, bcg::kTileCta1024};
+  const int64_t lim = (int64_t)bcg::tile_smem_limit(ctx->device);
+  std::vector<int64_t> per((size_t)B->n_bcc, 0);
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     if (cls[b] < 0) continue;
     const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
     size[b] = (int32_t)bcg::TileSlice::bytes(nb, B->row[vo + nb] - B->row[vo]);
     if (cls[b] == bcg::kTileWarp) { bucket[b] = 0; continue; }
-    const int64_t per = kSmPerSm / ((int64_t)bcg::tile_smem_bytes(bcg::kTileCta, nb, size[b]) + kReserved);
-    bucket[b] = (int8_t)(per >= 4 ? 1 : per == 3 ? 2 : per == 2 ? 3 : 4);
+    per[b] = kSmPerSm / ((int64_t)bcg::tile_smem_bytes(bcg::kTileCta, nb, size[b]) + kReserved);
+    bucket[b] = (int8_t)(per[b] >= 4 ? 1 : per[b] == 3 ? 2 : per[b] == 2 ? 4 : 6);
   }
-  int64_t total = 0;
-  for (int k = 0; k <= 4; ++k) {
+  // the grouped classes: a BCC moves up when its groups fit and the bucket's
+  // launch (sized by its largest BCC and largest slice) still fits, smallest
+  // BCCs first
+  auto promote = [&](int to, auto &&eligible) {
+    std::vector<int32_t> cand;
+    for (int32_t b = 0; b < B->n_bcc; ++b) {
+      if (cls[b] < 0 || cls[b] == bcg::kTileWarp || !eligible(b)) continue;
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+      if (2 * (int64_t)ecc_of[b] + 3 >= bcg::kTileGroupMaxLevels) continue;  // levels <= 2 ecc + 1
+      if ((int64_t)bcg::tile_smem_bytes(kBucketCls[to], nb, size[b]) > lim) continue;
+      cand.push_back(b);
+    }
+    std::stable_sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) {
+      return B->vtx_off[x + 1] - B->vtx_off[x] < B->vtx_off[y + 1] - B->vtx_off[y];
+    });
+    int64_t nmax = 0, smax = 0;
+    for (int32_t b : cand) {
+      const int64_t nb = B->vtx_off[b + 1] - B->vtx_off[b];
+      if ((int64_t)bcg::tile_smem_bytes(kBucketCls[to], std::max(nmax, nb), std::max<int64_t>(smax, size[b])) > lim) break;
+      nmax = std::max(nmax, nb);
+      smax = std::max<int64_t>(smax, size[b]);
+      bucket[b] = (int8_t)to;
+    }
+  };
+  promote(3, [&](int32_t b) { return per[b] <= 3; });                    // four sources in flight, not at most three
+  promote(5, [&](int32_t b) { return per[b] <= 1 && bucket[b] == 6; });  // two instead of one
+  int64_t total = 0, p_rows = 1;
+  for (int k = 0; k <= 6; ++k) {
     bc_plan::TileLaunch T;
-    T.cls = k == 0 ? bcg::kTileWarp : k <= 2 ? bcg::kTileCta : k == 3 ? bcg::kTileCta512 : bcg::kTileCta1024;
+    T.cls = kBucketCls[k];
     T.i0 = (int64_t)p->h_titems.size();
     int64_t nmax = 0, smax = 0, sources = 0;
     for (int32_t b = 0; b < B->n_bcc; ++b) {
@@ -475,7 +513,10 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, b
     const int per_sm = bcg::tile_ctas_per_sm(T.cls, T.smem);
     if (per_sm < 1) return fail(ctx, BCGPU_ECUDA, "small-BCC schedule: no CTA fits an SM");
     T.grid = ctx->sms * per_sm;
-    const int64_t floor_items = T.cls == bcg::kTileWarp ? bcg::kTileWarps : 1;  // a warp-class item feeds 8 warps
+    const int groups = bcg::tile_groups(T.cls);
+    if (T.cls != bcg::kTileWarp) p_rows = std::max<int64_t>(p_rows, (int64_t)T.grid * groups);
+    // a warp-class item feeds 8 warps, a grouped CTA's item its groups
+    const int64_t floor_items = T.cls == bcg::kTileWarp ? bcg::kTileWarps : groups;
     const int32_t per_item = (int32_t)std::max<int64_t>(
         floor_items, std::min<int64_t>(kTileItemSources, sources / ((int64_t)T.grid * kTileItemsPerCta)));
     for (int32_t b = 0; b < B->n_bcc; ++b) {
@@ -503,20 +544,17 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, b
     for (int64_t e = 0; e < arcs; ++e) C[e] = (uint16_t)B->col[e0 + e];
   }
   p->n_titems = (int64_t)p->h_titems.size();
-  int warp_grid = 1, cta_grid = 1;
+  int warp_grid = 1;
   for (const auto &T : p->tl) {
     if (T.cls == bcg::kTileWarp) warp_grid = T.grid;
-    else {
-      cta_grid = std::max(cta_grid, T.grid);
-      p->tcap_P = std::max<int64_t>(p->tcap_P, T.nmax);
-    }
+    else p->tcap_P = std::max<int64_t>(p->tcap_P, T.nmax);
   }
   const int64_t slots = (int64_t)warp_grid * bcg::kTileWarps;
   p->tcap = std::max<int64_t>(p->tcap, 2);
   if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) || (rc = upload(p, &p->slice_off, off.data(), B->n_bcc)) ||
       (rc = upload(p, &p->slice_bytes, size.data(), B->n_bcc)) ||
       (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
-      (rc = dalloc(p, &p->tws_P, (int64_t)cta_grid * std::max<int64_t>(p->tcap_P, 1))) ||
+      (rc = dalloc(p, &p->tws_P, p_rows * std::max<int64_t>(p->tcap_P, 1))) ||
       (rc = alloc_acc(p, B->n_packed)))
     return rc;
   for (const auto &it : p->h_titems) {
@@ -654,9 +692,10 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
   int64_t limit = ctx->opts.workspace_limit > 0 ? ctx->opts.workspace_limit : (int64_t)(0.8 * avail_b);
   // BATCHED: BCCs off the multi-source passes that fit the small-BCC schedule
   std::vector<int8_t> tile;
+  std::vector<int32_t> tile_ecc;
   int64_t n_tile = 0;
   if (p->mode == BCGPU_MODE_BATCHED && ctx->opts.tile_max >= 0 && n_on < B->n_bcc) {
-    route_tiles(ctx, B, on, tile);
+    route_tiles(ctx, B, on, tile, tile_ecc);
     for (int8_t x : tile) n_tile += x >= 0;
   }
   HOST_MARK("route_tiles");
@@ -751,7 +790,7 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     p->h2d_bytes += (int64_t)(sizeof(int32_t) * ep.size());
   }
   HOST_MARK("plain items+ws");
-  if (n_tile && (rc = build_tiles(ctx, B, tile, p))) return bail(rc);
+  if (n_tile && (rc = build_tiles(ctx, B, tile, tile_ecc, p))) return bail(rc);
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   HOST_MARK("tiles+sync");
   return BCGPU_OK;
@@ -1004,6 +1043,16 @@ extern "C" int bc_plan_unit_work(const bc_plan *p, int64_t begin, int64_t end, i
 }
 
 extern "C" int64_t bc_plan_device_bytes(const bc_plan *p) { return p ? p->device_bytes : 0; }
+
+extern "C" int bc_plan_tile_launches(const bc_plan *p, int32_t *cls, int32_t *grid, int32_t cap) {
+  if (!p || cap < 0 || (cap > 0 && (!cls || !grid))) return BCGPU_EINVAL;
+  const int32_t n = (int32_t)p->tl.size();
+  for (int32_t i = 0; i < std::min(n, cap); ++i) {
+    cls[i] = p->tl[(size_t)i].cls;
+    grid[i] = p->tl[(size_t)i].grid;
+  }
+  return n;
+}
 extern "C" int bc_plan_concurrency(const bc_plan *p) { return !p ? 0 : p->mode == BCGPU_MODE_BATCHED ? 1 : p->grid; }
 
 extern "C" int64_t bc_plan_unit_sources(const bc_plan *p, int64_t begin, int64_t end, int64_t *out, int64_t cap) {

@@ -13,7 +13,10 @@
 //    is bounded) and serves every source of the item;
 //  * levels, path counts (then q in place) and the visit order of each source
 //    live in shared memory: one set per warp in the warp class (a warp per
-//    source, eight in flight), one per CTA in the CTA class;
+//    source, eight in flight), one per source group in the CTA class (the
+//    whole CTA on one source, or, for BCCs whose single-source CTA fits only
+//    once or twice per SM, two or four groups of a 1024-thread CTA on their
+//    own sources from the one slice);
 //  * forward: level-synchronous, each frontier vertex pulls sigma from its
 //    predecessors and claims its successors in one scan of its row -- a row of
 //    up to kLaneDeg arcs by one lane (four arcs' loads in flight), a longer one
@@ -26,9 +29,10 @@
 //    per-source schedule does;
 //  * BC: contributions delta * (reach(s)+1) (Codes/kernels_free.cu:425) go to
 //    shared-memory fixed-point counters (warp class: integer atomics, any
-//    order) or to an FP64 partial row (CTA class: the CTA's sources run one
-//    after another, each vertex written by one thread, so the order is fixed),
-//    then once per item into the global fixed-point counters.
+//    order) or to an FP64 partial row per source group (CTA class: a group's
+//    sources, fixed by the item, run one after another, each vertex written
+//    by one thread, so the order is fixed), then once per item into the
+//    global fixed-point counters.
 // Path counts are FP64 without per-level scaling: the plan routes a BCC here
 // only when no path count can pass 2^1000 ((2 ecc + 1) levels of at most
 // maxdeg predecessors each); a non-finite value still flags kDevOverflow.
@@ -53,7 +57,6 @@ constexpr int kLongQueue = 1024;
 struct Ctl {
   unsigned long long bar;  // mbarrier of the slice copy
   int item, next, bcc, pad;
-  int cnt[4], nq[4];  // CTA class: queue tails and long-row queue lengths of three consecutive levels
   int tails[kTileWarps];
 };
 
@@ -66,14 +69,33 @@ struct WarpLayout {  // ctl | counters [nmax][kAccDigits] | per warp: d [nmax], 
   __host__ __device__ static int64_t warps(int64_t nmax) { return cnt() + align16(nmax * kAccDigits * 8); }
   __host__ __device__ static int64_t slice(int64_t nmax) { return warps(nmax) + kTileWarps * per_warp(nmax); }
 };
-template <int kBlock>
-struct CtaLayout {  // ctl | sq [nmax] | d int16 [nmax] | S uint16 [nmax] | lv [kTileMaxLevels] | q [kLongQueue] | slice
-  __host__ __device__ static int64_t sq() { return align16(sizeof(Ctl)); }
-  __host__ __device__ static int64_t d(int64_t nmax) { return sq() + align16(8 * nmax); }
+// CTA class: kBlock threads in kBlock / kGroup groups, each group on its own
+// sources with its own arrays and barrier, all groups on the one staged slice.
+// ctl | per group: sq [nmax] | d int16 [nmax] | S uint16 [nmax] | lv [kLevels]
+//     | long-row queue [kQueue] | counters cnt[4], nq[4] | slice
+// (one group: levels and queue of the class limits; several: the smaller
+// limits of the grouped classes, tile.h).
+template <int kBlock, int kGroup>
+struct CtaLayout {
+  static constexpr int kG = kBlock / kGroup;
+  static constexpr int kLevels = kG == 1 ? kTileMaxLevels : kTileGroupMaxLevels;
+  static constexpr int kQueue = kG == 1 ? kLongQueue : kGroupLongQueue;
+  __host__ __device__ static int64_t d(int64_t nmax) { return align16(8 * nmax); }
   __host__ __device__ static int64_t S(int64_t nmax) { return d(nmax) + align16(2 * nmax); }
   __host__ __device__ static int64_t lv(int64_t nmax) { return S(nmax) + align16(2 * nmax); }
-  __host__ __device__ static int64_t q(int64_t nmax) { return lv(nmax) + align16(4 * kTileMaxLevels); }
-  __host__ __device__ static int64_t slice(int64_t nmax) { return q(nmax) + align16(4 * kLongQueue); }
+  __host__ __device__ static int64_t q(int64_t nmax) { return lv(nmax) + align16(4 * kLevels); }
+  __host__ __device__ static int64_t ctr(int64_t nmax) { return q(nmax) + align16(4 * kQueue); }
+  __host__ __device__ static int64_t group_bytes(int64_t nmax) { return ctr(nmax) + align16(8 * sizeof(int)); }
+  __host__ __device__ static int64_t group(int g, int64_t nmax) { return align16(sizeof(Ctl)) + g * group_bytes(nmax); }
+  __host__ __device__ static int64_t slice(int64_t nmax) { return group(kG, nmax); }
+  // the group's barrier: the CTA's own when the group is the CTA, else named barrier g+1
+  __device__ __forceinline__ static void sync(int g) {
+    if constexpr (kG == 1) {
+      __syncthreads();
+    } else {
+      asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(kGroup) : "memory");
+    }
+  }
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -396,26 +418,28 @@ __global__ void __launch_bounds__(kThreads, 1) tile_warp_kernel(TileArgs a) {
 
 // ======================================================== CTA per source ===
 
-// BFS of the whole CTA from s, two barriers per level: the frontier's rows of
-// up to kLaneDeg arcs are scanned by one thread each (chunks of a level are
-// independent: they read the previous level only) while longer rows are
-// queued; after a barrier the warps share the queued rows; a second barrier
-// ends the level. Queue and tail counters of level l are cnt[l % 3] and
-// nq[l % 3]; those of level l+1 are cleared at the start of level l, two
-// barriers after their last reader.
-template <int kBlock>
+// BFS of one group (the whole CTA, or a fixed share of its threads) from s,
+// two group barriers per level: the frontier's rows of up to kLaneDeg arcs
+// are scanned by one thread each (chunks of a level are independent: they
+// read the previous level only) while longer rows are queued; after a
+// barrier the group's warps share the queued rows; a second barrier ends the
+// level. Queue and tail counters of level l are cnt[l % 3] and nq[l % 3];
+// those of level l+1 are cleared at the start of level l, two barriers after
+// their last reader.
+template <int kBlock, int kGroup>
 __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double *sq, uint16_t *S, int32_t *lv,
-                       int32_t *q, int *cnt, int *nq, int *err) {
-  constexpr int kWarps = kBlock / 32;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int v = tid; v < nb; v += kBlock) d[v] = -1;
+                       int32_t *q, int *cnt, int *nq, int *err, int grp, int tid) {
+  using L = CtaLayout<kBlock, kGroup>;
+  constexpr int kWarps = kGroup / 32;
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int v = tid; v < nb; v += kGroup) d[v] = -1;
   if (tid == 0) {
     cnt[0] = 0;
     cnt[1] = 0;
     nq[0] = 0;
     nq[1] = 0;
   }
-  __syncthreads();
+  L::sync(grp);
   if (tid == 0) {
     d[s] = 0;
     S[0] = (uint16_t)s;
@@ -423,7 +447,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
     lv[0] = 0;
     lv[1] = 1;
   }
-  __syncthreads();
+  L::sync(grp);
   int lev = 0, f0 = 0, f1 = 1;
   while (true) {
     const int dprev = lev == 0 ? INT_MIN : lev - 1, dnext = lev + 1;
@@ -432,7 +456,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
       cnt[(lev + 1) % 3] = 0;
       nq[(lev + 1) % 3] = 0;
     }
-    for (int c0 = f0; c0 < f1; c0 += kBlock) {  // uniform
+    for (int c0 = f0; c0 < f1; c0 += kGroup) {  // uniform over the group
       const int i = c0 + tid;
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < f1) {
@@ -448,7 +472,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
       bool mine = false;  // a long row the queue had no room for
       if (w >= 0 && big) {
         const int pos = atomicAdd(nql, 1);
-        if (pos < kLongQueue) q[pos] = w;
+        if (pos < L::kQueue) q[pos] = w;
         else mine = true;
       }
       uint32_t over = __ballot_sync(0xffffffffu, mine);
@@ -460,17 +484,17 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
         if (lane == 0 && lev > 0) sq[wj] = acc;
       }
     }
-    __syncthreads();
-    const int nlong = min(*(volatile int *)nql, kLongQueue);
+    L::sync(grp);
+    const int nlong = min(*(volatile int *)nql, L::kQueue);
     for (int k = warp; k < nlong; k += kWarps) {
       const int32_t w = q[k];
       const double acc = pull_row_warp(g, g.R[w], g.R[w + 1], d, sq, S + f1, tail, dprev, dnext, lane);
       if (lane == 0 && lev > 0) sq[w] = acc;
     }
-    __syncthreads();
+    L::sync(grp);
     const int t = f1 + *(volatile int *)tail;
     if (t == f1) break;
-    if (lev + 2 >= kTileMaxLevels) {  // uniform; routing keeps BCCs below this depth
+    if (lev + 2 >= L::kLevels) {  // uniform; routing keeps BCCs below this depth
       if (tid == 0) set_err(err, kDevWorkspace);
       return -1;
     }
@@ -482,23 +506,25 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
   return lev + 1;
 }
 
-// Dependency sweep of the whole CTA, two barriers per level as in cta_bfs;
-// contributions go to the FP64 row P, each vertex written by one thread.
-template <int kBlock>
+// Dependency sweep of one group, two group barriers per level as in cta_bfs;
+// contributions go to the group's FP64 row P, each vertex written by one
+// thread.
+template <int kBlock, int kGroup>
 __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq, const uint16_t *S, const int32_t *lv,
-                          int32_t *q, int *nq, double wsrc, double *P, int *err) {
-  constexpr int kWarps = kBlock / 32;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+                          int32_t *q, int *nq, double wsrc, double *P, int *err, int grp, int tid) {
+  using L = CtaLayout<kBlock, kGroup>;
+  constexpr int kWarps = kGroup / 32;
+  const int lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     nq[0] = 0;
     nq[1] = 0;
   }
-  __syncthreads();
+  L::sync(grp);
   for (int lev = nlev - 1, k3 = 0; lev >= 1; --lev, k3 = (k3 + 1) % 3) {
     const int dsucc = lev + 1, a0 = lv[lev], a1 = lv[lev + 1];
     int *nql = nq + k3;
     if (tid == 0) nq[(k3 + 1) % 3] = 0;
-    for (int c0 = a0; c0 < a1; c0 += kBlock) {  // uniform
+    for (int c0 = a0; c0 < a1; c0 += kGroup) {  // uniform over the group
       const int i = c0 + tid;
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < a1) {
@@ -511,7 +537,7 @@ __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq,
       bool mine = false;
       if (w >= 0 && big) {
         const int pos = atomicAdd(nql, 1);
-        if (pos < kLongQueue) q[pos] = w;
+        if (pos < L::kQueue) q[pos] = w;
         else mine = true;
       }
       uint32_t over = __ballot_sync(0xffffffffu, mine);
@@ -523,31 +549,38 @@ __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq,
         if (lane == 0) P[wj] += finish(g, wj, sum, sq, err) * wsrc;
       }
     }
-    __syncthreads();
-    const int nlong = min(*(volatile int *)nql, kLongQueue);
+    L::sync(grp);
+    const int nlong = min(*(volatile int *)nql, L::kQueue);
     for (int k = warp; k < nlong; k += kWarps) {
       const int32_t w = q[k];
       const double sum = push_row_warp(g, g.R[w], g.R[w + 1], d, sq, dsucc, lane);
       if (lane == 0) P[w] += finish(g, w, sum, sq, err) * wsrc;
     }
-    __syncthreads();
+    L::sync(grp);
   }
 }
 
 // 1024 / kBlock CTAs per SM at most (the shared-memory buckets), so 64
-// registers per thread whatever the block size.
-template <int kBlock>
+// registers per thread whatever the block size. Group grp of the CTA takes
+// the item's sources s0 + grp, s0 + grp + G, ... one after another (a fixed
+// assignment: its FP64 row P is summed in a fixed order), then flushes P into
+// the integer counters (any order).
+template <int kBlock, int kGroup>
 __global__ void __launch_bounds__(kBlock, 1024 / kBlock) tile_cta_kernel(TileArgs a) {
+  using L = CtaLayout<kBlock, kGroup>;
   extern __shared__ __align__(16) unsigned char s_raw[];
   const int64_t nmax = a.nmax;
   Ctl &ctl = *reinterpret_cast<Ctl *>(s_raw);
-  double *P = a.ws_P + (int64_t)blockIdx.x * a.cap_P;  // this CTA's FP64 partial row (global, L2-resident)
-  double *sq = reinterpret_cast<double *>(s_raw + CtaLayout<kBlock>::sq());
-  int16_t *d = reinterpret_cast<int16_t *>(s_raw + CtaLayout<kBlock>::d(nmax));
-  uint16_t *S = reinterpret_cast<uint16_t *>(s_raw + CtaLayout<kBlock>::S(nmax));
-  int32_t *lv = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::lv(nmax));
-  int32_t *q = reinterpret_cast<int32_t *>(s_raw + CtaLayout<kBlock>::q(nmax));
-  unsigned char *slice = s_raw + CtaLayout<kBlock>::slice(nmax);
+  const int grp = threadIdx.x / kGroup, gtid = threadIdx.x % kGroup;
+  unsigned char *mine = s_raw + L::group(grp, nmax);
+  double *P = a.ws_P + ((int64_t)blockIdx.x * L::kG + grp) * a.cap_P;  // the group's FP64 row (global, L2-resident)
+  double *sq = reinterpret_cast<double *>(mine);
+  int16_t *d = reinterpret_cast<int16_t *>(mine + L::d(nmax));
+  uint16_t *S = reinterpret_cast<uint16_t *>(mine + L::S(nmax));
+  int32_t *lv = reinterpret_cast<int32_t *>(mine + L::lv(nmax));
+  int32_t *q = reinterpret_cast<int32_t *>(mine + L::q(nmax));
+  int *cnt = reinterpret_cast<int *>(mine + L::ctr(nmax)), *nq = cnt + 4;
+  unsigned char *slice = s_raw + L::slice(nmax);
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&ctl.bar, 1);
@@ -559,33 +592,37 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) tile_cta_kernel(TileArg
   int64_t vo;
   int32_t nb;
   while (next_item(a, ctl, slice, phase, it, vo, nb)) {
-    for (int v = tid; v < nb; v += kBlock) P[v] = 0.0;
+    for (int v = gtid; v < nb; v += kGroup) P[v] = 0.0;
     __syncthreads();
     if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
     const View g = view_of(a, slice, nb, vo);
-    for (int32_t s = it.s0; s < it.s1; ++s) {  // one source at a time: P is summed in source order
-      const int nlev = cta_bfs<kBlock>(g, nb, s, d, sq, S, lv, q, ctl.cnt, ctl.nq, a.err);
+    for (int32_t s = it.s0 + grp; s < it.s1; s += L::kG) {  // the group's sources in order: P's sums are fixed
+      const int nlev = cta_bfs<kBlock, kGroup>(g, nb, s, d, sq, S, lv, q, cnt, nq, a.err, grp, gtid);
       if (nlev < 0) break;
-      cta_sweep<kBlock>(g, nlev, d, sq, S, lv, q, ctl.nq, (double)__ldg(g.rch + s) + 1.0, P, a.err);
+      cta_sweep<kBlock, kGroup>(g, nlev, d, sq, S, lv, q, nq, (double)__ldg(g.rch + s) + 1.0, P, a.err, grp, gtid);
     }
     __syncthreads();
     unsigned long long *acc = a.acc + (int64_t)kAccDigits * vo;
-    for (int v = tid; v < nb; v += kBlock)
+    for (int v = gtid; v < nb; v += kGroup)
       if (P[v] != 0.0) acc_add(acc + (int64_t)kAccDigits * v, P[v], a.err);
   }
 }
 
 }  // namespace
 
-int block_of(int cls) { return cls == kTileCta1024 ? 1024 : cls == kTileCta512 ? 512 : kThreads; }
+int block_of(int cls) { return cls >= kTileCta1024 ? 1024 : cls == kTileCta512 ? 512 : kThreads; }
 
 size_t tile_smem_bytes(int cls, int64_t nmax, int64_t slice_max) {
-  const int64_t head = cls == kTileWarp     ? WarpLayout::slice(nmax)
-                       : cls == kTileCta    ? CtaLayout<256>::slice(nmax)
-                       : cls == kTileCta512 ? CtaLayout<512>::slice(nmax)
-                                            : CtaLayout<1024>::slice(nmax);
+  const int64_t head = cls == kTileWarp       ? WarpLayout::slice(nmax)
+                       : cls == kTileCta      ? CtaLayout<256, 256>::slice(nmax)
+                       : cls == kTileCta512   ? CtaLayout<512, 512>::slice(nmax)
+                       : cls == kTileCta1024  ? CtaLayout<1024, 1024>::slice(nmax)
+                       : cls == kTileCta1024x2 ? CtaLayout<1024, 512>::slice(nmax)
+                                              : CtaLayout<1024, 256>::slice(nmax);
   return (size_t)(head + align16(slice_max));
 }
+
+int tile_groups(int cls) { return cls == kTileCta1024x2 ? 2 : cls == kTileCta1024x4 ? 4 : 1; }
 
 size_t tile_smem_limit(int device) {
   int v = 0;
@@ -595,10 +632,12 @@ size_t tile_smem_limit(int device) {
 
 namespace {
 const void *tile_fn(int cls) {
-  return cls == kTileWarp     ? reinterpret_cast<const void *>(tile_warp_kernel)
-         : cls == kTileCta    ? reinterpret_cast<const void *>(tile_cta_kernel<256>)
-         : cls == kTileCta512 ? reinterpret_cast<const void *>(tile_cta_kernel<512>)
-                              : reinterpret_cast<const void *>(tile_cta_kernel<1024>);
+  return cls == kTileWarp       ? reinterpret_cast<const void *>(tile_warp_kernel)
+         : cls == kTileCta      ? reinterpret_cast<const void *>(tile_cta_kernel<256, 256>)
+         : cls == kTileCta512   ? reinterpret_cast<const void *>(tile_cta_kernel<512, 512>)
+         : cls == kTileCta1024  ? reinterpret_cast<const void *>(tile_cta_kernel<1024, 1024>)
+         : cls == kTileCta1024x2 ? reinterpret_cast<const void *>(tile_cta_kernel<1024, 512>)
+                                : reinterpret_cast<const void *>(tile_cta_kernel<1024, 256>);
 }
 }  // namespace
 
@@ -615,9 +654,12 @@ cudaError_t launch_tile(int cls, const TileArgs &a, int grid, size_t smem, cudaS
   if (e != cudaSuccess) return e;
   switch (cls) {
     case kTileWarp: tile_warp_kernel<<<grid, kThreads, smem, stream>>>(a); break;
-    case kTileCta: tile_cta_kernel<256><<<grid, 256, smem, stream>>>(a); break;
-    case kTileCta512: tile_cta_kernel<512><<<grid, 512, smem, stream>>>(a); break;
-    default: tile_cta_kernel<1024><<<grid, 1024, smem, stream>>>(a); break;
+    case kTileCta: tile_cta_kernel<256, 256><<<grid, 256, smem, stream>>>(a); break;
+    case kTileCta512: tile_cta_kernel<512, 512><<<grid, 512, smem, stream>>>(a); break;
+    case kTileCta1024: tile_cta_kernel<1024, 1024><<<grid, 1024, smem, stream>>>(a); break;
+    case kTileCta1024x2: tile_cta_kernel<1024, 512><<<grid, 1024, smem, stream>>>(a); break;
+    case kTileCta1024x4: tile_cta_kernel<1024, 256><<<grid, 1024, smem, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }

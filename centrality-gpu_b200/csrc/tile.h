@@ -21,9 +21,16 @@ struct TileItem {
 // kTileCta512 / kTileCta1024: the CTA class with 512 / 1024 threads, for the
 // BCCs whose shared memory allows only two / one CTA per SM (more lanes on
 // each level and more warps per SM than two or one 256-thread CTAs).
-enum TileClass : int { kTileWarp = 0, kTileCta = 1, kTileCta512 = 2, kTileCta1024 = 3 };
+// kTileCta1024x2 / kTileCta1024x4: 1024 threads in two groups of 512 / four
+// of 256, each group on its own source with its own arrays, every group on
+// the one staged slice: two / four sources in flight per SM for BCCs whose
+// single-source CTA fits only once or twice per SM.
+enum TileClass : int { kTileWarp = 0, kTileCta = 1, kTileCta512 = 2, kTileCta1024 = 3, kTileCta1024x2 = 4,
+                       kTileCta1024x4 = 5 };
 constexpr int kTileWarps = 8;          // warps per CTA
 constexpr int kTileMaxLevels = 1024;   // BFS levels the CTA class records (routing keeps BCCs below)
+constexpr int kTileGroupMaxLevels = 256;  // the same for the grouped classes
+constexpr int kGroupLongQueue = 256;      // long-row queue of a group in the grouped classes
 constexpr int32_t kTileMaxVertices = 65535;  // neighbour ids are 16-bit in the slice
 
 // Byte layout of one BCC's staged slice, each part starting on a 16-byte
@@ -46,7 +53,7 @@ struct TileArgs {
   unsigned long long *acc;        // [n_packed][kAccDigits] fixed-point BC counters (plain.h)
   int32_t *ws_lv;                 // warp class: level offsets per warp slot ([slots][cap])
   int64_t cap;                    // per-slot row capacity (>= largest BCC of the class + 2)
-  double *ws_P;                   // CTA class: FP64 partial BC row per CTA ([grid][cap_P])
+  double *ws_P;                   // CTA class: FP64 partial BC row per source group ([grid * groups][cap_P])
   int64_t cap_P;
   int32_t nmax;                   // largest BCC of the launch (shared-memory rows are sized for it)
   int32_t slice_max;              // largest slice in bytes
@@ -57,6 +64,8 @@ struct TileArgs {
 // Dynamic shared memory of a launch of class cls for BCCs of up to nmax
 // vertices and slices of up to slice_max bytes.
 size_t tile_smem_bytes(int cls, int64_t nmax, int64_t slice_max);
+// Source groups per CTA of class cls (each with its own FP64 row in ws_P).
+int tile_groups(int cls);
 // Largest shared memory a CTA may use (opt-in limit of the device).
 size_t tile_smem_limit(int device);
 // CTAs of class cls resident per SM at this shared-memory size (0: none fits).

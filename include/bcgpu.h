@@ -91,7 +91,9 @@ typedef struct bc_ctx bc_ctx;
 /* Fills opts with defaults (device -1, BATCHED, FP32C, width 0 = 512, lazy tables on, graph off). */
 void bc_default_opts(bc_opts *opts);
 int bc_create(const bc_opts *opts, bc_ctx **out);
-/* Releases the context and every plan still alive on it. */
+/* Releases the context, every plan still alive on it and its device-memory
+ * pool (plans allocate from a pool of the context's; memory a destroyed plan
+ * held stays reserved for the context's next plans until bc_destroy). */
 void bc_destroy(bc_ctx *ctx);
 /* Message of the last failing call on ctx (or of bc_create when ctx is NULL). */
 const char *bc_last_error(const bc_ctx *ctx);
@@ -217,7 +219,9 @@ int bc_wait_probe(bc_ctx *ctx, int32_t limit_ms, double *waited_ms);
 typedef struct bc_plan bc_plan;
 int bc_plan_create(bc_ctx *ctx, const bc_bccs *bccs, bc_plan **out);
 /* Must not be called after bc_destroy of the plan's context (which already
- * released it). */
+ * released it). The plan's device memory returns to the context's pool,
+ * ordered on its stream: a later plan of the context reuses it without a new
+ * device allocation (the workspace limit counts it as free). */
 void bc_plan_destroy(bc_plan *plan);
 int64_t bc_plan_num_units(const bc_plan *plan);
 /* Work covered by units [begin, end): sources, TEPS arcs (sum over sources of
@@ -231,6 +235,12 @@ int bc_plan_unit_work(const bc_plan *plan, int64_t begin, int64_t end, int64_t *
 int64_t bc_plan_unit_sources(const bc_plan *plan, int64_t begin, int64_t end, int64_t *out, int64_t cap);
 /* Device buffers the plan consumes (for roofline accounting). */
 int64_t bc_plan_device_bytes(const bc_plan *plan);
+/* The small-BCC schedule's launches, in launch order: each one's CTA class
+ * (0 warp per source; 1, 2, 3: one source per 256-, 512-, 1024-thread CTA;
+ * 4, 5: a 1024-thread CTA of two / four source groups) and grid size. Writes
+ * up to cap entries; returns the number of launches (negative error code on
+ * failure). Introspection for tests and tools; no reference counterpart. */
+int bc_plan_tile_launches(const bc_plan *plan, int32_t *cls, int32_t *grid, int32_t cap);
 /* Work units that run at once: PLAIN, the resident CTAs (one item each);
  * BATCHED, 1 (one pass at a time over the whole GPU). No reference
  * counterpart: the reference launches one source at a time. */

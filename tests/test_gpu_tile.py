@@ -1,5 +1,6 @@
 """The small-BCC schedule on the B200 (one CTA per range of sources of a BCC,
-its CSR slice staged in shared memory by a bulk copy, one warp per source):
+its CSR slice staged in shared memory by a bulk copy; a warp, a CTA or a
+group of a CTA per source):
 BC against the oracle in FP64 (1e-12) on its own and mixed with the other two
 schedules in one plan, bit-identical reruns, and BCCs at the size limits of
 the schedule (the smallest, 3 vertices; the largest that fits shared
@@ -85,6 +86,31 @@ def test_tile_reruns_are_bit_identical():
         plan.close()
     ctx.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_grouped_ctas_match_the_oracle():
+    """Six BA graphs of 2,500-6,000 vertices: their BCCs (3,800-8,300
+    vertices with chains) fit a one-source CTA only once or twice per SM and
+    take the 1024-thread CTAs of four and two source groups sharing the
+    staged slice (classes 5 and 4) next to the one-source 1024-thread CTA;
+    FP64 BC against the oracle, and a second run bit-identical."""
+    P = pkg()
+    G = graphs()
+    n, u, v, _ = G.pack_graphs(G.gen_ba_batch(6, 2500, 6000, seed=21))
+    d = decomp(n, u, v)
+    ctx = P.Context(mode=P.MODE_BATCHED, delta=P.DELTA_FP64, tile_max=0)
+    plan = ctx.plan(d)
+    classes = [c for c, _ in plan.tile_launches()]
+    assert 4 in classes and 5 in classes, classes
+    plan.run()
+    got = plan.read()
+    plan.reset()
+    plan.run()
+    again = plan.read()
+    plan.close()
+    ctx.close()
+    assert np.array_equal(got, again)
+    assert rel_err(got, oracle_bc(n, u, v)) < TOL["fp64"]
 
 
 def test_tile_unit_ranges_add_up():

@@ -416,6 +416,27 @@ ctx.close()
         assert r[name] is not None and r[name][0] == 1 and msg in r[name][1], (name, r[name])
 
 
+def test_large_small_bccs_take_grouped_ctas(stub_dir):
+    """BCCs whose one-source CTA fits only once or twice per SM go to a
+    1024-thread CTA of two or four source groups sharing one staged slice
+    (classes 4, 5) when the groups fit shared memory; every source is in
+    exactly one item."""
+    res = run_stub(stub_dir, """
+n, u, v = G.pack_graphs(G.gen_ba_batch(12, 2500, 6000, seed=21))[:3]
+d = decomp(n, u, v)
+ctx = P.Context(mode=P.MODE_BATCHED, tile_max=0)
+plan = ctx.plan(d)
+out["launches"] = plan.tile_launches()
+out["sources"] = int(plan.unit_work()[0])
+out["n_packed"] = int(d.arrays()["n_packed"])
+plan.close()
+ctx.close()
+""")
+    classes = [c for c, _ in res["launches"]]
+    assert 4 in classes and 5 in classes, res["launches"]
+    assert res["sources"] == res["n_packed"]
+
+
 def test_failed_plan_builds_release_everything(stub_dir):
     """A device allocation failing at any point of a plan build (PLAIN, and
     multi-source with per-source items) returns BCGPU_ENOMEM (3) and leaves
