@@ -782,8 +782,8 @@ int build_plan(bc_ctx *ctx, const bc_bccs *B, const std::vector<bcg::PlainItem> 
     if ((rc = dalloc(p, &p->ws_i, slots * bcg::kWsIntRows * p->ws_n)) ||
         (rc = dalloc(p, &p->ws_f, slots * bcg::kWsDblRows * p->ws_n)) || (rc = dalloc(p, &p->epochs, 2 * slots)))
       return bail(rc);
-    if (cudaMemsetAsync(p->ws_i, 0, sizeof(int32_t) * (size_t)(slots * bcg::kWsIntRows * p->ws_n), ctx->stream) !=
-        cudaSuccess)
+    if (cudaMemsetAsync(p->ws_f, 0, sizeof(double) * (size_t)(slots * bcg::kWsDblRows * p->ws_n), ctx->stream) !=
+        cudaSuccess)  // row records: stamp 0, unvisited
       return bail(cuda_fail(ctx, cudaGetLastError(), "cudaMemsetAsync"));
     std::vector<int32_t> ep((size_t)(2 * slots), 1);
     CK(ctx, cudaMemcpyAsync(p->epochs, ep.data(), sizeof(int32_t) * ep.size(), cudaMemcpyHostToDevice, ctx->stream));

@@ -69,33 +69,46 @@ struct Shared {
   int cq[kBlock];
 };
 
-// Per-CTA workspace rows (capacity ws_n each), addressed from two base
-// pointers so that the row pointers are recomputed where used instead of
-// being held in registers. lxA/lxB: the power-of-two exponent X of each level
-// of rows A/B (path count = stored value * 2^X); lxM: the same for the merged
-// row of a chain vertex.
+// A vertex's entry in a BFS row: its level stamp and its path count -- q
+// once the dependency sweep has passed the vertex (q(w) replaces sigma(w) in
+// place: nothing reads sigma(w) after w's own sweep step) -- so that one
+// 16-byte load gives a neighbour's level and value (one sector instead of one
+// in each of two rows).
+struct __align__(16) Rec {
+  int32_t d;
+  int32_t pad;
+  double v;
+};
+__device__ __forceinline__ Rec ld_rec(const Rec *p) {
+  const int4 x = __ldcg(reinterpret_cast<const int4 *>(p));
+  return Rec{x.x, 0, __hiloint2double(x.w, x.z)};
+}
+
+// Per-CTA workspace (capacity ws_n each), addressed from two base pointers so
+// that the row pointers are recomputed where used instead of being held in
+// registers. Records: A (own BFS), B (right endpoint BFS), M (merged chain
+// rows). Int rows: visit orders and level offsets of A and B, and the
+// power-of-two exponent X of each level of A, B and M (path count = stored
+// value * 2^X).
 struct Rows {
   int32_t *wi;
-  double *wf;
+  Rec *wr;
   int64_t n;
-  __device__ __forceinline__ int32_t *dA() const { return wi; }
-  __device__ __forceinline__ int32_t *SA() const { return wi + n; }
-  __device__ __forceinline__ int32_t *lvA() const { return wi + 2 * n; }
-  __device__ __forceinline__ int32_t *dB() const { return wi + 3 * n; }
-  __device__ __forceinline__ int32_t *SB() const { return wi + 4 * n; }
-  __device__ __forceinline__ int32_t *lvB() const { return wi + 5 * n; }
-  __device__ __forceinline__ int32_t *dM() const { return wi + 6 * n; }
-  __device__ __forceinline__ int32_t *lxA() const { return wi + 7 * n; }
-  __device__ __forceinline__ int32_t *lxB() const { return wi + 8 * n; }
-  __device__ __forceinline__ int32_t *lxM() const { return wi + 9 * n; }
-  __device__ __forceinline__ double *sA() const { return wf; }
-  __device__ __forceinline__ double *sB() const { return wf + n; }
-  __device__ __forceinline__ double *sM() const { return wf + 2 * n; }
-  __device__ __forceinline__ double *q() const { return wf + 3 * n; }
+  __device__ __forceinline__ int32_t *SA() const { return wi; }
+  __device__ __forceinline__ int32_t *lvA() const { return wi + n; }
+  __device__ __forceinline__ int32_t *SB() const { return wi + 2 * n; }
+  __device__ __forceinline__ int32_t *lvB() const { return wi + 3 * n; }
+  __device__ __forceinline__ int32_t *lxA() const { return wi + 4 * n; }
+  __device__ __forceinline__ int32_t *lxB() const { return wi + 5 * n; }
+  __device__ __forceinline__ int32_t *lxM() const { return wi + 6 * n; }
+  __device__ __forceinline__ Rec *A() const { return wr; }
+  __device__ __forceinline__ Rec *B() const { return wr + n; }
+  __device__ __forceinline__ Rec *M() const { return wr + 2 * n; }
 };
 
 __device__ __forceinline__ Rows rows_of(const PlainArgs &a, int64_t slot) {
-  return Rows{a.ws_i + slot * kWsIntRows * a.ws_n, a.ws_f + slot * kWsDblRows * a.ws_n, a.ws_n};
+  return Rows{a.ws_i + slot * kWsIntRows * a.ws_n,
+              reinterpret_cast<Rec *>(a.ws_f + slot * kWsDblRows * a.ws_n), a.ws_n};
 }
 
 // Appends x to S (warp-aggregated atomic on the shared tail).
@@ -111,44 +124,41 @@ __device__ __forceinline__ void append(SH &sh, int32_t *S, int32_t x) {
 // Forward step for one arc (w -> x) at level lev: accumulate sigma from a
 // predecessor, or claim an unvisited vertex for level lev+1.
 template <class SH>
-__device__ __forceinline__ void fwd_arc(SH &sh, int32_t *d, const double *sig, int32_t *S, int32_t x, int dprev,
-                                        int dnext, int base, double &acc) {
-  int dx = __ldcg(d + x);
-  if (dx == dprev) {
-    acc += sig[x];
-  } else if (dx < base) {
-    int old = atomicMax(d + x, dnext);
+__device__ __forceinline__ void fwd_arc(SH &sh, Rec *r, int32_t *S, int32_t x, int dprev, int dnext, int base,
+                                        double &acc) {
+  const Rec rx = ld_rec(r + x);
+  if (rx.d == dprev) {
+    acc += rx.v;
+  } else if (rx.d < base) {
+    int old = atomicMax(&r[x].d, dnext);
     if (old < base) append(sh, S, x);
   }
 }
 
 // Forward scan of a low-degree vertex by one thread, kGather arcs at a time:
-// the neighbour ids, then their levels, then the predecessors' path counts
+// the neighbour ids, then their records (level and path count in one load)
 // are each issued as independent loads (one memory round trip per group
 // instead of one per arc). Sums and claims follow arc order, so sigma is the
 // same value the arc-by-arc form computes.
 constexpr int kGather = 4;
 
 template <class SH>
-__device__ __forceinline__ double fwd_small(SH &sh, const int32_t *Ce, int deg, int32_t *d, const double *sig, int32_t *S,
-                                            int dprev, int dnext, int base) {
+__device__ __forceinline__ double fwd_small(SH &sh, const int32_t *Ce, int deg, Rec *r, int32_t *S, int dprev,
+                                            int dnext, int base) {
   double acc = 0.0;
   for (int g = 0; g < deg; g += kGather) {
     int32_t x[kGather];
-    int dx[kGather];
-    double s[kGather];
+    Rec rx[kGather];
 #pragma unroll
     for (int j = 0; j < kGather; ++j) x[j] = g + j < deg ? ldg(Ce + g + j) : -1;
 #pragma unroll
-    for (int j = 0; j < kGather; ++j) dx[j] = x[j] >= 0 ? __ldcg(d + x[j]) : INT_MAX;  // INT_MAX: skipped
-#pragma unroll
-    for (int j = 0; j < kGather; ++j) s[j] = dx[j] == dprev ? sig[x[j]] : 0.0;
+    for (int j = 0; j < kGather; ++j) rx[j] = x[j] >= 0 ? ld_rec(r + x[j]) : Rec{INT_MAX, 0, 0.0};  // INT_MAX: skipped
 #pragma unroll
     for (int j = 0; j < kGather; ++j) {
-      if (dx[j] == dprev) {
-        acc += s[j];
-      } else if (dx[j] < base) {
-        const int old = atomicMax(d + x[j], dnext);
+      if (rx[j].d == dprev) {
+        acc += rx[j].v;
+      } else if (rx[j].d < base) {
+        const int old = atomicMax(&r[x[j]].d, dnext);
         if (old < base) append(sh, S, x[j]);
       }
     }
@@ -174,17 +184,17 @@ __device__ __forceinline__ double block_sum(Shared<kBlock> &sh, double v) {
   return t;
 }
 
-// CTA-wide BFS from s over one BCC: fills d (epoch base), the scaled path
-// counts sig, the level order S, level offsets lv[0..nlev] and the level
-// exponents lx[0..nlev) (path count of a vertex on level l = sig * 2^lx[l]).
-// Returns nlev (number of levels).
+// CTA-wide BFS from s over one BCC: fills the records r (level stamps from
+// epoch base, scaled path counts), the level order S, level offsets
+// lv[0..nlev] and the level exponents lx[0..nlev) (path count of a vertex on
+// level l = sigma * 2^lx[l]). Returns nlev (number of levels).
 template <int kBlock>
-__device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, int32_t s, int32_t *d, double *sig,
-                       int32_t *S, int32_t *lv, int32_t *lx, int base, int rescale_exp, int *err) {
+__device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, int32_t s, Rec *r, int32_t *S,
+                       int32_t *lv, int32_t *lx, int base, int rescale_exp, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
-    d[s] = base;
+    r[s].d = base;
     S[0] = s;
     lv[0] = 0;
     lv[1] = 1;
@@ -208,9 +218,9 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         const int64_t e0 = R[w], e1 = R[w + 1];
         const int64_t deg = e1 - e0;
         if (deg <= kSmallDeg) {
-          const double acc = fwd_small(sh, C + e0, (int)deg, d, sig, S, dprev, dnext, base);
+          const double acc = fwd_small(sh, C + e0, (int)deg, r, S, dprev, dnext, base);
           const double v = lev == 0 ? 1.0 : acc;
-          sig[w] = v;
+          r[w].v = v;
           emax = max(emax, exp_bits(v));
         } else if (deg <= kWarpDeg) {
           sh.wq[atomicAdd(&sh.nwq, 1)] = w;
@@ -223,11 +233,11 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         const int32_t w = sh.wq[k];
         const int64_t e0 = R[w], e1 = R[w + 1];
         double acc = 0.0;
-        for (int64_t e = e0 + lane; e < e1; e += 32) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+        for (int64_t e = e0 + lane; e < e1; e += 32) fwd_arc(sh, r, S, ldg(C + e), dprev, dnext, base, acc);
         acc = warp_sum(acc);
         if (lane == 0) {
           const double v = lev == 0 ? 1.0 : acc;
-          sig[w] = v;
+          r[w].v = v;
           emax = max(emax, exp_bits(v));
         }
       }
@@ -236,11 +246,11 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
         const int32_t w = sh.cq[k];
         const int64_t e0 = R[w], e1 = R[w + 1];
         double acc = 0.0;
-        for (int64_t e = e0 + tid; e < e1; e += kBlock) fwd_arc(sh, d, sig, S, ldg(C + e), dprev, dnext, base, acc);
+        for (int64_t e = e0 + tid; e < e1; e += kBlock) fwd_arc(sh, r, S, ldg(C + e), dprev, dnext, base, acc);
         acc = block_sum(sh, acc);
         if (tid == 0) {
           const double v = lev == 0 ? 1.0 : acc;
-          sig[w] = v;
+          r[w].v = v;
           emax = max(emax, exp_bits(v));
         }
       }
@@ -259,9 +269,9 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
       bool lost = false;
       for (int i = f0 + tid; i < f1; i += kBlock) {
         const int32_t w = S[i];
-        const double v = scale2(sig[w], -k);
+        const double v = scale2(r[w].v, -k);
         lost |= exp_bits(v) == 0;  // a count of this level fell out of the normal range
-        sig[w] = v;
+        r[w].v = v;
       }
       if (lost) set_err(err, kDevOverflow);
     }
@@ -282,26 +292,23 @@ __device__ int cta_bfs(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, i
 
 // Dependency of w at level lev of a row (d stamped as base + level):
 // delta(w) = sigma(w) * sum over successors x of q(x); then q(w) and BC.
-// (one thread; ids, levels and successor values gathered kGather at a time,
+// (one thread; ids, then the successors' records gathered kGather at a time,
 // summed in arc order as in fwd_small)
-__device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_t *C, const int32_t *d, const double *q,
-                                                  int32_t w, int dsucc) {
+__device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_t *C, const Rec *r, int32_t w,
+                                                  int dsucc) {
   double acc = 0.0;
   const int64_t e0 = R[w];
   const int deg = (int)(R[w + 1] - e0);
   for (int g = 0; g < deg; g += kGather) {
     int32_t x[kGather];
-    bool hit[kGather];
-    double v[kGather];
+    Rec rx[kGather];
 #pragma unroll
     for (int j = 0; j < kGather; ++j) x[j] = g + j < deg ? ldg(C + e0 + g + j) : -1;
 #pragma unroll
-    for (int j = 0; j < kGather; ++j) hit[j] = x[j] >= 0 && d[x[j]] == dsucc;
-#pragma unroll
-    for (int j = 0; j < kGather; ++j) v[j] = hit[j] ? q[x[j]] : 0.0;
+    for (int j = 0; j < kGather; ++j) rx[j] = x[j] >= 0 ? ld_rec(r + x[j]) : Rec{INT_MIN, 0, 0.0};
 #pragma unroll
     for (int j = 0; j < kGather; ++j)
-      if (hit[j]) acc += v[j];
+      if (rx[j].d == dsucc) acc += rx[j].v;
   }
   return acc;
 }
@@ -309,13 +316,13 @@ __device__ __forceinline__ double bwd_arcs_thread(const int64_t *R, const int32_
 // Successor sums arrive in the scale of the next level: 2^sdiff =
 // 2^(X(level) - X(level+1)) brings them to this level's, so that
 // delta = sig * sum is the unscaled dependency and q = (reach+1+delta)/sig is
-// in this level's scale.
-__device__ __forceinline__ void finish_vertex(int32_t w, double acc, int sdiff, const int32_t *rch, const double *sig,
-                                              double *q, unsigned long long *accb, double wsrc, int *err) {
-  const double sw = sig[w];
+// in this level's scale (stored over sigma).
+__device__ __forceinline__ void finish_vertex(int32_t w, double acc, int sdiff, const int32_t *rch, Rec *r,
+                                              unsigned long long *accb, double wsrc, int *err) {
+  const double sw = r[w].v;
   const double delta = sw * scale2(acc, sdiff);
   const double qw = ((double)rch[w] + 1.0 + delta) / sw;
-  q[w] = qw;
+  r[w].v = qw;
   if (exp_bits(qw) == 0x7ff || exp_bits(delta) == 0x7ff) set_err(err, kDevOverflow);
   if (delta != 0.0) acc_add(accb + (int64_t)kAccDigits * w, delta * wsrc, err);
 }
@@ -331,25 +338,25 @@ struct LevelList {
 // mode 1: merged row: keep w iff dM(w) == lev, with duplicates removed
 //         (tie vertices listed in both buckets are taken from the primary one).
 struct MergeFilter {
-  const int32_t *dA; int baseA; int ld;
-  const int32_t *dB; int baseB; int rd;
+  const Rec *A; int baseA; int ld;
+  const Rec *B; int baseB; int rd;
 };
 
-__device__ __forceinline__ bool keep_vertex(int mode, int list, int32_t w, int lev, const int32_t *dM,
+__device__ __forceinline__ bool keep_vertex(int mode, int list, int32_t w, int lev, const Rec *rM,
                                             const MergeFilter &mf) {
   if (mode == 0) return true;
-  if (dM[w] != lev) return false;
+  if (rM[w].d != lev) return false;
   if (list == 0) return true;
-  const bool inA = (mf.dA[w] - mf.baseA) + mf.ld == lev;
+  const bool inA = (mf.A[w].d - mf.baseA) + mf.ld == lev;
   if (list == 1) return !inA;
-  const bool inB = (mf.dB[w] - mf.baseB) + mf.rd == lev;
+  const bool inB = (mf.B[w].d - mf.baseB) + mf.rd == lev;
   return !inA && !inB;
 }
 
 template <int kBlock>
-__device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, const int32_t *d, const double *sig,
-                              double *q, const int32_t *rch, unsigned long long *accb, double wsrc, int dsucc, int lev,
-                              int sdiff, int mode, const LevelList &L, const MergeFilter &mf, int *err) {
+__device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_t *C, Rec *r, const int32_t *rch,
+                              unsigned long long *accb, double wsrc, int dsucc, int lev, int sdiff, int mode,
+                              const LevelList &L, const MergeFilter &mf, int *err) {
   constexpr int kWarps = kBlock / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int list = 0; list < 3; ++list) {
@@ -363,10 +370,10 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
       const int i = c0 + tid;
       if (i < b) {
         int32_t w = list < 2 ? S[i] : (i == 0 && L.ck0 >= 0 ? L.ck0 : L.ck1);
-        if (keep_vertex(mode, list, w, lev, d, mf)) {
+        if (keep_vertex(mode, list, w, lev, r, mf)) {
           const int64_t deg = R[w + 1] - R[w];
           if (deg <= kSmallDeg) {
-            finish_vertex(w, bwd_arcs_thread(R, C, d, q, w, dsucc), sdiff, rch, sig, q, accb, wsrc, err);
+            finish_vertex(w, bwd_arcs_thread(R, C, r, w, dsucc), sdiff, rch, r, accb, wsrc, err);
           } else if (deg <= kWarpDeg) {
             sh.wq[atomicAdd(&sh.nwq, 1)] = w;
           } else {
@@ -379,22 +386,22 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
         const int32_t w = sh.wq[k];
         double acc = 0.0;
         for (int64_t e = R[w] + lane; e < R[w + 1]; e += 32) {
-          int32_t x = ldg(C + e);
-          if (d[x] == dsucc) acc += q[x];
+          const Rec rx = ld_rec(r + ldg(C + e));
+          if (rx.d == dsucc) acc += rx.v;
         }
         acc = warp_sum(acc);
-        if (lane == 0) finish_vertex(w, acc, sdiff, rch, sig, q, accb, wsrc, err);
+        if (lane == 0) finish_vertex(w, acc, sdiff, rch, r, accb, wsrc, err);
       }
       const int ncq = sh.ncq;
       for (int k = 0; k < ncq; ++k) {
         const int32_t w = sh.cq[k];
         double acc = 0.0;
         for (int64_t e = R[w] + tid; e < R[w + 1]; e += kBlock) {
-          int32_t x = ldg(C + e);
-          if (d[x] == dsucc) acc += q[x];
+          const Rec rx = ld_rec(r + ldg(C + e));
+          if (rx.d == dsucc) acc += rx.v;
         }
         acc = block_sum(sh, acc);
-        if (tid == 0) finish_vertex(w, acc, sdiff, rch, sig, q, accb, wsrc, err);
+        if (tid == 0) finish_vertex(w, acc, sdiff, rch, r, accb, wsrc, err);
       }
       __syncthreads();
     }
@@ -403,9 +410,9 @@ __device__ void cta_bwd_level(Shared<kBlock> &sh, const int64_t *R, const int32_
 
 // Keeps epochs below 2^30: wraps the whole row (every BCC this CTA may see)
 // back to all-unvisited when the next BFS could overflow.
-__device__ void ensure_epoch(int32_t *d, int64_t cap, int &base, int span) {
+__device__ void ensure_epoch(Rec *r, int64_t cap, int &base, int span) {
   if (base + span + 2 < (1 << 30)) return;
-  for (int64_t k = threadIdx.x; k < cap; k += blockDim.x) d[k] = 0;
+  for (int64_t k = threadIdx.x; k < cap; k += blockDim.x) r[k].d = 0;
   __syncthreads();
   base = 1;
 }
@@ -437,7 +444,8 @@ __device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int base
   int mx = 0;
   bool bad = false;
   for (int k = threadIdx.x; k < nb; k += kBlock) {
-    const int la = __ldcg(r.dA() + k) - baseA, lb = __ldcg(r.dB() + k) - baseB;
+    const Rec ra = ld_rec(r.A() + k), rb = ld_rec(r.B() + k);
+    const int la = ra.d - baseA, lb = rb.d - baseB;
     if ((la < 0) | (lb < 0) | (la >= xm.nlevA) | (lb >= xm.nlevB)) {
       bad = true;
       continue;
@@ -445,15 +453,15 @@ __device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int base
     const int a = la + ld, b = lb + rd;
     int dm;
     double sm;
-    if (a < b) { dm = a; sm = scale2(r.sA()[k], xm.lxA[la] - xm(a)); }
-    else if (a > b) { dm = b; sm = scale2(r.sB()[k], xm.lxB[lb] - xm(b)); }
+    if (a < b) { dm = a; sm = scale2(ra.v, xm.lxA[la] - xm(a)); }
+    else if (a > b) { dm = b; sm = scale2(rb.v, xm.lxB[lb] - xm(b)); }
     else {
       dm = b;
       const int x = xm(b);
-      sm = scale2(r.sA()[k], xm.lxA[la] - x) + scale2(r.sB()[k], xm.lxB[lb] - x);
+      sm = scale2(ra.v, xm.lxA[la] - x) + scale2(rb.v, xm.lxB[lb] - x);
     }
-    r.dM()[k] = dm;
-    r.sM()[k] = sm;
+    r.M()[k].d = dm;
+    r.M()[k].v = sm;
     mx = max(mx, dm);
   }
   if (bad) set_err(err, kDevDisconnected);
@@ -468,8 +476,9 @@ __device__ int merge_rows(Shared<kBlock> &sh, const Rows &r, int baseA, int base
       const int k = start + j;
       const int dist = j > pos ? j - pos : pos - j;
       const double one = scale2(1.0, -xm(dist));  // one path, in the merged level's scale
-      if (r.dM()[k] > dist) { r.dM()[k] = dist; r.sM()[k] = one; }
-      else if (r.dM()[k] == dist) r.sM()[k] += one;
+      Rec &m = r.M()[k];
+      if (m.d > dist) { m.d = dist; m.v = one; }
+      else if (m.d == dist) m.v += one;
     }
   }
   for (int l = threadIdx.x; l <= maxlev; l += kBlock) r.lxM()[l] = xm(l);
@@ -488,16 +497,11 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
   unsigned long long *accb = a.acc + (int64_t)kAccDigits * vo;
   const MergeFilter none{nullptr, 0, 0, nullptr, 0, 0};
 
-  // own source: BFS into row A, then its dependency sweep
+  // own source: BFS into row A (its dependency sweep comes after the chains:
+  // their merged rows read row A's path counts, which the sweep replaces by q)
   int baseA = sh.base_a;
-  ensure_epoch(r.dA(), a.ws_n, baseA, nb);
-  const int nlevA = cta_bfs(sh, R, a.col, it.src, r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), baseA, a.rescale_exp, a.err);
-  const double wsrc = (double)rch[it.src] + 1.0;
-  for (int lev = it.own ? nlevA - 1 : 0; lev >= 1; --lev) {
-    LevelList L{r.SA(), r.lvA()[lev], r.lvA()[lev + 1], nullptr, 0, 0, -1, -1};
-    const int sdiff = lev + 1 < nlevA ? r.lxA()[lev] - r.lxA()[lev + 1] : 0;  // the deepest level has no successors
-    cta_bwd_level(sh, R, a.col, r.dA(), r.sA(), r.q(), rch, accb, wsrc, baseA + lev + 1, lev, sdiff, 0, L, none, a.err);
-  }
+  ensure_epoch(r.A(), a.ws_n, baseA, nb);
+  const int nlevA = cta_bfs(sh, R, a.col, it.src, r.A(), r.SA(), r.lvA(), r.lxA(), baseA, a.rescale_exp, a.err);
 
   int baseB = sh.base_b, nlevB = 0, prevR = -1;
   for (int32_t c = it.c0; c < it.c1; ++c) {
@@ -505,8 +509,8 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
     if (a.chain_l[c] != it.src || start < 0 || start + len > nb) { set_err(a.err, kDevBadItem); break; }
     if (cr != prevR) {
       if (prevR >= 0) baseB += nlevB + 1;
-      ensure_epoch(r.dB(), a.ws_n, baseB, nb);
-      nlevB = cta_bfs(sh, R, a.col, cr, r.dB(), r.sB(), r.SB(), r.lvB(), r.lxB(), baseB, a.rescale_exp, a.err);
+      ensure_epoch(r.B(), a.ws_n, baseB, nb);
+      nlevB = cta_bfs(sh, R, a.col, cr, r.B(), r.SB(), r.lvB(), r.lxB(), baseB, a.rescale_exp, a.err);
       prevR = cr;
     }
     for (int32_t pos = 0; pos < len; ++pos) {
@@ -515,7 +519,7 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
       const MergedExp xm{r.lxA(), r.lxB(), nlevA, nlevB, ld, rd};
       const int maxlev = merge_rows(sh, r, baseA, baseB, nb, start, len, pos, xm, a.err);
       const double wz = (double)rch[z] + 1.0;
-      const MergeFilter mf{r.dA(), baseA, ld, r.dB(), baseB, rd};
+      const MergeFilter mf{r.A(), baseA, ld, r.B(), baseB, rd};
       for (int lev = maxlev; lev >= 1; --lev) {
         LevelList L{r.SA(), 0, 0, r.SB(), 0, 0, -1, -1};
         const int la = lev - ld, lb = lev - rd;
@@ -524,11 +528,18 @@ __device__ void process_item(Shared<kBlock> &sh, const PlainArgs &a, const Rows 
         if (pos - lev >= 0) L.ck0 = start + pos - lev;
         if (pos + lev < len) L.ck1 = start + pos + lev;
         const int sdiff = lev < maxlev ? r.lxM()[lev] - r.lxM()[lev + 1] : 0;
-        cta_bwd_level(sh, R, a.col, r.dM(), r.sM(), r.q(), rch, accb, wz, lev + 1, lev, sdiff, 1, L, mf, a.err);
+        cta_bwd_level(sh, R, a.col, r.M(), rch, accb, wz, lev + 1, lev, sdiff, 1, L, mf, a.err);
       }
     }
   }
   if (prevR >= 0) baseB += nlevB + 1;
+
+  const double wsrc = (double)rch[it.src] + 1.0;
+  for (int lev = it.own ? nlevA - 1 : 0; lev >= 1; --lev) {
+    LevelList L{r.SA(), r.lvA()[lev], r.lvA()[lev + 1], nullptr, 0, 0, -1, -1};
+    const int sdiff = lev + 1 < nlevA ? r.lxA()[lev] - r.lxA()[lev + 1] : 0;  // the deepest level has no successors
+    cta_bwd_level(sh, R, a.col, r.A(), rch, accb, wsrc, baseA + lev + 1, lev, sdiff, 0, L, none, a.err);
+  }
   if (threadIdx.x == 0) {
     sh.base_a = baseA + nlevA + 1;
     sh.base_b = baseB;
@@ -572,22 +583,26 @@ __global__ void __launch_bounds__(kBlock, 1) rows_kernel(PlainArgs a, int32_t bc
   const int32_t nb = (int32_t)(a.vtx_off[bcc + 1] - vo);
   if ((int64_t)nb + 2 > a.ws_n) { set_err(a.err, kDevWorkspace); return; }
   const int64_t *R = a.row + vo;
-  for (int k = threadIdx.x; k < nb; k += kBlock) { r.dA()[k] = 0; r.dB()[k] = 0; }
+  for (int k = threadIdx.x; k < nb; k += kBlock) { r.A()[k].d = 0; r.B()[k].d = 0; }
   __syncthreads();
   if (chain < 0) {
-    cta_bfs(sh, R, a.col, src, r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
+    cta_bfs(sh, R, a.col, src, r.A(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
     for (int k = threadIdx.x; k < nb; k += kBlock) {
-      const int l = r.dA()[k] - 1;
+      const int l = r.A()[k].d - 1;
       d_out[k] = l;
-      s_out[k] = l >= 0 ? scale2(r.sA()[k], r.lxA()[l]) : 0.0;
+      s_out[k] = l >= 0 ? scale2(r.A()[k].v, r.lxA()[l]) : 0.0;
     }
   } else {
     const int32_t start = a.chain_start[chain], len = a.chain_len[chain], pos = src - start;
-    const int nlevA = cta_bfs(sh, R, a.col, a.chain_l[chain], r.dA(), r.sA(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
-    const int nlevB = cta_bfs(sh, R, a.col, a.chain_r[chain], r.dB(), r.sB(), r.SB(), r.lvB(), r.lxB(), 1, a.rescale_exp, a.err);
+    const int nlevA = cta_bfs(sh, R, a.col, a.chain_l[chain], r.A(), r.SA(), r.lvA(), r.lxA(), 1, a.rescale_exp, a.err);
+    const int nlevB = cta_bfs(sh, R, a.col, a.chain_r[chain], r.B(), r.SB(), r.lvB(), r.lxB(), 1, a.rescale_exp, a.err);
     const MergedExp xm{r.lxA(), r.lxB(), nlevA, nlevB, pos + 1, len - pos};
     merge_rows(sh, r, 1, 1, nb, start, len, pos, xm, a.err);
-    for (int k = threadIdx.x; k < nb; k += kBlock) { d_out[k] = r.dM()[k]; s_out[k] = scale2(r.sM()[k], xm(r.dM()[k])); }
+    for (int k = threadIdx.x; k < nb; k += kBlock) {
+      const Rec m = r.M()[k];
+      d_out[k] = m.d;
+      s_out[k] = scale2(m.v, xm(m.d));
+    }
   }
 }
 

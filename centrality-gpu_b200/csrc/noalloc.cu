@@ -35,7 +35,8 @@ constexpr int64_t kOffAcc = kOffItems + kBytesItems;  // fixed-point BC counters
 constexpr int64_t kBytesAcc = align256(kMaxVertices * kAccDigits * 8);
 constexpr int64_t kOffCtl = kOffAcc + kBytesAcc;  // vtx_off[2], counter, epochs[2*kSlots], err
 constexpr int64_t kBytesCtl = align256(16 + 8 + 8 * kSlots + 4);
-constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // 19,860,224 bytes (about 19 MiB)
+constexpr int64_t kScratchBytes = kOffCtl + kBytesCtl;  // 20,909,056 bytes (about 20 MiB)
+static_assert(kScratchBytes == 20909056, "the size the header documents");
 static_assert(kMaxVertices <= kAccMaxAdds, "one call's sources must fit the fixed-point counters' headroom");
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -155,7 +156,7 @@ extern "C" int bc_begin_free_noalloc(bc_ctx *ctx, const int32_t *R, const int32_
   // the previous call's error flag is still in the array: clear it (and, on a
   // device's first call or after a failed one, the rows and the counters)
   cudaError_t e = cudaMemsetAsync(L.err, 0, sizeof(int), stream);
-  if (e == cudaSuccess && first) e = cudaMemsetAsync(L.ws_i, 0, (size_t)kBytesWsI, stream);
+  if (e == cudaSuccess && first) e = cudaMemsetAsync(L.ws_f, 0, (size_t)kBytesWsF, stream);  // row records: unvisited
   if (e == cudaSuccess && first) e = cudaMemsetAsync(L.acc, 0, (size_t)kBytesAcc, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(bc, 0, sizeof(double) * (size_t)n, stream);
   if (e == cudaSuccess) {

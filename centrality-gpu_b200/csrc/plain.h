@@ -40,7 +40,7 @@ struct PlainArgs {
   unsigned long long *next_item;  // zeroed before each launch
   unsigned long long *acc;        // [n_packed][kAccDigits] fixed-point BC counters
   int32_t *ws_i;                  // kWsIntRows int rows per workspace slot
-  double *ws_f;                   // kWsDblRows double rows per workspace slot
+  double *ws_f;                   // kWsDblRows double rows per workspace slot (16-byte records, 16-byte aligned)
   int64_t ws_n;                   // row capacity (>= largest BCC + 2)
   int32_t *epochs;                // 2 per slot: level-stamp bases of rows A and B
   int64_t rows_slot;              // workspace slot reserved for launch_rows
@@ -48,11 +48,13 @@ struct PlainArgs {
   int *err;
 };
 
-// Workspace rows per slot: levels, visit order, level offsets and level
-// exponents of rows A and B, merged levels and level exponents (int); path
-// counts A, B, merged and q (double).
-constexpr int kWsIntRows = 10;
-constexpr int kWsDblRows = 4;
+// Workspace per slot: visit orders, level offsets and level exponents of
+// rows A and B and the merged row's level exponents (int rows); the records
+// (level stamp, path count then q) of rows A, B and merged, 16 bytes per
+// vertex each (as double rows: two per record row). The records start zeroed
+// (stamp 0: unvisited).
+constexpr int kWsIntRows = 7;
+constexpr int kWsDblRows = 6;
 
 // block: 64 ... 1024 threads (1024 / block CTAs fit an SM).
 cudaError_t launch_plain(const PlainArgs &a, int block, int grid, cudaStream_t stream);

@@ -175,7 +175,7 @@ int bc_begin_free(bc_ctx *ctx, const int32_t *R, const int32_t *C, int32_t n, in
  * accounting or stall the device. Inputs and the output are the CALLER's
  * DEVICE buffers: R[n+1], C[m] (m = arcs), req_nodes[n_req], reach[n], and
  * bc[n] (FP64, overwritten). All other working memory is one file-scope
- * __device__ array of about 19 MiB that every GPU loading this library holds
+ * __device__ array of about 20 MiB that every GPU loading this library holds
  * until the process exits. Limits: n <= 16384 and n_req <= 16384
  * (BCGPU_EOVERFLOW beyond, with the reason in bc_last_error).
  * The first call on a device looks up that array's device address
