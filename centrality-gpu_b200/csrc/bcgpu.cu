@@ -531,17 +531,28 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, c
     if (T.cls == bcg::kTileWarp) p->tcap = nmax + 2;
     p->tl.push_back(T);
   }
-  // slices: local row offsets (int32), neighbours (uint16), 16-byte aligned parts
+  // slices: local row offsets (uint16 when narrow, else int32), neighbours
+  // (uint16), 16-byte aligned parts; bit 0 of a narrow slice's offset set
   std::vector<unsigned char> blob((size_t)std::max<int64_t>(total, 16), 0);
 #pragma omp parallel for schedule(dynamic, 16)
   for (int32_t b = 0; b < B->n_bcc; ++b) {
     if (cls[b] < 0) continue;
     const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo, e0 = B->row[vo];
     const int64_t arcs = B->row[vo + nb] - e0;
-    int32_t *R = reinterpret_cast<int32_t *>(blob.data() + off[b]);
-    uint16_t *C = reinterpret_cast<uint16_t *>(blob.data() + off[b] + bcg::TileSlice::col_at(nb));
-    for (int64_t v = 0; v <= nb; ++v) R[v] = (int32_t)(B->row[vo + v] - e0);
+    const bool narrow = bcg::TileSlice::narrow(arcs);
+    unsigned char *base = blob.data() + off[b];
+    uint16_t *C = reinterpret_cast<uint16_t *>(base + bcg::TileSlice::col_at(nb, narrow));
+    for (int64_t v = 0; v <= nb; ++v) {
+      if (narrow) reinterpret_cast<uint16_t *>(base)[v] = (uint16_t)(B->row[vo + v] - e0);
+      else reinterpret_cast<int32_t *>(base)[v] = (int32_t)(B->row[vo + v] - e0);
+    }
     for (int64_t e = 0; e < arcs; ++e) C[e] = (uint16_t)B->col[e0 + e];
+  }
+  std::vector<int64_t> off_flag(off);  // what the kernels read: offset | narrow
+  for (int32_t b = 0; b < B->n_bcc; ++b) {
+    if (cls[b] < 0) continue;
+    const int64_t vo = B->vtx_off[b], nb = B->vtx_off[b + 1] - vo;
+    if (bcg::TileSlice::narrow(B->row[vo + nb] - B->row[vo])) off_flag[b] |= 1;
   }
   p->n_titems = (int64_t)p->h_titems.size();
   int warp_grid = 1;
@@ -551,7 +562,8 @@ int build_tiles(bc_ctx *ctx, const bc_bccs *B, const std::vector<int8_t> &cls, c
   }
   const int64_t slots = (int64_t)warp_grid * bcg::kTileWarps;
   p->tcap = std::max<int64_t>(p->tcap, 2);
-  if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) || (rc = upload(p, &p->slice_off, off.data(), B->n_bcc)) ||
+  if ((rc = upload(p, &p->slices, blob.data(), (int64_t)blob.size())) ||
+      (rc = upload(p, &p->slice_off, off_flag.data(), B->n_bcc)) ||
       (rc = upload(p, &p->slice_bytes, size.data(), B->n_bcc)) ||
       (rc = upload(p, &p->titems, p->h_titems.data(), p->n_titems)) || (rc = dalloc(p, &p->tws_lv, slots * p->tcap)) ||
       (rc = dalloc(p, &p->tws_P, p_rows * std::max<int64_t>(p->tcap_P, 1))) ||

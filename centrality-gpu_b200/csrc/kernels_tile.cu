@@ -136,12 +136,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
   return true;
 }
 
-// One BCC as the kernels read it: local row offsets and neighbours (shared
-// memory), reach (global).
+// One BCC as the kernels read it: local row offsets (uint16 or int32) and
+// neighbours (shared memory), reach (global).
 struct View {
-  const int32_t *R;
+  const int32_t *R32;
+  const uint16_t *R16;  // set for a narrow slice
   const uint16_t *C;
   const int32_t *rch;
+  __device__ __forceinline__ int row(int32_t w) const { return R16 ? (int)R16[w] : R32[w]; }
 };
 
 // Pulls the next item for the CTA (thread 0) and stages its BCC's slice if
@@ -160,8 +162,8 @@ __device__ bool next_item(const TileArgs &a, Ctl &ctl, unsigned char *slice, uns
   it = a.items[a.item_begin + ctl.item];
   vo = a.vtx_off[it.bcc];
   nb = (int32_t)(a.vtx_off[it.bcc + 1] - vo);
-  const int64_t soff = a.slice_off[it.bcc];
-  if (nb > a.nmax || soff < 0 || it.s0 < 0 || it.s1 > nb) {  // uniform over the CTA
+  const int64_t soff = a.slice_off[it.bcc] & ~int64_t(15);
+  if (nb > a.nmax || a.slice_off[it.bcc] < 0 || it.s0 < 0 || it.s1 > nb) {  // uniform over the CTA
     if (tid == 0) set_err(a.err, kDevBadItem);
     return false;
   }
@@ -183,9 +185,11 @@ __device__ bool next_item(const TileArgs &a, Ctl &ctl, unsigned char *slice, uns
   return true;
 }
 
-__device__ __forceinline__ View view_of(const TileArgs &a, const unsigned char *slice, int32_t nb, int64_t vo) {
-  const int32_t *R = reinterpret_cast<const int32_t *>(slice);
-  return View{R, reinterpret_cast<const uint16_t *>(slice + TileSlice::col_at(nb)), a.reach + vo};
+__device__ __forceinline__ View view_of(const TileArgs &a, const unsigned char *slice, int32_t nb, int64_t vo,
+                                        int32_t bcc) {
+  const bool narrow = (a.slice_off[bcc] & 1) != 0;
+  return View{reinterpret_cast<const int32_t *>(slice), narrow ? reinterpret_cast<const uint16_t *>(slice) : nullptr,
+              reinterpret_cast<const uint16_t *>(slice + TileSlice::col_at(nb, narrow)), a.reach + vo};
 }
 
 // Appends x to the visit order S: one atomic per group of lanes appending at
@@ -311,8 +315,8 @@ __device__ int warp_bfs(const View &g, int32_t nb, int32_t s, int32_t *d, double
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < f1) {
         w = S[i];
-        e0 = g.R[w];
-        e1 = g.R[w + 1];
+        e0 = g.row(w);
+        e1 = g.row(w + 1);
       }
       const bool big = e1 - e0 > kLaneDeg;
       if (w >= 0 && !big) {
@@ -350,8 +354,8 @@ __device__ void warp_sweep(const View &g, int nlev, const int32_t *d, double *sq
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < a1) {
         w = S[i];
-        e0 = g.R[w];
-        e1 = g.R[w + 1];
+        e0 = g.row(w);
+        e1 = g.row(w + 1);
       }
       const bool big = e1 - e0 > kLaneDeg;
       double sum = 0.0;
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(kThreads, 1) tile_warp_kernel(TileArgs a) {
     for (int64_t k = tid; k < (int64_t)kAccDigits * nb; k += kThreads) cnt[k] = 0ull;
     __syncthreads();
     if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
-    const View g = view_of(a, slice, nb, vo);
+    const View g = view_of(a, slice, nb, vo, it.bcc);
     while (true) {  // the warps take the item's sources one at a time
       int k = 0;
       if (lane == 0) k = atomicAdd(&ctl.next, 1);
@@ -461,8 +465,8 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < f1) {
         w = S[i];
-        e0 = g.R[w];
-        e1 = g.R[w + 1];
+        e0 = g.row(w);
+        e1 = g.row(w + 1);
       }
       const bool big = e1 - e0 > kLaneDeg;
       if (w >= 0 && !big) {
@@ -480,7 +484,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
         const int j = __ffs(over) - 1;
         over &= over - 1;
         const int32_t wj = __shfl_sync(0xffffffffu, w, j);
-        const double acc = pull_row_warp(g, g.R[wj], g.R[wj + 1], d, sq, S + f1, tail, dprev, dnext, lane);
+        const double acc = pull_row_warp(g, g.row(wj), g.row(wj + 1), d, sq, S + f1, tail, dprev, dnext, lane);
         if (lane == 0 && lev > 0) sq[wj] = acc;
       }
     }
@@ -488,7 +492,7 @@ __device__ int cta_bfs(const View &g, int32_t nb, int32_t s, int16_t *d, double 
     const int nlong = min(*(volatile int *)nql, L::kQueue);
     for (int k = warp; k < nlong; k += kWarps) {
       const int32_t w = q[k];
-      const double acc = pull_row_warp(g, g.R[w], g.R[w + 1], d, sq, S + f1, tail, dprev, dnext, lane);
+      const double acc = pull_row_warp(g, g.row(w), g.row(w + 1), d, sq, S + f1, tail, dprev, dnext, lane);
       if (lane == 0 && lev > 0) sq[w] = acc;
     }
     L::sync(grp);
@@ -529,8 +533,8 @@ __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq,
       int32_t w = -1, e0 = 0, e1 = 0;
       if (i < a1) {
         w = S[i];
-        e0 = g.R[w];
-        e1 = g.R[w + 1];
+        e0 = g.row(w);
+        e1 = g.row(w + 1);
       }
       const bool big = e1 - e0 > kLaneDeg;
       if (w >= 0 && !big) P[w] += finish(g, w, push_row(g, e0, e1, d, sq, dsucc), sq, err) * wsrc;
@@ -545,7 +549,7 @@ __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq,
         const int j = __ffs(over) - 1;
         over &= over - 1;
         const int32_t wj = __shfl_sync(0xffffffffu, w, j);
-        const double sum = push_row_warp(g, g.R[wj], g.R[wj + 1], d, sq, dsucc, lane);
+        const double sum = push_row_warp(g, g.row(wj), g.row(wj + 1), d, sq, dsucc, lane);
         if (lane == 0) P[wj] += finish(g, wj, sum, sq, err) * wsrc;
       }
     }
@@ -553,7 +557,7 @@ __device__ void cta_sweep(const View &g, int nlev, const int16_t *d, double *sq,
     const int nlong = min(*(volatile int *)nql, L::kQueue);
     for (int k = warp; k < nlong; k += kWarps) {
       const int32_t w = q[k];
-      const double sum = push_row_warp(g, g.R[w], g.R[w + 1], d, sq, dsucc, lane);
+      const double sum = push_row_warp(g, g.row(w), g.row(w + 1), d, sq, dsucc, lane);
       if (lane == 0) P[w] += finish(g, w, sum, sq, err) * wsrc;
     }
     L::sync(grp);
@@ -595,7 +599,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) tile_cta_kernel(TileArg
     for (int v = gtid; v < nb; v += kGroup) P[v] = 0.0;
     __syncthreads();
     if (tid == 0) ctl.bcc = it.bcc;  // read again only after the next barrier
-    const View g = view_of(a, slice, nb, vo);
+    const View g = view_of(a, slice, nb, vo, it.bcc);
     for (int32_t s = it.s0 + grp; s < it.s1; s += L::kG) {  // the group's sources in order: P's sums are fixed
       const int nlev = cta_bfs<kBlock, kGroup>(g, nb, s, d, sq, S, lv, q, cnt, nq, a.err, grp, gtid);
       if (nlev < 0) break;

@@ -34,18 +34,25 @@ constexpr int kGroupLongQueue = 256;      // long-row queue of a group in the gr
 constexpr int32_t kTileMaxVertices = 65535;  // neighbour ids are 16-bit in the slice
 
 // Byte layout of one BCC's staged slice, each part starting on a 16-byte
-// boundary: local row offsets int32 [n+1], neighbours uint16 [arcs].
+// boundary: local row offsets [n+1] -- uint16 when the BCC has fewer than
+// 2^16 arcs ("narrow", 2 bytes per vertex less in shared memory), else
+// int32 -- then neighbours uint16 [arcs]. A slice's offset in the slice
+// buffer is a multiple of 16; bit 0 of the offset recorded for the kernels
+// (TileArgs::slice_off) marks a narrow slice.
 struct TileSlice {
   __host__ __device__ static int64_t pad16(int64_t bytes) { return (bytes + 15) / 16 * 16; }
-  __host__ __device__ static int64_t col_at(int64_t n) { return pad16(4 * (n + 1)); }
-  __host__ __device__ static int64_t bytes(int64_t n, int64_t arcs) { return col_at(n) + pad16(2 * arcs); }
+  __host__ __device__ static bool narrow(int64_t arcs) { return arcs < 65536; }
+  __host__ __device__ static int64_t col_at(int64_t n, bool narrow) { return pad16((narrow ? 2 : 4) * (n + 1)); }
+  __host__ __device__ static int64_t bytes(int64_t n, int64_t arcs) {
+    return col_at(n, narrow(arcs)) + pad16(2 * arcs);
+  }
 };
 
 struct TileArgs {
   const int64_t *vtx_off;        // [n_bcc+1]
   const int32_t *reach;          // [n_packed]
   const unsigned char *slices;   // staged slices, 16-byte aligned
-  const int64_t *slice_off;      // [n_bcc] byte offset of BCC b's slice (-1: BCC not in this schedule)
+  const int64_t *slice_off;      // [n_bcc] byte offset of BCC b's slice, | 1 when narrow (-1: not in this schedule)
   const int32_t *slice_bytes;    // [n_bcc] its size (TileSlice::bytes)
   const TileItem *items;
   int64_t item_begin, item_end;
