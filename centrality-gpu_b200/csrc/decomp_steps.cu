@@ -6,8 +6,9 @@
 // slots or BCCs. A backend runs the steps: DevBackend as a grid-stride kernel
 // per step on one GPU, HostBackend as OpenMP loops over the very same
 // functors -- a check of the GPU steps on a machine without one. Prefix sums
-// are taken on the host in both, as are the stable regrouping of the BFS
-// order by BCC and the sort of rows longer than 32 arcs.
+// run on the device in DevBackend (three scan kernels) and as a host loop in
+// HostBackend; the stable regrouping of the BFS order by BCC and the sort of
+// rows longer than 32 arcs run on the host.
 //
 // Steps (vertex ids int32, counts int64):
 //   components   union-find over the edges, roots the smallest vertices
@@ -42,9 +43,11 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "decomp.h"
+#include "internal.h"
 
 namespace bcg {
 namespace decomp_steps {
@@ -382,6 +385,82 @@ __global__ void each_kernel(int64_t n, F f) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) f(i);
 }
 
+// Exclusive prefix sum on the device, in place, in three kernels: each tile
+// of kScanTile elements (kScanItems consecutive ones per thread) is summed;
+// one CTA scans the tile sums (and writes the total after them); each tile
+// then writes its elements' prefix sums from its tile's offset.
+constexpr int kScanBlock = 512, kScanItems = 8, kScanTile = kScanBlock * kScanItems;
+
+// Exclusive scan of v over the CTA (kScanBlock threads); *total gets the sum.
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t *warp_sums, int64_t *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int64_t w = lane < kScanBlock / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanBlock / 32) warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const int64_t before = (warp > 0 ? warp_sums[warp - 1] : 0) + x - v;
+  *total = warp_sums[kScanBlock / 32 - 1];
+  __syncthreads();  // warp_sums is reused by the caller's next scan
+  return before;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const int64_t *a, int64_t n, int64_t *sums) {
+  __shared__ int64_t ws[kScanBlock / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t t = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) t += base + j < n ? a[base + j] : 0;
+  int64_t total;
+  block_exclusive_scan(t, ws, &total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_sums_kernel(int64_t *sums, int64_t m) {
+  __shared__ int64_t ws[kScanBlock / 32];
+  int64_t carry = 0;
+  for (int64_t c0 = 0; c0 < m; c0 += kScanBlock) {
+    const int64_t i = c0 + threadIdx.x;
+    const int64_t v = i < m ? sums[i] : 0;
+    int64_t total;
+    const int64_t before = block_exclusive_scan(v, ws, &total);
+    if (i < m) sums[i] = carry + before;
+    carry += total;
+  }
+  if (threadIdx.x == 0) sums[m] = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_apply(int64_t *a, int64_t n, const int64_t *sums) {
+  __shared__ int64_t ws[kScanBlock / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t v[kScanItems], t = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    v[j] = base + j < n ? a[base + j] : 0;
+    t += v[j];
+  }
+  int64_t total;
+  int64_t run = sums[blockIdx.x] + block_exclusive_scan(t, ws, &total);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    if (base + j < n) a[base + j] = run;
+    run += v[j];
+  }
+}
+
 // Exclusive prefix sum of a[0, n) in place; returns the total.
 int64_t scan_host(int64_t *a, int64_t n) {
   int64_t s = 0;
@@ -428,7 +507,8 @@ struct DevBackend {
   int device = 0, grid_cap = 1024;
   cudaStream_t stream = nullptr;
   std::vector<void *> owned;
-  std::vector<int64_t> tmp;
+  int64_t *scan_sums = nullptr;  // tile sums of scan(), grown on demand
+  size_t scan_cap = 0;
   void check(cudaError_t e, const char *what) {
     if (e != cudaSuccess)
       throw StepError{e == cudaErrorMemoryAllocation ? BCGPU_ENOMEM : BCGPU_ECUDA,
@@ -444,6 +524,11 @@ struct DevBackend {
   ~DevBackend() {
     if (stream) cudaStreamSynchronize(stream);
     for (void *p : owned) cudaFree(p);
+    if (scan_sums) cudaFree(scan_sums);
+    for (int i = 0; i < 2; ++i) {
+      if (stage[i]) cudaFreeHost(stage[i]);
+      if (staged[i]) cudaEventDestroy(staged[i]);
+    }
     if (stream) cudaStreamDestroy(stream);
   }
   template <class T>
@@ -468,17 +553,86 @@ struct DevBackend {
   }
   template <class T>
   void download(T *dst, const T *src, size_t n) {
-    if (n) check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, stream), "download");
+    const size_t bytes = n * sizeof(T);
+    if (bytes >= kStageMin && stage_ok()) {
+      download_staged(reinterpret_cast<unsigned char *>(dst), reinterpret_cast<const unsigned char *>(src), bytes);
+      return;
+    }
+    if (n) check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream), "download");
     check(cudaStreamSynchronize(stream), "step");
   }
+  // Large results come back through two pinned buffers: the copy of chunk
+  // k+1 runs while chunk k is spread into the (pageable) destination by the
+  // host threads.
+  static constexpr size_t kStageMin = size_t(8) << 20, kStageChunk = size_t(16) << 20;
+  unsigned char *stage[2] = {nullptr, nullptr};
+  cudaEvent_t staged[2] = {nullptr, nullptr};
+  bool stage_tried = false;
+  bool stage_ok() {
+    if (!stage_tried) {
+      stage_tried = true;
+      for (int i = 0; i < 2; ++i)
+        if (cudaMallocHost(reinterpret_cast<void **>(&stage[i]), kStageChunk) != cudaSuccess ||
+            cudaEventCreateWithFlags(&staged[i], cudaEventDisableTiming) != cudaSuccess) {
+          cudaGetLastError();
+          return false;
+        }
+    }
+    return stage[1] && staged[1];
+  }
+  void download_staged(unsigned char *dst, const unsigned char *src, size_t bytes) {
+    const size_t chunks = (bytes + kStageChunk - 1) / kStageChunk;
+    auto issue = [&](size_t c) {
+      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+      check(cudaMemcpyAsync(stage[c & 1], src + off, len, cudaMemcpyDeviceToHost, stream), "download");
+      check(cudaEventRecord(staged[c & 1], stream), "download");
+    };
+    issue(0);
+    for (size_t c = 0; c < chunks; ++c) {
+      if (c + 1 < chunks) issue(c + 1);  // the other buffer: its previous chunk was spread last iteration
+      check(cudaEventSynchronize(staged[c & 1]), "download");
+      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+      const unsigned char *from = stage[c & 1];
+      constexpr size_t kPiece = size_t(1) << 20;
+#pragma omp parallel for schedule(static)
+      for (int64_t q = 0; q < (int64_t)((len + kPiece - 1) / kPiece); ++q) {
+        const size_t a = (size_t)q * kPiece;
+        std::memcpy(dst + off + a, from + a, std::min(kPiece, len - a));
+      }
+    }
+  }
+  // Exclusive prefix sum of a[0, n) in place on the device; returns the total.
   int64_t scan(int64_t *a, int64_t n) {
-    tmp.resize((size_t)n);
-    download(tmp.data(), a, (size_t)n);
-    const int64_t s = scan_host(tmp.data(), n);
-    upload(a, tmp.data(), (size_t)n);
-    return s;
+    if (n <= 0) return 0;
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if ((int64_t)scan_cap < tiles + 1) {
+      if (scan_sums) cudaFree(scan_sums);
+      scan_sums = nullptr;
+      check(cudaMalloc(&scan_sums, sizeof(int64_t) * (size_t)(tiles + 1)), "cudaMalloc");
+      scan_cap = (size_t)(tiles + 1);
+    }
+    scan_tile_sums<<<(unsigned)tiles, kScanBlock, 0, stream>>>(a, n, scan_sums);
+    scan_sums_kernel<<<1, kScanBlock, 0, stream>>>(scan_sums, tiles);
+    scan_apply<<<(unsigned)tiles, kScanBlock, 0, stream>>>(a, n, scan_sums);
+    check(cudaGetLastError(), "scan launch");
+    int64_t total = 0;
+    download(&total, scan_sums + tiles, 1);
+    return total;
   }
 };
+
+// Profiling builds (-DBCGPU_HOST_TIMERS): the wall time of each step group,
+// the device's queue drained first.
+template <class BE>
+void step_mark(BE &be, const char *name) {
+#ifdef BCGPU_HOST_TIMERS
+  if constexpr (std::is_same<BE, DevBackend>::value) cudaStreamSynchronize(be.stream);
+  HOST_MARK(name);
+#else
+  (void)be;
+  (void)name;
+#endif
+}
 
 // The split's results, resident where the backend runs (owned by it).
 struct DevSplit {
@@ -491,6 +645,7 @@ struct DevSplit {
 
 template <class BE>
 DevSplit run_split(BE &be, const bc_graph *g) {
+  step_mark(be, "d: start");
   const int32_t n = g->n;
   const int64_t arcs = g->row.empty() ? 0 : g->row[n];
   int64_t *R = be.template alloc<int64_t>((size_t)n + 1);
@@ -508,6 +663,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   int32_t *n_art = be.template alloc<int32_t>(1);
   double *art = be.template alloc<double>(n);
 
+  step_mark(be, "d: upload+alloc");
   // components
   be.each(n, Iota{uf});
   be.each(n, Hook{R, C, uf});
@@ -517,6 +673,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.each(n, Fill32{par, -2});
   be.each(n, RootScatter{uf, flag, roots, comp, order, par});
 
+  step_mark(be, "d: components");
   // BFS forest, one launch per level; tail (the end of the listed vertices)
   // carries over from level to level, so each level costs one read-back
   std::vector<int64_t> lvl{0, nroots};
@@ -534,6 +691,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   if (lvl.back() != n) throw StepError{BCGPU_EINVAL, "BFS forest does not cover the graph"};
   const int64_t nlev = (int64_t)lvl.size() - 1;
 
+  step_mark(be, "d: forest bfs");
   // subtree sizes, preorder, low/high
   be.each(n, Fill64{nd, 1});
   for (int64_t L = nlev - 1; L >= 1; --L) be.each(lvl[L + 1] - lvl[L], NdUp{order, par, nd, lvl[L]});
@@ -546,6 +704,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.each(n, LoHiLocal{R, C, par, pre, lo, hi});
   for (int64_t L = nlev - 1; L >= 1; --L) be.each(lvl[L + 1] - lvl[L], LoHiUp{order, par, lo, hi, lvl[L]});
 
+  step_mark(be, "d: sweeps");
   // BCCs: union-find over tree edges
   be.each(n, Iota{uf});
   be.each(n, TreeEdgeUnion{R, C, par, pre, lo, hi, nd, uf});
@@ -554,6 +713,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   const int64_t nbcc = be.scan(flag, n);
   be.each(n, BccOf{par, uf, flag, tbcc});
 
+  step_mark(be, "d: bcc union");
   // heads, reach terms, articulation terms
   int32_t *head = be.template alloc<int32_t>((size_t)nbcc);
   int64_t *below = be.template alloc<int64_t>((size_t)nbcc), *mem_off = be.template alloc<int64_t>((size_t)nbcc + 1);
@@ -566,6 +726,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.upload(n_art, &zero, 1);
   be.each(n, Art{comp, csize, hang, sq, art, n_art});
 
+  step_mark(be, "d: heads");
   // members (head last) and their arcs per BCC
   be.each(nbcc + 1, Fill64{mem_off, 0});
   be.each(n, LocalId{tbcc, mem_off, locid});
@@ -888,6 +1049,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   be.each(ns, SlotBcc{d.mem_off, d.nbcc, slot_b});
   const Slots S{d.mem_off, d.sdeg, d.sadj, slot_b, pkof, d.members};
 
+  step_mark(be, "d: members+order");
   // roots and the BFS of every packed BCC at once
   uint64_t *key = be.template alloc<uint64_t>((size_t)np);
   int32_t *cyc = be.template alloc<int32_t>((size_t)np), *seen = be.template alloc<int32_t>((size_t)ns);
@@ -913,6 +1075,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   }
   if (f1 != npk) throw StepError{BCGPU_EINVAL, "a BCC is not connected"};
 
+  step_mark(be, "d: packing bfs");
   // each BCC's queue: its subsequence of the level-major order
   std::vector<int32_t> h_bq((size_t)npk), h_slot_b((size_t)ns), h_q((size_t)npk);
   be.download(h_bq.data(), bq, (size_t)npk);
@@ -924,6 +1087,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   int32_t *q = bq;
   be.upload(q, h_q.data(), (size_t)npk);
 
+  step_mark(be, "d: regroup");
   // plain vertices
   int64_t *gidx = cnt;
   be.each(npk, PlainFlag{S, q, cyc, gidx});
@@ -943,6 +1107,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   be.each(npk, Fill32{old, -1});
   be.each(npk, PlainPlace{S, q, cyc, gidx, pbase, vtx_off, nid, pl, old});
 
+  step_mark(be, "d: plain");
   // chains: count, prefix sums, write
   int64_t *ccnt = be.template alloc<int64_t>((size_t)nplain_all + 1), *vcnt = be.template alloc<int64_t>((size_t)nplain_all + 1);
   int32_t *bad = be.template alloc<int32_t>(1);
@@ -976,6 +1141,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   be.download(&h_bad, bad, 1);
   if (h_bad) throw StepError{BCGPU_EINVAL, "packing left a vertex without a place"};
 
+  step_mark(be, "d: chains");
   // packed CSR in the new local ids, orig, reach
   int32_t *inv = claim;  // nid is no longer needed
   be.each(npk, Inverse{old, vtx_off, np, inv});
@@ -988,6 +1154,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   int32_t *reach = be.template alloc<int32_t>((size_t)npk);
   be.each(npk, ColFill{S, old, inv, d.head, d.comp, row, d.csize, d.below, d.hang, col, orig, reach});
 
+  step_mark(be, "d: packed csr");
   // to the host; rows longer than kSmallRow are sorted here
   D->row.resize((size_t)npk + 1);
   D->col.resize((size_t)parcs);
@@ -1007,9 +1174,11 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   be.download(D->chain_l.data(), ch + 2 * nchains, (size_t)nchains);
   be.download(D->chain_r.data(), ch + 3 * nchains, (size_t)nchains);
   be.download(D->art.data(), d.art, (size_t)d.n);
+  step_mark(be, "d: downloads");
 #pragma omp parallel for schedule(dynamic, 1024)
   for (int64_t k = 0; k < npk; ++k)
     if (D->row[k + 1] - D->row[k] > kSmallRow) std::sort(D->col.begin() + D->row[k], D->col.begin() + D->row[k + 1]);
+  step_mark(be, "d: sort");
   std::vector<int32_t> h_cyc((size_t)np);
   be.download(h_cyc.data(), cyc, (size_t)np);
   int64_t cycles = 0;

@@ -176,6 +176,15 @@ cudaError_t cudaFree(void *p) {
   return cudaSuccess;
 }
 cudaError_t cudaMallocAsync(void **p, size_t bytes, cudaStream_t) { return cudaMalloc(p, bytes); }
+// pinned host memory: ordinary host memory here
+cudaError_t cudaMallocHost(void **p, size_t bytes) {
+  *p = std::malloc(bytes ? bytes : 1);
+  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFreeHost(void *p) {
+  std::free(p);
+  return cudaSuccess;
+}
 cudaError_t cudaFreeAsync(void *p, cudaStream_t) { return cudaFree(p); }
 // Memory pools: a pool is a tag; its allocations are ordinary stand-in
 // allocations. An injected failure of a pool allocation also fails the
@@ -240,6 +249,7 @@ cudaError_t cudaStreamCreateWithFlags(cudaStream_t *s, unsigned) {
 cudaError_t cudaStreamDestroy(cudaStream_t s) { delete reinterpret_cast<char *>(s); return cudaSuccess; }
 cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
 cudaError_t cudaEventCreate(cudaEvent_t *e) { *e = reinterpret_cast<cudaEvent_t>(new char); return cudaSuccess; }
+cudaError_t cudaEventCreateWithFlags(cudaEvent_t *e, unsigned) { return cudaEventCreate(e); }
 cudaError_t cudaEventDestroy(cudaEvent_t e) { delete reinterpret_cast<char *>(e); return cudaSuccess; }
 cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t) { return cudaSuccess; }
 cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
