@@ -52,13 +52,19 @@ def stub_dir():
     if not all(o.exists() for o in objs):
         pkg_build.build()
     BUILD.mkdir(exist_ok=True)
-    stub_o = BUILD / "stub_cudart.o"
+    # built under names of this process, then renamed into place: test
+    # processes running side by side never load a half-written library
+    tag = f".{os.getpid()}"
+    stub_o = BUILD / f"stub_cudart{tag}.o"
     subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-I/usr/local/cuda/include", "-c",
                     str(STUB / "stub_cudart.cpp"), "-o", str(stub_o)], check=True)
     # -Bsymbolic: the library's calls bind to these stand-ins even when a real
     # CUDA runtime is already loaded in the process (torch brings one)
-    subprocess.run(["g++", "-shared", "-o", str(BUILD / "libbcgpu.so")] + [str(o) for o in objs] +
+    lib_tmp = BUILD / f"libbcgpu.so{tag}"
+    subprocess.run(["g++", "-shared", "-o", str(lib_tmp)] + [str(o) for o in objs] +
                    [str(stub_o), "-lgomp", "-Wl,--no-undefined", "-Wl,-Bsymbolic"], check=True)
+    stub_o.unlink()
+    os.replace(lib_tmp, BUILD / "libbcgpu.so")
     return BUILD
 
 
