@@ -102,6 +102,7 @@ _SIGS = {
     "bc_plan_record": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
     "bc_plan_read": (C.c_int, [C.c_void_p, _f64p]),
     "bc_plan_source_rows": (C.c_int, [C.c_void_p, C.c_int64, _i32p, _f64p]),
+    "bc_plan_pass_rows": (C.c_int, [C.c_void_p, C.c_int64, _i32p, _i32p, _i32p, _i32p, _f64p]),
     "bc_graph_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "bc_graph_from_edges": (C.c_int, [C.c_int32, C.c_int64, _i32p, _i32p, C.POINTER(C.c_void_p)]),
     "bc_graph_free": (None, [C.c_void_p]),
@@ -416,6 +417,19 @@ class Plan:
         s = np.zeros(nb, dtype=np.float64)
         self.ctx._check(lib().bc_plan_source_rows(self._h, int(packed), _ptr(d, _i32p), _ptr(s, _f64p)))
         return d, s
+
+    def pass_rows(self, unit):
+        """Runs multi-source pass `unit` and returns (sources, d, sigma): the
+        pass's sources (local ids in its BCC) and, per source (row) and core
+        vertex (column), the level and the path count (level bases applied)."""
+        ns, nc = C.c_int32(), C.c_int32()
+        self.ctx._check(lib().bc_plan_pass_rows(self._h, int(unit), C.byref(ns), C.byref(nc), None, None, None))
+        src = np.zeros(ns.value, dtype=np.int32)
+        d = np.zeros((ns.value, nc.value), dtype=np.int32)
+        s = np.zeros((ns.value, nc.value), dtype=np.float64)
+        self.ctx._check(lib().bc_plan_pass_rows(self._h, int(unit), C.byref(ns), C.byref(nc), _ptr(src, _i32p),
+                                                _ptr(d, _i32p), _ptr(s, _f64p)))
+        return src, d, s
 
     def close(self):
         if self._h and self.ctx._h:

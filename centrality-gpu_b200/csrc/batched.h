@@ -63,6 +63,15 @@ void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std:
 // and vertex visits.
 void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std::vector<int64_t> &teps,
                        std::vector<int64_t> &bfs, std::vector<int64_t> &aux, std::vector<int64_t> &visits);
+// Levels and path counts (level bases applied) of the core vertices for
+// every slot of pass `pass`, read from the workspace, which holds the pass
+// the plan ran last: d[b * n_core + v], sigma likewise; src[b] = slot b's
+// source (local id; a chain source at its own position). For parity tests.
+// BCC and slot count of pass `pass`.
+int batched_pass_shape(const BatchedPlan *p, int64_t pass, int32_t *bcc, int32_t *nslots);
+int batched_pass_rows(const BatchedPlan *p, int64_t pass, const int32_t *chain_start, int32_t n_core,
+                      cudaStream_t stream, std::vector<int32_t> &src, std::vector<int32_t> &d, std::vector<double> &sigma,
+                      std::string *msg);
 int batched_run(BatchedPlan *p, int64_t begin, int64_t end, cudaStream_t stream, int *launches, std::string *msg);
 // Batches whose FP32 dependency values left FP32's exponent range (their
 // contributions were withheld); synchronises the stream.

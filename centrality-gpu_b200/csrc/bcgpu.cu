@@ -1315,6 +1315,32 @@ extern "C" int bc_plan_source_rows(bc_plan *p, int64_t packed, int32_t *d_out, d
   return check_dev_err(p);
 }
 
+extern "C" int bc_plan_pass_rows(bc_plan *p, int64_t unit, int32_t *nslots, int32_t *ncore, int32_t *src_out,
+                                 int32_t *d_out, double *sigma_out) {
+  if (!p || !nslots || !ncore) return BCGPU_EINVAL;
+  bc_ctx *ctx = p->ctx;
+  int32_t b = 0, ns = 0;
+  if (!p->bp || unit < 0 || unit >= p->n_bat || bcg::batched_pass_shape(p->bp, unit, &b, &ns) != BCGPU_OK)
+    return fail(ctx, BCGPU_EINVAL, "unit is not a multi-source pass");
+  *nslots = ns;
+  *ncore = p->h_n_plain[b];
+  if (!src_out && !d_out && !sigma_out) return BCGPU_OK;  // sizes only
+  if (!src_out || !d_out || !sigma_out) return fail(ctx, BCGPU_EINVAL, "null output");
+  int rc = bc_plan_run(p, unit, unit + 1, nullptr);
+  if (rc) return rc;
+  std::vector<int32_t> src, d;
+  std::vector<double> sg;
+  std::string msg;
+  rc = bcg::batched_pass_rows(p->bp, unit, p->h_chain_start.data(), *ncore, ctx->stream, src, d, sg, &msg);
+  if (rc) return fail(ctx, rc, msg.c_str());
+  rc = check_dev_err(p);
+  if (rc) return rc;
+  std::copy(src.begin(), src.end(), src_out);
+  std::copy(d.begin(), d.end(), d_out);
+  std::copy(sg.begin(), sg.end(), sigma_out);
+  return BCGPU_OK;
+}
+
 namespace {
 
 int run_units(bc_ctx *ctx, const bc_bccs *bccs, int64_t begin, int64_t end, bool all, bool with_art, double *bc_out,

@@ -18,13 +18,14 @@
 static void usage() {
   std::fprintf(stderr,
                "usage: betc INPUT_FILE [--out FILE] [--mode plain|batched] [--delta fp64|fp32c]\n"
-               "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE] [--gpu-decomp]\n"
+               "            [--batch WIDTH] [--device ORDINAL] [--quiet] [--save-csr FILE] [--host-decomp]\n"
                "            [--plain-ctas 4|8|16]\n"
                "  INPUT_FILE: the edge list (n m, then u v w per edge) or a CSR written by --save-csr;\n"
                "    the graph is taken as simple and unweighted: repeated edges count once and\n"
                "    self-loops are dropped (the reference keeps repeated edges as parallel arcs,\n"
                "    which multiplies path counts)\n"
-               "  --gpu-decomp: run the BCC/chain decomposition on the GPU as well (same result)\n"
+               "  --host-decomp: run the BCC/chain decomposition on the host cores instead of the GPU\n"
+               "    (same result; the GPU steps are the default, --gpu-decomp names them explicitly)\n"
                "  --plain-ctas: per-source CTAs per SM (more sources in flight on deep BCCs)\n");
 }
 
@@ -33,7 +34,7 @@ int main(int argc, char **argv) {
   const char *input = nullptr, *out_path = nullptr, *save_path = nullptr;
   bc_opts opts;
   bc_default_opts(&opts);
-  bool quiet = false, gpu_decomp = false;
+  bool quiet = false, gpu_decomp = true;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     auto next = [&]() -> const char * {
@@ -56,6 +57,7 @@ int main(int argc, char **argv) {
     else if (a == "--quiet") quiet = true;
     else if (a == "--save-csr") save_path = next();
     else if (a == "--gpu-decomp") gpu_decomp = true;
+    else if (a == "--host-decomp") gpu_decomp = false;
     else if (a == "--plain-ctas") opts.plain_ctas_per_sm = std::atoi(next());
     else if (a == "-h" || a == "--help") { usage(); return 0; }
     else if (!input) input = argv[i];
@@ -73,23 +75,34 @@ int main(int argc, char **argv) {
     bc_graph_free(g);
     return 6;
   }
+  // the context first: its options are checked (and its GPU chosen) before
+  // any decomposition work
+  bc_ctx *ctx = nullptr;
+  rc = bc_create(&opts, &ctx);
+  if (rc) { std::fprintf(stderr, "betc: %s\n", bc_last_error(nullptr)); bc_graph_free(g); return 4; }
   bc_decomp *d = nullptr;
   if (gpu_decomp) {
     // on the --device GPU, else device 0
     rc = bc_decompose_gpu(g, opts.device >= 0 ? opts.device : 0, &d, err, sizeof(err));
-    if (rc == BCGPU_ECUDA) { std::fprintf(stderr, "betc: %s\n", err); bc_graph_free(g); return 4; }
-    if (rc) { std::fprintf(stderr, "betc: GPU decomposition failed (code %d): %s\n", rc, err); bc_graph_free(g); return 3; }
+    if (rc == BCGPU_ECUDA) { std::fprintf(stderr, "betc: %s\n", err); bc_destroy(ctx); bc_graph_free(g); return 4; }
+    if (rc) {
+      std::fprintf(stderr, "betc: GPU decomposition failed (code %d): %s\n", rc, err);
+      bc_destroy(ctx);
+      bc_graph_free(g);
+      return 3;
+    }
   } else {
     rc = bc_decompose(g, &d);
-    if (rc) { std::fprintf(stderr, "betc: decomposition failed (code %d)\n", rc); bc_graph_free(g); return 3; }
+    if (rc) {
+      std::fprintf(stderr, "betc: decomposition failed (code %d)\n", rc);
+      bc_destroy(ctx);
+      bc_graph_free(g);
+      return 3;
+    }
   }
   bc_decomp_info info;
   bc_decomp_get_info(d, &info);
   const bc_bccs *view = bc_decomp_view(d);
-
-  bc_ctx *ctx = nullptr;
-  rc = bc_create(&opts, &ctx);
-  if (rc) { std::fprintf(stderr, "betc: %s\n", bc_last_error(nullptr)); bc_decomp_free(d); bc_graph_free(g); return 4; }
   std::vector<double> bc((size_t)view->n_orig, 0.0);
   bc_stats st{};
   rc = bc_run_bccs(ctx, view, bc.data(), &st);

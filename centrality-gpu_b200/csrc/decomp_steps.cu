@@ -8,7 +8,10 @@
 // functors -- a check of the GPU steps on a machine without one. Prefix sums
 // run on the device in DevBackend (three scan kernels) and as a host loop in
 // HostBackend; the stable regrouping of the BFS order by BCC and the sort of
-// rows longer than 32 arcs run on the host.
+// packed rows longer than 4096 arcs run on the host (DevBackend sorts rows of
+// 33 to 4096 arcs on the GPU, HostBackend leaves every row beyond 32 arcs to
+// that host sort). Steps over whole rows run per arc where the arcs are
+// independent, else with a warp per long row.
 //
 // Steps (vertex ids int32, counts int64):
 //   components   union-find over the edges, roots the smallest vertices
@@ -136,7 +139,58 @@ __host__ __device__ inline void uf_union(int32_t *p, int32_t a, int32_t b) {
   }
 }
 
-// ---- the steps; operator()(i) handles item i
+// ---- warp helpers of the warp-per-row forms of the steps (device only)
+__device__ __forceinline__ unsigned lanes_below() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ int64_t warp_sum64(int64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// Inclusive prefix sum over the warp's lanes.
+__device__ __forceinline__ int64_t warp_incl64(int64_t v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+// Ascending bitonic sort of one value per lane across the warp.
+__device__ __forceinline__ int32_t warp_sort32(int32_t v, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+      v = (((lane & j) == 0) == ((lane & k) == 0)) ? min(v, o) : max(v, o);
+    }
+  return v;
+}
+
+// ---- the steps; operator()(i) handles item i. Steps over a vertex's whole
+// row come in two forms: per arc (operator()(e) over every arc, its vertex
+// from src[e]) where the row's arcs are independent, else per item with a
+// warp form (len(i), warp(i, lane)) that the GPU runs for rows longer than
+// kLightArcs, keeping the row's arc order wherever the output depends on it.
+// Packed rows of at most kSmallRow arcs are sorted as they are written
+// (ColFill); longer ones by the backend (sort_rows) and the host.
+constexpr int32_t kSmallRow = 32;
+
+struct ArcSrc {  // src[e] = the vertex whose row holds arc e
+  const int64_t *R;
+  int32_t *src;
+  __host__ __device__ void operator()(int64_t i) const {
+    for (int64_t e = R[i]; e < R[i + 1]; ++e) src[e] = (int32_t)i;
+  }
+  __device__ int64_t len(int64_t i) const { return R[i + 1] - R[i]; }
+  __device__ void warp(int64_t i, int lane) const {
+    for (int64_t e = R[i] + lane; e < R[i + 1]; e += 32) src[e] = (int32_t)i;
+  }
+};
 struct Iota {
   int32_t *p;
   __host__ __device__ void operator()(int64_t i) const { p[i] = (int32_t)i; }
@@ -156,14 +210,12 @@ struct Copy64 {
   const int64_t *src;
   __host__ __device__ void operator()(int64_t i) const { dst[i] = src[i]; }
 };
-struct Hook {  // components: one union per edge, from its larger end
-  const int64_t *R;
-  const int32_t *C;
+struct Hook {  // components: one union per edge, from its larger end (per arc)
+  const int32_t *C, *src;
   int32_t *uf;
-  __host__ __device__ void operator()(int64_t i) const {
-    const int32_t x = (int32_t)i;
-    for (int64_t e = R[x]; e < R[x + 1]; ++e)
-      if (C[e] < x) uf_union(uf, x, C[e]);
+  __host__ __device__ void operator()(int64_t e) const {
+    const int32_t x = src[e], y = C[e];
+    if (y < x) uf_union(uf, x, y);
   }
 };
 struct Compress {
@@ -200,6 +252,30 @@ struct BfsLevel {  // frontier position i: claim undiscovered neighbours
     for (int64_t e = R[x]; e < R[x + 1]; ++e) {
       const int32_t y = C[e];
       if (ld32(&par[y]) == -2 && cas32(&par[y], -2, x) == -2) order[add64(tail, 1)] = y;
+    }
+  }
+  __device__ int64_t len(int64_t i) const {
+    const int32_t x = order[f0 + i];
+    return R[x + 1] - R[x];
+  }
+  __device__ void warp(int64_t i, int lane) const {  // claims appended with one atomic per 32 arcs
+    const int32_t x = order[f0 + i];
+    const int64_t e1 = R[x + 1];
+    for (int64_t b = R[x]; b < e1; b += 32) {
+      const int64_t e = b + lane;
+      int32_t y = 0;
+      bool got = false;
+      if (e < e1) {
+        y = C[e];
+        got = ld32(&par[y]) == -2 && cas32(&par[y], -2, x) == -2;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, got);
+      if (!m) continue;
+      const int lead = __ffs(m) - 1;
+      int64_t at = 0;
+      if (lane == lead) at = add64(tail, __popc(m));
+      at = __shfl_sync(0xffffffffu, at, lead);
+      if (got) order[at + __popc(m & lanes_below())] = y;
     }
   }
 };
@@ -241,21 +317,20 @@ struct PreDown {  // level items: take the next range of the parent's interval
     cur[x] = q + 1;
   }
 };
-struct LoHiLocal {  // pre range over x and its neighbours other than its parent
-  const int64_t *R;
-  const int32_t *C, *par, *pre;
+struct LoHiInit {  // pre range over x ...
+  const int32_t *pre;
   int32_t *lo, *hi;
-  __host__ __device__ void operator()(int64_t i) const {
-    const int32_t x = (int32_t)i;
-    int32_t l = pre[x], h = pre[x];
-    for (int64_t e = R[x]; e < R[x + 1]; ++e)
-      if (C[e] != par[x]) {
-        const int32_t q = pre[C[e]];
-        l = q < l ? q : l;
-        h = q > h ? q : h;
-      }
-    lo[x] = l;
-    hi[x] = h;
+  __host__ __device__ void operator()(int64_t x) const { lo[x] = hi[x] = pre[x]; }
+};
+struct LoHiArc {  // ... and its neighbours other than its parent (per arc)
+  const int32_t *C, *src, *par, *pre;
+  int32_t *lo, *hi;
+  __host__ __device__ void operator()(int64_t e) const {
+    const int32_t x = src[e], y = C[e];
+    if (y == par[x]) return;
+    const int32_t q = pre[y];
+    if (q < ld32(&lo[x])) min32(&lo[x], q);
+    if (q > ld32(&hi[x])) max32(&hi[x], q);
   }
 };
 struct LoHiUp {
@@ -268,20 +343,28 @@ struct LoHiUp {
     max32(&hi[par[x]], hi[x]);
   }
 };
-struct TreeEdgeUnion {  // tree edges named by their child vertex
-  const int64_t *R;
-  const int32_t *C, *par, *pre, *lo, *hi;
+// Tree edges named by their child vertex: a child's with its parent's when
+// the child's subtree escapes the parent's (per vertex) ...
+struct TreeEdgeUnion {
+  const int32_t *par, *pre, *lo, *hi;
   const int64_t *nd;
   int32_t *uf;
   __host__ __device__ void operator()(int64_t i) const {
     const int32_t w = (int32_t)i, v = par[w];
     if (v >= 0 && par[v] >= 0 && (lo[w] < pre[v] || (int64_t)hi[w] >= (int64_t)pre[v] + nd[v])) uf_union(uf, v, w);
-    for (int64_t e = R[w]; e < R[w + 1]; ++e) {
-      const int32_t y = C[e];
-      if (y <= w || y == v || w == par[y]) continue;
-      const int32_t a = pre[w] < pre[y] ? w : y, b = a == w ? y : w;
-      if ((int64_t)pre[b] >= (int64_t)pre[a] + nd[a]) uf_union(uf, w, y);
-    }
+  }
+};
+// ... and the two tree edges of an unrelated non-tree edge (per arc, from
+// its larger end)
+struct TreeArcUnion {
+  const int32_t *C, *src, *par, *pre;
+  const int64_t *nd;
+  int32_t *uf;
+  __host__ __device__ void operator()(int64_t e) const {
+    const int32_t w = src[e], y = C[e];
+    if (y <= w || y == par[w] || w == par[y]) return;
+    const int32_t a = pre[w] < pre[y] ? w : y, b = a == w ? y : w;
+    if ((int64_t)pre[b] >= (int64_t)pre[a] + nd[a]) uf_union(uf, w, y);
   }
 };
 struct NameFlag {  // 1 for a BCC's name: a tree edge that is its set's root
@@ -360,22 +443,50 @@ struct HeadLast {
 // slots without atomics, in arc order.
 struct SlotArcs {
   const int64_t *R;
-  const int32_t *C, *tbcc, *pre, *head, *locid;
+  const int32_t *C, *src, *tbcc, *pre, *head, *locid;
   const int64_t *mem_off;
-  int64_t *cnt;           // count pass: arcs per slot
-  int64_t *cursor;        // fill pass: next free position per slot
+  int64_t *cnt;           // count pass (per arc): arcs per slot
+  int64_t *cursor;        // fill pass (per vertex): next free position per slot
   int32_t *sadj;
   __host__ __device__ int32_t local_of(int32_t x, int32_t b) const {
     return x == head[b] ? (int32_t)(mem_off[b + 1] - mem_off[b] - 1) : locid[x];
   }
+  __host__ __device__ int32_t bcc_of(int32_t x, int32_t y) const { return tbcc[pre[x] > pre[y] ? x : y]; }
   __host__ __device__ void operator()(int64_t i) const {
+    if (!cursor) {  // count: i is an arc
+      const int32_t x = src[i], b = bcc_of(x, C[i]);
+      add64(&cnt[mem_off[b] + local_of(x, b)], 1);
+      return;
+    }
     const int32_t x = (int32_t)i;
     for (int64_t e = R[x]; e < R[x + 1]; ++e) {
       const int32_t y = C[e];
-      const int32_t b = tbcc[pre[x] > pre[y] ? x : y];
+      const int32_t b = bcc_of(x, y);
       const int64_t s = mem_off[b] + local_of(x, b);
-      if (cursor) sadj[cursor[s]++] = local_of(y, b);
-      else cnt[s] += 1;
+      sadj[cursor[s]++] = local_of(y, b);
+    }
+  }
+  __device__ int64_t len(int64_t i) const { return R[i + 1] - R[i]; }
+  // fill pass, 32 arcs at a time: the lanes of one slot write in arc order
+  // from the slot's cursor, which the slot's lowest lane then advances
+  __device__ void warp(int64_t i, int lane) const {
+    const int32_t x = (int32_t)i;
+    const int64_t e1 = R[x + 1];
+    for (int64_t base = R[x]; base < e1; base += 32) {
+      const int64_t e = base + lane;
+      const bool on = e < e1;
+      const unsigned act = __ballot_sync(0xffffffffu, on);
+      if (on) {
+        const int32_t y = C[e], b = bcc_of(x, y);
+        const int64_t s = mem_off[b] + local_of(x, b);
+        const unsigned peers = __match_any_sync(act, s);
+        const int lead = __ffs(peers) - 1;
+        int64_t at = lane == lead ? cursor[s] : 0;
+        at = __shfl_sync(peers, at, lead);
+        sadj[at + __popc(peers & lanes_below())] = local_of(y, b);
+        if (lane == lead) cursor[s] = at + __popc(peers);
+      }
+      __syncwarp();
     }
   }
 };
@@ -383,6 +494,29 @@ struct SlotArcs {
 template <class F>
 __global__ void each_kernel(int64_t n, F f) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) f(i);
+}
+
+// Items with a row each, 32 per warp at a time: a lane runs its item's row
+// alone when it has at most kLightArcs arcs; longer rows then run one at a
+// time on the whole warp (f.warp), so a hub's row is spread over 32 lanes
+// instead of holding one thread while the rest of the grid idles.
+constexpr int64_t kLightArcs = 16;
+template <class F>
+__global__ void rows_kernel(int64_t n, F f) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = w * 32; base < n; base += nw * 32) {
+    const int64_t i = base + lane;
+    const bool heavy = i < n && f.len(i) > kLightArcs;
+    if (i < n && !heavy) f(i);
+    uint32_t todo = __ballot_sync(0xffffffffu, heavy);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      f.warp(base + j, lane);
+    }
+  }
 }
 
 // Exclusive prefix sum on the device, in place, in three kernels: each tile
@@ -492,9 +626,19 @@ struct HostBackend {
   }
   template <class F>
   void each(int64_t n, const F &f) {
+    if (n < kSerialItems) {  // a deep BFS's thin levels: no thread team per level
+      for (int64_t i = 0; i < n; ++i) f(i);
+      return;
+    }
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t i = 0; i < n; ++i) f(i);
   }
+  static constexpr int64_t kSerialItems = 2048;
+  template <class F>
+  void rows(int64_t n, const F &f) { each(n, f); }
+  // Sorts packed rows on the backend; returns the longest row length it
+  // covers (here none beyond the rows ColFill sorts itself).
+  int64_t sort_rows(const int64_t *, int32_t *, int64_t) { return kSmallRow; }
   template <class T>
   void upload(T *dst, const T *src, size_t n) { std::memcpy(dst, src, n * sizeof(T)); }
   template <class T>
@@ -546,6 +690,15 @@ struct DevBackend {
     each_kernel<<<(unsigned)blocks, kBlock, 0, stream>>>(n, f);
     check(cudaGetLastError(), "step launch");
   }
+  template <class F>
+  void rows(int64_t n, const F &f) {
+    if (n <= 0) return;
+    constexpr int kBlock = 256;
+    const int64_t blocks = std::min<int64_t>((n + kBlock - 1) / kBlock, grid_cap);
+    rows_kernel<<<(unsigned)blocks, kBlock, 0, stream>>>(n, f);
+    check(cudaGetLastError(), "step launch");
+  }
+  int64_t sort_rows(const int64_t *row, int32_t *col, int64_t npk);  // below the steps
   template <class T>
   void upload(T *dst, const T *src, size_t n) {
     if (n) check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
@@ -662,11 +815,13 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   int64_t *sq = be.template alloc<int64_t>(n), *tail = be.template alloc<int64_t>(1);
   int32_t *n_art = be.template alloc<int32_t>(1);
   double *art = be.template alloc<double>(n);
+  int32_t *src = be.template alloc<int32_t>((size_t)arcs);
+  be.rows(n, ArcSrc{R, src});
 
   step_mark(be, "d: upload+alloc");
   // components
   be.each(n, Iota{uf});
-  be.each(n, Hook{R, C, uf});
+  be.each(arcs, Hook{C, src, uf});
   be.each(n, Compress{uf});
   be.each(n, RootFlag{uf, flag});
   const int64_t nroots = be.scan(flag, n);
@@ -679,7 +834,7 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   std::vector<int64_t> lvl{0, nroots};
   be.upload(tail, &nroots, 1);
   for (int64_t f0 = 0, f1 = nroots; f1 > f0;) {
-    be.each(f1 - f0, BfsLevel{R, C, order, par, tail, f0});
+    be.rows(f1 - f0, BfsLevel{R, C, order, par, tail, f0});
     int64_t f2 = 0;
     be.download(&f2, tail, 1);
     if (f2 < f1 || f2 > n) throw StepError{BCGPU_EINVAL, "BFS forest: inconsistent frontier"};
@@ -701,13 +856,15 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.scan(cstart, nroots);
   be.each(nroots, RootPre{roots, cstart, pre, cur});
   for (int64_t L = 1; L < nlev; ++L) be.each(lvl[L + 1] - lvl[L], PreDown{order, par, nd, pre, cur, lvl[L]});
-  be.each(n, LoHiLocal{R, C, par, pre, lo, hi});
+  be.each(n, LoHiInit{pre, lo, hi});
+  be.each(arcs, LoHiArc{C, src, par, pre, lo, hi});
   for (int64_t L = nlev - 1; L >= 1; --L) be.each(lvl[L + 1] - lvl[L], LoHiUp{order, par, lo, hi, lvl[L]});
 
   step_mark(be, "d: sweeps");
   // BCCs: union-find over tree edges
   be.each(n, Iota{uf});
-  be.each(n, TreeEdgeUnion{R, C, par, pre, lo, hi, nd, uf});
+  be.each(n, TreeEdgeUnion{par, pre, lo, hi, nd, uf});
+  be.each(arcs, TreeArcUnion{C, src, par, pre, nd, uf});
   be.each(n, Compress{uf});
   be.each(n, NameFlag{par, uf, flag});
   const int64_t nbcc = be.scan(flag, n);
@@ -737,12 +894,12 @@ DevSplit run_split(BE &be, const bc_graph *g) {
   be.each(nbcc, HeadLast{head, mem_off, members});
   int64_t *sdeg = be.template alloc<int64_t>((size_t)n_slots + 1), *cursor = be.template alloc<int64_t>((size_t)n_slots);
   be.each(n_slots + 1, Fill64{sdeg, 0});
-  be.each(n, SlotArcs{R, C, tbcc, pre, head, locid, mem_off, sdeg, nullptr, nullptr});
+  be.each(arcs, SlotArcs{R, C, src, tbcc, pre, head, locid, mem_off, sdeg, nullptr, nullptr});
   const int64_t slot_arcs = be.scan(sdeg, n_slots + 1);
   if (slot_arcs != arcs) throw StepError{BCGPU_EINVAL, "member slots do not hold every arc once"};
   int32_t *sadj = be.template alloc<int32_t>((size_t)arcs);
   be.each(n_slots, Copy64{cursor, sdeg});
-  be.each(n, SlotArcs{R, C, tbcc, pre, head, locid, mem_off, nullptr, cursor, sadj});
+  be.rows(n, SlotArcs{R, C, src, tbcc, pre, head, locid, mem_off, nullptr, cursor, sadj});
 
   DevSplit d;
   d.n = n;
@@ -798,6 +955,9 @@ struct Slots {
     return (int32_t)(mem_off[slot_b[s]] + sadj[sdeg[s] + k]);
   }
   __host__ __device__ int32_t pk(int32_t s) const { return pk_of[slot_b[s]]; }
+  // nbr(s, k) = first(s) + sadj[at(s) + k]
+  __host__ __device__ int64_t first(int32_t s) const { return mem_off[slot_b[s]]; }
+  __host__ __device__ int64_t at(int32_t s) const { return sdeg[s]; }
   // Far end of the chain that leaves slot x through its neighbour cur (at
   // most nb steps; *len > nb when there is no end).
   __host__ __device__ int32_t walk(int32_t x, int32_t cur, int64_t nb, int64_t *len) const {
@@ -861,6 +1021,15 @@ struct PClaim {
       if (!seen[t]) min32(&claim[t], (int32_t)i);
     }
   }
+  __device__ int64_t len(int64_t i) const { return S.deg(bq[f0 + i]); }
+  __device__ void warp(int64_t i, int lane) const {
+    const int32_t s = bq[f0 + i], d = S.deg(s);
+    const int64_t b = S.first(s), a = S.at(s);
+    for (int32_t k = lane; k < d; k += 32) {
+      const int32_t t = (int32_t)(b + S.sadj[a + k]);
+      if (!seen[t]) min32(&claim[t], (int32_t)i);
+    }
+  }
 };
 struct PCount {
   Slots S;
@@ -876,6 +1045,18 @@ struct PCount {
     }
     cnt[i] = c;
   }
+  __device__ int64_t len(int64_t i) const { return S.deg(bq[f0 + i]); }
+  __device__ void warp(int64_t i, int lane) const {
+    const int32_t s = bq[f0 + i], d = S.deg(s);
+    const int64_t b = S.first(s), a = S.at(s);
+    int64_t c = 0;
+    for (int32_t k = lane; k < d; k += 32) {
+      const int32_t t = (int32_t)(b + S.sadj[a + k]);
+      c += !seen[t] && ld32(&claim[t]) == (int32_t)i;
+    }
+    c = warp_sum64(c);
+    if (lane == 0) cnt[i] = c;
+  }
 };
 struct PEmit {
   Slots S;
@@ -889,6 +1070,24 @@ struct PEmit {
     for (int32_t k = 0; k < S.deg(s); ++k) {
       const int32_t t = S.nbr(s, k);
       if (!seen[t] && ld32(&claim[t]) == (int32_t)i) bq[at++] = t;
+    }
+  }
+  __device__ int64_t len(int64_t i) const { return S.deg(bq[f0 + i]); }
+  __device__ void warp(int64_t i, int lane) const {  // emitted in arc order, 32 arcs at a time
+    const int32_t s = bq[f0 + i], d = S.deg(s);
+    const int64_t b = S.first(s), a = S.at(s);
+    int64_t at = f1 + at0[i];
+    for (int32_t k0 = 0; k0 < d; k0 += 32) {
+      const int32_t k = k0 + lane;
+      int32_t t = 0;
+      bool emit = false;
+      if (k < d) {
+        t = (int32_t)(b + S.sadj[a + k]);
+        emit = !seen[t] && ld32(&claim[t]) == (int32_t)i;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, emit);
+      if (emit) bq[at + __popc(m & lanes_below())] = t;
+      at += __popc(m);
     }
   }
 };
@@ -978,6 +1177,61 @@ struct Chains {
       vcnt[g] = nv;
     }
   }
+  __device__ int64_t len(int64_t g) const { return S.deg(pl[g]); }
+  // 32 arcs at a time: each lane walks its arc's chain; chain numbers and
+  // vertex positions follow arc order (a warp prefix sum of the lengths)
+  __device__ void warp(int64_t g, int lane) const {
+    const int32_t x = pl[g], i = S.pk(x);
+    if (cyc[i]) {
+      if (cnt && lane == 0) cnt[g] = vcnt[g] = 0;
+      return;
+    }
+    const int64_t nb = vtx_off[i + 1] - vtx_off[i];
+    const int32_t f = (int32_t)(g - plain_base[i]), d = S.deg(x);
+    int64_t c = cnt ? 0 : cidx[g];
+    int64_t pos = cnt ? 0 : n_plain[i] + (voff[g] - voff_base[i]);
+    for (int32_t k0 = 0; k0 < d; k0 += 32) {
+      const int32_t k = k0 + lane;
+      int32_t t = 0, far = 0;
+      int64_t len = 0;
+      bool take = false;
+      if (k < d) {
+        t = S.nbr(x, k);
+        if (S.deg(t) == 2) {
+          far = S.walk(x, t, nb, &len);
+          if (len > nb || far == x) st32(bad, 1);
+          else take = nid_plain[far] >= f;  // else numbered from its other end
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      const int64_t lv = take ? len : 0, incl = warp_incl64(lv, lane);
+      const int64_t tot = __shfl_sync(0xffffffffu, incl, 31);
+      if (!cnt && take) {
+        const int64_t cc = c + __popc(m & lanes_below());
+        int64_t p = pos + incl - lv;
+        ch_start[cc] = (int32_t)p;
+        ch_len[cc] = (int32_t)len;
+        ch_l[cc] = f;
+        ch_r[cc] = nid_plain[far];
+        int32_t prev = x, cur = t;
+        for (int64_t j = 0; j < len; ++j) {
+          nid[cur] = (int32_t)p;
+          old[vtx_off[i] + p] = cur;
+          ++p;
+          const int32_t a0 = S.nbr(cur, 0), a1 = S.nbr(cur, 1);
+          const int32_t nx = a0 == prev ? a1 : a0;
+          prev = cur;
+          cur = nx;
+        }
+      }
+      c += __popc(m);
+      pos += tot;
+    }
+    if (cnt && lane == 0) {
+      cnt[g] = c;
+      vcnt[g] = pos;
+    }
+  }
 };
 struct Unset {  // positions no step wrote
   const int32_t *old;
@@ -1001,7 +1255,6 @@ struct RowLen {
   int64_t *row;
   __host__ __device__ void operator()(int64_t k) const { row[k] = S.deg(old[k]); }
 };
-constexpr int32_t kSmallRow = 32;  // longer rows are sorted on the host
 struct ColFill {
   Slots S;
   const int32_t *old, *inv, *head, *comp;
@@ -1022,7 +1275,89 @@ struct ColFill {
     orig[k] = x;
     reach[k] = x == head[b] ? (int32_t)(csize[comp[x]] - 1 - below[b]) : (int32_t)hang[x];
   }
+  __device__ int64_t len(int64_t k) const { return S.deg(old[k]); }
+  __device__ void warp(int64_t k, int lane) const {
+    const int32_t s = old[k], b = S.slot_b[s], d = S.deg(s);
+    const int64_t f = S.first(s), a = S.at(s);
+    int32_t *dst = col + row[k];
+    if (d <= kSmallRow) {  // one neighbour per lane, sorted across the warp
+      const int32_t v = warp_sort32(lane < d ? inv[f + S.sadj[a + lane]] : INT32_MAX, lane);
+      if (lane < d) dst[lane] = v;
+    } else {
+      for (int32_t j = lane; j < d; j += 32) dst[j] = inv[f + S.sadj[a + j]];
+    }
+    if (lane == 0) {
+      const int32_t x = S.members[s];
+      orig[k] = x;
+      reach[k] = x == head[b] ? (int32_t)(csize[comp[x]] - 1 - below[b]) : (int32_t)hang[x];
+    }
+  }
 };
+
+// Rows of more than kSmallRow and at most kSortRow arcs, sorted on the GPU:
+// listed (flag, prefix sum, compaction), then one CTA per row sorts it in
+// shared memory (bitonic, padded to a power of two). Longer rows are sorted
+// on the host.
+constexpr int32_t kSortRow = 4096, kSortBlock = 512;
+struct LongRowFlag {
+  const int64_t *row;
+  int64_t *flag;
+  __host__ __device__ void operator()(int64_t k) const {
+    const int64_t d = row[k + 1] - row[k];
+    flag[k] = d > kSmallRow && d <= kSortRow;
+  }
+};
+struct LongRowList {  // flag holds its exclusive prefix sums (npk + 1 entries)
+  const int64_t *flag;
+  int32_t *list;
+  __host__ __device__ void operator()(int64_t k) const {
+    if (flag[k + 1] != flag[k]) list[flag[k]] = (int32_t)k;
+  }
+};
+__global__ void __launch_bounds__(kSortBlock) sort_rows_kernel(const int64_t *row, const int32_t *list, int64_t nlist,
+                                                                int32_t *col) {
+  __shared__ int32_t buf[kSortRow];
+  for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
+    const int32_t k = list[li];
+    const int64_t e0 = row[k];
+    const int d = (int)(row[k + 1] - e0);
+    int P = 64;
+    while (P < d) P <<= 1;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) buf[i] = i < d ? col[e0 + i] : INT32_MAX;
+    __syncthreads();
+    for (int kk = 2; kk <= P; kk <<= 1)
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+          const int o = i ^ j;
+          if (o > i) {
+            const int32_t x = buf[i], y = buf[o];
+            if ((x > y) == ((i & kk) == 0)) {
+              buf[i] = y;
+              buf[o] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    for (int i = threadIdx.x; i < d; i += blockDim.x) col[e0 + i] = buf[i];
+    __syncthreads();
+  }
+}
+
+inline int64_t DevBackend::sort_rows(const int64_t *row, int32_t *col, int64_t npk) {
+  int64_t *flag = alloc<int64_t>((size_t)npk + 1);
+  each(npk, LongRowFlag{row, flag});
+  each(1, Fill64{flag + npk, 0});
+  const int64_t nlist = scan(flag, npk + 1);
+  if (nlist > 0) {
+    int32_t *list = alloc<int32_t>((size_t)nlist);
+    each(npk, LongRowList{flag, list});
+    const int64_t blocks = std::min<int64_t>(nlist, (int64_t)grid_cap * 2);
+    sort_rows_kernel<<<(unsigned)blocks, kSortBlock, 0, stream>>>(row, list, nlist, col);
+    check(cudaGetLastError(), "sort launch");
+  }
+  return kSortRow;
+}
 
 template <class BE>
 void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clock::time_point t0) {
@@ -1064,11 +1399,11 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   int64_t f0 = 0, f1 = np;
   while (f1 > f0) {
     const int64_t fn = f1 - f0;
-    be.each(fn, PClaim{S, bq, seen, claim, f0});
-    be.each(fn, PCount{S, bq, seen, claim, cnt, f0});
+    be.rows(fn, PClaim{S, bq, seen, claim, f0});
+    be.rows(fn, PCount{S, bq, seen, claim, cnt, f0});
     const int64_t add = be.scan(cnt, fn);  // PEmit reads the starts of positions 0..fn-1 only
     if (f1 + add > npk) throw StepError{BCGPU_EINVAL, "packing BFS: inconsistent frontier"};
-    be.each(fn, PEmit{S, seen, claim, cnt, bq, f0, f1});
+    be.rows(fn, PEmit{S, seen, claim, cnt, bq, f0, f1});
     be.each(add, PMark{bq, seen, f1});
     f0 = f1;
     f1 += add;
@@ -1112,7 +1447,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   int64_t *ccnt = be.template alloc<int64_t>((size_t)nplain_all + 1), *vcnt = be.template alloc<int64_t>((size_t)nplain_all + 1);
   int32_t *bad = be.template alloc<int32_t>(1);
   be.each(1, Fill32{bad, 0});
-  be.each(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, ccnt, vcnt, nullptr, nullptr, nullptr, nullptr,
+  be.rows(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, ccnt, vcnt, nullptr, nullptr, nullptr, nullptr,
                              nullptr, nullptr, nullptr, nullptr, nullptr, nullptr});
   int32_t h_bad = 0;
   be.download(&h_bad, bad, 1);
@@ -1135,7 +1470,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   be.upload(vbase, voff_base.data(), (size_t)np);
   be.upload(nplain, D->n_plain.data(), (size_t)np);
   int32_t *ch = be.template alloc<int32_t>((size_t)nchains * 4);
-  be.each(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, nullptr, nullptr, ccnt, vcnt, vbase, nplain, ch,
+  be.rows(nplain_all, Chains{S, pl, cyc, nid, pbase, vtx_off, bad, nullptr, nullptr, ccnt, vcnt, vbase, nplain, ch,
                              ch + nchains, ch + 2 * nchains, ch + 3 * nchains, nid, old});
   be.each(npk, Unset{old, bad});
   be.download(&h_bad, bad, 1);
@@ -1152,8 +1487,9 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   if (parcs > (int64_t)INT32_MAX * 8) throw StepError{BCGPU_EOVERFLOW, "packed arcs overflow"};
   int32_t *col = be.template alloc<int32_t>((size_t)parcs), *orig = be.template alloc<int32_t>((size_t)npk);
   int32_t *reach = be.template alloc<int32_t>((size_t)npk);
-  be.each(npk, ColFill{S, old, inv, d.head, d.comp, row, d.csize, d.below, d.hang, col, orig, reach});
+  be.rows(npk, ColFill{S, old, inv, d.head, d.comp, row, d.csize, d.below, d.hang, col, orig, reach});
 
+  const int64_t sorted_max = be.sort_rows(row, col, npk);
   step_mark(be, "d: packed csr");
   // to the host; rows longer than kSmallRow are sorted here
   D->row.resize((size_t)npk + 1);
@@ -1177,7 +1513,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   step_mark(be, "d: downloads");
 #pragma omp parallel for schedule(dynamic, 1024)
   for (int64_t k = 0; k < npk; ++k)
-    if (D->row[k + 1] - D->row[k] > kSmallRow) std::sort(D->col.begin() + D->row[k], D->col.begin() + D->row[k + 1]);
+    if (D->row[k + 1] - D->row[k] > sorted_max) std::sort(D->col.begin() + D->row[k], D->col.begin() + D->row[k + 1]);
   step_mark(be, "d: sort");
   std::vector<int32_t> h_cyc((size_t)np);
   be.download(h_cyc.data(), cyc, (size_t)np);
@@ -1186,6 +1522,7 @@ void pack_steps(BE &be, const DevSplit &d, bc_decomp *D, std::chrono::steady_clo
   int32_t n_art = 0;
   be.download(&n_art, d.n_art, 1);
   decomp_finish(D, d.n, (int32_t)d.nroots, (int32_t)d.nbcc, n_art, cycles, t0);
+  step_mark(be, "d: finish");
 }
 
 }  // namespace decomp_steps
@@ -1201,8 +1538,11 @@ int decomp_gpu(const bc_graph *g, int device, bc_decomp *D, std::chrono::steady_
       decomp_steps::HostBackend be;
       decomp_steps::pack_steps(be, decomp_steps::run_split(be, g), D, t0);
     } else {
-      decomp_steps::DevBackend be(device);
-      decomp_steps::pack_steps(be, decomp_steps::run_split(be, g), D, t0);
+      {
+        decomp_steps::DevBackend be(device);
+        decomp_steps::pack_steps(be, decomp_steps::run_split(be, g), D, t0);
+      }
+      HOST_MARK("d: release");
     }
   } catch (const decomp_steps::StepError &e) {
     return fail(e.code, e.what);

@@ -71,12 +71,22 @@ constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
 constexpr int kHalf = 4;           // words per pass over a vertex row
 // Resident CTAs per SM the kernel is compiled for (registers per thread =
 // 65536 / (kThreads * kMinCtas)) and hit values gathered at once per lane in
-// a row pass; profiling builds may override both.
+// a row pass; profiling builds may override both. Six CTAs (40 registers,
+// some spilled to local memory) with the one-arc hit walk measured fastest
+// on RMAT-20 at 512 sources per pass: 135 / 139 / 147 / 124 GTEPS for 4 / 5 /
+// 6 / 8 CTAs per SM.
 #ifndef BCGPU_BATCHED_MIN_CTAS
-#define BCGPU_BATCHED_MIN_CTAS 4
+#define BCGPU_BATCHED_MIN_CTAS 6
 #endif
 #ifndef BCGPU_BATCHED_GATHER
 #define BCGPU_BATCHED_GATHER 4
+#endif
+// Hit walk of a row pass: n >= 1 = an arc is walked once for all kHalf
+// words of the task (one shuffle of its neighbour), n arcs' values loaded at
+// once (n * kHalf loads in flight); 0 = word by word, BCGPU_BATCHED_GATHER
+// hits at a time. The same terms are added in the same order either way.
+#ifndef BCGPU_BATCHED_WALK
+#define BCGPU_BATCHED_WALK 1
 #endif
 constexpr int kMinCtas = BCGPU_BATCHED_MIN_CTAS;
 constexpr int kGatherHits = BCGPU_BATCHED_GATHER;
@@ -391,6 +401,49 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
       f[k] &= filt[k];
       any[k] |= f[k];
     }
+#if BCGPU_BATCHED_WALK
+    uint32_t fo = 0;
+#pragma unroll
+    for (int k = 0; k < kHalf; ++k) fo |= f[k];
+    uint32_t hits = __ballot_sync(0xffffffffu, fo != 0u);
+    // level exponent bases of the task's slots: word k's at xb0 + k * xs
+    const int64_t xs = (int64_t)32 * (a.tcap + 2);
+    const int32_t *xb0 = kLev ? a.X + (int64_t)(w0 * 32 + lane) * (a.tcap + 2) : nullptr;
+    int xt[kHalf];
+#pragma unroll
+    for (int k = 0; k < kHalf; ++k) xt[k] = (kLev && hits) ? __ldcg(xb0 + k * xs + t) : 0;
+    const T *vrow = vals + (int64_t)w0 * 32 + lane;
+    constexpr int kArcs = BCGPU_BATCHED_WALK;  // hit arcs whose values are loaded at once
+    while (hits) {  // uniform: arcs with a hit in some word, in arc order
+      T x[kArcs][kHalf];
+#pragma unroll
+      for (int r = 0; r < kArcs; ++r) {
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) x[r][k] = (T)0;
+        if (!hits) continue;  // uniform
+        const int j = __ffs(hits) - 1;
+        hits &= hits - 1;
+        const int32_t uj = __shfl_sync(0xffffffffu, u, j);
+        const int lj = kLev ? __shfl_sync(0xffffffffu, lvl, j) : 0;
+        const T *vu = vrow + (int64_t)uj * W * 32;
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) {
+          const uint32_t fj = __shfl_sync(0xffffffffu, f[k], j);
+          if ((fj >> lane) & 1u) {
+            x[r][k] = __ldcg(vu + k * 32);
+            if (kLev) {
+              const int xl = __ldcg(xb0 + k * xs + lj);
+              x[r][k] = (T)scale2((double)x[r][k], kLev == 1 ? xl - xt[k] : xt[k] - xl);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kArcs; ++r)
+#pragma unroll
+        for (int k = 0; k < kHalf; ++k) acc[k].add((double)x[r][k]);
+    }
+#else
 #pragma unroll
     for (int k = 0; k < kHalf; ++k) {
       uint32_t hits = __ballot_sync(0xffffffffu, f[k] != 0u);
@@ -418,6 +471,7 @@ __device__ __forceinline__ void row_pass(const Args &a, const uint32_t *masks, c
         for (int r = 0; r < kGatherHits; ++r) acc[k].add((double)x[r]);
       }
     }
+#endif
   }
 }
 
@@ -1757,6 +1811,51 @@ void batched_unit_sources(const BatchedPlan *p, int64_t begin, int64_t end, std:
     const int64_t vo = p->h_vtx_off[bt.bcc];
     for (int32_t i = 0; i < bt.nslots; ++i) out.push_back(vo + p->h_slots[bt.slot_off + i].src);
   }
+}
+
+int batched_pass_shape(const BatchedPlan *p, int64_t pass, int32_t *bcc, int32_t *nslots) {
+  if (!p || pass < 0 || pass >= p->n_batches) return BCGPU_EINVAL;
+  *bcc = p->h_batches[pass].bcc;
+  *nslots = p->h_batches[pass].nslots;
+  return BCGPU_OK;
+}
+
+int batched_pass_rows(const BatchedPlan *p, int64_t pass, const int32_t *chain_start, int32_t n_core,
+                      cudaStream_t stream, std::vector<int32_t> &src, std::vector<int32_t> &d, std::vector<double> &sigma,
+                      std::string *msg) {
+  if (pass < 0 || pass >= p->n_batches) {
+    *msg = "not a multi-source pass";
+    return BCGPU_EINVAL;
+  }
+  const Batch &bt = p->h_batches[pass];
+  const int B = bt.nslots, WB = p->W * 32, L = p->tcap + 2;
+  std::vector<int32_t> hd((size_t)n_core * WB), hx((size_t)WB * L);
+  std::vector<double> hs((size_t)n_core * WB);
+  cudaError_t e = cudaMemcpyAsync(hd.data(), p->args.d, hd.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hs.data(), p->args.sig, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hx.data(), p->args.X, hx.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    *msg = std::string("pass row read-back: ") + cudaGetErrorString(e);
+    return BCGPU_ECUDA;
+  }
+  src.resize((size_t)B);
+  d.resize((size_t)B * n_core);
+  sigma.resize((size_t)B * n_core);
+  for (int b = 0; b < B; ++b) {
+    const Slot &sl = p->h_slots[bt.slot_off + b];
+    src[b] = sl.chain < 0 ? sl.src : chain_start[sl.chain] + sl.pos;
+    for (int32_t v = 0; v < n_core; ++v) {
+      const size_t i = (size_t)v * WB + b;
+      const int lv = hd[i];
+      d[(size_t)b * n_core + v] = lv;
+      // stored count s at level lv stands for s * 2^X(slot, lv)
+      sigma[(size_t)b * n_core + v] = std::ldexp(hs[i], hx[(size_t)b * L + std::min(std::max(lv, 0), L - 1)]);
+    }
+  }
+  return BCGPU_OK;
 }
 
 void batched_unit_work(const BatchedPlan *p, std::vector<int64_t> &sources, std::vector<int64_t> &teps,

@@ -274,6 +274,16 @@ int bc_plan_read(bc_plan *plan, double *bc_out);
  * (BFS, or the chain merge for chain vertices); d_out/sigma_out have the
  * source's BCC size. For parity tests. */
 int bc_plan_source_rows(bc_plan *plan, int64_t packed_source, int32_t *d_out, double *sigma_out);
+/* Multi-source pass `unit` (a unit below the plan's pass count): with null
+ * outputs, its slot count and its BCC's core vertex count only; else the pass
+ * is run (its BC contributions are added like any run's) and read back:
+ * src_out[b] = slot b's source (local id in the BCC), and for each slot b and
+ * core vertex v, d_out[b * ncore + v] its level and sigma_out[b * ncore + v]
+ * its path count with the per-level power-of-two bases applied. For parity
+ * tests of the multi-source form against per-source BFS (the reference keeps
+ * its per-source levels and counts in d_d / sigma_d, Codes/kernels_free.cu:55-62). */
+int bc_plan_pass_rows(bc_plan *plan, int64_t unit, int32_t *nslots, int32_t *ncore, int32_t *src_out, int32_t *d_out,
+                      double *sigma_out);
 
 #ifdef __cplusplus
 }

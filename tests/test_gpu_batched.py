@@ -111,6 +111,46 @@ def test_sigma_rescaling_path():
         c.close()
 
 
+@pytest.mark.parametrize("rescale_exp", [0, 4])
+def test_pass_rows_bit_exact(rescale_exp):
+    """Levels and path counts of the multi-source passes -- every slot, every
+    core vertex of its BCC, read back from the pass's workspace with the
+    per-level power-of-two bases applied -- equal the oracle's per-source BFS
+    rows bit for bit: core sources and chain sources (seeded at both chain
+    ends), on the golden inputs, an RMAT graph with chains and a grid, with the
+    default rescale limit and with a rescale on almost every level (2^4)."""
+    P = pkg()
+    O = oracle()
+    G = graphs()
+    cases = [load_case(name)[:3] for name in GOLDEN_CASES]
+    cases += [G.gen_rmat(10, 8, 0.3, 1, 4, seed=9), G.gen_grid(24, seed=5)]
+    c = ctx_for("fp64", 64, rescale_exp=rescale_exp)
+    checked = 0
+    for n, u, v in cases:
+        d = decomp(n, u, v)
+        arrs = d.arrays()
+        vo = arrs["vtx_off"]
+        plan = c.plan(d)
+        for unit in range(plan.n_units):
+            try:
+                src, dd, ss = plan.pass_rows(unit)
+            except P.BcError:  # the passes are the first units
+                break
+            packed = plan.unit_sources(unit, unit + 1)
+            b = int(np.searchsorted(vo, packed[0], side="right") - 1)
+            ncore = int(arrs["n_plain"][b])
+            assert dd.shape == (len(src), ncore)
+            assert np.array_equal(np.sort(src + vo[b]), np.sort(packed)), (b, unit)
+            for i, s in enumerate(src):
+                do, so = O.bcc_source_rows(arrs, b, int(s))
+                assert np.array_equal(dd[i], do[:ncore]), (b, int(s))
+                assert np.array_equal(ss[i], so[:ncore]), (b, int(s))
+            checked += len(src)
+        plan.close()
+    c.close()
+    assert checked > 1000
+
+
 def test_fp32_range_is_reported():
     """Path counts beyond FP32's range (a 90x90 grid: ~2^174 corner to corner)
     make the compensated-FP32 mode fail loudly instead of returning wrong BC;

@@ -550,7 +550,10 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     """The drop-in command's options, output format and exit codes, with the
     in-tree betc loading the stand-in library (its RUNPATH yields to
     LD_LIBRARY_PATH): `v bc` per vertex to --out, usage errors (1), unreadable
-    input (2), a rejected option value (4), an unwritable output (6)."""
+    input (2), a rejected option value (4), an unwritable output (6). The
+    decomposition runs on the host (--host-decomp): the stand-in runtime runs
+    no kernels, so the default GPU decomposition stops with its own error
+    (exit 3) instead."""
     from helpers import GOLDEN
 
     betc = PKG / "lib" / "betc"
@@ -565,14 +568,16 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     out = tmp_path / "bc.txt"
     for extra in ([], ["--mode", "plain"], ["--mode", "batched", "--delta", "fp64", "--batch", "64"],
                   ["--mode", "plain", "--plain-ctas", "16"]):
-        r = run(g, "--out", out, *extra)
+        r = run(g, "--out", out, "--host-decomp", *extra)
         assert r.returncode == 0, r.stderr
         assert "GPU total time is" in r.stderr
         rows = [ln.split() for ln in out.read_text().splitlines()]
         assert [int(a) for a, _ in rows] == list(range(n))
         [float(b) for _, b in rows]
-    r = run(g, "--quiet")
+    r = run(g, "--quiet", "--host-decomp")
     assert r.returncode == 0 and len(r.stdout.splitlines()) == n
+    r = run(g, "--quiet")
+    assert r.returncode == 3 and "GPU decomposition failed" in r.stderr
     assert run().returncode == 1
     assert run(g, "--mode", "bogus").returncode == 1
     assert run(g, "--delta").returncode == 1  # option without its value
@@ -583,7 +588,7 @@ def test_betc_cli_options_and_exit_codes(stub_dir, tmp_path):
     assert r.returncode == 4 and "multiple of 32" in r.stderr
     r = run(g, "--plain-ctas", "3")
     assert r.returncode == 4 and "plain_ctas_per_sm" in r.stderr
-    r = run(g, "--out", tmp_path / "no" / "such" / "dir.txt")
+    r = run(g, "--out", tmp_path / "no" / "such" / "dir.txt", "--host-decomp")
     assert r.returncode == 6
 
 
@@ -625,10 +630,11 @@ def test_betc_reads_the_csr_it_saved(stub_dir, tmp_path):
     betc = PKG / "lib" / "betc"
     env = dict(os.environ, LD_LIBRARY_PATH=str(stub_dir))
     csr = tmp_path / "g.csr"
-    a = subprocess.run([str(betc), str(GOLDEN / "small2000.txt"), "--save-csr", str(csr), "--quiet"], env=env,
-                       capture_output=True, text=True, timeout=120)
+    a = subprocess.run([str(betc), str(GOLDEN / "small2000.txt"), "--save-csr", str(csr), "--quiet", "--host-decomp"],
+                       env=env, capture_output=True, text=True, timeout=120)
     assert a.returncode == 0, a.stderr
-    b = subprocess.run([str(betc), str(csr), "--quiet"], env=env, capture_output=True, text=True, timeout=120)
+    b = subprocess.run([str(betc), str(csr), "--quiet", "--host-decomp"], env=env, capture_output=True, text=True,
+                       timeout=120)
     assert b.returncode == 0, b.stderr
     assert a.stdout == b.stdout and len(a.stdout.splitlines()) == 2000
     r = subprocess.run([str(betc), str(GOLDEN / "sample1.txt"), "--save-csr", str(tmp_path / "no" / "x.csr")], env=env,
@@ -694,13 +700,41 @@ c.close()
     assert res["range"][0] == 1 and res["batched"][0] == 1 and "PLAIN" in res["batched"][1]
 
 
+def test_pass_rows_arguments(stub_dir):
+    """Multi-source row export (for the parity tests): the arrays have one row
+    per slot of the pass and one column per core vertex of its BCC, the slots'
+    sources are the pass's sources; a unit that is not a multi-source pass (a
+    per-source unit, one beyond the plan, a PLAIN plan's) is BCGPU_EINVAL."""
+    res = run_stub(stub_dir, """
+n, u, v = G.gen_small(1)
+d = decomp(n, u, v)
+a = d.arrays()
+c = P.Context(mode=P.MODE_BATCHED, plain_core=-1, batch_width=64)
+plan = c.plan(d)
+src, dd, ss = plan.pass_rows(0)
+out["shape"] = [len(src), list(dd.shape), list(ss.shape), int(a["n_plain"][0])]
+out["same_sources"] = sorted((src + int(a["vtx_off"][0])).tolist()) == sorted(plan.unit_sources(0, 1).tolist())
+out["beyond"] = raises(lambda: plan.pass_rows(plan.n_units))
+plan.close()
+c.close()
+c = P.Context(mode=P.MODE_PLAIN)
+plan = c.plan(d)
+out["plain"] = raises(lambda: plan.pass_rows(0))
+plan.close()
+c.close()
+""")
+    ns, dshape, sshape, ncore = res["shape"]
+    assert ns == 64 and dshape == [64, ncore] and sshape == [64, ncore] and res["same_sources"]
+    assert res["beyond"][0] == 1 and res["plain"][0] == 1 and "multi-source" in res["plain"][1]
+
+
 @pytest.mark.parametrize("mode", ["batched", "plain"])
 def test_bench_main_arm_line(stub_dir, tmp_path, mode):
     """bench.py's main arm runs end to end on the stand-in runtime (torch.cuda
     stood in by tests/stub_cudart/torch_cuda_stub.py) and prints one JSON line
     with every key of the contract; the numbers are meaningless here."""
     args = ["--workload", "small", "--steps", "3", "--warmup", "3", "--plain-waves", "1", "--e2e-steps", "1",
-            "--mode", mode]
+            "--mode", mode, "--host-decomp"]  # the stand-in runtime runs no decomposition kernels
     env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir))
     r = subprocess.run([sys.executable, str(STUB / "bench_on_stub.py")] + args, env=env, capture_output=True,
                        text=True, timeout=600, cwd=tmp_path)
@@ -735,7 +769,7 @@ def test_bench_two_ranks_under_torchrun(stub_dir, tmp_path):
         port = sock.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(STUB / "bench_on_stub.py"),
-           "--gpus", "2", "--workload", "small", "--steps", "3", "--warmup", "3", "--e2e-steps", "1"]
+           "--gpus", "2", "--workload", "small", "--steps", "3", "--warmup", "3", "--e2e-steps", "1", "--host-decomp"]
     env = dict(os.environ, BCGPU_LIB_DIR=str(stub_dir), BCGPU_DIST_BACKEND="gloo", OMP_NUM_THREADS="2")
     r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600, cwd=tmp_path)
     assert r.returncode == 0, r.stderr[-3000:]
