@@ -89,6 +89,13 @@ constexpr int kHalf = 4;           // words per pass over a vertex row
 #define BCGPU_BATCHED_WALK 1
 #endif
 constexpr int kMinCtas = BCGPU_BATCHED_MIN_CTAS;
+// Light-row tasks per warp and level at least (smaller vertex blocks when
+// the core is small), so the slowest tasks at a level's end are short: on
+// RMAT-20 (512 sources per pass) 8 / 16 / 32 gave 147.2 / 150.4 / 151.8 GTEPS.
+#ifndef BCGPU_BATCHED_TASKS
+#define BCGPU_BATCHED_TASKS 32
+#endif
+constexpr int kTasksPerWarp = BCGPU_BATCHED_TASKS;
 constexpr int kGatherHits = BCGPU_BATCHED_GATHER;
 
 // One source of a pass. chain < 0: the core vertex src (level 0). Otherwise
@@ -671,7 +678,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
     // on large cores, smaller ones on small cores so that every warp of the
     // grid gets work on a level.
     const int halves = wpad / kHalf;
-    const int64_t bs_want = ((int64_t)n * halves + nwarps() * 8 - 1) / (nwarps() * 8);
+    const int64_t bs_want = ((int64_t)n * halves + nwarps() * kTasksPerWarp - 1) / (nwarps() * kTasksPerWarp);
     const int bs = bs_want >= 32 ? 32 : bs_want < 1 ? 1 : (int)bs_want;
     const int64_t nblk = ((int64_t)n + bs - 1) / bs;
     const int64_t ntask = nblk * halves;
