@@ -67,7 +67,10 @@ constexpr int kWarpsPerCta = kThreads / 32;
 constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs ...
 constexpr int kHeavyDegSmall = 32; // ... or than this, on cores small enough that one row is a level's critical path
 constexpr int kSmallCore = 16384;  // cores below this many vertices use kHeavyDegSmall
-constexpr int kChunkArcs = 2048;   // arcs per heavy chunk
+#ifndef BCGPU_BATCHED_CHUNK
+#define BCGPU_BATCHED_CHUNK 2048
+#endif
+constexpr int kChunkArcs = BCGPU_BATCHED_CHUNK;  // arcs per heavy chunk
 constexpr int kHalf = 4;           // words per pass over a vertex row
 // Resident CTAs per SM the kernel is compiled for (registers per thread =
 // 65536 / (kThreads * kMinCtas)) and hit values gathered at once per lane in
@@ -171,7 +174,7 @@ struct Args {
   int32_t *lmin, *lmax;
   int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
   int32_t *armed;   // [n_cap] first level on which some slot can reach the vertex (a neighbour was reached)
-  int *wq;          // [2*(tcap+3)] work counters of the forward (t) and backward (tcap+3+lev) phases
+  int *wq;          // [4*(tcap+3)] work counters: light rows forward (t), backward (tcap+3+lev); heavy chunks (2*(tcap+3)+t, 3*(tcap+3)+lev)
   double *bcpart;   // [n_cap][W] BC partials of the core vertices
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
   double *wsrc;     // [B] reach(source)+1 of each slot of the pass
@@ -636,6 +639,25 @@ __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
   return nwarps() + __shfl_sync(0xffffffffu, b, 0);
 }
 
+// Heavy-row chunk tasks of a phase: each CTA's first task is its own index;
+// later ones in a fixed stride (BCGPU_BATCHED_HEAVY_DYN 0) or from the
+// phase's work counter (1: a CTA that drew short chunks takes more).
+#ifndef BCGPU_BATCHED_HEAVY_DYN
+#define BCGPU_BATCHED_HEAVY_DYN 0
+#endif
+__device__ __forceinline__ int64_t next_chunk_task(int64_t task, int *counter) {
+#if BCGPU_BATCHED_HEAVY_DYN
+  __shared__ int s_next;
+  __syncthreads();  // every thread has read the previous s_next
+  if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+  __syncthreads();
+  return (int64_t)gridDim.x + s_next;
+#else
+  (void)counter;
+  return task + gridDim.x;
+#endif
+}
+
 }  // namespace
 
 // --------------------------------------------------------------- kernel ----
@@ -698,7 +720,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       a.X[i * (a.tcap + 2)] = 0;
       a.wsrc[i] = i < bt.nslots ? (double)rch[slots[i].src] + 1.0 : 0.0;
     }
-    for (int64_t i = gtid; i < 2 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
+    for (int64_t i = gtid; i < 4 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
     if (gtid == 0) {
       a.ctrl->more[0] = a.ctrl->more[1] = 0;
       a.ctrl->rescale[0] = a.ctrl->rescale[1] = 0;
@@ -740,7 +762,8 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       for (int64_t i = gtid; i < (int64_t)n * W; i += gthreads) a.lm[(int64_t)(t + 2) * a.n_cap * W + i] = 0;
       // heavy rows: chunks of their arcs, one CTA per (chunk, half); partials
       // are combined across the CTA's warps, then across chunks after the barrier
-      for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
+      for (int64_t task = blockIdx.x; task < nchunks * halves;
+           task = next_chunk_task(task, a.wq + 2 * (a.tcap + 3) + t)) {
         const int64_t c = task / halves;
         const int w0 = (int)(task % halves) * kHalf;
         const int nw = min(kHalf, wpad - w0);
@@ -941,7 +964,8 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       const uint32_t *lm_next = a.lm + (int64_t)(lev + 1) * a.n_cap * W;
       const QT *q = reinterpret_cast<const QT *>(a.q);
       // heavy rows: chunked successor sums, combined below
-      for (int64_t task = blockIdx.x; task < nchunks * halves; task += gridDim.x) {
+      for (int64_t task = blockIdx.x; task < nchunks * halves;
+           task = next_chunk_task(task, a.wq + 3 * (a.tcap + 3) + lev)) {
         const int64_t c = task / halves;
         const int w0 = (int)(task % halves) * kHalf;
         const int nw = min(kHalf, wpad - w0);
@@ -1639,7 +1663,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.armed = (int32_t *)p;
-  ok &= ok && alloc(&p, 2 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
+  ok &= ok && alloc(&p, 4 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 8); a.wsrc = (double *)p;
