@@ -641,9 +641,10 @@ __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
 
 // Heavy-row chunk tasks of a phase: each CTA's first task is its own index;
 // later ones in a fixed stride (BCGPU_BATCHED_HEAVY_DYN 0) or from the
-// phase's work counter (1: a CTA that drew short chunks takes more).
+// phase's work counter (1: a CTA that drew short chunks takes more; 153.0
+// against 151.3-151.4 GTEPS on RMAT-20 at 512 sources per pass).
 #ifndef BCGPU_BATCHED_HEAVY_DYN
-#define BCGPU_BATCHED_HEAVY_DYN 0
+#define BCGPU_BATCHED_HEAVY_DYN 1
 #endif
 __device__ __forceinline__ int64_t next_chunk_task(int64_t task, int *counter) {
 #if BCGPU_BATCHED_HEAVY_DYN
