@@ -64,7 +64,13 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarpsPerCta = kThreads / 32;
-constexpr int kHeavyDeg = 256;     // core rows longer than this are scanned in chunks by whole CTAs ...
+// Core rows longer than kHeavyDeg arcs are scanned in chunks by whole CTAs
+// (RMAT-20 at 512 sources per pass: 143.7 / 153.7 / 160.4 / 160.4 / 162.3 /
+// 156.1 GTEPS for 128 / 256 / 512 / 1024 / 2048 / 4096) ...
+#ifndef BCGPU_BATCHED_HEAVY_DEG
+#define BCGPU_BATCHED_HEAVY_DEG 1024
+#endif
+constexpr int kHeavyDeg = BCGPU_BATCHED_HEAVY_DEG;
 constexpr int kHeavyDegSmall = 32; // ... or than this, on cores small enough that one row is a level's critical path
 constexpr int kSmallCore = 16384;  // cores below this many vertices use kHeavyDegSmall
 #ifndef BCGPU_BATCHED_CHUNK
