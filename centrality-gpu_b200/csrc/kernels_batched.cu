@@ -180,7 +180,7 @@ struct Args {
   int32_t *lmin, *lmax;
   int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
   int32_t *armed;   // [n_cap] first level on which some slot can reach the vertex (a neighbour was reached)
-  int *wq;          // [4*(tcap+3)] work counters: light rows forward (t), backward (tcap+3+lev); heavy chunks (2*(tcap+3)+t, 3*(tcap+3)+lev)
+  int *wq;          // [4*(tcap+3)+1] work counters: light rows forward (t), backward (tcap+3+lev); heavy chunks (2*(tcap+3)+t, 3*(tcap+3)+lev); chain in-flow (4*(tcap+3))
   double *bcpart;   // [n_cap][W] BC partials of the core vertices
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
   double *wsrc;     // [B] reach(source)+1 of each slot of the pass
@@ -652,6 +652,11 @@ __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
 #ifndef BCGPU_BATCHED_HEAVY_DYN
 #define BCGPU_BATCHED_HEAVY_DYN 1
 #endif
+// Chain in-flow tasks (core vertex, word): a fixed warp stride (0) or a
+// work counter (1), as the light rows.
+#ifndef BCGPU_BATCHED_CHAININ_DYN
+#define BCGPU_BATCHED_CHAININ_DYN 0
+#endif
 __device__ __forceinline__ int64_t next_chunk_task(int64_t task, int *counter) {
 #if BCGPU_BATCHED_HEAVY_DYN
   __shared__ int s_next;
@@ -727,7 +732,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       a.X[i * (a.tcap + 2)] = 0;
       a.wsrc[i] = i < bt.nslots ? (double)rch[slots[i].src] + 1.0 : 0.0;
     }
-    for (int64_t i = gtid; i < 4 * ((int64_t)a.tcap + 3); i += gthreads) a.wq[i] = 0;
+    for (int64_t i = gtid; i < 4 * ((int64_t)a.tcap + 3) + 1; i += gthreads) a.wq[i] = 0;
     if (gtid == 0) {
       a.ctrl->more[0] = a.ctrl->more[1] = 0;
       a.ctrl->rescale[0] = a.ctrl->rescale[1] = 0;
@@ -954,7 +959,11 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
     }
     // what the core vertices receive from their chains' vertices
     if (bt.kmax) {
+#if BCGPU_BATCHED_CHAININ_DYN
+      for (int64_t task = gwarp(); task < (int64_t)n * words; task = next_block(a.wq + 4 * (a.tcap + 3), lane)) {
+#else
       for (int64_t task = gwarp(); task < (int64_t)n * words; task += nwarps()) {
+#endif
         const int32_t v = (int32_t)(task / words);
         const int w = (int)(task % words);
         const int64_t c0 = HS[v], c1 = HR[v + 1];
@@ -1670,7 +1679,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.armed = (int32_t *)p;
-  ok &= ok && alloc(&p, 4 * ((int64_t)tcap + 3) * 4); a.wq = (int *)p;
+  ok &= ok && alloc(&p, (4 * ((int64_t)tcap + 3) + 1) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 8); a.wsrc = (double *)p;
