@@ -180,7 +180,7 @@ struct Args {
   int32_t *lmin, *lmax;
   int32_t *gdone;   // [n_cap] groups of 4 words already seen by all their slots (a lower bound)
   int32_t *armed;   // [n_cap] first level on which some slot can reach the vertex (a neighbour was reached)
-  int *wq;          // [4*(tcap+3)+1] work counters: light rows forward (t), backward (tcap+3+lev); heavy chunks (2*(tcap+3)+t, 3*(tcap+3)+lev); chain in-flow (4*(tcap+3))
+  int *wq;          // [4*(tcap+3)+2] work counters: light rows forward (t), backward (tcap+3+lev); heavy chunks (2*(tcap+3)+t, 3*(tcap+3)+lev); chain in-flow (4*(tcap+3)); chain vertices (4*(tcap+3)+1)
   double *bcpart;   // [n_cap][W] BC partials of the core vertices
   double *cdep;     // [n_cap][W][32] dependency a core vertex receives from its chains' vertices
   double *wsrc;     // [B] reach(source)+1 of each slot of the pass
@@ -653,9 +653,15 @@ __device__ __forceinline__ int64_t next_block(int *counter, int lane) {
 #define BCGPU_BATCHED_HEAVY_DYN 1
 #endif
 // Chain in-flow tasks (core vertex, word): a fixed warp stride (0) or a
-// work counter (1), as the light rows.
+// work counter (1), as the light rows (168.7 against 161.9 GTEPS on
+// RMAT-20: a hub's words carry thousands of chain arcs each). Chain-vertex
+// tasks (one chain, every word) likewise (BCGPU_BATCHED_CHAINV_DYN: 167.9-
+// 168.0 against 165.5).
 #ifndef BCGPU_BATCHED_CHAININ_DYN
-#define BCGPU_BATCHED_CHAININ_DYN 0
+#define BCGPU_BATCHED_CHAININ_DYN 1
+#endif
+#ifndef BCGPU_BATCHED_CHAINV_DYN
+#define BCGPU_BATCHED_CHAINV_DYN 1
 #endif
 __device__ __forceinline__ int64_t next_chunk_task(int64_t task, int *counter) {
 #if BCGPU_BATCHED_HEAVY_DYN
@@ -732,7 +738,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       a.X[i * (a.tcap + 2)] = 0;
       a.wsrc[i] = i < bt.nslots ? (double)rch[slots[i].src] + 1.0 : 0.0;
     }
-    for (int64_t i = gtid; i < 4 * ((int64_t)a.tcap + 3) + 1; i += gthreads) a.wq[i] = 0;
+    for (int64_t i = gtid; i < 4 * ((int64_t)a.tcap + 3) + 2; i += gthreads) a.wq[i] = 0;
     if (gtid == 0) {
       a.ctrl->more[0] = a.ctrl->more[1] = 0;
       a.ctrl->rescale[0] = a.ctrl->rescale[1] = 0;
@@ -1085,7 +1091,11 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) batched_kernel(Args a) {
       const int bad = *(volatile int *)&a.ctrl->range_err;
       const int64_t ch0 = a.chain_off[bt.bcc];
       const int64_t nch = a.chain_off[bt.bcc + 1] - ch0;
+#if BCGPU_BATCHED_CHAINV_DYN
+      for (int64_t task = gwarp(); task < nch; task = next_block(a.wq + 4 * (a.tcap + 3) + 1, lane)) {
+#else
       for (int64_t task = gwarp(); task < nch; task += nwarps()) {
+#endif
         const int64_t c = ch0 + task;
         const int32_t L = a.chain_l[c], R = a.chain_r[c], cs = a.chain_start[c], k = a.chain_len[c];
         const int64_t poff = a.cpre_off[c];
@@ -1679,7 +1689,7 @@ int batched_build(const bc_bccs *B, const BatchedConfig &cfg, const int64_t *row
   ok &= ok && alloc(&p, n * 4); a.lmax = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.gdone = (int32_t *)p;
   ok &= ok && alloc(&p, n * 4); a.armed = (int32_t *)p;
-  ok &= ok && alloc(&p, (4 * ((int64_t)tcap + 3) + 1) * 4); a.wq = (int *)p;
+  ok &= ok && alloc(&p, (4 * ((int64_t)tcap + 3) + 2) * 4); a.wq = (int *)p;
   ok &= ok && alloc(&p, n * W * 8); a.bcpart = (double *)p;
   ok &= ok && alloc(&p, n * W * 32 * 8); a.cdep = (double *)p;
   ok &= ok && alloc(&p, (int64_t)W * 32 * 8); a.wsrc = (double *)p;
